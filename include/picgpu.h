@@ -1,0 +1,289 @@
+/*
+ * picgpu.h -- C-ABI of the B200 IFE-PIC step library (libpicgpu.so).
+ *
+ * Every entry point is plain C: pointers, sizes, return codes.  No torch or
+ * CUDA types cross this boundary, so a Fortran main program binds it with
+ * ISO_C_BINDING and Python binds it with ctypes.
+ *
+ * Each entry point names the reference subroutine it replaces.  Paths are
+ * relative to the PIC-IFE_GEC project of weqwoueu/pic-.
+ *
+ * Conventions
+ *  - Node n of an nnx x nny uniform mesh is n = i*nny + j (0-based i, j);
+ *    its Fortran id is n+1 = (i-1)*nny + j with 1-based i, j
+ *    (code/IFE-Rectangular/Cubic_Partition_2D.f90:60-66).
+ *  - Element e = i*(nny-1) + j; Fortran id e+1 = j + (i-1)*(nny-1); corners
+ *    HT(1:4,e) = (i,j), (i+1,j), (i+1,j+1), (i,j+1)
+ *    (code/IFE-Rectangular/Cubic_Partition_2D.f90:70-90).
+ *  - Index tables handed to pic_init (CSR rows/columns, patches) are 1-based
+ *    like the Fortran arrays they mirror; they are converted once at init.
+ *  - Return value 0 = ok, negative = error class (PIC_ERR_*).  Details of
+ *    the last failure are in pic_last_error().  Nothing calls exit/abort.
+ *  - Not re-entrant: one context per process, one CUDA device, one stream.
+ */
+#ifndef PICGPU_H
+#define PICGPU_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define PIC_OK 0
+#define PIC_ERR_ARG (-1)        /* bad argument or size                 */
+#define PIC_ERR_CUDA (-2)       /* CUDA runtime / launch failure        */
+#define PIC_ERR_SOLVER_CAP (-3) /* PCG reached its iteration cap        */
+#define PIC_ERR_NAN (-4)        /* NaN/Inf in a field or residual       */
+#define PIC_ERR_DOMAIN (-5)     /* particle outside the mesh            */
+#define PIC_ERR_STATE (-6)      /* call out of order (no init, ...)     */
+#define PIC_ERR_CAPACITY (-7)   /* particle array capacity exceeded     */
+#define PIC_ERR_SETUP (-8)      /* geometry the mesh builder rejects    */
+#define PIC_ERR_BREAKDOWN (-9)  /* PCG breakdown (rho or p.Ap == 0)     */
+
+#define PIC_MAX_SPECIES 4
+#define PIC_MAX_OBJECTS 32
+#define PIC_MAX_REACTIONS 8
+
+/* Object shapes, same codes as objects(i)%Shape in INPUT/object.inp. */
+#define PIC_SHAPE_CIRCLE 1
+#define PIC_SHAPE_BOX 3
+#define PIC_SHAPE_ELLIPSE 5
+
+/* Wall treatment of particles (MCC_jw/code/Interface_IFE/MCCInterface.f90:361-532). */
+#define PIC_WALL_ABSORB 0
+#define PIC_WALL_REFLECT 1
+
+/* Arithmetic of the step. */
+#define PIC_PREC_FP64 0  /* plain FP64 path                                  */
+#define PIC_PREC_MIXED 1 /* FP32 cell-relative push, FP32 PCG in FP64 refine */
+
+/* Linear solver of pic_ife_solve. */
+#define PIC_SOLVER_JPCG 0 /* Jacobi-PCG, MY_PCG.f90                   */
+#define PIC_SOLVER_FCG_UNET 1 /* flexible CG with the learned preconditioner */
+
+typedef struct pic_object {
+  int32_t shape;     /* PIC_SHAPE_*                                          */
+  int32_t conductor; /* 1: nodes inside are Dirichlet at phi                 */
+  double cx, cy;     /* centre (circle/ellipse) or lower-left corner (box)   */
+  double a, b;       /* radius (a); ellipse semi-axes; box upper-right (a,b) */
+  double angle;      /* ellipse rotation (rad)                               */
+  double eps;        /* relative permittivity inside (objects(i)%Eps)        */
+  double phi;        /* normalised potential of a conductor                  */
+} pic_object;
+
+/* Deck for the host-side mesh builder (Setup_IFE_Mesh_2D + IFE_Start_2D +
+ * Get_PointPatch).  Lengths and potentials are normalised (L_ref, Phi_ref). */
+typedef struct pic_deck {
+  int32_t nnx, nny;            /* nodes per direction                        */
+  double xmin, xmax, ymin, ymax;
+  int32_t delta;               /* 0 Cartesian (1 axisymmetric: not built)    */
+  int32_t wall_dirichlet[4];   /* left, right, bottom, top: 1 Dirichlet       */
+  double wall_phi[4];          /* Dirichlet values                            */
+  int32_t n_objects;
+  pic_object objects[PIC_MAX_OBJECTS];
+} pic_deck;
+
+/* Arrays the reference holds after its setup phase (IFE_Data module). */
+typedef struct pic_mesh_desc {
+  int32_t nnx, nny;
+  double xmin, xmax, ymin, ymax;
+  int32_t delta;
+  const int32_t *node_type;     /* [nodes] node_type(2,:): >0 unknown id, <0 Dirichlet */
+  const int32_t *node_index;    /* [nodes] -1 outside objects, object region (<=-2) inside */
+  const int32_t *element_index; /* [elems] -1 outside, <=-2 inside object, >0 interface id */
+  const double *phi_dirichlet;  /* [nodes] potential on Dirichlet nodes          */
+  const double *cell_volume;    /* [nodes] Cell_Volume_zwz(2,:)                  */
+  int32_t n_unknowns;
+  int64_t nnz;
+  const int32_t *a_srow;   /* [n_unknowns+1] 1-based (SPARSE%SROW of A_stiff)   */
+  const int32_t *a_jcol;   /* [nnz] 1-based unknown ids (SPARSE%JCOL)           */
+  const double *a_k;       /* [nnz] (SPARSE%K)                                  */
+  int64_t nnz_xt;
+  const int32_t *xt_srow;  /* [n_unknowns+1] A_stiff_xt rows                    */
+  const int32_t *xt_jcol;  /* [nnz_xt] 1-based NODE ids of Dirichlet columns    */
+  const double *xt_k;
+  const double *a_diag;    /* [n_unknowns] Jacobi diagonal A_diag               */
+  const double *rhs_fix;   /* [n_unknowns] rhs_FIX (Neumann), may be NULL       */
+  const double *mass_q1;   /* [16] Q1 element load matrix, row j col k          */
+  int32_t n_interface;
+  const double *ife_mass;  /* [n_interface*16] interface-element load matrices  */
+  const int32_t *patch_ptr;   /* [nodes+1] 0-based offsets into patch_nodes      */
+  const int32_t *patch_nodes; /* 1-based node ids (point_patch(i,2:))             */
+  int32_t n_objects;
+  const pic_object *objects;
+} pic_mesh_desc;
+
+typedef struct pic_species_desc {
+  double charge;      /* qs, units of e                                      */
+  double mass;        /* kg                                                  */
+  double weight;      /* real particles per macro-particle (ParticleBundle%Weight) */
+  int64_t capacity;   /* particle slots to reserve in HBM                    */
+} pic_species_desc;
+
+typedef struct pic_params {
+  int32_t n_species;
+  pic_species_desc species[PIC_MAX_SPECIES];
+  double dt;          /* normalised time step                                */
+  double n_ref;       /* m^-3                                                */
+  double T_ref_eV;    /* eV                                                  */
+  double pcg_tol;     /* relative residual ||r||/||b|| (PCG_Tol)             */
+  int32_t pcg_maxit;  /* PCG_MaxIT                                           */
+  int32_t wall_bc[4]; /* particle treatment at left, right, bottom, top      */
+  uint64_t seed;      /* Philox key                                          */
+  int32_t precision;  /* PIC_PREC_*                                          */
+  int32_t sort_interval; /* counting sort every k steps in pic_step (>=1)    */
+  int32_t solver;     /* PIC_SOLVER_*                                        */
+} pic_params;
+
+/* One MCC_jw collision bundle (Type MCCBundle, mc/TypeMCC.f90:9-20). */
+typedef struct pic_mcc_table {
+  int32_t species;       /* colliding species                                */
+  int32_t n_reaction;
+  int32_t n_sigma;
+  double energy_min;     /* log10(eV) of the first grid point                */
+  double energy_interval;/* log10 step                                       */
+  double energy_max;     /* eV of the last grid point                        */
+  double collision_ratio;/* P_null = 1 - exp(-nu_max dt)                     */
+  int32_t reaction_type[PIC_MAX_REACTIONS]; /* 11,12,13 (e-) or 101,103 (ion) */
+  double threshold[PIC_MAX_REACTIONS];      /* eV                              */
+  int32_t resultant[PIC_MAX_REACTIONS];     /* species created (ionisation)    */
+  const double *probability; /* [n_sigma*n_reaction] cumulative, normalised  */
+} pic_mcc_table;
+
+typedef struct pic_gas {
+  double mass;        /* kg                                                   */
+  double temperature; /* K                                                    */
+  double density;     /* m^-3                                                 */
+} pic_gas;
+
+typedef struct pic_solve_stats {
+  int32_t iterations;     /* PCG iterations performed                        */
+  int32_t ierr;           /* MY_PCG IERR: 0 ok, 1 cap, 2 rho0==0, 3 p.Ap==0   */
+  double rel_residual;    /* sqrt(normR/normRHS) at exit                      */
+  double ms;              /* device time of the solve                         */
+  int32_t fallback;       /* 1 when the learned FCG fell back to Jacobi-PCG   */
+  int32_t outer;          /* FP64 refinement sweeps (mixed precision)         */
+} pic_solve_stats;
+
+typedef struct pic_mcc_stats {
+  int64_t n_selected[PIC_MAX_SPECIES];
+  int64_t n_by_reaction[PIC_MAX_SPECIES][PIC_MAX_REACTIONS];
+  int64_t n_created[PIC_MAX_SPECIES];
+} pic_mcc_stats;
+
+typedef struct pic_step_stats {
+  int64_t n_particles[PIC_MAX_SPECIES]; /* live after the step                */
+  int64_t n_lost[PIC_MAX_SPECIES];      /* absorbed this step                 */
+  pic_solve_stats solve;
+  pic_mcc_stats mcc;
+  double ms_push, ms_solve, ms_ppr, ms_mcc, ms_sort, ms_total;
+  double ms_push_kernel;  /* device time of the fused push kernels alone      */
+  int64_t pushed;         /* particles pushed (live at the start of the step) */
+} pic_step_stats;
+
+/* ---- mesh builder (host C++; replaces the reference's setup chain) ---- */
+
+/* Builds the arrays of pic_mesh_desc from a deck:
+ *   Partition_Cube_2D.f90 (node_type), Cubic_Partition_2D.f90 (HP/HT),
+ *   El_Object_Intersection_info_2D_BL.f90 (interface elements),
+ *   Generate_stiffness_matrix_local_IFE.f90 + IFE_Start_2D.f90:320-479 (CSR),
+ *   Global_RHS_PDE_2D.f90 / IFE_RHS_2D.f90 (load matrices),
+ *   SetupGrids_2D_QLL.f90:197-330 (Cell_Volume_zwz), Get_PointPatch.f90.
+ * On success *out points at storage owned by the library until
+ * pic_mesh_free(*out). */
+int pic_mesh_build(const pic_deck *deck, pic_mesh_desc **out);
+void pic_mesh_free(pic_mesh_desc *mesh);
+/* Interface-element geometry for diagnostics/tests: per interface element
+ * (1-based id k) the element number, type (1 corner cut, 2 opposite edges),
+ * reference-vertex map pointer_reference_to_local(1:4), beta1, beta2, D, E. */
+int pic_mesh_interface_info(const pic_mesh_desc *mesh, int32_t k, int32_t *element,
+                            int32_t *type, int32_t *ref_to_local, double *beta,
+                            double *d, double *e);
+/* Q1 IFE basis of interface element k (Retangular_local_basis_IFE.f90):
+ * value and gradient of local basis `basis` (0..3, HT order) at (x, y). */
+int pic_mesh_ife_basis(const pic_mesh_desc *mesh, int32_t k, int32_t basis, double x,
+                       double y, double *value, double *dx, double *dy);
+
+/* ---- device context ---- */
+
+/* pic_init: copies the mesh tables to HBM, splits the stiffness into the
+ * regular Q1 stencil and explicit interface/boundary rows, builds the PPR
+ * pseudo-inverse rows, allocates particle storage.  Replaces the module
+ * state set up before Main_IFE_Test_2.f90:278. */
+int pic_init(const pic_mesh_desc *mesh, const pic_params *params);
+void pic_finalize(void);
+const char *pic_last_error(void);
+
+/* MCC_jw tables (MCCInit.F90:29-152) and gas, one table per colliding species. */
+int pic_mcc_init(const pic_gas *gas, int32_t n_tables, const pic_mcc_table *tables);
+
+/* Particle bundle I/O (ParticleBundle%Dump/Load, ParticleBundle.f90:286-375).
+ * id may be NULL (ids 0..n-1 are assigned); loc may be NULL (located on upload). */
+int pic_upload_particles(int32_t species, int64_t n, const double *x, const double *y,
+                         const double *vx, const double *vy, const double *vz,
+                         const int32_t *loc, const uint32_t *id);
+/* Copies the live particles in device order.  Any output pointer may be NULL. */
+int pic_download_particles(int32_t species, int64_t capacity, double *x, double *y,
+                           double *vx, double *vy, double *vz, int32_t *loc,
+                           uint32_t *id, int64_t *n_out);
+int pic_particle_count(int32_t species, int64_t *n);
+
+/* ParticlePositioning / InjectPositioning (ParticlePositioning.f90,
+ * InjectPositioning.f90:1-24, call site GetParChg_2D.f90:137-163):
+ * element of every particle of `species` (-1 for all species). */
+int pic_particle_positioning(int32_t species);
+
+/* Counting sort of `species` by element, ties by particle id; drops
+ * absorbed particles (ParticleBundle%DelOne swap-with-last, ParticleBundle.f90:120-127). */
+int pic_sort_particles(int32_t species);
+
+/* MoveAll (MCCInterface.f90:574-640) -> MoveOne (IMPIC/MoveOne.f90) with
+ * Get_ParticleEField_PPR (PPR/Get_ParticleEField_PPR.f90) and
+ * AdjustParticleBoundary (MCCInterface.f90:217-534).  push_flag as MoveAll. */
+int pic_move_all(int32_t species, int32_t push_flag);
+
+/* GetParChg_2D (PIC/GetParChg_2D.f90:1-911): locate, int64 fixed-point
+ * bilinear deposit, normalisation by the dual volume.  rho_out (host,
+ * [nodes]) may be NULL. */
+int pic_get_par_chg(int32_t delta, double *rho_out);
+
+/* IFE_Solve_2D (IFE-Rectangular/IFE_Solve_2D.f90:1-260) -> MY_JPCG_Solver ->
+ * MY_PCG (IFE-Solver/MY_PCG.f90).  phi_inout (host, [nodes]) may be NULL:
+ * then the device phi is the warm start and stays on the device. */
+int pic_ife_solve(double *phi_inout, double time, pic_solve_stats *stats);
+
+/* GetEField_SIDG_PPR (PPR/GetEfield_SIDG_PPR.f90:153-304): per-node
+ * quadratic recovery, efx = -d(phi)/dx.  Outputs may be NULL. */
+int pic_get_efield_ppr(double *efx_out, double *efy_out);
+
+/* MCCEntrance / MCC (MCCInterface.f90:560-569, mc/MCCPublic.F90:35-111). */
+int pic_mcc(uint64_t step, pic_mcc_stats *stats);
+
+/* One explicit step in the order of Main_IFE_Test_2.f90:329-341 with MCC after
+ * the field solve (MCC_jw/code/OneStep.F90:50-67): fused push+locate+deposit,
+ * RHS + PCG, PPR, MCC; counting sort every sort_interval steps. */
+int pic_step(uint64_t step, pic_step_stats *stats);
+
+/* Field readback (host, [nodes]).  which: 0 rho, 1 phi, 2 efx, 3 efy,
+ * 4+s rho_s of species s, 8+s Ek_tot of species s (normalised like rho_s),
+ * 12..16 coef_ppr(2..6,:). */
+int pic_get_field(int32_t which, double *host_out);
+/* Field upload (host, [nodes]): which 1 phi, 2 efx, 3 efy, 12..16 coef_ppr. */
+int pic_set_field(int32_t which, const double *host_in);
+
+/* Device pointers of the particle SoA, for zero-copy callers on the same
+ * device.  Order: x, y, vx, vy, vz (double*), loc (int32*), id (uint32*). */
+int pic_particle_device_ptrs(int32_t species, void **ptrs7, int64_t *n_slots);
+
+/* Number of library kernels launched since init (for launch accounting). */
+int64_t pic_kernel_launches(void);
+
+/* Device timer on the library's stream: op 0 records the start event,
+ * op 1 records the stop event, waits for it and writes the elapsed ms. */
+int pic_device_timer(int32_t op, double *ms_out);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* PICGPU_H */

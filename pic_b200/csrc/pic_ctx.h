@@ -1,0 +1,145 @@
+// pic_ctx.h -- device context of libpicgpu (internal).
+#ifndef PIC_CTX_H
+#define PIC_CTX_H
+
+#include <cuda_runtime.h>
+
+#include <string>
+#include <vector>
+
+#include "../../include/picgpu.h"
+#include "pic_common.h"
+
+namespace pic {
+
+void set_error(const std::string &msg);
+int cuda_fail(cudaError_t e, const char *where);
+extern long long g_launches;
+
+#define PIC_CUDA(call)                                      \
+  do {                                                      \
+    cudaError_t _e = (call);                                \
+    if (_e != cudaSuccess) return ::pic::cuda_fail(_e, #call); \
+  } while (0)
+
+#define PIC_LAUNCHED()                                          \
+  do {                                                          \
+    ++::pic::g_launches;                                        \
+    cudaError_t _e = cudaPeekAtLastError();                     \
+    if (_e != cudaSuccess) return ::pic::cuda_fail(_e, "launch"); \
+  } while (0)
+
+// Mesh geometry passed by value to kernels.
+struct MeshK {
+  int nnx, nny, nex, ney;
+  double xmin, xmax, ymin, ymax, hx, hy;
+  const double *xs, *ys;          // node coordinates (x_s + h_x*(i))
+  const int32_t *element_index;   // [ne]
+  const int32_t *node_index;      // [nn]
+};
+
+struct ObjK {
+  int n;
+  pic_object o[PIC_MAX_OBJECTS];
+};
+
+struct Species {
+  double charge = 0, mass = 0, weight = 0, qm = 0;
+  int64_t capacity = 0, n_slots = 0, n_live = 0;
+  uint32_t next_id = 0;
+  double *x = nullptr, *y = nullptr, *vx = nullptr, *vy = nullptr, *vz = nullptr;
+  int32_t *loc = nullptr;
+  uint32_t *id = nullptr;
+  // second buffer for the counting sort
+  double *x2 = nullptr, *y2 = nullptr, *vx2 = nullptr, *vy2 = nullptr, *vz2 = nullptr;
+  int32_t *loc2 = nullptr;
+  uint32_t *id2 = nullptr;
+  // deposit accumulators (fixed point) and normalised per-species fields
+  unsigned long long *q_acc = nullptr, *e_acc = nullptr;
+  double *rho_s = nullptr, *ek_s = nullptr;
+  // MCC
+  bool has_mcc = false;
+  pic_mcc_table tab;
+  double *prob = nullptr;  // [n_sigma*n_reaction]
+};
+
+struct PcgState {
+  double rho, rho0, alpha, beta, normR, normRHS, tol2;
+  int iter, maxit, done, ierr;
+  unsigned int ticket;
+  int pad;
+};
+
+struct Ctx {
+  bool inited = false;
+  MeshK m;
+  int64_t nn = 0, ne = 0;
+  pic_params P;
+  double L_ref = 0, t_ref = 0, v_ref = 0, phi_ref = 0;
+  cudaStream_t st = nullptr;
+  cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+  // mesh
+  double *d_xs = nullptr, *d_ys = nullptr;
+  int32_t *d_element_index = nullptr, *d_node_index = nullptr, *d_node_type = nullptr;
+  double *d_phi_dir = nullptr, *d_cell_volume = nullptr, *d_rhs_fix = nullptr;
+  double *d_mass_q1 = nullptr, *d_ife_mass = nullptr;
+  int32_t *d_xt_ptr = nullptr, *d_xt_col = nullptr;  // per unknown row, 0-based node columns
+  double *d_xt_val = nullptr;
+  // PCG operator: row kind per node (-1 Dirichlet, 0..n_mat-1 stencil, >= n_mat explicit row)
+  int32_t *d_row_kind = nullptr;
+  int32_t *d_ex_ptr = nullptr, *d_ex_col = nullptr;  // explicit rows (0-based node columns)
+  double *d_ex_val = nullptr;
+  int n_mat = 0;
+  double h_stencil[16][9];
+  double *d_diag = nullptr;  // [nn], 1 on Dirichlet nodes
+  // PPR
+  int32_t *d_ppr_kind = nullptr;  // 0 regular 3x3, 1 explicit, 2 none
+  int32_t *d_ppr_ptr = nullptr, *d_ppr_nodes = nullptr;  // explicit patches
+  double *d_ppr_rows = nullptr;  // [5][n] per explicit node, at 5*ptr
+  double *d_ppr_h = nullptr;     // h per node
+  double h_ppr_reg[5][9];
+  // fields
+  double *d_phi = nullptr, *d_rho = nullptr, *d_efx = nullptr, *d_efy = nullptr;
+  double *d_coef = nullptr;  // [5][nn] coef_ppr(2..6,:)
+  // PCG vectors (full grid)
+  double *d_b = nullptr, *d_x = nullptr, *d_r = nullptr, *d_w = nullptr, *d_p[2] = {nullptr, nullptr},
+         *d_q = nullptr;
+  double *d_part = nullptr;  // block partials [3][nblk]
+  PcgState *d_pcg = nullptr;
+  int red_blocks = 0;
+  int ebc_dirty = 1;
+  // species
+  int ns = 0;
+  Species sp[PIC_MAX_SPECIES];
+  // scratch
+  int32_t *d_cell_count = nullptr, *d_cell_start = nullptr, *d_cell_fill = nullptr;
+  int32_t *d_perm = nullptr;
+  uint32_t *d_sort_id = nullptr;
+  int32_t *d_scan_blk = nullptr;
+  unsigned long long *d_counters = nullptr;  // misc device counters
+  // MCC
+  pic_gas gas;
+  bool mcc_ready = false;
+  uint32_t *d_hist = nullptr;          // [65536]
+  int32_t *d_sel = nullptr;            // selected slots
+  uint64_t *d_cand = nullptr;          // candidates (key<<32 | id), slot in d_cand_slot
+  int32_t *d_cand_slot = nullptr;
+  int64_t mcc_cap = 0;
+  int64_t *d_mcc_misc = nullptr;       // [16] counters
+  int64_t *d_ion_parent = nullptr;     // ionising parents: (id<<32 | slot)
+  double *d_ion_data = nullptr;        // per ionisation: new e- v(3), ion v(3)
+  int64_t step_count = 0;
+};
+
+extern Ctx g;
+
+// kernels launched from other translation units
+int launch_locate(Species &s, int64_t begin, int64_t end);
+int sort_species(int sidx);
+int mcc_run(uint64_t step, pic_mcc_stats *stats);
+
+inline int blocks_for(int64_t n, int threads) { return (int)((n + threads - 1) / threads); }
+
+}  // namespace pic
+
+#endif

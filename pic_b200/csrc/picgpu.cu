@@ -1,0 +1,1633 @@
+// picgpu.cu -- B200 kernels and C-ABI of the IFE-PIC step.
+//
+// Layout in HBM
+//   particles : SoA per species, FP64 x, y, vx, vy, vz, int32 element (loc),
+//               uint32 id; loc = -1 marks an absorbed slot until the next sort.
+//   fields    : node-indexed FP64 arrays on the full nnx*nny grid
+//               (n = i*nny + j); Dirichlet nodes hold 0 in the PCG vectors.
+//   deposit   : int64 fixed-point accumulators per species and node.
+//
+// Kernels (all FP64; compiled with --fmad=false, FMAs are written explicitly
+// so the CPU oracle repeats the same roundings):
+//   k_locate ........ InjectPositioning.f90:1-24 / GetParChg_2D.f90:137-163
+//   k_push .......... MoveOne.f90 + Get_ParticleEField_PPR.f90 +
+//                     AdjustParticleBoundary (MCCInterface.f90:361-532), fused
+//                     with locate + bilinear deposit (GetParChg_2D.f90:788-843)
+//   k_rho ........... GetParChg_2D.f90:849-911 (normalise by dual volume)
+//   k_rhs ........... Global_RHS_PDE_2D.f90:72-138 + IFE_Solve_2D.f90:188-192
+//   k_pcg_* ......... MY_PCG.f90:56-127 with MATVEC_1/MSOLVE_1
+//   k_ppr ........... GetEfield_SIDG_PPR.f90:153-304
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <string>
+#include <vector>
+
+#include "pic_ctx.h"
+
+namespace pic {
+
+Ctx g;
+long long g_launches = 0;
+static std::string g_err;
+
+void set_error(const std::string &msg) { g_err = msg; }
+int cuda_fail(cudaError_t e, const char *where) {
+  g_err = std::string("CUDA error in ") + where + ": " + cudaGetErrorString(e);
+  return PIC_ERR_CUDA;
+}
+
+// ----------------------------------------------------------------------------
+// device helpers
+// ----------------------------------------------------------------------------
+
+struct FieldK {
+  const double *efx, *efy;
+  const double *c2, *c3, *c4, *c5, *c6;
+};
+
+__device__ __forceinline__ int locate_elem(const MeshK &m, double x, double y) {
+  // InjectPositioning.f90:13-22: i = INT((x - dxmin)/dx) + 1 (1-based)
+  double rxp = (x - m.xmin) / m.hx;
+  double ryp = (y - m.ymin) / m.hy;
+  int i = (int)rxp + 1;
+  int j = (int)ryp + 1;
+  if (i == m.nnx) i = m.nnx - 1;  // GetParChg_2D.f90:143-149 clamp
+  if (j == m.nny) j = m.nny - 1;
+  if (!(rxp >= 0.0) || !(ryp >= 0.0) || i < 1 || j < 1 || i > m.nex || j > m.ney) return -1;
+  return (i - 1) * m.ney + (j - 1);
+}
+
+__device__ __forceinline__ void bilinear(const MeshK &m, int e, double x, double y, double W[4],
+                                         int nodes[4], int *ie, int *je) {
+  int i = e / m.ney, j = e - i * m.ney;
+  double x1 = m.xs[i], x2 = m.xs[i + 1], y1 = m.ys[j], y2 = m.ys[j + 1];
+  double hxp = x2 - x1, hyp = y2 - y1;
+  double dx = (x - x1) / hxp;
+  double dy = (y - y1) / hyp;
+  double xc = 1.0 - dx, yc = 1.0 - dy;
+  W[0] = xc * yc;
+  W[1] = dx * yc;
+  W[2] = dx * dy;
+  W[3] = xc * dy;
+  int n1 = i * m.nny + j;
+  nodes[0] = n1;
+  nodes[1] = n1 + m.nny;
+  nodes[2] = n1 + m.nny + 1;
+  nodes[3] = n1 + 1;
+  *ie = i;
+  *je = j;
+}
+
+// Canonical block reduction of up to 3 values (see PIC_RED_* in pic_common.h).
+template <int NV>
+__device__ __forceinline__ void block_sum_canon(double v[NV], double *out /*[NV], thread 0*/) {
+  __shared__ double ws[NV][PIC_RED_THREADS / 32];
+#pragma unroll
+  for (int k = 0; k < NV; ++k)
+    for (int off = 16; off > 0; off >>= 1) v[k] = v[k] + __shfl_xor_sync(0xffffffffu, v[k], off);
+  int w = threadIdx.x >> 5, l = threadIdx.x & 31;
+  if (l == 0)
+    for (int k = 0; k < NV; ++k) ws[k][w] = v[k];
+  __syncthreads();
+  if (threadIdx.x == 0)
+    for (int k = 0; k < NV; ++k) {
+      double s = 0.0;
+      for (int q = 0; q < PIC_RED_THREADS / 32; ++q) s = s + ws[k][q];
+      out[k] = s;
+    }
+  __syncthreads();
+}
+
+// Final reduction of nb per-block partials by the last block (canonical order).
+template <int NV>
+__device__ __forceinline__ void final_sum_canon(const double *part, int nb, double *out) {
+  double v[NV];
+  for (int k = 0; k < NV; ++k) {
+    double a = 0.0;
+    for (int b = threadIdx.x; b < nb; b += PIC_RED_THREADS) a = a + __ldcg(part + (size_t)k * nb + b);
+    v[k] = a;
+  }
+  block_sum_canon<NV>(v, out);
+}
+
+__device__ __forceinline__ bool arrive_last(unsigned int *ticket) {
+  __shared__ bool last;
+  if (threadIdx.x == 0) {
+    __threadfence();
+    unsigned int t = atomicAdd(ticket, 1u);
+    last = (t == gridDim.x - 1);
+  }
+  __syncthreads();
+  return last;
+}
+
+// ----------------------------------------------------------------------------
+// particle kernels
+// ----------------------------------------------------------------------------
+
+__global__ void k_locate(MeshK m, const double *__restrict__ x, const double *__restrict__ y,
+                         int32_t *__restrict__ loc, int64_t begin, int64_t end,
+                         unsigned long long *bad) {
+  int64_t p = begin + (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (p >= end) return;
+  if (loc[p] < 0 && loc[p] != -2) return;  // absorbed slot stays absorbed
+  int e = locate_elem(m, x[p], y[p]);
+  if (e < 0) atomicAdd(bad, 1ull);
+  loc[p] = e;
+}
+
+struct PushK {
+  double qm, dt, mass, vref;
+  int do_push, do_deposit;
+  int wall[4];
+};
+
+struct SpK {
+  double *x, *y, *vx, *vy, *vz;
+  int32_t *loc;
+  unsigned long long *q_acc, *e_acc;
+  unsigned long long *lost, *bad;
+  int64_t n;
+};
+
+__constant__ ObjK c_obj;
+
+__device__ __forceinline__ bool absorbed_by_object(double x, double y) {
+  for (int k = 0; k < c_obj.n; ++k) {
+    const pic_object &o = c_obj.o[k];
+    if (o.shape == PIC_SHAPE_CIRCLE) {
+      double dx = x - o.cx, dy = y - o.cy;
+      if (dx * dx + dy * dy < o.a * o.a) return true;
+    } else if (o.shape == PIC_SHAPE_BOX) {
+      if (x > o.cx && x < o.a && y > o.cy && y < o.b) return true;
+    } else if (o.shape == PIC_SHAPE_ELLIPSE) {
+      double c = cos(o.angle), s = sin(o.angle);
+      double u = (x - o.cx) * c + (y - o.cy) * s;
+      double v = -(x - o.cx) * s + (y - o.cy) * c;
+      if ((u * u) / (o.a * o.a) + (v * v) / (o.b * o.b) < 1.0) return true;
+    }
+  }
+  return false;
+}
+
+// Segmented warp sum of an int64 value over lanes with the same key
+// (particles are cell-sorted, so neighbouring lanes usually share a cell).
+__device__ __forceinline__ long long seg_sum(long long v, int lane, int seg_end) {
+#pragma unroll
+  for (int off = 1; off < 32; off <<= 1) {
+    long long o = __shfl_down_sync(0xffffffffu, v, off);
+    if (lane + off <= seg_end) v += o;
+  }
+  return v;
+}
+
+// One particle per thread: gather E (old element), leapfrog push, wall/object
+// absorption, locate, fixed-point deposit of weight and weight*energy.
+__global__ void __launch_bounds__(256) k_push(MeshK m, FieldK f, PushK prm, SpK s) {
+  int64_t p = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  int lane = threadIdx.x & 31;
+  int key = -1;
+  double W[4] = {0, 0, 0, 0};
+  int nodes[4] = {0, 0, 0, 0};
+  double energy = 0.0;
+  bool lost = false;
+  if (p < s.n) {
+    int e = s.loc[p];
+    if (e >= 0) {
+      double x = s.x[p], y = s.y[p];
+      double vx = s.vx[p], vy = s.vy[p];
+      if (prm.do_push) {
+        int ie, je;
+        bilinear(m, e, x, y, W, nodes, &ie, &je);
+        double Ex, Ey;
+        if (m.element_index[e] > 0) {
+          // Get_ParticleEField_PPR.f90:19-33: average of the PPR gradients of the
+          // element's outside nodes
+          double ex = 0.0, ey = 0.0;
+          int cnt = 0;
+          for (int c = 0; c < 4; ++c) {
+            int n = nodes[c];
+            if (m.node_index[n] == -1) {
+              ++cnt;
+              int ni = n / m.nny, nj = n - ni * m.nny;
+              double xr = x - m.xs[ni], yr = y - m.ys[nj];
+              ex = ((ex + f.c2[n]) + (2.0 * f.c4[n]) * xr) + f.c5[n] * yr;
+              ey = ((ey + f.c3[n]) + (2.0 * f.c6[n]) * yr) + f.c5[n] * xr;
+            }
+          }
+          ex = ex / (double)cnt;
+          ey = ey / (double)cnt;
+          Ex = -ex;
+          Ey = -ey;
+        } else {
+          Ex = ((W[0] * f.efx[nodes[0]] + W[1] * f.efx[nodes[1]]) + W[2] * f.efx[nodes[2]]) +
+               W[3] * f.efx[nodes[3]];
+          Ey = ((W[0] * f.efy[nodes[0]] + W[1] * f.efy[nodes[1]]) + W[2] * f.efy[nodes[2]]) +
+               W[3] * f.efy[nodes[3]];
+        }
+        vx = vx + (prm.qm * Ex) * prm.dt;
+        vy = vy + (prm.qm * Ey) * prm.dt;
+        x = x + prm.dt * vx;
+        y = y + prm.dt * vy;
+        // walls: left, right, bottom, top
+        if (x <= m.xmin) {
+          if (prm.wall[0] == PIC_WALL_REFLECT) { x = m.xmin + (m.xmin - x); vx = -vx; }
+          else lost = true;
+        } else if (x > m.xmax) {
+          if (prm.wall[1] == PIC_WALL_REFLECT) { x = m.xmax - (x - m.xmax); vx = -vx; }
+          else lost = true;
+        } else if (y < m.ymin) {
+          if (prm.wall[2] == PIC_WALL_REFLECT) { y = m.ymin + (m.ymin - y); vy = -vy; }
+          else lost = true;
+        } else if (y > m.ymax) {
+          if (prm.wall[3] == PIC_WALL_REFLECT) { y = m.ymax - (y - m.ymax); vy = -vy; }
+          else lost = true;
+        }
+        if (!lost && absorbed_by_object(x, y)) lost = true;
+        s.x[p] = x;
+        s.y[p] = y;
+        s.vx[p] = vx;
+        s.vy[p] = vy;
+      }
+      if (lost) {
+        s.loc[p] = -1;
+      } else if (prm.do_deposit) {
+        int en = locate_elem(m, x, y);
+        if (en < 0) {
+          atomicAdd(s.bad, 1ull);
+          s.loc[p] = -1;
+          lost = true;
+        } else {
+          s.loc[p] = en;
+          key = en;
+          int ie, je;
+          bilinear(m, en, x, y, W, nodes, &ie, &je);
+          double vz = s.vz[p];
+          energy = ((((0.5 * prm.mass) * ((vx * vx + vy * vy) + vz * vz)) * prm.vref) * prm.vref) /
+                   PIC_JTOEV;
+        }
+      }
+    }
+  }
+  // lost-particle count (warp aggregated)
+  unsigned int lm = __ballot_sync(0xffffffffu, lost);
+  if (lane == 0 && lm) atomicAdd(s.lost, (unsigned long long)__popc(lm));
+  if (!prm.do_deposit) return;
+  // segmented warp aggregation by element, then one atomic per node and value
+  int prev = __shfl_up_sync(0xffffffffu, key, 1);
+  bool head = (lane == 0) || (key != prev);
+  unsigned int heads = __ballot_sync(0xffffffffu, head);
+  unsigned int above = (lane == 31) ? 0u : (heads & ~((2u << lane) - 1u));
+  int seg_end = above ? (__ffs(above) - 2) : 31;
+  long long qv[4], ev[4];
+#pragma unroll
+  for (int c = 0; c < 4; ++c) {
+    qv[c] = (key >= 0) ? __double2ll_rn(W[c] * PIC_Q_SCALE) : 0ll;
+    ev[c] = (key >= 0) ? __double2ll_rn((W[c] * energy) * PIC_E_SCALE) : 0ll;
+  }
+#pragma unroll
+  for (int c = 0; c < 4; ++c) {
+    qv[c] = seg_sum(qv[c], lane, seg_end);
+    ev[c] = seg_sum(ev[c], lane, seg_end);
+  }
+  if (head && key >= 0) {
+#pragma unroll
+    for (int c = 0; c < 4; ++c) {
+      atomicAdd(s.q_acc + nodes[c], (unsigned long long)qv[c]);
+      atomicAdd(s.e_acc + nodes[c], (unsigned long long)ev[c]);
+    }
+  }
+}
+
+// ----------------------------------------------------------------------------
+// field kernels
+// ----------------------------------------------------------------------------
+
+struct RhoK {
+  const unsigned long long *q[PIC_MAX_SPECIES], *e[PIC_MAX_SPECIES];
+  double *rho_s[PIC_MAX_SPECIES], *ek_s[PIC_MAX_SPECIES];
+  double wq[PIC_MAX_SPECIES], w[PIC_MAX_SPECIES];
+  int ns;
+  double L_ref, n_ref;
+};
+
+// GetParChg_2D.f90:869-911: rho_s = Weight*qs*sum/L_ref/L_ref/n_ref/V; the
+// mean energy per particle (eV) Ek_s = sum(W*E)/sum(W) is kept per node.
+__global__ void k_rho(RhoK r, const double *__restrict__ vol, double *__restrict__ rho, int64_t nn) {
+  int64_t n = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (n >= nn) return;
+  double acc = 0.0;
+  double V = vol[n];
+  for (int s = 0; s < r.ns; ++s) {
+    double cnt = (double)(long long)r.q[s][n] * (1.0 / PIC_Q_SCALE);
+    double esum = (double)(long long)r.e[s][n] * (1.0 / PIC_E_SCALE);
+    double rs = ((((r.wq[s] * cnt) / r.L_ref) / r.L_ref) / r.n_ref) / V;
+    r.rho_s[s][n] = rs;
+    r.ek_s[s][n] = (cnt != 0.0) ? esum / cnt : 0.0;
+    acc = acc + rs;
+  }
+  rho[n] = acc;
+}
+
+struct RhsK {
+  const double *rho, *mass_q1, *ife_mass, *rhs_fix, *phi_dir, *xt_val;
+  const int32_t *node_type, *element_index, *xt_ptr, *xt_col;
+  double *b;
+  int nnx, nny, ney;
+  int64_t nn;
+};
+
+// b = M*rho - rhs_FIX - A_xt*phi_D on the full node grid (0 on Dirichlet nodes).
+__global__ void k_rhs(RhsK k) {
+  int64_t n = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (n >= k.nn) return;
+  int u = k.node_type[n];
+  if (u <= 0) {
+    k.b[n] = 0.0;
+    return;
+  }
+  int i = (int)(n / k.nny), j = (int)(n - (int64_t)i * k.nny);
+  // adjacent elements in element order and this node's corner in each
+  const int di[4] = {-1, -1, 0, 0}, dj[4] = {-1, 0, -1, 0}, corner[4] = {2, 1, 3, 0};
+  double acc = 0.0;
+  for (int t = 0; t < 4; ++t) {
+    int ei = i + di[t], ej = j + dj[t];
+    if (ei < 0 || ej < 0 || ei >= k.nnx - 1 || ej >= k.nny - 1) continue;
+    int e = ei * k.ney + ej;
+    int id = k.element_index[e];
+    const double *M = (id > 0) ? (k.ife_mass + 16 * (size_t)(id - 1)) : k.mass_q1;
+    int n1 = ei * k.nny + ej;
+    double R0 = k.rho[n1], R1 = k.rho[n1 + k.nny], R2 = k.rho[n1 + k.nny + 1], R3 = k.rho[n1 + 1];
+    const double *Mr = M + 4 * corner[t];
+    double el = ((Mr[0] * R0 + Mr[1] * R1) + Mr[2] * R2) + Mr[3] * R3;
+    acc = acc + el;
+  }
+  double ebc = 0.0;
+  for (int q = k.xt_ptr[u - 1]; q < k.xt_ptr[u]; ++q) ebc = ebc + k.phi_dir[k.xt_col[q]] * k.xt_val[q];
+  k.b[n] = (acc - k.rhs_fix[u - 1]) - ebc;
+}
+
+__constant__ double c_stencil[16][9];
+
+struct PcgK {
+  const int32_t *row_kind, *ex_ptr, *ex_col;
+  const double *ex_val, *diag;
+  double *x, *r, *w, *q, *b;
+  const double *p_old;
+  double *p_new;
+  double *part;
+  PcgState *st;
+  const double *phi;
+  const int32_t *node_type;
+  int nny, n_mat;
+  int64_t nn;
+  int nb;
+};
+
+// y = A*v on the full grid for a node given a functor that returns v at a node.
+template <class F>
+__device__ __forceinline__ double row_apply(const PcgK &k, int64_t n, F v) {
+  int kind = k.row_kind[n];
+  if (kind < 0) return 0.0;
+  double acc = 0.0;
+  if (kind < k.n_mat) {
+    const int64_t base = n - k.nny - 1;
+#pragma unroll
+    for (int a = 0; a < 3; ++a)
+#pragma unroll
+      for (int c = 0; c < 3; ++c) acc = fma(c_stencil[kind][3 * a + c], v(base + (int64_t)a * k.nny + c), acc);
+  } else {
+    int rix = kind - k.n_mat;
+    for (int q = k.ex_ptr[rix]; q < k.ex_ptr[rix + 1]; ++q) acc = fma(k.ex_val[q], v((int64_t)k.ex_col[q]), acc);
+  }
+  return acc;
+}
+
+// r = b - A x0, w = r/diag, partials of b.b and r.w  (MY_PCG.f90:56-71, 77-83)
+__global__ void __launch_bounds__(PIC_RED_THREADS) k_pcg_init(PcgK k) {
+  double vb = 0.0, vrw = 0.0;
+  for (int it = 0; it < PIC_RED_ITEMS; ++it) {
+    int64_t n = (int64_t)blockIdx.x * PIC_RED_CHUNK + it * PIC_RED_THREADS + threadIdx.x;
+    if (n >= k.nn) continue;
+    double bb = k.b[n];
+    double ax = row_apply(k, n, [&](int64_t m) { return k.x[m]; });
+    double rr = (k.row_kind[n] < 0) ? 0.0 : bb - ax;
+    double ww = rr / k.diag[n];
+    k.r[n] = rr;
+    k.w[n] = ww;
+    vb = fma(bb, bb, vb);
+    vrw = fma(rr, ww, vrw);
+  }
+  double v[2] = {vb, vrw}, out[2];
+  block_sum_canon<2>(v, out);
+  if (threadIdx.x == 0) {
+    k.part[blockIdx.x] = out[0];
+    k.part[k.nb + blockIdx.x] = out[1];
+  }
+  if (arrive_last(&k.st->ticket)) {
+    double tot[2];
+    final_sum_canon<2>(k.part, k.nb, tot);
+    if (threadIdx.x == 0) {
+      PcgState *s = k.st;
+      s->normRHS = tot[0];
+      s->rho = tot[1];
+      s->rho0 = 0.0;
+      s->iter = 0;
+      s->ierr = 0;
+      s->done = 0;
+      s->beta = 0.0;
+      s->normR = 0.0;
+      s->ticket = 0;
+      if (!(tot[0] > 0.0)) {  // zero right-hand side: x = x0 already solves b=0 only if r=0
+        s->done = 1;
+        s->normR = 0.0;
+      }
+    }
+  }
+}
+
+// Warm start from phi at unknown nodes (IFE_Solve_2D.f90:80-85).
+__global__ void k_pcg_x0(PcgK k) {
+  int64_t n = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (n >= k.nn) return;
+  k.x[n] = (k.node_type[n] > 0) ? k.phi[n] : 0.0;
+}
+
+// p = w (+ beta p), q = A p, partial p.q  (MY_PCG.f90:86-111)
+__global__ void __launch_bounds__(PIC_RED_THREADS) k_pcg_dir(PcgK k) {
+  const PcgState *s = k.st;
+  if (*(volatile const int *)&s->done) return;
+  const bool first = (*(volatile const int *)&s->iter) == 0;
+  const double beta = *(volatile const double *)&s->beta;
+  auto pn = [&](int64_t m) { return first ? k.w[m] : fma(beta, k.p_old[m], k.w[m]); };
+  double vpq = 0.0;
+  for (int it = 0; it < PIC_RED_ITEMS; ++it) {
+    int64_t n = (int64_t)blockIdx.x * PIC_RED_CHUNK + it * PIC_RED_THREADS + threadIdx.x;
+    if (n >= k.nn) continue;
+    double pv = pn(n);
+    double qv = row_apply(k, n, pn);
+    k.p_new[n] = pv;
+    k.q[n] = qv;
+    vpq = fma(pv, qv, vpq);
+  }
+  double v[1] = {vpq}, out[1];
+  block_sum_canon<1>(v, out);
+  if (threadIdx.x == 0) k.part[blockIdx.x] = out[0];
+  if (arrive_last(&k.st->ticket)) {
+    double tot[1];
+    final_sum_canon<1>(k.part, k.nb, tot);
+    if (threadIdx.x == 0) {
+      PcgState *st = k.st;
+      st->ticket = 0;
+      if (tot[0] == 0.0) {
+        st->ierr = 3;
+        st->done = 1;
+      } else {
+        st->alpha = st->rho / tot[0];
+      }
+    }
+  }
+}
+
+// x += alpha p, r -= alpha q, w = r/diag, partials r.r and r.w; convergence test
+// normR/normRHS <= tol^2 (MY_PCG.f90:113-125).
+__global__ void __launch_bounds__(PIC_RED_THREADS) k_pcg_upd(PcgK k) {
+  PcgState *s = k.st;
+  if (*(volatile int *)&s->done) return;
+  const double alpha = *(volatile double *)&s->alpha;
+  double vrr = 0.0, vrw = 0.0;
+  for (int it = 0; it < PIC_RED_ITEMS; ++it) {
+    int64_t n = (int64_t)blockIdx.x * PIC_RED_CHUNK + it * PIC_RED_THREADS + threadIdx.x;
+    if (n >= k.nn) continue;
+    double pv = k.p_new[n];
+    double xv = fma(alpha, pv, k.x[n]);
+    double rv = fma(-alpha, k.q[n], k.r[n]);
+    double wv = rv / k.diag[n];
+    k.x[n] = xv;
+    k.r[n] = rv;
+    k.w[n] = wv;
+    vrr = fma(rv, rv, vrr);
+    vrw = fma(rv, wv, vrw);
+  }
+  double v[2] = {vrr, vrw}, out[2];
+  block_sum_canon<2>(v, out);
+  if (threadIdx.x == 0) {
+    k.part[blockIdx.x] = out[0];
+    k.part[k.nb + blockIdx.x] = out[1];
+  }
+  if (arrive_last(&s->ticket)) {
+    double tot[2];
+    final_sum_canon<2>(k.part, k.nb, tot);
+    if (threadIdx.x == 0) {
+      s->ticket = 0;
+      s->normR = tot[0];
+      s->rho0 = s->rho;
+      s->rho = tot[1];
+      s->iter = s->iter + 1;
+      if (s->normR / s->normRHS <= s->tol2) {
+        s->done = 1;
+      } else if (s->iter >= s->maxit) {
+        s->ierr = 1;
+        s->done = 1;
+      } else if (s->rho0 == 0.0) {
+        s->ierr = 2;
+        s->done = 1;
+      } else {
+        s->beta = s->rho / s->rho0;
+      }
+    }
+  }
+}
+
+// U_fe_full from U_fe (IFE_Solve_2D.f90:240-247)
+__global__ void k_phi_out(const double *__restrict__ x, const int32_t *__restrict__ node_type,
+                          const double *__restrict__ phi_dir, double *__restrict__ phi, int64_t nn) {
+  int64_t n = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (n >= nn) return;
+  phi[n] = (node_type[n] > 0) ? x[n] : phi_dir[n];
+}
+
+__constant__ double c_ppr_reg[5][9];
+
+struct PprK {
+  const double *phi, *h;
+  const int32_t *kind, *ptr, *nodes;
+  const double *rows;
+  double *coef;  // [5][nn]
+  double *efx, *efy;
+  int nny;
+  int64_t nn;
+};
+
+// PPR: coef(2..6) = P_i * phi(patch_i) scaled by 1/h, 1/h^2; E = -grad.
+__global__ void k_ppr(PprK k) {
+  int64_t n = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (n >= k.nn) return;
+  int kind = k.kind[n];
+  double c[5] = {0, 0, 0, 0, 0};
+  if (kind == 0) {
+    double ph[9];
+    const int64_t base = n - k.nny - 1;
+#pragma unroll
+    for (int a = 0; a < 3; ++a)
+#pragma unroll
+      for (int b = 0; b < 3; ++b) ph[3 * a + b] = k.phi[base + (int64_t)a * k.nny + b];
+#pragma unroll
+    for (int r = 0; r < 5; ++r) {
+      double acc = 0.0;
+#pragma unroll
+      for (int q = 0; q < 9; ++q) acc = fma(c_ppr_reg[r][q], ph[q], acc);
+      c[r] = acc;
+    }
+  } else if (kind == 1) {
+    int b0 = k.ptr[n], cnt = k.ptr[n + 1] - b0;
+    const double *R = k.rows + 5 * (size_t)b0;
+    for (int r = 0; r < 5; ++r) {
+      double acc = 0.0;
+      for (int q = 0; q < cnt; ++q) acc = fma(R[(size_t)r * cnt + q], k.phi[k.nodes[b0 + q]], acc);
+      c[r] = acc;
+    }
+  }
+  double h = k.h[n];
+  if (kind != 2) {
+    c[0] = c[0] / h;
+    c[1] = c[1] / h;
+    c[2] = c[2] / (h * h);
+    c[3] = c[3] / (h * h);
+    c[4] = c[4] / (h * h);
+  }
+  for (int r = 0; r < 5; ++r) k.coef[(size_t)r * k.nn + n] = c[r];
+  k.efx[n] = -c[0];
+  k.efy[n] = -c[1];
+}
+
+__global__ void k_fill_u64(unsigned long long *a, int64_t n) {
+  int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i < n) a[i] = 0ull;
+}
+
+// ----------------------------------------------------------------------------
+// host helpers
+// ----------------------------------------------------------------------------
+
+static MeshK mesh_k() {
+  MeshK m = g.m;
+  m.xs = g.d_xs;
+  m.ys = g.d_ys;
+  m.element_index = g.d_element_index;
+  m.node_index = g.d_node_index;
+  return m;
+}
+
+template <class T>
+static int dalloc(T **p, size_t n) {
+  if (n == 0) n = 1;
+  PIC_CUDA(cudaMalloc((void **)p, n * sizeof(T)));
+  return PIC_OK;
+}
+template <class T>
+static int upload(T **p, const T *h, size_t n) {
+  int rc = dalloc(p, n);
+  if (rc) return rc;
+  if (h && n) PIC_CUDA(cudaMemcpy(*p, h, n * sizeof(T), cudaMemcpyHostToDevice));
+  return PIC_OK;
+}
+
+// Gauss-Jordan inverse with full pivoting of an n x n matrix (row-major),
+// as BRINV does for the 6x6 normal matrix (PPR/BRINV.f90:11-70).
+static bool brinv(double *a, int n) {
+  std::vector<int> is(n), js(n);
+  for (int k = 0; k < n; ++k) {
+    double d = 0.0;
+    for (int i = k; i < n; ++i)
+      for (int j = k; j < n; ++j) {
+        double p = std::fabs(a[i * n + j]);
+        if (p > d) { d = p; is[k] = i; js[k] = j; }
+      }
+    if (d + 1.0 == 1.0) return false;
+    if (is[k] != k)
+      for (int j = 0; j < n; ++j) std::swap(a[k * n + j], a[is[k] * n + j]);
+    if (js[k] != k)
+      for (int i = 0; i < n; ++i) std::swap(a[i * n + k], a[i * n + js[k]]);
+    a[k * n + k] = 1.0 / a[k * n + k];
+    for (int j = 0; j < n; ++j)
+      if (j != k) a[k * n + j] = a[k * n + j] * a[k * n + k];
+    for (int i = 0; i < n; ++i)
+      if (i != k)
+        for (int j = 0; j < n; ++j)
+          if (j != k) a[i * n + j] = a[i * n + j] - a[i * n + k] * a[k * n + j];
+    for (int i = 0; i < n; ++i)
+      if (i != k) a[i * n + k] = -a[i * n + k] * a[k * n + k];
+  }
+  for (int k = n - 1; k >= 0; --k) {
+    if (js[k] != k)
+      for (int j = 0; j < n; ++j) std::swap(a[k * n + j], a[js[k] * n + j]);
+    if (is[k] != k)
+      for (int i = 0; i < n; ++i) std::swap(a[i * n + k], a[i * n + is[k]]);
+  }
+  return true;
+}
+
+// Rows 2..6 of (A^T A)^-1 A^T for normalised patch offsets (GetEfield_SIDG_PPR.f90:158-197).
+static bool ppr_rows(const std::vector<double> &px, const std::vector<double> &py, double *out5xn) {
+  int n = (int)px.size();
+  std::vector<double> AT(6 * n);
+  for (int m = 0; m < n; ++m) {
+    AT[0 * n + m] = 1.0;
+    AT[1 * n + m] = px[m];
+    AT[2 * n + m] = py[m];
+    AT[3 * n + m] = px[m] * px[m];
+    AT[4 * n + m] = px[m] * py[m];
+    AT[5 * n + m] = py[m] * py[m];
+  }
+  double N[36];
+  for (int a = 0; a < 6; ++a)
+    for (int b = 0; b < 6; ++b) {
+      double s = 0.0;
+      for (int m = 0; m < n; ++m) s = s + AT[a * n + m] * AT[b * n + m];
+      N[a * 6 + b] = s;
+    }
+  if (!brinv(N, 6)) return false;
+  for (int a = 1; a < 6; ++a)
+    for (int m = 0; m < n; ++m) {
+      double s = 0.0;
+      for (int b = 0; b < 6; ++b) s = s + N[a * 6 + b] * AT[b * n + m];
+      out5xn[(a - 1) * n + m] = s;
+    }
+  return true;
+}
+
+static void free_all() {
+  auto F = [](void *p) {
+    if (p) cudaFree(p);
+  };
+  F(g.d_xs); F(g.d_ys); F(g.d_element_index); F(g.d_node_index); F(g.d_node_type);
+  F(g.d_phi_dir); F(g.d_cell_volume); F(g.d_rhs_fix); F(g.d_mass_q1); F(g.d_ife_mass);
+  F(g.d_xt_ptr); F(g.d_xt_col); F(g.d_xt_val); F(g.d_row_kind); F(g.d_ex_ptr); F(g.d_ex_col);
+  F(g.d_ex_val); F(g.d_diag); F(g.d_ppr_kind); F(g.d_ppr_ptr); F(g.d_ppr_nodes); F(g.d_ppr_rows);
+  F(g.d_ppr_h); F(g.d_phi); F(g.d_rho); F(g.d_efx); F(g.d_efy); F(g.d_coef); F(g.d_b); F(g.d_x);
+  F(g.d_r); F(g.d_w); F(g.d_p[0]); F(g.d_p[1]); F(g.d_q); F(g.d_part); F(g.d_pcg);
+  F(g.d_cell_count); F(g.d_cell_start); F(g.d_cell_fill); F(g.d_perm); F(g.d_sort_id);
+  F(g.d_scan_blk); F(g.d_counters); F(g.d_hist); F(g.d_sel); F(g.d_cand); F(g.d_cand_slot);
+  F(g.d_mcc_misc); F(g.d_ion_parent); F(g.d_ion_data);
+  for (int s = 0; s < PIC_MAX_SPECIES; ++s) {
+    Species &p = g.sp[s];
+    F(p.x); F(p.y); F(p.vx); F(p.vy); F(p.vz); F(p.loc); F(p.id);
+    F(p.x2); F(p.y2); F(p.vx2); F(p.vy2); F(p.vz2); F(p.loc2); F(p.id2);
+    F(p.q_acc); F(p.e_acc); F(p.rho_s); F(p.ek_s); F(p.prob);
+  }
+  if (g.ev0) cudaEventDestroy(g.ev0);
+  if (g.ev1) cudaEventDestroy(g.ev1);
+  if (g.st) cudaStreamDestroy(g.st);
+  g = Ctx();
+}
+
+int launch_locate(Species &s, int64_t begin, int64_t end) {
+  if (end <= begin) return PIC_OK;
+  k_locate<<<blocks_for(end - begin, 256), 256, 0, g.st>>>(mesh_k(), s.x, s.y, s.loc, begin, end,
+                                                           g.d_counters + 1);
+  PIC_LAUNCHED();
+  return PIC_OK;
+}
+
+static int read_counter(int idx, unsigned long long *v) {
+  PIC_CUDA(cudaMemcpyAsync(v, g.d_counters + idx, sizeof *v, cudaMemcpyDeviceToHost, g.st));
+  PIC_CUDA(cudaStreamSynchronize(g.st));
+  return PIC_OK;
+}
+
+static int zero_counter(int idx) {
+  PIC_CUDA(cudaMemsetAsync(g.d_counters + idx, 0, sizeof(unsigned long long), g.st));
+  return PIC_OK;
+}
+
+// push and/or locate+deposit for one species
+static int run_push(int sidx, bool do_push, bool do_deposit) {
+  Species &s = g.sp[sidx];
+  if (s.n_slots == 0) return PIC_OK;
+  FieldK f{g.d_efx, g.d_efy, g.d_coef, g.d_coef + g.nn, g.d_coef + 2 * g.nn, g.d_coef + 3 * g.nn,
+           g.d_coef + 4 * g.nn};
+  PushK prm;
+  prm.qm = s.qm;
+  prm.dt = g.P.dt;
+  prm.mass = s.mass;
+  prm.vref = g.v_ref;
+  prm.do_push = do_push;
+  prm.do_deposit = do_deposit;
+  for (int w = 0; w < 4; ++w) prm.wall[w] = g.P.wall_bc[w];
+  SpK k{s.x, s.y, s.vx, s.vy, s.vz, s.loc, s.q_acc, s.e_acc, g.d_counters + 8 + sidx, g.d_counters + 1,
+        s.n_slots};
+  k_push<<<blocks_for(s.n_slots, 256), 256, 0, g.st>>>(mesh_k(), f, prm, k);
+  PIC_LAUNCHED();
+  return PIC_OK;
+}
+
+static int zero_deposit() {
+  for (int s = 0; s < g.ns; ++s) {
+    PIC_CUDA(cudaMemsetAsync(g.sp[s].q_acc, 0, g.nn * sizeof(unsigned long long), g.st));
+    PIC_CUDA(cudaMemsetAsync(g.sp[s].e_acc, 0, g.nn * sizeof(unsigned long long), g.st));
+  }
+  return PIC_OK;
+}
+
+static int run_rho() {
+  RhoK r;
+  std::memset(&r, 0, sizeof r);
+  r.ns = g.ns;
+  r.L_ref = g.L_ref;
+  r.n_ref = g.P.n_ref;
+  for (int s = 0; s < g.ns; ++s) {
+    r.q[s] = g.sp[s].q_acc;
+    r.e[s] = g.sp[s].e_acc;
+    r.rho_s[s] = g.sp[s].rho_s;
+    r.ek_s[s] = g.sp[s].ek_s;
+    r.wq[s] = g.sp[s].weight * g.sp[s].charge;
+    r.w[s] = g.sp[s].weight;
+  }
+  k_rho<<<blocks_for(g.nn, 256), 256, 0, g.st>>>(r, g.d_cell_volume, g.d_rho, g.nn);
+  PIC_LAUNCHED();
+  return PIC_OK;
+}
+
+static PcgK pcg_k(int parity) {
+  PcgK k;
+  k.row_kind = g.d_row_kind;
+  k.ex_ptr = g.d_ex_ptr;
+  k.ex_col = g.d_ex_col;
+  k.ex_val = g.d_ex_val;
+  k.diag = g.d_diag;
+  k.x = g.d_x;
+  k.r = g.d_r;
+  k.w = g.d_w;
+  k.q = g.d_q;
+  k.b = g.d_b;
+  k.p_old = g.d_p[parity];
+  k.p_new = g.d_p[parity ^ 1];
+  k.part = g.d_part;
+  k.st = g.d_pcg;
+  k.phi = g.d_phi;
+  k.node_type = g.d_node_type;
+  k.nny = g.m.nny;
+  k.n_mat = g.n_mat;
+  k.nn = g.nn;
+  k.nb = g.red_blocks;
+  return k;
+}
+
+static int run_rhs() {
+  RhsK k;
+  k.rho = g.d_rho;
+  k.mass_q1 = g.d_mass_q1;
+  k.ife_mass = g.d_ife_mass;
+  k.rhs_fix = g.d_rhs_fix;
+  k.phi_dir = g.d_phi_dir;
+  k.xt_val = g.d_xt_val;
+  k.node_type = g.d_node_type;
+  k.element_index = g.d_element_index;
+  k.xt_ptr = g.d_xt_ptr;
+  k.xt_col = g.d_xt_col;
+  k.b = g.d_b;
+  k.nnx = g.m.nnx;
+  k.nny = g.m.nny;
+  k.ney = g.m.ney;
+  k.nn = g.nn;
+  k_rhs<<<blocks_for(g.nn, 256), 256, 0, g.st>>>(k);
+  PIC_LAUNCHED();
+  return PIC_OK;
+}
+
+static int run_pcg(pic_solve_stats *stats) {
+  PcgState h;
+  std::memset(&h, 0, sizeof h);
+  h.tol2 = g.P.pcg_tol * g.P.pcg_tol;
+  h.maxit = g.P.pcg_maxit;
+  PIC_CUDA(cudaMemcpyAsync(g.d_pcg, &h, sizeof h, cudaMemcpyHostToDevice, g.st));
+  PcgK k0 = pcg_k(0);
+  k_pcg_x0<<<blocks_for(g.nn, 256), 256, 0, g.st>>>(k0);
+  PIC_LAUNCHED();
+  k_pcg_init<<<g.red_blocks, PIC_RED_THREADS, 0, g.st>>>(k0);
+  PIC_LAUNCHED();
+  const int chunk = 32;
+  int parity = 0;
+  PcgState hs;
+  for (int it = 0; it < g.P.pcg_maxit + chunk; it += chunk) {
+    for (int c = 0; c < chunk; ++c) {
+      PcgK k = pcg_k(parity);
+      k_pcg_dir<<<g.red_blocks, PIC_RED_THREADS, 0, g.st>>>(k);
+      PIC_LAUNCHED();
+      k_pcg_upd<<<g.red_blocks, PIC_RED_THREADS, 0, g.st>>>(k);
+      PIC_LAUNCHED();
+      parity ^= 1;
+    }
+    PIC_CUDA(cudaMemcpyAsync(&hs, g.d_pcg, sizeof hs, cudaMemcpyDeviceToHost, g.st));
+    PIC_CUDA(cudaStreamSynchronize(g.st));
+    if (hs.done) break;
+  }
+  k_phi_out<<<blocks_for(g.nn, 256), 256, 0, g.st>>>(g.d_x, g.d_node_type, g.d_phi_dir, g.d_phi, g.nn);
+  PIC_LAUNCHED();
+  if (stats) {
+    stats->iterations = hs.iter;
+    stats->ierr = hs.ierr;
+    stats->rel_residual = (hs.normRHS > 0) ? std::sqrt(hs.normR / hs.normRHS) : 0.0;
+    stats->fallback = 0;
+    stats->outer = 0;
+  }
+  if (!(hs.normR == hs.normR)) {
+    set_error("pic_ife_solve: NaN residual");
+    return PIC_ERR_NAN;
+  }
+  if (hs.ierr == 1) {
+    set_error("pic_ife_solve: PCG reached the iteration cap");
+    return PIC_ERR_SOLVER_CAP;
+  }
+  if (hs.ierr >= 2) {
+    set_error("pic_ife_solve: PCG breakdown");
+    return PIC_ERR_BREAKDOWN;
+  }
+  return PIC_OK;
+}
+
+static int run_ppr() {
+  PprK k;
+  k.phi = g.d_phi;
+  k.h = g.d_ppr_h;
+  k.kind = g.d_ppr_kind;
+  k.ptr = g.d_ppr_ptr;
+  k.nodes = g.d_ppr_nodes;
+  k.rows = g.d_ppr_rows;
+  k.coef = g.d_coef;
+  k.efx = g.d_efx;
+  k.efy = g.d_efy;
+  k.nny = g.m.nny;
+  k.nn = g.nn;
+  k_ppr<<<blocks_for(g.nn, 256), 256, 0, g.st>>>(k);
+  PIC_LAUNCHED();
+  return PIC_OK;
+}
+
+static int check_init() {
+  if (!g.inited) {
+    set_error("library not initialised (pic_init)");
+    return PIC_ERR_STATE;
+  }
+  return PIC_OK;
+}
+
+static int check_species(int s) {
+  if (s < 0 || s >= g.ns) {
+    set_error("species index out of range");
+    return PIC_ERR_ARG;
+  }
+  return PIC_OK;
+}
+
+}  // namespace pic
+
+using namespace pic;
+
+extern "C" {
+
+const char *pic_last_error(void) { return g_err.c_str(); }
+int64_t pic_kernel_launches(void) { return (int64_t)g_launches; }
+
+int pic_device_timer(int32_t op, double *ms_out) {
+  if (!g.inited) {
+    set_error("pic_device_timer: library not initialised");
+    return PIC_ERR_STATE;
+  }
+  static cudaEvent_t t0 = nullptr, t1 = nullptr;
+  if (!t0) {
+    PIC_CUDA(cudaEventCreate(&t0));
+    PIC_CUDA(cudaEventCreate(&t1));
+  }
+  if (op == 0) {
+    PIC_CUDA(cudaEventRecord(t0, g.st));
+    return PIC_OK;
+  }
+  if (op != 1) return PIC_ERR_ARG;
+  PIC_CUDA(cudaEventRecord(t1, g.st));
+  PIC_CUDA(cudaEventSynchronize(t1));
+  float ms = 0;
+  PIC_CUDA(cudaEventElapsedTime(&ms, t0, t1));
+  if (ms_out) *ms_out = ms;
+  return PIC_OK;
+}
+
+void pic_finalize(void) {
+  if (g.inited) cudaStreamSynchronize(g.st);
+  free_all();
+}
+
+int pic_init(const pic_mesh_desc *mesh, const pic_params *params) {
+  if (!mesh || !params) {
+    set_error("pic_init: null argument");
+    return PIC_ERR_ARG;
+  }
+  if (g.inited) free_all();
+  const pic_params &P = *params;
+  if (mesh->nnx < 3 || mesh->nny < 3 || P.n_species < 1 || P.n_species > PIC_MAX_SPECIES ||
+      !(P.dt > 0) || !(P.n_ref > 0) || !(P.T_ref_eV > 0) || P.pcg_maxit < 1 || !(P.pcg_tol > 0) ||
+      mesh->n_objects < 0 || mesh->n_objects > PIC_MAX_OBJECTS) {
+    set_error("pic_init: bad mesh size or parameters");
+    return PIC_ERR_ARG;
+  }
+  if (mesh->delta != 0) {
+    set_error("pic_init: axisymmetric meshes (delta=1) are not supported by this build");
+    return PIC_ERR_ARG;
+  }
+  if ((int64_t)mesh->nnx * mesh->nny > (int64_t)1 << 30) {
+    set_error("pic_init: mesh too large for int32 node ids");
+    return PIC_ERR_ARG;
+  }
+  g = Ctx();
+  g.P = P;
+  if (g.P.sort_interval < 1) g.P.sort_interval = 1;
+  MeshK &m = g.m;
+  m.nnx = mesh->nnx;
+  m.nny = mesh->nny;
+  m.nex = m.nnx - 1;
+  m.ney = m.nny - 1;
+  m.xmin = mesh->xmin;
+  m.xmax = mesh->xmax;
+  m.ymin = mesh->ymin;
+  m.ymax = mesh->ymax;
+  m.hx = (m.xmax - m.xmin) / (m.nnx - 1);
+  m.hy = (m.ymax - m.ymin) / (m.nny - 1);
+  g.nn = (int64_t)m.nnx * m.nny;
+  g.ne = (int64_t)m.nex * m.ney;
+  const int64_t nn = g.nn, ne = g.ne;
+  // reference scales, Input_2D.f90:362-392
+  double T_ref = P.T_ref_eV * PIC_EVTOK;
+  g.L_ref = std::sqrt(PIC_EPS0 * PIC_KB * T_ref / P.n_ref / PIC_QE / PIC_QE);
+  g.t_ref = std::sqrt(PIC_EPS0 * PIC_ME / P.n_ref / PIC_QE / PIC_QE);
+  g.v_ref = std::sqrt(PIC_KB * T_ref / PIC_ME);
+  g.phi_ref = PIC_KB * T_ref / PIC_QE;
+
+  int rc;
+  PIC_CUDA(cudaStreamCreateWithFlags(&g.st, cudaStreamNonBlocking));
+  PIC_CUDA(cudaEventCreate(&g.ev0));
+  PIC_CUDA(cudaEventCreate(&g.ev1));
+  std::vector<double> xs(m.nnx), ys(m.nny);
+  for (int i = 0; i < m.nnx; ++i) xs[i] = m.xmin + m.hx * i;
+  for (int j = 0; j < m.nny; ++j) ys[j] = m.ymin + m.hy * j;
+  if ((rc = upload(&g.d_xs, xs.data(), xs.size()))) return rc;
+  if ((rc = upload(&g.d_ys, ys.data(), ys.size()))) return rc;
+  if ((rc = upload(&g.d_element_index, mesh->element_index, ne))) return rc;
+  if ((rc = upload(&g.d_node_index, mesh->node_index, nn))) return rc;
+  if ((rc = upload(&g.d_node_type, mesh->node_type, nn))) return rc;
+  if ((rc = upload(&g.d_phi_dir, mesh->phi_dirichlet, nn))) return rc;
+  if ((rc = upload(&g.d_cell_volume, mesh->cell_volume, nn))) return rc;
+  const int nu = mesh->n_unknowns;
+  std::vector<double> rhs_fix(nu, 0.0);
+  if (mesh->rhs_fix) std::copy(mesh->rhs_fix, mesh->rhs_fix + nu, rhs_fix.begin());
+  if ((rc = upload(&g.d_rhs_fix, rhs_fix.data(), rhs_fix.size()))) return rc;
+  if ((rc = upload(&g.d_mass_q1, mesh->mass_q1, 16))) return rc;
+  if ((rc = upload(&g.d_ife_mass, mesh->ife_mass, 16 * (size_t)mesh->n_interface))) return rc;
+  ObjK ob;
+  std::memset(&ob, 0, sizeof ob);
+  ob.n = mesh->n_objects;
+  for (int k = 0; k < ob.n; ++k) ob.o[k] = mesh->objects[k];
+  PIC_CUDA(cudaMemcpyToSymbol(c_obj, &ob, sizeof ob));
+
+  // validate every index table before it reaches a kernel
+  {
+    auto bad = [](const char *what) {
+      set_error(std::string("pic_init: invalid ") + what);
+      return PIC_ERR_ARG;
+    };
+    if (nu < 0 || nu > nn) return bad("n_unknowns");
+    if (mesh->n_interface < 0 || (mesh->n_interface > 0 && !mesh->ife_mass)) return bad("interface data");
+    for (int64_t e = 0; e < ne; ++e) {
+      int v = mesh->element_index[e];
+      if (v > mesh->n_interface || v == 0) return bad("element_index");
+    }
+    if (mesh->a_srow[0] != 1 || mesh->xt_srow[0] != 1) return bad("CSR row pointers");
+    for (int u = 0; u < nu; ++u)
+      if (mesh->a_srow[u + 1] < mesh->a_srow[u] || mesh->xt_srow[u + 1] < mesh->xt_srow[u])
+        return bad("CSR row pointers");
+    if (mesh->a_srow[nu] - 1 != mesh->nnz || mesh->xt_srow[nu] - 1 != mesh->nnz_xt) return bad("nnz");
+    for (int64_t q = 0; q < mesh->nnz; ++q)
+      if (mesh->a_jcol[q] < 1 || mesh->a_jcol[q] > nu) return bad("a_jcol");
+    for (int64_t q = 0; q < mesh->nnz_xt; ++q)
+      if (mesh->xt_jcol[q] < 1 || mesh->xt_jcol[q] > nn || mesh->node_type[mesh->xt_jcol[q] - 1] > 0)
+        return bad("xt_jcol");
+    if (mesh->patch_ptr[0] != 0) return bad("patch_ptr");
+    for (int64_t n = 0; n < nn; ++n)
+      if (mesh->patch_ptr[n + 1] < mesh->patch_ptr[n]) return bad("patch_ptr");
+    for (int64_t q = 0; q < mesh->patch_ptr[nn]; ++q)
+      if (mesh->patch_nodes[q] < 1 || mesh->patch_nodes[q] > nn) return bad("patch_nodes");
+    for (int64_t n = 0; n < nn; ++n)
+      if (!(mesh->cell_volume[n] > 0)) return bad("cell_volume");
+  }
+  // unknown id -> node map, sanity of the CSR
+  std::vector<int32_t> u2n(nu, -1);
+  for (int64_t n = 0; n < nn; ++n) {
+    int t = mesh->node_type[n];
+    if (t > 0) {
+      if (t > nu) { set_error("pic_init: node_type out of range"); return PIC_ERR_ARG; }
+      u2n[t - 1] = (int32_t)n;
+    }
+  }
+  for (int u = 0; u < nu; ++u)
+    if (u2n[u] < 0) { set_error("pic_init: unknown numbering has holes"); return PIC_ERR_ARG; }
+  // A_xt rows in 0-based node columns
+  {
+    std::vector<int32_t> ptr(nu + 1), col;
+    std::vector<double> val;
+    for (int u = 0; u < nu; ++u) {
+      ptr[u] = (int32_t)col.size();
+      for (int64_t q = mesh->xt_srow[u] - 1; q < mesh->xt_srow[u + 1] - 1; ++q) {
+        col.push_back(mesh->xt_jcol[q] - 1);
+        val.push_back(mesh->xt_k[q]);
+      }
+    }
+    ptr[nu] = (int32_t)col.size();
+    if ((rc = upload(&g.d_xt_ptr, ptr.data(), ptr.size()))) return rc;
+    if ((rc = upload(&g.d_xt_col, col.data(), col.size()))) return rc;
+    if ((rc = upload(&g.d_xt_val, val.data(), val.size()))) return rc;
+  }
+  // split A into material stencils and explicit rows
+  {
+    const int nny = m.nny;
+    auto row_entries = [&](int u, std::vector<std::pair<int64_t, double>> &out) {
+      out.clear();
+      for (int64_t q = mesh->a_srow[u] - 1; q < mesh->a_srow[u + 1] - 1; ++q)
+        out.push_back({(int64_t)u2n[mesh->a_jcol[q] - 1], mesh->a_k[q]});
+    };
+    std::vector<std::pair<int64_t, double>> ent;
+    g.n_mat = 0;
+    // pass 1: stencils from rows whose four elements are one non-interface material
+    for (int i = 1; i < m.nnx - 1 && g.n_mat < 16; ++i)
+      for (int j = 1; j < nny - 1 && g.n_mat < 16; ++j) {
+        int64_t n = (int64_t)i * nny + j;
+        int u = mesh->node_type[n];
+        if (u <= 0) continue;
+        int e0 = mesh->element_index[(i - 1) * m.ney + (j - 1)];
+        bool same = e0 < 0;
+        for (int di = -1; di <= 0 && same; ++di)
+          for (int dj = -1; dj <= 0 && same; ++dj)
+            same = mesh->element_index[(i + di) * m.ney + (j + dj)] == e0;
+        if (!same) continue;
+        row_entries(u - 1, ent);
+        if (ent.size() != 9) continue;
+        double S[9];
+        bool ok = true;
+        for (int t = 0; t < 9 && ok; ++t) {
+          int64_t want = n + (int64_t)(t / 3 - 1) * nny + (t % 3 - 1);
+          ok = ent[t].first == want;
+          S[t] = ent[t].second;
+        }
+        if (!ok) continue;
+        bool known = false;
+        for (int q = 0; q < g.n_mat && !known; ++q) known = std::memcmp(g.h_stencil[q], S, sizeof S) == 0;
+        if (!known) std::memcpy(g.h_stencil[g.n_mat++], S, sizeof S);
+      }
+    std::vector<int32_t> kind(nn, -1), ex_ptr(1, 0), ex_col;
+    std::vector<double> ex_val, diag(nn, 1.0);
+    for (int64_t n = 0; n < nn; ++n) {
+      int u = mesh->node_type[n];
+      if (u <= 0) continue;
+      diag[n] = mesh->a_diag[u - 1];
+      row_entries(u - 1, ent);
+      int i = (int)(n / nny), j = (int)(n % nny);
+      int mat = -1;
+      if (i >= 1 && j >= 1 && i < m.nnx - 1 && j < nny - 1) {
+        for (int q = 0; q < g.n_mat && mat < 0; ++q) {
+          size_t pos = 0;
+          bool ok = true;
+          for (int t = 0; t < 9 && ok; ++t) {
+            int64_t want = n + (int64_t)(t / 3 - 1) * nny + (t % 3 - 1);
+            if (mesh->node_type[want] > 0) {
+              ok = pos < ent.size() && ent[pos].first == want &&
+                   std::memcmp(&ent[pos].second, &g.h_stencil[q][t], sizeof(double)) == 0;
+              ++pos;
+            }
+          }
+          if (ok && pos == ent.size()) mat = q;
+        }
+      }
+      if (mat >= 0) {
+        kind[n] = mat;
+      } else {
+        kind[n] = g.n_mat + (int32_t)(ex_ptr.size() - 1);
+        for (auto &pr : ent) {
+          ex_col.push_back((int32_t)pr.first);
+          ex_val.push_back(pr.second);
+        }
+        ex_ptr.push_back((int32_t)ex_col.size());
+      }
+    }
+    PIC_CUDA(cudaMemcpyToSymbol(c_stencil, g.h_stencil, sizeof g.h_stencil));
+    if ((rc = upload(&g.d_row_kind, kind.data(), kind.size()))) return rc;
+    if ((rc = upload(&g.d_ex_ptr, ex_ptr.data(), ex_ptr.size()))) return rc;
+    if ((rc = upload(&g.d_ex_col, ex_col.data(), ex_col.size()))) return rc;
+    if ((rc = upload(&g.d_ex_val, ex_val.data(), ex_val.size()))) return rc;
+    if ((rc = upload(&g.d_diag, diag.data(), diag.size()))) return rc;
+  }
+  // PPR patches: regular 3x3 patches share one pseudo-inverse, others get their own rows
+  {
+    const int nny = m.nny;
+    std::vector<int32_t> kind(nn, 2), ptr(nn + 1, 0), nodes;
+    std::vector<double> rows, hs(nn, 1.0);
+    {
+      double h = std::max(m.hx, m.hy);
+      std::vector<double> px, py;
+      for (int a = -1; a <= 1; ++a)
+        for (int b = -1; b <= 1; ++b) {
+          px.push_back(a * m.hx / h);
+          py.push_back(b * m.hy / h);
+        }
+      double R[45];
+      if (!ppr_rows(px, py, R)) { set_error("pic_init: singular regular PPR patch"); return PIC_ERR_ARG; }
+      for (int r = 0; r < 5; ++r)
+        for (int q = 0; q < 9; ++q) g.h_ppr_reg[r][q] = R[r * 9 + q];
+    }
+    for (int64_t n = 0; n < nn; ++n) {
+      ptr[n] = (int32_t)nodes.size();
+      int b0 = mesh->patch_ptr[n], cnt = mesh->patch_ptr[n + 1] - b0;
+      int i = (int)(n / nny), j = (int)(n % nny);
+      double xi = xs[i], yi = ys[j];
+      double h = 0.0;
+      for (int q = 0; q < cnt; ++q) {
+        int32_t mm = mesh->patch_nodes[b0 + q] - 1;
+        double dx = std::fabs(xs[mm / nny] - xi), dy = std::fabs(ys[mm % nny] - yi);
+        h = std::max(h, std::max(dx, dy));
+      }
+      hs[n] = (h > 0) ? h : 1.0;
+      if (cnt < 6) continue;
+      bool regular = (cnt == 9) && i >= 1 && j >= 1 && i < m.nnx - 1 && j < nny - 1;
+      for (int t = 0; t < 9 && regular; ++t)
+        regular = (mesh->patch_nodes[b0 + t] - 1) == n + (int64_t)(t / 3 - 1) * nny + (t % 3 - 1);
+      if (regular) {
+        kind[n] = 0;
+        continue;
+      }
+      std::vector<double> px(cnt), py(cnt);
+      for (int q = 0; q < cnt; ++q) {
+        int32_t mm = mesh->patch_nodes[b0 + q] - 1;
+        px[q] = (xs[mm / nny] - xi) / h;
+        py[q] = (ys[mm % nny] - yi) / h;
+      }
+      std::vector<double> R(5 * cnt);
+      if (!ppr_rows(px, py, R.data())) continue;  // singular patch: no recovery at this node
+      kind[n] = 1;
+      ptr[n] = (int32_t)nodes.size();
+      for (int q = 0; q < cnt; ++q) nodes.push_back(mesh->patch_nodes[b0 + q] - 1);
+      rows.insert(rows.end(), R.begin(), R.end());
+    }
+    ptr[nn] = (int32_t)nodes.size();
+    // kind 1 rows are stored at 5*ptr[n]; ptr for kinds 0/2 is unused
+    PIC_CUDA(cudaMemcpyToSymbol(c_ppr_reg, g.h_ppr_reg, sizeof g.h_ppr_reg));
+    if ((rc = upload(&g.d_ppr_kind, kind.data(), kind.size()))) return rc;
+    // make ptr monotone for kind-1 lookups: ptr[n+1] must be the end of node n's patch
+    std::vector<int32_t> ptr2(nn + 1, 0);
+    {
+      int32_t acc = 0;
+      for (int64_t n = 0; n < nn; ++n) {
+        ptr2[n] = acc;
+        if (kind[n] == 1) {
+          int b0 = mesh->patch_ptr[n], cnt = mesh->patch_ptr[n + 1] - b0;
+          acc += cnt;
+        }
+      }
+      ptr2[nn] = acc;
+    }
+    if ((rc = upload(&g.d_ppr_ptr, ptr2.data(), ptr2.size()))) return rc;
+    if ((rc = upload(&g.d_ppr_nodes, nodes.data(), nodes.size()))) return rc;
+    if ((rc = upload(&g.d_ppr_rows, rows.data(), rows.size()))) return rc;
+    if ((rc = upload(&g.d_ppr_h, hs.data(), hs.size()))) return rc;
+  }
+  // fields and solver vectors
+  if ((rc = dalloc(&g.d_phi, nn))) return rc;
+  if ((rc = dalloc(&g.d_rho, nn))) return rc;
+  if ((rc = dalloc(&g.d_efx, nn))) return rc;
+  if ((rc = dalloc(&g.d_efy, nn))) return rc;
+  if ((rc = dalloc(&g.d_coef, 5 * nn))) return rc;
+  PIC_CUDA(cudaMemset(g.d_efx, 0, nn * sizeof(double)));
+  PIC_CUDA(cudaMemset(g.d_efy, 0, nn * sizeof(double)));
+  PIC_CUDA(cudaMemset(g.d_coef, 0, 5 * nn * sizeof(double)));
+  PIC_CUDA(cudaMemset(g.d_rho, 0, nn * sizeof(double)));
+  PIC_CUDA(cudaMemcpy(g.d_phi, mesh->phi_dirichlet, nn * sizeof(double), cudaMemcpyHostToDevice));
+  for (double **v : {&g.d_b, &g.d_x, &g.d_r, &g.d_w, &g.d_p[0], &g.d_p[1], &g.d_q}) {
+    if ((rc = dalloc(v, nn))) return rc;
+    PIC_CUDA(cudaMemset(*v, 0, nn * sizeof(double)));
+  }
+  g.red_blocks = (int)((nn + PIC_RED_CHUNK - 1) / PIC_RED_CHUNK);
+  if ((rc = dalloc(&g.d_part, 3 * (size_t)g.red_blocks))) return rc;
+  if ((rc = dalloc(&g.d_pcg, 1))) return rc;
+  PIC_CUDA(cudaMemset(g.d_pcg, 0, sizeof(PcgState)));
+  if ((rc = dalloc(&g.d_counters, 32))) return rc;
+  PIC_CUDA(cudaMemset(g.d_counters, 0, 32 * sizeof(unsigned long long)));
+  // sort scratch sized for the largest species
+  if ((rc = dalloc(&g.d_cell_count, ne + 1))) return rc;
+  if ((rc = dalloc(&g.d_cell_start, ne + 1))) return rc;
+  if ((rc = dalloc(&g.d_cell_fill, ne + 1))) return rc;
+  if ((rc = dalloc(&g.d_scan_blk, 4100))) return rc;
+  int64_t maxcap = 1;
+  g.ns = P.n_species;
+  for (int s = 0; s < g.ns; ++s) {
+    Species &sp = g.sp[s];
+    const pic_species_desc &d = P.species[s];
+    if (!(d.mass > 0) || d.capacity < 0 || d.capacity > ((int64_t)1 << 31) - 1) {
+      set_error("pic_init: bad species description");
+      free_all();
+      return PIC_ERR_ARG;
+    }
+    sp.charge = d.charge;
+    sp.mass = d.mass;
+    sp.weight = d.weight;
+    sp.qm = d.charge / (d.mass / PIC_ME);
+    sp.capacity = d.capacity;
+    maxcap = std::max(maxcap, d.capacity);
+    size_t c = (size_t)std::max<int64_t>(d.capacity, 1);
+    for (double **v : {&sp.x, &sp.y, &sp.vx, &sp.vy, &sp.vz, &sp.x2, &sp.y2, &sp.vx2, &sp.vy2, &sp.vz2})
+      if ((rc = dalloc(v, c))) return rc;
+    if ((rc = dalloc(&sp.loc, c))) return rc;
+    if ((rc = dalloc(&sp.loc2, c))) return rc;
+    if ((rc = dalloc(&sp.id, c))) return rc;
+    if ((rc = dalloc(&sp.id2, c))) return rc;
+    if ((rc = dalloc(&sp.q_acc, nn))) return rc;
+    if ((rc = dalloc(&sp.e_acc, nn))) return rc;
+    if ((rc = dalloc(&sp.rho_s, nn))) return rc;
+    if ((rc = dalloc(&sp.ek_s, nn))) return rc;
+    PIC_CUDA(cudaMemset(sp.q_acc, 0, nn * sizeof(unsigned long long)));
+    PIC_CUDA(cudaMemset(sp.e_acc, 0, nn * sizeof(unsigned long long)));
+    PIC_CUDA(cudaMemset(sp.rho_s, 0, nn * sizeof(double)));
+    PIC_CUDA(cudaMemset(sp.ek_s, 0, nn * sizeof(double)));
+  }
+  if ((rc = dalloc(&g.d_perm, maxcap))) return rc;
+  if ((rc = dalloc(&g.d_sort_id, maxcap))) return rc;
+  PIC_CUDA(cudaDeviceSynchronize());
+  g.inited = true;
+  return PIC_OK;
+}
+
+int pic_upload_particles(int32_t species, int64_t n, const double *x, const double *y,
+                         const double *vx, const double *vy, const double *vz, const int32_t *loc,
+                         const uint32_t *id) {
+  int rc;
+  if ((rc = check_init()) || (rc = check_species(species))) return rc;
+  Species &s = g.sp[species];
+  if (n < 0 || (n > 0 && (!x || !y || !vx || !vy || !vz))) {
+    set_error("pic_upload_particles: bad arguments");
+    return PIC_ERR_ARG;
+  }
+  if (n > s.capacity) {
+    set_error("pic_upload_particles: more particles than the species capacity");
+    return PIC_ERR_CAPACITY;
+  }
+  size_t b = (size_t)n * sizeof(double);
+  PIC_CUDA(cudaMemcpyAsync(s.x, x, b, cudaMemcpyHostToDevice, g.st));
+  PIC_CUDA(cudaMemcpyAsync(s.y, y, b, cudaMemcpyHostToDevice, g.st));
+  PIC_CUDA(cudaMemcpyAsync(s.vx, vx, b, cudaMemcpyHostToDevice, g.st));
+  PIC_CUDA(cudaMemcpyAsync(s.vy, vy, b, cudaMemcpyHostToDevice, g.st));
+  PIC_CUDA(cudaMemcpyAsync(s.vz, vz, b, cudaMemcpyHostToDevice, g.st));
+  std::vector<uint32_t> ids;
+  if (!id) {
+    ids.resize(n);
+    for (int64_t k = 0; k < n; ++k) ids[k] = (uint32_t)k;
+    id = ids.data();
+  }
+  uint32_t mx = 0;
+  for (int64_t k = 0; k < n; ++k) mx = std::max(mx, id[k]);
+  PIC_CUDA(cudaMemcpyAsync(s.id, id, (size_t)n * 4, cudaMemcpyHostToDevice, g.st));
+  s.n_slots = n;
+  s.n_live = n;
+  s.next_id = n ? mx + 1 : 0;
+  if (loc) {
+    for (int64_t k = 0; k < n; ++k)
+      if (loc[k] < -1 || loc[k] >= g.ne) {
+        s.n_slots = s.n_live = 0;
+        set_error("pic_upload_particles: element index out of range");
+        return PIC_ERR_ARG;
+      }
+    PIC_CUDA(cudaMemcpyAsync(s.loc, loc, (size_t)n * 4, cudaMemcpyHostToDevice, g.st));
+    PIC_CUDA(cudaStreamSynchronize(g.st));
+  } else {
+    PIC_CUDA(cudaMemsetAsync(s.loc, 0, (size_t)n * 4, g.st));
+    if ((rc = zero_counter(1))) return rc;
+    if ((rc = launch_locate(s, 0, n))) return rc;
+    unsigned long long bad = 0;
+    if ((rc = read_counter(1, &bad))) return rc;
+    if (bad) {
+      set_error("pic_upload_particles: particle outside the mesh");
+      return PIC_ERR_DOMAIN;
+    }
+  }
+  return PIC_OK;
+}
+
+int pic_particle_count(int32_t species, int64_t *n) {
+  int rc;
+  if ((rc = check_init()) || (rc = check_species(species))) return rc;
+  if (n) *n = g.sp[species].n_live;
+  return PIC_OK;
+}
+
+int pic_download_particles(int32_t species, int64_t capacity, double *x, double *y, double *vx,
+                           double *vy, double *vz, int32_t *loc, uint32_t *id, int64_t *n_out) {
+  int rc;
+  if ((rc = check_init()) || (rc = check_species(species))) return rc;
+  Species &s = g.sp[species];
+  // compact on the host side: copy all slots, keep live ones in order
+  int64_t ns = s.n_slots;
+  std::vector<int32_t> hl(ns);
+  PIC_CUDA(cudaMemcpyAsync(hl.data(), s.loc, ns * 4, cudaMemcpyDeviceToHost, g.st));
+  PIC_CUDA(cudaStreamSynchronize(g.st));
+  int64_t live = 0;
+  for (int64_t k = 0; k < ns; ++k) live += hl[k] >= 0;
+  if (n_out) *n_out = live;
+  if (live > capacity) {
+    set_error("pic_download_particles: output capacity too small");
+    return PIC_ERR_CAPACITY;
+  }
+  auto pull = [&](const void *src, void *dst, size_t esz) -> int {
+    if (!dst) return PIC_OK;
+    std::vector<char> tmp(ns * esz);
+    PIC_CUDA(cudaMemcpy(tmp.data(), src, ns * esz, cudaMemcpyDeviceToHost));
+    int64_t o = 0;
+    for (int64_t k = 0; k < ns; ++k)
+      if (hl[k] >= 0) std::memcpy((char *)dst + (o++) * esz, tmp.data() + k * esz, esz);
+    return PIC_OK;
+  };
+  if ((rc = pull(s.x, x, 8)) || (rc = pull(s.y, y, 8)) || (rc = pull(s.vx, vx, 8)) ||
+      (rc = pull(s.vy, vy, 8)) || (rc = pull(s.vz, vz, 8)) || (rc = pull(s.loc, loc, 4)) ||
+      (rc = pull(s.id, id, 4)))
+    return rc;
+  return PIC_OK;
+}
+
+int pic_particle_device_ptrs(int32_t species, void **ptrs7, int64_t *n_slots) {
+  int rc;
+  if ((rc = check_init()) || (rc = check_species(species))) return rc;
+  Species &s = g.sp[species];
+  if (ptrs7) {
+    ptrs7[0] = s.x; ptrs7[1] = s.y; ptrs7[2] = s.vx; ptrs7[3] = s.vy; ptrs7[4] = s.vz;
+    ptrs7[5] = s.loc; ptrs7[6] = s.id;
+  }
+  if (n_slots) *n_slots = s.n_slots;
+  return PIC_OK;
+}
+
+int pic_particle_positioning(int32_t species) {
+  int rc;
+  if ((rc = check_init())) return rc;
+  int s0 = species < 0 ? 0 : species, s1 = species < 0 ? g.ns : species + 1;
+  if (species >= 0 && (rc = check_species(species))) return rc;
+  if ((rc = zero_counter(1))) return rc;
+  for (int s = s0; s < s1; ++s)
+    if ((rc = launch_locate(g.sp[s], 0, g.sp[s].n_slots))) return rc;
+  unsigned long long bad = 0;
+  if ((rc = read_counter(1, &bad))) return rc;
+  if (bad) {
+    set_error("pic_particle_positioning: particle outside the mesh");
+    return PIC_ERR_DOMAIN;
+  }
+  return PIC_OK;
+}
+
+static int count_live(int sidx) {
+  Species &s = g.sp[sidx];
+  unsigned long long lost = 0;
+  int rc = read_counter(8 + sidx, &lost);
+  if (rc) return rc;
+  s.n_live -= (int64_t)lost;
+  return zero_counter(8 + sidx);
+}
+
+int pic_move_all(int32_t species, int32_t push_flag) {
+  int rc;
+  if ((rc = check_init()) || (rc = check_species(species))) return rc;
+  (void)push_flag;
+  if ((rc = zero_counter(8 + species))) return rc;
+  if ((rc = run_push(species, true, false))) return rc;
+  return count_live(species);
+}
+
+int pic_get_par_chg(int32_t delta, double *rho_out) {
+  int rc;
+  if ((rc = check_init())) return rc;
+  if (delta != 0) {
+    set_error("pic_get_par_chg: only delta = 0 is supported");
+    return PIC_ERR_ARG;
+  }
+  if ((rc = zero_deposit())) return rc;
+  if ((rc = zero_counter(1))) return rc;
+  for (int s = 0; s < g.ns; ++s) {
+    if ((rc = zero_counter(8 + s))) return rc;
+    if ((rc = run_push(s, false, true))) return rc;
+    if ((rc = count_live(s))) return rc;
+  }
+  if ((rc = run_rho())) return rc;
+  unsigned long long bad = 0;
+  if ((rc = read_counter(1, &bad))) return rc;
+  if (bad) {
+    set_error("pic_get_par_chg: particle outside the mesh");
+    return PIC_ERR_DOMAIN;
+  }
+  if (rho_out) {
+    PIC_CUDA(cudaMemcpyAsync(rho_out, g.d_rho, g.nn * sizeof(double), cudaMemcpyDeviceToHost, g.st));
+    PIC_CUDA(cudaStreamSynchronize(g.st));
+  }
+  return PIC_OK;
+}
+
+int pic_ife_solve(double *phi_inout, double time, pic_solve_stats *stats) {
+  int rc;
+  if ((rc = check_init())) return rc;
+  (void)time;
+  if (phi_inout)
+    PIC_CUDA(cudaMemcpyAsync(g.d_phi, phi_inout, g.nn * sizeof(double), cudaMemcpyHostToDevice, g.st));
+  PIC_CUDA(cudaEventRecord(g.ev0, g.st));
+  if ((rc = run_rhs())) return rc;
+  int src = run_pcg(stats);
+  PIC_CUDA(cudaEventRecord(g.ev1, g.st));
+  if (phi_inout)
+    PIC_CUDA(cudaMemcpyAsync(phi_inout, g.d_phi, g.nn * sizeof(double), cudaMemcpyDeviceToHost, g.st));
+  PIC_CUDA(cudaStreamSynchronize(g.st));
+  if (stats) {
+    float ms = 0;
+    cudaEventElapsedTime(&ms, g.ev0, g.ev1);
+    stats->ms = ms;
+  }
+  return src;
+}
+
+int pic_get_efield_ppr(double *efx_out, double *efy_out) {
+  int rc;
+  if ((rc = check_init())) return rc;
+  if ((rc = run_ppr())) return rc;
+  if (efx_out)
+    PIC_CUDA(cudaMemcpyAsync(efx_out, g.d_efx, g.nn * sizeof(double), cudaMemcpyDeviceToHost, g.st));
+  if (efy_out)
+    PIC_CUDA(cudaMemcpyAsync(efy_out, g.d_efy, g.nn * sizeof(double), cudaMemcpyDeviceToHost, g.st));
+  PIC_CUDA(cudaStreamSynchronize(g.st));
+  return PIC_OK;
+}
+
+int pic_sort_particles(int32_t species) {
+  int rc;
+  if ((rc = check_init()) || (rc = check_species(species))) return rc;
+  return sort_species(species);
+}
+
+int pic_step(uint64_t step, pic_step_stats *stats) {
+  int rc;
+  if ((rc = check_init())) return rc;
+  cudaEvent_t e[8];
+  for (auto &ev : e) PIC_CUDA(cudaEventCreate(&ev));
+  PIC_CUDA(cudaEventRecord(e[0], g.st));
+  // 1. fused push + locate + deposit (MoveAll, then GetParChg_2D)
+  if ((rc = zero_deposit())) return rc;
+  if ((rc = zero_counter(1))) return rc;
+  int64_t before[PIC_MAX_SPECIES];
+  int64_t pushed = 0;
+  for (int s = 0; s < g.ns; ++s) {
+    before[s] = g.sp[s].n_live;
+    pushed += before[s];
+    if ((rc = zero_counter(8 + s))) return rc;
+  }
+  PIC_CUDA(cudaEventRecord(e[6], g.st));
+  for (int s = 0; s < g.ns; ++s)
+    if ((rc = run_push(s, true, true))) return rc;
+  PIC_CUDA(cudaEventRecord(e[7], g.st));
+  if ((rc = run_rho())) return rc;
+  PIC_CUDA(cudaEventRecord(e[1], g.st));
+  // 2. Poisson (IFE_Solve_2D)
+  pic_solve_stats ss;
+  std::memset(&ss, 0, sizeof ss);
+  if ((rc = run_rhs())) return rc;
+  int solve_rc = run_pcg(&ss);
+  PIC_CUDA(cudaEventRecord(e[2], g.st));
+  // 3. PPR field recovery
+  if ((rc = run_ppr())) return rc;
+  PIC_CUDA(cudaEventRecord(e[3], g.st));
+  for (int s = 0; s < g.ns; ++s)
+    if ((rc = count_live(s))) return rc;
+  // 4. MCC
+  pic_mcc_stats ms;
+  std::memset(&ms, 0, sizeof ms);
+  if (g.mcc_ready)
+    if ((rc = mcc_run(step, &ms))) return rc;
+  PIC_CUDA(cudaEventRecord(e[4], g.st));
+  // 5. counting sort
+  if ((int64_t)(step % (uint64_t)g.P.sort_interval) == 0)
+    for (int s = 0; s < g.ns; ++s)
+      if ((rc = sort_species(s))) return rc;
+  PIC_CUDA(cudaEventRecord(e[5], g.st));
+  PIC_CUDA(cudaStreamSynchronize(g.st));
+  unsigned long long bad = 0;
+  if ((rc = read_counter(1, &bad))) return rc;
+  ++g.step_count;
+  if (stats) {
+    std::memset(stats, 0, sizeof *stats);
+    for (int s = 0; s < g.ns; ++s) {
+      stats->n_particles[s] = g.sp[s].n_live;
+      stats->n_lost[s] = before[s] - g.sp[s].n_live + ms.n_created[s];
+    }
+    stats->solve = ss;
+    stats->mcc = ms;
+    float t;
+    cudaEventElapsedTime(&t, e[0], e[1]); stats->ms_push = t;
+    cudaEventElapsedTime(&t, e[1], e[2]); stats->ms_solve = t; stats->solve.ms = t;
+    cudaEventElapsedTime(&t, e[2], e[3]); stats->ms_ppr = t;
+    cudaEventElapsedTime(&t, e[3], e[4]); stats->ms_mcc = t;
+    cudaEventElapsedTime(&t, e[4], e[5]); stats->ms_sort = t;
+    cudaEventElapsedTime(&t, e[0], e[5]); stats->ms_total = t;
+    cudaEventElapsedTime(&t, e[6], e[7]); stats->ms_push_kernel = t;
+    stats->pushed = pushed;
+  }
+  for (auto &ev : e) cudaEventDestroy(ev);
+  if (bad) {
+    set_error("pic_step: particle outside the mesh after the push");
+    return PIC_ERR_DOMAIN;
+  }
+  return solve_rc;
+}
+
+int pic_get_field(int32_t which, double *host_out) {
+  int rc;
+  if ((rc = check_init())) return rc;
+  if (!host_out) return PIC_ERR_ARG;
+  const double *src = nullptr;
+  if (which == 0) src = g.d_rho;
+  else if (which == 1) src = g.d_phi;
+  else if (which == 2) src = g.d_efx;
+  else if (which == 3) src = g.d_efy;
+  else if (which >= 4 && which < 4 + g.ns) src = g.sp[which - 4].rho_s;
+  else if (which >= 8 && which < 8 + g.ns) src = g.sp[which - 8].ek_s;
+  else if (which >= 12 && which <= 16) src = g.d_coef + (size_t)(which - 12) * g.nn;
+  else if (which == 20) src = g.d_b;
+  if (!src) {
+    set_error("pic_get_field: unknown field");
+    return PIC_ERR_ARG;
+  }
+  PIC_CUDA(cudaMemcpyAsync(host_out, src, g.nn * sizeof(double), cudaMemcpyDeviceToHost, g.st));
+  PIC_CUDA(cudaStreamSynchronize(g.st));
+  return PIC_OK;
+}
+
+int pic_set_field(int32_t which, const double *host_in) {
+  int rc;
+  if ((rc = check_init())) return rc;
+  if (!host_in) return PIC_ERR_ARG;
+  double *dst = nullptr;
+  if (which == 0) dst = g.d_rho;
+  else if (which == 1) dst = g.d_phi;
+  else if (which == 2) dst = g.d_efx;
+  else if (which == 3) dst = g.d_efy;
+  else if (which >= 12 && which <= 16) dst = g.d_coef + (size_t)(which - 12) * g.nn;
+  if (!dst) {
+    set_error("pic_set_field: unknown field");
+    return PIC_ERR_ARG;
+  }
+  PIC_CUDA(cudaMemcpyAsync(dst, host_in, g.nn * sizeof(double), cudaMemcpyHostToDevice, g.st));
+  PIC_CUDA(cudaStreamSynchronize(g.st));
+  return PIC_OK;
+}
+
+}  // extern "C"

@@ -1,0 +1,545 @@
+// sort_mcc.cu -- counting sort of the particle SoA and MCC_jw null collisions.
+//
+// Counting sort: particles are ordered by element, ties by particle id, so the
+// permutation is a pure function of (element, id) and the oracle reproduces it
+// exactly.  Absorbed slots (loc = -1) are dropped, which replaces the
+// reference's swap-with-last deletion (ParticleBundle.f90:120-127).
+//
+// MCC: the reference picks N = INT(NPar*P_null) (+1 with probability equal to
+// the residue) distinct particles by a partial Fisher-Yates shuffle
+// (mc/MCCPublic.F90:113-171).  Here every live particle gets a Philox key
+// keyed by (seed, id, step, species); the N particles with the smallest
+// (key, id) are selected.  That is the same law -- a uniform random N-subset --
+// computed with a histogram instead of a serial shuffle.  The collision itself
+// restates mc/TypeMCC.f90:58-198, mc/MCCChi.f90, mc/MCCElectron.F90:13-148 and
+// mc/MCCIon.F90:6-75 with Philox draws instead of RANDOM_NUMBER.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cmath>
+#include <cstring>
+#include <vector>
+
+#include "pic_ctx.h"
+#include "pic_mcc_kin.h"
+
+namespace pic {
+
+// ---------------------------------------------------------------------------
+// counting sort
+// ---------------------------------------------------------------------------
+
+__global__ void k_sort_count(const int32_t *__restrict__ loc, int64_t n, int32_t *__restrict__ count) {
+  int64_t p = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  int key = (p < n) ? loc[p] : -1;
+  unsigned int peers = __match_any_sync(0xffffffffu, key);
+  int lane = threadIdx.x & 31;
+  if (key >= 0 && (__ffs(peers) - 1) == lane) atomicAdd(count + key, __popc(peers));
+}
+
+// exclusive scan, 3 passes of 4096 items per block
+__global__ void __launch_bounds__(1024) k_scan_block(const int32_t *in, int32_t *out, int64_t n,
+                                                     int32_t *blk) {
+  __shared__ int32_t s[1024];
+  int64_t base = (int64_t)blockIdx.x * 4096 + threadIdx.x * 4;
+  int32_t v[4], sum = 0;
+  for (int k = 0; k < 4; ++k) {
+    v[k] = (base + k < n) ? in[base + k] : 0;
+    sum += v[k];
+  }
+  s[threadIdx.x] = sum;
+  __syncthreads();
+  for (int off = 1; off < 1024; off <<= 1) {
+    int32_t t = (threadIdx.x >= off) ? s[threadIdx.x - off] : 0;
+    __syncthreads();
+    s[threadIdx.x] += t;
+    __syncthreads();
+  }
+  int32_t run = s[threadIdx.x] - sum;
+  for (int k = 0; k < 4; ++k) {
+    if (base + k < n) out[base + k] = run;
+    run += v[k];
+  }
+  if (threadIdx.x == 1023) blk[blockIdx.x] = s[1023];
+}
+
+__global__ void k_scan_add(int32_t *out, int64_t n, const int32_t *blk_scanned) {
+  int64_t i = (int64_t)blockIdx.x * 4096 + threadIdx.x;
+  int32_t add = blk_scanned[blockIdx.x];
+  for (int k = 0; k < 4; ++k) {
+    int64_t q = i + k * 1024;
+    if (q < n) out[q] += add;
+  }
+}
+
+static int scan_exclusive(int32_t *in, int32_t *out, int64_t n) {
+  int nb = (int)((n + 4095) / 4096);
+  if (nb > 4096) {
+    set_error("scan: more than 16.7M cells");
+    return PIC_ERR_ARG;
+  }
+  k_scan_block<<<nb, 1024, 0, g.st>>>(in, out, n, g.d_scan_blk);
+  PIC_LAUNCHED();
+  if (nb > 1) {
+    // scan the block totals in place (<= 4096 of them: one block)
+    k_scan_block<<<1, 1024, 0, g.st>>>(g.d_scan_blk, g.d_scan_blk, nb, g.d_scan_blk + 4096);
+    PIC_LAUNCHED();
+    k_scan_add<<<nb, 1024, 0, g.st>>>(out, n, g.d_scan_blk);
+    PIC_LAUNCHED();
+  }
+  return PIC_OK;
+}
+
+__global__ void k_sort_scatter(const int32_t *__restrict__ loc, const uint32_t *__restrict__ id, int64_t n,
+                               int32_t *__restrict__ cursor, int32_t *__restrict__ perm,
+                               uint32_t *__restrict__ sid) {
+  int64_t p = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  int key = (p < n) ? loc[p] : -1;
+  unsigned int peers = __match_any_sync(0xffffffffu, key);
+  int lane = threadIdx.x & 31;
+  int leader = __ffs(peers) - 1;
+  int base = 0;
+  if (key >= 0 && lane == leader) base = atomicAdd(cursor + key, __popc(peers));
+  base = __shfl_sync(peers, base, leader);
+  if (key >= 0) {
+    int rank = __popc(peers & ((1u << lane) - 1u));
+    int dst = base + rank;
+    perm[dst] = (int32_t)p;
+    sid[dst] = id[p];
+  }
+}
+
+// One warp per element: order its segment by id (ids are unique), writing the
+// source slots to perm2.
+__global__ void k_sort_cells(const int32_t *__restrict__ start, int64_t ne, const int32_t *__restrict__ perm,
+                             const uint32_t *__restrict__ sid, int32_t *__restrict__ perm2) {
+  __shared__ uint32_t sh[8][128];
+  int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  int64_t c = (int64_t)blockIdx.x * 8 + warp;
+  if (c >= ne) return;
+  int s0 = start[c], s1 = start[c + 1], m = s1 - s0;
+  if (m <= 0) return;
+  if (m == 1) {
+    if (lane == 0) perm2[s0] = perm[s0];
+    return;
+  }
+  const bool in_smem = m <= 128;
+  if (in_smem)
+    for (int k = lane; k < m; k += 32) sh[warp][k] = sid[s0 + k];
+  __syncwarp();
+  for (int k = lane; k < m; k += 32) {
+    uint32_t me = in_smem ? sh[warp][k] : sid[s0 + k];
+    int rank = 0;
+    for (int q = 0; q < m; ++q) rank += ((in_smem ? sh[warp][q] : sid[s0 + q]) < me);
+    perm2[s0 + rank] = perm[s0 + k];
+  }
+}
+
+template <class T>
+__global__ void k_gather(const T *__restrict__ src, T *__restrict__ dst, const int32_t *__restrict__ perm,
+                         int64_t n) {
+  int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i < n) dst[i] = src[perm[i]];
+}
+
+struct Gather7 {
+  const double *x, *y, *vx, *vy, *vz;
+  const int32_t *loc;
+  const uint32_t *id;
+  double *ox, *oy, *ovx, *ovy, *ovz;
+  int32_t *oloc;
+  uint32_t *oid;
+};
+
+__global__ void k_gather_all(Gather7 g7, const int32_t *__restrict__ perm, int64_t n) {
+  int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  int32_t p = perm[i];
+  g7.ox[i] = g7.x[p];
+  g7.oy[i] = g7.y[p];
+  g7.ovx[i] = g7.vx[p];
+  g7.ovy[i] = g7.vy[p];
+  g7.ovz[i] = g7.vz[p];
+  g7.oloc[i] = g7.loc[p];
+  g7.oid[i] = g7.id[p];
+}
+
+static int32_t *g_perm2 = nullptr;
+static int64_t g_perm2_cap = 0;
+
+int sort_species(int sidx) {
+  Species &s = g.sp[sidx];
+  const int64_t ne = g.ne;
+  if (s.n_slots == 0) return PIC_OK;
+  if (g_perm2_cap < s.capacity) {
+    if (g_perm2) cudaFree(g_perm2);
+    g_perm2 = nullptr;
+    PIC_CUDA(cudaMalloc(&g_perm2, std::max<int64_t>(s.capacity, 1) * sizeof(int32_t)));
+    g_perm2_cap = s.capacity;
+  }
+  PIC_CUDA(cudaMemsetAsync(g.d_cell_count, 0, (ne + 1) * sizeof(int32_t), g.st));
+  k_sort_count<<<blocks_for(s.n_slots, 256), 256, 0, g.st>>>(s.loc, s.n_slots, g.d_cell_count);
+  PIC_LAUNCHED();
+  int rc = scan_exclusive(g.d_cell_count, g.d_cell_start, ne + 1);
+  if (rc) return rc;
+  PIC_CUDA(cudaMemcpyAsync(g.d_cell_fill, g.d_cell_start, (ne + 1) * sizeof(int32_t),
+                           cudaMemcpyDeviceToDevice, g.st));
+  int32_t total = 0;
+  PIC_CUDA(cudaMemcpyAsync(&total, g.d_cell_start + ne, sizeof total, cudaMemcpyDeviceToHost, g.st));
+  k_sort_scatter<<<blocks_for(s.n_slots, 256), 256, 0, g.st>>>(s.loc, s.id, s.n_slots, g.d_cell_fill,
+                                                               g.d_perm, g.d_sort_id);
+  PIC_LAUNCHED();
+  k_sort_cells<<<blocks_for(ne, 8), 256, 0, g.st>>>(g.d_cell_start, ne, g.d_perm, g.d_sort_id, g_perm2);
+  PIC_LAUNCHED();
+  PIC_CUDA(cudaStreamSynchronize(g.st));
+  if (total > 0) {
+    Gather7 g7{s.x, s.y, s.vx, s.vy, s.vz, s.loc, s.id, s.x2, s.y2, s.vx2, s.vy2, s.vz2, s.loc2, s.id2};
+    k_gather_all<<<blocks_for(total, 256), 256, 0, g.st>>>(g7, g_perm2, total);
+    PIC_LAUNCHED();
+  }
+  std::swap(s.x, s.x2);
+  std::swap(s.y, s.y2);
+  std::swap(s.vx, s.vx2);
+  std::swap(s.vy, s.vy2);
+  std::swap(s.vz, s.vz2);
+  std::swap(s.loc, s.loc2);
+  std::swap(s.id, s.id2);
+  s.n_slots = total;
+  s.n_live = total;
+  return PIC_OK;
+}
+
+// ---------------------------------------------------------------------------
+// MCC
+// ---------------------------------------------------------------------------
+
+struct MccK {
+  double *x, *y, *vx, *vy, *vz;
+  const int32_t *loc;
+  const uint32_t *id;
+  int64_t n;
+  uint32_t seed0, seed1, step_lo, step_hi, species;
+};
+
+__global__ void k_mcc_hist(MccK k, uint32_t *__restrict__ hist) {
+  int64_t p = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (p >= k.n || k.loc[p] < 0) return;
+  uint32_t key = mcc_select_key(k.id[p], k.step_lo, k.step_hi, k.species, k.seed0, k.seed1);
+  atomicAdd(hist + (key >> 16), 1u);
+}
+
+// particles below the threshold bin are selected; the threshold bin's
+// particles become candidates ordered later by (key, id)
+__global__ void k_mcc_pick(MccK k, uint32_t bstar, int32_t *__restrict__ sel, int64_t *__restrict__ misc,
+                           uint64_t *__restrict__ cand, int32_t *__restrict__ cand_slot, int64_t cand_cap) {
+  int64_t p = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (p >= k.n || k.loc[p] < 0) return;
+  uint32_t key = mcc_select_key(k.id[p], k.step_lo, k.step_hi, k.species, k.seed0, k.seed1);
+  uint32_t bin = key >> 16;
+  if (bin < bstar) {
+    long long i = atomicAdd((unsigned long long *)&misc[0], 1ull);
+    sel[i] = (int32_t)p;
+  } else if (bin == bstar) {
+    long long i = atomicAdd((unsigned long long *)&misc[1], 1ull);
+    if (i < cand_cap) {
+      cand[i] = ((uint64_t)key << 32) | (uint64_t)k.id[p];
+      cand_slot[i] = (int32_t)p;
+    }
+  }
+}
+
+struct CollK {
+  MccK k;
+  const int32_t *sel;
+  int64_t n_sel;
+  const double *prob;
+  McTable tab;
+  McGas gas;
+  double mass, vref;
+  int64_t *misc;        // [2..2+NR) reaction counts, [12] ionisations
+  int64_t *ion_parent;  // (id << 32) | slot
+  double *ion_data;     // 6 doubles per ionisation
+  int64_t ion_cap;
+};
+
+__global__ void k_mcc_collide(CollK c) {
+  int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= c.n_sel) return;
+  int32_t p = c.sel[t];
+  McParticle P;
+  P.vx = c.k.vx[p] * c.vref;
+  P.vy = c.k.vy[p] * c.vref;
+  P.vz = c.k.vz[p] * c.vref;
+  McOut out;
+  McRng rng;
+  mc_rng_init(&rng, c.k.id[p], c.k.step_lo, c.k.step_hi, c.k.species, c.k.seed0, c.k.seed1);
+  mc_collide(&P, &c.tab, c.prob, &c.gas, c.mass, &rng, &out);
+  c.k.vx[p] = P.vx / c.vref;
+  c.k.vy[p] = P.vy / c.vref;
+  c.k.vz[p] = P.vz / c.vref;
+  if (out.reaction > 0) atomicAdd((unsigned long long *)&c.misc[2 + out.reaction - 1], 1ull);
+  if (out.ionised) {
+    long long i = atomicAdd((unsigned long long *)&c.misc[12], 1ull);
+    if (i < c.ion_cap) {
+      c.ion_parent[i] = ((int64_t)c.k.id[p] << 32) | (int64_t)p;
+      double *d = c.ion_data + 6 * i;
+      d[0] = out.e_new[0] / c.vref;
+      d[1] = out.e_new[1] / c.vref;
+      d[2] = out.e_new[2] / c.vref;
+      d[3] = out.ion_new[0];  // SI, converted with the ion species' factor on append
+      d[4] = out.ion_new[1];
+      d[5] = out.ion_new[2];
+    }
+  }
+}
+
+struct AppendK {
+  const double *px, *py;
+  const int32_t *ploc;
+  double *x, *y, *vx, *vy, *vz;
+  int32_t *loc;
+  uint32_t *id;
+  int64_t base;
+  uint32_t id_base;
+  const int32_t *parent_slot;  // in rank order
+  const double *vel;           // 3 per created particle, normalised
+  int64_t n;
+};
+
+__global__ void k_mcc_append(AppendK a) {
+  int64_t r = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (r >= a.n) return;
+  int32_t ps = a.parent_slot[r];
+  int64_t d = a.base + r;
+  a.x[d] = a.px[ps];
+  a.y[d] = a.py[ps];
+  a.vx[d] = a.vel[3 * r + 0];
+  a.vy[d] = a.vel[3 * r + 1];
+  a.vz[d] = a.vel[3 * r + 2];
+  a.loc[d] = a.ploc[ps];
+  a.id[d] = a.id_base + (uint32_t)r;
+}
+
+static int mcc_alloc(int64_t need) {
+  if (need <= g.mcc_cap) return PIC_OK;
+  int64_t cap = std::max<int64_t>(need, 1 << 16);
+  cudaFree(g.d_sel);
+  cudaFree(g.d_cand);
+  cudaFree(g.d_cand_slot);
+  cudaFree(g.d_ion_parent);
+  cudaFree(g.d_ion_data);
+  PIC_CUDA(cudaMalloc(&g.d_sel, cap * sizeof(int32_t)));
+  PIC_CUDA(cudaMalloc(&g.d_cand, cap * sizeof(uint64_t)));
+  PIC_CUDA(cudaMalloc(&g.d_cand_slot, cap * sizeof(int32_t)));
+  PIC_CUDA(cudaMalloc(&g.d_ion_parent, cap * sizeof(int64_t)));
+  PIC_CUDA(cudaMalloc(&g.d_ion_data, 6 * cap * sizeof(double)));
+  g.mcc_cap = cap;
+  return PIC_OK;
+}
+
+struct Pending {
+  int32_t from_species;
+  std::vector<int64_t> parent;  // sorted (id<<32 | slot)
+  std::vector<double> data;     // 6 per entry, parent order
+  int32_t e_species, ion_species;
+};
+
+int mcc_run(uint64_t step, pic_mcc_stats *stats) {
+  std::vector<Pending> pend;
+  const uint32_t seed0 = (uint32_t)g.P.seed, seed1 = (uint32_t)(g.P.seed >> 32);
+  const uint32_t slo = (uint32_t)step, shi = (uint32_t)(step >> 32);
+  for (int s = 0; s < g.ns; ++s) {
+    Species &sp = g.sp[s];
+    if (!sp.has_mcc || sp.n_live == 0) continue;
+    int64_t npar = sp.n_live;
+    int64_t ncoll = mcc_n_collisions(npar, sp.tab.collision_ratio, slo, shi, (uint32_t)s, seed0, seed1);
+    if (stats) stats->n_selected[s] = ncoll;
+    if (ncoll <= 0) continue;
+    int rc = mcc_alloc(ncoll + 4096);
+    if (rc) return rc;
+    MccK k{sp.x, sp.y, sp.vx, sp.vy, sp.vz, sp.loc, sp.id, sp.n_slots, seed0, seed1, slo, shi, (uint32_t)s};
+    PIC_CUDA(cudaMemsetAsync(g.d_hist, 0, 65536 * sizeof(uint32_t), g.st));
+    PIC_CUDA(cudaMemsetAsync(g.d_mcc_misc, 0, 16 * sizeof(int64_t), g.st));
+    k_mcc_hist<<<blocks_for(sp.n_slots, 256), 256, 0, g.st>>>(k, g.d_hist);
+    PIC_LAUNCHED();
+    std::vector<uint32_t> hist(65536);
+    PIC_CUDA(cudaMemcpyAsync(hist.data(), g.d_hist, 65536 * 4, cudaMemcpyDeviceToHost, g.st));
+    PIC_CUDA(cudaStreamSynchronize(g.st));
+    int64_t below = 0;
+    uint32_t bstar = 0;
+    for (; bstar < 65536; ++bstar) {
+      if (below + hist[bstar] >= ncoll) break;
+      below += hist[bstar];
+    }
+    if (bstar >= 65536) {
+      set_error("mcc: fewer live particles than collisions requested");
+      return PIC_ERR_STATE;
+    }
+    int64_t need = ncoll - below;
+    int64_t ncand_expect = hist[bstar];
+    rc = mcc_alloc(std::max<int64_t>(ncoll, ncand_expect) + 4096);
+    if (rc) return rc;
+    k_mcc_pick<<<blocks_for(sp.n_slots, 256), 256, 0, g.st>>>(k, bstar, g.d_sel, g.d_mcc_misc, g.d_cand,
+                                                              g.d_cand_slot, g.mcc_cap);
+    PIC_LAUNCHED();
+    int64_t misc[2];
+    PIC_CUDA(cudaMemcpyAsync(misc, g.d_mcc_misc, 2 * sizeof(int64_t), cudaMemcpyDeviceToHost, g.st));
+    PIC_CUDA(cudaStreamSynchronize(g.st));
+    int64_t nsel = misc[0], ncand = misc[1];
+    if (ncand != ncand_expect || nsel != below) {
+      set_error("mcc: selection histogram mismatch");
+      return PIC_ERR_CUDA;
+    }
+    {
+      std::vector<uint64_t> cand(ncand);
+      std::vector<int32_t> cslot(ncand);
+      PIC_CUDA(cudaMemcpy(cand.data(), g.d_cand, ncand * 8, cudaMemcpyDeviceToHost));
+      PIC_CUDA(cudaMemcpy(cslot.data(), g.d_cand_slot, ncand * 4, cudaMemcpyDeviceToHost));
+      std::vector<int64_t> order(ncand);
+      for (int64_t i = 0; i < ncand; ++i) order[i] = i;
+      std::sort(order.begin(), order.end(), [&](int64_t a, int64_t b) { return cand[a] < cand[b]; });
+      std::vector<int32_t> add(need);
+      for (int64_t i = 0; i < need; ++i) add[i] = cslot[order[i]];
+      if (need > 0)
+        PIC_CUDA(cudaMemcpy(g.d_sel + nsel, add.data(), need * 4, cudaMemcpyHostToDevice));
+    }
+    CollK c;
+    c.k = k;
+    c.sel = g.d_sel;
+    c.n_sel = ncoll;
+    c.prob = sp.prob;
+    c.tab = mc_table_from(sp.tab);
+    c.gas.mass = g.gas.mass;
+    c.gas.temperature = g.gas.temperature;
+    c.mass = sp.mass;
+    c.vref = g.v_ref;
+    c.misc = g.d_mcc_misc;
+    c.ion_parent = g.d_ion_parent;
+    c.ion_data = g.d_ion_data;
+    c.ion_cap = g.mcc_cap;
+    k_mcc_collide<<<blocks_for(ncoll, 128), 128, 0, g.st>>>(c);
+    PIC_LAUNCHED();
+    int64_t m2[16];
+    PIC_CUDA(cudaMemcpyAsync(m2, g.d_mcc_misc, sizeof m2, cudaMemcpyDeviceToHost, g.st));
+    PIC_CUDA(cudaStreamSynchronize(g.st));
+    if (stats)
+      for (int r = 0; r < sp.tab.n_reaction && r < 8; ++r) stats->n_by_reaction[s][r] = m2[2 + r];
+    int64_t nion = m2[12];
+    if (nion > g.mcc_cap) {
+      set_error("mcc: ionisation buffer overflow");
+      return PIC_ERR_CAPACITY;
+    }
+    if (nion > 0) {
+      Pending pd;
+      pd.from_species = s;
+      pd.parent.resize(nion);
+      std::vector<double> data(6 * nion);
+      PIC_CUDA(cudaMemcpy(pd.parent.data(), g.d_ion_parent, nion * 8, cudaMemcpyDeviceToHost));
+      PIC_CUDA(cudaMemcpy(data.data(), g.d_ion_data, nion * 48, cudaMemcpyDeviceToHost));
+      std::vector<int64_t> order(nion);
+      for (int64_t i = 0; i < nion; ++i) order[i] = i;
+      std::sort(order.begin(), order.end(), [&](int64_t a, int64_t b) { return pd.parent[a] < pd.parent[b]; });
+      std::vector<int64_t> par2(nion);
+      pd.data.resize(6 * nion);
+      for (int64_t i = 0; i < nion; ++i) {
+        par2[i] = pd.parent[order[i]];
+        for (int q = 0; q < 6; ++q) pd.data[6 * i + q] = data[6 * order[i] + q];
+      }
+      pd.parent.swap(par2);
+      pd.e_species = s;
+      // resultant of the ionisation reaction
+      pd.ion_species = -1;
+      for (int r = 0; r < sp.tab.n_reaction; ++r)
+        if (sp.tab.reaction_type[r] == 13) pd.ion_species = sp.tab.resultant[r];
+      pend.push_back(std::move(pd));
+    }
+  }
+  // MCCAddNewParticle: append the created particles after all species collided
+  for (auto &pd : pend) {
+    int64_t nion = (int64_t)pd.parent.size();
+    std::vector<int32_t> pslot(nion);
+    for (int64_t i = 0; i < nion; ++i) pslot[i] = (int32_t)(pd.parent[i] & 0xffffffff);
+    int32_t *d_pslot = nullptr;
+    double *d_vel = nullptr;
+    PIC_CUDA(cudaMalloc(&d_pslot, nion * 4));
+    PIC_CUDA(cudaMalloc(&d_vel, 3 * nion * 8));
+    PIC_CUDA(cudaMemcpy(d_pslot, pslot.data(), nion * 4, cudaMemcpyHostToDevice));
+    Species &from = g.sp[pd.from_species];
+    for (int which = 0; which < 2; ++which) {
+      int ts = which == 0 ? pd.e_species : pd.ion_species;
+      if (ts < 0 || ts >= g.ns) continue;
+      Species &to = g.sp[ts];
+      if (to.n_slots + nion > to.capacity) {
+        cudaFree(d_pslot);
+        cudaFree(d_vel);
+        set_error("mcc: particle capacity exceeded by ionisation");
+        return PIC_ERR_CAPACITY;
+      }
+      std::vector<double> vel(3 * nion);
+      for (int64_t i = 0; i < nion; ++i)
+        for (int q = 0; q < 3; ++q)
+          vel[3 * i + q] = which == 0 ? pd.data[6 * i + q] : pd.data[6 * i + 3 + q] / g.v_ref;
+      PIC_CUDA(cudaMemcpy(d_vel, vel.data(), 3 * nion * 8, cudaMemcpyHostToDevice));
+      AppendK a{from.x, from.y, from.loc, to.x, to.y, to.vx, to.vy, to.vz, to.loc, to.id,
+                to.n_slots, to.next_id, d_pslot, d_vel, nion};
+      k_mcc_append<<<blocks_for(nion, 256), 256, 0, g.st>>>(a);
+      PIC_LAUNCHED();
+      PIC_CUDA(cudaStreamSynchronize(g.st));
+      to.n_slots += nion;
+      to.n_live += nion;
+      to.next_id += (uint32_t)nion;
+      if (stats) stats->n_created[ts] += nion;
+    }
+    cudaFree(d_pslot);
+    cudaFree(d_vel);
+  }
+  return PIC_OK;
+}
+
+}  // namespace pic
+
+using namespace pic;
+
+extern "C" int pic_mcc_init(const pic_gas *gas, int32_t n_tables, const pic_mcc_table *tables) {
+  if (!g.inited) {
+    set_error("pic_mcc_init: library not initialised");
+    return PIC_ERR_STATE;
+  }
+  if (!gas || n_tables < 0 || (n_tables > 0 && !tables)) {
+    set_error("pic_mcc_init: bad arguments");
+    return PIC_ERR_ARG;
+  }
+  g.gas = *gas;
+  for (int t = 0; t < n_tables; ++t) {
+    const pic_mcc_table &T = tables[t];
+    if (T.species < 0 || T.species >= g.ns || T.n_reaction < 1 || T.n_reaction > PIC_MAX_REACTIONS ||
+        T.n_sigma < 2 || !T.probability || !(T.collision_ratio >= 0 && T.collision_ratio < 1)) {
+      set_error("pic_mcc_init: bad table");
+      return PIC_ERR_ARG;
+    }
+    Species &sp = g.sp[T.species];
+    sp.tab = T;
+    sp.has_mcc = true;
+    if (sp.prob) cudaFree(sp.prob);
+    size_t n = (size_t)T.n_sigma * T.n_reaction;
+    PIC_CUDA(cudaMalloc(&sp.prob, n * sizeof(double)));
+    PIC_CUDA(cudaMemcpy(sp.prob, T.probability, n * sizeof(double), cudaMemcpyHostToDevice));
+    sp.tab.probability = nullptr;
+  }
+  if (!g.d_hist) PIC_CUDA(cudaMalloc(&g.d_hist, 65536 * sizeof(uint32_t)));
+  if (!g.d_mcc_misc) PIC_CUDA(cudaMalloc(&g.d_mcc_misc, 16 * sizeof(int64_t)));
+  g.mcc_ready = n_tables > 0;
+  return PIC_OK;
+}
+
+extern "C" int pic_mcc(uint64_t step, pic_mcc_stats *stats) {
+  if (!g.inited) {
+    set_error("pic_mcc: library not initialised");
+    return PIC_ERR_STATE;
+  }
+  pic_mcc_stats local;
+  std::memset(&local, 0, sizeof local);
+  int rc = g.mcc_ready ? mcc_run(step, &local) : PIC_OK;
+  if (stats) *stats = local;
+  return rc;
+}

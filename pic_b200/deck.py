@@ -1,0 +1,264 @@
+"""Input decks of the IFE-PIC step: the benchmark configurations, the
+reference normalisation (Input_2D.f90:362-392), the mesh built by the
+library's mesh builder, and the seeded particle loader.
+
+All lengths handed to the library are normalised by L_ref (the Debye length
+at n_ref = n0, T_ref = Te), potentials by Phi_ref = kB*T_ref/e, velocities by
+v_ref = sqrt(kB*T_ref/m_e) and time by time_ref = 1/omega_pe.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import math
+from dataclasses import dataclass, field
+
+import numpy as np
+
+from . import api
+
+KB = 1.3807e-23
+QE = 1.6022e-19
+ME = 9.1095e-31
+AMU = 1.660539040e-27
+EPS0 = 8.8542e-12
+EVTOK = 11605.0
+AR_MASS = 39.95 * AMU
+
+
+def reference_scales(n_ref: float, T_eV: float) -> dict:
+    """L_ref, time_ref, v_ref, Phi_ref exactly as Input_2D.f90:362-392."""
+    T_ref = T_eV * EVTOK
+    return {
+        "L_ref": math.sqrt(EPS0 * KB * T_ref / n_ref / QE / QE),
+        "time_ref": math.sqrt(EPS0 * ME / n_ref / QE / QE),
+        "v_ref": math.sqrt(KB * T_ref / ME),
+        "Phi_ref": KB * T_ref / QE,
+    }
+
+
+@dataclass
+class ObjectSpec:
+    shape: int                 # api.PIC_SHAPE_*
+    cx: float                  # m
+    cy: float
+    a: float                   # radius / semi-axis / box upper-right x (m)
+    b: float = 0.0
+    angle: float = 0.0
+    eps: float = 1.0
+    conductor: bool = False
+    phi_V: float = 0.0
+
+
+@dataclass
+class Config:
+    name: str
+    Lx: float
+    Ly: float
+    ncx: int
+    ncy: int
+    objects: list = field(default_factory=list)
+    wall_dirichlet: tuple = (1, 1, 1, 1)    # left, right, bottom, top
+    wall_V: tuple = (0.0, 0.0, 0.0, 0.0)
+    wall_particles: tuple = (0, 0, 0, 0)    # api.PIC_WALL_*
+    n0: float = 1e15
+    ppc: int = 50
+    Te_eV: float = 2.0
+    Ti_eV: float = 0.026
+    gas_p_Pa: float = 1.33
+    gas_T_K: float = 300.0
+    dt: float = 0.05
+    nt: int = 1000
+    pcg_tol: float = 1e-10
+    pcg_maxit: int = 50000
+    seed: int = 0
+    mcc: bool = True
+    precision: int = api.PIC_PREC_FP64
+    sort_interval: int = 10
+
+    @property
+    def scales(self) -> dict:
+        return reference_scales(self.n0, self.Te_eV)
+
+
+def _seeded_disks(rng, n, Lx, Ly, rmin, rmax, margin):
+    disks = []
+    for _ in range(10000):
+        if len(disks) == n:
+            break
+        r = rng.uniform(rmin, rmax)
+        cx = rng.uniform(r + margin, Lx - r - margin)
+        cy = rng.uniform(r + margin, Ly - r - margin)
+        if all(math.hypot(cx - x, cy - y) > r + rr + margin for x, y, rr in disks):
+            disks.append((cx, cy, r))
+    if len(disks) < n:
+        raise RuntimeError("could not place non-overlapping objects")
+    return disks
+
+
+def config(name: str, **over) -> Config:
+    """The five benchmark decks (seeded; geometry in metres)."""
+    if name == "cfg1":
+        c = Config("cfg1-64x64-disk", 0.04, 0.04, 64, 64,
+                   objects=[ObjectSpec(api.PIC_SHAPE_CIRCLE, 0.02, 0.02, 0.008, eps=4.0)],
+                   wall_V=(50.0, 0.0, 0.0, 0.0), n0=1e15, ppc=50, Te_eV=2.0, nt=1000,
+                   pcg_tol=1e-10, seed=0)
+    elif name == "cfg2":
+        rng = np.random.default_rng(20240602)
+        disks = _seeded_disks(rng, 4, 0.16, 0.16, 0.01, 0.02, 0.004)
+        eps = [2.0, 4.0, 10.0]
+        objs = [ObjectSpec(api.PIC_SHAPE_CIRCLE, x, y, r, eps=eps[k]) for k, (x, y, r) in
+                enumerate(disks[:3])]
+        x, y, r = disks[3]
+        objs.append(ObjectSpec(api.PIC_SHAPE_CIRCLE, x, y, r, conductor=True, phi_V=-20.0))
+        c = Config("cfg2-512x512-4disks", 0.16, 0.16, 512, 512, objects=objs,
+                   wall_V=(0.0, 0.0, 0.0, 0.0), n0=5e15, ppc=100, Te_eV=3.0, nt=2000,
+                   pcg_tol=1e-10, seed=1)
+    elif name == "cfg3":
+        c = Config("cfg3-1024x1024-disk-mixed", 0.04, 0.04, 1024, 1024,
+                   objects=[ObjectSpec(api.PIC_SHAPE_CIRCLE, 0.02, 0.02, 0.008, eps=4.0)],
+                   wall_V=(50.0, 0.0, 0.0, 0.0), n0=1e15, ppc=64, Te_eV=2.0, nt=1000,
+                   pcg_tol=1e-8, seed=0, precision=api.PIC_PREC_MIXED)
+    elif name == "cfg4":
+        rng = np.random.default_rng(20240604)
+        objs = []
+        placed = []
+        while len(objs) < 8:
+            a, b = rng.uniform(0.005, 0.03, size=2)
+            ang = rng.uniform(0, math.pi)
+            R = max(a, b)
+            cx = rng.uniform(R + 0.004, 0.16 - R - 0.004)
+            cy = rng.uniform(R + 0.004, 0.16 - R - 0.004)
+            if all(math.hypot(cx - x, cy - y) > R + rr + 0.004 for x, y, rr in placed):
+                placed.append((cx, cy, R))
+                eps = math.exp(rng.uniform(0.0, math.log(20.0)))
+                objs.append(ObjectSpec(api.PIC_SHAPE_ELLIPSE, cx, cy, a, b, ang, eps=eps))
+        c = Config("cfg4-1024x1024-8ellipses", 0.16, 0.16, 1024, 1024, objects=objs,
+                   wall_V=(0.0, 0.0, 0.0, 0.0), n0=5e15, ppc=64, Te_eV=3.0, nt=5000,
+                   pcg_tol=1e-8, seed=4)
+    elif name == "tiny":
+        c = Config("tiny-16x16-disk", 0.01, 0.01, 16, 16,
+                   objects=[ObjectSpec(api.PIC_SHAPE_CIRCLE, 0.005, 0.0051, 0.0023, eps=4.0)],
+                   wall_V=(5.0, 0.0, 0.0, 0.0), n0=1e15, ppc=8, Te_eV=2.0, nt=10,
+                   pcg_tol=1e-10, seed=3)
+    else:
+        raise KeyError(name)
+    for k, v in over.items():
+        setattr(c, k, v)
+    return c
+
+
+def make_deck(cfg: Config) -> api.Deck:
+    sc = cfg.scales
+    L, P = sc["L_ref"], sc["Phi_ref"]
+    d = api.Deck()
+    d.nnx, d.nny = cfg.ncx + 1, cfg.ncy + 1
+    d.xmin, d.xmax, d.ymin, d.ymax = 0.0, cfg.Lx / L, 0.0, cfg.Ly / L
+    d.delta = 0
+    for k in range(4):
+        d.wall_dirichlet[k] = int(cfg.wall_dirichlet[k])
+        d.wall_phi[k] = cfg.wall_V[k] / P
+    d.n_objects = len(cfg.objects)
+    for k, o in enumerate(cfg.objects):
+        t = d.objects[k]
+        t.shape = o.shape
+        t.conductor = int(o.conductor)
+        t.cx, t.cy = o.cx / L, o.cy / L
+        if o.shape == api.PIC_SHAPE_BOX:
+            t.a, t.b = o.a / L, o.b / L
+        else:
+            t.a = o.a / L
+            t.b = (o.b if o.b else o.a) / L
+        t.angle = o.angle
+        t.eps = o.eps
+        t.phi = o.phi_V / P
+    return d
+
+
+class Mesh:
+    """Mesh built by pic_mesh_build; owns the library storage."""
+
+    def __init__(self, cfg: Config):
+        lib = api.load()
+        self.cfg = cfg
+        self.deck = make_deck(cfg)
+        self.ptr = C.POINTER(api.MeshDesc)()
+        api.check(lib.pic_mesh_build(C.byref(self.deck), C.byref(self.ptr)), "pic_mesh_build")
+        self.desc = self.ptr.contents
+        d = self.desc
+        self.nnx, self.nny = d.nnx, d.nny
+        self.nn = d.nnx * d.nny
+        self.ne = (d.nnx - 1) * (d.nny - 1)
+        self.hx = (d.xmax - d.xmin) / (d.nnx - 1)
+        self.hy = (d.ymax - d.ymin) / (d.nny - 1)
+
+    def array(self, name: str) -> np.ndarray:
+        d = self.desc
+        sizes = {"node_type": self.nn, "node_index": self.nn, "element_index": self.ne,
+                 "phi_dirichlet": self.nn, "cell_volume": self.nn,
+                 "a_srow": d.n_unknowns + 1, "a_jcol": d.nnz, "a_k": d.nnz,
+                 "xt_srow": d.n_unknowns + 1, "xt_jcol": d.nnz_xt, "xt_k": d.nnz_xt,
+                 "a_diag": d.n_unknowns, "rhs_fix": d.n_unknowns, "mass_q1": 16,
+                 "ife_mass": 16 * d.n_interface, "patch_ptr": self.nn + 1}
+        if name == "patch_nodes":
+            n = int(self.array("patch_ptr")[-1])
+        else:
+            n = sizes[name]
+        ptr = getattr(d, name)
+        dt = np.float64 if ptr._type_ is C.c_double else np.int32
+        return api.as_np(ptr, int(n), dt)
+
+    def close(self):
+        if self.ptr:
+            api.load().pic_mesh_free(self.ptr)
+            self.ptr = C.POINTER(api.MeshDesc)()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+def species_params(cfg: Config):
+    """[(charge, mass, weight, sigma_v_normalised)] for e- and Ar+."""
+    sc = cfg.scales
+    L = sc["L_ref"]
+    hx_m, hy_m = cfg.Lx / cfg.ncx, cfg.Ly / cfg.ncy
+    weight = cfg.n0 * hx_m * hy_m / cfg.ppc
+    out = []
+    for q, m, T in ((-1.0, ME, cfg.Te_eV), (1.0, AR_MASS, cfg.Ti_eV)):
+        sigma = math.sqrt(KB * T * EVTOK / m) / sc["v_ref"]
+        out.append((q, m, weight, sigma))
+    return out, L
+
+
+def load_particles(cfg: Config, mesh: Mesh, species: int, n_cells_limit: int | None = None):
+    """Seeded uniform loading, ppc per cell, outside the objects; Maxwellian velocities."""
+    sp, _ = species_params(cfg)
+    sigma = sp[species][3]
+    rng = np.random.default_rng([cfg.seed, species, 7919])
+    ncx, ncy = cfg.ncx, cfg.ncy
+    ncell = ncx * ncy if n_cells_limit is None else min(n_cells_limit, ncx * ncy)
+    cell = np.arange(ncell, dtype=np.int64)
+    ci, cj = cell // ncy, cell % ncy
+    n = ncell * cfg.ppc
+    x = (np.repeat(ci, cfg.ppc) + rng.random(n)) * mesh.hx
+    y = (np.repeat(cj, cfg.ppc) + rng.random(n)) * mesh.hy
+    keep = np.ones(n, dtype=bool)
+    dk = mesh.deck
+    for k in range(dk.n_objects):
+        o = dk.objects[k]
+        if o.shape == api.PIC_SHAPE_CIRCLE:
+            keep &= ~((x - o.cx) ** 2 + (y - o.cy) ** 2 < o.a * o.a)
+        elif o.shape == api.PIC_SHAPE_BOX:
+            keep &= ~((x > o.cx) & (x < o.a) & (y > o.cy) & (y < o.b))
+        elif o.shape == api.PIC_SHAPE_ELLIPSE:
+            c, s = math.cos(o.angle), math.sin(o.angle)
+            u = (x - o.cx) * c + (y - o.cy) * s
+            v = -(x - o.cx) * s + (y - o.cy) * c
+            keep &= ~(u * u / (o.a * o.a) + v * v / (o.b * o.b) < 1.0)
+    x, y = x[keep], y[keep]
+    m = x.size
+    v = rng.standard_normal((3, m)) * sigma
+    return (np.ascontiguousarray(x), np.ascontiguousarray(y), np.ascontiguousarray(v[0]),
+            np.ascontiguousarray(v[1]), np.ascontiguousarray(v[2]))

@@ -1,0 +1,62 @@
+"""Generates the golden fixtures of tests/golden from the reference's own
+committed outputs (weqwoueu/pic-, PIC-IFE_GEC):
+
+  physics_parameter.json  <- OUTPUT/physics_parameter.inp:38-70 (reference
+                             scales at n_ref = 1e21 m^-3, T_ref = 1 eV, and the
+                             1-amu ion mass in units of m_e)
+  norm_error.json         <- Norm_Error_{0064,0128,0256}.txt (IFE L2/H1 errors)
+  philox4x32_10_kat.json  <- known-answer vectors of Philox4x32-10 published
+                             with the Random123 library (Salmon et al., SC'11)
+
+Usage: python tests/golden/make_golden.py [/path/to/PIC-IFE_GEC]
+"""
+import json
+import os
+import re
+import sys
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+
+
+def numbers(line):
+    return [float(v.replace("D", "E")) for v in re.findall(r"[-+]?\d+\.\d*(?:[EeDd][-+]?\d+)?", line)]
+
+
+def main(root):
+    txt = open(os.path.join(root, "OUTPUT", "physics_parameter.inp")).read().splitlines()
+    def after(label):
+        for l in txt:
+            if l.strip().startswith(label):
+                return numbers(l)[-1]
+        raise KeyError(label)
+    phys = {
+        "n_ref": after("density ref"),
+        "T_ref_eV": after("temperature ref") / 11605.0,
+        "L_ref": after("length ref"),
+        "time_ref": after("time ref"),
+        "v_ref": after("velocity ref"),
+        "Phi_ref": after("potential ref"),
+    }
+    masses = [numbers(l)[-1] for l in txt if l.strip().startswith("mass:")]
+    phys["ion_mass_over_me"] = [m for m in masses if m > 100.0][0]
+    phys["ion_mass_kg"] = [m for m in masses if 1e-28 < m < 1e-25][0]
+    json.dump(phys, open(os.path.join(HERE, "physics_parameter.json"), "w"), indent=1)
+    ne = {}
+    for n in (64, 128, 256):
+        lines = open(os.path.join(root, "Norm_Error_%04d.txt" % n)).read().splitlines()
+        l2, h1 = numbers(lines[2])[:2]
+        ne[str(n)] = {"L2": l2, "H1": h1}
+    json.dump(ne, open(os.path.join(HERE, "norm_error.json"), "w"), indent=1)
+    kat = [
+        {"ctr": [0, 0, 0, 0], "key": [0, 0],
+         "out": [0x6627e8d5, 0xe169c58d, 0xbc57ac4c, 0x9b00dbd8]},
+        {"ctr": [0xffffffff] * 4, "key": [0xffffffff] * 2,
+         "out": [0x408f276d, 0x41c83b0e, 0xa20bc7c6, 0x6d5451fd]},
+        {"ctr": [0x243f6a88, 0x85a308d3, 0x13198a2e, 0x03707344], "key": [0xa4093822, 0x299f31d0],
+         "out": [0xd16cfe09, 0x94fdcceb, 0x5001e420, 0x24126ea1]},
+    ]
+    json.dump(kat, open(os.path.join(HERE, "philox4x32_10_kat.json"), "w"), indent=1)
+
+
+if __name__ == "__main__":
+    main(sys.argv[1] if len(sys.argv) > 1 else "/root/reference/PIC-IFE_GEC")

@@ -1,0 +1,170 @@
+"""ctypes binding of the CPU oracle (oracle/liboracle.so), test infrastructure."""
+from __future__ import annotations
+
+import ctypes as C
+import os
+import subprocess
+
+import numpy as np
+
+from pic_b200 import api
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+ORACLE_DIR = os.path.join(ROOT, "oracle")
+ORACLE_LIB = os.path.join(ORACLE_DIR, "liboracle.so")
+
+_P = C.POINTER
+_d = _P(C.c_double)
+_i = _P(C.c_int32)
+_u = _P(C.c_uint32)
+_l = _P(C.c_int64)
+
+_lib = None
+
+
+def load():
+    global _lib
+    if _lib is not None:
+        return _lib
+    src = os.path.join(ORACLE_DIR, "oracle.c")
+    if not os.path.exists(ORACLE_LIB) or os.path.getmtime(ORACLE_LIB) < os.path.getmtime(src):
+        subprocess.run(["make", "-s", "-C", ORACLE_DIR], check=True)
+    lib = C.CDLL(ORACLE_LIB)
+    M = _P(api.MeshDesc)
+    lib.or_reference_scales.argtypes = [C.c_double, C.c_double, _d]
+    lib.or_philox.argtypes = [_u, _u, _u]
+    lib.or_locate.argtypes = [M, C.c_double, C.c_double]
+    lib.or_move_all.argtypes = [M, C.c_int64, _d, _d, _d, _d, _d, _i, _d, _d, _d, C.c_double,
+                                C.c_double, _i]
+    lib.or_move_all.restype = C.c_int64
+    lib.or_deposit.argtypes = [M, C.c_int64, _d, _d, _d, _d, _d, _i, C.c_double, C.c_double, _l, _l]
+    lib.or_deposit.restype = C.c_int64
+    lib.or_normalize.argtypes = [M, C.c_int, _P(_l), _P(_l), _d, C.c_double, C.c_double, _d,
+                                 _P(_d), _P(_d)]
+    lib.or_rhs.argtypes = [M, _d, _d]
+    lib.or_pcg.argtypes = [M, _d, _d, C.c_double, C.c_int, _d]
+    lib.or_ppr.argtypes = [M, _d, _d, _d, _d]
+    lib.or_sort_perm.argtypes = [C.c_int64, _i, _u, _l]
+    lib.or_sort_perm.restype = C.c_int64
+    lib.or_canon_dot.argtypes = [_d, _d, C.c_int64]
+    lib.or_canon_dot.restype = C.c_double
+    lib.or_mcc.argtypes = [_P(api.MccTable), _P(api.Gas), C.c_double, C.c_double, C.c_uint64,
+                           C.c_uint64, C.c_int32, C.c_int64, _i, _u, _d, _d, _d, _l, _l, _l, _d, _d]
+    lib.or_mcc.restype = C.c_int64
+    lib.or_ife_closed_form.argtypes = [C.c_int, C.c_int, C.c_int, C.c_double, C.c_double,
+                                       C.c_double, _d]
+    _lib = lib
+    return lib
+
+
+def d(a):
+    return a.ctypes.data_as(_d)
+
+
+def i32(a):
+    return a.ctypes.data_as(_i)
+
+
+def u32(a):
+    return a.ctypes.data_as(_u)
+
+
+def i64(a):
+    return a.ctypes.data_as(_l)
+
+
+def scales(n_ref, T_eV):
+    out = np.zeros(4)
+    load().or_reference_scales(n_ref, T_eV, d(out))
+    return out
+
+
+def philox(ctr, key):
+    c = (C.c_uint32 * 4)(*ctr)
+    k = (C.c_uint32 * 2)(*key)
+    o = (C.c_uint32 * 4)()
+    load().or_philox(c, k, o)
+    return list(o)
+
+
+def move_all(mesh_ptr, parts, efx, efy, coef, qm, dt, wall=(0, 0, 0, 0)):
+    """parts: dict x,y,vx,vy,vz,loc (modified in place).  Returns lost count."""
+    w = (C.c_int32 * 4)(*wall)
+    return load().or_move_all(mesh_ptr, parts["x"].size, d(parts["x"]), d(parts["y"]),
+                              d(parts["vx"]), d(parts["vy"]), d(parts["vz"]), i32(parts["loc"]),
+                              d(efx), d(efy), d(coef), qm, dt, w)
+
+
+def deposit(mesh_ptr, parts, mass, vref, nn):
+    q = np.zeros(nn, np.int64)
+    e = np.zeros(nn, np.int64)
+    bad = load().or_deposit(mesh_ptr, parts["x"].size, d(parts["x"]), d(parts["y"]),
+                            d(parts["vx"]), d(parts["vy"]), d(parts["vz"]), i32(parts["loc"]),
+                            mass, vref, i64(q), i64(e))
+    return q, e, bad
+
+
+def normalize(mesh_ptr, qs, es, wq, L_ref, n_ref, nn):
+    ns = len(qs)
+    rho = np.zeros(nn)
+    rho_s = [np.zeros(nn) for _ in range(ns)]
+    ek_s = [np.zeros(nn) for _ in range(ns)]
+    qa = (_l * ns)(*[i64(a) for a in qs])
+    ea = (_l * ns)(*[i64(a) for a in es])
+    ra = (_d * ns)(*[d(a) for a in rho_s])
+    ka = (_d * ns)(*[d(a) for a in ek_s])
+    w = np.ascontiguousarray(wq, dtype=np.float64)
+    load().or_normalize(mesh_ptr, ns, qa, ea, d(w), L_ref, n_ref, d(rho), ra, ka)
+    return rho, rho_s, ek_s
+
+
+def rhs(mesh_ptr, rho, nn):
+    b = np.zeros(nn)
+    load().or_rhs(mesh_ptr, d(np.ascontiguousarray(rho)), d(b))
+    return b
+
+
+def pcg(mesh_ptr, b, phi0, tol, maxit):
+    phi = np.ascontiguousarray(phi0, dtype=np.float64).copy()
+    st = np.zeros(4)
+    load().or_pcg(mesh_ptr, d(np.ascontiguousarray(b)), d(phi), tol, maxit, d(st))
+    return phi, {"iterations": int(st[0]), "ierr": int(st[1]), "normR": st[2], "normRHS": st[3]}
+
+
+def ppr(mesh_ptr, phi, nn):
+    coef = np.zeros(5 * nn)
+    efx = np.zeros(nn)
+    efy = np.zeros(nn)
+    load().or_ppr(mesh_ptr, d(np.ascontiguousarray(phi)), d(coef), d(efx), d(efy))
+    return coef.reshape(5, nn), efx, efy
+
+
+def sort_perm(loc, ids):
+    perm = np.zeros(loc.size, np.int64)
+    m = load().or_sort_perm(loc.size, i32(loc), u32(ids), i64(perm))
+    return perm[:m]
+
+
+def canon_dot(a, b):
+    return load().or_canon_dot(d(a), d(b), a.size)
+
+
+def mcc(table, gas, mass, vref, seed, step, species, parts):
+    n = parts["x"].size
+    counts = np.zeros(8, np.int64)
+    n_new = np.zeros(1, np.int64)
+    cap = n + 16
+    par = np.zeros(cap, np.int64)
+    ne = np.zeros(3 * cap)
+    ni = np.zeros(3 * cap)
+    ncoll = load().or_mcc(C.byref(table), C.byref(gas), mass, vref, seed, step, species, n,
+                          i32(parts["loc"]), u32(parts["id"]), d(parts["vx"]), d(parts["vy"]),
+                          d(parts["vz"]), i64(counts), i64(n_new), i64(par), d(ne), d(ni))
+    k = int(n_new[0])
+    return ncoll, counts, par[:k], ne[:3 * k].reshape(k, 3), ni[:3 * k].reshape(k, 3)
+
+
+def closed_form(typ, bi, pf, a, b, R):
+    C4 = np.zeros(4)
+    ok = load().or_ife_closed_form(typ, bi, pf, a, b, R, d(C4))
+    return C4 if ok else None

@@ -1,0 +1,48 @@
+"""The C-ABI library loads on a CPU-only host and exports every entry point
+declared in include/picgpu.h; CPU-side error paths need no device."""
+import ctypes as C
+import os
+import re
+
+from pic_b200 import api, deck
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+
+
+def _declared():
+    txt = open(os.path.join(ROOT, "include", "picgpu.h")).read()
+    txt = re.sub(r"/\*.*?\*/", "", txt, flags=re.S)
+    return sorted(set(re.findall(r"\b(pic_[a-z0-9_]+)\s*\(", txt)))
+
+
+def test_every_declared_symbol_is_exported():
+    lib = api.load()
+    names = _declared()
+    assert len(names) >= 20
+    for n in names:
+        assert hasattr(lib, n), n
+    assert sorted(api.EXPORTS) == names
+
+
+def test_calls_before_init_fail_cleanly():
+    lib = api.load()
+    lib.pic_finalize()
+    rc = lib.pic_step(1, None)
+    assert rc == -6
+    assert b"pic_init" in lib.pic_last_error()
+
+
+def test_mesh_builder_rejects_bad_decks():
+    lib = api.load()
+    d = deck.make_deck(deck.config("tiny"))
+    d.nnx = 2
+    ptr = C.POINTER(api.MeshDesc)()
+    assert lib.pic_mesh_build(C.byref(d), C.byref(ptr)) == -1
+    d = deck.make_deck(deck.config("tiny"))
+    d.delta = 1
+    assert lib.pic_mesh_build(C.byref(d), C.byref(ptr)) == -8
+    # two overlapping objects
+    d = deck.make_deck(deck.config("tiny"))
+    d.n_objects = 2
+    d.objects[1] = d.objects[0]
+    assert lib.pic_mesh_build(C.byref(d), C.byref(ptr)) == -8
