@@ -283,6 +283,33 @@ int64_t pic_kernel_launches(void);
  * op 1 records the stop event, waits for it and writes the elapsed ms. */
 int pic_device_timer(int32_t op, double *ms_out);
 
+/* ---- allocation-free deposit ---- */
+
+/* Largest mesh (nnx*nny nodes) pic_deposit_noalloc accepts: its int64
+ * accumulator is a fixed 4 MiB __device__ array. */
+#define PIC_NOALLOC_MAX_NODES 524288
+
+/* Charge density of one species, like the per-species rho_s of
+ * pic_get_par_chg, for callers that may not allocate device memory (their
+ * device memory comes from an arena owned by someone else, or they run a
+ * loop that must not pay cudaMalloc's implicit synchronisation).  No
+ * counterpart in the reference: it exists only for such callers.
+ *
+ * Needs no pic_init.  x, y (and loc, may be NULL; loc < 0 skips a particle),
+ * cell_volume ([nnx*nny]) and rho_out ([nnx*nny]) are DEVICE pointers of the
+ * current device; stream is a cudaStream_t (NULL: default stream).  The call
+ * only enqueues work: synchronise the stream before reading rho_out.
+ * Allocates and frees nothing.  The scratch is one file-scope __device__
+ * array shared by every call on a device: calls that overlap on the GPU
+ * (different streams, or several host threads) race on it.  The first call
+ * on a device looks up the array's device address (cudaGetSymbolAddress); make
+ * that first call before any stream capture.  Meshes above
+ * PIC_NOALLOC_MAX_NODES nodes are rejected with PIC_ERR_ARG. */
+int pic_deposit_noalloc(int32_t nnx, int32_t nny, double xmin, double xmax, double ymin,
+                        double ymax, int64_t n, const double *x, const double *y,
+                        const int32_t *loc, const double *cell_volume, double weight_charge,
+                        double L_ref, double n_ref, double *rho_out, void *stream);
+
 #ifdef __cplusplus
 }
 #endif

@@ -36,6 +36,7 @@ EXPORTS = [
     "pic_sort_particles", "pic_move_all", "pic_get_par_chg", "pic_ife_solve",
     "pic_get_efield_ppr", "pic_mcc", "pic_step", "pic_get_field", "pic_set_field",
     "pic_particle_device_ptrs", "pic_kernel_launches", "pic_device_timer",
+    "pic_deposit_noalloc",
 ]
 
 
@@ -168,6 +169,10 @@ def load() -> C.CDLL:
     lib.pic_get_field.argtypes = [C.c_int32, d]
     lib.pic_set_field.argtypes = [C.c_int32, d]
     lib.pic_device_timer.argtypes = [C.c_int32, _P(C.c_double)]
+    lib.pic_deposit_noalloc.argtypes = [C.c_int32, C.c_int32, C.c_double, C.c_double, C.c_double,
+                                        C.c_double, C.c_int64, C.c_void_p, C.c_void_p, C.c_void_p,
+                                        C.c_void_p, C.c_double, C.c_double, C.c_double, C.c_void_p,
+                                        C.c_void_p]
     lib.pic_particle_device_ptrs.argtypes = [C.c_int32, _P(C.c_void_p), _P(C.c_int64)]
     _lib = lib
     return lib

@@ -15,7 +15,7 @@ import sys
 HERE = os.path.dirname(os.path.abspath(__file__))
 CSRC = os.path.join(HERE, "csrc")
 LIB = os.path.join(HERE, "libpicgpu.so")
-SOURCES = ["picgpu.cu", "sort_mcc.cu", "mesh_build.cpp"]
+SOURCES = ["picgpu.cu", "sort_mcc.cu", "mesh_build.cpp", "noalloc.cu"]
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 
 
