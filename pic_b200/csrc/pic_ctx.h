@@ -107,6 +107,10 @@ struct Ctx {
   double *d_part = nullptr;  // block partials [3][nblk]
   PcgState *d_pcg = nullptr;
   int red_blocks = 0;
+  int coop_grid = 0;               // CTAs of the persistent PCG (0: two-kernel loop)
+  unsigned int *d_bar = nullptr;   // grid barrier: count, generation, error flag
+  long long pcg_spin_limit = 1ll << 24;
+  unsigned int pcg_bar_extra = 0;
   int ebc_dirty = 1;
   // species
   int ns = 0;

@@ -543,6 +543,154 @@ __global__ void __launch_bounds__(PIC_RED_THREADS) k_pcg_upd(PcgK k) {
   }
 }
 
+// ---------------------------------------------------------------------------
+// Persistent Jacobi-PCG: one cooperative launch per solve.  Every CTA owns
+// the 1024-node chunks blockIdx.x, blockIdx.x + gridDim.x, ...; per iteration
+// two grid barriers separate (A) direction + SpMV + p.q partials and (B) the
+// x/r/w update + r.r, r.w partials.  Each CTA then reduces all chunk partials
+// itself in the canonical order, so every CTA holds identical scalars and
+// takes identical decisions.  Phase A and phase B partials live in separate
+// arrays: a CTA that races ahead never overwrites partials that a slower CTA
+// is still reducing.  Cross-CTA data is read with ld.global.cg (L2), never
+// from a possibly stale L1 line.
+// ---------------------------------------------------------------------------
+struct PcgP {
+  PcgK k;
+  double *p0, *p1;
+  double *partA, *partB;  // [nb], [2*nb]
+  unsigned int *bar;      // [0] arrive count, [1] generation
+  int *bar_err;
+  long long spin_limit;
+  unsigned int bar_extra; // arrivals expected beyond the grid (0; >0 only to test the timeout)
+};
+
+// Grid-wide barrier with a bounded wait: after `limit` polls the CTA records
+// the timeout in *err and leaves; every CTA then exits the solve, so a lost
+// CTA ends the kernel with an error status instead of a hang.
+__device__ __forceinline__ bool grid_barrier(unsigned int *bar, int *err, long long limit,
+                                             unsigned int extra) {
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    volatile unsigned int *vgen = bar + 1;
+    unsigned int g0 = *vgen;
+    __threadfence();
+    unsigned int t = atomicAdd(bar, 1u);
+    if (t == gridDim.x - 1 + extra) {
+      atomicExch(bar, 0u);
+      __threadfence();
+      atomicAdd(bar + 1, 1u);
+    } else {
+      long long spins = 0;
+      while (*vgen == g0) {
+        __nanosleep(32);
+        if (++spins > limit) {
+          atomicExch(err, 1);
+          break;
+        }
+      }
+    }
+    __threadfence();
+  }
+  __syncthreads();
+  return *(volatile int *)err == 0;
+}
+
+template <int NV>
+__device__ __forceinline__ void final_sum_bcast(const double *part, int nb, double *out_all) {
+  __shared__ double bc[NV];
+  double o[NV];
+  final_sum_canon<NV>(part, nb, o);
+  if (threadIdx.x == 0)
+    for (int k = 0; k < NV; ++k) bc[k] = o[k];
+  __syncthreads();
+  for (int k = 0; k < NV; ++k) out_all[k] = bc[k];
+  __syncthreads();
+}
+
+__global__ void __launch_bounds__(PIC_RED_THREADS) k_pcg_persist(PcgP P) {
+  const PcgK &k = P.k;
+  PcgState *S = k.st;
+  double rho = __ldcg(&S->rho), normRHS = __ldcg(&S->normRHS);
+  const double tol2 = S->tol2;
+  const int maxit = S->maxit;
+  int done = __ldcg(&S->done), iter = 0, ierr = 0, parity = 0;
+  double beta = 0.0, normR = 0.0, rho0 = 0.0;
+  bool ok = true;
+  while (!done) {
+    const double *pold = parity ? P.p1 : P.p0;
+    double *pnew = parity ? P.p0 : P.p1;
+    const bool first = iter == 0;
+    auto pn = [&](int64_t m) {
+      double wm = __ldcg(k.w + m);
+      return first ? wm : fma(beta, __ldcg(pold + m), wm);
+    };
+    for (int c = blockIdx.x; c < k.nb; c += gridDim.x) {
+      double vpq = 0.0;
+      for (int it = 0; it < PIC_RED_ITEMS; ++it) {
+        int64_t n = (int64_t)c * PIC_RED_CHUNK + it * PIC_RED_THREADS + threadIdx.x;
+        if (n >= k.nn) continue;
+        double pv = pn(n);
+        double qv = row_apply(k, n, pn);
+        pnew[n] = pv;
+        k.q[n] = qv;
+        vpq = fma(pv, qv, vpq);
+      }
+      double v[1] = {vpq}, out[1];
+      block_sum_canon<1>(v, out);
+      if (threadIdx.x == 0) P.partA[c] = out[0];
+    }
+    if (!(ok = grid_barrier(P.bar, P.bar_err, P.spin_limit, P.bar_extra))) break;
+    double pq;
+    final_sum_bcast<1>(P.partA, k.nb, &pq);
+    if (pq == 0.0) {
+      ierr = 3;
+      break;
+    }
+    const double alpha = rho / pq;
+    for (int c = blockIdx.x; c < k.nb; c += gridDim.x) {
+      double vrr = 0.0, vrw = 0.0;
+      for (int it = 0; it < PIC_RED_ITEMS; ++it) {
+        int64_t n = (int64_t)c * PIC_RED_CHUNK + it * PIC_RED_THREADS + threadIdx.x;
+        if (n >= k.nn) continue;
+        double pv = pnew[n];
+        double xv = fma(alpha, pv, k.x[n]);
+        double rv = fma(-alpha, k.q[n], k.r[n]);
+        double wv = rv / k.diag[n];
+        k.x[n] = xv;
+        k.r[n] = rv;
+        k.w[n] = wv;
+        vrr = fma(rv, rv, vrr);
+        vrw = fma(rv, wv, vrw);
+      }
+      double v[2] = {vrr, vrw}, out[2];
+      block_sum_canon<2>(v, out);
+      if (threadIdx.x == 0) {
+        P.partB[c] = out[0];
+        P.partB[k.nb + c] = out[1];
+      }
+    }
+    if (!(ok = grid_barrier(P.bar, P.bar_err, P.spin_limit, P.bar_extra))) break;
+    double tot[2];
+    final_sum_bcast<2>(P.partB, k.nb, tot);
+    normR = tot[0];
+    rho0 = rho;
+    rho = tot[1];
+    ++iter;
+    if (normR / normRHS <= tol2) done = 1;
+    else if (iter >= maxit) { ierr = 1; done = 1; }
+    else if (rho0 == 0.0) { ierr = 2; done = 1; }
+    else beta = rho / rho0;
+    parity ^= 1;
+  }
+  if (blockIdx.x == 0 && threadIdx.x == 0) {
+    S->iter = iter;
+    S->ierr = ok ? ierr : 4;
+    S->normR = normR;
+    S->rho = rho;
+    S->done = 1;
+  }
+}
+
 // U_fe_full from U_fe (IFE_Solve_2D.f90:240-247)
 __global__ void k_phi_out(const double *__restrict__ x, const int32_t *__restrict__ node_type,
                           const double *__restrict__ phi_dir, double *__restrict__ phi, int64_t nn) {
@@ -710,7 +858,7 @@ static void free_all() {
   F(g.d_xt_ptr); F(g.d_xt_col); F(g.d_xt_val); F(g.d_row_kind); F(g.d_ex_ptr); F(g.d_ex_col);
   F(g.d_ex_val); F(g.d_diag); F(g.d_ppr_kind); F(g.d_ppr_ptr); F(g.d_ppr_nodes); F(g.d_ppr_rows);
   F(g.d_ppr_h); F(g.d_phi); F(g.d_rho); F(g.d_efx); F(g.d_efy); F(g.d_coef); F(g.d_b); F(g.d_x);
-  F(g.d_r); F(g.d_w); F(g.d_p[0]); F(g.d_p[1]); F(g.d_q); F(g.d_part); F(g.d_pcg);
+  F(g.d_r); F(g.d_w); F(g.d_p[0]); F(g.d_p[1]); F(g.d_q); F(g.d_part); F(g.d_pcg); F(g.d_bar);
   F(g.d_cell_count); F(g.d_cell_start); F(g.d_cell_fill); F(g.d_perm); F(g.d_sort_id);
   F(g.d_scan_blk); F(g.d_counters); F(g.d_hist); F(g.d_sel); F(g.d_cand); F(g.d_cand_slot);
   F(g.d_mcc_misc); F(g.d_ion_parent); F(g.d_ion_data);
@@ -854,7 +1002,30 @@ static int run_pcg(pic_solve_stats *stats) {
   const int chunk = 32;
   int parity = 0;
   PcgState hs;
-  for (int it = 0; it < g.P.pcg_maxit + chunk; it += chunk) {
+  if (g.coop_grid > 0) {
+    PcgP P;
+    P.k = pcg_k(0);
+    P.p0 = g.d_p[0];
+    P.p1 = g.d_p[1];
+    P.partA = g.d_part;
+    P.partB = g.d_part + g.red_blocks;
+    P.bar = g.d_bar;
+    P.bar_err = (int *)(g.d_bar + 2);
+    P.spin_limit = g.pcg_spin_limit;
+    P.bar_extra = g.pcg_bar_extra;
+    PIC_CUDA(cudaMemsetAsync(g.d_bar, 0, 4 * sizeof(unsigned int), g.st));
+    void *args[] = {&P};
+    PIC_CUDA(cudaLaunchCooperativeKernel((const void *)k_pcg_persist, dim3(g.coop_grid),
+                                         dim3(PIC_RED_THREADS), args, 0, g.st));
+    PIC_LAUNCHED();
+    PIC_CUDA(cudaMemcpyAsync(&hs, g.d_pcg, sizeof hs, cudaMemcpyDeviceToHost, g.st));
+    PIC_CUDA(cudaStreamSynchronize(g.st));
+    if (hs.ierr == 4) {
+      set_error("pic_ife_solve: PCG grid barrier timed out");
+      return PIC_ERR_CUDA;
+    }
+  }
+  for (int it = 0; g.coop_grid == 0 && it < g.P.pcg_maxit + chunk; it += chunk) {
     for (int c = 0; c < chunk; ++c) {
       PcgK k = pcg_k(parity);
       k_pcg_dir<<<g.red_blocks, PIC_RED_THREADS, 0, g.st>>>(k);
@@ -1260,6 +1431,25 @@ int pic_init(const pic_mesh_desc *mesh, const pic_params *params) {
   if ((rc = dalloc(&g.d_part, 3 * (size_t)g.red_blocks))) return rc;
   if ((rc = dalloc(&g.d_pcg, 1))) return rc;
   PIC_CUDA(cudaMemset(g.d_pcg, 0, sizeof(PcgState)));
+  if ((rc = dalloc(&g.d_bar, 4))) return rc;
+  PIC_CUDA(cudaMemset(g.d_bar, 0, 4 * sizeof(unsigned int)));
+  {
+    // persistent PCG when the device supports cooperative launch and every
+    // CTA of the grid can be resident at once
+    int dev = 0, coop = 0, nsm = 0, per_sm = 0;
+    PIC_CUDA(cudaGetDevice(&dev));
+    PIC_CUDA(cudaDeviceGetAttribute(&coop, cudaDevAttrCooperativeLaunch, dev));
+    PIC_CUDA(cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev));
+    PIC_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_pcg_persist, PIC_RED_THREADS, 0));
+    const char *env = getenv("PIC_PCG_PERSISTENT");
+    bool want = !(env && env[0] == '0');
+    g.coop_grid = (want && coop && per_sm > 0) ? std::min(g.red_blocks, per_sm * nsm) : 0;
+    // failure-path test hooks: a short wait limit and an arrival that never comes
+    const char *lim = getenv("PIC_PCG_SPIN_LIMIT");
+    g.pcg_spin_limit = lim ? std::max(1ll, atoll(lim)) : (1ll << 24);
+    const char *extra = getenv("PIC_PCG_BARRIER_EXTRA");
+    g.pcg_bar_extra = extra ? (unsigned int)std::max(0, atoi(extra)) : 0u;
+  }
   if ((rc = dalloc(&g.d_counters, 32))) return rc;
   PIC_CUDA(cudaMemset(g.d_counters, 0, 32 * sizeof(unsigned long long)));
   // sort scratch sized for the largest species

@@ -106,8 +106,15 @@ def test_get_par_chg_bit_exact():
         sim.close()
 
 
+@pytest.fixture
+def pcg_mode(request, monkeypatch):
+    monkeypatch.setenv("PIC_PCG_PERSISTENT", "1" if request.param == "persistent" else "0")
+    return request.param
+
+
+@pytest.mark.parametrize("pcg_mode", ["persistent", "two-kernel"], indirect=True)
 @pytest.mark.parametrize("name", ["tiny", "cfg1"])
-def test_ife_solve_bit_exact(name):
+def test_ife_solve_bit_exact(name, pcg_mode):
     sim = _sim(name)
     try:
         rng = np.random.default_rng(5)
@@ -127,6 +134,31 @@ def test_ife_solve_bit_exact(name):
         # warm start from the solution converges at once
         st2 = sim.ife_solve(phi)
         assert st2.iterations <= 2
+    finally:
+        sim.close()
+
+
+def test_pcg_barrier_wait_times_out_cleanly(monkeypatch):
+    """The persistent PCG's grid barrier waits at most PIC_PCG_SPIN_LIMIT
+    polls.  Expecting one arrival that never comes makes every CTA give up:
+    the solve returns an error status and the context stays usable."""
+    monkeypatch.setenv("PIC_PCG_PERSISTENT", "1")
+    monkeypatch.setenv("PIC_PCG_BARRIER_EXTRA", "1")
+    monkeypatch.setenv("PIC_PCG_SPIN_LIMIT", "20000")
+    sim = _sim("tiny")
+    try:
+        sim.set_field("rho", np.full(sim.mesh.nn, 0.01))
+        with pytest.raises(api.PicError) as ei:
+            sim.ife_solve()
+        assert ei.value.code == -2 and "timed out" in str(ei.value)
+    finally:
+        sim.close()
+    monkeypatch.delenv("PIC_PCG_BARRIER_EXTRA")
+    monkeypatch.delenv("PIC_PCG_SPIN_LIMIT")
+    sim = _sim("tiny")
+    try:
+        sim.set_field("rho", np.full(sim.mesh.nn, 0.01))
+        assert sim.ife_solve().ierr == 0
     finally:
         sim.close()
 
