@@ -134,6 +134,9 @@ typedef struct pic_params {
   int32_t precision;  /* PIC_PREC_*                                          */
   int32_t sort_interval; /* counting sort every k steps in pic_step (>=1)    */
   int32_t solver;     /* PIC_SOLVER_*                                        */
+  int32_t diag_interval; /* pic_step deposits the per-node energy (Ek_tot, a
+                          * diagnostic) on steps that are multiples of this;
+                          * <= 1: every step.  pic_get_par_chg always does. */
 } pic_params;
 
 /* One MCC_jw collision bundle (Type MCCBundle, mc/TypeMCC.f90:9-20). */

@@ -90,7 +90,7 @@ class Params(C.Structure):
                 ("dt", C.c_double), ("n_ref", C.c_double), ("T_ref_eV", C.c_double),
                 ("pcg_tol", C.c_double), ("pcg_maxit", C.c_int32), ("wall_bc", C.c_int32 * 4),
                 ("seed", C.c_uint64), ("precision", C.c_int32), ("sort_interval", C.c_int32),
-                ("solver", C.c_int32)]
+                ("solver", C.c_int32), ("diag_interval", C.c_int32)]
 
 
 class MccTable(C.Structure):

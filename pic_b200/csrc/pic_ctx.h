@@ -33,6 +33,7 @@ extern long long g_launches;
 struct MeshK {
   int nnx, nny, nex, ney;
   double xmin, xmax, ymin, ymax, hx, hy;
+  double inv_ney;                 // 1/ney for the element -> column split
   const double *xs, *ys;          // node coordinates (x_s + h_x*(i))
   const int32_t *element_index;   // [ne]
   const int32_t *node_index;      // [nn]
@@ -87,7 +88,7 @@ struct Ctx {
   double *d_xt_val = nullptr;
   // PCG operator: row kind per node (-1 Dirichlet, 0..n_mat-1 stencil, >= n_mat explicit row)
   int32_t *d_row_kind = nullptr;
-  int32_t *d_ex_ptr = nullptr, *d_ex_col = nullptr;  // explicit rows (0-based node columns)
+  int32_t *d_ex_cnt = nullptr, *d_ex_col = nullptr;  // explicit rows: count + 9 padded slots
   double *d_ex_val = nullptr;
   int n_mat = 0;
   double h_stencil[16][9];
@@ -108,6 +109,9 @@ struct Ctx {
   PcgState *d_pcg = nullptr;
   int red_blocks = 0;
   int coop_grid = 0;               // CTAs of the persistent PCG (0: two-kernel loop)
+  int smem_grid = 0;               // CTAs of the shared-memory-resident PCG (0: not eligible)
+  bool ex_local = true;            // every explicit row stays inside its 3x3 neighbourhood
+  size_t smem_bytes = 0;
   unsigned int *d_bar = nullptr;   // grid barrier: count, generation, error flag
   long long pcg_spin_limit = 1ll << 24;
   unsigned int pcg_bar_extra = 0;
@@ -117,7 +121,7 @@ struct Ctx {
   Species sp[PIC_MAX_SPECIES];
   // scratch
   int32_t *d_cell_count = nullptr, *d_cell_start = nullptr, *d_cell_fill = nullptr;
-  int32_t *d_perm = nullptr;
+  int32_t *d_perm = nullptr, *d_perm2 = nullptr;
   uint32_t *d_sort_id = nullptr;
   int32_t *d_scan_blk = nullptr;
   unsigned long long *d_counters = nullptr;  // misc device counters

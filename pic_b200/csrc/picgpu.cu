@@ -61,9 +61,18 @@ __device__ __forceinline__ int locate_elem(const MeshK &m, double x, double y) {
   return (i - 1) * m.ney + (j - 1);
 }
 
+// e / ney without an integer division: a double-reciprocal estimate and an
+// exact integer correction.
+__device__ __forceinline__ int elem_column(const MeshK &m, int e) {
+  int i = (int)((double)e * m.inv_ney);
+  if (i * m.ney > e) --i;
+  if ((i + 1) * m.ney <= e) ++i;
+  return i;
+}
+
 __device__ __forceinline__ void bilinear(const MeshK &m, int e, double x, double y, double W[4],
                                          int nodes[4], int *ie, int *je) {
-  int i = e / m.ney, j = e - i * m.ney;
+  int i = elem_column(m, e), j = e - i * m.ney;
   double x1 = m.xs[i], x2 = m.xs[i + 1], y1 = m.ys[j], y2 = m.ys[j + 1];
   double hxp = x2 - x1, hyp = y2 - y1;
   double dx = (x - x1) / hxp;
@@ -142,7 +151,7 @@ __global__ void k_locate(MeshK m, const double *__restrict__ x, const double *__
 
 struct PushK {
   double qm, dt, mass, vref;
-  int do_push, do_deposit;
+  int do_push, do_deposit, do_energy;
   int wall[4];
 };
 
@@ -174,8 +183,8 @@ __device__ __forceinline__ bool absorbed_by_object(double x, double y) {
   return false;
 }
 
-// Segmented warp sum of an int64 value over lanes with the same key
-// (particles are cell-sorted, so neighbouring lanes usually share a cell).
+// Segmented warp sum of an int64 value over lanes [lane, seg_end] of one
+// segment (reduction toward the segment head).
 __device__ __forceinline__ long long seg_sum(long long v, int lane, int seg_end) {
 #pragma unroll
   for (int off = 1; off < 32; off <<= 1) {
@@ -266,7 +275,7 @@ __global__ void __launch_bounds__(256) k_push(MeshK m, FieldK f, PushK prm, SpK 
           key = en;
           int ie, je;
           bilinear(m, en, x, y, W, nodes, &ie, &je);
-          double vz = s.vz[p];
+          double vz = prm.do_energy ? s.vz[p] : 0.0;
           energy = ((((0.5 * prm.mass) * ((vx * vx + vy * vy) + vz * vz)) * prm.vref) * prm.vref) /
                    PIC_JTOEV;
         }
@@ -277,30 +286,29 @@ __global__ void __launch_bounds__(256) k_push(MeshK m, FieldK f, PushK prm, SpK 
   unsigned int lm = __ballot_sync(0xffffffffu, lost);
   if (lane == 0 && lm) atomicAdd(s.lost, (unsigned long long)__popc(lm));
   if (!prm.do_deposit) return;
-  // segmented warp aggregation by element, then one atomic per node and value
+  // Segmented warp aggregation by element (particles are cell-sorted, so
+  // neighbouring lanes usually share an element), then one atomic per node and
+  // value from the segment head.  Integer sums are exact: node totals do not
+  // depend on the segmentation.
   int prev = __shfl_up_sync(0xffffffffu, key, 1);
   bool head = (lane == 0) || (key != prev);
   unsigned int heads = __ballot_sync(0xffffffffu, head);
   unsigned int above = (lane == 31) ? 0u : (heads & ~((2u << lane) - 1u));
   int seg_end = above ? (__ffs(above) - 2) : 31;
-  long long qv[4], ev[4];
+  long long qv[4];
 #pragma unroll
-  for (int c = 0; c < 4; ++c) {
-    qv[c] = (key >= 0) ? __double2ll_rn(W[c] * PIC_Q_SCALE) : 0ll;
-    ev[c] = (key >= 0) ? __double2ll_rn((W[c] * energy) * PIC_E_SCALE) : 0ll;
-  }
+  for (int c = 0; c < 4; ++c) qv[c] = seg_sum((key >= 0) ? __double2ll_rn(W[c] * PIC_Q_SCALE) : 0ll, lane, seg_end);
+  if (head && key >= 0)
 #pragma unroll
-  for (int c = 0; c < 4; ++c) {
-    qv[c] = seg_sum(qv[c], lane, seg_end);
-    ev[c] = seg_sum(ev[c], lane, seg_end);
-  }
-  if (head && key >= 0) {
+    for (int c = 0; c < 4; ++c) atomicAdd(s.q_acc + nodes[c], (unsigned long long)qv[c]);
+  if (!prm.do_energy) return;
+  long long ev[4];
 #pragma unroll
-    for (int c = 0; c < 4; ++c) {
-      atomicAdd(s.q_acc + nodes[c], (unsigned long long)qv[c]);
-      atomicAdd(s.e_acc + nodes[c], (unsigned long long)ev[c]);
-    }
-  }
+  for (int c = 0; c < 4; ++c)
+    ev[c] = seg_sum((key >= 0) ? __double2ll_rn((W[c] * energy) * PIC_E_SCALE) : 0ll, lane, seg_end);
+  if (head && key >= 0)
+#pragma unroll
+    for (int c = 0; c < 4; ++c) atomicAdd(s.e_acc + nodes[c], (unsigned long long)ev[c]);
 }
 
 // ----------------------------------------------------------------------------
@@ -313,6 +321,7 @@ struct RhoK {
   double wq[PIC_MAX_SPECIES], w[PIC_MAX_SPECIES];
   int ns;
   double L_ref, n_ref;
+  int energy;  // update the per-node mean energy (diagnostic steps)
 };
 
 // GetParChg_2D.f90:869-911: rho_s = Weight*qs*sum/L_ref/L_ref/n_ref/V; the
@@ -327,7 +336,7 @@ __global__ void k_rho(RhoK r, const double *__restrict__ vol, double *__restrict
     double esum = (double)(long long)r.e[s][n] * (1.0 / PIC_E_SCALE);
     double rs = ((((r.wq[s] * cnt) / r.L_ref) / r.L_ref) / r.n_ref) / V;
     r.rho_s[s][n] = rs;
-    r.ek_s[s][n] = (cnt != 0.0) ? esum / cnt : 0.0;
+    if (r.energy) r.ek_s[s][n] = (cnt != 0.0) ? esum / cnt : 0.0;
     acc = acc + rs;
   }
   rho[n] = acc;
@@ -374,7 +383,7 @@ __global__ void k_rhs(RhsK k) {
 __constant__ double c_stencil[16][9];
 
 struct PcgK {
-  const int32_t *row_kind, *ex_ptr, *ex_col;
+  const int32_t *row_kind, *ex_cnt, *ex_col;
   const double *ex_val, *diag;
   double *x, *r, *w, *q, *b;
   const double *p_old;
@@ -401,8 +410,22 @@ __device__ __forceinline__ double row_apply(const PcgK &k, int64_t n, F v) {
 #pragma unroll
       for (int c = 0; c < 3; ++c) acc = fma(c_stencil[kind][3 * a + c], v(base + (int64_t)a * k.nny + c), acc);
   } else {
-    int rix = kind - k.n_mat;
-    for (int q = k.ex_ptr[rix]; q < k.ex_ptr[rix + 1]; ++q) acc = fma(k.ex_val[q], v((int64_t)k.ex_col[q]), acc);
+    // explicit row, padded to 9 slots so all loads are in flight together;
+    // only the first cnt slots enter the sum, in CSR order
+    const int rix = kind - k.n_mat;
+    const int cnt = k.ex_cnt[rix];
+    int32_t col[9];
+    double val[9], xv[9];
+#pragma unroll
+    for (int q = 0; q < 9; ++q) {
+      col[q] = k.ex_col[9 * (size_t)rix + q];
+      val[q] = k.ex_val[9 * (size_t)rix + q];
+    }
+#pragma unroll
+    for (int q = 0; q < 9; ++q) xv[q] = v((int64_t)col[q]);
+#pragma unroll
+    for (int q = 0; q < 9; ++q)
+      if (q < cnt) acc = fma(val[q], xv[q], acc);
   }
   return acc;
 }
@@ -564,52 +587,111 @@ struct PcgP {
   unsigned int bar_extra; // arrivals expected beyond the grid (0; >0 only to test the timeout)
 };
 
-// Grid-wide barrier with a bounded wait: after `limit` polls the CTA records
-// the timeout in *err and leaves; every CTA then exits the solve, so a lost
-// CTA ends the kernel with an error status instead of a hang.
+__device__ __forceinline__ unsigned int ld_acquire_gpu(const unsigned int *p) {
+  unsigned int v;
+  asm volatile("ld.acquire.gpu.global.u32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
+  return v;
+}
+
+__device__ __forceinline__ unsigned int atom_add_release_gpu(unsigned int *p, unsigned int v) {
+  unsigned int o;
+  asm volatile("atom.add.release.gpu.global.u32 %0, [%1], %2;" : "=r"(o) : "l"(p), "r"(v) : "memory");
+  return o;
+}
+
+// Grid-wide barrier on a monotonic arrival counter: thread 0 of every CTA
+// adds 1 with release semantics (after the CTA barrier, so the whole CTA's
+// writes are ordered before it) and polls with acquire loads until the count
+// reaches the end of its round.  The wait is bounded: after `limit` polls the
+// CTA records the timeout in *err and leaves; every CTA then exits the solve,
+// so a lost CTA ends the kernel with an error status instead of a hang.
 __device__ __forceinline__ bool grid_barrier(unsigned int *bar, int *err, long long limit,
                                              unsigned int extra) {
   __syncthreads();
   if (threadIdx.x == 0) {
-    volatile unsigned int *vgen = bar + 1;
-    unsigned int g0 = *vgen;
-    __threadfence();
-    unsigned int t = atomicAdd(bar, 1u);
-    if (t == gridDim.x - 1 + extra) {
-      atomicExch(bar, 0u);
-      __threadfence();
-      atomicAdd(bar + 1, 1u);
-    } else {
-      long long spins = 0;
-      while (*vgen == g0) {
-        __nanosleep(32);
-        if (++spins > limit) {
-          atomicExch(err, 1);
-          break;
-        }
+    const unsigned int n = gridDim.x + extra;
+    unsigned int t = atom_add_release_gpu(bar, 1u);
+    unsigned int target = (t / n + 1u) * n;
+    long long spins = 0;
+    while ((int)(ld_acquire_gpu(bar) - target) < 0) {
+      if (++spins > limit) {
+        atomicExch(err, 1);
+        break;
       }
     }
-    __threadfence();
   }
   __syncthreads();
   return *(volatile int *)err == 0;
 }
 
+// The persistent solver runs CTAs of PIC_RED_CHUNK (1024) threads, one chunk
+// node per thread, so all loads of a phase are in flight together.  Products
+// are staged in shared memory and the first PIC_RED_THREADS threads then sum
+// them exactly as the canonical reduction does (items t, t+256, t+512, t+768
+// in order, xor butterfly, warp sums in order).
+constexpr int kWide = PIC_RED_CHUNK;
+
+// Canonical partial of a chunk: NV dot products sum_i fma(a_k[i], b_k[i], .)
+// over the first nvalid entries; result valid in thread 0.
 template <int NV>
-__device__ __forceinline__ void final_sum_bcast(const double *part, int nb, double *out_all) {
-  __shared__ double bc[NV];
-  double o[NV];
-  final_sum_canon<NV>(part, nb, o);
-  if (threadIdx.x == 0)
-    for (int k = 0; k < NV; ++k) bc[k] = o[k];
+__device__ __forceinline__ void chunk_dots(const double (*a)[kWide], const double (*b)[kWide], int nvalid,
+                                           double *out) {
+  __shared__ double ws[NV][PIC_RED_THREADS / 32];
+  if (threadIdx.x < PIC_RED_THREADS) {
+#pragma unroll
+    for (int k = 0; k < NV; ++k) {
+      double acc = 0.0;
+      for (int it = 0; it < PIC_RED_ITEMS; ++it) {
+        int i = it * PIC_RED_THREADS + threadIdx.x;
+        if (i < nvalid) acc = fma(a[k][i], b[k][i], acc);
+      }
+      for (int off = 16; off > 0; off >>= 1) acc = acc + __shfl_xor_sync(0xffffffffu, acc, off);
+      if ((threadIdx.x & 31) == 0) ws[k][threadIdx.x >> 5] = acc;
+    }
+  }
   __syncthreads();
+  if (threadIdx.x == 0)
+#pragma unroll
+    for (int k = 0; k < NV; ++k) {
+      double t = 0.0;
+      for (int q = 0; q < PIC_RED_THREADS / 32; ++q) t = t + ws[k][q];
+      out[k] = t;
+    }
+  __syncthreads();
+}
+
+// Sum of nb chunk partials in the canonical order, broadcast to every thread.
+template <int NV>
+__device__ __forceinline__ void final_sum_wide(const double *part, int nb, double *out_all) {
+  __shared__ double ws[NV][PIC_RED_THREADS / 32];
+  __shared__ double bc[NV];
+  if (threadIdx.x < PIC_RED_THREADS) {
+#pragma unroll
+    for (int k = 0; k < NV; ++k) {
+      double a = 0.0;
+      for (int b = threadIdx.x; b < nb; b += PIC_RED_THREADS) a = a + __ldcg(part + (size_t)k * nb + b);
+      for (int off = 16; off > 0; off >>= 1) a = a + __shfl_xor_sync(0xffffffffu, a, off);
+      if ((threadIdx.x & 31) == 0) ws[k][threadIdx.x >> 5] = a;
+    }
+  }
+  __syncthreads();
+  if (threadIdx.x == 0)
+#pragma unroll
+    for (int k = 0; k < NV; ++k) {
+      double t = 0.0;
+      for (int q = 0; q < PIC_RED_THREADS / 32; ++q) t = t + ws[k][q];
+      bc[k] = t;
+    }
+  __syncthreads();
+#pragma unroll
   for (int k = 0; k < NV; ++k) out_all[k] = bc[k];
   __syncthreads();
 }
 
-__global__ void __launch_bounds__(PIC_RED_THREADS) k_pcg_persist(PcgP P) {
+__global__ void __launch_bounds__(kWide, 1) k_pcg_persist(PcgP P) {
   const PcgK &k = P.k;
   PcgState *S = k.st;
+  __shared__ double sa[2][kWide], sb[2][kWide];
   double rho = __ldcg(&S->rho), normRHS = __ldcg(&S->normRHS);
   const double tol2 = S->tol2;
   const int maxit = S->maxit;
@@ -624,54 +706,62 @@ __global__ void __launch_bounds__(PIC_RED_THREADS) k_pcg_persist(PcgP P) {
       double wm = __ldcg(k.w + m);
       return first ? wm : fma(beta, __ldcg(pold + m), wm);
     };
+    // (A) p = w + beta p, q = A p, chunk partials of p.q
     for (int c = blockIdx.x; c < k.nb; c += gridDim.x) {
-      double vpq = 0.0;
-      for (int it = 0; it < PIC_RED_ITEMS; ++it) {
-        int64_t n = (int64_t)c * PIC_RED_CHUNK + it * PIC_RED_THREADS + threadIdx.x;
-        if (n >= k.nn) continue;
-        double pv = pn(n);
-        double qv = row_apply(k, n, pn);
+      const int64_t base = (int64_t)c * kWide;
+      const int nvalid = (int)min((int64_t)kWide, k.nn - base);
+      const int64_t n = base + threadIdx.x;
+      double pv = 0.0, qv = 0.0;
+      if (threadIdx.x < nvalid) {
+        pv = pn(n);
+        qv = row_apply(k, n, pn);
         pnew[n] = pv;
         k.q[n] = qv;
-        vpq = fma(pv, qv, vpq);
       }
-      double v[1] = {vpq}, out[1];
-      block_sum_canon<1>(v, out);
-      if (threadIdx.x == 0) P.partA[c] = out[0];
+      sa[0][threadIdx.x] = pv;
+      sb[0][threadIdx.x] = qv;
+      __syncthreads();
+      double part[1];
+      chunk_dots<1>(sa, sb, nvalid, part);
+      if (threadIdx.x == 0) P.partA[c] = part[0];
     }
     if (!(ok = grid_barrier(P.bar, P.bar_err, P.spin_limit, P.bar_extra))) break;
     double pq;
-    final_sum_bcast<1>(P.partA, k.nb, &pq);
+    final_sum_wide<1>(P.partA, k.nb, &pq);
     if (pq == 0.0) {
       ierr = 3;
       break;
     }
     const double alpha = rho / pq;
+    // (B) x += alpha p, r -= alpha q, w = r/diag, chunk partials of r.r and r.w
     for (int c = blockIdx.x; c < k.nb; c += gridDim.x) {
-      double vrr = 0.0, vrw = 0.0;
-      for (int it = 0; it < PIC_RED_ITEMS; ++it) {
-        int64_t n = (int64_t)c * PIC_RED_CHUNK + it * PIC_RED_THREADS + threadIdx.x;
-        if (n >= k.nn) continue;
-        double pv = pnew[n];
-        double xv = fma(alpha, pv, k.x[n]);
-        double rv = fma(-alpha, k.q[n], k.r[n]);
-        double wv = rv / k.diag[n];
+      const int64_t base = (int64_t)c * kWide;
+      const int nvalid = (int)min((int64_t)kWide, k.nn - base);
+      const int64_t n = base + threadIdx.x;
+      double rv = 0.0, wv = 0.0;
+      if (threadIdx.x < nvalid) {
+        double xv = fma(alpha, pnew[n], k.x[n]);
+        rv = fma(-alpha, k.q[n], k.r[n]);
+        wv = rv / k.diag[n];
         k.x[n] = xv;
         k.r[n] = rv;
         k.w[n] = wv;
-        vrr = fma(rv, rv, vrr);
-        vrw = fma(rv, wv, vrw);
       }
-      double v[2] = {vrr, vrw}, out[2];
-      block_sum_canon<2>(v, out);
+      sa[0][threadIdx.x] = rv;
+      sb[0][threadIdx.x] = rv;
+      sa[1][threadIdx.x] = rv;
+      sb[1][threadIdx.x] = wv;
+      __syncthreads();
+      double part[2];
+      chunk_dots<2>(sa, sb, nvalid, part);
       if (threadIdx.x == 0) {
-        P.partB[c] = out[0];
-        P.partB[k.nb + c] = out[1];
+        P.partB[c] = part[0];
+        P.partB[k.nb + c] = part[1];
       }
     }
     if (!(ok = grid_barrier(P.bar, P.bar_err, P.spin_limit, P.bar_extra))) break;
     double tot[2];
-    final_sum_bcast<2>(P.partB, k.nb, tot);
+    final_sum_wide<2>(P.partB, k.nb, tot);
     normR = tot[0];
     rho0 = rho;
     rho = tot[1];
@@ -682,6 +772,190 @@ __global__ void __launch_bounds__(PIC_RED_THREADS) k_pcg_persist(PcgP P) {
     else beta = rho / rho0;
     parity ^= 1;
   }
+  if (blockIdx.x == 0 && threadIdx.x == 0) {
+    S->iter = iter;
+    S->ierr = ok ? ierr : 4;
+    S->normR = normR;
+    S->rho = rho;
+    S->done = 1;
+  }
+}
+
+// ---------------------------------------------------------------------------
+// Shared-memory-resident persistent Jacobi-PCG.  CTA b owns the contiguous
+// chunks [c0, c1) (nodes [n0, n1), at most kSmemChunks chunks) and keeps
+// x, r, q, diag, p_new of its nodes and a window [n0-H, n1+H) of w and p
+// (H = nny+1, the reach of a 3x3 stencil) in shared memory for the whole
+// solve.  Per iteration only the H-wide boundary strips of w and p cross
+// L2: published before the second barrier, read after it.  Same chunk
+// partials and canonical sums as the other PCG kernels, so the same bits.
+// ---------------------------------------------------------------------------
+constexpr int kSmemChunks = 2;
+
+struct PcgS {
+  PcgK k;
+  double *w_g, *p_g;      // boundary-strip exchange (full-grid arrays)
+  double *partA, *partB;
+  unsigned int *bar;
+  int *bar_err;
+  long long spin_limit;
+  unsigned int bar_extra;
+  int H;                  // halo width in nodes
+};
+
+__host__ __device__ inline void smem_range(int b, int G, int nb, int *c0, int *c1) {
+  *c0 = (int)((int64_t)b * nb / G);
+  *c1 = (int)((int64_t)(b + 1) * nb / G);
+}
+
+__global__ void __launch_bounds__(kWide, 1) k_pcg_smem(PcgS P) {
+  extern __shared__ double smem[];
+  const PcgK &k = P.k;
+  PcgState *S = k.st;
+  int c0, c1;
+  smem_range(blockIdx.x, gridDim.x, k.nb, &c0, &c1);
+  const int64_t n0 = (int64_t)c0 * kWide;
+  const int64_t n1 = min((int64_t)c1 * kWide, k.nn);
+  const int L = (int)(n1 - n0);
+  const int H = P.H;
+  const int64_t wbase = n0 - H;     // node of window slot 0
+  const int W = L + 2 * H;
+  double *win_w = smem, *win_p = win_w + W;
+  double *s_x = win_p + W, *s_r = s_x + kSmemChunks * kWide, *s_q = s_r + kSmemChunks * kWide;
+  double *s_d = s_q + kSmemChunks * kWide, *s_pn = s_d + kSmemChunks * kWide;
+  // load own x, r, diag and the window of w (p is not read before iteration 1)
+  for (int i = threadIdx.x; i < L; i += kWide) {
+    s_x[i] = __ldcg(k.x + n0 + i);
+    s_r[i] = __ldcg(k.r + n0 + i);
+    s_d[i] = k.diag[n0 + i];
+  }
+  for (int i = threadIdx.x; i < W; i += kWide) {
+    int64_t m = wbase + i;
+    win_w[i] = (m >= 0 && m < k.nn) ? __ldcg(k.w + m) : 0.0;
+    win_p[i] = 0.0;
+  }
+  __syncthreads();
+  double rho = __ldcg(&S->rho), normRHS = __ldcg(&S->normRHS);
+  const double tol2 = S->tol2;
+  const int maxit = S->maxit;
+  int done = __ldcg(&S->done), iter = 0, ierr = 0;
+  double beta = 0.0, normR = 0.0, rho0 = 0.0;
+  bool ok = true;
+  while (!done) {
+    const bool first = iter == 0;
+    auto pn = [&](int64_t m) {
+      const int64_t i = m - wbase;
+      return first ? win_w[i] : fma(beta, win_p[i], win_w[i]);
+    };
+    // (A) p = w + beta p, q = A p, chunk partials of p.q
+    for (int c = c0; c < c1; ++c) {
+      const int off = (c - c0) * kWide;
+      const int nvalid = (int)min((int64_t)kWide, n1 - (int64_t)c * kWide);
+      const int64_t n = (int64_t)c * kWide + threadIdx.x;
+      double pv = 0.0, qv = 0.0;
+      if (threadIdx.x < nvalid) {
+        pv = pn(n);
+        qv = row_apply(k, n, pn);
+      }
+      s_pn[off + threadIdx.x] = pv;
+      s_q[off + threadIdx.x] = qv;
+      __syncthreads();
+      double part[1];
+      const double(*a)[kWide] = reinterpret_cast<const double(*)[kWide]>(s_pn + off);
+      const double(*b)[kWide] = reinterpret_cast<const double(*)[kWide]>(s_q + off);
+      chunk_dots<1>(a, b, nvalid, part);
+      if (threadIdx.x == 0) P.partA[c] = part[0];
+    }
+    if (!(ok = grid_barrier(P.bar, P.bar_err, P.spin_limit, P.bar_extra))) break;
+    double pq;
+    final_sum_wide<1>(P.partA, k.nb, &pq);
+    if (pq == 0.0) {
+      ierr = 3;
+      break;
+    }
+    const double alpha = rho / pq;
+    // (B) x += alpha p, r -= alpha q, w = r/diag; window gets w and p for the
+    // next iteration; boundary strips are published to L2
+    for (int c = c0; c < c1; ++c) {
+      const int off = (c - c0) * kWide;
+      const int nvalid = (int)min((int64_t)kWide, n1 - (int64_t)c * kWide);
+      const int i = off + threadIdx.x;
+      if (threadIdx.x < nvalid) {
+        const double pv = s_pn[i];
+        s_x[i] = fma(alpha, pv, s_x[i]);
+        const double rv = fma(-alpha, s_q[i], s_r[i]);
+        const double wv = rv / s_d[i];
+        s_r[i] = rv;
+        s_q[i] = wv;  // q is dead after the update: reuse its slot for w
+        win_w[H + i] = wv;
+        win_p[H + i] = pv;
+        if (i < H || i >= L - H) {
+          P.w_g[n0 + i] = wv;
+          P.p_g[n0 + i] = pv;
+        }
+      }
+      __syncthreads();
+      double part[2];
+      const double *ra = s_r + off;
+      const double *wa = s_q + off;
+      // r.r and r.w in one canonical pass
+      {
+        __shared__ double ws2[2][PIC_RED_THREADS / 32];
+        if (threadIdx.x < PIC_RED_THREADS) {
+          double arr = 0.0, arw = 0.0;
+          for (int it = 0; it < PIC_RED_ITEMS; ++it) {
+            int j = it * PIC_RED_THREADS + threadIdx.x;
+            if (j < nvalid) {
+              arr = fma(ra[j], ra[j], arr);
+              arw = fma(ra[j], wa[j], arw);
+            }
+          }
+          for (int o2 = 16; o2 > 0; o2 >>= 1) {
+            arr = arr + __shfl_xor_sync(0xffffffffu, arr, o2);
+            arw = arw + __shfl_xor_sync(0xffffffffu, arw, o2);
+          }
+          if ((threadIdx.x & 31) == 0) {
+            ws2[0][threadIdx.x >> 5] = arr;
+            ws2[1][threadIdx.x >> 5] = arw;
+          }
+        }
+        __syncthreads();
+        if (threadIdx.x == 0) {
+          double t0 = 0.0, t1 = 0.0;
+          for (int q = 0; q < PIC_RED_THREADS / 32; ++q) {
+            t0 = t0 + ws2[0][q];
+            t1 = t1 + ws2[1][q];
+          }
+          part[0] = t0;
+          part[1] = t1;
+          P.partB[c] = part[0];
+          P.partB[k.nb + c] = part[1];
+        }
+        __syncthreads();
+      }
+    }
+    if (!(ok = grid_barrier(P.bar, P.bar_err, P.spin_limit, P.bar_extra))) break;
+    // halo of the window from the neighbours' published strips
+    for (int i = threadIdx.x; i < 2 * H; i += kWide) {
+      const int slot = (i < H) ? i : (L + i);
+      const int64_t m = wbase + slot;
+      if (m >= 0 && m < k.nn) {
+        win_w[slot] = __ldcg(P.w_g + m);
+        win_p[slot] = __ldcg(P.p_g + m);
+      }
+    }
+    double tot[2];
+    final_sum_wide<2>(P.partB, k.nb, tot);
+    normR = tot[0];
+    rho0 = rho;
+    rho = tot[1];
+    ++iter;
+    if (normR / normRHS <= tol2) done = 1;
+    else if (iter >= maxit) { ierr = 1; done = 1; }
+    else if (rho0 == 0.0) { ierr = 2; done = 1; }
+    else beta = rho / rho0;
+  }
+  for (int i = threadIdx.x; i < L; i += kWide) k.x[n0 + i] = s_x[i];
   if (blockIdx.x == 0 && threadIdx.x == 0) {
     S->iter = iter;
     S->ierr = ok ? ierr : 4;
@@ -855,11 +1129,11 @@ static void free_all() {
   };
   F(g.d_xs); F(g.d_ys); F(g.d_element_index); F(g.d_node_index); F(g.d_node_type);
   F(g.d_phi_dir); F(g.d_cell_volume); F(g.d_rhs_fix); F(g.d_mass_q1); F(g.d_ife_mass);
-  F(g.d_xt_ptr); F(g.d_xt_col); F(g.d_xt_val); F(g.d_row_kind); F(g.d_ex_ptr); F(g.d_ex_col);
+  F(g.d_xt_ptr); F(g.d_xt_col); F(g.d_xt_val); F(g.d_row_kind); F(g.d_ex_cnt); F(g.d_ex_col);
   F(g.d_ex_val); F(g.d_diag); F(g.d_ppr_kind); F(g.d_ppr_ptr); F(g.d_ppr_nodes); F(g.d_ppr_rows);
   F(g.d_ppr_h); F(g.d_phi); F(g.d_rho); F(g.d_efx); F(g.d_efy); F(g.d_coef); F(g.d_b); F(g.d_x);
   F(g.d_r); F(g.d_w); F(g.d_p[0]); F(g.d_p[1]); F(g.d_q); F(g.d_part); F(g.d_pcg); F(g.d_bar);
-  F(g.d_cell_count); F(g.d_cell_start); F(g.d_cell_fill); F(g.d_perm); F(g.d_sort_id);
+  F(g.d_cell_count); F(g.d_cell_start); F(g.d_cell_fill); F(g.d_perm); F(g.d_perm2); F(g.d_sort_id);
   F(g.d_scan_blk); F(g.d_counters); F(g.d_hist); F(g.d_sel); F(g.d_cand); F(g.d_cand_slot);
   F(g.d_mcc_misc); F(g.d_ion_parent); F(g.d_ion_data);
   for (int s = 0; s < PIC_MAX_SPECIES; ++s) {
@@ -894,7 +1168,7 @@ static int zero_counter(int idx) {
 }
 
 // push and/or locate+deposit for one species
-static int run_push(int sidx, bool do_push, bool do_deposit) {
+static int run_push(int sidx, bool do_push, bool do_deposit, bool do_energy) {
   Species &s = g.sp[sidx];
   if (s.n_slots == 0) return PIC_OK;
   FieldK f{g.d_efx, g.d_efy, g.d_coef, g.d_coef + g.nn, g.d_coef + 2 * g.nn, g.d_coef + 3 * g.nn,
@@ -906,6 +1180,7 @@ static int run_push(int sidx, bool do_push, bool do_deposit) {
   prm.vref = g.v_ref;
   prm.do_push = do_push;
   prm.do_deposit = do_deposit;
+  prm.do_energy = do_deposit && do_energy;
   for (int w = 0; w < 4; ++w) prm.wall[w] = g.P.wall_bc[w];
   SpK k{s.x, s.y, s.vx, s.vy, s.vz, s.loc, s.q_acc, s.e_acc, g.d_counters + 8 + sidx, g.d_counters + 1,
         s.n_slots};
@@ -914,18 +1189,19 @@ static int run_push(int sidx, bool do_push, bool do_deposit) {
   return PIC_OK;
 }
 
-static int zero_deposit() {
+static int zero_deposit(bool energy) {
   for (int s = 0; s < g.ns; ++s) {
     PIC_CUDA(cudaMemsetAsync(g.sp[s].q_acc, 0, g.nn * sizeof(unsigned long long), g.st));
-    PIC_CUDA(cudaMemsetAsync(g.sp[s].e_acc, 0, g.nn * sizeof(unsigned long long), g.st));
+    if (energy) PIC_CUDA(cudaMemsetAsync(g.sp[s].e_acc, 0, g.nn * sizeof(unsigned long long), g.st));
   }
   return PIC_OK;
 }
 
-static int run_rho() {
+static int run_rho(bool energy) {
   RhoK r;
   std::memset(&r, 0, sizeof r);
   r.ns = g.ns;
+  r.energy = energy;
   r.L_ref = g.L_ref;
   r.n_ref = g.P.n_ref;
   for (int s = 0; s < g.ns; ++s) {
@@ -944,7 +1220,7 @@ static int run_rho() {
 static PcgK pcg_k(int parity) {
   PcgK k;
   k.row_kind = g.d_row_kind;
-  k.ex_ptr = g.d_ex_ptr;
+  k.ex_cnt = g.d_ex_cnt;
   k.ex_col = g.d_ex_col;
   k.ex_val = g.d_ex_val;
   k.diag = g.d_diag;
@@ -1014,9 +1290,26 @@ static int run_pcg(pic_solve_stats *stats) {
     P.spin_limit = g.pcg_spin_limit;
     P.bar_extra = g.pcg_bar_extra;
     PIC_CUDA(cudaMemsetAsync(g.d_bar, 0, 4 * sizeof(unsigned int), g.st));
-    void *args[] = {&P};
-    PIC_CUDA(cudaLaunchCooperativeKernel((const void *)k_pcg_persist, dim3(g.coop_grid),
-                                         dim3(PIC_RED_THREADS), args, 0, g.st));
+    if (g.smem_grid > 0) {
+      PcgS Q;
+      Q.k = pcg_k(0);
+      Q.w_g = g.d_p[1];  // strip exchange buffers: free while the smem solver runs
+      Q.p_g = g.d_p[0];
+      Q.partA = P.partA;
+      Q.partB = P.partB;
+      Q.bar = P.bar;
+      Q.bar_err = P.bar_err;
+      Q.spin_limit = P.spin_limit;
+      Q.bar_extra = P.bar_extra;
+      Q.H = g.m.nny + 1;
+      void *args[] = {&Q};
+      PIC_CUDA(cudaLaunchCooperativeKernel((const void *)k_pcg_smem, dim3(g.smem_grid), dim3(kWide), args,
+                                           g.smem_bytes, g.st));
+    } else {
+      void *args[] = {&P};
+      PIC_CUDA(cudaLaunchCooperativeKernel((const void *)k_pcg_persist, dim3(g.coop_grid), dim3(kWide),
+                                           args, 0, g.st));
+    }
     PIC_LAUNCHED();
     PIC_CUDA(cudaMemcpyAsync(&hs, g.d_pcg, sizeof hs, cudaMemcpyDeviceToHost, g.st));
     PIC_CUDA(cudaStreamSynchronize(g.st));
@@ -1168,6 +1461,7 @@ int pic_init(const pic_mesh_desc *mesh, const pic_params *params) {
   m.ymax = mesh->ymax;
   m.hx = (m.xmax - m.xmin) / (m.nnx - 1);
   m.hy = (m.ymax - m.ymin) / (m.nny - 1);
+  m.inv_ney = 1.0 / m.ney;
   g.nn = (int64_t)m.nnx * m.nny;
   g.ne = (int64_t)m.nex * m.ney;
   const int64_t nn = g.nn, ne = g.ne;
@@ -1297,7 +1591,7 @@ int pic_init(const pic_mesh_desc *mesh, const pic_params *params) {
         for (int q = 0; q < g.n_mat && !known; ++q) known = std::memcmp(g.h_stencil[q], S, sizeof S) == 0;
         if (!known) std::memcpy(g.h_stencil[g.n_mat++], S, sizeof S);
       }
-    std::vector<int32_t> kind(nn, -1), ex_ptr(1, 0), ex_col;
+    std::vector<int32_t> kind(nn, -1), ex_cnt, ex_col;
     std::vector<double> ex_val, diag(nn, 1.0);
     for (int64_t n = 0; n < nn; ++n) {
       int u = mesh->node_type[n];
@@ -1324,17 +1618,23 @@ int pic_init(const pic_mesh_desc *mesh, const pic_params *params) {
       if (mat >= 0) {
         kind[n] = mat;
       } else {
-        kind[n] = g.n_mat + (int32_t)(ex_ptr.size() - 1);
-        for (auto &pr : ent) {
-          ex_col.push_back((int32_t)pr.first);
-          ex_val.push_back(pr.second);
+        if (ent.size() > 9) {
+          set_error("pic_init: stiffness row with more than 9 entries");
+          return PIC_ERR_ARG;
         }
-        ex_ptr.push_back((int32_t)ex_col.size());
+        kind[n] = g.n_mat + (int32_t)ex_cnt.size();
+        ex_cnt.push_back((int32_t)ent.size());
+        for (auto &pr : ent)
+          if (pr.first < n - nny - 1 || pr.first > n + nny + 1) g.ex_local = false;
+        for (size_t q = 0; q < 9; ++q) {
+          ex_col.push_back(q < ent.size() ? (int32_t)ent[q].first : (int32_t)n);
+          ex_val.push_back(q < ent.size() ? ent[q].second : 0.0);
+        }
       }
     }
     PIC_CUDA(cudaMemcpyToSymbol(c_stencil, g.h_stencil, sizeof g.h_stencil));
     if ((rc = upload(&g.d_row_kind, kind.data(), kind.size()))) return rc;
-    if ((rc = upload(&g.d_ex_ptr, ex_ptr.data(), ex_ptr.size()))) return rc;
+    if ((rc = upload(&g.d_ex_cnt, ex_cnt.data(), ex_cnt.size()))) return rc;
     if ((rc = upload(&g.d_ex_col, ex_col.data(), ex_col.size()))) return rc;
     if ((rc = upload(&g.d_ex_val, ex_val.data(), ex_val.size()))) return rc;
     if ((rc = upload(&g.d_diag, diag.data(), diag.size()))) return rc;
@@ -1440,13 +1740,32 @@ int pic_init(const pic_mesh_desc *mesh, const pic_params *params) {
     PIC_CUDA(cudaGetDevice(&dev));
     PIC_CUDA(cudaDeviceGetAttribute(&coop, cudaDevAttrCooperativeLaunch, dev));
     PIC_CUDA(cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev));
-    PIC_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_pcg_persist, PIC_RED_THREADS, 0));
+    PIC_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_pcg_persist, kWide, 0));
     const char *env = getenv("PIC_PCG_PERSISTENT");
     bool want = !(env && env[0] == '0');
     g.coop_grid = (want && coop && per_sm > 0) ? std::min(g.red_blocks, per_sm * nsm) : 0;
+    // shared-memory-resident variant: every CTA owns at most kSmemChunks
+    // chunks and its window of w and p fits next to them
+    g.smem_grid = 0;
+    const char *env2 = getenv("PIC_PCG_SMEM");
+    bool want_smem = want && !(env2 && env2[0] == '0');
+    const int H = m.nny + 1;
+    const size_t bytes = (size_t)(2 * (kSmemChunks * kWide + 2 * H) + 5 * kSmemChunks * kWide) * sizeof(double);
+    int max_smem = 0;
+    PIC_CUDA(cudaDeviceGetAttribute(&max_smem, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev));
+    if (want_smem && coop && g.ex_local && bytes + 2048 <= (size_t)max_smem) {
+      PIC_CUDA(cudaFuncSetAttribute(k_pcg_smem, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes));
+      int per_sm2 = 0;
+      PIC_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm2, k_pcg_smem, kWide, bytes));
+      int G = std::min(g.red_blocks, per_sm2 * nsm);
+      if (per_sm2 > 0 && (int64_t)G * kSmemChunks >= g.red_blocks) {
+        g.smem_grid = G;
+        g.smem_bytes = bytes;
+      }
+    }
     // failure-path test hooks: a short wait limit and an arrival that never comes
     const char *lim = getenv("PIC_PCG_SPIN_LIMIT");
-    g.pcg_spin_limit = lim ? std::max(1ll, atoll(lim)) : (1ll << 24);
+    g.pcg_spin_limit = lim ? std::max(1ll, atoll(lim)) : (1ll << 22);
     const char *extra = getenv("PIC_PCG_BARRIER_EXTRA");
     g.pcg_bar_extra = extra ? (unsigned int)std::max(0, atoi(extra)) : 0u;
   }
@@ -1490,6 +1809,7 @@ int pic_init(const pic_mesh_desc *mesh, const pic_params *params) {
     PIC_CUDA(cudaMemset(sp.ek_s, 0, nn * sizeof(double)));
   }
   if ((rc = dalloc(&g.d_perm, maxcap))) return rc;
+  if ((rc = dalloc(&g.d_perm2, maxcap))) return rc;
   if ((rc = dalloc(&g.d_sort_id, maxcap))) return rc;
   PIC_CUDA(cudaDeviceSynchronize());
   g.inited = true;
@@ -1634,7 +1954,7 @@ int pic_move_all(int32_t species, int32_t push_flag) {
   if ((rc = check_init()) || (rc = check_species(species))) return rc;
   (void)push_flag;
   if ((rc = zero_counter(8 + species))) return rc;
-  if ((rc = run_push(species, true, false))) return rc;
+  if ((rc = run_push(species, true, false, false))) return rc;
   return count_live(species);
 }
 
@@ -1645,14 +1965,14 @@ int pic_get_par_chg(int32_t delta, double *rho_out) {
     set_error("pic_get_par_chg: only delta = 0 is supported");
     return PIC_ERR_ARG;
   }
-  if ((rc = zero_deposit())) return rc;
+  if ((rc = zero_deposit(true))) return rc;
   if ((rc = zero_counter(1))) return rc;
   for (int s = 0; s < g.ns; ++s) {
     if ((rc = zero_counter(8 + s))) return rc;
-    if ((rc = run_push(s, false, true))) return rc;
+    if ((rc = run_push(s, false, true, true))) return rc;
     if ((rc = count_live(s))) return rc;
   }
-  if ((rc = run_rho())) return rc;
+  if ((rc = run_rho(true))) return rc;
   unsigned long long bad = 0;
   if ((rc = read_counter(1, &bad))) return rc;
   if (bad) {
@@ -1711,8 +2031,12 @@ int pic_step(uint64_t step, pic_step_stats *stats) {
   cudaEvent_t e[8];
   for (auto &ev : e) PIC_CUDA(cudaEventCreate(&ev));
   PIC_CUDA(cudaEventRecord(e[0], g.st));
-  // 1. fused push + locate + deposit (MoveAll, then GetParChg_2D)
-  if ((rc = zero_deposit())) return rc;
+  // 1. fused push + locate + deposit (MoveAll, then GetParChg_2D).  The
+  // per-node energy (Ek_tot) is a diagnostic the reference only writes at its
+  // output cadence: it is deposited on steps that are multiples of
+  // diag_interval (every step when diag_interval <= 1).
+  const bool diag = g.P.diag_interval <= 1 || (step % (uint64_t)g.P.diag_interval) == 0;
+  if ((rc = zero_deposit(diag))) return rc;
   if ((rc = zero_counter(1))) return rc;
   int64_t before[PIC_MAX_SPECIES];
   int64_t pushed = 0;
@@ -1723,9 +2047,9 @@ int pic_step(uint64_t step, pic_step_stats *stats) {
   }
   PIC_CUDA(cudaEventRecord(e[6], g.st));
   for (int s = 0; s < g.ns; ++s)
-    if ((rc = run_push(s, true, true))) return rc;
+    if ((rc = run_push(s, true, true, diag))) return rc;
   PIC_CUDA(cudaEventRecord(e[7], g.st));
-  if ((rc = run_rho())) return rc;
+  if ((rc = run_rho(diag))) return rc;
   PIC_CUDA(cudaEventRecord(e[1], g.st));
   // 2. Poisson (IFE_Solve_2D)
   pic_solve_stats ss;

@@ -164,19 +164,10 @@ __global__ void k_gather_all(Gather7 g7, const int32_t *__restrict__ perm, int64
   g7.oid[i] = g7.id[p];
 }
 
-static int32_t *g_perm2 = nullptr;
-static int64_t g_perm2_cap = 0;
-
 int sort_species(int sidx) {
   Species &s = g.sp[sidx];
   const int64_t ne = g.ne;
   if (s.n_slots == 0) return PIC_OK;
-  if (g_perm2_cap < s.capacity) {
-    if (g_perm2) cudaFree(g_perm2);
-    g_perm2 = nullptr;
-    PIC_CUDA(cudaMalloc(&g_perm2, std::max<int64_t>(s.capacity, 1) * sizeof(int32_t)));
-    g_perm2_cap = s.capacity;
-  }
   PIC_CUDA(cudaMemsetAsync(g.d_cell_count, 0, (ne + 1) * sizeof(int32_t), g.st));
   k_sort_count<<<blocks_for(s.n_slots, 256), 256, 0, g.st>>>(s.loc, s.n_slots, g.d_cell_count);
   PIC_LAUNCHED();
@@ -189,12 +180,12 @@ int sort_species(int sidx) {
   k_sort_scatter<<<blocks_for(s.n_slots, 256), 256, 0, g.st>>>(s.loc, s.id, s.n_slots, g.d_cell_fill,
                                                                g.d_perm, g.d_sort_id);
   PIC_LAUNCHED();
-  k_sort_cells<<<blocks_for(ne, 8), 256, 0, g.st>>>(g.d_cell_start, ne, g.d_perm, g.d_sort_id, g_perm2);
+  k_sort_cells<<<blocks_for(ne, 8), 256, 0, g.st>>>(g.d_cell_start, ne, g.d_perm, g.d_sort_id, g.d_perm2);
   PIC_LAUNCHED();
   PIC_CUDA(cudaStreamSynchronize(g.st));
   if (total > 0) {
     Gather7 g7{s.x, s.y, s.vx, s.vy, s.vz, s.loc, s.id, s.x2, s.y2, s.vx2, s.vy2, s.vz2, s.loc2, s.id2};
-    k_gather_all<<<blocks_for(total, 256), 256, 0, g.st>>>(g7, g_perm2, total);
+    k_gather_all<<<blocks_for(total, 256), 256, 0, g.st>>>(g7, g.d_perm2, total);
     PIC_LAUNCHED();
   }
   std::swap(s.x, s.x2);

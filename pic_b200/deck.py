@@ -74,6 +74,9 @@ class Config:
     mcc: bool = True
     precision: int = api.PIC_PREC_FP64
     sort_interval: int = 10
+    # per-node energy deposit (a diagnostic) only on output steps; the
+    # reference writes its profiles every 1000 steps (Main_IFE_Test_2.f90:466-470)
+    diag_interval: int = 1000
 
     @property
     def scales(self) -> dict:

@@ -48,6 +48,7 @@ class Simulation:
         p.seed = cfg.seed
         p.precision = cfg.precision
         p.sort_interval = cfg.sort_interval
+        p.diag_interval = cfg.diag_interval
         p.solver = api.PIC_SOLVER_JPCG
         self.params = p
         api.check(self.lib.pic_init(self.mesh.ptr, C.byref(p)), "pic_init")

@@ -108,11 +108,12 @@ def test_get_par_chg_bit_exact():
 
 @pytest.fixture
 def pcg_mode(request, monkeypatch):
-    monkeypatch.setenv("PIC_PCG_PERSISTENT", "1" if request.param == "persistent" else "0")
+    monkeypatch.setenv("PIC_PCG_PERSISTENT", "0" if request.param == "two-kernel" else "1")
+    monkeypatch.setenv("PIC_PCG_SMEM", "1" if request.param == "smem-resident" else "0")
     return request.param
 
 
-@pytest.mark.parametrize("pcg_mode", ["persistent", "two-kernel"], indirect=True)
+@pytest.mark.parametrize("pcg_mode", ["smem-resident", "persistent", "two-kernel"], indirect=True)
 @pytest.mark.parametrize("name", ["tiny", "cfg1"])
 def test_ife_solve_bit_exact(name, pcg_mode):
     sim = _sim(name)
@@ -285,7 +286,8 @@ def _oracle_step(sim, parts, phi, step):
         qs.append(q)
         es.append(e)
         wq.append(sim.species[s][2] * sim.species[s][0])
-    rho, _, _ = ob.normalize(m.ptr, qs, es, wq, sim.scales["L_ref"], sim.cfg.n0, nn)
+    rho, _, ek = ob.normalize(m.ptr, qs, es, wq, sim.scales["L_ref"], sim.cfg.n0, nn)
+    parts["_ek"] = ek
     b = ob.rhs(m.ptr, rho, nn)
     phi, st = ob.pcg(m.ptr, b, phi, sim.cfg.pcg_tol, sim.cfg.pcg_maxit)
     c, efx, efy = ob.ppr(m.ptr, phi, nn)
@@ -317,7 +319,7 @@ def _oracle_step(sim, parts, phi, step):
 
 
 def test_full_steps_match_oracle():
-    sim = _sim("tiny", gas_p_Pa=300.0, Te_eV=20.0, sort_interval=3)
+    sim = _sim("tiny", gas_p_Pa=300.0, Te_eV=20.0, sort_interval=3, diag_interval=4)
     try:
         st0 = sim.initial_fields()
         parts = {}
@@ -344,6 +346,10 @@ def test_full_steps_match_oracle():
             created += sum(gst.mcc.n_created)
             gphi = sim.field("phi")
             assert np.abs(gphi - phi).max() <= 1e-10 * max(1.0, np.abs(phi).max()), step
+            if step % 4 == 0:  # diagnostic step: per-node mean energies deposited
+                for s, nm in ((0, "ek_e"), (1, "ek_i")):
+                    ref = parts["_ek"][s]
+                    assert np.abs(sim.field(nm) - ref).max() <= 1e-10 * max(1.0, np.abs(ref).max())
             for s in range(2):
                 g = _by_id(sim.download(s))
                 o = parts[s]
