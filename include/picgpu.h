@@ -165,7 +165,10 @@ typedef struct pic_solve_stats {
   int32_t ierr;           /* MY_PCG IERR: 0 ok, 1 cap, 2 rho0==0, 3 p.Ap==0   */
   double rel_residual;    /* sqrt(normR/normRHS) at exit                      */
   double ms;              /* device time of the solve                         */
-  int32_t fallback;       /* 1 when the learned FCG fell back to Jacobi-PCG   */
+  int32_t fallback;       /* 0, or why flexible CG handed over to Jacobi-PCG:
+                           * 1 cap, 2 breakdown (p.Ap <= 0), 3 stall, 4 NaN,
+                           * 5 preconditioner failed, 6 true residual above
+                           * tolerance after restarts                         */
   int32_t outer;          /* FP64 refinement sweeps (mixed precision)         */
 } pic_solve_stats;
 
@@ -285,6 +288,37 @@ int64_t pic_kernel_launches(void);
 /* Device timer on the library's stream: op 0 records the start event,
  * op 1 records the stop event, waits for it and writes the elapsed ms. */
 int pic_device_timer(int32_t op, double *ms_out);
+
+/* ---- learned preconditioner hook (flexible CG) ---- */
+
+/* Preconditioner z = M(r) for flexible CG: r and z are device vectors on the
+ * full node grid (0 on Dirichlet nodes).  Called on the host between two
+ * kernels of pic_ife_solve; it must leave z complete in the order of the
+ * library stream (enqueue on pic_cuda_stream(), or synchronise before
+ * returning).  Returns 0, or non-zero to make the solve fall back to
+ * Jacobi-PCG.  No reference counterpart: MY_PCG (IFE-Solver/MY_PCG.f90) is
+ * Jacobi-preconditioned only. */
+typedef int (*pic_precond_fn)(const double *r_dev, double *z_dev, void *user);
+
+/* Registers fn (NULL clears it).  With solver PIC_SOLVER_FCG_UNET and a
+ * registered fn, pic_ife_solve runs truncated flexible CG (FCG(m), Notay
+ * 2000) to the same relative tolerance as MY_PCG, accepted on the true
+ * residual b - A x, and falls back to Jacobi-PCG from the current iterate
+ * when FCG stalls or fn fails; pic_solve_stats.fallback reports why. */
+int pic_set_preconditioner(pic_precond_fn fn, void *user);
+/* Selects the linear solver at run time (PIC_SOLVER_*). */
+int pic_set_solver(int32_t solver);
+/* Directions FCG keeps for A-orthogonalisation, 1..8 (default 4; 1 = FCG(1)). */
+int pic_set_fcg_window(int32_t window);
+/* The library's CUDA stream (a cudaStream_t) for callers that enqueue work
+ * in its order. */
+int pic_cuda_stream(void **stream);
+/* out = A v on the full grid with the solver's operator (Dirichlet rows give
+ * 0); device vectors, enqueued on the library stream. */
+int pic_apply_operator(const double *v_dev, double *out_dev);
+/* Device pointers of the solver's right-hand side b and potential phi
+ * (full grid), valid until pic_finalize. */
+int pic_solver_vectors(double **b_dev, double **phi_dev);
 
 /* ---- allocation-free deposit ---- */
 

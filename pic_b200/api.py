@@ -36,8 +36,12 @@ EXPORTS = [
     "pic_sort_particles", "pic_move_all", "pic_get_par_chg", "pic_ife_solve",
     "pic_get_efield_ppr", "pic_mcc", "pic_step", "pic_get_field", "pic_set_field",
     "pic_particle_device_ptrs", "pic_kernel_launches", "pic_device_timer",
-    "pic_deposit_noalloc",
+    "pic_deposit_noalloc", "pic_set_preconditioner", "pic_set_solver", "pic_set_fcg_window",
+    "pic_cuda_stream", "pic_apply_operator", "pic_solver_vectors",
 ]
+
+# z = M(r) callback of flexible CG: (r_dev, z_dev, user) -> 0 or failure
+PRECOND_FN = C.CFUNCTYPE(C.c_int, C.c_void_p, C.c_void_p, C.c_void_p)
 
 
 class PicError(RuntimeError):
@@ -169,6 +173,12 @@ def load() -> C.CDLL:
     lib.pic_get_field.argtypes = [C.c_int32, d]
     lib.pic_set_field.argtypes = [C.c_int32, d]
     lib.pic_device_timer.argtypes = [C.c_int32, _P(C.c_double)]
+    lib.pic_set_preconditioner.argtypes = [PRECOND_FN, C.c_void_p]
+    lib.pic_set_solver.argtypes = [C.c_int32]
+    lib.pic_set_fcg_window.argtypes = [C.c_int32]
+    lib.pic_cuda_stream.argtypes = [_P(C.c_void_p)]
+    lib.pic_apply_operator.argtypes = [C.c_void_p, C.c_void_p]
+    lib.pic_solver_vectors.argtypes = [_P(C.c_void_p), _P(C.c_void_p)]
     lib.pic_deposit_noalloc.argtypes = [C.c_int32, C.c_int32, C.c_double, C.c_double, C.c_double,
                                         C.c_double, C.c_int64, C.c_void_p, C.c_void_p, C.c_void_p,
                                         C.c_void_p, C.c_double, C.c_double, C.c_double, C.c_void_p,

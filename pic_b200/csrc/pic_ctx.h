@@ -71,6 +71,16 @@ struct PcgState {
   int pad;
 };
 
+// Flexible-CG scalars, resident on the device during a solve.
+#define PIC_FCG_MAX_WINDOW 8
+struct FcgState {
+  double pq, pr, alpha, rr, rhs, tol2, best;
+  double beta[PIC_FCG_MAX_WINDOW];     // against the last `count` directions, newest first
+  double pq_hist[PIC_FCG_MAX_WINDOW];  // P_j.Q_j per ring slot
+  int iter, maxit, done, ierr, best_iter, count, stall_window;
+  unsigned int ticket;
+};
+
 struct Ctx {
   bool inited = false;
   MeshK m;
@@ -113,6 +123,17 @@ struct Ctx {
   bool ex_local = true;            // every explicit row stays inside its 3x3 neighbourhood
   size_t smem_bytes = 0;
   unsigned int *d_bar = nullptr;   // grid barrier: count, generation, error flag
+  // flexible CG with a registered preconditioner
+  pic_precond_fn precond = nullptr;
+  void *precond_user = nullptr;
+  int solver = PIC_SOLVER_JPCG;
+  double *d_z = nullptr, *d_dot = nullptr;  // preconditioned residual, dot results [2]
+  unsigned int *d_dot_ticket = nullptr;
+  FcgState *d_fcg = nullptr;
+  int fcg_window = 4;                       // FCG(m) directions kept
+  double *d_fcg_P = nullptr, *d_fcg_Q = nullptr, *d_fcg_part = nullptr;  // allocated on first use
+  int fcg_last_iters = 8;                   // iterations of the previous FCG solve (chunk sizing)
+  int64_t fcg_precond_calls = 0;
   long long pcg_spin_limit = 1ll << 24;
   unsigned int pcg_bar_extra = 0;
   int ebc_dirty = 1;

@@ -973,6 +973,216 @@ __global__ void k_phi_out(const double *__restrict__ x, const int32_t *__restric
   phi[n] = (node_type[n] > 0) ? x[n] : phi_dir[n];
 }
 
+// ---- operator and dot products used by flexible CG -------------------------
+
+__global__ void k_spmv(PcgK k, const double *__restrict__ v, double *__restrict__ out) {
+  int64_t n = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (n >= k.nn) return;
+  out[n] = row_apply(k, n, [&](int64_t m) { return v[m]; });
+}
+
+struct DotK {
+  const double *a, *b, *c, *d;
+  double *part, *out;
+  unsigned int *ticket;
+  int64_t nn;
+  int nb;
+};
+
+// Canonical a.b and c.d (c may be NULL); the last block writes out[0..1].
+__global__ void __launch_bounds__(PIC_RED_THREADS) k_dot(DotK k) {
+  double v0 = 0.0, v1 = 0.0;
+  for (int it = 0; it < PIC_RED_ITEMS; ++it) {
+    int64_t n = (int64_t)blockIdx.x * PIC_RED_CHUNK + it * PIC_RED_THREADS + threadIdx.x;
+    if (n >= k.nn) continue;
+    v0 = fma(k.a[n], k.b[n], v0);
+    if (k.c) v1 = fma(k.c[n], k.d[n], v1);
+  }
+  double v[2] = {v0, v1}, out[2];
+  block_sum_canon<2>(v, out);
+  if (threadIdx.x == 0) {
+    k.part[blockIdx.x] = out[0];
+    k.part[k.nb + blockIdx.x] = out[1];
+  }
+  if (arrive_last(k.ticket)) {
+    double tot[2];
+    final_sum_canon<2>(k.part, k.nb, tot);
+    if (threadIdx.x == 0) {
+      k.out[0] = tot[0];
+      k.out[1] = tot[1];
+      *k.ticket = 0;
+    }
+  }
+}
+
+// r = b - q on unknown nodes, 0 on Dirichlet nodes
+__global__ void k_fcg_r0(const int32_t *__restrict__ row_kind, const double *__restrict__ b,
+                         const double *__restrict__ q, double *__restrict__ r, int64_t nn) {
+  int64_t n = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (n < nn) r[n] = (row_kind[n] < 0) ? 0.0 : b[n] - q[n];
+}
+
+// ---- flexible CG, truncated FCG(m) (Notay, SIAM J. Sci. Comput. 22, 2000) --
+// One iteration = preconditioner z = M(r) (host callback, enqueued on the
+// same stream) + k_fcg_beta + k_fcg_p + k_fcg_dir + k_fcg_upd.  The new
+// direction is A-orthogonalised against the last m <= PIC_FCG_MAX_WINDOW
+// directions, kept in ring slots P[j], Q[j] = A P[j]; m = 1 is FCG(1).  The
+// scalars live in FcgState on the device; the host reads it once per chunk of
+// iterations.  Reductions use the canonical block/final sums of the PCG.
+
+struct FcgK {
+  PcgK op;        // operator; op.w = z, op.x, op.r
+  double *P, *Q;  // ring [window][nn]
+  double *part;   // [PIC_FCG_MAX_WINDOW][nb]
+  FcgState *s;
+  int slot, window;  // ring slot of the new direction, window m
+};
+
+// ring slot of the t-th previous direction (t = 1..count)
+__device__ __forceinline__ int fcg_slot(const FcgK &k, int t) { return (k.slot - t + k.window) % k.window; }
+
+// beta_t = -(z.Q_t)/(P_t.Q_t) for the last `count` directions.
+__global__ void __launch_bounds__(PIC_RED_THREADS) k_fcg_beta(FcgK k) {
+  FcgState *s = k.s;
+  if (*(volatile int *)&s->done) return;
+  const int cnt = *(volatile const int *)&s->count;
+  if (cnt == 0) return;
+  const int64_t nn = k.op.nn;
+  double v[PIC_FCG_MAX_WINDOW];
+#pragma unroll
+  for (int t = 0; t < PIC_FCG_MAX_WINDOW; ++t) v[t] = 0.0;
+  for (int it = 0; it < PIC_RED_ITEMS; ++it) {
+    int64_t n = (int64_t)blockIdx.x * PIC_RED_CHUNK + it * PIC_RED_THREADS + threadIdx.x;
+    if (n >= nn) continue;
+    const double zv = k.op.w[n];
+#pragma unroll
+    for (int t = 0; t < PIC_FCG_MAX_WINDOW; ++t)
+      if (t < cnt) v[t] = fma(zv, k.Q[(size_t)fcg_slot(k, t + 1) * nn + n], v[t]);
+  }
+  double out[PIC_FCG_MAX_WINDOW];
+  block_sum_canon<PIC_FCG_MAX_WINDOW>(v, out);
+  if (threadIdx.x == 0)
+    for (int t = 0; t < PIC_FCG_MAX_WINDOW; ++t) k.part[(size_t)t * k.op.nb + blockIdx.x] = out[t];
+  if (arrive_last(&s->ticket)) {
+    double tot[PIC_FCG_MAX_WINDOW];
+    final_sum_canon<PIC_FCG_MAX_WINDOW>(k.part, k.op.nb, tot);
+    if (threadIdx.x == 0) {
+      s->ticket = 0;
+      for (int t = 0; t < cnt; ++t) s->beta[t] = -tot[t] / s->pq_hist[fcg_slot(k, t + 1)];
+    }
+  }
+}
+
+// P_new = z + sum_t beta_t P_t on unknown nodes (0 on Dirichlet nodes).  The
+// new slot may hold the oldest direction, which each thread reads before it
+// overwrites the same element.
+__global__ void k_fcg_p(FcgK k) {
+  const FcgState *s = k.s;
+  if (*(volatile const int *)&s->done) return;
+  const int64_t n = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  const int64_t nn = k.op.nn;
+  if (n >= nn) return;
+  const int cnt = *(volatile const int *)&s->count;
+  double pv = 0.0;
+  if (k.op.row_kind[n] >= 0) {
+    pv = k.op.w[n];
+    for (int t = 0; t < cnt; ++t)
+      pv = fma(*(volatile const double *)&s->beta[t], k.P[(size_t)fcg_slot(k, t + 1) * nn + n], pv);
+  }
+  k.P[(size_t)k.slot * nn + n] = pv;
+}
+
+// Q_new = A P_new, p.q and p.r; alpha = p.r / p.q.
+__global__ void __launch_bounds__(PIC_RED_THREADS) k_fcg_dir(FcgK k) {
+  FcgState *s = k.s;
+  if (*(volatile int *)&s->done) return;
+  const int64_t nn = k.op.nn;
+  const double *pn = k.P + (size_t)k.slot * nn;
+  double *qn = k.Q + (size_t)k.slot * nn;
+  double vpq = 0.0, vpr = 0.0;
+  for (int it = 0; it < PIC_RED_ITEMS; ++it) {
+    int64_t n = (int64_t)blockIdx.x * PIC_RED_CHUNK + it * PIC_RED_THREADS + threadIdx.x;
+    if (n >= nn) continue;
+    double pv = pn[n];
+    double qv = row_apply(k.op, n, [&](int64_t m) { return pn[m]; });
+    qn[n] = qv;
+    vpq = fma(pv, qv, vpq);
+    vpr = fma(pv, k.op.r[n], vpr);
+  }
+  double v[2] = {vpq, vpr}, out[2];
+  block_sum_canon<2>(v, out);
+  if (threadIdx.x == 0) {
+    k.part[blockIdx.x] = out[0];
+    k.part[k.op.nb + blockIdx.x] = out[1];
+  }
+  if (arrive_last(&s->ticket)) {
+    double tot[2];
+    final_sum_canon<2>(k.part, k.op.nb, tot);
+    if (threadIdx.x == 0) {
+      s->ticket = 0;
+      s->pq = tot[0];
+      s->pr = tot[1];
+      s->pq_hist[k.slot] = tot[0];
+      s->count = min(s->count + 1, k.window);
+      if (!(tot[0] > 0.0) || !(tot[1] == tot[1])) {
+        s->ierr = 2;  // breakdown: M not positive on this residual
+        s->done = 1;
+      } else {
+        s->alpha = tot[1] / tot[0];
+      }
+    }
+  }
+}
+
+// x += alpha P_new, r -= alpha Q_new, r.r; convergence / cap / stall decisions.
+__global__ void __launch_bounds__(PIC_RED_THREADS) k_fcg_upd(FcgK k) {
+  FcgState *s = k.s;
+  if (*(volatile int *)&s->done) return;
+  const double alpha = *(volatile const double *)&s->alpha;
+  const int64_t nn = k.op.nn;
+  const double *pn = k.P + (size_t)k.slot * nn, *qn = k.Q + (size_t)k.slot * nn;
+  double vrr = 0.0;
+  for (int it = 0; it < PIC_RED_ITEMS; ++it) {
+    int64_t n = (int64_t)blockIdx.x * PIC_RED_CHUNK + it * PIC_RED_THREADS + threadIdx.x;
+    if (n >= nn) continue;
+    k.op.x[n] = fma(alpha, pn[n], k.op.x[n]);
+    double rv = fma(-alpha, qn[n], k.op.r[n]);
+    k.op.r[n] = rv;
+    vrr = fma(rv, rv, vrr);
+  }
+  double v[1] = {vrr}, out[1];
+  block_sum_canon<1>(v, out);
+  if (threadIdx.x == 0) k.part[blockIdx.x] = out[0];
+  if (arrive_last(&s->ticket)) {
+    double tot[1];
+    final_sum_canon<1>(k.part, k.op.nb, tot);
+    if (threadIdx.x == 0) {
+      const double rr = tot[0];
+      s->ticket = 0;
+      s->rr = rr;
+      s->iter = s->iter + 1;
+      if (!(rr == rr)) {
+        s->ierr = 4;
+        s->done = 1;
+      } else if (rr / s->rhs <= s->tol2) {
+        s->done = 1;
+      } else if (s->iter >= s->maxit) {
+        s->ierr = 1;
+        s->done = 1;
+      } else {
+        if (rr < s->best) {
+          s->best = rr;
+          s->best_iter = s->iter;
+        }
+        if (s->iter - s->best_iter > s->stall_window || rr > 1e6 * s->best) {
+          s->ierr = 3;  // stalled
+          s->done = 1;
+        }
+      }
+    }
+  }
+}
+
 __constant__ double c_ppr_reg[5][9];
 
 struct PprK {
@@ -1133,6 +1343,7 @@ static void free_all() {
   F(g.d_ex_val); F(g.d_diag); F(g.d_ppr_kind); F(g.d_ppr_ptr); F(g.d_ppr_nodes); F(g.d_ppr_rows);
   F(g.d_ppr_h); F(g.d_phi); F(g.d_rho); F(g.d_efx); F(g.d_efy); F(g.d_coef); F(g.d_b); F(g.d_x);
   F(g.d_r); F(g.d_w); F(g.d_p[0]); F(g.d_p[1]); F(g.d_q); F(g.d_part); F(g.d_pcg); F(g.d_bar);
+  F(g.d_z); F(g.d_dot); F(g.d_dot_ticket); F(g.d_fcg); F(g.d_fcg_P); F(g.d_fcg_Q); F(g.d_fcg_part);
   F(g.d_cell_count); F(g.d_cell_start); F(g.d_cell_fill); F(g.d_perm); F(g.d_perm2); F(g.d_sort_id);
   F(g.d_scan_blk); F(g.d_counters); F(g.d_hist); F(g.d_sel); F(g.d_cand); F(g.d_cand_slot);
   F(g.d_mcc_misc); F(g.d_ion_parent); F(g.d_ion_data);
@@ -1355,6 +1566,136 @@ static int run_pcg(pic_solve_stats *stats) {
   return PIC_OK;
 }
 
+static int dot2(const double *a, const double *b, const double *c, const double *d, double out[2]) {
+  DotK k{a, b, c, d, g.d_part, g.d_dot, g.d_dot_ticket, g.nn, g.red_blocks};
+  k_dot<<<g.red_blocks, PIC_RED_THREADS, 0, g.st>>>(k);
+  PIC_LAUNCHED();
+  PIC_CUDA(cudaMemcpyAsync(out, g.d_dot, 2 * sizeof(double), cudaMemcpyDeviceToHost, g.st));
+  PIC_CUDA(cudaStreamSynchronize(g.st));
+  return PIC_OK;
+}
+
+static int fcg_alloc() {
+  if (g.d_fcg_P) return PIC_OK;
+  int rc;
+  const size_t ring = (size_t)PIC_FCG_MAX_WINDOW * (size_t)g.nn;
+  if ((rc = dalloc(&g.d_fcg_P, ring))) return rc;
+  if ((rc = dalloc(&g.d_fcg_Q, ring))) return rc;
+  if ((rc = dalloc(&g.d_fcg_part, (size_t)PIC_FCG_MAX_WINDOW * g.red_blocks))) return rc;
+  return PIC_OK;
+}
+
+// Flexible CG with the registered preconditioner.  Iterations are enqueued
+// in chunks sized from the previous solve's count; kernels after convergence
+// inside a chunk return at once.  Convergence is accepted only on the true
+// residual b - A x (recomputed in FP64 with the same operator and canonical
+// dots); if the recursive residual drifted, the iteration restarts from the
+// true one with no previous directions.  Returns 0 when converged, else the
+// reason it hands over to Jacobi-PCG (the fallback codes of pic_solve_stats).
+static int run_fcg(pic_solve_stats *stats, int *fcg_iters, int *rc_out) {
+  *rc_out = PIC_OK;
+  const int64_t nn = g.nn;
+  const int nb = blocks_for(nn, 256);
+  int rc;
+  if ((rc = fcg_alloc())) { *rc_out = rc; return 1; }
+  PcgK k0 = pcg_k(0);
+  k0.w = g.d_z;
+  FcgK fk{k0, g.d_fcg_P, g.d_fcg_Q, g.d_fcg_part, g.d_fcg, 0, g.fcg_window};
+  k_pcg_x0<<<nb, 256, 0, g.st>>>(k0);
+  PIC_LAUNCHED();
+  k_spmv<<<nb, 256, 0, g.st>>>(k0, g.d_x, g.d_q);
+  PIC_LAUNCHED();
+  k_fcg_r0<<<nb, 256, 0, g.st>>>(g.d_row_kind, g.d_b, g.d_q, g.d_r, nn);
+  PIC_LAUNCHED();
+  double s2[2];
+  if ((rc = dot2(g.d_b, g.d_b, g.d_r, g.d_r, s2))) { *rc_out = rc; return 1; }
+  FcgState hs{};
+  hs.rhs = s2[0];
+  hs.rr = s2[1];
+  hs.best = s2[1];
+  hs.tol2 = g.P.pcg_tol * g.P.pcg_tol;
+  hs.maxit = std::min(g.P.pcg_maxit, 1000);
+  hs.stall_window = 50;
+  hs.count = 0;
+  auto finish = [&](int fallback) {
+    *fcg_iters = hs.iter;
+    if (stats) {
+      stats->iterations = hs.iter;
+      stats->rel_residual = hs.rhs > 0 ? std::sqrt(hs.rr / hs.rhs) : 0.0;
+      stats->ierr = 0;
+    }
+    if (!fallback) g.fcg_last_iters = std::max(hs.iter, 1);
+    return fallback;
+  };
+  if (!(hs.rhs > 0.0) || hs.rr / hs.rhs <= hs.tol2) return finish(0);
+  PIC_CUDA(cudaMemcpyAsync(g.d_fcg, &hs, sizeof hs, cudaMemcpyHostToDevice, g.st));
+  int judged = 0;
+  int64_t enq = 0;  // iterations enqueued (ring slot = enq mod m)
+  for (;;) {
+    int chunk = g.fcg_last_iters - hs.iter;
+    chunk = std::min(std::max(chunk, 2), 64);
+    for (int c = 0; c < chunk; ++c) {
+      ++g.fcg_precond_calls;
+      if (g.precond(g.d_r, g.d_z, g.precond_user) != 0) {
+        PIC_CUDA(cudaMemcpyAsync(&hs, g.d_fcg, sizeof hs, cudaMemcpyDeviceToHost, g.st));
+        PIC_CUDA(cudaStreamSynchronize(g.st));
+        return finish(5);
+      }
+      fk.slot = (int)(enq++ % g.fcg_window);
+      k_fcg_beta<<<g.red_blocks, PIC_RED_THREADS, 0, g.st>>>(fk);
+      PIC_LAUNCHED();
+      k_fcg_p<<<nb, 256, 0, g.st>>>(fk);
+      PIC_LAUNCHED();
+      k_fcg_dir<<<g.red_blocks, PIC_RED_THREADS, 0, g.st>>>(fk);
+      PIC_LAUNCHED();
+      k_fcg_upd<<<g.red_blocks, PIC_RED_THREADS, 0, g.st>>>(fk);
+      PIC_LAUNCHED();
+    }
+    PIC_CUDA(cudaMemcpyAsync(&hs, g.d_fcg, sizeof hs, cudaMemcpyDeviceToHost, g.st));
+    PIC_CUDA(cudaStreamSynchronize(g.st));
+    if (!hs.done) continue;
+    if (hs.ierr) return finish(hs.ierr);
+    // judge the converged iterate on its true residual
+    k_spmv<<<nb, 256, 0, g.st>>>(k0, g.d_x, g.d_q);
+    PIC_LAUNCHED();
+    k_fcg_r0<<<nb, 256, 0, g.st>>>(g.d_row_kind, g.d_b, g.d_q, g.d_r, nn);
+    PIC_LAUNCHED();
+    if ((rc = dot2(g.d_r, g.d_r, nullptr, nullptr, s2))) { *rc_out = rc; return 1; }
+    hs.rr = s2[0];
+    if (hs.rr / hs.rhs <= hs.tol2) return finish(0);
+    if (++judged > 3 || hs.iter >= hs.maxit) return finish(6);
+    hs.done = 0;
+    hs.count = 0;
+    PIC_CUDA(cudaMemcpyAsync(g.d_fcg, &hs, sizeof hs, cudaMemcpyHostToDevice, g.st));
+  }
+}
+
+// Solver dispatch: flexible CG with the registered preconditioner, else (or
+// after an FCG hand-over) Jacobi-PCG warm-started from the FCG iterate.
+static int run_solve(pic_solve_stats *stats) {
+  if (g.solver == PIC_SOLVER_FCG_UNET && g.precond) {
+    int fcg_iters = 0, rc = PIC_OK;
+    int fallback = run_fcg(stats, &fcg_iters, &rc);
+    if (rc) return rc;
+    k_phi_out<<<blocks_for(g.nn, 256), 256, 0, g.st>>>(g.d_x, g.d_node_type, g.d_phi_dir, g.d_phi, g.nn);
+    PIC_LAUNCHED();
+    if (!fallback) {
+      if (stats) {
+        stats->fallback = 0;
+        stats->outer = 0;
+      }
+      return PIC_OK;
+    }
+    int prc = run_pcg(stats);
+    if (stats) {
+      stats->iterations += fcg_iters;
+      stats->fallback = fallback;
+    }
+    return prc;
+  }
+  return run_pcg(stats);
+}
+
 static int run_ppr() {
   PprK k;
   k.phi = g.d_phi;
@@ -1397,6 +1738,63 @@ extern "C" {
 
 const char *pic_last_error(void) { return g_err.c_str(); }
 int64_t pic_kernel_launches(void) { return (int64_t)g_launches; }
+
+int pic_set_preconditioner(pic_precond_fn fn, void *user) {
+  g.precond = fn;
+  g.precond_user = user;
+  return PIC_OK;
+}
+
+int pic_set_solver(int32_t solver) {
+  if (solver != PIC_SOLVER_JPCG && solver != PIC_SOLVER_FCG_UNET) {
+    set_error("pic_set_solver: unknown solver");
+    return PIC_ERR_ARG;
+  }
+  g.solver = solver;
+  return PIC_OK;
+}
+
+int pic_set_fcg_window(int32_t window) {
+  if (window < 1 || window > PIC_FCG_MAX_WINDOW) {
+    set_error("pic_set_fcg_window: window must be 1..8");
+    return PIC_ERR_ARG;
+  }
+  g.fcg_window = window;
+  return PIC_OK;
+}
+
+int pic_cuda_stream(void **stream) {
+  if (!g.inited) {
+    set_error("pic_cuda_stream: library not initialised");
+    return PIC_ERR_STATE;
+  }
+  if (stream) *stream = (void *)g.st;
+  return PIC_OK;
+}
+
+int pic_apply_operator(const double *v_dev, double *out_dev) {
+  if (!g.inited) {
+    set_error("pic_apply_operator: library not initialised");
+    return PIC_ERR_STATE;
+  }
+  if (!v_dev || !out_dev) {
+    set_error("pic_apply_operator: null vector");
+    return PIC_ERR_ARG;
+  }
+  k_spmv<<<blocks_for(g.nn, 256), 256, 0, g.st>>>(pcg_k(0), v_dev, out_dev);
+  PIC_LAUNCHED();
+  return PIC_OK;
+}
+
+int pic_solver_vectors(double **b_dev, double **phi_dev) {
+  if (!g.inited) {
+    set_error("pic_solver_vectors: library not initialised");
+    return PIC_ERR_STATE;
+  }
+  if (b_dev) *b_dev = g.d_b;
+  if (phi_dev) *phi_dev = g.d_phi;
+  return PIC_OK;
+}
 
 int pic_device_timer(int32_t op, double *ms_out) {
   if (!g.inited) {
@@ -1449,6 +1847,7 @@ int pic_init(const pic_mesh_desc *mesh, const pic_params *params) {
   }
   g = Ctx();
   g.P = P;
+  g.solver = (P.solver == PIC_SOLVER_FCG_UNET) ? PIC_SOLVER_FCG_UNET : PIC_SOLVER_JPCG;
   if (g.P.sort_interval < 1) g.P.sort_interval = 1;
   MeshK &m = g.m;
   m.nnx = mesh->nnx;
@@ -1733,6 +2132,13 @@ int pic_init(const pic_mesh_desc *mesh, const pic_params *params) {
   PIC_CUDA(cudaMemset(g.d_pcg, 0, sizeof(PcgState)));
   if ((rc = dalloc(&g.d_bar, 4))) return rc;
   PIC_CUDA(cudaMemset(g.d_bar, 0, 4 * sizeof(unsigned int)));
+  if ((rc = dalloc(&g.d_z, nn))) return rc;
+  PIC_CUDA(cudaMemset(g.d_z, 0, nn * sizeof(double)));
+  if ((rc = dalloc(&g.d_dot, 2))) return rc;
+  if ((rc = dalloc(&g.d_dot_ticket, 1))) return rc;
+  PIC_CUDA(cudaMemset(g.d_dot_ticket, 0, sizeof(unsigned int)));
+  if ((rc = dalloc(&g.d_fcg, 1))) return rc;
+  PIC_CUDA(cudaMemset(g.d_fcg, 0, sizeof(FcgState)));
   {
     // persistent PCG when the device supports cooperative launch and every
     // CTA of the grid can be resident at once
@@ -1994,7 +2400,7 @@ int pic_ife_solve(double *phi_inout, double time, pic_solve_stats *stats) {
     PIC_CUDA(cudaMemcpyAsync(g.d_phi, phi_inout, g.nn * sizeof(double), cudaMemcpyHostToDevice, g.st));
   PIC_CUDA(cudaEventRecord(g.ev0, g.st));
   if ((rc = run_rhs())) return rc;
-  int src = run_pcg(stats);
+  int src = run_solve(stats);
   PIC_CUDA(cudaEventRecord(g.ev1, g.st));
   if (phi_inout)
     PIC_CUDA(cudaMemcpyAsync(phi_inout, g.d_phi, g.nn * sizeof(double), cudaMemcpyDeviceToHost, g.st));
@@ -2055,7 +2461,7 @@ int pic_step(uint64_t step, pic_step_stats *stats) {
   pic_solve_stats ss;
   std::memset(&ss, 0, sizeof ss);
   if ((rc = run_rhs())) return rc;
-  int solve_rc = run_pcg(&ss);
+  int solve_rc = run_solve(&ss);
   PIC_CUDA(cudaEventRecord(e[2], g.st));
   // 3. PPR field recovery
   if ((rc = run_ppr())) return rc;
