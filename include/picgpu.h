@@ -310,6 +310,23 @@ int pic_set_preconditioner(pic_precond_fn fn, void *user);
 int pic_set_solver(int32_t solver);
 /* Directions FCG keeps for A-orthogonalisation, 1..8 (default 4; 1 = FCG(1)). */
 int pic_set_fcg_window(int32_t window);
+/* Preconditioner of flexible CG as a composition of stages:
+ *   1. damped-Jacobi pre-smoothing        z1 = omega D^-1 r          (smoothing)
+ *   2. Galerkin coarse correction         z2 = z1 + P Ac^-1 P^T (r - A z1)
+ *   3. learned correction (the callback)  z3 = z2 + fn(r - A z2)     (learned)
+ *   4. damped-Jacobi post-smoothing       z  = z3 + omega D^-1 (r - A z3)
+ * Defaults: smoothing off, learned on, no coarse space, so registering fn
+ * alone gives M = fn. */
+int pic_set_precond_stages(int32_t smoothing, double omega, int32_t learned);
+/* Builds the coarse space of stage 2: bilinear prolongation P from a uniform
+ * coarse grid whose spacing is about min(cells)/coarse_cells nodes (a divisor
+ * of both cell counts), Ac = P^T A P from mesh's stiffness matrix, inverted
+ * on the host (at most 4500 coarse nodes).  coarse_cells = 0 removes it. */
+int pic_coarse_setup(const pic_mesh_desc *mesh, int32_t coarse_cells);
+/* z = M(r) (full != 0), or stages 1-2 only (full == 0): the classical part
+ * whose residual r - A z is the learned correction's input.  Device vectors,
+ * enqueued on the library stream. */
+int pic_precond_apply(int32_t full, const double *r_dev, double *z_dev);
 /* The library's CUDA stream (a cudaStream_t) for callers that enqueue work
  * in its order. */
 int pic_cuda_stream(void **stream);

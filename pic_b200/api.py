@@ -37,7 +37,8 @@ EXPORTS = [
     "pic_get_efield_ppr", "pic_mcc", "pic_step", "pic_get_field", "pic_set_field",
     "pic_particle_device_ptrs", "pic_kernel_launches", "pic_device_timer",
     "pic_deposit_noalloc", "pic_set_preconditioner", "pic_set_solver", "pic_set_fcg_window",
-    "pic_cuda_stream", "pic_apply_operator", "pic_solver_vectors",
+    "pic_cuda_stream", "pic_apply_operator", "pic_solver_vectors", "pic_set_precond_stages",
+    "pic_coarse_setup", "pic_precond_apply",
 ]
 
 # z = M(r) callback of flexible CG: (r_dev, z_dev, user) -> 0 or failure
@@ -179,6 +180,9 @@ def load() -> C.CDLL:
     lib.pic_cuda_stream.argtypes = [_P(C.c_void_p)]
     lib.pic_apply_operator.argtypes = [C.c_void_p, C.c_void_p]
     lib.pic_solver_vectors.argtypes = [_P(C.c_void_p), _P(C.c_void_p)]
+    lib.pic_set_precond_stages.argtypes = [C.c_int32, C.c_double, C.c_int32]
+    lib.pic_coarse_setup.argtypes = [_P(MeshDesc), C.c_int32]
+    lib.pic_precond_apply.argtypes = [C.c_int32, C.c_void_p, C.c_void_p]
     lib.pic_deposit_noalloc.argtypes = [C.c_int32, C.c_int32, C.c_double, C.c_double, C.c_double,
                                         C.c_double, C.c_int64, C.c_void_p, C.c_void_p, C.c_void_p,
                                         C.c_void_p, C.c_double, C.c_double, C.c_double, C.c_void_p,

@@ -134,6 +134,13 @@ struct Ctx {
   double *d_fcg_P = nullptr, *d_fcg_Q = nullptr, *d_fcg_part = nullptr;  // allocated on first use
   int fcg_last_iters = 8;                   // iterations of the previous FCG solve (chunk sizing)
   int64_t fcg_precond_calls = 0;
+  // composite preconditioner of FCG (precond.cu)
+  int pc_sweeps = 0;                        // damped-Jacobi pre/post smoothing on (1) or off (0)
+  double pc_omega = 2.0 / 3.0;
+  int pc_learned = 1;                       // apply the registered callback as stage 3
+  int pc_cs = 0, pc_ncx = 0, pc_ncy = 0;    // coarse spacing in nodes (0: no coarse space)
+  double *d_pc_t = nullptr, *d_pc_y = nullptr, *d_pc_tmp = nullptr;
+  double *d_pc_ainv = nullptr, *d_pc_rc = nullptr, *d_pc_ec = nullptr;
   long long pcg_spin_limit = 1ll << 24;
   unsigned int pcg_bar_extra = 0;
   int ebc_dirty = 1;
@@ -166,6 +173,10 @@ extern Ctx g;
 int launch_locate(Species &s, int64_t begin, int64_t end);
 int sort_species(int sidx);
 int mcc_run(uint64_t step, pic_mcc_stats *stats);
+int launch_spmv(const double *v, double *out);  // out = A v (solver operator)
+int coarse_setup(const pic_mesh_desc *mesh, int coarse_cells);
+int precond_apply(int full, const double *r, double *z);
+void precond_free();
 
 inline int blocks_for(int64_t n, int threads) { return (int)((n + threads - 1) / threads); }
 

@@ -1344,6 +1344,7 @@ static void free_all() {
   F(g.d_ppr_h); F(g.d_phi); F(g.d_rho); F(g.d_efx); F(g.d_efy); F(g.d_coef); F(g.d_b); F(g.d_x);
   F(g.d_r); F(g.d_w); F(g.d_p[0]); F(g.d_p[1]); F(g.d_q); F(g.d_part); F(g.d_pcg); F(g.d_bar);
   F(g.d_z); F(g.d_dot); F(g.d_dot_ticket); F(g.d_fcg); F(g.d_fcg_P); F(g.d_fcg_Q); F(g.d_fcg_part);
+  precond_free();
   F(g.d_cell_count); F(g.d_cell_start); F(g.d_cell_fill); F(g.d_perm); F(g.d_perm2); F(g.d_sort_id);
   F(g.d_scan_blk); F(g.d_counters); F(g.d_hist); F(g.d_sel); F(g.d_cand); F(g.d_cand_slot);
   F(g.d_mcc_misc); F(g.d_ion_parent); F(g.d_ion_data);
@@ -1566,6 +1567,12 @@ static int run_pcg(pic_solve_stats *stats) {
   return PIC_OK;
 }
 
+int launch_spmv(const double *v, double *out) {
+  k_spmv<<<blocks_for(g.nn, 256), 256, 0, g.st>>>(pcg_k(0), v, out);
+  PIC_LAUNCHED();
+  return PIC_OK;
+}
+
 static int dot2(const double *a, const double *b, const double *c, const double *d, double out[2]) {
   DotK k{a, b, c, d, g.d_part, g.d_dot, g.d_dot_ticket, g.nn, g.red_blocks};
   k_dot<<<g.red_blocks, PIC_RED_THREADS, 0, g.st>>>(k);
@@ -1636,7 +1643,8 @@ static int run_fcg(pic_solve_stats *stats, int *fcg_iters, int *rc_out) {
     chunk = std::min(std::max(chunk, 2), 64);
     for (int c = 0; c < chunk; ++c) {
       ++g.fcg_precond_calls;
-      if (g.precond(g.d_r, g.d_z, g.precond_user) != 0) {
+      if ((rc = precond_apply(1, g.d_r, g.d_z)) != 0) {
+        if (rc < 0) { *rc_out = rc; return 1; }
         PIC_CUDA(cudaMemcpyAsync(&hs, g.d_fcg, sizeof hs, cudaMemcpyDeviceToHost, g.st));
         PIC_CUDA(cudaStreamSynchronize(g.st));
         return finish(5);
@@ -1673,7 +1681,7 @@ static int run_fcg(pic_solve_stats *stats, int *fcg_iters, int *rc_out) {
 // Solver dispatch: flexible CG with the registered preconditioner, else (or
 // after an FCG hand-over) Jacobi-PCG warm-started from the FCG iterate.
 static int run_solve(pic_solve_stats *stats) {
-  if (g.solver == PIC_SOLVER_FCG_UNET && g.precond) {
+  if (g.solver == PIC_SOLVER_FCG_UNET && ((g.pc_learned && g.precond) || g.pc_cs > 0 || g.pc_sweeps > 0)) {
     int fcg_iters = 0, rc = PIC_OK;
     int fallback = run_fcg(stats, &fcg_iters, &rc);
     if (rc) return rc;
@@ -1761,6 +1769,46 @@ int pic_set_fcg_window(int32_t window) {
   }
   g.fcg_window = window;
   return PIC_OK;
+}
+
+int pic_set_precond_stages(int32_t smoothing, double omega, int32_t learned) {
+  if (smoothing < 0 || smoothing > 1 || !(omega > 0.0 && omega < 2.0)) {
+    set_error("pic_set_precond_stages: smoothing must be 0 or 1 and 0 < omega < 2");
+    return PIC_ERR_ARG;
+  }
+  g.pc_sweeps = smoothing;
+  g.pc_omega = omega;
+  g.pc_learned = learned ? 1 : 0;
+  return PIC_OK;
+}
+
+int pic_coarse_setup(const pic_mesh_desc *mesh, int32_t coarse_cells) {
+  if (!g.inited) {
+    set_error("pic_coarse_setup: library not initialised");
+    return PIC_ERR_STATE;
+  }
+  if (!mesh || mesh->nnx != g.m.nnx || mesh->nny != g.m.nny) {
+    set_error("pic_coarse_setup: mesh does not match the initialised one");
+    return PIC_ERR_ARG;
+  }
+  return coarse_setup(mesh, coarse_cells);
+}
+
+int pic_precond_apply(int32_t full, const double *r_dev, double *z_dev) {
+  if (!g.inited) {
+    set_error("pic_precond_apply: library not initialised");
+    return PIC_ERR_STATE;
+  }
+  if (!r_dev || !z_dev) {
+    set_error("pic_precond_apply: null vector");
+    return PIC_ERR_ARG;
+  }
+  int rc = precond_apply(full, r_dev, z_dev);
+  if (rc > 0) {
+    set_error("pic_precond_apply: the learned correction failed");
+    return PIC_ERR_STATE;
+  }
+  return rc;
 }
 
 int pic_cuda_stream(void **stream) {

@@ -1,0 +1,308 @@
+// precond.cu -- the preconditioner M(r) of flexible CG (pic_ife_solve with
+// PIC_SOLVER_FCG_UNET): a composition of
+//   1. damped-Jacobi pre-smoothing       z1 = w D^-1 r
+//   2. Galerkin coarse correction        z2 = z1 + P Ac^-1 P^T (r - A z1)
+//   3. learned correction (callback)     z3 = z2 + N(r - A z2)
+//   4. damped-Jacobi post-smoothing      z  = z3 + w D^-1 (r - A z3)
+// Each stage can be switched off.  The smoother removes the rough part of
+// the error, the coarse space (bilinear P on a uniform coarse grid of spacing
+// cs nodes, Ac = P^T A P inverted once on the host) the global part, and the
+// network what lies between -- it is trained on exactly the residuals stage 3
+// sees.  The reference solver (IFE-Solver/MY_PCG.f90) is Jacobi-PCG only:
+// none of this has a counterpart there.
+#include <cmath>
+#include <cstring>
+#include <vector>
+
+#include "pic_ctx.h"
+
+namespace pic {
+
+namespace {
+
+constexpr int PC_THREADS = 256;
+
+// z = w (r - tmp)/diag (+ z when add), 0 on Dirichlet nodes; tmp may be NULL.
+__global__ void k_pc_jacobi(const double *__restrict__ r, const double *__restrict__ tmp,
+                            const double *__restrict__ diag, const int32_t *__restrict__ row_kind, double omega,
+                            int add, double *__restrict__ z, int64_t nn) {
+  int64_t n = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (n >= nn) return;
+  if (row_kind[n] < 0) {
+    z[n] = 0.0;
+    return;
+  }
+  const double res = tmp ? r[n] - tmp[n] : r[n];
+  const double v = omega * res / diag[n];
+  z[n] = add ? z[n] + v : v;
+}
+
+// t = r - tmp on unknown nodes, 0 on Dirichlet nodes
+__global__ void k_pc_resid(const double *__restrict__ r, const double *__restrict__ tmp,
+                           const int32_t *__restrict__ row_kind, double *__restrict__ t, int64_t nn) {
+  int64_t n = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (n < nn) t[n] = (row_kind[n] < 0) ? 0.0 : r[n] - tmp[n];
+}
+
+// z += y on unknown nodes
+__global__ void k_pc_add(const double *__restrict__ y, const int32_t *__restrict__ row_kind,
+                         double *__restrict__ z, int64_t nn) {
+  int64_t n = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (n < nn && row_kind[n] >= 0) z[n] += y[n];
+}
+
+struct CoarseK {
+  int nnx, nny, cs, ncx, ncy;
+};
+
+// rc[C] = sum over the fine nodes f of C's support of P[f,C] t[f]
+// (t is 0 on Dirichlet nodes).  One block per coarse node; fixed-order
+// block reduction.
+__global__ void __launch_bounds__(PC_THREADS) k_pc_restrict(CoarseK c, const double *__restrict__ t,
+                                                             double *__restrict__ rc) {
+  const int C = blockIdx.x;
+  const int I = C / c.ncy, J = C % c.ncy;
+  const int i0 = max(0, (I - 1) * c.cs + 1), i1 = min(c.nnx - 1, (I + 1) * c.cs - 1);
+  const int j0 = max(0, (J - 1) * c.cs + 1), j1 = min(c.nny - 1, (J + 1) * c.cs - 1);
+  const int ni = i1 - i0 + 1, nj = j1 - j0 + 1;
+  const double inv = 1.0 / c.cs;
+  double s = 0.0;
+  for (int e = threadIdx.x; e < ni * nj; e += PC_THREADS) {
+    const int i = i0 + e / nj, j = j0 + e % nj;
+    const double w = (1.0 - fabs((double)(i - I * c.cs)) * inv) * (1.0 - fabs((double)(j - J * c.cs)) * inv);
+    s = fma(w, t[(int64_t)i * c.nny + j], s);
+  }
+  __shared__ double ws[PC_THREADS / 32];
+  for (int off = 16; off > 0; off >>= 1) s += __shfl_xor_sync(0xffffffffu, s, off);
+  if ((threadIdx.x & 31) == 0) ws[threadIdx.x >> 5] = s;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    double a = 0.0;
+    for (int q = 0; q < PC_THREADS / 32; ++q) a += ws[q];
+    rc[C] = a;
+  }
+}
+
+// ec = Ainv rc, one warp per row (row-major FP64 inverse)
+__global__ void k_pc_gemv(const double *__restrict__ ainv, const double *__restrict__ rc, double *__restrict__ ec,
+                          int nc) {
+  const int row = blockIdx.x * (blockDim.x / 32) + (threadIdx.x >> 5);
+  const int lane = threadIdx.x & 31;
+  if (row >= nc) return;
+  const double *a = ainv + (size_t)row * nc;
+  double s = 0.0;
+  for (int k = lane; k < nc; k += 32) s = fma(a[k], rc[k], s);
+  for (int off = 16; off > 0; off >>= 1) s += __shfl_xor_sync(0xffffffffu, s, off);
+  if (lane == 0) ec[row] = s;
+}
+
+// z += P ec on unknown nodes (bilinear from the four coarse nodes around)
+__global__ void k_pc_prolong(CoarseK c, const double *__restrict__ ec, const int32_t *__restrict__ row_kind,
+                             double *__restrict__ z, int64_t nn) {
+  int64_t n = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (n >= nn || row_kind[n] < 0) return;
+  const int i = (int)(n / c.nny), j = (int)(n % c.nny);
+  const int I = i / c.cs, J = j / c.cs;
+  const double fx = (double)(i - I * c.cs) / c.cs, fy = (double)(j - J * c.cs) / c.cs;
+  const int I1 = min(I + 1, c.ncx - 1), J1 = min(J + 1, c.ncy - 1);
+  double v = (1.0 - fx) * (1.0 - fy) * ec[I * c.ncy + J];
+  v = fma(fx * (1.0 - fy), ec[I1 * c.ncy + J], v);
+  v = fma((1.0 - fx) * fy, ec[I * c.ncy + J1], v);
+  v = fma(fx * fy, ec[I1 * c.ncy + J1], v);
+  z[n] += v;
+}
+
+template <class T>
+int pc_alloc(T **p, size_t n) {
+  PIC_CUDA(cudaMalloc((void **)p, (n ? n : 1) * sizeof(T)));
+  return PIC_OK;
+}
+
+int pc_vectors() {
+  int rc;
+  if (!g.d_pc_t && (rc = pc_alloc(&g.d_pc_t, g.nn))) return rc;
+  if (!g.d_pc_y && (rc = pc_alloc(&g.d_pc_y, g.nn))) return rc;
+  if (!g.d_pc_tmp && (rc = pc_alloc(&g.d_pc_tmp, g.nn))) return rc;
+  return PIC_OK;
+}
+
+CoarseK coarse_k() { return CoarseK{g.m.nnx, g.m.nny, g.pc_cs, g.pc_ncx, g.pc_ncy}; }
+
+// z += P Ac^-1 P^T t
+int coarse_correct(const double *t, double *z) {
+  CoarseK c = coarse_k();
+  const int nc = c.ncx * c.ncy;
+  k_pc_restrict<<<nc, PC_THREADS, 0, g.st>>>(c, t, g.d_pc_rc);
+  PIC_LAUNCHED();
+  k_pc_gemv<<<(nc + 7) / 8, 256, 0, g.st>>>(g.d_pc_ainv, g.d_pc_rc, g.d_pc_ec, nc);
+  PIC_LAUNCHED();
+  k_pc_prolong<<<blocks_for(g.nn, PC_THREADS), PC_THREADS, 0, g.st>>>(c, g.d_pc_ec, g.d_row_kind, z, g.nn);
+  PIC_LAUNCHED();
+  return PIC_OK;
+}
+
+// In-place Cholesky of a dense SPD matrix (row-major, lower factor), then
+// the inverse from it.  Returns false when a pivot is not positive.
+bool dense_spd_inverse(std::vector<double> &A, int n) {
+  std::vector<double> L(A);
+  for (int j = 0; j < n; ++j) {
+    double d = L[(size_t)j * n + j];
+    for (int k = 0; k < j; ++k) d -= L[(size_t)j * n + k] * L[(size_t)j * n + k];
+    if (!(d > 0.0)) return false;
+    d = std::sqrt(d);
+    L[(size_t)j * n + j] = d;
+    for (int i = j + 1; i < n; ++i) {
+      double s = L[(size_t)i * n + j];
+      const double *li = &L[(size_t)i * n], *lj = &L[(size_t)j * n];
+      for (int k = 0; k < j; ++k) s -= li[k] * lj[k];
+      L[(size_t)i * n + j] = s / d;
+    }
+  }
+  // inv(L) (lower), column by column
+  std::vector<double> Li((size_t)n * n, 0.0);
+  for (int j = 0; j < n; ++j) {
+    Li[(size_t)j * n + j] = 1.0 / L[(size_t)j * n + j];
+    for (int i = j + 1; i < n; ++i) {
+      double s = 0.0;
+      for (int k = j; k < i; ++k) s -= L[(size_t)i * n + k] * Li[(size_t)k * n + j];
+      Li[(size_t)i * n + j] = s / L[(size_t)i * n + i];
+    }
+  }
+  // A^-1 = inv(L)^T inv(L)
+  for (int i = 0; i < n; ++i)
+    for (int j = 0; j <= i; ++j) {
+      double s = 0.0;
+      for (int k = i; k < n; ++k) s += Li[(size_t)k * n + i] * Li[(size_t)k * n + j];
+      A[(size_t)i * n + j] = s;
+      A[(size_t)j * n + i] = s;
+    }
+  return true;
+}
+
+}  // namespace
+
+// Builds Ac = P^T A P from the mesh's CSR stiffness matrix (unknowns,
+// 1-based) and uploads its inverse.
+int coarse_setup(const pic_mesh_desc *mesh, int coarse_cells) {
+  if (g.d_pc_ainv) {
+    cudaFree(g.d_pc_ainv);
+    cudaFree(g.d_pc_rc);
+    cudaFree(g.d_pc_ec);
+    g.d_pc_ainv = g.d_pc_rc = g.d_pc_ec = nullptr;
+  }
+  g.pc_cs = 0;
+  if (coarse_cells <= 0) return PIC_OK;
+  const int ex = g.m.nnx - 1, ey = g.m.nny - 1;
+  int cs = std::max(1, std::min(ex, ey) / coarse_cells);
+  while (cs > 1 && (ex % cs || ey % cs)) --cs;
+  const int ncx = ex / cs + 1, ncy = ey / cs + 1, nc = ncx * ncy;
+  if (nc > 4500) {
+    set_error("pic_coarse_setup: coarse grid too large (at most 4500 coarse nodes)");
+    return PIC_ERR_ARG;
+  }
+  const int64_t nn = (int64_t)g.m.nnx * g.m.nny;
+  const int nu = mesh->n_unknowns;
+  std::vector<int64_t> node_of(nu);
+  for (int64_t n = 0; n < nn; ++n)
+    if (mesh->node_type[n] > 0) node_of[mesh->node_type[n] - 1] = n;
+  // P rows: up to 4 (coarse index, weight) per unknown
+  std::vector<int> pc((size_t)nu * 4);
+  std::vector<double> pw((size_t)nu * 4);
+  for (int u = 0; u < nu; ++u) {
+    const int64_t n = node_of[u];
+    const int i = (int)(n / g.m.nny), j = (int)(n % g.m.nny);
+    const int I = i / cs, J = j / cs;
+    const double fx = (double)(i - I * cs) / cs, fy = (double)(j - J * cs) / cs;
+    const int I1 = std::min(I + 1, ncx - 1), J1 = std::min(J + 1, ncy - 1);
+    const int cc[4] = {I * ncy + J, I1 * ncy + J, I * ncy + J1, I1 * ncy + J1};
+    const double ww[4] = {(1 - fx) * (1 - fy), fx * (1 - fy), (1 - fx) * fy, fx * fy};
+    for (int q = 0; q < 4; ++q) {
+      pc[4 * (size_t)u + q] = cc[q];
+      pw[4 * (size_t)u + q] = ww[q];
+    }
+  }
+  std::vector<double> Ac((size_t)nc * nc, 0.0);
+  for (int u = 0; u < nu; ++u)
+    for (int64_t e = mesh->a_srow[u] - 1; e < mesh->a_srow[u + 1] - 1; ++e) {
+      const int v = mesh->a_jcol[e] - 1;
+      const double a = mesh->a_k[e];
+      for (int p = 0; p < 4; ++p) {
+        const double wp = pw[4 * (size_t)u + p];
+        if (wp == 0.0) continue;
+        for (int q = 0; q < 4; ++q) {
+          const double wq = pw[4 * (size_t)v + q];
+          if (wq == 0.0) continue;
+          Ac[(size_t)pc[4 * (size_t)u + p] * nc + pc[4 * (size_t)v + q]] += wp * a * wq;
+        }
+      }
+    }
+  for (int C = 0; C < nc; ++C)  // coarse nodes without unknowns in their support
+    if (Ac[(size_t)C * nc + C] == 0.0) Ac[(size_t)C * nc + C] = 1.0;
+  if (!dense_spd_inverse(Ac, nc)) {
+    set_error("pic_coarse_setup: coarse operator is not positive definite");
+    return PIC_ERR_SETUP;
+  }
+  int rc;
+  if ((rc = pc_alloc(&g.d_pc_ainv, (size_t)nc * nc))) return rc;
+  if ((rc = pc_alloc(&g.d_pc_rc, nc))) return rc;
+  if ((rc = pc_alloc(&g.d_pc_ec, nc))) return rc;
+  PIC_CUDA(cudaMemcpy(g.d_pc_ainv, Ac.data(), Ac.size() * sizeof(double), cudaMemcpyHostToDevice));
+  g.pc_cs = cs;
+  g.pc_ncx = ncx;
+  g.pc_ncy = ncy;
+  return PIC_OK;
+}
+
+// z = M(r) (full != 0) or the classical part before the learned correction,
+// z2 = S r + P Ac^-1 P^T (r - A S r) (full == 0).  Returns non-zero when the
+// learned correction's callback fails.
+int precond_apply(int full, const double *r, double *z) {
+  int rc;
+  if ((rc = pc_vectors())) return rc;
+  const int nb = blocks_for(g.nn, PC_THREADS);
+  const bool smooth = g.pc_sweeps > 0, coarse = g.pc_cs > 0, learned = g.pc_learned && g.precond;
+  // 1. pre-smoothing
+  if (smooth) {
+    k_pc_jacobi<<<nb, PC_THREADS, 0, g.st>>>(r, nullptr, g.d_diag, g.d_row_kind, g.pc_omega, 0, z, g.nn);
+  } else {
+    k_pc_resid<<<nb, PC_THREADS, 0, g.st>>>(r, r, g.d_row_kind, z, g.nn);  // z = 0
+  }
+  PIC_LAUNCHED();
+  // 2. coarse correction on t = r - A z1
+  if (coarse) {
+    if (smooth) {
+      if ((rc = launch_spmv(z, g.d_pc_tmp))) return rc;
+      k_pc_resid<<<nb, PC_THREADS, 0, g.st>>>(r, g.d_pc_tmp, g.d_row_kind, g.d_pc_t, g.nn);
+      PIC_LAUNCHED();
+      if ((rc = coarse_correct(g.d_pc_t, z))) return rc;
+    } else {
+      if ((rc = coarse_correct(r, z))) return rc;
+    }
+  }
+  if (!full) return PIC_OK;
+  // 3. learned correction on t = r - A z2
+  if (learned) {
+    if ((rc = launch_spmv(z, g.d_pc_tmp))) return rc;
+    k_pc_resid<<<nb, PC_THREADS, 0, g.st>>>(r, g.d_pc_tmp, g.d_row_kind, g.d_pc_t, g.nn);
+    PIC_LAUNCHED();
+    if (g.precond(g.d_pc_t, g.d_pc_y, g.precond_user) != 0) return 1;
+    k_pc_add<<<nb, PC_THREADS, 0, g.st>>>(g.d_pc_y, g.d_row_kind, z, g.nn);
+    PIC_LAUNCHED();
+  }
+  // 4. post-smoothing
+  if (smooth && (coarse || learned)) {
+    if ((rc = launch_spmv(z, g.d_pc_tmp))) return rc;
+    k_pc_jacobi<<<nb, PC_THREADS, 0, g.st>>>(r, g.d_pc_tmp, g.d_diag, g.d_row_kind, g.pc_omega, 1, z, g.nn);
+    PIC_LAUNCHED();
+  }
+  return PIC_OK;
+}
+
+void precond_free() {
+  auto F = [](void *p) {
+    if (p) cudaFree(p);
+  };
+  F(g.d_pc_t); F(g.d_pc_y); F(g.d_pc_tmp); F(g.d_pc_ainv); F(g.d_pc_rc); F(g.d_pc_ec);
+}
+
+}  // namespace pic
