@@ -1333,6 +1333,8 @@ static bool ppr_rows(const std::vector<double> &px, const std::vector<double> &p
   return true;
 }
 
+static void fcg_graphs_free();
+
 static void free_all() {
   auto F = [](void *p) {
     if (p) cudaFree(p);
@@ -1345,6 +1347,7 @@ static void free_all() {
   F(g.d_r); F(g.d_w); F(g.d_p[0]); F(g.d_p[1]); F(g.d_q); F(g.d_part); F(g.d_pcg); F(g.d_bar);
   F(g.d_z); F(g.d_dot); F(g.d_dot_ticket); F(g.d_fcg); F(g.d_fcg_P); F(g.d_fcg_Q); F(g.d_fcg_part);
   precond_free();
+  fcg_graphs_free();
   F(g.d_cell_count); F(g.d_cell_start); F(g.d_cell_fill); F(g.d_perm); F(g.d_perm2); F(g.d_sort_id);
   F(g.d_scan_blk); F(g.d_counters); F(g.d_hist); F(g.d_sel); F(g.d_cand); F(g.d_cand_slot);
   F(g.d_mcc_misc); F(g.d_ion_parent); F(g.d_ion_data);
@@ -1582,6 +1585,43 @@ static int dot2(const double *a, const double *b, const double *c, const double 
   return PIC_OK;
 }
 
+static void fcg_graphs_free() {
+  for (auto &e : g.fcg_graph)
+    if (e) {
+      cudaGraphExecDestroy(e);
+      e = nullptr;
+    }
+  g.fcg_graph_key = 0;
+}
+
+// Captures `body` (kernel launches on g.st) into an executable graph and
+// records how many kernels it launches.
+template <class F>
+static int fcg_capture(cudaGraphExec_t *ex, long long *launches, F body) {
+  cudaGraph_t gr = nullptr;
+  const long long before = g_launches;
+  PIC_CUDA(cudaStreamBeginCapture(g.st, cudaStreamCaptureModeThreadLocal));
+  const int rc = body();
+  const cudaError_t e = cudaStreamEndCapture(g.st, &gr);
+  *launches = g_launches - before;
+  g_launches = before;
+  if (rc) {
+    if (gr) cudaGraphDestroy(gr);
+    return rc;
+  }
+  if (e != cudaSuccess) return cuda_fail(e, "cudaStreamEndCapture");
+  const cudaError_t ei = cudaGraphInstantiate(ex, gr, 0);
+  cudaGraphDestroy(gr);
+  if (ei != cudaSuccess) return cuda_fail(ei, "cudaGraphInstantiate");
+  return PIC_OK;
+}
+
+static int fcg_graph_launch(int i) {
+  PIC_CUDA(cudaGraphLaunch(g.fcg_graph[i], g.st));
+  g_launches += g.fcg_graph_launches[i];
+  return PIC_OK;
+}
+
 static int fcg_alloc() {
   if (g.d_fcg_P) return PIC_OK;
   int rc;
@@ -1636,6 +1676,22 @@ static int run_fcg(pic_solve_stats *stats, int *fcg_iters, int *rc_out) {
   };
   if (!(hs.rhs > 0.0) || hs.rr / hs.rhs <= hs.tol2) return finish(0);
   PIC_CUDA(cudaMemcpyAsync(g.d_fcg, &hs, sizeof hs, cudaMemcpyHostToDevice, g.st));
+  // stage buffers exist before any capture; graphs are rebuilt when the
+  // stage configuration or the window changed
+  if ((rc = precond_prepare())) { *rc_out = rc; return 1; }
+  const int learned = precond_learned_on();
+  const bool use_graphs = g.fcg_graphs != 0;
+  if (use_graphs) {
+    unsigned long long key = g.fcg_graph_gen;
+    key = key * 1000003ull + (unsigned long long)g.fcg_window;
+    key = key * 1000003ull + (unsigned long long)(g.pc_sweeps * 2 + learned);
+    key = key * 1000003ull + (unsigned long long)g.pc_cs;
+    key = key * 1000003ull + (unsigned long long)std::llround(g.pc_omega * 1e9);
+    if (key != g.fcg_graph_key) {
+      fcg_graphs_free();
+      g.fcg_graph_key = key;
+    }
+  }
   int judged = 0;
   int64_t enq = 0;  // iterations enqueued (ring slot = enq mod m)
   for (;;) {
@@ -1643,21 +1699,48 @@ static int run_fcg(pic_solve_stats *stats, int *fcg_iters, int *rc_out) {
     chunk = std::min(std::max(chunk, 2), 64);
     for (int c = 0; c < chunk; ++c) {
       ++g.fcg_precond_calls;
-      if ((rc = precond_apply(1, g.d_r, g.d_z)) != 0) {
-        if (rc < 0) { *rc_out = rc; return 1; }
+      const int slot = (int)(enq++ % g.fcg_window);
+      if (use_graphs) {
+        if (!g.fcg_graph[0] && (rc = fcg_capture(&g.fcg_graph[0], &g.fcg_graph_launches[0],
+                                                 [&] { return precond_stage_a(g.d_r, g.d_z, learned); }))) {
+          *rc_out = rc;
+          return 1;
+        }
+        if ((rc = fcg_graph_launch(0))) { *rc_out = rc; return 1; }
+      } else if ((rc = precond_stage_a(g.d_r, g.d_z, learned))) {
+        *rc_out = rc;
+        return 1;
+      }
+      if (learned && precond_callback()) {
         PIC_CUDA(cudaMemcpyAsync(&hs, g.d_fcg, sizeof hs, cudaMemcpyDeviceToHost, g.st));
         PIC_CUDA(cudaStreamSynchronize(g.st));
         return finish(5);
       }
-      fk.slot = (int)(enq++ % g.fcg_window);
-      k_fcg_beta<<<g.red_blocks, PIC_RED_THREADS, 0, g.st>>>(fk);
-      PIC_LAUNCHED();
-      k_fcg_p<<<nb, 256, 0, g.st>>>(fk);
-      PIC_LAUNCHED();
-      k_fcg_dir<<<g.red_blocks, PIC_RED_THREADS, 0, g.st>>>(fk);
-      PIC_LAUNCHED();
-      k_fcg_upd<<<g.red_blocks, PIC_RED_THREADS, 0, g.st>>>(fk);
-      PIC_LAUNCHED();
+      fk.slot = slot;
+      auto tail = [&] {
+        int r2;
+        if ((r2 = precond_stage_b(g.d_r, g.d_z, learned))) return r2;
+        k_fcg_beta<<<g.red_blocks, PIC_RED_THREADS, 0, g.st>>>(fk);
+        PIC_LAUNCHED();
+        k_fcg_p<<<nb, 256, 0, g.st>>>(fk);
+        PIC_LAUNCHED();
+        k_fcg_dir<<<g.red_blocks, PIC_RED_THREADS, 0, g.st>>>(fk);
+        PIC_LAUNCHED();
+        k_fcg_upd<<<g.red_blocks, PIC_RED_THREADS, 0, g.st>>>(fk);
+        PIC_LAUNCHED();
+        return PIC_OK;
+      };
+      if (use_graphs) {
+        if (!g.fcg_graph[1 + slot] &&
+            (rc = fcg_capture(&g.fcg_graph[1 + slot], &g.fcg_graph_launches[1 + slot], tail))) {
+          *rc_out = rc;
+          return 1;
+        }
+        if ((rc = fcg_graph_launch(1 + slot))) { *rc_out = rc; return 1; }
+      } else if ((rc = tail())) {
+        *rc_out = rc;
+        return 1;
+      }
     }
     PIC_CUDA(cudaMemcpyAsync(&hs, g.d_fcg, sizeof hs, cudaMemcpyDeviceToHost, g.st));
     PIC_CUDA(cudaStreamSynchronize(g.st));
@@ -2222,6 +2305,10 @@ int pic_init(const pic_mesh_desc *mesh, const pic_params *params) {
     g.pcg_spin_limit = lim ? std::max(1ll, atoll(lim)) : (1ll << 22);
     const char *extra = getenv("PIC_PCG_BARRIER_EXTRA");
     g.pcg_bar_extra = extra ? (unsigned int)std::max(0, atoi(extra)) : 0u;
+  }
+  {
+    const char *fg = getenv("PIC_FCG_GRAPHS");  // 0: enqueue FCG iterations kernel by kernel
+    g.fcg_graphs = (fg && atoi(fg) == 0) ? 0 : 1;
   }
   if ((rc = dalloc(&g.d_counters, 32))) return rc;
   PIC_CUDA(cudaMemset(g.d_counters, 0, 32 * sizeof(unsigned long long)));

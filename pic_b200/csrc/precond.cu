@@ -191,6 +191,7 @@ int coarse_setup(const pic_mesh_desc *mesh, int coarse_cells) {
     g.d_pc_ainv = g.d_pc_rc = g.d_pc_ec = nullptr;
   }
   g.pc_cs = 0;
+  ++g.fcg_graph_gen;  // captured iterations hold the old buffers
   if (coarse_cells <= 0) return PIC_OK;
   const int ex = g.m.nnx - 1, ey = g.m.nny - 1;
   int cs = std::max(1, std::min(ex, ey) / coarse_cells);
@@ -253,22 +254,19 @@ int coarse_setup(const pic_mesh_desc *mesh, int coarse_cells) {
   return PIC_OK;
 }
 
-// z = M(r) (full != 0) or the classical part before the learned correction,
-// z2 = S r + P Ac^-1 P^T (r - A S r) (full == 0).  Returns non-zero when the
-// learned correction's callback fails.
-int precond_apply(int full, const double *r, double *z) {
+// Stage A: smoothing and coarse correction into z; with `learned`, also the
+// learned stage's input t = r - A z2 into d_pc_t.
+int precond_stage_a(const double *r, double *z, int learned) {
   int rc;
   if ((rc = pc_vectors())) return rc;
   const int nb = blocks_for(g.nn, PC_THREADS);
-  const bool smooth = g.pc_sweeps > 0, coarse = g.pc_cs > 0, learned = g.pc_learned && g.precond;
-  // 1. pre-smoothing
+  const bool smooth = g.pc_sweeps > 0, coarse = g.pc_cs > 0;
   if (smooth) {
     k_pc_jacobi<<<nb, PC_THREADS, 0, g.st>>>(r, nullptr, g.d_diag, g.d_row_kind, g.pc_omega, 0, z, g.nn);
   } else {
     k_pc_resid<<<nb, PC_THREADS, 0, g.st>>>(r, r, g.d_row_kind, z, g.nn);  // z = 0
   }
   PIC_LAUNCHED();
-  // 2. coarse correction on t = r - A z1
   if (coarse) {
     if (smooth) {
       if ((rc = launch_spmv(z, g.d_pc_tmp))) return rc;
@@ -279,23 +277,49 @@ int precond_apply(int full, const double *r, double *z) {
       if ((rc = coarse_correct(r, z))) return rc;
     }
   }
-  if (!full) return PIC_OK;
-  // 3. learned correction on t = r - A z2
   if (learned) {
     if ((rc = launch_spmv(z, g.d_pc_tmp))) return rc;
     k_pc_resid<<<nb, PC_THREADS, 0, g.st>>>(r, g.d_pc_tmp, g.d_row_kind, g.d_pc_t, g.nn);
     PIC_LAUNCHED();
-    if (g.precond(g.d_pc_t, g.d_pc_y, g.precond_user) != 0) return 1;
+  }
+  return PIC_OK;
+}
+
+// Stage B: with `learned`, z += y (the callback's output in d_pc_y); then
+// post-smoothing.
+int precond_stage_b(const double *r, double *z, int learned) {
+  int rc;
+  const int nb = blocks_for(g.nn, PC_THREADS);
+  if (learned) {
     k_pc_add<<<nb, PC_THREADS, 0, g.st>>>(g.d_pc_y, g.d_row_kind, z, g.nn);
     PIC_LAUNCHED();
   }
-  // 4. post-smoothing
-  if (smooth && (coarse || learned)) {
+  if (g.pc_sweeps > 0 && (g.pc_cs > 0 || learned)) {
     if ((rc = launch_spmv(z, g.d_pc_tmp))) return rc;
     k_pc_jacobi<<<nb, PC_THREADS, 0, g.st>>>(r, g.d_pc_tmp, g.d_diag, g.d_row_kind, g.pc_omega, 1, z, g.nn);
     PIC_LAUNCHED();
   }
   return PIC_OK;
+}
+
+int precond_prepare() { return pc_vectors(); }
+
+int precond_learned_on() { return (g.pc_learned && g.precond) ? 1 : 0; }
+
+// The learned stage: y = fn(t) for the callback registered by the caller.
+// Returns 1 when it fails.
+int precond_callback() { return g.precond(g.d_pc_t, g.d_pc_y, g.precond_user) != 0 ? 1 : 0; }
+
+// z = M(r) (full != 0) or the classical part before the learned stage,
+// z2 = S r + P Ac^-1 P^T (r - A S r) (full == 0).  Returns 1 when the
+// learned stage's callback fails, a negative PIC_ERR_* on a CUDA error.
+int precond_apply(int full, const double *r, double *z) {
+  int rc;
+  const int learned = full ? precond_learned_on() : 0;
+  if ((rc = precond_stage_a(r, z, learned))) return rc;
+  if (!full) return PIC_OK;
+  if (learned && precond_callback()) return 1;
+  return precond_stage_b(r, z, learned);
 }
 
 void precond_free() {

@@ -420,3 +420,29 @@ def test_learned_preconditioner_gain_and_tolerance():
         assert st_l.iterations < st_c.iterations < st_j.iterations
     finally:
         sim.close()
+
+
+@gpu
+def test_fcg_graphs_match_eager():
+    """Captured FCG iterations (CUDA graphs) give the same solve, bit for
+    bit, as the kernel-by-kernel path."""
+    from pic_b200.simulation import Simulation
+    out = []
+    for flag in ("0", "1"):
+        os.environ["PIC_FCG_GRAPHS"] = flag
+        try:
+            sim = Simulation(deck.config("cfg1", ncx=128, ncy=128, ppc=2, pcg_tol=1e-10))
+        finally:
+            del os.environ["PIC_FCG_GRAPHS"]
+        try:
+            sim.initial_fields()
+            api.check(sim.lib.pic_set_precond_stages(1, 2.0 / 3.0, 0), "stages")
+            api.check(sim.lib.pic_coarse_setup(sim.mesh.ptr, 16), "coarse")
+            api.check(sim.lib.pic_set_fcg_window(2), "window")
+            st, phi = _solve_from(sim, np.zeros(sim.mesh.nn), api.PIC_SOLVER_FCG_UNET)
+            assert st.fallback == 0 and _true_rel_residual(sim) <= sim.cfg.pcg_tol * 1.0001
+            out.append((st.iterations, phi))
+            api.check(sim.lib.pic_set_solver(api.PIC_SOLVER_JPCG), "set")
+        finally:
+            sim.close()
+    assert out[0][0] == out[1][0] and np.array_equal(out[0][1], out[1][1])
