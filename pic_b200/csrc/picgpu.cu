@@ -1038,14 +1038,35 @@ struct FcgK {
   int slot, window;  // ring slot of the new direction, window m
 };
 
+// The FCG scalars a kernel needs, read once per block (thread 0) and shared:
+// every thread polling the same device word would queue on one L2 line.
+struct FcgScal {
+  int done, count;
+  double alpha;
+  double beta[PIC_FCG_MAX_WINDOW];
+};
+
+__device__ __forceinline__ void fcg_scalars(const FcgState *s, FcgScal *out, bool betas) {
+  if (threadIdx.x == 0) {
+    out->done = *(volatile const int *)&s->done;
+    out->count = *(volatile const int *)&s->count;
+    out->alpha = *(volatile const double *)&s->alpha;
+    if (betas)
+      for (int t = 0; t < PIC_FCG_MAX_WINDOW; ++t) out->beta[t] = *(volatile const double *)&s->beta[t];
+  }
+  __syncthreads();
+}
+
 // ring slot of the t-th previous direction (t = 1..count)
 __device__ __forceinline__ int fcg_slot(const FcgK &k, int t) { return (k.slot - t + k.window) % k.window; }
 
 // beta_t = -(z.Q_t)/(P_t.Q_t) for the last `count` directions.
 __global__ void __launch_bounds__(PIC_RED_THREADS) k_fcg_beta(FcgK k) {
   FcgState *s = k.s;
-  if (*(volatile int *)&s->done) return;
-  const int cnt = *(volatile const int *)&s->count;
+  __shared__ FcgScal sc;
+  fcg_scalars(s, &sc, false);
+  if (sc.done) return;
+  const int cnt = sc.count;
   if (cnt == 0) return;
   const int64_t nn = k.op.nn;
   double v[PIC_FCG_MAX_WINDOW];
@@ -1077,17 +1098,17 @@ __global__ void __launch_bounds__(PIC_RED_THREADS) k_fcg_beta(FcgK k) {
 // new slot may hold the oldest direction, which each thread reads before it
 // overwrites the same element.
 __global__ void k_fcg_p(FcgK k) {
-  const FcgState *s = k.s;
-  if (*(volatile const int *)&s->done) return;
+  __shared__ FcgScal sc;
+  fcg_scalars(k.s, &sc, true);
+  if (sc.done) return;
   const int64_t n = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
   const int64_t nn = k.op.nn;
   if (n >= nn) return;
-  const int cnt = *(volatile const int *)&s->count;
+  const int cnt = sc.count;
   double pv = 0.0;
   if (k.op.row_kind[n] >= 0) {
     pv = k.op.w[n];
-    for (int t = 0; t < cnt; ++t)
-      pv = fma(*(volatile const double *)&s->beta[t], k.P[(size_t)fcg_slot(k, t + 1) * nn + n], pv);
+    for (int t = 0; t < cnt; ++t) pv = fma(sc.beta[t], k.P[(size_t)fcg_slot(k, t + 1) * nn + n], pv);
   }
   k.P[(size_t)k.slot * nn + n] = pv;
 }
@@ -1095,7 +1116,9 @@ __global__ void k_fcg_p(FcgK k) {
 // Q_new = A P_new, p.q and p.r; alpha = p.r / p.q.
 __global__ void __launch_bounds__(PIC_RED_THREADS) k_fcg_dir(FcgK k) {
   FcgState *s = k.s;
-  if (*(volatile int *)&s->done) return;
+  __shared__ FcgScal sc;
+  fcg_scalars(s, &sc, false);
+  if (sc.done) return;
   const int64_t nn = k.op.nn;
   const double *pn = k.P + (size_t)k.slot * nn;
   double *qn = k.Q + (size_t)k.slot * nn;
@@ -1137,8 +1160,10 @@ __global__ void __launch_bounds__(PIC_RED_THREADS) k_fcg_dir(FcgK k) {
 // x += alpha P_new, r -= alpha Q_new, r.r; convergence / cap / stall decisions.
 __global__ void __launch_bounds__(PIC_RED_THREADS) k_fcg_upd(FcgK k) {
   FcgState *s = k.s;
-  if (*(volatile int *)&s->done) return;
-  const double alpha = *(volatile const double *)&s->alpha;
+  __shared__ FcgScal sc;
+  fcg_scalars(s, &sc, false);
+  if (sc.done) return;
+  const double alpha = sc.alpha;
   const int64_t nn = k.op.nn;
   const double *pn = k.P + (size_t)k.slot * nn, *qn = k.Q + (size_t)k.slot * nn;
   double vrr = 0.0;
