@@ -1,18 +1,24 @@
 """Benchmark of the B200 IFE-PIC step.
 
-    python bench.py [--gpus N] [--steps K] [--warmup W] [--config cfg2] [--impl ours|reference]
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--config cfg4] [--impl ours|reference]
 
 One step = one explicit IFE-PIC time step on one GPU (fused push + locate +
-deposit of all particles, RHS + Jacobi-PCG Poisson solve to the deck's
-tolerance, PPR field recovery, MCC null collisions, counting sort every
-sort_interval steps), data resident in HBM.  The metric is particle
-pushes/s; Poisson ms/step, PCG iterations/step and full-step ms ride along.
+deposit of all particles, RHS + Poisson solve to the deck's tolerance, PPR
+field recovery, MCC null collisions, counting sort every sort_interval
+steps), data resident in HBM.  The metric is particle pushes/s with the
+Poisson ms/step of the solvers side by side: the reference's Jacobi-PCG,
+flexible CG with smoothing + coarse space, and the same with the learned
+U-Net stage, all at the deck's tolerance on the same systems.
 
-The default workload is the 512x512-cell, 4-disk deck (about 52M
-particles).  With N > 1 (launched by torch.distributed.run) every rank runs
-an independent replica with its own seed ("replicas only": the reference has
-no domain decomposition), the timed region is bracketed by a barrier and the
-slowest rank's time is used.
+The default workload is the 1024x1024-cell, 8-ellipse deck (about 134M
+particles, Poisson tolerance 1e-8).  The run (1) trains the learned stage
+online on --train-steps Jacobi-PCG steps, (2) solves the same systems with
+every solver, (3) times --plain-steps steps of the plain FP64 Jacobi-PCG path,
+(4) times --steps steps of the product path (the fastest FCG variant), then
+the same through host buffers (e2e).  With N > 1 (launched by
+torch.distributed.run) every rank runs an independent replica with its own
+seed ("replicas only": the reference has no domain decomposition), the timed
+region is bracketed by a barrier and the slowest rank's time is used.
 
 --impl reference times the CPU restatement of the reference's step
 (oracle/liboracle.so, the reference being Fortran with no compiler on the
@@ -135,16 +141,20 @@ def _peaks():
         return None
 
 
-def cpu_baseline(cfg_name: str, sample_particles: int, steps: int, seed_offset: int = 0):
+def cpu_baseline(cfg_name: str, sample_particles: int, steps: int, pcg_iters: int | None = None,
+                 pcg_cap: int = 200):
     """Times the oracle (C restatement of the reference step, one host thread)
     on a bounded sample: push+deposit of `sample_particles` particles per
     species for `steps` steps, extrapolated to the full particle count, plus
-    RHS + Jacobi-PCG + PPR on the full mesh (warm started).  Returns
-    (pushes/s, description)."""
+    RHS + Jacobi-PCG + PPR on the full mesh.  The PCG runs at most `pcg_cap`
+    iterations per step and its time is scaled to `pcg_iters` iterations (the
+    count the reference's PCG needs for the step: the GPU Jacobi-PCG's, which
+    runs the same algorithm, or one full oracle solve when None).  Returns
+    (pushes/s, description, seconds per step)."""
     sys.path.insert(0, os.path.join(ROOT, "tests"))
     import oracle_bind as ob
     from pic_b200 import deck
-    cfg = deck.config(cfg_name, seed=deck.config(cfg_name).seed + seed_offset)
+    cfg = deck.config(cfg_name)
     mesh = deck.Mesh(cfg)
     sp, _ = deck.species_params(cfg)
     sc = cfg.scales
@@ -157,13 +167,14 @@ def cpu_baseline(cfg_name: str, sample_particles: int, steps: int, seed_offset: 
         loc = np.array([ob.load().or_locate(mesh.ptr, a, b) for a, b in zip(x[:k], y[:k])], np.int32)
         parts.append({"x": x[:k].copy(), "y": y[:k].copy(), "vx": vx[:k].copy(), "vy": vy[:k].copy(),
                       "vz": vz[:k].copy(), "loc": loc})
+        del x, y, vx, vy, vz
     sample_n = sum(p["x"].size for p in parts)
     phi = mesh.array("phi_dirichlet")
     efx = np.zeros(nn)
     efy = np.zeros(nn)
     coef = np.zeros(5 * nn)
-    t_part = 0.0
-    t_field = 0.0
+    t_part = t_field = 0.0
+    note = ""
     for step in range(steps):
         t0 = time.perf_counter()
         qs, es, wq = [], [], []
@@ -174,37 +185,42 @@ def cpu_baseline(cfg_name: str, sample_particles: int, steps: int, seed_offset: 
             qs.append(q)
             es.append(e)
             wq.append(sp[s][2] * sp[s][0])
-        t1 = time.perf_counter()
+        t_part += time.perf_counter() - t0
         # full-size field phase on the sampled charge scaled to the full count
+        t1 = time.perf_counter()
         rho, _, _ = ob.normalize(mesh.ptr, qs, es, wq, sc["L_ref"], cfg.n0, nn)
         rho *= full_n / max(sample_n, 1)
         b = ob.rhs(mesh.ptr, rho, nn)
-        phi, st = ob.pcg(mesh.ptr, b, phi, cfg.pcg_tol, cfg.pcg_maxit)
+        t_rhs = time.perf_counter() - t1
+        if pcg_iters is None:  # one full solve gives the iteration count (not timed)
+            tf = time.perf_counter()
+            _, stf = ob.pcg(mesh.ptr, b, phi, cfg.pcg_tol, cfg.pcg_maxit)
+            pcg_iters = max(1, stf["iterations"])
+            note = f"; count from one full oracle solve ({time.perf_counter() - tf:.1f} s)"
+        tp = time.perf_counter()
+        phi, st = ob.pcg(mesh.ptr, b, phi, cfg.pcg_tol, min(pcg_cap, cfg.pcg_maxit))
+        t_pcg = (time.perf_counter() - tp) / max(1, st["iterations"]) * pcg_iters
+        t3 = time.perf_counter()
         c, efx, efy = ob.ppr(mesh.ptr, phi, nn)
         coef = np.ascontiguousarray(c.ravel())
-        t2 = time.perf_counter()
-        t_part += t1 - t0
-        t_field += t2 - t1
+        t_field += t_rhs + t_pcg + (time.perf_counter() - t3)
     per_step = t_part / steps * (full_n / sample_n) + t_field / steps
     mesh.close()
-    desc = (f"{cfg.name}: push+deposit of {sample_n} of {full_n} particles for {steps} steps, "
-            f"extrapolated by particle count; RHS+Jacobi-PCG+PPR on the full {cfg.ncx}x{cfg.ncy} mesh")
+    desc = (f"{cfg.name}: push+deposit of {sample_n} of {full_n} particles for {steps} step(s), extrapolated "
+            f"by particle count; RHS+Jacobi-PCG+PPR on the full {cfg.ncx}x{cfg.ncy} mesh, the PCG timed over "
+            f"<= {pcg_cap} iterations and scaled to the step's {pcg_iters} iterations{note}")
     return full_n / per_step, desc, per_step
 
 
 def run_reference(args, dist, rank, ws):
     if rank != 0:
         return 0
-    value, desc, per_step = None, None, None
-    vals = []
-    # warm-up + timed steps of the CPU restatement, each step a bounded sample
-    v, desc, per_step = cpu_baseline(args.config, args.cpu_sample, max(1, args.warmup))
-    t0 = time.perf_counter()
-    tot_steps = max(1, args.steps)
-    v, desc, per_step = cpu_baseline(args.config, args.cpu_sample, tot_steps)
+    cpu_baseline(args.config, min(args.cpu_sample, 20000), 1, pcg_iters=1, pcg_cap=1)  # warm-up (caches)
+    steps = max(1, args.steps)
+    v, desc, per_step = cpu_baseline(args.config, args.cpu_sample, min(steps, 2))
     line = {
         "impl": "reference", "metric": METRIC, "value": v, "unit": "particle pushes/s",
-        "n_gpus": args.gpus, "steps": tot_steps, "warmup": args.warmup,
+        "n_gpus": args.gpus, "steps": steps, "warmup": args.warmup,
         "ms_per_step": per_step * 1e3, "higher_is_better": True, "scaling": "weak",
         "vs_baseline": None, "dtype": "f64", "data": "synthetic",
         "config": {"workload": args.config},
@@ -217,9 +233,47 @@ def run_reference(args, dist, rank, ws):
     return 0
 
 
+def _timed_steps(sim, lib, api, n):
+    """n steps timed on the library stream; returns (ms, [StepStats])."""
+    stats = []
+    api.check(lib.pic_device_timer(0, None), "timer")
+    for _ in range(n):
+        stats.append(sim.step())
+    ms = C.c_double()
+    api.check(lib.pic_device_timer(1, C.byref(ms)), "timer")
+    return ms.value, stats
+
+
+def _poisson_compare(sim, lib, api, variants, repeats=3):
+    """Each variant solves the same systems: the step's push + deposit, then
+    the Poisson solve from the previous phi, `repeats` times (device timer).
+    variants: name -> callable that selects the solver."""
+    phi_prev = sim.field("phi")
+    for s in range(2):
+        sim.move_all(s)
+    sim.get_par_chg()
+    out = {}
+    for name, select in variants.items():
+        select()
+        ms, its, fb = [], [], []
+        for _ in range(repeats):
+            sim.set_field("phi", phi_prev)
+            st = api.SolveStats()
+            api.check(lib.pic_device_timer(0, None), "timer")
+            api.check(lib.pic_ife_solve(None, 0.0, C.byref(st)), "solve")
+            t = C.c_double()
+            api.check(lib.pic_device_timer(1, C.byref(t)), "timer")
+            ms.append(t.value)
+            its.append(st.iterations)
+            fb.append(st.fallback)
+        out[name] = {"ms": statistics.median(ms), "iterations": statistics.median(its),
+                     "fallback": max(fb)}
+    return out
+
+
 def run_ours(args, dist, rank, ws):
     import torch
-    from pic_b200 import api, build, deck
+    from pic_b200 import api, build, deck, unet
     from pic_b200.simulation import Simulation
 
     build.build()
@@ -233,25 +287,58 @@ def run_ours(args, dist, rank, ws):
     lib = sim.lib
     st0 = sim.initial_fields()
     setup_s = time.perf_counter() - t_setup
+    # ---- online training of the learned stage on Jacobi-PCG warm-up steps
+    lp = None
+    t_train = time.perf_counter()
+    if args.train_steps > 0:
+        lp = unet.LearnedPreconditioner(sim, seed=rank, crop=128, batch=4, lr=2e-3, window=4)
+        sim.set_solver("jpcg")
+        for _ in range(args.train_steps):
+            lp.before_step()
+            sim.step()
+            lp.after_step(train_iters=8)
+    train_s = time.perf_counter() - t_train
+
+    def sel_jpcg():
+        sim.set_solver("jpcg")
+
+    def sel_fcg():
+        sim.set_solver("fcg", coarse_cells=32, window=1)
+
+    def sel_learned():
+        sim.set_solver("fcg", coarse_cells=32, window=4)
+        lp.set_learned(True)
+
+    variants = {"jacobi_pcg": sel_jpcg, "fcg_smooth_coarse": sel_fcg}
+    if lp is not None:
+        variants["fcg_smooth_coarse_learned"] = sel_learned
+    poisson = _poisson_compare(sim, lib, api, variants)
+    # product path: the fastest FCG variant that converged without falling back
+    fcg_names = [k for k in variants if k != "jacobi_pcg" and poisson[k]["fallback"] == 0]
+    best = min(fcg_names, key=lambda k: poisson[k]["ms"]) if fcg_names else "jacobi_pcg"
+    # ---- the plain FP64 GPU path (the reference's algorithms, Jacobi-PCG)
+    sel_jpcg()
+    sim.step()
+    _barrier(dist)
+    ms_plain, st_plain = _timed_steps(sim, lib, api, max(1, args.plain_steps))
+    ms_plain_max = _max_over_ranks(dist, ms_plain)
+    # ---- product path, device-resident timed region
+    variants[best]()
+    if lp is not None and best != "fcg_smooth_coarse_learned":
+        lp.set_learned(False)
     for _ in range(args.warmup):
         sim.step()
-    # ---- device-resident timed region
     _barrier(dist)
     if torch.cuda.is_available():
         torch.cuda.synchronize()
     launches0 = lib.pic_kernel_launches()
-    stats = []
     with ClockSampler(dev) as clk:
-        api.check(lib.pic_device_timer(0, None), "timer")
-        for _ in range(args.steps):
-            stats.append(sim.step())
-        ms = C.c_double()
-        api.check(lib.pic_device_timer(1, C.byref(ms)), "timer")
+        ms_total, stats = _timed_steps(sim, lib, api, args.steps)
     launches = lib.pic_kernel_launches() - launches0
     if torch.cuda.is_available():
         torch.cuda.synchronize()
     _barrier(dist)
-    ms_total = _max_over_ranks(dist, ms.value)
+    ms_total = _max_over_ranks(dist, ms_total)
     pushed = _sum_over_ranks(dist, float(sum(s.pushed for s in stats)))
     value = pushed / (ms_total / 1e3)
     # ---- end to end through the C-ABI with host buffers (drop-in use)
@@ -286,25 +373,36 @@ def run_ours(args, dist, rank, ws):
         peak, peak_src = 6650.0, "fallback"
     solve_ms = [s.ms_solve for s in stats]
     its = [s.solve.iterations for s in stats]
+    ms_step = ms_total / args.steps
+    plain_step = ms_plain_max / len(st_plain)
     line = {
         "metric": METRIC, "value": value, "unit": "particle pushes/s", "n_gpus": ws,
-        "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms_total / args.steps,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms_step,
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
         "data": "synthetic (seeded uniform Maxwellian plasma, seeded objects)",
         "config": {"workload": cfg.name, "cells": [cfg.ncx, cfg.ncy],
                    "particles": int(stats[0].pushed), "objects": len(cfg.objects),
-                   "precision": "fp64", "solver": "jacobi-pcg", "pcg_tol": cfg.pcg_tol,
+                   "precision": "fp64", "solver": best, "pcg_tol": cfg.pcg_tol,
                    "sort_interval": cfg.sort_interval, "mcc": bool(cfg.mcc),
                    "parallelism": f"replicas x{ws}",
                    "l2": "inputs larger than L2 (particle SoA %.1f GB)" % (push_n * 48 / 1e9)},
         "poisson_ms_per_step": sum(solve_ms) / len(solve_ms),
-        "pcg_iterations_per_step": sum(its) / len(its),
+        "poisson_iterations_per_step": sum(its) / len(its),
+        "poisson_solvers_same_systems": poisson,
+        "plain_fp64_jacobi_pcg_path": {
+            "ms_per_step": plain_step, "steps": len(st_plain),
+            "poisson_ms_per_step": sum(s.ms_solve for s in st_plain) / len(st_plain),
+            "pcg_iterations_per_step": sum(s.solve.iterations for s in st_plain) / len(st_plain),
+            "speedup_of_product_path": plain_step / ms_step},
         "push_ms_per_step": push_ms,
         "ppr_ms_per_step": sum(s.ms_ppr for s in stats) / len(stats),
         "mcc_ms_per_step": sum(s.ms_mcc for s in stats) / len(stats),
         "sort_ms_per_step": sum(s.ms_sort for s in stats) / len(stats),
         "initial_pcg_iterations": st0.iterations,
         "setup_s": setup_s,
+        "learned_training": None if lp is None else {
+            "warmup_steps": args.train_steps, "adam_steps": len(lp.losses), "seconds": train_s,
+            "loss_first": lp.losses[0], "loss_last": lp.losses[-1]},
         "roofline": {"kernel": "k_push (fused push+locate+deposit)", "bound": "hbm",
                      "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
                      "peak_source": peak_src, "bytes_per_particle": FP64_PUSH_BYTES,
@@ -315,7 +413,8 @@ def run_ours(args, dist, rank, ws):
         "clocks": clk.summary(),
     }
     if rank == 0 and ws == 1 and not args.no_cpu_baseline:
-        v, desc, _ = cpu_baseline(args.config, args.cpu_sample, 2)
+        jp = poisson["jacobi_pcg"]["iterations"]
+        v, desc, _ = cpu_baseline(args.config, args.cpu_sample, 1, pcg_iters=int(jp))
         line["cpu_baseline"] = {"value": v, "unit": "particle pushes/s", "cores": 1, "kind": "port",
                                 "sample": desc}
     sim.close()
@@ -329,7 +428,11 @@ def main():
     ap.add_argument("--gpus", type=int, default=1)
     ap.add_argument("--steps", type=int, default=20)
     ap.add_argument("--warmup", type=int, default=3)
-    ap.add_argument("--config", default="cfg2")
+    ap.add_argument("--config", default="cfg4")
+    ap.add_argument("--train-steps", type=int, default=30,
+                    help="Jacobi-PCG warm-up steps that train the learned stage (0: no learned stage)")
+    ap.add_argument("--plain-steps", type=int, default=5,
+                    help="steps of the plain FP64 Jacobi-PCG path timed for comparison")
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--cpu-sample", type=int, default=400000)
     ap.add_argument("--no-cpu-baseline", action="store_true")

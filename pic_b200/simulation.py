@@ -128,6 +128,23 @@ class Simulation:
         api.check(self.lib.pic_step(self.step_index, C.byref(st)), "pic_step")
         return st
 
+    # ---- Poisson solver ---------------------------------------------------
+    def set_solver(self, kind: str = "jpcg", coarse_cells: int = 32, window: int = 1,
+                   omega: float = 2.0 / 3.0):
+        """'jpcg': the reference's Jacobi-PCG.  'fcg': flexible CG with damped
+        Jacobi smoothing and a Galerkin coarse space (no learned stage).
+        'fcg-learned' is set up by unet.LearnedPreconditioner on top of 'fcg'."""
+        lib = self.lib
+        if kind == "jpcg":
+            api.check(lib.pic_set_solver(api.PIC_SOLVER_JPCG), "pic_set_solver")
+            return
+        if kind != "fcg":
+            raise ValueError(kind)
+        api.check(lib.pic_set_precond_stages(1, omega, 0), "pic_set_precond_stages")
+        api.check(lib.pic_coarse_setup(self.mesh.ptr, coarse_cells), "pic_coarse_setup")
+        api.check(lib.pic_set_fcg_window(window), "pic_set_fcg_window")
+        api.check(lib.pic_set_solver(api.PIC_SOLVER_FCG_UNET), "pic_set_solver")
+
     # ---- fields ---------------------------------------------------------
     FIELDS = {"rho": 0, "phi": 1, "efx": 2, "efy": 3, "rho_e": 4, "rho_i": 5, "ek_e": 8,
               "ek_i": 9, "c2": 12, "c3": 13, "c4": 14, "c5": 15, "c6": 16, "b": 20}
