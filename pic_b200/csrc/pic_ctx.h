@@ -42,6 +42,9 @@ struct MeshK {
 struct ObjK {
   int n;
   pic_object o[PIC_MAX_OBJECTS];
+  // per object, computed on the host: cos/sin of the ellipse angle (the
+  // host's libm, as the oracle) and the half-width of a box that holds it
+  double ca[PIC_MAX_OBJECTS], sa[PIC_MAX_OBJECTS], half[PIC_MAX_OBJECTS];
 };
 
 struct Species {

@@ -174,7 +174,9 @@ __device__ __forceinline__ bool absorbed_by_object(double x, double y) {
     } else if (o.shape == PIC_SHAPE_BOX) {
       if (x > o.cx && x < o.a && y > o.cy && y < o.b) return true;
     } else if (o.shape == PIC_SHAPE_ELLIPSE) {
-      double c = cos(o.angle), s = sin(o.angle);
+      // outside the box of half-width max(a, b): outside the ellipse
+      if (fabs(x - o.cx) > c_obj.half[k] || fabs(y - o.cy) > c_obj.half[k]) continue;
+      const double c = c_obj.ca[k], s = c_obj.sa[k];
       double u = (x - o.cx) * c + (y - o.cy) * s;
       double v = -(x - o.cx) * s + (y - o.cy) * c;
       if ((u * u) / (o.a * o.a) + (v * v) / (o.b * o.b) < 1.0) return true;
@@ -2050,7 +2052,12 @@ int pic_init(const pic_mesh_desc *mesh, const pic_params *params) {
   ObjK ob;
   std::memset(&ob, 0, sizeof ob);
   ob.n = mesh->n_objects;
-  for (int k = 0; k < ob.n; ++k) ob.o[k] = mesh->objects[k];
+  for (int k = 0; k < ob.n; ++k) {
+    ob.o[k] = mesh->objects[k];
+    ob.ca[k] = std::cos(ob.o[k].angle);
+    ob.sa[k] = std::sin(ob.o[k].angle);
+    ob.half[k] = std::max(std::fabs(ob.o[k].a), std::fabs(ob.o[k].b)) * (1.0 + 1e-9);
+  }
   PIC_CUDA(cudaMemcpyToSymbol(c_obj, &ob, sizeof ob));
 
   // validate every index table before it reaches a kernel

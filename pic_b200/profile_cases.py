@@ -1,0 +1,88 @@
+"""Small, self-contained workloads for profiling one part of the step under
+ncu (each runs a few launches of its kernels and exits):
+
+    python -m pic_b200.profile_cases step  <deck> <ppc> <steps> [jpcg|fcg]
+    python -m pic_b200.profile_cases solve <cells> [jpcg|fcg] [repeats]
+    python -m pic_b200.profile_cases unet  <nodes> [repeats]
+
+step:  the deck at <ppc> particles per cell and species, <steps> steps.
+solve: the 8-ellipse deck at <cells>^2 without particles, a seeded random
+       charge density, Poisson solves from phi = 0.
+unet:  forward passes of the learned stage's network on a <nodes>^2 grid.
+Each prints one line with its own CUDA-event time.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import sys
+
+import numpy as np
+
+
+def _step(deck_name, ppc, steps, solver="fcg"):
+    import torch
+    from . import deck
+    from .simulation import Simulation
+    cfg = deck.config(deck_name, ppc=int(ppc))
+    sim = Simulation(cfg)
+    sim.initial_fields()
+    if solver != "jpcg":
+        sim.set_solver("fcg")
+    sim.step()
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record()
+    for _ in range(int(steps)):
+        sim.step()
+    e1.record()
+    torch.cuda.synchronize()
+    print(f"step {cfg.name} ppc={ppc} solver={solver}: {e0.elapsed_time(e1) / int(steps):.3f} ms/step")
+    sim.close()
+
+
+def _solve(cells, solver="fcg", repeats=3):
+    import torch
+    from . import api, deck
+    from .simulation import Simulation
+    n = int(cells)
+    cfg = deck.config("cfg4", ncx=n, ncy=n, ppc=1)
+    sim = Simulation(cfg, load=False)
+    sim.set_field("rho", np.random.default_rng(0).standard_normal(sim.mesh.nn))
+    sim.set_solver(solver)
+    out = []
+    for _ in range(int(repeats)):
+        sim.set_field("phi", np.zeros(sim.mesh.nn))
+        st = api.SolveStats()
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        api.check(sim.lib.pic_ife_solve(None, 0.0, C.byref(st)), "pic_ife_solve")
+        e1.record()
+        torch.cuda.synchronize()
+        out.append((st.iterations, round(e0.elapsed_time(e1), 3)))
+    print(f"solve {n}^2 {solver}: (iterations, ms) {out}")
+    sim.close()
+
+
+def _unet(nodes, repeats=10):
+    import torch
+    from . import unet
+    n = int(nodes)
+    net = unet.UNet(seed=0)
+    net._ensure(1, n, n)
+    torch.cuda.synchronize()
+    for _ in range(2):
+        net.forward()
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record()
+    for _ in range(int(repeats)):
+        net.forward()
+    e1.record()
+    torch.cuda.synchronize()
+    print(f"unet forward {n}x{n}: {e0.elapsed_time(e1) / int(repeats):.3f} ms")
+
+
+if __name__ == "__main__":
+    case, rest = sys.argv[1], sys.argv[2:]
+    {"step": _step, "solve": _solve, "unet": _unet}[case](*rest)
