@@ -142,12 +142,12 @@ struct Ctx {
   double pc_omega = 2.0 / 3.0;
   int pc_learned = 1;                       // apply the registered callback as stage 3
   int pc_cs = 0, pc_ncx = 0, pc_ncy = 0;    // coarse spacing in nodes (0: no coarse space)
-  double *d_pc_t = nullptr, *d_pc_y = nullptr, *d_pc_tmp = nullptr;
+  double *d_pc_t = nullptr, *d_pc_y = nullptr, *d_pc_za = nullptr, *d_pc_dinv = nullptr;
   double *d_pc_ainv = nullptr, *d_pc_rc = nullptr, *d_pc_ec = nullptr;
   // CUDA graphs of one FCG iteration: [0] stage A, [1 + slot] stage B + FCG
   // kernels of ring slot `slot`; rebuilt when the configuration key changes
-  cudaGraphExec_t fcg_graph[1 + PIC_FCG_MAX_WINDOW] = {};
-  long long fcg_graph_launches[1 + PIC_FCG_MAX_WINDOW] = {};
+  cudaGraphExec_t fcg_graph[2 + PIC_FCG_MAX_WINDOW] = {};
+  long long fcg_graph_launches[2 + PIC_FCG_MAX_WINDOW] = {};
   unsigned long long fcg_graph_key = 0, fcg_graph_gen = 1;
   int fcg_graphs = 1;                       // capture iterations (PIC_FCG_GRAPHS=0 turns it off)
   long long pcg_spin_limit = 1ll << 24;
@@ -185,8 +185,7 @@ int mcc_run(uint64_t step, pic_mcc_stats *stats);
 int launch_spmv(const double *v, double *out);  // out = A v (solver operator)
 int coarse_setup(const pic_mesh_desc *mesh, int coarse_cells);
 int precond_apply(int full, const double *r, double *z);
-int precond_stage_a(const double *r, double *z, int learned);
-int precond_stage_b(const double *r, double *z, int learned);
+int coarse_correct(const double *t, double *z, int assign);
 int precond_learned_on();
 int precond_prepare();
 int precond_callback();

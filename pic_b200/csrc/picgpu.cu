@@ -198,7 +198,7 @@ __device__ __forceinline__ long long seg_sum(long long v, int lane, int seg_end)
 
 // One particle per thread: gather E (old element), leapfrog push, wall/object
 // absorption, locate, fixed-point deposit of weight and weight*energy.
-__global__ void __launch_bounds__(256) k_push(MeshK m, FieldK f, PushK prm, SpK s) {
+__global__ void __launch_bounds__(256, 4) k_push(MeshK m, FieldK f, PushK prm, SpK s) {
   int64_t p = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
   int lane = threadIdx.x & 31;
   int key = -1;
@@ -1025,19 +1025,22 @@ __global__ void k_fcg_r0(const int32_t *__restrict__ row_kind, const double *__r
 }
 
 // ---- flexible CG, truncated FCG(m) (Notay, SIAM J. Sci. Comput. 22, 2000) --
-// One iteration = preconditioner z = M(r) (host callback, enqueued on the
-// same stream) + k_fcg_beta + k_fcg_p + k_fcg_dir + k_fcg_upd.  The new
-// direction is A-orthogonalised against the last m <= PIC_FCG_MAX_WINDOW
-// directions, kept in ring slots P[j], Q[j] = A P[j]; m = 1 is FCG(1).  The
-// scalars live in FcgState on the device; the host reads it once per chunk of
-// iterations.  Reductions use the canonical block/final sums of the PCG.
+// One iteration = preconditioner stage A (pre-smoothing, coarse correction),
+// the learned stage (host callback, enqueued on the same stream), then
+// k_fcg_post (post-smoothing + the A-orthogonalisation dots), k_fcg_dir (new
+// direction + SpMV + p.q, p.r) and k_fcg_upd.  The new direction is
+// A-orthogonalised against the last m <= PIC_FCG_MAX_WINDOW directions, kept
+// in a ring of m + 1 slots P[j], Q[j] = A P[j] (one more than m, so the slot
+// being written is never read as an old direction); m = 1 is FCG(1).  The
+// scalars live in FcgState on the device; the host reads it once per chunk
+// of iterations.  Reductions use the canonical block/final sums of the PCG.
 
 struct FcgK {
-  PcgK op;        // operator; op.w = z, op.x, op.r
-  double *P, *Q;  // ring [window][nn]
+  PcgK op;        // operator; op.w = z (final preconditioned residual), op.x, op.r
+  double *P, *Q;  // ring [window + 1][nn]
   double *part;   // [PIC_FCG_MAX_WINDOW][nb]
-  FcgState *s;
-  int slot, window;  // ring slot of the new direction, window m
+  FcgState *s;    // NULL: no FCG bookkeeping (a bare preconditioner application)
+  int slot, ring, window;  // ring slot of the new direction, ring size m + 1, window m
 };
 
 // The FCG scalars a kernel needs, read once per block (thread 0) and shared:
@@ -1050,87 +1053,122 @@ struct FcgScal {
 
 __device__ __forceinline__ void fcg_scalars(const FcgState *s, FcgScal *out, bool betas) {
   if (threadIdx.x == 0) {
-    out->done = *(volatile const int *)&s->done;
-    out->count = *(volatile const int *)&s->count;
-    out->alpha = *(volatile const double *)&s->alpha;
-    if (betas)
-      for (int t = 0; t < PIC_FCG_MAX_WINDOW; ++t) out->beta[t] = *(volatile const double *)&s->beta[t];
+    if (s) {
+      out->done = *(volatile const int *)&s->done;
+      out->count = *(volatile const int *)&s->count;
+      out->alpha = *(volatile const double *)&s->alpha;
+      if (betas)
+        for (int t = 0; t < PIC_FCG_MAX_WINDOW; ++t) out->beta[t] = *(volatile const double *)&s->beta[t];
+    } else {
+      out->done = 0;
+      out->count = 0;
+      out->alpha = 0.0;
+    }
   }
   __syncthreads();
 }
 
 // ring slot of the t-th previous direction (t = 1..count)
-__device__ __forceinline__ int fcg_slot(const FcgK &k, int t) { return (k.slot - t + k.window) % k.window; }
+__device__ __forceinline__ int fcg_slot(const FcgK &k, int t) { return (k.slot - t + k.ring) % k.ring; }
 
-// beta_t = -(z.Q_t)/(P_t.Q_t) for the last `count` directions.
-__global__ void __launch_bounds__(PIC_RED_THREADS) k_fcg_beta(FcgK k) {
+// Pre-smoothing: zA = w D^-1 r and t = r - A zA, the product formed from
+// r at the neighbours (no intermediate vector).  dinv = 1/diag (1 on
+// Dirichlet nodes, where r is 0).
+__global__ void k_pc_pre(PcgK k, const double *__restrict__ r, const double *__restrict__ dinv, double omega,
+                         double *__restrict__ zA, double *__restrict__ t) {
+  int64_t n = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (n >= k.nn) return;
+  if (k.row_kind[n] < 0) {
+    zA[n] = 0.0;
+    t[n] = 0.0;
+    return;
+  }
+  auto z1 = [&](int64_t m) { return (omega * r[m]) * dinv[m]; };
+  zA[n] = z1(n);
+  t[n] = r[n] - row_apply(k, n, z1);
+}
+
+// t = r - A zA (the learned stage's input)
+__global__ void k_pc_mid(PcgK k, const double *__restrict__ r, const double *__restrict__ zA,
+                         double *__restrict__ t) {
+  int64_t n = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (n >= k.nn) return;
+  t[n] = (k.row_kind[n] < 0) ? 0.0 : r[n] - row_apply(k, n, [&](int64_t m) { return zA[m]; });
+}
+
+// Post-smoothing of z3 = zA (+ y): zF = z3 + w D^-1 (r - A z3) (zF = z3 when
+// smooth == 0), then, inside FCG, beta_t = -(zF.Q_t)/(P_t.Q_t) for the last
+// `count` directions.
+__global__ void __launch_bounds__(PIC_RED_THREADS) k_fcg_post(FcgK k, const double *__restrict__ r,
+                                                              const double *__restrict__ zA,
+                                                              const double *__restrict__ y,
+                                                              const double *__restrict__ dinv, double omega,
+                                                              int smooth, double *__restrict__ zF) {
   FcgState *s = k.s;
   __shared__ FcgScal sc;
   fcg_scalars(s, &sc, false);
   if (sc.done) return;
   const int cnt = sc.count;
-  if (cnt == 0) return;
   const int64_t nn = k.op.nn;
+  auto z3 = [&](int64_t m) { return y ? zA[m] + y[m] : zA[m]; };
   double v[PIC_FCG_MAX_WINDOW];
 #pragma unroll
-  for (int t = 0; t < PIC_FCG_MAX_WINDOW; ++t) v[t] = 0.0;
+  for (int q = 0; q < PIC_FCG_MAX_WINDOW; ++q) v[q] = 0.0;
   for (int it = 0; it < PIC_RED_ITEMS; ++it) {
     int64_t n = (int64_t)blockIdx.x * PIC_RED_CHUNK + it * PIC_RED_THREADS + threadIdx.x;
     if (n >= nn) continue;
-    const double zv = k.op.w[n];
+    double zf = 0.0;
+    if (k.op.row_kind[n] >= 0) {
+      zf = z3(n);
+      if (smooth) zf = fma(omega * dinv[n], r[n] - row_apply(k.op, n, z3), zf);
+    }
+    zF[n] = zf;
 #pragma unroll
-    for (int t = 0; t < PIC_FCG_MAX_WINDOW; ++t)
-      if (t < cnt) v[t] = fma(zv, k.Q[(size_t)fcg_slot(k, t + 1) * nn + n], v[t]);
+    for (int q = 0; q < PIC_FCG_MAX_WINDOW; ++q)
+      if (q < cnt) v[q] = fma(zf, k.Q[(size_t)fcg_slot(k, q + 1) * nn + n], v[q]);
   }
+  if (!s || cnt == 0) return;
   double out[PIC_FCG_MAX_WINDOW];
   block_sum_canon<PIC_FCG_MAX_WINDOW>(v, out);
   if (threadIdx.x == 0)
-    for (int t = 0; t < PIC_FCG_MAX_WINDOW; ++t) k.part[(size_t)t * k.op.nb + blockIdx.x] = out[t];
+    for (int q = 0; q < PIC_FCG_MAX_WINDOW; ++q) k.part[(size_t)q * k.op.nb + blockIdx.x] = out[q];
   if (arrive_last(&s->ticket)) {
     double tot[PIC_FCG_MAX_WINDOW];
     final_sum_canon<PIC_FCG_MAX_WINDOW>(k.part, k.op.nb, tot);
     if (threadIdx.x == 0) {
       s->ticket = 0;
-      for (int t = 0; t < cnt; ++t) s->beta[t] = -tot[t] / s->pq_hist[fcg_slot(k, t + 1)];
+      for (int q = 0; q < cnt; ++q) s->beta[q] = -tot[q] / s->pq_hist[fcg_slot(k, q + 1)];
     }
   }
 }
 
-// P_new = z + sum_t beta_t P_t on unknown nodes (0 on Dirichlet nodes).  The
-// new slot may hold the oldest direction, which each thread reads before it
-// overwrites the same element.
-__global__ void k_fcg_p(FcgK k) {
-  __shared__ FcgScal sc;
-  fcg_scalars(k.s, &sc, true);
-  if (sc.done) return;
-  const int64_t n = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
-  const int64_t nn = k.op.nn;
-  if (n >= nn) return;
-  const int cnt = sc.count;
-  double pv = 0.0;
-  if (k.op.row_kind[n] >= 0) {
-    pv = k.op.w[n];
-    for (int t = 0; t < cnt; ++t) pv = fma(sc.beta[t], k.P[(size_t)fcg_slot(k, t + 1) * nn + n], pv);
-  }
-  k.P[(size_t)k.slot * nn + n] = pv;
-}
-
-// Q_new = A P_new, p.q and p.r; alpha = p.r / p.q.
+// New direction P_new = z + sum_t beta_t P_t (on unknown nodes), formed at
+// every neighbour on the fly for Q_new = A P_new; p.q and p.r; alpha = p.r/p.q.
 __global__ void __launch_bounds__(PIC_RED_THREADS) k_fcg_dir(FcgK k) {
   FcgState *s = k.s;
   __shared__ FcgScal sc;
-  fcg_scalars(s, &sc, false);
+  fcg_scalars(s, &sc, true);
   if (sc.done) return;
+  const int cnt = sc.count;
   const int64_t nn = k.op.nn;
-  const double *pn = k.P + (size_t)k.slot * nn;
-  double *qn = k.Q + (size_t)k.slot * nn;
+  int off[PIC_FCG_MAX_WINDOW];
+#pragma unroll
+  for (int q = 0; q < PIC_FCG_MAX_WINDOW; ++q) off[q] = fcg_slot(k, q + 1);
+  auto pn = [&](int64_t m) {
+    if (k.op.row_kind[m] < 0) return 0.0;
+    double v = k.op.w[m];
+    for (int q = 0; q < cnt; ++q) v = fma(sc.beta[q], k.P[(size_t)off[q] * nn + m], v);
+    return v;
+  };
+  double *Pn = k.P + (size_t)k.slot * nn, *Qn = k.Q + (size_t)k.slot * nn;
   double vpq = 0.0, vpr = 0.0;
   for (int it = 0; it < PIC_RED_ITEMS; ++it) {
     int64_t n = (int64_t)blockIdx.x * PIC_RED_CHUNK + it * PIC_RED_THREADS + threadIdx.x;
     if (n >= nn) continue;
-    double pv = pn[n];
-    double qv = row_apply(k.op, n, [&](int64_t m) { return pn[m]; });
-    qn[n] = qv;
+    const double pv = pn(n);
+    const double qv = row_apply(k.op, n, pn);
+    Pn[n] = pv;
+    Qn[n] = qv;
     vpq = fma(pv, qv, vpq);
     vpr = fma(pv, k.op.r[n], vpr);
   }
@@ -1603,6 +1641,60 @@ int launch_spmv(const double *v, double *out) {
   return PIC_OK;
 }
 
+// Preconditioner stage A: pre-smoothing and coarse correction into zA; with
+// `learned`, also the learned stage's input t = r - A zA into d_pc_t.
+static int precond_stage_a(const double *r, double *zA, int learned) {
+  int rc;
+  const int nb = blocks_for(g.nn, 256);
+  const PcgK k0 = pcg_k(0);
+  if (g.pc_sweeps > 0) {
+    k_pc_pre<<<nb, 256, 0, g.st>>>(k0, r, g.d_pc_dinv, g.pc_omega, zA, g.d_pc_t);
+    PIC_LAUNCHED();
+    if (g.pc_cs > 0 && (rc = coarse_correct(g.d_pc_t, zA, 0))) return rc;
+  } else if (g.pc_cs > 0) {
+    if ((rc = coarse_correct(r, zA, 1))) return rc;
+  } else {
+    PIC_CUDA(cudaMemsetAsync(zA, 0, g.nn * sizeof(double), g.st));
+  }
+  if (learned) {
+    k_pc_mid<<<nb, 256, 0, g.st>>>(k0, r, zA, g.d_pc_t);
+    PIC_LAUNCHED();
+  }
+  return PIC_OK;
+}
+
+// Preconditioner stage B: zF = post-smoothing of zA (+ the learned stage's
+// y); inside FCG (fk != NULL) also the A-orthogonalisation coefficients.
+static int precond_stage_b(const double *r, const double *zA, double *zF, int learned, const FcgK *fk) {
+  FcgK k{};
+  if (fk) {
+    k = *fk;
+  } else {
+    k.op = pcg_k(0);
+    k.part = g.d_part;
+    k.ring = 1;
+    k.window = 1;
+  }
+  const int smooth = (g.pc_sweeps > 0 && (g.pc_cs > 0 || learned)) ? 1 : 0;
+  k_fcg_post<<<g.red_blocks, PIC_RED_THREADS, 0, g.st>>>(k, r, zA, learned ? g.d_pc_y : nullptr, g.d_pc_dinv,
+                                                         g.pc_omega, smooth, zF);
+  PIC_LAUNCHED();
+  return PIC_OK;
+}
+
+// z = M(r) (full != 0) or the classical stages only (full == 0).  Returns 1
+// when the learned stage's callback fails, a negative PIC_ERR_* on a CUDA
+// error.
+int precond_apply(int full, const double *r, double *z) {
+  int rc;
+  if ((rc = precond_prepare())) return rc;
+  if (!full) return precond_stage_a(r, z, 0);
+  const int learned = precond_learned_on();
+  if ((rc = precond_stage_a(r, g.d_pc_za, learned))) return rc;
+  if (learned && precond_callback()) return 1;
+  return precond_stage_b(r, g.d_pc_za, z, learned, nullptr);
+}
+
 static int dot2(const double *a, const double *b, const double *c, const double *d, double out[2]) {
   DotK k{a, b, c, d, g.d_part, g.d_dot, g.d_dot_ticket, g.nn, g.red_blocks};
   k_dot<<<g.red_blocks, PIC_RED_THREADS, 0, g.st>>>(k);
@@ -1652,7 +1744,7 @@ static int fcg_graph_launch(int i) {
 static int fcg_alloc() {
   if (g.d_fcg_P) return PIC_OK;
   int rc;
-  const size_t ring = (size_t)PIC_FCG_MAX_WINDOW * (size_t)g.nn;
+  const size_t ring = (size_t)(PIC_FCG_MAX_WINDOW + 1) * (size_t)g.nn;
   if ((rc = dalloc(&g.d_fcg_P, ring))) return rc;
   if ((rc = dalloc(&g.d_fcg_Q, ring))) return rc;
   if ((rc = dalloc(&g.d_fcg_part, (size_t)PIC_FCG_MAX_WINDOW * g.red_blocks))) return rc;
@@ -1674,7 +1766,7 @@ static int run_fcg(pic_solve_stats *stats, int *fcg_iters, int *rc_out) {
   if ((rc = fcg_alloc())) { *rc_out = rc; return 1; }
   PcgK k0 = pcg_k(0);
   k0.w = g.d_z;
-  FcgK fk{k0, g.d_fcg_P, g.d_fcg_Q, g.d_fcg_part, g.d_fcg, 0, g.fcg_window};
+  FcgK fk{k0, g.d_fcg_P, g.d_fcg_Q, g.d_fcg_part, g.d_fcg, 0, g.fcg_window + 1, g.fcg_window};
   k_pcg_x0<<<nb, 256, 0, g.st>>>(k0);
   PIC_LAUNCHED();
   k_spmv<<<nb, 256, 0, g.st>>>(k0, g.d_x, g.d_q);
@@ -1726,15 +1818,15 @@ static int run_fcg(pic_solve_stats *stats, int *fcg_iters, int *rc_out) {
     chunk = std::min(std::max(chunk, 2), 64);
     for (int c = 0; c < chunk; ++c) {
       ++g.fcg_precond_calls;
-      const int slot = (int)(enq++ % g.fcg_window);
+      const int slot = (int)(enq++ % (g.fcg_window + 1));
       if (use_graphs) {
         if (!g.fcg_graph[0] && (rc = fcg_capture(&g.fcg_graph[0], &g.fcg_graph_launches[0],
-                                                 [&] { return precond_stage_a(g.d_r, g.d_z, learned); }))) {
+                                                 [&] { return precond_stage_a(g.d_r, g.d_pc_za, learned); }))) {
           *rc_out = rc;
           return 1;
         }
         if ((rc = fcg_graph_launch(0))) { *rc_out = rc; return 1; }
-      } else if ((rc = precond_stage_a(g.d_r, g.d_z, learned))) {
+      } else if ((rc = precond_stage_a(g.d_r, g.d_pc_za, learned))) {
         *rc_out = rc;
         return 1;
       }
@@ -1746,11 +1838,7 @@ static int run_fcg(pic_solve_stats *stats, int *fcg_iters, int *rc_out) {
       fk.slot = slot;
       auto tail = [&] {
         int r2;
-        if ((r2 = precond_stage_b(g.d_r, g.d_z, learned))) return r2;
-        k_fcg_beta<<<g.red_blocks, PIC_RED_THREADS, 0, g.st>>>(fk);
-        PIC_LAUNCHED();
-        k_fcg_p<<<nb, 256, 0, g.st>>>(fk);
-        PIC_LAUNCHED();
+        if ((r2 = precond_stage_b(g.d_r, g.d_pc_za, g.d_z, learned, &fk))) return r2;
         k_fcg_dir<<<g.red_blocks, PIC_RED_THREADS, 0, g.st>>>(fk);
         PIC_LAUNCHED();
         k_fcg_upd<<<g.red_blocks, PIC_RED_THREADS, 0, g.st>>>(fk);

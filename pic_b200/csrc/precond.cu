@@ -16,40 +16,15 @@
 
 #include "pic_ctx.h"
 
+// The smoothing and post-smoothing kernels (they need the solver's stencil
+// operator) and the FCG kernels are in picgpu.cu; this file holds the coarse
+// space.
+
 namespace pic {
 
 namespace {
 
 constexpr int PC_THREADS = 256;
-
-// z = w (r - tmp)/diag (+ z when add), 0 on Dirichlet nodes; tmp may be NULL.
-__global__ void k_pc_jacobi(const double *__restrict__ r, const double *__restrict__ tmp,
-                            const double *__restrict__ diag, const int32_t *__restrict__ row_kind, double omega,
-                            int add, double *__restrict__ z, int64_t nn) {
-  int64_t n = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
-  if (n >= nn) return;
-  if (row_kind[n] < 0) {
-    z[n] = 0.0;
-    return;
-  }
-  const double res = tmp ? r[n] - tmp[n] : r[n];
-  const double v = omega * res / diag[n];
-  z[n] = add ? z[n] + v : v;
-}
-
-// t = r - tmp on unknown nodes, 0 on Dirichlet nodes
-__global__ void k_pc_resid(const double *__restrict__ r, const double *__restrict__ tmp,
-                           const int32_t *__restrict__ row_kind, double *__restrict__ t, int64_t nn) {
-  int64_t n = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
-  if (n < nn) t[n] = (row_kind[n] < 0) ? 0.0 : r[n] - tmp[n];
-}
-
-// z += y on unknown nodes
-__global__ void k_pc_add(const double *__restrict__ y, const int32_t *__restrict__ row_kind,
-                         double *__restrict__ z, int64_t nn) {
-  int64_t n = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
-  if (n < nn && row_kind[n] >= 0) z[n] += y[n];
-}
 
 struct CoarseK {
   int nnx, nny, cs, ncx, ncy;
@@ -96,11 +71,16 @@ __global__ void k_pc_gemv(const double *__restrict__ ainv, const double *__restr
   if (lane == 0) ec[row] = s;
 }
 
-// z += P ec on unknown nodes (bilinear from the four coarse nodes around)
+// z (+)= P ec on unknown nodes (bilinear from the four coarse nodes around);
+// with assign, z = P ec and 0 on Dirichlet nodes
 __global__ void k_pc_prolong(CoarseK c, const double *__restrict__ ec, const int32_t *__restrict__ row_kind,
-                             double *__restrict__ z, int64_t nn) {
+                             int assign, double *__restrict__ z, int64_t nn) {
   int64_t n = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
-  if (n >= nn || row_kind[n] < 0) return;
+  if (n >= nn) return;
+  if (row_kind[n] < 0) {
+    if (assign) z[n] = 0.0;
+    return;
+  }
   const int i = (int)(n / c.nny), j = (int)(n % c.nny);
   const int I = i / c.cs, J = j / c.cs;
   const double fx = (double)(i - I * c.cs) / c.cs, fy = (double)(j - J * c.cs) / c.cs;
@@ -109,7 +89,12 @@ __global__ void k_pc_prolong(CoarseK c, const double *__restrict__ ec, const int
   v = fma(fx * (1.0 - fy), ec[I1 * c.ncy + J], v);
   v = fma((1.0 - fx) * fy, ec[I * c.ncy + J1], v);
   v = fma(fx * fy, ec[I1 * c.ncy + J1], v);
-  z[n] += v;
+  z[n] = assign ? v : z[n] + v;
+}
+
+__global__ void k_pc_dinv(const double *__restrict__ diag, double *__restrict__ dinv, int64_t nn) {
+  int64_t n = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (n < nn) dinv[n] = 1.0 / diag[n];
 }
 
 template <class T>
@@ -122,24 +107,34 @@ int pc_vectors() {
   int rc;
   if (!g.d_pc_t && (rc = pc_alloc(&g.d_pc_t, g.nn))) return rc;
   if (!g.d_pc_y && (rc = pc_alloc(&g.d_pc_y, g.nn))) return rc;
-  if (!g.d_pc_tmp && (rc = pc_alloc(&g.d_pc_tmp, g.nn))) return rc;
+  if (!g.d_pc_za && (rc = pc_alloc(&g.d_pc_za, g.nn))) return rc;
+  if (!g.d_pc_dinv) {
+    if ((rc = pc_alloc(&g.d_pc_dinv, g.nn))) return rc;
+    k_pc_dinv<<<blocks_for(g.nn, PC_THREADS), PC_THREADS, 0, g.st>>>(g.d_diag, g.d_pc_dinv, g.nn);
+    PIC_LAUNCHED();
+  }
   return PIC_OK;
 }
 
 CoarseK coarse_k() { return CoarseK{g.m.nnx, g.m.nny, g.pc_cs, g.pc_ncx, g.pc_ncy}; }
 
-// z += P Ac^-1 P^T t
-int coarse_correct(const double *t, double *z) {
+}  // namespace
+
+// z += P Ac^-1 P^T t (z = P Ac^-1 P^T t with assign)
+int coarse_correct(const double *t, double *z, int assign) {
   CoarseK c = coarse_k();
   const int nc = c.ncx * c.ncy;
   k_pc_restrict<<<nc, PC_THREADS, 0, g.st>>>(c, t, g.d_pc_rc);
   PIC_LAUNCHED();
   k_pc_gemv<<<(nc + 7) / 8, 256, 0, g.st>>>(g.d_pc_ainv, g.d_pc_rc, g.d_pc_ec, nc);
   PIC_LAUNCHED();
-  k_pc_prolong<<<blocks_for(g.nn, PC_THREADS), PC_THREADS, 0, g.st>>>(c, g.d_pc_ec, g.d_row_kind, z, g.nn);
+  k_pc_prolong<<<blocks_for(g.nn, PC_THREADS), PC_THREADS, 0, g.st>>>(c, g.d_pc_ec, g.d_row_kind, assign, z,
+                                                                        g.nn);
   PIC_LAUNCHED();
   return PIC_OK;
 }
+
+namespace {
 
 // In-place Cholesky of a dense SPD matrix (row-major, lower factor), then
 // the inverse from it.  Returns false when a pivot is not positive.
@@ -254,79 +249,19 @@ int coarse_setup(const pic_mesh_desc *mesh, int coarse_cells) {
   return PIC_OK;
 }
 
-// Stage A: smoothing and coarse correction into z; with `learned`, also the
-// learned stage's input t = r - A z2 into d_pc_t.
-int precond_stage_a(const double *r, double *z, int learned) {
-  int rc;
-  if ((rc = pc_vectors())) return rc;
-  const int nb = blocks_for(g.nn, PC_THREADS);
-  const bool smooth = g.pc_sweeps > 0, coarse = g.pc_cs > 0;
-  if (smooth) {
-    k_pc_jacobi<<<nb, PC_THREADS, 0, g.st>>>(r, nullptr, g.d_diag, g.d_row_kind, g.pc_omega, 0, z, g.nn);
-  } else {
-    k_pc_resid<<<nb, PC_THREADS, 0, g.st>>>(r, r, g.d_row_kind, z, g.nn);  // z = 0
-  }
-  PIC_LAUNCHED();
-  if (coarse) {
-    if (smooth) {
-      if ((rc = launch_spmv(z, g.d_pc_tmp))) return rc;
-      k_pc_resid<<<nb, PC_THREADS, 0, g.st>>>(r, g.d_pc_tmp, g.d_row_kind, g.d_pc_t, g.nn);
-      PIC_LAUNCHED();
-      if ((rc = coarse_correct(g.d_pc_t, z))) return rc;
-    } else {
-      if ((rc = coarse_correct(r, z))) return rc;
-    }
-  }
-  if (learned) {
-    if ((rc = launch_spmv(z, g.d_pc_tmp))) return rc;
-    k_pc_resid<<<nb, PC_THREADS, 0, g.st>>>(r, g.d_pc_tmp, g.d_row_kind, g.d_pc_t, g.nn);
-    PIC_LAUNCHED();
-  }
-  return PIC_OK;
-}
-
-// Stage B: with `learned`, z += y (the callback's output in d_pc_y); then
-// post-smoothing.
-int precond_stage_b(const double *r, double *z, int learned) {
-  int rc;
-  const int nb = blocks_for(g.nn, PC_THREADS);
-  if (learned) {
-    k_pc_add<<<nb, PC_THREADS, 0, g.st>>>(g.d_pc_y, g.d_row_kind, z, g.nn);
-    PIC_LAUNCHED();
-  }
-  if (g.pc_sweeps > 0 && (g.pc_cs > 0 || learned)) {
-    if ((rc = launch_spmv(z, g.d_pc_tmp))) return rc;
-    k_pc_jacobi<<<nb, PC_THREADS, 0, g.st>>>(r, g.d_pc_tmp, g.d_diag, g.d_row_kind, g.pc_omega, 1, z, g.nn);
-    PIC_LAUNCHED();
-  }
-  return PIC_OK;
-}
-
 int precond_prepare() { return pc_vectors(); }
 
 int precond_learned_on() { return (g.pc_learned && g.precond) ? 1 : 0; }
 
-// The learned stage: y = fn(t) for the callback registered by the caller.
+// The learned stage: y = fn(t) with the callback registered by the caller.
 // Returns 1 when it fails.
 int precond_callback() { return g.precond(g.d_pc_t, g.d_pc_y, g.precond_user) != 0 ? 1 : 0; }
-
-// z = M(r) (full != 0) or the classical part before the learned stage,
-// z2 = S r + P Ac^-1 P^T (r - A S r) (full == 0).  Returns 1 when the
-// learned stage's callback fails, a negative PIC_ERR_* on a CUDA error.
-int precond_apply(int full, const double *r, double *z) {
-  int rc;
-  const int learned = full ? precond_learned_on() : 0;
-  if ((rc = precond_stage_a(r, z, learned))) return rc;
-  if (!full) return PIC_OK;
-  if (learned && precond_callback()) return 1;
-  return precond_stage_b(r, z, learned);
-}
 
 void precond_free() {
   auto F = [](void *p) {
     if (p) cudaFree(p);
   };
-  F(g.d_pc_t); F(g.d_pc_y); F(g.d_pc_tmp); F(g.d_pc_ainv); F(g.d_pc_rc); F(g.d_pc_ec);
+  F(g.d_pc_t); F(g.d_pc_y); F(g.d_pc_za); F(g.d_pc_dinv); F(g.d_pc_ainv); F(g.d_pc_rc); F(g.d_pc_ec);
 }
 
 }  // namespace pic
