@@ -122,6 +122,7 @@ struct Ctx {
   PcgState *d_pcg = nullptr;
   int red_blocks = 0;
   int coop_grid = 0;               // CTAs of the persistent PCG (0: two-kernel loop)
+  int fcg_coop_grid = 0;           // CTAs of the persistent FCG (0: graph-launched iterations)
   int smem_grid = 0;               // CTAs of the shared-memory-resident PCG (0: not eligible)
   bool ex_local = true;            // every explicit row stays inside its 3x3 neighbourhood
   size_t smem_bytes = 0;

@@ -1248,6 +1248,225 @@ __global__ void __launch_bounds__(PIC_RED_THREADS) k_fcg_upd(FcgK k) {
   }
 }
 
+// ---- persistent flexible CG (window 1, classical stages) -------------------
+// The whole solve in one cooperative kernel of kWide-thread CTAs: per
+// iteration the phases below, separated by the bounded grid barrier of the
+// persistent Jacobi-PCG.  Scalars (beta, alpha, r.r) are formed by every CTA
+// from the chunk partials in the canonical order, so all CTAs take the same
+// decisions.  Phases:
+//   (1) zA = w D^-1 r, t = r - A zA          (pre-smoothing)
+//   (2) rc = P^T t                             (restriction, warp per coarse node)
+//   (3) ec = Ac^-1 rc                          (GEMV, warp per row)
+//   (4) zA += P ec                             (prolongation)
+//   (5) zF = zA + w D^-1 (r - A zA), zF.Q_old  (post-smoothing)
+//   (6) P_new = zF + beta P_old
+//   (7) Q_new = A P_new, p.q, p.r
+//   (8) x += alpha P_new, r -= alpha Q_new, r.r
+// Without a coarse space phases 2-4 are skipped.
+struct FcgP {
+  PcgK k;                        // operator, x, r
+  const double *dinv;
+  double *zA, *t, *zF, *P0, *P1, *Q0, *Q1;
+  double *part;                  // [2][nb] chunk partials
+  const double *ainv;
+  double *rc, *ec;
+  int nnx, cs, ncx, ncy, coarse;
+  double omega;
+  FcgState *s;
+  unsigned int *bar;
+  int *bar_err;
+  long long spin_limit;
+  unsigned int bar_extra;
+};
+
+__global__ void __launch_bounds__(kWide, 1) k_fcg_persist(FcgP F) {
+  const PcgK &k = F.k;
+  FcgState *S = F.s;
+  __shared__ double sa[2][kWide], sb[2][kWide];
+  const int64_t nn = k.nn;
+  const int nb = k.nb;
+  const double rhs = S->rhs, tol2 = S->tol2, omega = F.omega;
+  const int maxit = S->maxit, stall_window = S->stall_window;
+  int iter = S->iter, ierr = 0, best_iter = S->best_iter;
+  double rr = S->rr, best = S->best, pq_old = 0.0;
+  bool have_old = false, ok = true;
+  int parity = 0;
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  const int gwarp = blockIdx.x * (kWide / 32) + warp, nwarps = gridDim.x * (kWide / 32);
+  const int nc = F.ncx * F.ncy;
+  auto barrier = [&]() { return grid_barrier(F.bar, F.bar_err, F.spin_limit, F.bar_extra); };
+  for (;;) {
+    double *Pn = parity ? F.P1 : F.P0, *Qn = parity ? F.Q1 : F.Q0;
+    const double *Po = parity ? F.P0 : F.P1, *Qo = parity ? F.Q0 : F.Q1;
+    // (1) pre-smoothing
+    for (int c = blockIdx.x; c < nb; c += gridDim.x) {
+      const int64_t n = (int64_t)c * kWide + threadIdx.x;
+      if (n < nn) {
+        if (k.row_kind[n] < 0) {
+          F.zA[n] = 0.0;
+          F.t[n] = 0.0;
+        } else {
+          auto z1 = [&](int64_t m) { return (omega * __ldcg(k.r + m)) * F.dinv[m]; };
+          F.zA[n] = z1(n);
+          F.t[n] = __ldcg(k.r + n) - row_apply(k, n, z1);
+        }
+      }
+    }
+    if (F.coarse) {
+      if (!(ok = barrier())) break;
+      // (2) restriction
+      for (int C = gwarp; C < nc; C += nwarps) {
+        const int I = C / F.ncy, J = C % F.ncy;
+        const int i0 = max(0, (I - 1) * F.cs + 1), i1 = min(F.nnx - 1, (I + 1) * F.cs - 1);
+        const int j0 = max(0, (J - 1) * F.cs + 1), j1 = min(k.nny - 1, (J + 1) * F.cs - 1);
+        const int ni = i1 - i0 + 1, nj = j1 - j0 + 1;
+        const double inv = 1.0 / F.cs;
+        double a = 0.0;
+        for (int e = lane; e < ni * nj; e += 32) {
+          const int i = i0 + e / nj, j = j0 + e % nj;
+          const double w = (1.0 - fabs((double)(i - I * F.cs)) * inv) * (1.0 - fabs((double)(j - J * F.cs)) * inv);
+          a = fma(w, __ldcg(F.t + (int64_t)i * k.nny + j), a);
+        }
+        for (int off = 16; off > 0; off >>= 1) a += __shfl_xor_sync(0xffffffffu, a, off);
+        if (lane == 0) F.rc[C] = a;
+      }
+      if (!(ok = barrier())) break;
+      // (3) coarse solve
+      for (int row = gwarp; row < nc; row += nwarps) {
+        const double *arow = F.ainv + (size_t)row * nc;
+        double a = 0.0;
+        for (int q = lane; q < nc; q += 32) a = fma(arow[q], __ldcg(F.rc + q), a);
+        for (int off = 16; off > 0; off >>= 1) a += __shfl_xor_sync(0xffffffffu, a, off);
+        if (lane == 0) F.ec[row] = a;
+      }
+      if (!(ok = barrier())) break;
+      // (4) prolongation
+      for (int c = blockIdx.x; c < nb; c += gridDim.x) {
+        const int64_t n = (int64_t)c * kWide + threadIdx.x;
+        if (n < nn && k.row_kind[n] >= 0) {
+          const int i = (int)(n / k.nny), j = (int)(n % k.nny);
+          const int I = i / F.cs, J = j / F.cs;
+          const double fx = (double)(i - I * F.cs) / F.cs, fy = (double)(j - J * F.cs) / F.cs;
+          const int I1 = min(I + 1, F.ncx - 1), J1 = min(J + 1, F.ncy - 1);
+          double v = (1.0 - fx) * (1.0 - fy) * __ldcg(F.ec + I * F.ncy + J);
+          v = fma(fx * (1.0 - fy), __ldcg(F.ec + I1 * F.ncy + J), v);
+          v = fma((1.0 - fx) * fy, __ldcg(F.ec + I * F.ncy + J1), v);
+          v = fma(fx * fy, __ldcg(F.ec + I1 * F.ncy + J1), v);
+          F.zA[n] += v;
+        }
+      }
+    }
+    if (!(ok = barrier())) break;
+    // (5) post-smoothing and zF.Q_old
+    for (int c = blockIdx.x; c < nb; c += gridDim.x) {
+      const int64_t base = (int64_t)c * kWide;
+      const int nvalid = (int)min((int64_t)kWide, nn - base);
+      const int64_t n = base + threadIdx.x;
+      double zf = 0.0, qo = 0.0;
+      if (threadIdx.x < nvalid) {
+        if (k.row_kind[n] >= 0) {
+          auto za = [&](int64_t m) { return __ldcg(F.zA + m); };
+          zf = fma(omega * F.dinv[n], __ldcg(k.r + n) - row_apply(k, n, za), za(n));
+        }
+        F.zF[n] = zf;
+        if (have_old) qo = __ldcg(Qo + n);
+      }
+      sa[0][threadIdx.x] = zf;
+      sb[0][threadIdx.x] = qo;
+      __syncthreads();
+      double part[1];
+      chunk_dots<1>(sa, sb, nvalid, part);
+      if (threadIdx.x == 0) F.part[c] = part[0];
+    }
+    if (!(ok = barrier())) break;
+    double beta = 0.0;
+    if (have_old) {
+      double zq;
+      final_sum_wide<1>(F.part, nb, &zq);
+      beta = -zq / pq_old;
+    }
+    // (6) new direction
+    for (int c = blockIdx.x; c < nb; c += gridDim.x) {
+      const int64_t n = (int64_t)c * kWide + threadIdx.x;
+      if (n < nn) {
+        double pv = 0.0;
+        if (k.row_kind[n] >= 0) pv = have_old ? fma(beta, __ldcg(Po + n), __ldcg(F.zF + n)) : __ldcg(F.zF + n);
+        Pn[n] = pv;
+      }
+    }
+    if (!(ok = barrier())) break;
+    // (7) Q_new = A P_new, p.q, p.r
+    for (int c = blockIdx.x; c < nb; c += gridDim.x) {
+      const int64_t base = (int64_t)c * kWide;
+      const int nvalid = (int)min((int64_t)kWide, nn - base);
+      const int64_t n = base + threadIdx.x;
+      double pv = 0.0, qv = 0.0, rv = 0.0;
+      if (threadIdx.x < nvalid) {
+        pv = __ldcg(Pn + n);
+        qv = row_apply(k, n, [&](int64_t m) { return __ldcg(Pn + m); });
+        Qn[n] = qv;
+        rv = __ldcg(k.r + n);
+      }
+      sa[0][threadIdx.x] = pv;
+      sb[0][threadIdx.x] = qv;
+      sa[1][threadIdx.x] = pv;
+      sb[1][threadIdx.x] = rv;
+      __syncthreads();
+      double part[2];
+      chunk_dots<2>(sa, sb, nvalid, part);
+      if (threadIdx.x == 0) {
+        F.part[c] = part[0];
+        F.part[nb + c] = part[1];
+      }
+    }
+    if (!(ok = barrier())) break;
+    double pqpr[2];
+    final_sum_wide<2>(F.part, nb, pqpr);
+    if (!(pqpr[0] > 0.0) || !(pqpr[1] == pqpr[1])) {
+      ierr = 2;
+      break;
+    }
+    const double alpha = pqpr[1] / pqpr[0];
+    // (8) update, r.r
+    for (int c = blockIdx.x; c < nb; c += gridDim.x) {
+      const int64_t base = (int64_t)c * kWide;
+      const int nvalid = (int)min((int64_t)kWide, nn - base);
+      const int64_t n = base + threadIdx.x;
+      double rv = 0.0;
+      if (threadIdx.x < nvalid) {
+        k.x[n] = fma(alpha, __ldcg(Pn + n), k.x[n]);
+        rv = fma(-alpha, __ldcg(Qn + n), __ldcg(k.r + n));
+        k.r[n] = rv;
+      }
+      sa[0][threadIdx.x] = rv;
+      sb[0][threadIdx.x] = rv;
+      __syncthreads();
+      double part[1];
+      chunk_dots<1>(sa, sb, nvalid, part);
+      if (threadIdx.x == 0) F.part[2 * nb + c] = part[0];
+    }
+    if (!(ok = barrier())) break;
+    final_sum_wide<1>(F.part + 2 * nb, nb, &rr);
+    ++iter;
+    pq_old = pqpr[0];
+    have_old = true;
+    parity ^= 1;
+    if (!(rr == rr)) { ierr = 4; break; }
+    if (rr / rhs <= tol2) break;
+    if (iter >= maxit) { ierr = 1; break; }
+    if (rr < best) { best = rr; best_iter = iter; }
+    if (iter - best_iter > stall_window || rr > 1e6 * best) { ierr = 3; break; }
+  }
+  if (blockIdx.x == 0 && threadIdx.x == 0) {
+    S->iter = iter;
+    S->rr = rr;
+    S->best = best;
+    S->best_iter = best_iter;
+    S->ierr = ok ? ierr : 7;  // 7: a grid barrier timed out
+    S->done = 1;
+  }
+}
+
 __constant__ double c_ppr_reg[5][9];
 
 struct PprK {
@@ -1812,6 +2031,59 @@ static int run_fcg(pic_solve_stats *stats, int *fcg_iters, int *rc_out) {
     }
   }
   int judged = 0;
+  if (g.fcg_coop_grid > 0 && g.fcg_window == 1 && !learned && g.pc_sweeps > 0) {
+    FcgP F;
+    F.k = k0;
+    F.dinv = g.d_pc_dinv;
+    F.zA = g.d_pc_za;
+    F.t = g.d_pc_t;
+    F.zF = g.d_z;
+    F.P0 = g.d_fcg_P;
+    F.P1 = g.d_fcg_P + nn;
+    F.Q0 = g.d_fcg_Q;
+    F.Q1 = g.d_fcg_Q + nn;
+    F.part = g.d_fcg_part;
+    F.ainv = g.d_pc_ainv;
+    F.rc = g.d_pc_rc;
+    F.ec = g.d_pc_ec;
+    F.nnx = g.m.nnx;
+    F.cs = g.pc_cs;
+    F.ncx = g.pc_ncx;
+    F.ncy = g.pc_ncy;
+    F.coarse = g.pc_cs > 0 ? 1 : 0;
+    F.omega = g.pc_omega;
+    F.s = g.d_fcg;
+    F.bar = g.d_bar;
+    F.bar_err = (int *)(g.d_bar + 2);
+    F.spin_limit = g.pcg_spin_limit;
+    F.bar_extra = g.pcg_bar_extra;
+    for (;;) {
+      PIC_CUDA(cudaMemsetAsync(g.d_bar, 0, 4 * sizeof(unsigned int), g.st));
+      void *args[] = {&F};
+      PIC_CUDA(cudaLaunchCooperativeKernel((const void *)k_fcg_persist, dim3(g.fcg_coop_grid), dim3(kWide), args,
+                                           0, g.st));
+      PIC_LAUNCHED();
+      PIC_CUDA(cudaMemcpyAsync(&hs, g.d_fcg, sizeof hs, cudaMemcpyDeviceToHost, g.st));
+      PIC_CUDA(cudaStreamSynchronize(g.st));
+      if (hs.ierr == 7) {
+        set_error("pic_ife_solve: FCG grid barrier timed out");
+        *rc_out = PIC_ERR_CUDA;
+        return 1;
+      }
+      if (hs.ierr) return finish(hs.ierr);
+      k_spmv<<<nb, 256, 0, g.st>>>(k0, g.d_x, g.d_q);
+      PIC_LAUNCHED();
+      k_fcg_r0<<<nb, 256, 0, g.st>>>(g.d_row_kind, g.d_b, g.d_q, g.d_r, nn);
+      PIC_LAUNCHED();
+      if ((rc = dot2(g.d_r, g.d_r, nullptr, nullptr, s2))) { *rc_out = rc; return 1; }
+      hs.rr = s2[0];
+      if (hs.rr / hs.rhs <= hs.tol2) return finish(0);
+      if (++judged > 3 || hs.iter >= hs.maxit) return finish(6);
+      hs.done = 0;
+      hs.count = 0;
+      PIC_CUDA(cudaMemcpyAsync(g.d_fcg, &hs, sizeof hs, cudaMemcpyHostToDevice, g.st));
+    }
+  }
   int64_t enq = 0;  // iterations enqueued (ring slot = enq mod m)
   for (;;) {
     int chunk = g.fcg_last_iters - hs.iter;
@@ -2401,6 +2673,11 @@ int pic_init(const pic_mesh_desc *mesh, const pic_params *params) {
     const char *env = getenv("PIC_PCG_PERSISTENT");
     bool want = !(env && env[0] == '0');
     g.coop_grid = (want && coop && per_sm > 0) ? std::min(g.red_blocks, per_sm * nsm) : 0;
+    int per_sm_f = 0;
+    PIC_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm_f, k_fcg_persist, kWide, 0));
+    const char *envf = getenv("PIC_FCG_PERSISTENT");
+    const bool want_f = !(envf && envf[0] == '0');
+    g.fcg_coop_grid = (want_f && coop && per_sm_f > 0) ? std::min(g.red_blocks, per_sm_f * nsm) : 0;
     // shared-memory-resident variant: every CTA owns at most kSmemChunks
     // chunks and its window of w and p fits next to them
     g.smem_grid = 0;

@@ -447,3 +447,29 @@ def test_fcg_graphs_match_eager():
         finally:
             sim.close()
     assert out[0][0] == out[1][0] and np.array_equal(out[0][1], out[1][1])
+
+
+@gpu
+def test_persistent_fcg_matches_graph_path():
+    """The one-kernel FCG (window 1, classical stages) and the graph-launched
+    iterations reach the same tolerance in the same number of iterations to
+    within a few (their restriction sums in a different order)."""
+    from pic_b200.simulation import Simulation
+    out = []
+    for flag in ("0", "1"):
+        os.environ["PIC_FCG_PERSISTENT"] = flag
+        try:
+            sim = Simulation(deck.config("cfg1", ncx=256, ncy=256, ppc=2, pcg_tol=1e-10))
+        finally:
+            del os.environ["PIC_FCG_PERSISTENT"]
+        try:
+            sim.initial_fields()
+            sim.set_solver("fcg", coarse_cells=32, window=1)
+            st, phi = _solve_from(sim, np.zeros(sim.mesh.nn), api.PIC_SOLVER_FCG_UNET)
+            assert st.fallback == 0 and _true_rel_residual(sim) <= sim.cfg.pcg_tol * 1.0001
+            out.append((st.iterations, phi))
+            api.check(sim.lib.pic_set_solver(api.PIC_SOLVER_JPCG), "set")
+        finally:
+            sim.close()
+    assert abs(out[0][0] - out[1][0]) <= 2
+    assert np.abs(out[0][1] - out[1][1]).max() <= 1e-7 * np.abs(out[0][1]).max()
