@@ -1262,7 +1262,10 @@ __global__ void __launch_bounds__(PIC_RED_THREADS) k_fcg_upd(FcgK k) {
 //   (6) P_new = zF + beta P_old
 //   (7) Q_new = A P_new, p.q, p.r
 //   (8) x += alpha P_new, r -= alpha Q_new, r.r
-// Without a coarse space phases 2-4 are skipped.
+// Without a coarse space phases 2-4 are skipped.  Loads after a grid barrier
+// are plain (L1-cached) loads: the barrier's release/acquire pair orders
+// every CTA's writes before them, and a stencil reads each value up to nine
+// times, from L1.
 struct FcgP {
   PcgK k;                        // operator, x, r
   const double *dinv;
@@ -1306,9 +1309,9 @@ __global__ void __launch_bounds__(kWide, 1) k_fcg_persist(FcgP F) {
           F.zA[n] = 0.0;
           F.t[n] = 0.0;
         } else {
-          auto z1 = [&](int64_t m) { return (omega * __ldcg(k.r + m)) * F.dinv[m]; };
+          auto z1 = [&](int64_t m) { return (omega * k.r[m]) * F.dinv[m]; };
           F.zA[n] = z1(n);
-          F.t[n] = __ldcg(k.r + n) - row_apply(k, n, z1);
+          F.t[n] = k.r[n] - row_apply(k, n, z1);
         }
       }
     }
@@ -1325,7 +1328,7 @@ __global__ void __launch_bounds__(kWide, 1) k_fcg_persist(FcgP F) {
         for (int e = lane; e < ni * nj; e += 32) {
           const int i = i0 + e / nj, j = j0 + e % nj;
           const double w = (1.0 - fabs((double)(i - I * F.cs)) * inv) * (1.0 - fabs((double)(j - J * F.cs)) * inv);
-          a = fma(w, __ldcg(F.t + (int64_t)i * k.nny + j), a);
+          a = fma(w, F.t[(int64_t)i * k.nny + j], a);
         }
         for (int off = 16; off > 0; off >>= 1) a += __shfl_xor_sync(0xffffffffu, a, off);
         if (lane == 0) F.rc[C] = a;
@@ -1365,8 +1368,8 @@ __global__ void __launch_bounds__(kWide, 1) k_fcg_persist(FcgP F) {
       double zf = 0.0, qo = 0.0;
       if (threadIdx.x < nvalid) {
         if (k.row_kind[n] >= 0) {
-          auto za = [&](int64_t m) { return __ldcg(F.zA + m); };
-          zf = fma(omega * F.dinv[n], __ldcg(k.r + n) - row_apply(k, n, za), za(n));
+          auto za = [&](int64_t m) { return F.zA[m]; };
+          zf = fma(omega * F.dinv[n], k.r[n] - row_apply(k, n, za), za(n));
         }
         F.zF[n] = zf;
         if (have_old) qo = __ldcg(Qo + n);
@@ -1402,8 +1405,8 @@ __global__ void __launch_bounds__(kWide, 1) k_fcg_persist(FcgP F) {
       const int64_t n = base + threadIdx.x;
       double pv = 0.0, qv = 0.0, rv = 0.0;
       if (threadIdx.x < nvalid) {
-        pv = __ldcg(Pn + n);
-        qv = row_apply(k, n, [&](int64_t m) { return __ldcg(Pn + m); });
+        pv = Pn[n];
+        qv = row_apply(k, n, [&](int64_t m) { return Pn[m]; });
         Qn[n] = qv;
         rv = __ldcg(k.r + n);
       }
