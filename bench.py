@@ -303,10 +303,10 @@ def run_ours(args, dist, rank, ws):
         sim.set_solver("jpcg")
 
     def sel_fcg():
-        sim.set_solver("fcg", coarse_cells=32, window=1)
+        sim.set_solver("fcg", coarse_cells=64, window=1)
 
     def sel_learned():
-        sim.set_solver("fcg", coarse_cells=32, window=4)
+        sim.set_solver("fcg", coarse_cells=64, window=4)
         lp.set_learned(True)
 
     variants = {"jacobi_pcg": sel_jpcg, "fcg_smooth_coarse": sel_fcg}

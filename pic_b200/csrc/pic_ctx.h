@@ -144,7 +144,8 @@ struct Ctx {
   int pc_learned = 1;                       // apply the registered callback as stage 3
   int pc_cs = 0, pc_ncx = 0, pc_ncy = 0;    // coarse spacing in nodes (0: no coarse space)
   double *d_pc_t = nullptr, *d_pc_y = nullptr, *d_pc_za = nullptr, *d_pc_dinv = nullptr;
-  double *d_pc_ainv = nullptr, *d_pc_rc = nullptr, *d_pc_ec = nullptr;
+  float *d_pc_ainv = nullptr;              // coarse inverse (FP32 copy, row-major)
+  double *d_pc_rc = nullptr, *d_pc_ec = nullptr;
   // CUDA graphs of one FCG iteration: [0] stage A, [1 + slot] stage B + FCG
   // kernels of ring slot `slot`; rebuilt when the configuration key changes
   cudaGraphExec_t fcg_graph[2 + PIC_FCG_MAX_WINDOW] = {};

@@ -1271,7 +1271,7 @@ struct FcgP {
   const double *dinv;
   double *zA, *t, *zF, *P0, *P1, *Q0, *Q1;
   double *part;                  // [2][nb] chunk partials
-  const double *ainv;
+  const float *ainv;
   double *rc, *ec;
   int nnx, cs, ncx, ncy, coarse;
   double omega;
@@ -1336,9 +1336,9 @@ __global__ void __launch_bounds__(kWide, 1) k_fcg_persist(FcgP F) {
       if (!(ok = barrier())) break;
       // (3) coarse solve
       for (int row = gwarp; row < nc; row += nwarps) {
-        const double *arow = F.ainv + (size_t)row * nc;
+        const float *arow = F.ainv + (size_t)row * nc;
         double a = 0.0;
-        for (int q = lane; q < nc; q += 32) a = fma(arow[q], __ldcg(F.rc + q), a);
+        for (int q = lane; q < nc; q += 32) a = fma((double)arow[q], __ldcg(F.rc + q), a);
         for (int off = 16; off > 0; off >>= 1) a += __shfl_xor_sync(0xffffffffu, a, off);
         if (lane == 0) F.ec[row] = a;
       }

@@ -6,7 +6,8 @@
 //   4. damped-Jacobi post-smoothing      z  = z3 + w D^-1 (r - A z3)
 // Each stage can be switched off.  The smoother removes the rough part of
 // the error, the coarse space (bilinear P on a uniform coarse grid of spacing
-// cs nodes, Ac = P^T A P inverted once on the host) the global part, and the
+// cs nodes, Ac = P^T A P assembled on the host and inverted once on the
+// device) the global part, and the
 // network what lies between -- it is trained on exactly the residuals stage 3
 // sees.  The reference solver (IFE-Solver/MY_PCG.f90) is Jacobi-PCG only:
 // none of this has a counterpart there.
@@ -59,14 +60,14 @@ __global__ void __launch_bounds__(PC_THREADS) k_pc_restrict(CoarseK c, const dou
 }
 
 // ec = Ainv rc, one warp per row (row-major FP64 inverse)
-__global__ void k_pc_gemv(const double *__restrict__ ainv, const double *__restrict__ rc, double *__restrict__ ec,
+__global__ void k_pc_gemv(const float *__restrict__ ainv, const double *__restrict__ rc, double *__restrict__ ec,
                           int nc) {
   const int row = blockIdx.x * (blockDim.x / 32) + (threadIdx.x >> 5);
   const int lane = threadIdx.x & 31;
   if (row >= nc) return;
-  const double *a = ainv + (size_t)row * nc;
+  const float *a = ainv + (size_t)row * nc;
   double s = 0.0;
-  for (int k = lane; k < nc; k += 32) s = fma(a[k], rc[k], s);
+  for (int k = lane; k < nc; k += 32) s = fma((double)a[k], rc[k], s);
   for (int off = 16; off > 0; off >>= 1) s += __shfl_xor_sync(0xffffffffu, s, off);
   if (lane == 0) ec[row] = s;
 }
@@ -136,42 +137,36 @@ int coarse_correct(const double *t, double *z, int assign) {
 
 namespace {
 
-// In-place Cholesky of a dense SPD matrix (row-major, lower factor), then
-// the inverse from it.  Returns false when a pivot is not positive.
-bool dense_spd_inverse(std::vector<double> &A, int n) {
-  std::vector<double> L(A);
-  for (int j = 0; j < n; ++j) {
-    double d = L[(size_t)j * n + j];
-    for (int k = 0; k < j; ++k) d -= L[(size_t)j * n + k] * L[(size_t)j * n + k];
-    if (!(d > 0.0)) return false;
-    d = std::sqrt(d);
-    L[(size_t)j * n + j] = d;
-    for (int i = j + 1; i < n; ++i) {
-      double s = L[(size_t)i * n + j];
-      const double *li = &L[(size_t)i * n], *lj = &L[(size_t)j * n];
-      for (int k = 0; k < j; ++k) s -= li[k] * lj[k];
-      L[(size_t)i * n + j] = s / d;
-    }
-  }
-  // inv(L) (lower), column by column
-  std::vector<double> Li((size_t)n * n, 0.0);
-  for (int j = 0; j < n; ++j) {
-    Li[(size_t)j * n + j] = 1.0 / L[(size_t)j * n + j];
-    for (int i = j + 1; i < n; ++i) {
-      double s = 0.0;
-      for (int k = j; k < i; ++k) s -= L[(size_t)i * n + k] * Li[(size_t)k * n + j];
-      Li[(size_t)i * n + j] = s / L[(size_t)i * n + i];
-    }
-  }
-  // A^-1 = inv(L)^T inv(L)
-  for (int i = 0; i < n; ++i)
-    for (int j = 0; j <= i; ++j) {
-      double s = 0.0;
-      for (int k = i; k < n; ++k) s += Li[(size_t)k * n + i] * Li[(size_t)k * n + j];
-      A[(size_t)i * n + j] = s;
-      A[(size_t)j * n + i] = s;
-    }
-  return true;
+// Gauss-Jordan inversion of the dense SPD coarse operator on the device,
+// without pivoting (SPD pivots stay positive), one elimination step per
+// pair of launches: k_gj_pivot copies the scaled pivot row and the pivot
+// column, k_gj_update eliminates column k from every other row and writes
+// the new row and column k.  In-place, FP64.
+__global__ void k_gj_pivot(const double *__restrict__ A, int n, int k, double *__restrict__ rowk,
+                           double *__restrict__ colk, int *__restrict__ bad) {
+  const int j = blockIdx.x * blockDim.x + threadIdx.x;
+  if (j >= n) return;
+  const double p = A[(size_t)k * n + k];
+  if (j == 0 && !(p > 0.0)) *bad = 1;
+  rowk[j] = (j == k) ? 1.0 / p : A[(size_t)k * n + j] / p;
+  colk[j] = A[(size_t)j * n + k];
+}
+
+__global__ void k_gj_update(double *__restrict__ A, int n, int k, const double *__restrict__ rowk,
+                            const double *__restrict__ colk) {
+  const int64_t e = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (e >= (int64_t)n * n) return;
+  const int i = (int)(e / n), j = (int)(e % n);
+  double v;
+  if (i == k) v = rowk[j];
+  else if (j == k) v = -colk[i] * rowk[k];
+  else v = fma(-colk[i], rowk[j], A[e]);
+  A[e] = v;
+}
+
+__global__ void k_to_f32(const double *__restrict__ a, float *__restrict__ b, int64_t n) {
+  const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i < n) b[i] = (float)a[i];
 }
 
 }  // namespace
@@ -183,7 +178,8 @@ int coarse_setup(const pic_mesh_desc *mesh, int coarse_cells) {
     cudaFree(g.d_pc_ainv);
     cudaFree(g.d_pc_rc);
     cudaFree(g.d_pc_ec);
-    g.d_pc_ainv = g.d_pc_rc = g.d_pc_ec = nullptr;
+    g.d_pc_ainv = nullptr;
+    g.d_pc_rc = g.d_pc_ec = nullptr;
   }
   g.pc_cs = 0;
   ++g.fcg_graph_gen;  // captured iterations hold the old buffers
@@ -192,8 +188,8 @@ int coarse_setup(const pic_mesh_desc *mesh, int coarse_cells) {
   int cs = std::max(1, std::min(ex, ey) / coarse_cells);
   while (cs > 1 && (ex % cs || ey % cs)) --cs;
   const int ncx = ex / cs + 1, ncy = ey / cs + 1, nc = ncx * ncy;
-  if (nc > 4500) {
-    set_error("pic_coarse_setup: coarse grid too large (at most 4500 coarse nodes)");
+  if (nc > 9000) {
+    set_error("pic_coarse_setup: coarse grid too large (at most 9000 coarse nodes)");
     return PIC_ERR_ARG;
   }
   const int64_t nn = (int64_t)g.m.nnx * g.m.nny;
@@ -234,15 +230,52 @@ int coarse_setup(const pic_mesh_desc *mesh, int coarse_cells) {
     }
   for (int C = 0; C < nc; ++C)  // coarse nodes without unknowns in their support
     if (Ac[(size_t)C * nc + C] == 0.0) Ac[(size_t)C * nc + C] = 1.0;
-  if (!dense_spd_inverse(Ac, nc)) {
+  int rc;
+  double *d_a = nullptr, *d_row = nullptr, *d_col = nullptr;
+  int *d_bad = nullptr;
+  const size_t nc2 = (size_t)nc * nc;
+  if ((rc = pc_alloc(&d_a, nc2))) return rc;
+  if ((rc = pc_alloc(&d_row, nc)) || (rc = pc_alloc(&d_col, nc)) || (rc = pc_alloc(&d_bad, 1))) {
+    cudaFree(d_a);
+    return rc;
+  }
+  auto release = [&]() {
+    cudaFree(d_a);
+    cudaFree(d_row);
+    cudaFree(d_col);
+    cudaFree(d_bad);
+  };
+  int bad = 0;
+  cudaError_t e = cudaMemcpyAsync(d_a, Ac.data(), nc2 * sizeof(double), cudaMemcpyHostToDevice, g.st);
+  if (e == cudaSuccess) e = cudaMemsetAsync(d_bad, 0, sizeof(int), g.st);
+  for (int k = 0; e == cudaSuccess && k < nc; ++k) {
+    k_gj_pivot<<<(nc + 255) / 256, 256, 0, g.st>>>(d_a, nc, k, d_row, d_col, d_bad);
+    k_gj_update<<<(unsigned)((nc2 + 255) / 256), 256, 0, g.st>>>(d_a, nc, k, d_row, d_col);
+    e = cudaPeekAtLastError();
+  }
+  if (e == cudaSuccess) e = cudaMemcpyAsync(&bad, d_bad, sizeof(int), cudaMemcpyDeviceToHost, g.st);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(g.st);
+  if (e != cudaSuccess) {
+    release();
+    return cuda_fail(e, "coarse operator inversion");
+  }
+  if (bad) {
+    release();
     set_error("pic_coarse_setup: coarse operator is not positive definite");
     return PIC_ERR_SETUP;
   }
-  int rc;
-  if ((rc = pc_alloc(&g.d_pc_ainv, (size_t)nc * nc))) return rc;
+  // the per-iteration GEMV reads an FP32 copy (half the bytes; at 65x65 coarse
+  // nodes it stays in L2) and accumulates in FP64
+  rc = pc_alloc(&g.d_pc_ainv, nc2);
+  if (!rc) {
+    k_to_f32<<<(unsigned)((nc2 + 255) / 256), 256, 0, g.st>>>(d_a, g.d_pc_ainv, (int64_t)nc2);
+    e = cudaStreamSynchronize(g.st);
+    if (e != cudaSuccess) rc = cuda_fail(e, "coarse inverse copy");
+  }
+  release();
+  if (rc) return rc;
   if ((rc = pc_alloc(&g.d_pc_rc, nc))) return rc;
   if ((rc = pc_alloc(&g.d_pc_ec, nc))) return rc;
-  PIC_CUDA(cudaMemcpy(g.d_pc_ainv, Ac.data(), Ac.size() * sizeof(double), cudaMemcpyHostToDevice));
   g.pc_cs = cs;
   g.pc_ncx = ncx;
   g.pc_ncy = ncy;

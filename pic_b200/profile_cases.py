@@ -2,7 +2,7 @@
 ncu (each runs a few launches of its kernels and exits):
 
     python -m pic_b200.profile_cases step  <deck> <ppc> <steps> [jpcg|fcg]
-    python -m pic_b200.profile_cases solve <cells> [jpcg|fcg] [repeats]
+    python -m pic_b200.profile_cases solve <cells> [jpcg|fcg] [repeats] [coarse_cells]
     python -m pic_b200.profile_cases unet  <nodes> [repeats]
 
 step:  the deck at <ppc> particles per cell and species, <steps> steps.
@@ -40,7 +40,7 @@ def _step(deck_name, ppc, steps, solver="fcg"):
     sim.close()
 
 
-def _solve(cells, solver="fcg", repeats=3):
+def _solve(cells, solver="fcg", repeats=3, coarse_cells=64):
     import torch
     from . import api, deck
     from .simulation import Simulation
@@ -48,7 +48,10 @@ def _solve(cells, solver="fcg", repeats=3):
     cfg = deck.config("cfg4", ncx=n, ncy=n, ppc=1)
     sim = Simulation(cfg, load=False)
     sim.set_field("rho", np.random.default_rng(0).standard_normal(sim.mesh.nn))
-    sim.set_solver(solver)
+    import time
+    t0 = time.perf_counter()
+    sim.set_solver(solver, coarse_cells=int(coarse_cells))
+    setup = time.perf_counter() - t0
     out = []
     for _ in range(int(repeats)):
         sim.set_field("phi", np.zeros(sim.mesh.nn))
@@ -60,7 +63,7 @@ def _solve(cells, solver="fcg", repeats=3):
         e1.record()
         torch.cuda.synchronize()
         out.append((st.iterations, round(e0.elapsed_time(e1), 3)))
-    print(f"solve {n}^2 {solver}: (iterations, ms) {out}")
+    print(f"solve {n}^2 {solver} coarse_cells={coarse_cells} (setup {setup:.2f} s): (iterations, ms) {out}")
     sim.close()
 
 

@@ -129,7 +129,7 @@ class Simulation:
         return st
 
     # ---- Poisson solver ---------------------------------------------------
-    def set_solver(self, kind: str = "jpcg", coarse_cells: int = 32, window: int = 1,
+    def set_solver(self, kind: str = "jpcg", coarse_cells: int = 64, window: int = 1,
                    omega: float = 2.0 / 3.0):
         """'jpcg': the reference's Jacobi-PCG.  'fcg': flexible CG with damped
         Jacobi smoothing and a Galerkin coarse space (no learned stage).

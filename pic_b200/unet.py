@@ -298,7 +298,7 @@ class LearnedPreconditioner:
 
     def __init__(self, sim, seed: int = 0, crop: int = 128, batch: int = 4, buffer: int = 32,
                  lr: float = 1e-3, synthetic: float = 0.5, smoothing: bool = True, omega: float = 2.0 / 3.0,
-                 coarse_cells: int = 32, window: int = 4, use_graph: bool = True):
+                 coarse_cells: int = 64, window: int = 4, use_graph: bool = True):
         import torch
         self.torch = torch
         self.sim = sim
