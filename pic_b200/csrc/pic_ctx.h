@@ -48,6 +48,11 @@ struct ObjK {
 };
 
 struct Species {
+  // With PIC_PREC_MIXED (f32) the five value arrays x, y, vx, vy, vz hold FP32
+  // data in the first half of their storage: x, y are the offsets inside the
+  // element loc (in element widths, [0, 1]), vx, vy, vz the velocities.  The
+  // FP64 layout is used only to stage uploads and downloads.
+  bool f32 = false;
   double charge = 0, mass = 0, weight = 0, qm = 0;
   int64_t capacity = 0, n_slots = 0, n_live = 0;
   uint32_t next_id = 0;
@@ -115,6 +120,8 @@ struct Ctx {
   // fields
   double *d_phi = nullptr, *d_rho = nullptr, *d_efx = nullptr, *d_efy = nullptr;
   double *d_coef = nullptr;  // [5][nn] coef_ppr(2..6,:)
+  bool mixed = false;        // PIC_PREC_MIXED
+  float *d_coef32 = nullptr; // mixed: per node {c2, c3, c4, c5, c6, 0, 0, 0} in FP32 (32 B records)
   // PCG vectors (full grid)
   double *d_b = nullptr, *d_x = nullptr, *d_r = nullptr, *d_w = nullptr, *d_p[2] = {nullptr, nullptr},
          *d_q = nullptr;

@@ -196,6 +196,37 @@ __device__ __forceinline__ long long seg_sum(long long v, int lane, int seg_end)
   return v;
 }
 
+// Lost-particle count and fixed-point deposit of one warp's particles (key =
+// the particle's element, -1 for none).  Segmented warp aggregation by
+// element (particles are cell-sorted, so neighbouring lanes usually share an
+// element), then one atomic per node and value from the segment head.
+// Integer sums are exact: node totals do not depend on the segmentation.
+__device__ __forceinline__ void warp_deposit(const SpK &s, int lane, int key, const double W[4], const int nodes[4],
+                                             double energy, bool lost, int do_deposit, int do_energy) {
+  unsigned int lm = __ballot_sync(0xffffffffu, lost);
+  if (lane == 0 && lm) atomicAdd(s.lost, (unsigned long long)__popc(lm));
+  if (!do_deposit) return;
+  int prev = __shfl_up_sync(0xffffffffu, key, 1);
+  bool head = (lane == 0) || (key != prev);
+  unsigned int heads = __ballot_sync(0xffffffffu, head);
+  unsigned int above = (lane == 31) ? 0u : (heads & ~((2u << lane) - 1u));
+  int seg_end = above ? (__ffs(above) - 2) : 31;
+  long long qv[4];
+#pragma unroll
+  for (int c = 0; c < 4; ++c) qv[c] = seg_sum((key >= 0) ? __double2ll_rn(W[c] * PIC_Q_SCALE) : 0ll, lane, seg_end);
+  if (head && key >= 0)
+#pragma unroll
+    for (int c = 0; c < 4; ++c) atomicAdd(s.q_acc + nodes[c], (unsigned long long)qv[c]);
+  if (!do_energy) return;
+  long long ev[4];
+#pragma unroll
+  for (int c = 0; c < 4; ++c)
+    ev[c] = seg_sum((key >= 0) ? __double2ll_rn((W[c] * energy) * PIC_E_SCALE) : 0ll, lane, seg_end);
+  if (head && key >= 0)
+#pragma unroll
+    for (int c = 0; c < 4; ++c) atomicAdd(s.e_acc + nodes[c], (unsigned long long)ev[c]);
+}
+
 // One particle per thread: gather E (old element), leapfrog push, wall/object
 // absorption, locate, fixed-point deposit of weight and weight*energy.
 __global__ void __launch_bounds__(256, 4) k_push(MeshK m, FieldK f, PushK prm, SpK s) {
@@ -284,33 +315,210 @@ __global__ void __launch_bounds__(256, 4) k_push(MeshK m, FieldK f, PushK prm, S
       }
     }
   }
-  // lost-particle count (warp aggregated)
-  unsigned int lm = __ballot_sync(0xffffffffu, lost);
-  if (lane == 0 && lm) atomicAdd(s.lost, (unsigned long long)__popc(lm));
-  if (!prm.do_deposit) return;
-  // Segmented warp aggregation by element (particles are cell-sorted, so
-  // neighbouring lanes usually share an element), then one atomic per node and
-  // value from the segment head.  Integer sums are exact: node totals do not
-  // depend on the segmentation.
-  int prev = __shfl_up_sync(0xffffffffu, key, 1);
-  bool head = (lane == 0) || (key != prev);
-  unsigned int heads = __ballot_sync(0xffffffffu, head);
-  unsigned int above = (lane == 31) ? 0u : (heads & ~((2u << lane) - 1u));
-  int seg_end = above ? (__ffs(above) - 2) : 31;
-  long long qv[4];
+  warp_deposit(s, lane, key, W, nodes, energy, lost, prm.do_deposit, prm.do_energy);
+}
+
+struct PushM {
+  float qmdt;      // q/m * dt
+  float dtx, dty;  // dt/hx, dt/hy: cells moved per unit velocity per step
+  float hx, hy;
+  double mass, vref;
+  int do_push, do_deposit, do_energy;
+  int wall[4];
+};
+
+// Mixed-precision form of k_push (PIC_PREC_MIXED): the particle is its
+// element (int32) plus FP32 offsets inside it (element widths) and FP32
+// velocities; the gather reads 32-byte FP32 node records {efx, efy, c2..c6},
+// the move is in element units (no division), walls are decided on (element,
+// offset) exactly, the object test runs in FP64 on the absolute position, and
+// the deposit is the same int64 fixed point.  40 bytes per particle (44 with
+// vz on diagnostic steps) against 80 for k_push.
+__global__ void __launch_bounds__(256, 4) k_push_mixed(MeshK m, const float *__restrict__ c32, PushM prm, SpK s) {
+  const int64_t p = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  const int lane = threadIdx.x & 31;
+  float *fx = reinterpret_cast<float *>(s.x), *fy = reinterpret_cast<float *>(s.y);
+  float *fvx = reinterpret_cast<float *>(s.vx), *fvy = reinterpret_cast<float *>(s.vy);
+  const float *fvz = reinterpret_cast<const float *>(s.vz);
+  int key = -1;
+  double W[4] = {0, 0, 0, 0};
+  int nodes[4] = {0, 0, 0, 0};
+  double energy = 0.0;
+  bool lost = false;
+  if (p < s.n) {
+    const int e = s.loc[p];
+    if (e >= 0) {
+      float ax = fx[p], ay = fy[p];
+      float vx = fvx[p], vy = fvy[p];
+      int i = elem_column(m, e), j = e - i * m.ney;
+      if (prm.do_push) {
+        const int n1 = i * m.nny + j;
+        const int cn[4] = {n1, n1 + m.nny, n1 + m.nny + 1, n1 + 1};
+        float Ex, Ey;
+        if (m.element_index[e] > 0) {
+          // average of the PPR gradients of the element's outside nodes
+          const float ox[4] = {0.f, 1.f, 1.f, 0.f}, oy[4] = {0.f, 0.f, 1.f, 1.f};
+          float ex = 0.f, ey = 0.f;
+          int cnt = 0;
 #pragma unroll
-  for (int c = 0; c < 4; ++c) qv[c] = seg_sum((key >= 0) ? __double2ll_rn(W[c] * PIC_Q_SCALE) : 0ll, lane, seg_end);
-  if (head && key >= 0)
+          for (int c = 0; c < 4; ++c) {
+            if (m.node_index[cn[c]] != -1) continue;
+            ++cnt;
+            const float4 r0 = *reinterpret_cast<const float4 *>(c32 + 8 * (size_t)cn[c]);
+            const float4 r1 = *reinterpret_cast<const float4 *>(c32 + 8 * (size_t)cn[c] + 4);
+            const float xr = (ax - ox[c]) * prm.hx, yr = (ay - oy[c]) * prm.hy;
+            ex = ((ex + r0.z) + (2.f * r1.x) * xr) + r1.y * yr;
+            ey = ((ey + r0.w) + (2.f * r1.z) * yr) + r1.y * xr;
+          }
+          Ex = -ex / (float)cnt;
+          Ey = -ey / (float)cnt;
+        } else {
+          const float xc = 1.f - ax, yc = 1.f - ay;
+          const float w[4] = {xc * yc, ax * yc, ax * ay, xc * ay};
+          Ex = 0.f;
+          Ey = 0.f;
 #pragma unroll
-    for (int c = 0; c < 4; ++c) atomicAdd(s.q_acc + nodes[c], (unsigned long long)qv[c]);
-  if (!prm.do_energy) return;
-  long long ev[4];
-#pragma unroll
-  for (int c = 0; c < 4; ++c)
-    ev[c] = seg_sum((key >= 0) ? __double2ll_rn((W[c] * energy) * PIC_E_SCALE) : 0ll, lane, seg_end);
-  if (head && key >= 0)
-#pragma unroll
-    for (int c = 0; c < 4; ++c) atomicAdd(s.e_acc + nodes[c], (unsigned long long)ev[c]);
+          for (int c = 0; c < 4; ++c) {
+            const float2 ef = *reinterpret_cast<const float2 *>(c32 + 8 * (size_t)cn[c]);
+            Ex = fmaf(w[c], ef.x, Ex);
+            Ey = fmaf(w[c], ef.y, Ey);
+          }
+        }
+        vx = fmaf(prm.qmdt, Ex, vx);
+        vy = fmaf(prm.qmdt, Ey, vy);
+        ax = fmaf(prm.dtx, vx, ax);
+        ay = fmaf(prm.dty, vy, ay);
+        // re-home the offsets into [0, 1)
+        const float dfx = floorf(ax), dfy = floorf(ay);
+        ax -= dfx;
+        ay -= dfy;
+        i += (int)dfx;
+        j += (int)dfy;
+        if (ax >= 1.f) { ax -= 1.f; ++i; }
+        if (ay >= 1.f) { ay -= 1.f; ++j; }
+        // walls, in the order and with the comparisons of k_push: x <= xmin,
+        // x > xmax, y < ymin, y > ymax on u = i + ax, v = j + ay
+        auto rehome = [](float u, int *ii, float *aa) {
+          const float f = floorf(u);
+          *ii = (int)f;
+          *aa = u - f;
+          if (*aa >= 1.f) { *aa -= 1.f; ++*ii; }
+        };
+        if (i < 0 || (i == 0 && ax == 0.f)) {
+          if (prm.wall[0] == PIC_WALL_REFLECT) { rehome(-((float)i + ax), &i, &ax); vx = -vx; }
+          else lost = true;
+        } else if (i > m.nex || (i == m.nex && ax > 0.f)) {
+          if (prm.wall[1] == PIC_WALL_REFLECT) {
+            int k2;
+            float a2;
+            rehome(-((float)(i - m.nex) + ax), &k2, &a2);
+            i = m.nex + k2;
+            ax = a2;
+            vx = -vx;
+          } else lost = true;
+        } else if (j < 0) {
+          if (prm.wall[2] == PIC_WALL_REFLECT) { rehome(-((float)j + ay), &j, &ay); vy = -vy; }
+          else lost = true;
+        } else if (j > m.ney || (j == m.ney && ay > 0.f)) {
+          if (prm.wall[3] == PIC_WALL_REFLECT) {
+            int k2;
+            float a2;
+            rehome(-((float)(j - m.ney) + ay), &k2, &a2);
+            j = m.ney + k2;
+            ay = a2;
+            vy = -vy;
+          } else lost = true;
+        }
+        // on the far walls: the last element, offset 1 (the clamp of GetParChg_2D.f90:143-149)
+        if (i == m.nex && ax == 0.f) { i = m.nex - 1; ax = 1.f; }
+        if (j == m.ney && ay == 0.f) { j = m.ney - 1; ay = 1.f; }
+        if (!lost && (i < 0 || i >= m.nex || j < 0 || j >= m.ney)) {
+          atomicAdd(s.bad, 1ull);  // still outside after one reflection
+          lost = true;
+        }
+        if (!lost) {
+          const double X = m.xmin + ((double)i + (double)ax) * m.hx;
+          const double Y = m.ymin + ((double)j + (double)ay) * m.hy;
+          if (absorbed_by_object(X, Y)) lost = true;
+        }
+        fx[p] = ax;
+        fy[p] = ay;
+        fvx[p] = vx;
+        fvy[p] = vy;
+      }
+      if (lost) {
+        s.loc[p] = -1;
+      } else {
+        const int en = i * m.ney + j;
+        if (prm.do_push) s.loc[p] = en;
+        if (prm.do_deposit) {
+          key = en;
+          const double dx = ax, dy = ay, xc = 1.0 - dx, yc = 1.0 - dy;
+          W[0] = xc * yc;
+          W[1] = dx * yc;
+          W[2] = dx * dy;
+          W[3] = xc * dy;
+          const int n1 = i * m.nny + j;
+          nodes[0] = n1;
+          nodes[1] = n1 + m.nny;
+          nodes[2] = n1 + m.nny + 1;
+          nodes[3] = n1 + 1;
+          if (prm.do_energy) {
+            const double vz = fvz[p], wx = vx, wy = vy;
+            energy = ((((0.5 * prm.mass) * ((wx * wx + wy * wy) + vz * vz)) * prm.vref) * prm.vref) / PIC_JTOEV;
+          }
+        }
+      }
+    }
+  }
+  warp_deposit(s, lane, key, W, nodes, energy, lost, prm.do_deposit, prm.do_energy);
+}
+
+// FP64 absolute particles (staging set) -> FP32 offsets inside the located
+// element and FP32 velocities (live set).  Slots with loc < 0 are copied as 0.
+__global__ void k_to_mixed(MeshK m, const double *__restrict__ x, const double *__restrict__ y,
+                           const double *__restrict__ vx, const double *__restrict__ vy,
+                           const double *__restrict__ vz, const int32_t *__restrict__ loc, float *__restrict__ ox,
+                           float *__restrict__ oy, float *__restrict__ ovx, float *__restrict__ ovy,
+                           float *__restrict__ ovz, int64_t n) {
+  const int64_t p = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (p >= n) return;
+  const int e = loc[p];
+  float a = 0.f, b = 0.f;
+  if (e >= 0) {
+    const int i = elem_column(m, e), j = e - i * m.ney;
+    a = (float)((x[p] - m.xs[i]) / (m.xs[i + 1] - m.xs[i]));
+    b = (float)((y[p] - m.ys[j]) / (m.ys[j + 1] - m.ys[j]));
+    a = fminf(fmaxf(a, 0.f), 1.f);
+    b = fminf(fmaxf(b, 0.f), 1.f);
+  }
+  ox[p] = a;
+  oy[p] = b;
+  ovx[p] = (float)vx[p];
+  ovy[p] = (float)vy[p];
+  ovz[p] = (float)vz[p];
+}
+
+// FP32 live set -> FP64 absolute positions and velocities (staging set).
+__global__ void k_from_mixed(MeshK m, const float *__restrict__ ax, const float *__restrict__ ay,
+                             const float *__restrict__ avx, const float *__restrict__ avy,
+                             const float *__restrict__ avz, const int32_t *__restrict__ loc, double *__restrict__ x,
+                             double *__restrict__ y, double *__restrict__ vx, double *__restrict__ vy,
+                             double *__restrict__ vz, int64_t n) {
+  const int64_t p = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (p >= n) return;
+  const int e = loc[p];
+  double X = 0.0, Y = 0.0;
+  if (e >= 0) {
+    const int i = elem_column(m, e), j = e - i * m.ney;
+    X = m.xmin + ((double)i + (double)ax[p]) * m.hx;
+    Y = m.ymin + ((double)j + (double)ay[p]) * m.hy;
+  }
+  x[p] = X;
+  y[p] = Y;
+  vx[p] = avx[p];
+  vy[p] = avy[p];
+  vz[p] = avz[p];
 }
 
 // ----------------------------------------------------------------------------
@@ -1478,6 +1686,7 @@ struct PprK {
   const double *rows;
   double *coef;  // [5][nn]
   double *efx, *efy;
+  float *coef32;  // NULL, or [nn][8] FP32 records (mixed precision)
   int nny;
   int64_t nn;
 };
@@ -1522,6 +1731,22 @@ __global__ void k_ppr(PprK k) {
   for (int r = 0; r < 5; ++r) k.coef[(size_t)r * k.nn + n] = c[r];
   k.efx[n] = -c[0];
   k.efy[n] = -c[1];
+  if (k.coef32) {  // mixed precision: one 32-byte FP32 record per node
+    float4 *o = reinterpret_cast<float4 *>(k.coef32 + 8 * (size_t)n);
+    o[0] = make_float4((float)-c[0], (float)-c[1], (float)c[0], (float)c[1]);
+    o[1] = make_float4((float)c[2], (float)c[3], (float)c[4], 0.0f);
+  }
+}
+
+// FP32 node records {efx, efy, c2, c3, c4, c5, c6, 0} from the FP64 fields
+// (mixed precision, after the caller set a field).
+__global__ void k_coef32(const double *__restrict__ efx, const double *__restrict__ efy,
+                         const double *__restrict__ coef, float *__restrict__ coef32, int64_t nn) {
+  int64_t n = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (n >= nn) return;
+  float4 *o = reinterpret_cast<float4 *>(coef32 + 8 * (size_t)n);
+  o[0] = make_float4((float)efx[n], (float)efy[n], (float)coef[n], (float)coef[nn + n]);
+  o[1] = make_float4((float)coef[2 * nn + n], (float)coef[3 * nn + n], (float)coef[4 * nn + n], 0.0f);
 }
 
 __global__ void k_fill_u64(unsigned long long *a, int64_t n) {
@@ -1630,7 +1855,7 @@ static void free_all() {
   F(g.d_phi_dir); F(g.d_cell_volume); F(g.d_rhs_fix); F(g.d_mass_q1); F(g.d_ife_mass);
   F(g.d_xt_ptr); F(g.d_xt_col); F(g.d_xt_val); F(g.d_row_kind); F(g.d_ex_cnt); F(g.d_ex_col);
   F(g.d_ex_val); F(g.d_diag); F(g.d_ppr_kind); F(g.d_ppr_ptr); F(g.d_ppr_nodes); F(g.d_ppr_rows);
-  F(g.d_ppr_h); F(g.d_phi); F(g.d_rho); F(g.d_efx); F(g.d_efy); F(g.d_coef); F(g.d_b); F(g.d_x);
+  F(g.d_ppr_h); F(g.d_phi); F(g.d_rho); F(g.d_efx); F(g.d_efy); F(g.d_coef); F(g.d_coef32); F(g.d_b); F(g.d_x);
   F(g.d_r); F(g.d_w); F(g.d_p[0]); F(g.d_p[1]); F(g.d_q); F(g.d_part); F(g.d_pcg); F(g.d_bar);
   F(g.d_z); F(g.d_dot); F(g.d_dot_ticket); F(g.d_fcg); F(g.d_fcg_P); F(g.d_fcg_Q); F(g.d_fcg_part);
   precond_free();
@@ -1686,7 +1911,49 @@ static int run_push(int sidx, bool do_push, bool do_deposit, bool do_energy) {
   for (int w = 0; w < 4; ++w) prm.wall[w] = g.P.wall_bc[w];
   SpK k{s.x, s.y, s.vx, s.vy, s.vz, s.loc, s.q_acc, s.e_acc, g.d_counters + 8 + sidx, g.d_counters + 1,
         s.n_slots};
-  k_push<<<blocks_for(s.n_slots, 256), 256, 0, g.st>>>(mesh_k(), f, prm, k);
+  if (s.f32) {
+    const MeshK m = mesh_k();
+    PushM pm;
+    pm.qmdt = (float)(s.qm * g.P.dt);
+    pm.dtx = (float)(g.P.dt / m.hx);
+    pm.dty = (float)(g.P.dt / m.hy);
+    pm.hx = (float)m.hx;
+    pm.hy = (float)m.hy;
+    pm.mass = s.mass;
+    pm.vref = g.v_ref;
+    pm.do_push = do_push;
+    pm.do_deposit = do_deposit;
+    pm.do_energy = do_deposit && do_energy;
+    for (int w = 0; w < 4; ++w) pm.wall[w] = g.P.wall_bc[w];
+    k_push_mixed<<<blocks_for(s.n_slots, 256), 256, 0, g.st>>>(m, g.d_coef32, pm, k);
+  } else {
+    k_push<<<blocks_for(s.n_slots, 256), 256, 0, g.st>>>(mesh_k(), f, prm, k);
+  }
+  PIC_LAUNCHED();
+  return PIC_OK;
+}
+
+// mixed precision: staging (FP64 absolute, set 2) <-> live (FP32 relative, set 1)
+static int to_mixed(Species &s) {
+  if (s.n_slots == 0) return PIC_OK;
+  // the FP64 data sits in the live set; convert into set 2 and swap
+  k_to_mixed<<<blocks_for(s.n_slots, 256), 256, 0, g.st>>>(
+      mesh_k(), s.x, s.y, s.vx, s.vy, s.vz, s.loc, (float *)s.x2, (float *)s.y2, (float *)s.vx2, (float *)s.vy2,
+      (float *)s.vz2, s.n_slots);
+  PIC_LAUNCHED();
+  std::swap(s.x, s.x2);
+  std::swap(s.y, s.y2);
+  std::swap(s.vx, s.vx2);
+  std::swap(s.vy, s.vy2);
+  std::swap(s.vz, s.vz2);
+  return PIC_OK;
+}
+
+static int from_mixed(Species &s) {
+  if (s.n_slots == 0) return PIC_OK;
+  k_from_mixed<<<blocks_for(s.n_slots, 256), 256, 0, g.st>>>(
+      mesh_k(), (const float *)s.x, (const float *)s.y, (const float *)s.vx, (const float *)s.vy,
+      (const float *)s.vz, s.loc, s.x2, s.y2, s.vx2, s.vy2, s.vz2, s.n_slots);
   PIC_LAUNCHED();
   return PIC_OK;
 }
@@ -2188,6 +2455,7 @@ static int run_ppr() {
   k.coef = g.d_coef;
   k.efx = g.d_efx;
   k.efy = g.d_efy;
+  k.coef32 = g.d_coef32;
   k.nny = g.m.nny;
   k.nn = g.nn;
   k_ppr<<<blocks_for(g.nn, 256), 256, 0, g.st>>>(k);
@@ -2356,6 +2624,10 @@ int pic_init(const pic_mesh_desc *mesh, const pic_params *params) {
       !(P.dt > 0) || !(P.n_ref > 0) || !(P.T_ref_eV > 0) || P.pcg_maxit < 1 || !(P.pcg_tol > 0) ||
       mesh->n_objects < 0 || mesh->n_objects > PIC_MAX_OBJECTS) {
     set_error("pic_init: bad mesh size or parameters");
+    return PIC_ERR_ARG;
+  }
+  if (P.precision != PIC_PREC_FP64 && P.precision != PIC_PREC_MIXED) {
+    set_error("pic_init: unknown precision");
     return PIC_ERR_ARG;
   }
   if (mesh->delta != 0) {
@@ -2646,6 +2918,11 @@ int pic_init(const pic_mesh_desc *mesh, const pic_params *params) {
   PIC_CUDA(cudaMemset(g.d_efx, 0, nn * sizeof(double)));
   PIC_CUDA(cudaMemset(g.d_efy, 0, nn * sizeof(double)));
   PIC_CUDA(cudaMemset(g.d_coef, 0, 5 * nn * sizeof(double)));
+  g.mixed = (P.precision == PIC_PREC_MIXED);
+  if (g.mixed) {
+    if ((rc = dalloc(&g.d_coef32, 8 * nn))) return rc;
+    PIC_CUDA(cudaMemset(g.d_coef32, 0, 8 * nn * sizeof(float)));
+  }
   PIC_CUDA(cudaMemset(g.d_rho, 0, nn * sizeof(double)));
   PIC_CUDA(cudaMemcpy(g.d_phi, mesh->phi_dirichlet, nn * sizeof(double), cudaMemcpyHostToDevice));
   for (double **v : {&g.d_b, &g.d_x, &g.d_r, &g.d_w, &g.d_p[0], &g.d_p[1], &g.d_q}) {
@@ -2732,6 +3009,7 @@ int pic_init(const pic_mesh_desc *mesh, const pic_params *params) {
     sp.weight = d.weight;
     sp.qm = d.charge / (d.mass / PIC_ME);
     sp.capacity = d.capacity;
+    sp.f32 = (P.precision == PIC_PREC_MIXED);
     maxcap = std::max(maxcap, d.capacity);
     size_t c = (size_t)std::max<int64_t>(d.capacity, 1);
     for (double **v : {&sp.x, &sp.y, &sp.vx, &sp.vy, &sp.vz, &sp.x2, &sp.y2, &sp.vx2, &sp.vy2, &sp.vz2})
@@ -2809,6 +3087,7 @@ int pic_upload_particles(int32_t species, int64_t n, const double *x, const doub
       return PIC_ERR_DOMAIN;
     }
   }
+  if (s.f32 && (rc = to_mixed(s))) return rc;
   return PIC_OK;
 }
 
@@ -2845,8 +3124,18 @@ int pic_download_particles(int32_t species, int64_t capacity, double *x, double 
       if (hl[k] >= 0) std::memcpy((char *)dst + (o++) * esz, tmp.data() + k * esz, esz);
     return PIC_OK;
   };
-  if ((rc = pull(s.x, x, 8)) || (rc = pull(s.y, y, 8)) || (rc = pull(s.vx, vx, 8)) ||
-      (rc = pull(s.vy, vy, 8)) || (rc = pull(s.vz, vz, 8)) || (rc = pull(s.loc, loc, 4)) ||
+  const double *sx = s.x, *sy = s.y, *svx = s.vx, *svy = s.vy, *svz = s.vz;
+  if (s.f32) {  // absolute FP64 values into the staging set
+    if ((rc = from_mixed(s))) return rc;
+    PIC_CUDA(cudaStreamSynchronize(g.st));
+    sx = s.x2;
+    sy = s.y2;
+    svx = s.vx2;
+    svy = s.vy2;
+    svz = s.vz2;
+  }
+  if ((rc = pull(sx, x, 8)) || (rc = pull(sy, y, 8)) || (rc = pull(svx, vx, 8)) ||
+      (rc = pull(svy, vy, 8)) || (rc = pull(svz, vz, 8)) || (rc = pull(s.loc, loc, 4)) ||
       (rc = pull(s.id, id, 4)))
     return rc;
   return PIC_OK;
@@ -2870,8 +3159,8 @@ int pic_particle_positioning(int32_t species) {
   int s0 = species < 0 ? 0 : species, s1 = species < 0 ? g.ns : species + 1;
   if (species >= 0 && (rc = check_species(species))) return rc;
   if ((rc = zero_counter(1))) return rc;
-  for (int s = s0; s < s1; ++s)
-    if ((rc = launch_locate(g.sp[s], 0, g.sp[s].n_slots))) return rc;
+  for (int s = s0; s < s1; ++s)  // mixed precision: the element is part of the position
+    if (!g.sp[s].f32 && (rc = launch_locate(g.sp[s], 0, g.sp[s].n_slots))) return rc;
   unsigned long long bad = 0;
   if ((rc = read_counter(1, &bad))) return rc;
   if (bad) {
@@ -3081,6 +3370,10 @@ int pic_set_field(int32_t which, const double *host_in) {
     return PIC_ERR_ARG;
   }
   PIC_CUDA(cudaMemcpyAsync(dst, host_in, g.nn * sizeof(double), cudaMemcpyHostToDevice, g.st));
+  if (g.mixed && (which == 2 || which == 3 || which >= 12)) {
+    k_coef32<<<blocks_for(g.nn, 256), 256, 0, g.st>>>(g.d_efx, g.d_efy, g.d_coef, g.d_coef32, g.nn);
+    PIC_LAUNCHED();
+  }
   PIC_CUDA(cudaStreamSynchronize(g.st));
   return PIC_OK;
 }

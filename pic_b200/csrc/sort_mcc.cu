@@ -142,16 +142,20 @@ __global__ void k_gather(const T *__restrict__ src, T *__restrict__ dst, const i
   if (i < n) dst[i] = src[perm[i]];
 }
 
+// T = double (FP64 particles) or float (mixed precision: offsets in the
+// element and velocities, in the first half of the same storage)
+template <class T>
 struct Gather7 {
-  const double *x, *y, *vx, *vy, *vz;
+  const T *x, *y, *vx, *vy, *vz;
   const int32_t *loc;
   const uint32_t *id;
-  double *ox, *oy, *ovx, *ovy, *ovz;
+  T *ox, *oy, *ovx, *ovy, *ovz;
   int32_t *oloc;
   uint32_t *oid;
 };
 
-__global__ void k_gather_all(Gather7 g7, const int32_t *__restrict__ perm, int64_t n) {
+template <class T>
+__global__ void k_gather_all(Gather7<T> g7, const int32_t *__restrict__ perm, int64_t n) {
   int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= n) return;
   int32_t p = perm[i];
@@ -184,8 +188,15 @@ int sort_species(int sidx) {
   PIC_LAUNCHED();
   PIC_CUDA(cudaStreamSynchronize(g.st));
   if (total > 0) {
-    Gather7 g7{s.x, s.y, s.vx, s.vy, s.vz, s.loc, s.id, s.x2, s.y2, s.vx2, s.vy2, s.vz2, s.loc2, s.id2};
-    k_gather_all<<<blocks_for(total, 256), 256, 0, g.st>>>(g7, g.d_perm2, total);
+    if (s.f32) {
+      auto F = [](double *v) { return reinterpret_cast<float *>(v); };
+      Gather7<float> g7{F(s.x), F(s.y), F(s.vx), F(s.vy), F(s.vz), s.loc, s.id,
+                        F(s.x2), F(s.y2), F(s.vx2), F(s.vy2), F(s.vz2), s.loc2, s.id2};
+      k_gather_all<float><<<blocks_for(total, 256), 256, 0, g.st>>>(g7, g.d_perm2, total);
+    } else {
+      Gather7<double> g7{s.x, s.y, s.vx, s.vy, s.vz, s.loc, s.id, s.x2, s.y2, s.vx2, s.vy2, s.vz2, s.loc2, s.id2};
+      k_gather_all<double><<<blocks_for(total, 256), 256, 0, g.st>>>(g7, g.d_perm2, total);
+    }
     PIC_LAUNCHED();
   }
   std::swap(s.x, s.x2);
@@ -205,12 +216,22 @@ int sort_species(int sidx) {
 // ---------------------------------------------------------------------------
 
 struct MccK {
-  double *x, *y, *vx, *vy, *vz;
+  double *x, *y, *vx, *vy, *vz;  // FP32 data in the same storage when f32
   const int32_t *loc;
   const uint32_t *id;
   int64_t n;
   uint32_t seed0, seed1, step_lo, step_hi, species;
+  int f32;
 };
+
+__device__ __forceinline__ double mcc_get(const double *a, int f32, int64_t p) {
+  return f32 ? (double)reinterpret_cast<const float *>(a)[p] : a[p];
+}
+
+__device__ __forceinline__ void mcc_put(double *a, int f32, int64_t p, double v) {
+  if (f32) reinterpret_cast<float *>(a)[p] = (float)v;
+  else a[p] = v;
+}
 
 __global__ void k_mcc_hist(MccK k, uint32_t *__restrict__ hist) {
   int64_t p = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
@@ -258,16 +279,16 @@ __global__ void k_mcc_collide(CollK c) {
   if (t >= c.n_sel) return;
   int32_t p = c.sel[t];
   McParticle P;
-  P.vx = c.k.vx[p] * c.vref;
-  P.vy = c.k.vy[p] * c.vref;
-  P.vz = c.k.vz[p] * c.vref;
+  P.vx = mcc_get(c.k.vx, c.k.f32, p) * c.vref;
+  P.vy = mcc_get(c.k.vy, c.k.f32, p) * c.vref;
+  P.vz = mcc_get(c.k.vz, c.k.f32, p) * c.vref;
   McOut out;
   McRng rng;
   mc_rng_init(&rng, c.k.id[p], c.k.step_lo, c.k.step_hi, c.k.species, c.k.seed0, c.k.seed1);
   mc_collide(&P, &c.tab, c.prob, &c.gas, c.mass, &rng, &out);
-  c.k.vx[p] = P.vx / c.vref;
-  c.k.vy[p] = P.vy / c.vref;
-  c.k.vz[p] = P.vz / c.vref;
+  mcc_put(c.k.vx, c.k.f32, p, P.vx / c.vref);
+  mcc_put(c.k.vy, c.k.f32, p, P.vy / c.vref);
+  mcc_put(c.k.vz, c.k.f32, p, P.vz / c.vref);
   if (out.reaction > 0) atomicAdd((unsigned long long *)&c.misc[2 + out.reaction - 1], 1ull);
   if (out.ionised) {
     long long i = atomicAdd((unsigned long long *)&c.misc[12], 1ull);
@@ -295,6 +316,7 @@ struct AppendK {
   const int32_t *parent_slot;  // in rank order
   const double *vel;           // 3 per created particle, normalised
   int64_t n;
+  int f32;                     // both species mixed precision: FP32 offsets/velocities
 };
 
 __global__ void k_mcc_append(AppendK a) {
@@ -302,11 +324,16 @@ __global__ void k_mcc_append(AppendK a) {
   if (r >= a.n) return;
   int32_t ps = a.parent_slot[r];
   int64_t d = a.base + r;
-  a.x[d] = a.px[ps];
-  a.y[d] = a.py[ps];
-  a.vx[d] = a.vel[3 * r + 0];
-  a.vy[d] = a.vel[3 * r + 1];
-  a.vz[d] = a.vel[3 * r + 2];
+  if (a.f32) {  // the parent's element and offsets are the new particle's position
+    reinterpret_cast<float *>(a.x)[d] = reinterpret_cast<const float *>(a.px)[ps];
+    reinterpret_cast<float *>(a.y)[d] = reinterpret_cast<const float *>(a.py)[ps];
+  } else {
+    a.x[d] = a.px[ps];
+    a.y[d] = a.py[ps];
+  }
+  mcc_put(a.vx, a.f32, d, a.vel[3 * r + 0]);
+  mcc_put(a.vy, a.f32, d, a.vel[3 * r + 1]);
+  mcc_put(a.vz, a.f32, d, a.vel[3 * r + 2]);
   a.loc[d] = a.ploc[ps];
   a.id[d] = a.id_base + (uint32_t)r;
 }
@@ -348,7 +375,8 @@ int mcc_run(uint64_t step, pic_mcc_stats *stats) {
     if (ncoll <= 0) continue;
     int rc = mcc_alloc(ncoll + 4096);
     if (rc) return rc;
-    MccK k{sp.x, sp.y, sp.vx, sp.vy, sp.vz, sp.loc, sp.id, sp.n_slots, seed0, seed1, slo, shi, (uint32_t)s};
+    MccK k{sp.x, sp.y, sp.vx, sp.vy, sp.vz, sp.loc, sp.id, sp.n_slots, seed0, seed1, slo, shi, (uint32_t)s,
+           sp.f32 ? 1 : 0};
     PIC_CUDA(cudaMemsetAsync(g.d_hist, 0, 65536 * sizeof(uint32_t), g.st));
     PIC_CUDA(cudaMemsetAsync(g.d_mcc_misc, 0, 16 * sizeof(int64_t), g.st));
     k_mcc_hist<<<blocks_for(sp.n_slots, 256), 256, 0, g.st>>>(k, g.d_hist);
@@ -472,7 +500,7 @@ int mcc_run(uint64_t step, pic_mcc_stats *stats) {
           vel[3 * i + q] = which == 0 ? pd.data[6 * i + q] : pd.data[6 * i + 3 + q] / g.v_ref;
       PIC_CUDA(cudaMemcpy(d_vel, vel.data(), 3 * nion * 8, cudaMemcpyHostToDevice));
       AppendK a{from.x, from.y, from.loc, to.x, to.y, to.vx, to.vy, to.vz, to.loc, to.id,
-                to.n_slots, to.next_id, d_pslot, d_vel, nion};
+                to.n_slots, to.next_id, d_pslot, d_vel, nion, to.f32 ? 1 : 0};
       k_mcc_append<<<blocks_for(nion, 256), 256, 0, g.st>>>(a);
       PIC_LAUNCHED();
       PIC_CUDA(cudaStreamSynchronize(g.st));
