@@ -1,7 +1,7 @@
 """Small, self-contained workloads for profiling one part of the step under
 ncu (each runs a few launches of its kernels and exits):
 
-    python -m pic_b200.profile_cases step  <deck> <ppc> <steps> [jpcg|fcg]
+    python -m pic_b200.profile_cases step  <deck> <ppc> <steps> [jpcg|fcg] [fp64|mixed]
     python -m pic_b200.profile_cases solve <cells> [jpcg|fcg] [repeats] [coarse_cells]
     python -m pic_b200.profile_cases unet  <nodes> [repeats]
 
@@ -19,11 +19,12 @@ import sys
 import numpy as np
 
 
-def _step(deck_name, ppc, steps, solver="fcg"):
+def _step(deck_name, ppc, steps, solver="fcg", precision="fp64"):
     import torch
-    from . import deck
+    from . import api, deck
     from .simulation import Simulation
-    cfg = deck.config(deck_name, ppc=int(ppc))
+    prec = api.PIC_PREC_MIXED if precision == "mixed" else api.PIC_PREC_FP64
+    cfg = deck.config(deck_name, ppc=int(ppc), precision=prec)
     sim = Simulation(cfg)
     sim.initial_fields()
     if solver != "jpcg":
@@ -36,7 +37,7 @@ def _step(deck_name, ppc, steps, solver="fcg"):
         sim.step()
     e1.record()
     torch.cuda.synchronize()
-    print(f"step {cfg.name} ppc={ppc} solver={solver}: {e0.elapsed_time(e1) / int(steps):.3f} ms/step")
+    print(f"step {cfg.name} ppc={ppc} solver={solver} {precision}: {e0.elapsed_time(e1) / int(steps):.3f} ms/step")
     sim.close()
 
 
