@@ -37,6 +37,7 @@ struct MeshK {
   const double *xs, *ys;          // node coordinates (x_s + h_x*(i))
   const int32_t *element_index;   // [ne]
   const int32_t *node_index;      // [nn]
+  const uint8_t *elem_near;       // [ne] 1: the element's box meets an object's box
 };
 
 struct ObjK {
@@ -100,6 +101,7 @@ struct Ctx {
   // mesh
   double *d_xs = nullptr, *d_ys = nullptr;
   int32_t *d_element_index = nullptr, *d_node_index = nullptr, *d_node_type = nullptr;
+  uint8_t *d_elem_near = nullptr;
   double *d_phi_dir = nullptr, *d_cell_volume = nullptr, *d_rhs_fix = nullptr;
   double *d_mass_q1 = nullptr, *d_ife_mass = nullptr;
   int32_t *d_xt_ptr = nullptr, *d_xt_col = nullptr;  // per unknown row, 0-based node columns

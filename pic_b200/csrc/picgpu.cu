@@ -206,6 +206,28 @@ __device__ __forceinline__ void warp_deposit(const SpK &s, int lane, int key, co
   unsigned int lm = __ballot_sync(0xffffffffu, lost);
   if (lane == 0 && lm) atomicAdd(s.lost, (unsigned long long)__popc(lm));
   if (!do_deposit) return;
+  if (__all_sync(0xffffffffu, key >= 0 && key == __shfl_sync(0xffffffffu, key, 0))) {
+    // one element for the whole warp: exact integer warp sums with redux on
+    // the low 24 bits and the rest (values are non-negative; the sums fit in
+    // 32 bits for values below 2^51, i.e. particle energies below ~5e5 eV)
+    auto wsum = [&](long long v) {
+      const unsigned lo = (unsigned)(v & 0xffffff), hi = (unsigned)(v >> 24);
+      return ((long long)__reduce_add_sync(0xffffffffu, hi) << 24) + (long long)__reduce_add_sync(0xffffffffu, lo);
+    };
+    long long qv[4];
+#pragma unroll
+    for (int c = 0; c < 4; ++c) qv[c] = wsum(__double2ll_rn(W[c] * PIC_Q_SCALE));
+    if (lane == 0)
+#pragma unroll
+      for (int c = 0; c < 4; ++c) atomicAdd(s.q_acc + nodes[c], (unsigned long long)qv[c]);
+    if (!do_energy) return;
+#pragma unroll
+    for (int c = 0; c < 4; ++c) qv[c] = wsum(__double2ll_rn((W[c] * energy) * PIC_E_SCALE));
+    if (lane == 0)
+#pragma unroll
+      for (int c = 0; c < 4; ++c) atomicAdd(s.e_acc + nodes[c], (unsigned long long)qv[c]);
+    return;
+  }
   int prev = __shfl_up_sync(0xffffffffu, key, 1);
   bool head = (lane == 0) || (key != prev);
   unsigned int heads = __ballot_sync(0xffffffffu, head);
@@ -436,7 +458,7 @@ __global__ void __launch_bounds__(256, 4) k_push_mixed(MeshK m, const float *__r
           atomicAdd(s.bad, 1ull);  // still outside after one reflection
           lost = true;
         }
-        if (!lost) {
+        if (!lost && m.elem_near[i * m.ney + j]) {
           const double X = m.xmin + ((double)i + (double)ax) * m.hx;
           const double Y = m.ymin + ((double)j + (double)ay) * m.hy;
           if (absorbed_by_object(X, Y)) lost = true;
@@ -1764,6 +1786,7 @@ static MeshK mesh_k() {
   m.ys = g.d_ys;
   m.element_index = g.d_element_index;
   m.node_index = g.d_node_index;
+  m.elem_near = g.d_elem_near;
   return m;
 }
 
@@ -1851,7 +1874,7 @@ static void free_all() {
   auto F = [](void *p) {
     if (p) cudaFree(p);
   };
-  F(g.d_xs); F(g.d_ys); F(g.d_element_index); F(g.d_node_index); F(g.d_node_type);
+  F(g.d_xs); F(g.d_ys); F(g.d_element_index); F(g.d_node_index); F(g.d_node_type); F(g.d_elem_near);
   F(g.d_phi_dir); F(g.d_cell_volume); F(g.d_rhs_fix); F(g.d_mass_q1); F(g.d_ife_mass);
   F(g.d_xt_ptr); F(g.d_xt_col); F(g.d_xt_val); F(g.d_row_kind); F(g.d_ex_cnt); F(g.d_ex_col);
   F(g.d_ex_val); F(g.d_diag); F(g.d_ppr_kind); F(g.d_ppr_ptr); F(g.d_ppr_nodes); F(g.d_ppr_rows);
@@ -2674,6 +2697,29 @@ int pic_init(const pic_mesh_desc *mesh, const pic_params *params) {
   if ((rc = upload(&g.d_xs, xs.data(), xs.size()))) return rc;
   if ((rc = upload(&g.d_ys, ys.data(), ys.size()))) return rc;
   if ((rc = upload(&g.d_element_index, mesh->element_index, ne))) return rc;
+  {
+    // elements whose box meets an object's bounding box: only particles in
+    // them can be inside an object (the mixed push tests objects there only)
+    std::vector<uint8_t> near(ne, 0);
+    const double hx = (mesh->xmax - mesh->xmin) / (mesh->nnx - 1), hy = (mesh->ymax - mesh->ymin) / (mesh->nny - 1);
+    for (int k = 0; k < mesh->n_objects; ++k) {
+      const pic_object &o = mesh->objects[k];
+      double x0, x1, y0, y1;
+      if (o.shape == PIC_SHAPE_BOX) {
+        x0 = o.cx; x1 = o.a; y0 = o.cy; y1 = o.b;
+      } else {
+        const double hw = std::max(std::fabs(o.a), std::fabs(o.b)) * (1.0 + 1e-9);
+        x0 = o.cx - hw; x1 = o.cx + hw; y0 = o.cy - hw; y1 = o.cy + hw;
+      }
+      const int i0 = std::max(0, (int)std::floor((x0 - mesh->xmin) / hx) - 1);
+      const int i1 = std::min(mesh->nnx - 2, (int)std::floor((x1 - mesh->xmin) / hx) + 1);
+      const int j0 = std::max(0, (int)std::floor((y0 - mesh->ymin) / hy) - 1);
+      const int j1 = std::min(mesh->nny - 2, (int)std::floor((y1 - mesh->ymin) / hy) + 1);
+      for (int i = i0; i <= i1; ++i)
+        for (int j = j0; j <= j1; ++j) near[(size_t)i * (mesh->nny - 1) + j] = 1;
+    }
+    if ((rc = upload(&g.d_elem_near, near.data(), ne))) return rc;
+  }
   if ((rc = upload(&g.d_node_index, mesh->node_index, nn))) return rc;
   if ((rc = upload(&g.d_node_type, mesh->node_type, nn))) return rc;
   if ((rc = upload(&g.d_phi_dir, mesh->phi_dirichlet, nn))) return rc;
