@@ -206,7 +206,8 @@ __device__ __forceinline__ void warp_deposit(const SpK &s, int lane, int key, co
   unsigned int lm = __ballot_sync(0xffffffffu, lost);
   if (lane == 0 && lm) atomicAdd(s.lost, (unsigned long long)__popc(lm));
   if (!do_deposit) return;
-  if (__all_sync(0xffffffffu, key >= 0 && key == __shfl_sync(0xffffffffu, key, 0))) {
+  const int key0 = __shfl_sync(0xffffffffu, key, 0);  // every lane, before any test
+  if (__all_sync(0xffffffffu, key >= 0 && key == key0)) {
     // one element for the whole warp: exact integer warp sums with redux on
     // the low 24 bits and the rest (values are non-negative; the sums fit in
     // 32 bits for values below 2^51, i.e. particle energies below ~5e5 eV)
