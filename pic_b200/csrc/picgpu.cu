@@ -1481,27 +1481,29 @@ __global__ void __launch_bounds__(PIC_RED_THREADS) k_fcg_upd(FcgK k) {
 
 // ---- persistent flexible CG (window 1, classical stages) -------------------
 // The whole solve in one cooperative kernel of kWide-thread CTAs: per
-// iteration the phases below, separated by the bounded grid barrier of the
+// iteration six phases, separated by the bounded grid barrier of the
 // persistent Jacobi-PCG.  Scalars (beta, alpha, r.r) are formed by every CTA
 // from the chunk partials in the canonical order, so all CTAs take the same
 // decisions.  Phases:
-//   (1) zA = w D^-1 r, t = r - A zA          (pre-smoothing)
-//   (2) rc = P^T t                             (restriction, warp per coarse node)
-//   (3) ec = Ac^-1 rc                          (GEMV, warp per row)
-//   (4) zA += P ec                             (prolongation)
-//   (5) zF = zA + w D^-1 (r - A zA), zF.Q_old  (post-smoothing)
-//   (6) P_new = zF + beta P_old
-//   (7) Q_new = A P_new, p.q, p.r
-//   (8) x += alpha P_new, r -= alpha Q_new, r.r
-// Without a coarse space phases 2-4 are skipped.  Loads after a grid barrier
-// are plain (L1-cached) loads: the barrier's release/acquire pair orders
-// every CTA's writes before them, and a stencil reads each value up to nine
-// times, from L1.
+//   (A) x += alpha P, r' = r - alpha Q (previous direction; r ping-pongs,
+//       r' is formed at the neighbours), r'.r', then pre-smoothing
+//       zA = w D^-1 r', t = r' - A zA
+//   (B) rc = P^T t                             (restriction, warp per coarse node)
+//   (C) ec = Ac^-1 rc                          (GEMV, warp per row)
+//   (D) zA += P ec                             (prolongation)
+//   (E) zF = zA + w D^-1 (r - A zA), zF.Q_old  (post-smoothing)
+//   (F) P_new = zF + beta P_old formed at the neighbours, Q_new = A P_new,
+//       p.q, p.r
+// The convergence test on r'.r' follows phase A.  Without a coarse space
+// phases B-D are skipped.  Loads after a grid barrier are plain (L1-cached)
+// loads: the barrier's release/acquire pair orders every CTA's writes before
+// them, and a stencil reads each value up to nine times, from L1.
 struct FcgP {
   PcgK k;                        // operator, x, r
+  double *r2;                    // second residual buffer (ping-pong)
   const double *dinv;
   double *zA, *t, *zF, *P0, *P1, *Q0, *Q1;
-  double *part;                  // [2][nb] chunk partials
+  double *part;                  // [4][nb] chunk partials: F p.q, F p.r, A r.r, E zF.Q
   const float *ainv;
   double *rc, *ec;
   int nnx, cs, ncx, ncy, coarse;
@@ -1522,59 +1524,96 @@ __global__ void __launch_bounds__(kWide, 1) k_fcg_persist(FcgP F) {
   const double rhs = S->rhs, tol2 = S->tol2, omega = F.omega;
   const int maxit = S->maxit, stall_window = S->stall_window;
   int iter = S->iter, ierr = 0, best_iter = S->best_iter;
-  double rr = S->rr, best = S->best, pq_old = 0.0;
+  double rr = S->rr, best = S->best, pq_old = 0.0, alpha = 0.0;
   bool have_old = false, ok = true;
   int parity = 0;
+  double *rc_ = k.r, *rn_ = F.r2;  // current residual, next residual
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
   const int gwarp = blockIdx.x * (kWide / 32) + warp, nwarps = gridDim.x * (kWide / 32);
   const int nc = F.ncx * F.ncy;
   auto barrier = [&]() { return grid_barrier(F.bar, F.bar_err, F.spin_limit, F.bar_extra); };
   for (;;) {
+    // the previous direction (written last iteration), the new one
+    const double *Pl = parity ? F.P0 : F.P1, *Ql = parity ? F.Q0 : F.Q1;
     double *Pn = parity ? F.P1 : F.P0, *Qn = parity ? F.Q1 : F.Q0;
-    const double *Po = parity ? F.P0 : F.P1, *Qo = parity ? F.Q0 : F.Q1;
-    // (1) pre-smoothing
-    for (int c = blockIdx.x; c < nb; c += gridDim.x) {
-      const int64_t n = (int64_t)c * kWide + threadIdx.x;
-      if (n < nn) {
-        if (k.row_kind[n] < 0) {
-          F.zA[n] = 0.0;
-          F.t[n] = 0.0;
-        } else {
-          auto z1 = [&](int64_t m) { return (omega * k.r[m]) * F.dinv[m]; };
-          F.zA[n] = z1(n);
-          F.t[n] = k.r[n] - row_apply(k, n, z1);
+    // (A) update with the previous direction, then pre-smoothing
+    {
+      const double *r = rc_, *Qp = Ql;
+      const double a = alpha;
+      const bool upd = have_old;
+      auto rnew = [&](int64_t m) { return upd ? fma(-a, Qp[m], r[m]) : r[m]; };
+      for (int c = blockIdx.x; c < nb; c += gridDim.x) {
+        const int64_t base = (int64_t)c * kWide;
+        const int nvalid = (int)min((int64_t)kWide, nn - base);
+        const int64_t n = base + threadIdx.x;
+        double rv = 0.0;
+        if (threadIdx.x < nvalid) {
+          rv = rnew(n);
+          if (upd) {
+            k.x[n] = fma(a, Pl[n], k.x[n]);
+            rn_[n] = rv;
+          }
+          if (k.row_kind[n] < 0) {
+            F.zA[n] = 0.0;
+            F.t[n] = 0.0;
+          } else {
+            auto z1 = [&](int64_t m) { return (omega * rnew(m)) * F.dinv[m]; };
+            F.zA[n] = z1(n);
+            F.t[n] = rv - row_apply(k, n, z1);
+          }
+        }
+        if (upd) {
+          sa[0][threadIdx.x] = rv;
+          sb[0][threadIdx.x] = rv;
+          __syncthreads();
+          double part[1];
+          chunk_dots<1>(sa, sb, nvalid, part);
+          if (threadIdx.x == 0) F.part[2 * nb + c] = part[0];
         }
       }
-    }
-    if (F.coarse) {
       if (!(ok = barrier())) break;
-      // (2) restriction
+      if (upd) {
+        final_sum_wide<1>(F.part + 2 * nb, nb, &rr);
+        ++iter;
+        double *tmp = rc_;
+        rc_ = rn_;
+        rn_ = tmp;
+        if (!(rr == rr)) { ierr = 4; break; }
+        if (rr / rhs <= tol2) break;
+        if (iter >= maxit) { ierr = 1; break; }
+        if (rr < best) { best = rr; best_iter = iter; }
+        if (iter - best_iter > stall_window || rr > 1e6 * best) { ierr = 3; break; }
+      }
+    }
+    const double *r = rc_;
+    if (F.coarse) {
+      // (B) restriction
       for (int C = gwarp; C < nc; C += nwarps) {
         const int I = C / F.ncy, J = C % F.ncy;
         const int i0 = max(0, (I - 1) * F.cs + 1), i1 = min(F.nnx - 1, (I + 1) * F.cs - 1);
         const int j0 = max(0, (J - 1) * F.cs + 1), j1 = min(k.nny - 1, (J + 1) * F.cs - 1);
         const int ni = i1 - i0 + 1, nj = j1 - j0 + 1;
         const double inv = 1.0 / F.cs;
-        double a = 0.0;
+        double acc = 0.0;
         for (int e = lane; e < ni * nj; e += 32) {
           const int i = i0 + e / nj, j = j0 + e % nj;
           const double w = (1.0 - fabs((double)(i - I * F.cs)) * inv) * (1.0 - fabs((double)(j - J * F.cs)) * inv);
-          a = fma(w, F.t[(int64_t)i * k.nny + j], a);
+          acc = fma(w, F.t[(int64_t)i * k.nny + j], acc);
         }
-        for (int off = 16; off > 0; off >>= 1) a += __shfl_xor_sync(0xffffffffu, a, off);
-        if (lane == 0) F.rc[C] = a;
+        for (int off = 16; off > 0; off >>= 1) acc += __shfl_xor_sync(0xffffffffu, acc, off);
+        if (lane == 0) F.rc[C] = acc;
       }
       if (!(ok = barrier())) break;
-      // (3) coarse solve
+      // (C) coarse solve
       for (int row = gwarp; row < nc; row += nwarps) {
         const float *arow = F.ainv + (size_t)row * nc;
-        double a = 0.0;
-        for (int q = lane; q < nc; q += 32) a = fma((double)arow[q], __ldcg(F.rc + q), a);
-        for (int off = 16; off > 0; off >>= 1) a += __shfl_xor_sync(0xffffffffu, a, off);
-        if (lane == 0) F.ec[row] = a;
+        double acc = 0.0;
+        for (int q = lane; q < nc; q += 32) acc = fma((double)arow[q], __ldcg(F.rc + q), acc);
+        for (int off = 16; off > 0; off >>= 1) acc += __shfl_xor_sync(0xffffffffu, acc, off);
+        if (lane == 0) F.ec[row] = acc;
       }
       if (!(ok = barrier())) break;
-      // (4) prolongation
+      // (D) prolongation
       for (int c = blockIdx.x; c < nb; c += gridDim.x) {
         const int64_t n = (int64_t)c * kWide + threadIdx.x;
         if (n < nn && k.row_kind[n] >= 0) {
@@ -1591,7 +1630,7 @@ __global__ void __launch_bounds__(kWide, 1) k_fcg_persist(FcgP F) {
       }
     }
     if (!(ok = barrier())) break;
-    // (5) post-smoothing and zF.Q_old
+    // (E) post-smoothing and zF.Q_old (Q_old is this iteration's Ql)
     for (int c = blockIdx.x; c < nb; c += gridDim.x) {
       const int64_t base = (int64_t)c * kWide;
       const int nvalid = (int)min((int64_t)kWide, nn - base);
@@ -1600,57 +1639,55 @@ __global__ void __launch_bounds__(kWide, 1) k_fcg_persist(FcgP F) {
       if (threadIdx.x < nvalid) {
         if (k.row_kind[n] >= 0) {
           auto za = [&](int64_t m) { return F.zA[m]; };
-          zf = fma(omega * F.dinv[n], k.r[n] - row_apply(k, n, za), za(n));
+          zf = fma(omega * F.dinv[n], r[n] - row_apply(k, n, za), za(n));
         }
         F.zF[n] = zf;
-        if (have_old) qo = __ldcg(Qo + n);
+        if (have_old) qo = Ql[n];
       }
       sa[0][threadIdx.x] = zf;
       sb[0][threadIdx.x] = qo;
       __syncthreads();
       double part[1];
       chunk_dots<1>(sa, sb, nvalid, part);
-      if (threadIdx.x == 0) F.part[c] = part[0];
+      if (threadIdx.x == 0) F.part[3 * nb + c] = part[0];
     }
     if (!(ok = barrier())) break;
     double beta = 0.0;
     if (have_old) {
+      // its own region: phase F writes [0, 2 nb) while slower CTAs may still read this
       double zq;
-      final_sum_wide<1>(F.part, nb, &zq);
+      final_sum_wide<1>(F.part + 3 * nb, nb, &zq);
       beta = -zq / pq_old;
     }
-    // (6) new direction
-    for (int c = blockIdx.x; c < nb; c += gridDim.x) {
-      const int64_t n = (int64_t)c * kWide + threadIdx.x;
-      if (n < nn) {
-        double pv = 0.0;
-        if (k.row_kind[n] >= 0) pv = have_old ? fma(beta, __ldcg(Po + n), __ldcg(F.zF + n)) : __ldcg(F.zF + n);
-        Pn[n] = pv;
-      }
-    }
-    if (!(ok = barrier())) break;
-    // (7) Q_new = A P_new, p.q, p.r
-    for (int c = blockIdx.x; c < nb; c += gridDim.x) {
-      const int64_t base = (int64_t)c * kWide;
-      const int nvalid = (int)min((int64_t)kWide, nn - base);
-      const int64_t n = base + threadIdx.x;
-      double pv = 0.0, qv = 0.0, rv = 0.0;
-      if (threadIdx.x < nvalid) {
-        pv = Pn[n];
-        qv = row_apply(k, n, [&](int64_t m) { return Pn[m]; });
-        Qn[n] = qv;
-        rv = __ldcg(k.r + n);
-      }
-      sa[0][threadIdx.x] = pv;
-      sb[0][threadIdx.x] = qv;
-      sa[1][threadIdx.x] = pv;
-      sb[1][threadIdx.x] = rv;
-      __syncthreads();
-      double part[2];
-      chunk_dots<2>(sa, sb, nvalid, part);
-      if (threadIdx.x == 0) {
-        F.part[c] = part[0];
-        F.part[nb + c] = part[1];
+    // (F) P_new = zF + beta P_old at every neighbour (0 on Dirichlet nodes,
+    // where zF and P_old are 0), Q_new = A P_new, p.q, p.r
+    {
+      const double bt = beta;
+      const bool ho = have_old;
+      auto pnew = [&](int64_t m) { return ho ? fma(bt, Pl[m], F.zF[m]) : F.zF[m]; };
+      for (int c = blockIdx.x; c < nb; c += gridDim.x) {
+        const int64_t base = (int64_t)c * kWide;
+        const int nvalid = (int)min((int64_t)kWide, nn - base);
+        const int64_t n = base + threadIdx.x;
+        double pv = 0.0, qv = 0.0, rv = 0.0;
+        if (threadIdx.x < nvalid) {
+          pv = pnew(n);
+          qv = row_apply(k, n, pnew);
+          Pn[n] = pv;
+          Qn[n] = qv;
+          rv = r[n];
+        }
+        sa[0][threadIdx.x] = pv;
+        sb[0][threadIdx.x] = qv;
+        sa[1][threadIdx.x] = pv;
+        sb[1][threadIdx.x] = rv;
+        __syncthreads();
+        double part[2];
+        chunk_dots<2>(sa, sb, nvalid, part);
+        if (threadIdx.x == 0) {
+          F.part[c] = part[0];
+          F.part[nb + c] = part[1];
+        }
       }
     }
     if (!(ok = barrier())) break;
@@ -1660,36 +1697,10 @@ __global__ void __launch_bounds__(kWide, 1) k_fcg_persist(FcgP F) {
       ierr = 2;
       break;
     }
-    const double alpha = pqpr[1] / pqpr[0];
-    // (8) update, r.r
-    for (int c = blockIdx.x; c < nb; c += gridDim.x) {
-      const int64_t base = (int64_t)c * kWide;
-      const int nvalid = (int)min((int64_t)kWide, nn - base);
-      const int64_t n = base + threadIdx.x;
-      double rv = 0.0;
-      if (threadIdx.x < nvalid) {
-        k.x[n] = fma(alpha, __ldcg(Pn + n), k.x[n]);
-        rv = fma(-alpha, __ldcg(Qn + n), __ldcg(k.r + n));
-        k.r[n] = rv;
-      }
-      sa[0][threadIdx.x] = rv;
-      sb[0][threadIdx.x] = rv;
-      __syncthreads();
-      double part[1];
-      chunk_dots<1>(sa, sb, nvalid, part);
-      if (threadIdx.x == 0) F.part[2 * nb + c] = part[0];
-    }
-    if (!(ok = barrier())) break;
-    final_sum_wide<1>(F.part + 2 * nb, nb, &rr);
-    ++iter;
+    alpha = pqpr[1] / pqpr[0];
     pq_old = pqpr[0];
     have_old = true;
     parity ^= 1;
-    if (!(rr == rr)) { ierr = 4; break; }
-    if (rr / rhs <= tol2) break;
-    if (iter >= maxit) { ierr = 1; break; }
-    if (rr < best) { best = rr; best_iter = iter; }
-    if (iter - best_iter > stall_window || rr > 1e6 * best) { ierr = 3; break; }
   }
   if (blockIdx.x == 0 && threadIdx.x == 0) {
     S->iter = iter;
@@ -2328,6 +2339,7 @@ static int run_fcg(pic_solve_stats *stats, int *fcg_iters, int *rc_out) {
   if (g.fcg_coop_grid > 0 && g.fcg_window == 1 && !learned && g.pc_sweeps > 0) {
     FcgP F;
     F.k = k0;
+    F.r2 = g.d_w;  // free while FCG runs
     F.dinv = g.d_pc_dinv;
     F.zA = g.d_pc_za;
     F.t = g.d_pc_t;
