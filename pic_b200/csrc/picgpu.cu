@@ -1494,6 +1494,9 @@ __global__ void __launch_bounds__(PIC_RED_THREADS) k_fcg_upd(FcgK k) {
 //   (E) zF = zA + w D^-1 (r - A zA), zF.Q_old  (post-smoothing)
 //   (F) P_new = zF + beta P_old formed at the neighbours, Q_new = A P_new,
 //       p.q, p.r
+// Dot products are summed per thread over the CTA's chunks and once per CTA
+// (cta_sum), so warps run through their chunks without CTA-wide waits; the
+// order is fixed for a given grid, so the solve is deterministic.
 // The convergence test on r'.r' follows phase A.  Without a coarse space
 // phases B-D are skipped.  Loads after a grid barrier are plain (L1-cached)
 // loads: the barrier's release/acquire pair orders every CTA's writes before
@@ -1515,12 +1518,34 @@ struct FcgP {
   unsigned int bar_extra;
 };
 
+// Sum over the CTA's kWide threads of NV values, in a fixed order (warp
+// butterflies, then the warp sums in warp order); result valid in thread 0.
+template <int NV>
+__device__ __forceinline__ void cta_sum(double v[NV], double *out) {
+  __shared__ double ws[NV][kWide / 32];
+#pragma unroll
+  for (int q = 0; q < NV; ++q)
+    for (int off = 16; off > 0; off >>= 1) v[q] += __shfl_xor_sync(0xffffffffu, v[q], off);
+  if ((threadIdx.x & 31) == 0)
+#pragma unroll
+    for (int q = 0; q < NV; ++q) ws[q][threadIdx.x >> 5] = v[q];
+  __syncthreads();
+  if (threadIdx.x == 0)
+#pragma unroll
+    for (int q = 0; q < NV; ++q) {
+      double t = 0.0;
+      for (int w = 0; w < kWide / 32; ++w) t += ws[q][w];
+      out[q] = t;
+    }
+  __syncthreads();
+}
+
 __global__ void __launch_bounds__(kWide, 1) k_fcg_persist(FcgP F) {
   const PcgK &k = F.k;
   FcgState *S = F.s;
-  __shared__ double sa[2][kWide], sb[2][kWide];
   const int64_t nn = k.nn;
   const int nb = k.nb;
+  const int G = gridDim.x;  // one partial per CTA and value, summed in CTA order
   const double rhs = S->rhs, tol2 = S->tol2, omega = F.omega;
   const int maxit = S->maxit, stall_window = S->stall_window;
   int iter = S->iter, ierr = 0, best_iter = S->best_iter;
@@ -1542,16 +1567,17 @@ __global__ void __launch_bounds__(kWide, 1) k_fcg_persist(FcgP F) {
       const double a = alpha;
       const bool upd = have_old;
       auto rnew = [&](int64_t m) { return upd ? fma(-a, Qp[m], r[m]) : r[m]; };
+      double acc_rr = 0.0;
       for (int c = blockIdx.x; c < nb; c += gridDim.x) {
         const int64_t base = (int64_t)c * kWide;
         const int nvalid = (int)min((int64_t)kWide, nn - base);
         const int64_t n = base + threadIdx.x;
-        double rv = 0.0;
         if (threadIdx.x < nvalid) {
-          rv = rnew(n);
+          const double rv = rnew(n);
           if (upd) {
             k.x[n] = fma(a, Pl[n], k.x[n]);
             rn_[n] = rv;
+            acc_rr = fma(rv, rv, acc_rr);
           }
           if (k.row_kind[n] < 0) {
             F.zA[n] = 0.0;
@@ -1562,18 +1588,15 @@ __global__ void __launch_bounds__(kWide, 1) k_fcg_persist(FcgP F) {
             F.t[n] = rv - row_apply(k, n, z1);
           }
         }
-        if (upd) {
-          sa[0][threadIdx.x] = rv;
-          sb[0][threadIdx.x] = rv;
-          __syncthreads();
-          double part[1];
-          chunk_dots<1>(sa, sb, nvalid, part);
-          if (threadIdx.x == 0) F.part[2 * nb + c] = part[0];
-        }
+      }
+      if (upd) {
+        double v[1] = {acc_rr}, o[1];
+        cta_sum<1>(v, o);
+        if (threadIdx.x == 0) F.part[2 * G + blockIdx.x] = o[0];
       }
       if (!(ok = barrier())) break;
       if (upd) {
-        final_sum_wide<1>(F.part + 2 * nb, nb, &rr);
+        final_sum_wide<1>(F.part + 2 * G, G, &rr);
         ++iter;
         double *tmp = rc_;
         rc_ = rn_;
@@ -1631,32 +1654,30 @@ __global__ void __launch_bounds__(kWide, 1) k_fcg_persist(FcgP F) {
     }
     if (!(ok = barrier())) break;
     // (E) post-smoothing and zF.Q_old (Q_old is this iteration's Ql)
-    for (int c = blockIdx.x; c < nb; c += gridDim.x) {
-      const int64_t base = (int64_t)c * kWide;
-      const int nvalid = (int)min((int64_t)kWide, nn - base);
-      const int64_t n = base + threadIdx.x;
-      double zf = 0.0, qo = 0.0;
-      if (threadIdx.x < nvalid) {
-        if (k.row_kind[n] >= 0) {
-          auto za = [&](int64_t m) { return F.zA[m]; };
-          zf = fma(omega * F.dinv[n], r[n] - row_apply(k, n, za), za(n));
+    {
+      double acc_zq = 0.0;
+      for (int c = blockIdx.x; c < nb; c += gridDim.x) {
+        const int64_t n = (int64_t)c * kWide + threadIdx.x;
+        if (n < nn) {
+          double zf = 0.0;
+          if (k.row_kind[n] >= 0) {
+            auto za = [&](int64_t m) { return F.zA[m]; };
+            zf = fma(omega * F.dinv[n], r[n] - row_apply(k, n, za), za(n));
+          }
+          F.zF[n] = zf;
+          if (have_old) acc_zq = fma(zf, Ql[n], acc_zq);
         }
-        F.zF[n] = zf;
-        if (have_old) qo = Ql[n];
       }
-      sa[0][threadIdx.x] = zf;
-      sb[0][threadIdx.x] = qo;
-      __syncthreads();
-      double part[1];
-      chunk_dots<1>(sa, sb, nvalid, part);
-      if (threadIdx.x == 0) F.part[3 * nb + c] = part[0];
+      double v[1] = {acc_zq}, o[1];
+      cta_sum<1>(v, o);
+      if (threadIdx.x == 0) F.part[3 * G + blockIdx.x] = o[0];
     }
     if (!(ok = barrier())) break;
     double beta = 0.0;
     if (have_old) {
-      // its own region: phase F writes [0, 2 nb) while slower CTAs may still read this
+      // its own region: phase F writes [0, 2 G) while slower CTAs may still read this
       double zq;
-      final_sum_wide<1>(F.part + 3 * nb, nb, &zq);
+      final_sum_wide<1>(F.part + 3 * G, G, &zq);
       beta = -zq / pq_old;
     }
     // (F) P_new = zF + beta P_old at every neighbour (0 on Dirichlet nodes,
@@ -1665,34 +1686,28 @@ __global__ void __launch_bounds__(kWide, 1) k_fcg_persist(FcgP F) {
       const double bt = beta;
       const bool ho = have_old;
       auto pnew = [&](int64_t m) { return ho ? fma(bt, Pl[m], F.zF[m]) : F.zF[m]; };
+      double acc[2] = {0.0, 0.0};
       for (int c = blockIdx.x; c < nb; c += gridDim.x) {
-        const int64_t base = (int64_t)c * kWide;
-        const int nvalid = (int)min((int64_t)kWide, nn - base);
-        const int64_t n = base + threadIdx.x;
-        double pv = 0.0, qv = 0.0, rv = 0.0;
-        if (threadIdx.x < nvalid) {
-          pv = pnew(n);
-          qv = row_apply(k, n, pnew);
+        const int64_t n = (int64_t)c * kWide + threadIdx.x;
+        if (n < nn) {
+          const double pv = pnew(n);
+          const double qv = row_apply(k, n, pnew);
           Pn[n] = pv;
           Qn[n] = qv;
-          rv = r[n];
+          acc[0] = fma(pv, qv, acc[0]);
+          acc[1] = fma(pv, r[n], acc[1]);
         }
-        sa[0][threadIdx.x] = pv;
-        sb[0][threadIdx.x] = qv;
-        sa[1][threadIdx.x] = pv;
-        sb[1][threadIdx.x] = rv;
-        __syncthreads();
-        double part[2];
-        chunk_dots<2>(sa, sb, nvalid, part);
-        if (threadIdx.x == 0) {
-          F.part[c] = part[0];
-          F.part[nb + c] = part[1];
-        }
+      }
+      double o[2];
+      cta_sum<2>(acc, o);
+      if (threadIdx.x == 0) {
+        F.part[blockIdx.x] = o[0];
+        F.part[G + blockIdx.x] = o[1];
       }
     }
     if (!(ok = barrier())) break;
     double pqpr[2];
-    final_sum_wide<2>(F.part, nb, pqpr);
+    final_sum_wide<2>(F.part, G, pqpr);
     if (!(pqpr[0] > 0.0) || !(pqpr[1] == pqpr[1])) {
       ierr = 2;
       break;
