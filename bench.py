@@ -451,7 +451,7 @@ def main():
     ap.add_argument("--plain-steps", type=int, default=5,
                     help="steps of the plain FP64 Jacobi-PCG path timed for comparison")
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--precision", default="fp64", choices=["fp64", "mixed"],
+    ap.add_argument("--precision", default="mixed", choices=["fp64", "mixed"],
                     help="particles in FP64, or element + FP32 offsets and velocities")
     ap.add_argument("--cpu-sample", type=int, default=400000)
     ap.add_argument("--no-cpu-baseline", action="store_true")

@@ -184,6 +184,9 @@ struct Ctx {
   int64_t *d_mcc_misc = nullptr;       // [16] counters
   int64_t *d_ion_parent = nullptr;     // ionising parents: (id<<32 | slot)
   double *d_ion_data = nullptr;        // per ionisation: new e- v(3), ion v(3)
+  int32_t *d_mcc_pslot = nullptr;      // created particles: parent slots, velocities
+  double *d_mcc_vel = nullptr;
+  int64_t mcc_new_cap = 0;
   int64_t step_count = 0;
 };
 

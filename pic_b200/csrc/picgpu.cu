@@ -1912,7 +1912,7 @@ static void free_all() {
   fcg_graphs_free();
   F(g.d_cell_count); F(g.d_cell_start); F(g.d_cell_fill); F(g.d_perm); F(g.d_perm2); F(g.d_sort_id);
   F(g.d_scan_blk); F(g.d_counters); F(g.d_hist); F(g.d_sel); F(g.d_cand); F(g.d_cand_slot);
-  F(g.d_mcc_misc); F(g.d_ion_parent); F(g.d_ion_data);
+  F(g.d_mcc_misc); F(g.d_ion_parent); F(g.d_ion_data); F(g.d_mcc_pslot); F(g.d_mcc_vel);
   for (int s = 0; s < PIC_MAX_SPECIES; ++s) {
     Species &p = g.sp[s];
     F(p.x); F(p.y); F(p.vx); F(p.vy); F(p.vz); F(p.loc); F(p.id);

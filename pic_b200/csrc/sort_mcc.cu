@@ -478,19 +478,26 @@ int mcc_run(uint64_t step, pic_mcc_stats *stats) {
     int64_t nion = (int64_t)pd.parent.size();
     std::vector<int32_t> pslot(nion);
     for (int64_t i = 0; i < nion; ++i) pslot[i] = (int32_t)(pd.parent[i] & 0xffffffff);
-    int32_t *d_pslot = nullptr;
-    double *d_vel = nullptr;
-    PIC_CUDA(cudaMalloc(&d_pslot, nion * 4));
-    PIC_CUDA(cudaMalloc(&d_vel, 3 * nion * 8));
-    PIC_CUDA(cudaMemcpy(d_pslot, pslot.data(), nion * 4, cudaMemcpyHostToDevice));
+    if (nion > g.mcc_new_cap) {  // grow the created-particle staging (kept across steps)
+      cudaFree(g.d_mcc_pslot);
+      cudaFree(g.d_mcc_vel);
+      g.d_mcc_pslot = nullptr;
+      g.d_mcc_vel = nullptr;
+      g.mcc_new_cap = 0;
+      const int64_t cap = std::max<int64_t>(2 * nion, 1 << 16);
+      PIC_CUDA(cudaMalloc(&g.d_mcc_pslot, cap * 4));
+      PIC_CUDA(cudaMalloc(&g.d_mcc_vel, 3 * cap * 8));
+      g.mcc_new_cap = cap;
+    }
+    int32_t *d_pslot = g.d_mcc_pslot;
+    double *d_vel = g.d_mcc_vel;
+    PIC_CUDA(cudaMemcpyAsync(d_pslot, pslot.data(), nion * 4, cudaMemcpyHostToDevice, g.st));
     Species &from = g.sp[pd.from_species];
     for (int which = 0; which < 2; ++which) {
       int ts = which == 0 ? pd.e_species : pd.ion_species;
       if (ts < 0 || ts >= g.ns) continue;
       Species &to = g.sp[ts];
       if (to.n_slots + nion > to.capacity) {
-        cudaFree(d_pslot);
-        cudaFree(d_vel);
         set_error("mcc: particle capacity exceeded by ionisation");
         return PIC_ERR_CAPACITY;
       }
@@ -498,7 +505,7 @@ int mcc_run(uint64_t step, pic_mcc_stats *stats) {
       for (int64_t i = 0; i < nion; ++i)
         for (int q = 0; q < 3; ++q)
           vel[3 * i + q] = which == 0 ? pd.data[6 * i + q] : pd.data[6 * i + 3 + q] / g.v_ref;
-      PIC_CUDA(cudaMemcpy(d_vel, vel.data(), 3 * nion * 8, cudaMemcpyHostToDevice));
+      PIC_CUDA(cudaMemcpyAsync(d_vel, vel.data(), 3 * nion * 8, cudaMemcpyHostToDevice, g.st));
       AppendK a{from.x, from.y, from.loc, to.x, to.y, to.vx, to.vy, to.vz, to.loc, to.id,
                 to.n_slots, to.next_id, d_pslot, d_vel, nion, to.f32 ? 1 : 0};
       k_mcc_append<<<blocks_for(nion, 256), 256, 0, g.st>>>(a);
@@ -509,8 +516,6 @@ int mcc_run(uint64_t step, pic_mcc_stats *stats) {
       to.next_id += (uint32_t)nion;
       if (stats) stats->n_created[ts] += nion;
     }
-    cudaFree(d_pslot);
-    cudaFree(d_vel);
   }
   return PIC_OK;
 }
