@@ -111,9 +111,11 @@ def test_mixed_1000_steps_profiles():
     mixed precision with flexible CG, same seed.  Reports the relative error of
     phi and E at step 1000, and of the x-profiles (averaged over y) of the ion
     density and the electron temperature (mean energy).  Particle trajectories
-    decorrelate over 1000 steps (the plasma is chaotic), so the bars are on
-    the profiles, which average ~3200 particles per column: density within 5%,
-    temperature within 10%, phi and E within 5% of their largest magnitude."""
+    decorrelate over 1000 steps (the plasma is chaotic) and the walls absorb
+    most electrons by step 1000 (~1400 remain), so the bars leave room above
+    the measured errors (B200: phi 4.9e-5, E 1.3e-4, ion density profile
+    3.0e-4, electron temperature profile 5.5e-2): phi 1e-3, E 2e-3, ion
+    density profile 1e-2, electron temperature profile 0.2."""
     def fn(sim):
         sim.initial_fields()
         if sim.cfg.precision == api.PIC_PREC_MIXED:
@@ -131,6 +133,6 @@ def test_mixed_1000_steps_profiles():
     for f in ("phi", "efx", "efy", "rho_i_profile", "ek_e_profile"):
         err = np.abs(a[f] - b[f]).max() / np.abs(a[f]).max()
         print(f"\nstep 1000: {f} max |mixed - fp64| / max|fp64| = {err:.3e}")
-        bar = {"rho_i_profile": 0.05, "ek_e_profile": 0.10}.get(f, 0.05)
+        bar = {"phi": 1e-3, "efx": 2e-3, "efy": 2e-3, "rho_i_profile": 1e-2, "ek_e_profile": 0.2}[f]
         assert err <= bar
     print(f"particles fp64 {a['n']} mixed {b['n']}")
