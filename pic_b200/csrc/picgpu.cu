@@ -614,10 +614,12 @@ __global__ void k_rhs(RhsK k) {
 }
 
 __constant__ double c_stencil[16][9];
+__constant__ float c_stencil32[16][9];  // FP32 copy for the inner iterations of the mixed-precision FCG
 
 struct PcgK {
   const int32_t *row_kind, *ex_cnt, *ex_col;
   const double *ex_val, *diag;
+  const float *ex_val32;  // FP32 copy of ex_val
   double *x, *r, *w, *q, *b;
   const double *p_old;
   double *p_new;
@@ -1501,23 +1503,6 @@ __global__ void __launch_bounds__(PIC_RED_THREADS) k_fcg_upd(FcgK k) {
 // phases B-D are skipped.  Loads after a grid barrier are plain (L1-cached)
 // loads: the barrier's release/acquire pair orders every CTA's writes before
 // them, and a stencil reads each value up to nine times, from L1.
-struct FcgP {
-  PcgK k;                        // operator, x, r
-  double *r2;                    // second residual buffer (ping-pong)
-  const double *dinv;
-  double *zA, *t, *zF, *P0, *P1, *Q0, *Q1;
-  double *part;                  // [4][nb] chunk partials: F p.q, F p.r, A r.r, E zF.Q
-  const float *ainv;
-  double *rc, *ec;
-  int nnx, cs, ncx, ncy, coarse;
-  double omega;
-  FcgState *s;
-  unsigned int *bar;
-  int *bar_err;
-  long long spin_limit;
-  unsigned int bar_extra;
-};
-
 // Sum over the CTA's kWide threads of NV values, in a fixed order (warp
 // butterflies, then the warp sums in warp order); result valid in thread 0.
 template <int NV>
@@ -1540,52 +1525,114 @@ __device__ __forceinline__ void cta_sum(double v[NV], double *out) {
   __syncthreads();
 }
 
-__global__ void __launch_bounds__(kWide, 1) k_fcg_persist(FcgP F) {
+template <class V>
+struct FcgP {
+  PcgK k;                        // operator (row kinds, FP64 and FP32 coefficients)
+  V *x, *r, *r2;                 // solution, residual, second residual buffer (ping-pong)
+  const V *dinv;
+  V *zA, *t, *zF, *P0, *P1, *Q0, *Q1;
+  double *part;                  // [4][grid] partials: F p.q, F p.r, A r.r, E zF.Q
+  const float *ainv;
+  double *rc, *ec;
+  int nnx, cs, ncx, ncy, coarse;
+  double omega;
+  FcgState *s;
+  unsigned int *bar;
+  int *bar_err;
+  long long spin_limit;
+  unsigned int bar_extra;
+};
+
+__device__ __forceinline__ double vfma(double a, double b, double c) { return fma(a, b, c); }
+__device__ __forceinline__ float vfma(float a, float b, float c) { return fmaf(a, b, c); }
+
+// A*v for one node in the vector type: FP64 with the FP64 coefficients, FP32
+// with their FP32 copies (same rows, same order).
+template <class V, class F>
+__device__ __forceinline__ V row_apply_v(const PcgK &k, int64_t n, F v) {
+  if constexpr (sizeof(V) == sizeof(double)) {
+    return row_apply(k, n, v);
+  } else {
+    const int kind = k.row_kind[n];
+    if (kind < 0) return 0.0f;
+    float acc = 0.0f;
+    if (kind < k.n_mat) {
+      const int64_t base = n - k.nny - 1;
+#pragma unroll
+      for (int a = 0; a < 3; ++a)
+#pragma unroll
+        for (int c = 0; c < 3; ++c) acc = fmaf(c_stencil32[kind][3 * a + c], v(base + (int64_t)a * k.nny + c), acc);
+    } else {
+      const int rix = kind - k.n_mat;
+      const int cnt = k.ex_cnt[rix];
+      int32_t col[9];
+      float val[9], xv[9];
+#pragma unroll
+      for (int q = 0; q < 9; ++q) {
+        col[q] = k.ex_col[9 * (size_t)rix + q];
+        val[q] = k.ex_val32[9 * (size_t)rix + q];
+      }
+#pragma unroll
+      for (int q = 0; q < 9; ++q) xv[q] = v((int64_t)col[q]);
+#pragma unroll
+      for (int q = 0; q < 9; ++q)
+        if (q < cnt) acc = fmaf(val[q], xv[q], acc);
+    }
+    return acc;
+  }
+}
+
+// V = double: the FP64 solve.  V = float: the inner solve A e = r of the FP64
+// iterative refinement (vectors and coefficients FP32, dot products and the
+// coarse solve accumulated in FP64), started from e = 0.
+template <class V>
+__global__ void __launch_bounds__(kWide, 1) k_fcg_persist(FcgP<V> F) {
   const PcgK &k = F.k;
   FcgState *S = F.s;
   const int64_t nn = k.nn;
   const int nb = k.nb;
   const int G = gridDim.x;  // one partial per CTA and value, summed in CTA order
   const double rhs = S->rhs, tol2 = S->tol2, omega = F.omega;
+  const V om = (V)omega;
   const int maxit = S->maxit, stall_window = S->stall_window;
   int iter = S->iter, ierr = 0, best_iter = S->best_iter;
   double rr = S->rr, best = S->best, pq_old = 0.0, alpha = 0.0;
   bool have_old = false, ok = true;
   int parity = 0;
-  double *rc_ = k.r, *rn_ = F.r2;  // current residual, next residual
+  V *rc_ = F.r, *rn_ = F.r2;  // current residual, next residual
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
   const int gwarp = blockIdx.x * (kWide / 32) + warp, nwarps = gridDim.x * (kWide / 32);
   const int nc = F.ncx * F.ncy;
   auto barrier = [&]() { return grid_barrier(F.bar, F.bar_err, F.spin_limit, F.bar_extra); };
   for (;;) {
     // the previous direction (written last iteration), the new one
-    const double *Pl = parity ? F.P0 : F.P1, *Ql = parity ? F.Q0 : F.Q1;
-    double *Pn = parity ? F.P1 : F.P0, *Qn = parity ? F.Q1 : F.Q0;
+    const V *Pl = parity ? F.P0 : F.P1, *Ql = parity ? F.Q0 : F.Q1;
+    V *Pn = parity ? F.P1 : F.P0, *Qn = parity ? F.Q1 : F.Q0;
     // (A) update with the previous direction, then pre-smoothing
     {
-      const double *r = rc_, *Qp = Ql;
-      const double a = alpha;
+      const V *r = rc_, *Qp = Ql;
+      const V a = (V)alpha;
       const bool upd = have_old;
-      auto rnew = [&](int64_t m) { return upd ? fma(-a, Qp[m], r[m]) : r[m]; };
+      auto rnew = [&](int64_t m) { return upd ? vfma(-a, Qp[m], r[m]) : r[m]; };
       double acc_rr = 0.0;
       for (int c = blockIdx.x; c < nb; c += gridDim.x) {
         const int64_t base = (int64_t)c * kWide;
         const int nvalid = (int)min((int64_t)kWide, nn - base);
         const int64_t n = base + threadIdx.x;
         if (threadIdx.x < nvalid) {
-          const double rv = rnew(n);
+          const V rv = rnew(n);
           if (upd) {
-            k.x[n] = fma(a, Pl[n], k.x[n]);
+            F.x[n] = vfma(a, Pl[n], F.x[n]);
             rn_[n] = rv;
-            acc_rr = fma(rv, rv, acc_rr);
+            acc_rr = fma((double)rv, (double)rv, acc_rr);
           }
           if (k.row_kind[n] < 0) {
-            F.zA[n] = 0.0;
-            F.t[n] = 0.0;
+            F.zA[n] = (V)0;
+            F.t[n] = (V)0;
           } else {
-            auto z1 = [&](int64_t m) { return (omega * rnew(m)) * F.dinv[m]; };
+            auto z1 = [&](int64_t m) { return (om * rnew(m)) * F.dinv[m]; };
             F.zA[n] = z1(n);
-            F.t[n] = rv - row_apply(k, n, z1);
+            F.t[n] = rv - row_apply_v<V>(k, n, z1);
           }
         }
       }
@@ -1598,7 +1645,7 @@ __global__ void __launch_bounds__(kWide, 1) k_fcg_persist(FcgP F) {
       if (upd) {
         final_sum_wide<1>(F.part + 2 * G, G, &rr);
         ++iter;
-        double *tmp = rc_;
+        V *tmp = rc_;
         rc_ = rn_;
         rn_ = tmp;
         if (!(rr == rr)) { ierr = 4; break; }
@@ -1608,7 +1655,7 @@ __global__ void __launch_bounds__(kWide, 1) k_fcg_persist(FcgP F) {
         if (iter - best_iter > stall_window || rr > 1e6 * best) { ierr = 3; break; }
       }
     }
-    const double *r = rc_;
+    const V *r = rc_;
     if (F.coarse) {
       // (B) restriction
       for (int C = gwarp; C < nc; C += nwarps) {
@@ -1621,7 +1668,7 @@ __global__ void __launch_bounds__(kWide, 1) k_fcg_persist(FcgP F) {
         for (int e = lane; e < ni * nj; e += 32) {
           const int i = i0 + e / nj, j = j0 + e % nj;
           const double w = (1.0 - fabs((double)(i - I * F.cs)) * inv) * (1.0 - fabs((double)(j - J * F.cs)) * inv);
-          acc = fma(w, F.t[(int64_t)i * k.nny + j], acc);
+          acc = fma(w, (double)F.t[(int64_t)i * k.nny + j], acc);
         }
         for (int off = 16; off > 0; off >>= 1) acc += __shfl_xor_sync(0xffffffffu, acc, off);
         if (lane == 0) F.rc[C] = acc;
@@ -1648,7 +1695,7 @@ __global__ void __launch_bounds__(kWide, 1) k_fcg_persist(FcgP F) {
           v = fma(fx * (1.0 - fy), __ldcg(F.ec + I1 * F.ncy + J), v);
           v = fma((1.0 - fx) * fy, __ldcg(F.ec + I * F.ncy + J1), v);
           v = fma(fx * fy, __ldcg(F.ec + I1 * F.ncy + J1), v);
-          F.zA[n] += v;
+          F.zA[n] += (V)v;
         }
       }
     }
@@ -1659,13 +1706,13 @@ __global__ void __launch_bounds__(kWide, 1) k_fcg_persist(FcgP F) {
       for (int c = blockIdx.x; c < nb; c += gridDim.x) {
         const int64_t n = (int64_t)c * kWide + threadIdx.x;
         if (n < nn) {
-          double zf = 0.0;
+          V zf = (V)0;
           if (k.row_kind[n] >= 0) {
             auto za = [&](int64_t m) { return F.zA[m]; };
-            zf = fma(omega * F.dinv[n], r[n] - row_apply(k, n, za), za(n));
+            zf = vfma(om * F.dinv[n], r[n] - row_apply_v<V>(k, n, za), za(n));
           }
           F.zF[n] = zf;
-          if (have_old) acc_zq = fma(zf, Ql[n], acc_zq);
+          if (have_old) acc_zq = fma((double)zf, (double)Ql[n], acc_zq);
         }
       }
       double v[1] = {acc_zq}, o[1];
@@ -1683,19 +1730,19 @@ __global__ void __launch_bounds__(kWide, 1) k_fcg_persist(FcgP F) {
     // (F) P_new = zF + beta P_old at every neighbour (0 on Dirichlet nodes,
     // where zF and P_old are 0), Q_new = A P_new, p.q, p.r
     {
-      const double bt = beta;
+      const V bt = (V)beta;
       const bool ho = have_old;
-      auto pnew = [&](int64_t m) { return ho ? fma(bt, Pl[m], F.zF[m]) : F.zF[m]; };
+      auto pnew = [&](int64_t m) { return ho ? vfma(bt, Pl[m], F.zF[m]) : F.zF[m]; };
       double acc[2] = {0.0, 0.0};
       for (int c = blockIdx.x; c < nb; c += gridDim.x) {
         const int64_t n = (int64_t)c * kWide + threadIdx.x;
         if (n < nn) {
-          const double pv = pnew(n);
-          const double qv = row_apply(k, n, pnew);
+          const V pv = pnew(n);
+          const V qv = row_apply_v<V>(k, n, pnew);
           Pn[n] = pv;
           Qn[n] = qv;
-          acc[0] = fma(pv, qv, acc[0]);
-          acc[1] = fma(pv, r[n], acc[1]);
+          acc[0] = fma((double)pv, (double)qv, acc[0]);
+          acc[1] = fma((double)pv, (double)r[n], acc[1]);
         }
       }
       double o[2];
@@ -1725,6 +1772,19 @@ __global__ void __launch_bounds__(kWide, 1) k_fcg_persist(FcgP F) {
     S->ierr = ok ? ierr : 7;  // 7: a grid barrier timed out
     S->done = 1;
   }
+}
+
+// FP64 <-> FP32 helpers of the iterative refinement
+__global__ void k_f64_to_f32(const double *__restrict__ a, float *__restrict__ b, int64_t n) {
+  const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i < n) b[i] = (float)a[i];
+}
+
+// x += e on unknown nodes (FP64 += FP32)
+__global__ void k_add_f32(const int32_t *__restrict__ row_kind, const float *__restrict__ e, double *__restrict__ x,
+                          int64_t n) {
+  const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i < n && row_kind[i] >= 0) x[i] += (double)e[i];
 }
 
 __constant__ double c_ppr_reg[5][9];
@@ -1904,7 +1964,7 @@ static void free_all() {
   F(g.d_xs); F(g.d_ys); F(g.d_element_index); F(g.d_node_index); F(g.d_node_type); F(g.d_elem_near);
   F(g.d_phi_dir); F(g.d_cell_volume); F(g.d_rhs_fix); F(g.d_mass_q1); F(g.d_ife_mass);
   F(g.d_xt_ptr); F(g.d_xt_col); F(g.d_xt_val); F(g.d_row_kind); F(g.d_ex_cnt); F(g.d_ex_col);
-  F(g.d_ex_val); F(g.d_diag); F(g.d_ppr_kind); F(g.d_ppr_ptr); F(g.d_ppr_nodes); F(g.d_ppr_rows);
+  F(g.d_ex_val); F(g.d_ex_val32); F(g.d_fcg32); F(g.d_diag); F(g.d_ppr_kind); F(g.d_ppr_ptr); F(g.d_ppr_nodes); F(g.d_ppr_rows);
   F(g.d_ppr_h); F(g.d_phi); F(g.d_rho); F(g.d_efx); F(g.d_efy); F(g.d_coef); F(g.d_coef32); F(g.d_b); F(g.d_x);
   F(g.d_r); F(g.d_w); F(g.d_p[0]); F(g.d_p[1]); F(g.d_q); F(g.d_part); F(g.d_pcg); F(g.d_bar);
   F(g.d_z); F(g.d_dot); F(g.d_dot_ticket); F(g.d_fcg); F(g.d_fcg_P); F(g.d_fcg_Q); F(g.d_fcg_part);
@@ -2042,6 +2102,7 @@ static PcgK pcg_k(int parity) {
   k.ex_cnt = g.d_ex_cnt;
   k.ex_col = g.d_ex_col;
   k.ex_val = g.d_ex_val;
+  k.ex_val32 = g.d_ex_val32;
   k.diag = g.d_diag;
   k.x = g.d_x;
   k.r = g.d_r;
@@ -2352,8 +2413,111 @@ static int run_fcg(pic_solve_stats *stats, int *fcg_iters, int *rc_out) {
   }
   int judged = 0;
   if (g.fcg_coop_grid > 0 && g.fcg_window == 1 && !learned && g.pc_sweeps > 0) {
-    FcgP F;
-    F.k = k0;
+    auto common = [&](auto &F) {
+      F.k = k0;
+      F.part = g.d_fcg_part;
+      F.ainv = g.d_pc_ainv;
+      F.rc = g.d_pc_rc;
+      F.ec = g.d_pc_ec;
+      F.nnx = g.m.nnx;
+      F.cs = g.pc_cs;
+      F.ncx = g.pc_ncx;
+      F.ncy = g.pc_ncy;
+      F.coarse = g.pc_cs > 0 ? 1 : 0;
+      F.omega = g.pc_omega;
+      F.s = g.d_fcg;
+      F.bar = g.d_bar;
+      F.bar_err = (int *)(g.d_bar + 2);
+      F.spin_limit = g.pcg_spin_limit;
+      F.bar_extra = g.pcg_bar_extra;
+    };
+    auto launch = [&](auto &F, const void *fn) -> int {
+      PIC_CUDA(cudaMemsetAsync(g.d_bar, 0, 4 * sizeof(unsigned int), g.st));
+      void *args[] = {&F};
+      PIC_CUDA(cudaLaunchCooperativeKernel(fn, dim3(g.fcg_coop_grid), dim3(kWide), args, 0, g.st));
+      PIC_LAUNCHED();
+      return PIC_OK;
+    };
+    auto true_residual = [&]() -> int {
+      k_spmv<<<nb, 256, 0, g.st>>>(k0, g.d_x, g.d_q);
+      PIC_LAUNCHED();
+      k_fcg_r0<<<nb, 256, 0, g.st>>>(g.d_row_kind, g.d_b, g.d_q, g.d_r, nn);
+      PIC_LAUNCHED();
+      int r2 = dot2(g.d_r, g.d_r, nullptr, nullptr, s2);
+      if (!r2) hs.rr = s2[0];
+      return r2;
+    };
+    if (g.mixed && g.fcg_inner32) {
+      // Mixed precision: FP32 inner FCG solves of A e = r inside FP64 iterative
+      // refinement (x += e, r = b - A x in FP64, tested against the tolerance).
+      if (!g.d_fcg32) {
+        if ((rc = dalloc(&g.d_fcg32, 11 * (size_t)nn))) { *rc_out = rc; return 1; }
+        k_f64_to_f32<<<nb, 256, 0, g.st>>>(g.d_pc_dinv, g.d_fcg32 + 10 * (size_t)nn, nn);
+        PIC_LAUNCHED();
+      }
+      float *v32 = g.d_fcg32;
+      FcgP<float> F;
+      common(F);
+      F.r = v32;
+      F.r2 = v32 + nn;
+      F.x = v32 + 2 * nn;
+      F.zA = v32 + 3 * nn;
+      F.t = v32 + 4 * nn;
+      F.zF = v32 + 5 * nn;
+      F.P0 = v32 + 6 * nn;
+      F.P1 = v32 + 7 * nn;
+      F.Q0 = v32 + 8 * nn;
+      F.Q1 = v32 + 9 * nn;
+      F.dinv = v32 + 10 * nn;
+      int outer = 0, total = 0;
+      for (;;) {
+        if (hs.rr / hs.rhs <= hs.tol2) {
+          hs.iter = total;
+          if (stats) stats->outer = outer;
+          return finish(0);
+        }
+        if (++outer > 8 || total >= hs.maxit) {
+          hs.iter = total;
+          if (stats) stats->outer = outer;
+          return finish(6);
+        }
+        k_f64_to_f32<<<nb, 256, 0, g.st>>>(g.d_r, F.r, nn);
+        PIC_LAUNCHED();
+        PIC_CUDA(cudaMemsetAsync(F.x, 0, nn * sizeof(float), g.st));
+        FcgState in{};
+        in.rhs = hs.rr;
+        in.rr = hs.rr;
+        in.best = hs.rr;
+        // the reduction the outer residual still needs, but at most 1e-5 per
+        // sweep (FP32 vectors)
+        in.tol2 = std::max(hs.tol2 * hs.rhs / hs.rr, 1e-10);
+        in.maxit = hs.maxit - total;
+        in.stall_window = 50;
+        PIC_CUDA(cudaMemcpyAsync(g.d_fcg, &in, sizeof in, cudaMemcpyHostToDevice, g.st));
+        if ((rc = launch(F, (const void *)k_fcg_persist<float>))) { *rc_out = rc; return 1; }
+        PIC_CUDA(cudaMemcpyAsync(&in, g.d_fcg, sizeof in, cudaMemcpyDeviceToHost, g.st));
+        PIC_CUDA(cudaStreamSynchronize(g.st));
+        if (in.ierr == 7) {
+          set_error("pic_ife_solve: FCG grid barrier timed out");
+          *rc_out = PIC_ERR_CUDA;
+          return 1;
+        }
+        total += in.iter;
+        const double rr_before = hs.rr;
+        k_add_f32<<<nb, 256, 0, g.st>>>(g.d_row_kind, F.x, g.d_x, nn);
+        PIC_LAUNCHED();
+        if ((rc = true_residual())) { *rc_out = rc; return 1; }
+        if (in.ierr && !(hs.rr < 0.25 * rr_before)) {  // the sweep failed and gained little
+          hs.iter = total;
+          if (stats) stats->outer = outer;
+          return finish(in.ierr);
+        }
+      }
+    }
+    FcgP<double> F;
+    common(F);
+    F.x = g.d_x;
+    F.r = g.d_r;
     F.r2 = g.d_w;  // free while FCG runs
     F.dinv = g.d_pc_dinv;
     F.zA = g.d_pc_za;
@@ -2363,27 +2527,8 @@ static int run_fcg(pic_solve_stats *stats, int *fcg_iters, int *rc_out) {
     F.P1 = g.d_fcg_P + nn;
     F.Q0 = g.d_fcg_Q;
     F.Q1 = g.d_fcg_Q + nn;
-    F.part = g.d_fcg_part;
-    F.ainv = g.d_pc_ainv;
-    F.rc = g.d_pc_rc;
-    F.ec = g.d_pc_ec;
-    F.nnx = g.m.nnx;
-    F.cs = g.pc_cs;
-    F.ncx = g.pc_ncx;
-    F.ncy = g.pc_ncy;
-    F.coarse = g.pc_cs > 0 ? 1 : 0;
-    F.omega = g.pc_omega;
-    F.s = g.d_fcg;
-    F.bar = g.d_bar;
-    F.bar_err = (int *)(g.d_bar + 2);
-    F.spin_limit = g.pcg_spin_limit;
-    F.bar_extra = g.pcg_bar_extra;
     for (;;) {
-      PIC_CUDA(cudaMemsetAsync(g.d_bar, 0, 4 * sizeof(unsigned int), g.st));
-      void *args[] = {&F};
-      PIC_CUDA(cudaLaunchCooperativeKernel((const void *)k_fcg_persist, dim3(g.fcg_coop_grid), dim3(kWide), args,
-                                           0, g.st));
-      PIC_LAUNCHED();
+      if ((rc = launch(F, (const void *)k_fcg_persist<double>))) { *rc_out = rc; return 1; }
       PIC_CUDA(cudaMemcpyAsync(&hs, g.d_fcg, sizeof hs, cudaMemcpyDeviceToHost, g.st));
       PIC_CUDA(cudaStreamSynchronize(g.st));
       if (hs.ierr == 7) {
@@ -2392,12 +2537,7 @@ static int run_fcg(pic_solve_stats *stats, int *fcg_iters, int *rc_out) {
         return 1;
       }
       if (hs.ierr) return finish(hs.ierr);
-      k_spmv<<<nb, 256, 0, g.st>>>(k0, g.d_x, g.d_q);
-      PIC_LAUNCHED();
-      k_fcg_r0<<<nb, 256, 0, g.st>>>(g.d_row_kind, g.d_b, g.d_q, g.d_r, nn);
-      PIC_LAUNCHED();
-      if ((rc = dot2(g.d_r, g.d_r, nullptr, nullptr, s2))) { *rc_out = rc; return 1; }
-      hs.rr = s2[0];
+      if ((rc = true_residual())) { *rc_out = rc; return 1; }
       if (hs.rr / hs.rhs <= hs.tol2) return finish(0);
       if (++judged > 3 || hs.iter >= hs.maxit) return finish(6);
       hs.done = 0;
@@ -2904,6 +3044,14 @@ int pic_init(const pic_mesh_desc *mesh, const pic_params *params) {
       }
     }
     PIC_CUDA(cudaMemcpyToSymbol(c_stencil, g.h_stencil, sizeof g.h_stencil));
+    {
+      float st32[16][9];
+      for (int a = 0; a < 16; ++a)
+        for (int c = 0; c < 9; ++c) st32[a][c] = (float)g.h_stencil[a][c];
+      PIC_CUDA(cudaMemcpyToSymbol(c_stencil32, st32, sizeof st32));
+      std::vector<float> ev32(ex_val.begin(), ex_val.end());
+      if ((rc = upload(&g.d_ex_val32, ev32.data(), ev32.size()))) return rc;
+    }
     if ((rc = upload(&g.d_row_kind, kind.data(), kind.size()))) return rc;
     if ((rc = upload(&g.d_ex_cnt, ex_cnt.data(), ex_cnt.size()))) return rc;
     if ((rc = upload(&g.d_ex_col, ex_col.data(), ex_col.size()))) return rc;
@@ -3028,7 +3176,10 @@ int pic_init(const pic_mesh_desc *mesh, const pic_params *params) {
     bool want = !(env && env[0] == '0');
     g.coop_grid = (want && coop && per_sm > 0) ? std::min(g.red_blocks, per_sm * nsm) : 0;
     int per_sm_f = 0;
-    PIC_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm_f, k_fcg_persist, kWide, 0));
+    int per_sm_f32 = 0;
+    PIC_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm_f, k_fcg_persist<double>, kWide, 0));
+    PIC_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm_f32, k_fcg_persist<float>, kWide, 0));
+    per_sm_f = std::min(per_sm_f, per_sm_f32);
     const char *envf = getenv("PIC_FCG_PERSISTENT");
     const bool want_f = !(envf && envf[0] == '0');
     g.fcg_coop_grid = (want_f && coop && per_sm_f > 0) ? std::min(g.red_blocks, per_sm_f * nsm) : 0;
@@ -3060,6 +3211,8 @@ int pic_init(const pic_mesh_desc *mesh, const pic_params *params) {
   {
     const char *fg = getenv("PIC_FCG_GRAPHS");  // 0: enqueue FCG iterations kernel by kernel
     g.fcg_graphs = (fg && atoi(fg) == 0) ? 0 : 1;
+    const char *fi = getenv("PIC_FCG_INNER");  // "fp64": no FP32 inner iterations in mixed precision
+    g.fcg_inner32 = (fi && std::strcmp(fi, "fp64") == 0) ? 0 : 1;
   }
   if ((rc = dalloc(&g.d_counters, 32))) return rc;
   PIC_CUDA(cudaMemset(g.d_counters, 0, 32 * sizeof(unsigned long long)));

@@ -2,7 +2,7 @@
 ncu (each runs a few launches of its kernels and exits):
 
     python -m pic_b200.profile_cases step  <deck> <ppc> <steps> [jpcg|fcg] [fp64|mixed]
-    python -m pic_b200.profile_cases solve <cells> [jpcg|fcg] [repeats] [coarse_cells]
+    python -m pic_b200.profile_cases solve <cells> [jpcg|fcg] [repeats] [coarse_cells] [fp64|mixed]
     python -m pic_b200.profile_cases unet  <nodes> [repeats]
 
 step:  the deck at <ppc> particles per cell and species, <steps> steps.
@@ -41,12 +41,13 @@ def _step(deck_name, ppc, steps, solver="fcg", precision="fp64"):
     sim.close()
 
 
-def _solve(cells, solver="fcg", repeats=3, coarse_cells=64):
+def _solve(cells, solver="fcg", repeats=3, coarse_cells=64, precision="fp64"):
     import torch
     from . import api, deck
     from .simulation import Simulation
     n = int(cells)
-    cfg = deck.config("cfg4", ncx=n, ncy=n, ppc=1)
+    prec = api.PIC_PREC_MIXED if precision == "mixed" else api.PIC_PREC_FP64
+    cfg = deck.config("cfg4", ncx=n, ncy=n, ppc=1, precision=prec)
     sim = Simulation(cfg, load=False)
     sim.set_field("rho", np.random.default_rng(0).standard_normal(sim.mesh.nn))
     import time
@@ -63,8 +64,9 @@ def _solve(cells, solver="fcg", repeats=3, coarse_cells=64):
         api.check(sim.lib.pic_ife_solve(None, 0.0, C.byref(st)), "pic_ife_solve")
         e1.record()
         torch.cuda.synchronize()
-        out.append((st.iterations, round(e0.elapsed_time(e1), 3)))
-    print(f"solve {n}^2 {solver} coarse_cells={coarse_cells} (setup {setup:.2f} s): (iterations, ms) {out}")
+        out.append((st.iterations, st.outer, round(e0.elapsed_time(e1), 3)))
+    print(f"solve {n}^2 {solver} {precision} coarse_cells={coarse_cells} (setup {setup:.2f} s): "
+          f"(iterations, outer, ms) {out}")
     sim.close()
 
 

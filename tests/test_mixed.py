@@ -136,3 +136,38 @@ def test_mixed_1000_steps_profiles():
         bar = {"phi": 1e-3, "efx": 2e-3, "efy": 2e-3, "rho_i_profile": 1e-2, "ek_e_profile": 0.2}[f]
         assert err <= bar
     print(f"particles fp64 {a['n']} mixed {b['n']}")
+
+
+def test_fp32_inner_fcg_in_fp64_refinement():
+    """Mixed precision runs the persistent FCG's iterations in FP32 inside an
+    FP64 iterative refinement: the final x meets the tolerance on the FP64
+    true residual and equals the FP64 FCG solution to that accuracy."""
+    import ctypes as C
+
+    def fn(sim):
+        rng = np.random.default_rng(3)
+        sim.set_field("rho", rng.standard_normal(sim.mesh.nn))
+        sim.set_field("phi", np.zeros(sim.mesh.nn))
+        sim.set_solver("fcg")
+        st = api.SolveStats()
+        api.check(sim.lib.pic_ife_solve(None, 0.0, C.byref(st)), "solve")
+        b = sim.field("b")
+        phi = sim.field("phi")
+        return phi, (st.iterations, st.outer, st.fallback, st.rel_residual), b
+
+    cfg_over = dict(ncx=256, ncy=256, pcg_tol=1e-8)
+    d = Simulation(deck.config("cfg4", precision=api.PIC_PREC_FP64, **cfg_over), load=False)
+    try:
+        pd, sd, bd = fn(d)
+    finally:
+        d.close()
+    m = Simulation(deck.config("cfg4", precision=api.PIC_PREC_MIXED, **cfg_over), load=False)
+    try:
+        pm, sm, bm = fn(m)
+    finally:
+        m.close()
+    print(f"\nFCG fp64 (it, outer, fallback, rel) {sd}; fp32 inner in fp64 refinement {sm}")
+    assert np.array_equal(bd, bm)
+    assert sd[2] == 0 and sm[2] == 0 and sm[1] >= 1
+    assert sd[3] <= 1e-8 and sm[3] <= 1e-8
+    assert np.abs(pd - pm).max() <= 1e-5 * np.abs(pd).max()
