@@ -2488,9 +2488,9 @@ static int run_fcg(pic_solve_stats *stats, int *fcg_iters, int *rc_out) {
         in.rhs = hs.rr;
         in.rr = hs.rr;
         in.best = hs.rr;
-        // the reduction the outer residual still needs, but at most 1e-5 per
+        // the reduction the outer residual still needs, but at most 1e-6 per
         // sweep (FP32 vectors)
-        in.tol2 = std::max(hs.tol2 * hs.rhs / hs.rr, 1e-10);
+        in.tol2 = std::max(hs.tol2 * hs.rhs / hs.rr, 1e-12);
         in.maxit = hs.maxit - total;
         in.stall_window = 50;
         PIC_CUDA(cudaMemcpyAsync(g.d_fcg, &in, sizeof in, cudaMemcpyHostToDevice, g.st));
@@ -2614,15 +2614,13 @@ static int run_fcg(pic_solve_stats *stats, int *fcg_iters, int *rc_out) {
 static int run_solve(pic_solve_stats *stats) {
   if (g.solver == PIC_SOLVER_FCG_UNET && ((g.pc_learned && g.precond) || g.pc_cs > 0 || g.pc_sweeps > 0)) {
     int fcg_iters = 0, rc = PIC_OK;
+    if (stats) stats->outer = 0;
     int fallback = run_fcg(stats, &fcg_iters, &rc);
     if (rc) return rc;
     k_phi_out<<<blocks_for(g.nn, 256), 256, 0, g.st>>>(g.d_x, g.d_node_type, g.d_phi_dir, g.d_phi, g.nn);
     PIC_LAUNCHED();
     if (!fallback) {
-      if (stats) {
-        stats->fallback = 0;
-        stats->outer = 0;
-      }
+      if (stats) stats->fallback = 0;
       return PIC_OK;
     }
     int prc = run_pcg(stats);
