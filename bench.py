@@ -322,7 +322,12 @@ def run_ours(args, dist, rank, ws):
         sim.set_solver("fcg", coarse_cells=64, window=4)
         lp.set_learned(True)
 
+    def sel_fcg32():
+        sim.set_solver("fcg", coarse_cells=64, window=1, inner_fp32=True)
+
     variants = {"jacobi_pcg": sel_jpcg, "fcg_smooth_coarse": sel_fcg}
+    if args.precision == "mixed":
+        variants["fcg_smooth_coarse_fp32_iterations_in_fp64_refinement"] = sel_fcg32
     if lp is not None:
         variants["fcg_smooth_coarse_learned"] = sel_learned
     poisson = _poisson_compare(sim, lib, api, variants)

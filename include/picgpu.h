@@ -310,6 +310,11 @@ int pic_set_preconditioner(pic_precond_fn fn, void *user);
 int pic_set_solver(int32_t solver);
 /* Directions FCG keeps for A-orthogonalisation, 1..8 (default 4; 1 = FCG(1)). */
 int pic_set_fcg_window(int32_t window);
+/* With PIC_PREC_MIXED: 1 runs the one-kernel FCG's iterations in FP32 (FP32
+ * vectors and coefficients, FP64 dot products and coarse solve) inside an
+ * FP64 iterative refinement x += e, r = b - A x until the tolerance holds on
+ * the FP64 residual; 0 (default) keeps the iterations in FP64. */
+int pic_set_fcg_inner(int32_t fp32);
 /* Preconditioner of flexible CG as a composition of stages:
  *   1. damped-Jacobi pre-smoothing        z1 = omega D^-1 r          (smoothing)
  *   2. Galerkin coarse correction         z2 = z1 + P Ac^-1 P^T (r - A z1)

@@ -38,7 +38,7 @@ EXPORTS = [
     "pic_particle_device_ptrs", "pic_kernel_launches", "pic_device_timer",
     "pic_deposit_noalloc", "pic_set_preconditioner", "pic_set_solver", "pic_set_fcg_window",
     "pic_cuda_stream", "pic_apply_operator", "pic_solver_vectors", "pic_set_precond_stages",
-    "pic_coarse_setup", "pic_precond_apply",
+    "pic_coarse_setup", "pic_precond_apply", "pic_set_fcg_inner",
 ]
 
 # z = M(r) callback of flexible CG: (r_dev, z_dev, user) -> 0 or failure
@@ -177,6 +177,7 @@ def load() -> C.CDLL:
     lib.pic_set_preconditioner.argtypes = [PRECOND_FN, C.c_void_p]
     lib.pic_set_solver.argtypes = [C.c_int32]
     lib.pic_set_fcg_window.argtypes = [C.c_int32]
+    lib.pic_set_fcg_inner.argtypes = [C.c_int32]
     lib.pic_cuda_stream.argtypes = [_P(C.c_void_p)]
     lib.pic_apply_operator.argtypes = [C.c_void_p, C.c_void_p]
     lib.pic_solver_vectors.argtypes = [_P(C.c_void_p), _P(C.c_void_p)]

@@ -112,7 +112,7 @@ struct Ctx {
   double *d_ex_val = nullptr;
   float *d_ex_val32 = nullptr;     // FP32 copy (inner iterations of the mixed-precision FCG)
   float *d_fcg32 = nullptr;        // mixed-precision FCG: 11 FP32 vectors, allocated on first use
-  int fcg_inner32 = 1;             // mixed precision: FP32 inner FCG in FP64 refinement (PIC_FCG_INNER=fp64: off)
+  int fcg_inner32 = 0;             // mixed precision: FP32 inner FCG in FP64 refinement (pic_set_fcg_inner)
   int n_mat = 0;
   double h_stencil[16][9];
   double *d_diag = nullptr;  // [nn], 1 on Dirichlet nodes

@@ -130,9 +130,10 @@ class Simulation:
 
     # ---- Poisson solver ---------------------------------------------------
     def set_solver(self, kind: str = "jpcg", coarse_cells: int = 64, window: int = 1,
-                   omega: float = 2.0 / 3.0):
+                   omega: float = 2.0 / 3.0, inner_fp32: bool = False):
         """'jpcg': the reference's Jacobi-PCG.  'fcg': flexible CG with damped
-        Jacobi smoothing and a Galerkin coarse space (no learned stage).
+        Jacobi smoothing and a Galerkin coarse space (no learned stage);
+        inner_fp32 (mixed precision only): FP32 iterations in FP64 refinement.
         'fcg-learned' is set up by unet.LearnedPreconditioner on top of 'fcg'."""
         lib = self.lib
         if kind == "jpcg":
@@ -143,6 +144,7 @@ class Simulation:
         api.check(lib.pic_set_precond_stages(1, omega, 0), "pic_set_precond_stages")
         api.check(lib.pic_coarse_setup(self.mesh.ptr, coarse_cells), "pic_coarse_setup")
         api.check(lib.pic_set_fcg_window(window), "pic_set_fcg_window")
+        api.check(lib.pic_set_fcg_inner(int(inner_fp32)), "pic_set_fcg_inner")
         api.check(lib.pic_set_solver(api.PIC_SOLVER_FCG_UNET), "pic_set_solver")
 
     # ---- fields ---------------------------------------------------------

@@ -148,7 +148,7 @@ def test_fp32_inner_fcg_in_fp64_refinement():
         rng = np.random.default_rng(3)
         sim.set_field("rho", rng.standard_normal(sim.mesh.nn))
         sim.set_field("phi", np.zeros(sim.mesh.nn))
-        sim.set_solver("fcg")
+        sim.set_solver("fcg", inner_fp32=True)
         st = api.SolveStats()
         api.check(sim.lib.pic_ife_solve(None, 0.0, C.byref(st)), "solve")
         b = sim.field("b")
