@@ -233,20 +233,24 @@ __device__ __forceinline__ void mcc_put(double *a, int f32, int64_t p, double v)
   else a[p] = v;
 }
 
-__global__ void k_mcc_hist(MccK k, uint32_t *__restrict__ hist) {
+// Selection keys of the live particles: histogram of their top 16 bits, and
+// the key itself for k_mcc_pick (one Philox evaluation per particle and step).
+__global__ void k_mcc_hist(MccK k, uint32_t *__restrict__ hist, uint32_t *__restrict__ keys) {
   int64_t p = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
   if (p >= k.n || k.loc[p] < 0) return;
   uint32_t key = mcc_select_key(k.id[p], k.step_lo, k.step_hi, k.species, k.seed0, k.seed1);
+  keys[p] = key;
   atomicAdd(hist + (key >> 16), 1u);
 }
 
 // particles below the threshold bin are selected; the threshold bin's
 // particles become candidates ordered later by (key, id)
-__global__ void k_mcc_pick(MccK k, uint32_t bstar, int32_t *__restrict__ sel, int64_t *__restrict__ misc,
-                           uint64_t *__restrict__ cand, int32_t *__restrict__ cand_slot, int64_t cand_cap) {
+__global__ void k_mcc_pick(MccK k, const uint32_t *__restrict__ keys, uint32_t bstar, int32_t *__restrict__ sel,
+                           int64_t *__restrict__ misc, uint64_t *__restrict__ cand, int32_t *__restrict__ cand_slot,
+                           int64_t cand_cap) {
   int64_t p = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
   if (p >= k.n || k.loc[p] < 0) return;
-  uint32_t key = mcc_select_key(k.id[p], k.step_lo, k.step_hi, k.species, k.seed0, k.seed1);
+  const uint32_t key = keys[p];
   uint32_t bin = key >> 16;
   if (bin < bstar) {
     long long i = atomicAdd((unsigned long long *)&misc[0], 1ull);
@@ -379,7 +383,8 @@ int mcc_run(uint64_t step, pic_mcc_stats *stats) {
            sp.f32 ? 1 : 0};
     PIC_CUDA(cudaMemsetAsync(g.d_hist, 0, 65536 * sizeof(uint32_t), g.st));
     PIC_CUDA(cudaMemsetAsync(g.d_mcc_misc, 0, 16 * sizeof(int64_t), g.st));
-    k_mcc_hist<<<blocks_for(sp.n_slots, 256), 256, 0, g.st>>>(k, g.d_hist);
+    uint32_t *keys = g.d_sort_id;  // sort scratch, free while MCC runs
+    k_mcc_hist<<<blocks_for(sp.n_slots, 256), 256, 0, g.st>>>(k, g.d_hist, keys);
     PIC_LAUNCHED();
     std::vector<uint32_t> hist(65536);
     PIC_CUDA(cudaMemcpyAsync(hist.data(), g.d_hist, 65536 * 4, cudaMemcpyDeviceToHost, g.st));
@@ -398,7 +403,7 @@ int mcc_run(uint64_t step, pic_mcc_stats *stats) {
     int64_t ncand_expect = hist[bstar];
     rc = mcc_alloc(std::max<int64_t>(ncoll, ncand_expect) + 4096);
     if (rc) return rc;
-    k_mcc_pick<<<blocks_for(sp.n_slots, 256), 256, 0, g.st>>>(k, bstar, g.d_sel, g.d_mcc_misc, g.d_cand,
+    k_mcc_pick<<<blocks_for(sp.n_slots, 256), 256, 0, g.st>>>(k, keys, bstar, g.d_sel, g.d_mcc_misc, g.d_cand,
                                                               g.d_cand_slot, g.mcc_cap);
     PIC_LAUNCHED();
     int64_t misc[2];
