@@ -2,6 +2,7 @@
 #ifndef PIC_CTX_H
 #define PIC_CTX_H
 
+#include <cuda_fp16.h>
 #include <cuda_runtime.h>
 
 #include <string>
@@ -156,7 +157,8 @@ struct Ctx {
   int pc_learned = 1;                       // apply the registered callback as stage 3
   int pc_cs = 0, pc_ncx = 0, pc_ncy = 0;    // coarse spacing in nodes (0: no coarse space)
   double *d_pc_t = nullptr, *d_pc_y = nullptr, *d_pc_za = nullptr, *d_pc_dinv = nullptr;
-  float *d_pc_ainv = nullptr;              // coarse inverse (FP32 copy, row-major)
+  __half *d_pc_ainv = nullptr;             // coarse inverse / pc_ainv_scale, FP16, row-major
+  double pc_ainv_scale = 1.0;
   double *d_pc_rc = nullptr, *d_pc_ec = nullptr;
   // CUDA graphs of one FCG iteration: [0] stage A, [1 + slot] stage B + FCG
   // kernels of ring slot `slot`; rebuilt when the configuration key changes

@@ -1532,7 +1532,8 @@ struct FcgP {
   const V *dinv;
   V *zA, *t, *zF, *P0, *P1, *Q0, *Q1;
   double *part;                  // [4][grid] partials: F p.q, F p.r, A r.r, E zF.Q
-  const float *ainv;
+  const __half *ainv;            // coarse inverse / ainv_scale
+  double ainv_scale;
   double *rc, *ec;
   int nnx, cs, ncx, ncy, coarse;
   double omega;
@@ -1676,11 +1677,11 @@ __global__ void __launch_bounds__(kWide, 1) k_fcg_persist(FcgP<V> F) {
       if (!(ok = barrier())) break;
       // (C) coarse solve
       for (int row = gwarp; row < nc; row += nwarps) {
-        const float *arow = F.ainv + (size_t)row * nc;
+        const __half *arow = F.ainv + (size_t)row * nc;
         double acc = 0.0;
-        for (int q = lane; q < nc; q += 32) acc = fma((double)arow[q], __ldcg(F.rc + q), acc);
+        for (int q = lane; q < nc; q += 32) acc = fma((double)__half2float(arow[q]), __ldcg(F.rc + q), acc);
         for (int off = 16; off > 0; off >>= 1) acc += __shfl_xor_sync(0xffffffffu, acc, off);
-        if (lane == 0) F.ec[row] = acc;
+        if (lane == 0) F.ec[row] = acc * F.ainv_scale;
       }
       if (!(ok = barrier())) break;
       // (D) prolongation
@@ -2417,6 +2418,7 @@ static int run_fcg(pic_solve_stats *stats, int *fcg_iters, int *rc_out) {
       F.k = k0;
       F.part = g.d_fcg_part;
       F.ainv = g.d_pc_ainv;
+      F.ainv_scale = g.pc_ainv_scale;
       F.rc = g.d_pc_rc;
       F.ec = g.d_pc_ec;
       F.nnx = g.m.nnx;

@@ -7,10 +7,12 @@
 // Each stage can be switched off.  The smoother removes the rough part of
 // the error, the coarse space (bilinear P on a uniform coarse grid of spacing
 // cs nodes, Ac = P^T A P assembled on the host and inverted once on the
-// device) the global part, and the
+// device, applied from a scaled FP16 copy) the global part, and the
 // network what lies between -- it is trained on exactly the residuals stage 3
 // sees.  The reference solver (IFE-Solver/MY_PCG.f90) is Jacobi-PCG only:
 // none of this has a counterpart there.
+#include <cuda_fp16.h>
+
 #include <cmath>
 #include <cstring>
 #include <vector>
@@ -60,16 +62,16 @@ __global__ void __launch_bounds__(PC_THREADS) k_pc_restrict(CoarseK c, const dou
 }
 
 // ec = Ainv rc, one warp per row (row-major FP64 inverse)
-__global__ void k_pc_gemv(const float *__restrict__ ainv, const double *__restrict__ rc, double *__restrict__ ec,
-                          int nc) {
+__global__ void k_pc_gemv(const __half *__restrict__ ainv, double scale, const double *__restrict__ rc,
+                          double *__restrict__ ec, int nc) {
   const int row = blockIdx.x * (blockDim.x / 32) + (threadIdx.x >> 5);
   const int lane = threadIdx.x & 31;
   if (row >= nc) return;
-  const float *a = ainv + (size_t)row * nc;
+  const __half *a = ainv + (size_t)row * nc;
   double s = 0.0;
-  for (int k = lane; k < nc; k += 32) s = fma((double)a[k], rc[k], s);
+  for (int k = lane; k < nc; k += 32) s = fma((double)__half2float(a[k]), rc[k], s);
   for (int off = 16; off > 0; off >>= 1) s += __shfl_xor_sync(0xffffffffu, s, off);
-  if (lane == 0) ec[row] = s;
+  if (lane == 0) ec[row] = s * scale;
 }
 
 // z (+)= P ec on unknown nodes (bilinear from the four coarse nodes around);
@@ -127,7 +129,7 @@ int coarse_correct(const double *t, double *z, int assign) {
   const int nc = c.ncx * c.ncy;
   k_pc_restrict<<<nc, PC_THREADS, 0, g.st>>>(c, t, g.d_pc_rc);
   PIC_LAUNCHED();
-  k_pc_gemv<<<(nc + 7) / 8, 256, 0, g.st>>>(g.d_pc_ainv, g.d_pc_rc, g.d_pc_ec, nc);
+  k_pc_gemv<<<(nc + 7) / 8, 256, 0, g.st>>>(g.d_pc_ainv, g.pc_ainv_scale, g.d_pc_rc, g.d_pc_ec, nc);
   PIC_LAUNCHED();
   k_pc_prolong<<<blocks_for(g.nn, PC_THREADS), PC_THREADS, 0, g.st>>>(c, g.d_pc_ec, g.d_row_kind, assign, z,
                                                                         g.nn);
@@ -164,9 +166,16 @@ __global__ void k_gj_update(double *__restrict__ A, int n, int k, const double *
   A[e] = v;
 }
 
-__global__ void k_to_f32(const double *__restrict__ a, float *__restrict__ b, int64_t n) {
+// FP16 copy of the inverse, divided by `scale` so the largest entry (on the
+// diagonal, as for any SPD matrix) sits near 2^14
+__global__ void k_to_f16(const double *__restrict__ a, __half *__restrict__ b, double inv_scale, int64_t n) {
   const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
-  if (i < n) b[i] = (float)a[i];
+  if (i < n) b[i] = __float2half_rn((float)(a[i] * inv_scale));
+}
+
+__global__ void k_diag_of(const double *__restrict__ a, double *__restrict__ d, int n) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i < n) d[i] = a[(size_t)i * n + i];
 }
 
 }  // namespace
@@ -264,11 +273,22 @@ int coarse_setup(const pic_mesh_desc *mesh, int coarse_cells) {
     set_error("pic_coarse_setup: coarse operator is not positive definite");
     return PIC_ERR_SETUP;
   }
-  // the per-iteration GEMV reads an FP32 copy (half the bytes; at 65x65 coarse
-  // nodes it stays in L2) and accumulates in FP64
-  rc = pc_alloc(&g.d_pc_ainv, nc2);
+  // The per-iteration GEMV reads a scaled FP16 copy (a quarter of the FP64
+  // bytes: 36 MB at 65x65 coarse nodes, so it and the solver's vectors fit in
+  // L2 together) and accumulates in FP64.  A preconditioner tolerates the
+  // 2^-11 relative rounding of the coarse correction; convergence is always
+  // judged on the FP64 residual.
+  std::vector<double> dg(nc);
+  k_diag_of<<<(nc + 255) / 256, 256, 0, g.st>>>(d_a, d_row, nc);
+  e = cudaMemcpyAsync(dg.data(), d_row, nc * sizeof(double), cudaMemcpyDeviceToHost, g.st);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(g.st);
+  double dmax = 0.0;
+  for (double v : dg) dmax = std::max(dmax, std::fabs(v));
+  g.pc_ainv_scale = (dmax > 0.0) ? dmax / 16384.0 : 1.0;
+  rc = (e == cudaSuccess) ? pc_alloc(&g.d_pc_ainv, nc2) : cuda_fail(e, "coarse inverse diagonal");
   if (!rc) {
-    k_to_f32<<<(unsigned)((nc2 + 255) / 256), 256, 0, g.st>>>(d_a, g.d_pc_ainv, (int64_t)nc2);
+    k_to_f16<<<(unsigned)((nc2 + 255) / 256), 256, 0, g.st>>>(d_a, g.d_pc_ainv, 1.0 / g.pc_ainv_scale,
+                                                               (int64_t)nc2);
     e = cudaStreamSynchronize(g.st);
     if (e != cudaSuccess) rc = cuda_fail(e, "coarse inverse copy");
   }
