@@ -44,6 +44,10 @@ sys.path.insert(0, ROOT)
 METRIC = "particle pushes/s + Poisson ms/step: learned-precond FCG vs plain PCG at 1e-8"
 FP64_PUSH_BYTES = 80   # read x,y,vx,vy,elem (36 B) + vz on diagnostic steps, write x,y,vx,vy,elem (36 B)
 MIXED_PUSH_BYTES = 40  # read elem + 4 FP32 (20 B), write the same (20 B)
+# DRAM bytes per particle of one push launch measured by ncu (dram__bytes_read
+# + dram__bytes_write on the 1024^2 deck at 8 particles per cell; the traffic
+# grows in proportion to the particle count)
+NCU_PUSH_TRAFFIC = {"fp64": 68.0, "mixed": 37.9}
 
 
 def _dist():
@@ -428,7 +432,8 @@ def run_ours(args, dist, rank, ws):
         "roofline": {"kernel": "k_push (fused push+locate+deposit)", "bound": "hbm",
                      "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
                      "peak_source": peak_src, "bytes_per_particle": push_bytes,
-                     "traffic": None},
+                     "traffic": NCU_PUSH_TRAFFIC[args.precision] * push_n,
+                     "traffic_note": "ncu DRAM bytes/particle of a 6.4M-particle launch x particles per step"},
         "e2e": {"value": e2e_value, "unit": "particle pushes/s", "steps": e2e_steps,
                 "h2d_bytes_per_step": 8 * nn, "d2h_bytes_per_step": 4 * 8 * nn},
         "gpu_launches": int(launches),
