@@ -148,8 +148,8 @@ def _peaks():
 
 def cpu_baseline(cfg_name: str, sample_particles: int, steps: int, pcg_iters: int | None = None,
                  pcg_cap: int = 200):
-    """Times the oracle (C restatement of the reference step, one host thread)
-    on a bounded sample: push+deposit of `sample_particles` particles per
+    """Times the oracle (C restatement of the reference step, OpenMP on all
+    the host's threads) on a bounded sample: push+deposit of `sample_particles` particles per
     species for `steps` steps, extrapolated to the full particle count, plus
     RHS + Jacobi-PCG + PPR on the full mesh.  The PCG runs at most `pcg_cap`
     iterations per step and its time is scaled to `pcg_iters` iterations (the
@@ -211,10 +211,12 @@ def cpu_baseline(cfg_name: str, sample_particles: int, steps: int, pcg_iters: in
         t_field += t_rhs + t_pcg + (time.perf_counter() - t3)
     per_step = t_part / steps * (full_n / sample_n) + t_field / steps
     mesh.close()
-    desc = (f"{cfg.name}: push+deposit of {sample_n} of {full_n} particles for {steps} step(s), extrapolated "
+    threads = ob.load().or_threads()
+    desc = (f"{cfg.name}: {threads} host threads; push+deposit of {sample_n} of {full_n} particles for {steps} "
+            f"step(s), extrapolated "
             f"by particle count; RHS+Jacobi-PCG+PPR on the full {cfg.ncx}x{cfg.ncy} mesh, the PCG timed over "
             f"<= {pcg_cap} iterations and scaled to the step's {pcg_iters} iterations{note}")
-    return full_n / per_step, desc, per_step
+    return full_n / per_step, desc, per_step, threads
 
 
 def run_reference(args, dist, rank, ws):
@@ -222,14 +224,14 @@ def run_reference(args, dist, rank, ws):
         return 0
     cpu_baseline(args.config, min(args.cpu_sample, 20000), 1, pcg_iters=1, pcg_cap=1)  # warm-up (caches)
     steps = max(1, args.steps)
-    v, desc, per_step = cpu_baseline(args.config, args.cpu_sample, min(steps, 2))
+    v, desc, per_step, threads = cpu_baseline(args.config, args.cpu_sample, min(steps, 2))
     line = {
         "impl": "reference", "metric": METRIC, "value": v, "unit": "particle pushes/s",
         "n_gpus": args.gpus, "steps": steps, "warmup": args.warmup,
         "ms_per_step": per_step * 1e3, "higher_is_better": True, "scaling": "weak",
         "vs_baseline": None, "dtype": "f64", "data": "synthetic",
         "config": {"workload": args.config},
-        "cpu_baseline": {"value": v, "unit": "particle pushes/s", "cores": 1, "kind": "port",
+        "cpu_baseline": {"value": v, "unit": "particle pushes/s", "cores": threads, "kind": "port",
                          "sample": desc},
         "e2e": {"value": v, "unit": "particle pushes/s", "h2d_bytes_per_step": 0,
                 "d2h_bytes_per_step": 0},
@@ -441,8 +443,8 @@ def run_ours(args, dist, rank, ws):
     }
     if rank == 0 and ws == 1 and not args.no_cpu_baseline:
         jp = poisson["jacobi_pcg"]["iterations"]
-        v, desc, _ = cpu_baseline(args.config, args.cpu_sample, 1, pcg_iters=int(jp))
-        line["cpu_baseline"] = {"value": v, "unit": "particle pushes/s", "cores": 1, "kind": "port",
+        v, desc, _, threads = cpu_baseline(args.config, args.cpu_sample, 1, pcg_iters=int(jp))
+        line["cpu_baseline"] = {"value": v, "unit": "particle pushes/s", "cores": threads, "kind": "port",
                                 "sample": desc}
     sim.close()
     if rank == 0:

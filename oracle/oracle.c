@@ -18,6 +18,9 @@
  * convergence rates of Norm_Error_{0064,0128,0256}.txt; see tests/.
  */
 #include <math.h>
+#ifdef _OPENMP
+#include <omp.h>
+#endif
 #include <stdint.h>
 #include <stdlib.h>
 #include <string.h>
@@ -151,6 +154,7 @@ int64_t or_move_all(const pic_mesh_desc *d, int64_t n, double *x, double *y, dou
   mesh_open(&m, d);
   const int64_t nn = m.nn;
   int64_t lost = 0;
+#pragma omp parallel for schedule(static) reduction(+ : lost)
   for (int64_t p = 0; p < n; ++p) {
     int e = loc[p];
     if (e < 0) continue;
@@ -211,6 +215,8 @@ int64_t or_deposit(const pic_mesh_desc *d, int64_t n, const double *x, const dou
   Mesh m;
   mesh_open(&m, d);
   int64_t bad = 0;
+  /* integer sums: the node totals do not depend on the thread order */
+#pragma omp parallel for schedule(static) reduction(+ : bad)
   for (int64_t p = 0; p < n; ++p) {
     if (loc[p] < 0) continue;
     int e = locate(&m, x[p], y[p]);
@@ -221,8 +227,11 @@ int64_t or_deposit(const pic_mesh_desc *d, int64_t n, const double *x, const dou
     weights(&m, e, x[p], y[p], W, nd);
     double energy = ((((0.5 * mass) * ((vx[p] * vx[p] + vy[p] * vy[p]) + vz[p] * vz[p])) * vref) * vref) / OR_JTOEV;
     for (int c = 0; c < 4; ++c) {
-      q_acc[nd[c]] += llrint(W[c] * OR_QSCALE);
-      e_acc[nd[c]] += llrint((W[c] * energy) * OR_ESCALE);
+      const int64_t dq = llrint(W[c] * OR_QSCALE), de = llrint((W[c] * energy) * OR_ESCALE);
+#pragma omp atomic
+      q_acc[nd[c]] += dq;
+#pragma omp atomic
+      e_acc[nd[c]] += de;
     }
   }
   mesh_close(&m);
@@ -322,6 +331,8 @@ static double final_sum(const double *part, int nb) {
 double or_canon_dot(const double *a, const double *b, int64_t n) {
   int nb = (int)((n + RT * RI - 1) / (RT * RI));
   double *part = (double *)malloc(sizeof(double) * (nb > 0 ? nb : 1));
+  /* blocks are independent; their partials are summed in block order */
+#pragma omp parallel for schedule(static)
   for (int blk = 0; blk < nb; ++blk) {
     double t[RT];
     for (int th = 0; th < RT; ++th) {
@@ -342,6 +353,7 @@ double or_canon_dot(const double *a, const double *b, int64_t n) {
 /* CSR matvec over the full grid (MATVEC_1.f90:14-22); Dirichlet rows 0 */
 static void matvec(const pic_mesh_desc *d, const int64_t *u2n, const double *v, double *y) {
   int64_t nn = (int64_t)d->nnx * d->nny;
+#pragma omp parallel for schedule(static)
   for (int64_t i = 0; i < nn; ++i) {
     int u = d->node_type[i];
     if (u <= 0) { y[i] = 0.0; continue; }
@@ -377,11 +389,13 @@ void or_pcg(const pic_mesh_desc *d, const double *b, double *phi, double tol, in
   double tol2 = tol * tol;
   int iter = 0, ierr = 0, done = !(normRHS > 0.0);
   while (!done) {
+#pragma omp parallel for schedule(static)
     for (int64_t i = 0; i < nn; ++i) p[i] = iter == 0 ? w[i] : fma(beta, p[i], w[i]);
     matvec(d, u2n, p, q);
     double pq = or_canon_dot(p, q, nn);
     if (pq == 0.0) { ierr = 3; break; }
     double alpha = rho / pq;
+#pragma omp parallel for schedule(static)
     for (int64_t i = 0; i < nn; ++i) {
       x[i] = fma(alpha, p[i], x[i]);
       r[i] = fma(-alpha, q[i], r[i]);
@@ -434,6 +448,7 @@ void or_ppr(const pic_mesh_desc *d, const double *phi, double *coef, double *efx
   Mesh m;
   mesh_open(&m, d);
   int64_t nn = m.nn;
+#pragma omp parallel for schedule(dynamic, 1024)
   for (int64_t i = 0; i < nn; ++i) {
     int b0 = d->patch_ptr[i], cnt = d->patch_ptr[i + 1] - b0;
     double c[5] = {0, 0, 0, 0, 0};
@@ -741,4 +756,13 @@ int or_ife_closed_form(int typ, int bi, int pf, double a, double b, double R, do
     return 0;
   }
   return 0;
+}
+
+/* Host threads the oracle's parallel loops use (OpenMP; 1 without it). */
+int or_threads(void) {
+#ifdef _OPENMP
+  return omp_get_max_threads();
+#else
+  return 1;
+#endif
 }

@@ -43,6 +43,7 @@ def load():
                                  _P(_d), _P(_d)]
     lib.or_rhs.argtypes = [M, _d, _d]
     lib.or_pcg.argtypes = [M, _d, _d, C.c_double, C.c_int, _d]
+    lib.or_threads.restype = C.c_int
     lib.or_ppr.argtypes = [M, _d, _d, _d, _d]
     lib.or_sort_perm.argtypes = [C.c_int64, _i, _u, _l]
     lib.or_sort_perm.restype = C.c_int64
