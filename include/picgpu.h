@@ -272,8 +272,11 @@ int pic_mcc(uint64_t step, pic_mcc_stats *stats);
 int pic_step(uint64_t step, pic_step_stats *stats);
 
 /* Field readback (host, [nodes]).  which: 0 rho, 1 phi, 2 efx, 3 efy,
- * 4+s rho_s of species s, 8+s Ek_tot of species s (normalised like rho_s),
- * 12..16 coef_ppr(2..6,:). */
+ * 4+s rho_s of species s, 8+s Ek_s of species s (mean energy per particle,
+ * eV), 12..16 coef_ppr(2..6,:), 20 the solver's right-hand side b, 24+s
+ * Ek_tot of species s (energy density, normalised like rho_s:
+ * GetParChg_2D.f90:895-904).  Ek_s and Ek_tot are those of the last step
+ * that deposited energy (pic_params.diag_interval). */
 int pic_get_field(int32_t which, double *host_out);
 /* Field upload (host, [nodes]): which 1 phi, 2 efx, 3 efy, 12..16 coef_ppr. */
 int pic_set_field(int32_t which, const double *host_in);
@@ -341,6 +344,37 @@ int pic_apply_operator(const double *v_dev, double *out_dev);
 /* Device pointers of the solver's right-hand side b and potential phi
  * (full grid), valid until pic_finalize. */
 int pic_solver_vectors(double **b_dev, double **phi_dev);
+
+/* ---- diagnostics (computed on the device) ---- */
+
+/* Average_x (In-Output/Output_To_Tecplot_IJK_2D.f90:166-226, the column
+ * profiles of the field output): for each mesh column x = x_i the mean over
+ * its nodes, in the file's output scaling.  out is host memory,
+ * [(3 + 3*n_species) * nnx], column-major by quantity: x*L_ref, phi*Phi_ref,
+ * rho*n_ref, then rho_s*n_ref, Ek_s and Ek_tot of each species in species
+ * order (the reference's nine columns for two species).  Each column is summed
+ * in node order (j ascending), as the reference does. */
+int pic_average_x(double *out);
+
+/* Output_Energy.f90:41-71: counts of one species' live particles whose
+ * energy (eV, EnergyParticleOne with VFactor, base/ParticleOne.f90:235-244)
+ * lies in (E_max*(b-1)/N, E_max*b/N] and whose vx lies in
+ * (V_max*(b-1-N/2)/N, V_max*(b-N/2)/N], b = 1..N (0-based arrays here), with
+ * the reference's edge arithmetic.  The reference uses N = 100, E_max = 5 eV
+ * and V_max = 10, 0.1, 0.01 by species; dN/dE = 10*count/n_ini is the
+ * caller's.  count_e, count_vx: host [nbins].  1 <= nbins <= 4096. */
+int pic_energy_spectrum(int32_t species, int32_t nbins, double e_max_ev, double v_max,
+                        int64_t *count_e, int64_t *count_vx);
+
+/* OUTPUT_velocity.f90:48-103: one species' live particles binned by x column
+ * b = min(max(floor(x), 0), nbins-1) (the reference uses 1024); per column
+ * the count, the drift velocity (mean of vx, vy, vz; 0 for an empty column)
+ * and the thermal velocity sqrt(mean (v - drift)^2).  count: host [nbins];
+ * drift, thermal: host [3][nbins] (vx, vy, vz).  FP64 sums (the reference
+ * sums in FP32); their order varies from call to call, so the last bits
+ * can.  1 <= nbins <= 2048. */
+int pic_velocity_moments(int32_t species, int32_t nbins, int64_t *count, double *drift,
+                         double *thermal);
 
 /* ---- allocation-free deposit ---- */
 

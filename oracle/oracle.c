@@ -766,3 +766,103 @@ int or_threads(void) {
   return 1;
 #endif
 }
+
+/* ------------------------------------------------------------------ */
+/* Diagnostics                                                          */
+/* ------------------------------------------------------------------ */
+
+/* GetParChg_2D.f90:880-904 (delta = 0): node energy density of one species,
+ * Ek_tot = Weight * sum(W*E) / L_ref / L_ref / n_ref / V, from the
+ * fixed-point energy sums of or_deposit. */
+void or_ek_tot(const pic_mesh_desc *d, const int64_t *e_acc, double weight, double L_ref, double n_ref,
+               double *ek_tot) {
+  int64_t nn = (int64_t)d->nnx * d->nny;
+  for (int64_t i = 0; i < nn; ++i) {
+    double es = (double)e_acc[i] * (1.0 / OR_ESCALE);
+    ek_tot[i] = ((((weight * es) / L_ref) / L_ref) / n_ref) / d->cell_volume[i];
+  }
+}
+
+/* Output_To_Tecplot_IJK_2D.f90:184-215 (Average_x): the nodes with x = x_i
+ * are column i of the grid, visited in node order (j ascending); their sum
+ * divided by their count, times the output scale of :220-223. */
+void or_average_x(int nnx, int nny, const double *f, double scale, double *out) {
+  for (int i = 0; i < nnx; ++i) {
+    double s = 0.0;
+    int count = 0;
+    for (int j = 0; j < nny; ++j) {
+      s = s + f[(int64_t)i * nny + j];
+      count = count + 1;
+    }
+    out[i] = (s / (double)count) * scale;
+  }
+}
+
+/* Output_Energy.f90:41-71: bin edges Ek_per(i+1) = Ek_max*REAL(i)/N and
+ * Vk_per(i+1) = Vk_max*REAL(i-(0.5*N))/N (REAL: single precision, exact
+ * here), i = 0..N; a particle counts in bin b when edge(b) < value <=
+ * edge(b+1), tested against every bin as the reference does.  Energy:
+ * EnergyParticleOne (base/ParticleOne.f90:235-244) times VFactor^2, / JtoeV.
+ * Only live particles (loc >= 0). */
+void or_energy_spectrum(int64_t n, const double *vx, const double *vy, const double *vz, const int32_t *loc,
+                        double mass, double vref, int nbins, double e_max, double v_max, int64_t *count_e,
+                        int64_t *count_vx) {
+  double *ee = (double *)malloc(sizeof(double) * (nbins + 1));
+  double *ve = (double *)malloc(sizeof(double) * (nbins + 1));
+  for (int i = 0; i <= nbins; ++i) {
+    ee[i] = (e_max * (double)(float)i) / (double)nbins;
+    ve[i] = (v_max * (double)((float)i - 0.5f * (float)nbins)) / (double)nbins;
+  }
+  for (int b = 0; b < nbins; ++b) count_e[b] = count_vx[b] = 0;
+  for (int64_t p = 0; p < n; ++p) {
+    if (loc[p] < 0) continue;
+    double e = ((((0.5 * mass) * ((vx[p] * vx[p] + vy[p] * vy[p]) + vz[p] * vz[p])) * vref) * vref) / OR_JTOEV;
+    double v = vx[p];
+    for (int b = 0; b < nbins; ++b) {
+      if (e <= ee[b + 1] && e > ee[b]) count_e[b] += 1;
+      if (v <= ve[b + 1] && v > ve[b]) count_vx[b] += 1;
+    }
+  }
+  free(ee);
+  free(ve);
+}
+
+/* OUTPUT_velocity.f90:48-103: column num = MIN(MAX(1, FLOOR(X)+1), N)
+ * (0-based here); pass 1 sums vx, vy, vz and counts per column, drift =
+ * sum/count (0 for an empty column); pass 2 sums (v - drift)^2, thermal =
+ * sqrt(that/count).  FP64 sums in particle order (the reference's are FP32).
+ * drift, thermal: [3][nbins]. */
+void or_velocity_moments(int64_t n, const double *x, const double *vx, const double *vy, const double *vz,
+                         const int32_t *loc, int nbins, int64_t *count, double *drift, double *thermal) {
+  const double *v[3] = {vx, vy, vz};
+  double *sum = (double *)calloc((size_t)3 * nbins, sizeof(double));
+  for (int b = 0; b < nbins; ++b) count[b] = 0;
+  for (int pass = 0; pass < 2; ++pass) {
+    for (int b = 0; b < 3 * nbins; ++b) sum[b] = 0.0;
+    for (int64_t p = 0; p < n; ++p) {
+      if (loc[p] < 0) continue;
+      double f = floor(x[p]);
+      int b = (f >= 0.0) ? ((f >= (double)(nbins - 1)) ? nbins - 1 : (int)f) : 0;
+      if (pass == 0) count[b] += 1;
+      for (int c = 0; c < 3; ++c) {
+        double t = v[c][p];
+        if (pass == 1) {
+          double dd = t - drift[c * nbins + b];
+          t = dd * dd;
+        }
+        sum[c * nbins + b] = sum[c * nbins + b] + t;
+      }
+    }
+    double *out = pass == 0 ? drift : thermal;
+    for (int c = 0; c < 3; ++c)
+      for (int b = 0; b < nbins; ++b) {
+        double r = 0.0;
+        if (count[b] != 0) {
+          r = sum[c * nbins + b] / (double)count[b];
+          if (pass == 1) r = sqrt(r);
+        }
+        out[c * nbins + b] = r;
+      }
+  }
+  free(sum);
+}

@@ -21,6 +21,7 @@ PIC_SHAPE_CIRCLE, PIC_SHAPE_BOX, PIC_SHAPE_ELLIPSE = 1, 3, 5
 PIC_WALL_ABSORB, PIC_WALL_REFLECT = 0, 1
 PIC_PREC_FP64, PIC_PREC_MIXED = 0, 1
 PIC_SOLVER_JPCG, PIC_SOLVER_FCG_UNET = 0, 1
+PIC_ERR_ARG, PIC_ERR_STATE = -1, -6
 
 ERRORS = {
     -1: "PIC_ERR_ARG", -2: "PIC_ERR_CUDA", -3: "PIC_ERR_SOLVER_CAP", -4: "PIC_ERR_NAN",
@@ -38,7 +39,8 @@ EXPORTS = [
     "pic_particle_device_ptrs", "pic_kernel_launches", "pic_device_timer",
     "pic_deposit_noalloc", "pic_set_preconditioner", "pic_set_solver", "pic_set_fcg_window",
     "pic_cuda_stream", "pic_apply_operator", "pic_solver_vectors", "pic_set_precond_stages",
-    "pic_coarse_setup", "pic_precond_apply", "pic_set_fcg_inner",
+    "pic_coarse_setup", "pic_precond_apply", "pic_set_fcg_inner", "pic_average_x",
+    "pic_energy_spectrum", "pic_velocity_moments",
 ]
 
 # z = M(r) callback of flexible CG: (r_dev, z_dev, user) -> 0 or failure
@@ -189,6 +191,10 @@ def load() -> C.CDLL:
                                         C.c_void_p, C.c_double, C.c_double, C.c_double, C.c_void_p,
                                         C.c_void_p]
     lib.pic_particle_device_ptrs.argtypes = [C.c_int32, _P(C.c_void_p), _P(C.c_int64)]
+    lib.pic_average_x.argtypes = [d]
+    lib.pic_energy_spectrum.argtypes = [C.c_int32, C.c_int32, C.c_double, C.c_double,
+                                        _P(C.c_int64), _P(C.c_int64)]
+    lib.pic_velocity_moments.argtypes = [C.c_int32, C.c_int32, _P(C.c_int64), d, d]
     _lib = lib
     return lib
 
@@ -218,6 +224,13 @@ def uptr(a: np.ndarray | None):
         return None
     assert a.dtype == np.uint32 and a.flags.c_contiguous
     return a.ctypes.data_as(_P(C.c_uint32))
+
+
+def lptr(a: np.ndarray | None):
+    if a is None:
+        return None
+    assert a.dtype == np.int64 and a.flags.c_contiguous
+    return a.ctypes.data_as(_P(C.c_int64))
 
 
 def as_np(ptr, n: int, dtype) -> np.ndarray:

@@ -5,6 +5,7 @@
 #include <cuda_fp16.h>
 #include <cuda_runtime.h>
 
+#include <cstring>
 #include <string>
 #include <vector>
 
@@ -65,9 +66,11 @@ struct Species {
   double *x2 = nullptr, *y2 = nullptr, *vx2 = nullptr, *vy2 = nullptr, *vz2 = nullptr;
   int32_t *loc2 = nullptr;
   uint32_t *id2 = nullptr;
-  // deposit accumulators (fixed point) and normalised per-species fields
+  // deposit accumulators (fixed point) and normalised per-species fields:
+  // rho_s charge density, ek_s mean energy per particle (eV), ek_tot energy
+  // density (GetParChg_2D.f90:880-904; ek_s and ek_tot on energy steps)
   unsigned long long *q_acc = nullptr, *e_acc = nullptr;
-  double *rho_s = nullptr, *ek_s = nullptr;
+  double *rho_s = nullptr, *ek_s = nullptr, *ek_tot = nullptr;
   // MCC
   bool has_mcc = false;
   pic_mcc_table tab;
@@ -209,6 +212,7 @@ int precond_learned_on();
 int precond_prepare();
 int precond_callback();
 void precond_free();
+void diag_free();
 
 inline int blocks_for(int64_t n, int threads) { return (int)((n + threads - 1) / threads); }
 

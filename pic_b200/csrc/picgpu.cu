@@ -550,15 +550,16 @@ __global__ void k_from_mixed(MeshK m, const float *__restrict__ ax, const float 
 
 struct RhoK {
   const unsigned long long *q[PIC_MAX_SPECIES], *e[PIC_MAX_SPECIES];
-  double *rho_s[PIC_MAX_SPECIES], *ek_s[PIC_MAX_SPECIES];
+  double *rho_s[PIC_MAX_SPECIES], *ek_s[PIC_MAX_SPECIES], *ek_tot[PIC_MAX_SPECIES];
   double wq[PIC_MAX_SPECIES], w[PIC_MAX_SPECIES];
   int ns;
   double L_ref, n_ref;
   int energy;  // update the per-node mean energy (diagnostic steps)
 };
 
-// GetParChg_2D.f90:869-911: rho_s = Weight*qs*sum/L_ref/L_ref/n_ref/V; the
-// mean energy per particle (eV) Ek_s = sum(W*E)/sum(W) is kept per node.
+// GetParChg_2D.f90:869-911: rho_s = Weight*qs*sum/L_ref/L_ref/n_ref/V; on
+// energy steps the mean energy per particle (eV) Ek_s = sum(W*E)/sum(W) and
+// the energy density Ek_tot = Weight*sum(W*E)/L_ref/L_ref/n_ref/V per node.
 __global__ void k_rho(RhoK r, const double *__restrict__ vol, double *__restrict__ rho, int64_t nn) {
   int64_t n = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
   if (n >= nn) return;
@@ -569,7 +570,10 @@ __global__ void k_rho(RhoK r, const double *__restrict__ vol, double *__restrict
     double esum = (double)(long long)r.e[s][n] * (1.0 / PIC_E_SCALE);
     double rs = ((((r.wq[s] * cnt) / r.L_ref) / r.L_ref) / r.n_ref) / V;
     r.rho_s[s][n] = rs;
-    if (r.energy) r.ek_s[s][n] = (cnt != 0.0) ? esum / cnt : 0.0;
+    if (r.energy) {
+      r.ek_s[s][n] = (cnt != 0.0) ? esum / cnt : 0.0;
+      r.ek_tot[s][n] = ((((r.w[s] * esum) / r.L_ref) / r.L_ref) / r.n_ref) / V;
+    }
     acc = acc + rs;
   }
   rho[n] = acc;
@@ -1970,6 +1974,7 @@ static void free_all() {
   F(g.d_r); F(g.d_w); F(g.d_p[0]); F(g.d_p[1]); F(g.d_q); F(g.d_part); F(g.d_pcg); F(g.d_bar);
   F(g.d_z); F(g.d_dot); F(g.d_dot_ticket); F(g.d_fcg); F(g.d_fcg_P); F(g.d_fcg_Q); F(g.d_fcg_part);
   precond_free();
+  diag_free();
   fcg_graphs_free();
   F(g.d_cell_count); F(g.d_cell_start); F(g.d_cell_fill); F(g.d_perm); F(g.d_perm2); F(g.d_sort_id);
   F(g.d_scan_blk); F(g.d_counters); F(g.d_hist); F(g.d_sel); F(g.d_cand); F(g.d_cand_slot);
@@ -1978,7 +1983,7 @@ static void free_all() {
     Species &p = g.sp[s];
     F(p.x); F(p.y); F(p.vx); F(p.vy); F(p.vz); F(p.loc); F(p.id);
     F(p.x2); F(p.y2); F(p.vx2); F(p.vy2); F(p.vz2); F(p.loc2); F(p.id2);
-    F(p.q_acc); F(p.e_acc); F(p.rho_s); F(p.ek_s); F(p.prob);
+    F(p.q_acc); F(p.e_acc); F(p.rho_s); F(p.ek_s); F(p.ek_tot); F(p.prob);
   }
   if (g.ev0) cudaEventDestroy(g.ev0);
   if (g.ev1) cudaEventDestroy(g.ev1);
@@ -2089,6 +2094,7 @@ static int run_rho(bool energy) {
     r.e[s] = g.sp[s].e_acc;
     r.rho_s[s] = g.sp[s].rho_s;
     r.ek_s[s] = g.sp[s].ek_s;
+    r.ek_tot[s] = g.sp[s].ek_tot;
     r.wq[s] = g.sp[s].weight * g.sp[s].charge;
     r.w[s] = g.sp[s].weight;
   }
@@ -3259,10 +3265,12 @@ int pic_init(const pic_mesh_desc *mesh, const pic_params *params) {
     if ((rc = dalloc(&sp.e_acc, nn))) return rc;
     if ((rc = dalloc(&sp.rho_s, nn))) return rc;
     if ((rc = dalloc(&sp.ek_s, nn))) return rc;
+    if ((rc = dalloc(&sp.ek_tot, nn))) return rc;
     PIC_CUDA(cudaMemset(sp.q_acc, 0, nn * sizeof(unsigned long long)));
     PIC_CUDA(cudaMemset(sp.e_acc, 0, nn * sizeof(unsigned long long)));
     PIC_CUDA(cudaMemset(sp.rho_s, 0, nn * sizeof(double)));
     PIC_CUDA(cudaMemset(sp.ek_s, 0, nn * sizeof(double)));
+    PIC_CUDA(cudaMemset(sp.ek_tot, 0, nn * sizeof(double)));
   }
   if ((rc = dalloc(&g.d_perm, maxcap))) return rc;
   if ((rc = dalloc(&g.d_perm2, maxcap))) return rc;
@@ -3583,6 +3591,7 @@ int pic_get_field(int32_t which, double *host_out) {
   else if (which >= 8 && which < 8 + g.ns) src = g.sp[which - 8].ek_s;
   else if (which >= 12 && which <= 16) src = g.d_coef + (size_t)(which - 12) * g.nn;
   else if (which == 20) src = g.d_b;
+  else if (which >= 24 && which < 24 + g.ns) src = g.sp[which - 24].ek_tot;
   if (!src) {
     set_error("pic_get_field: unknown field");
     return PIC_ERR_ARG;

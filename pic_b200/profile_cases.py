@@ -4,11 +4,14 @@ ncu (each runs a few launches of its kernels and exits):
     python -m pic_b200.profile_cases step  <deck> <ppc> <steps> [jpcg|fcg] [fp64|mixed]
     python -m pic_b200.profile_cases solve <cells> [jpcg|fcg] [repeats] [coarse_cells] [fp64|mixed]
     python -m pic_b200.profile_cases unet  <nodes> [repeats]
+    python -m pic_b200.profile_cases diag  <deck> <ppc> [fp64|mixed] [repeats]
 
 step:  the deck at <ppc> particles per cell and species, <steps> steps.
 solve: the 8-ellipse deck at <cells>^2 without particles, a seeded random
        charge density, Poisson solves from phi = 0.
 unet:  forward passes of the learned stage's network on a <nodes>^2 grid.
+diag:  the deck after one step, then the device diagnostics (Average_x
+       profiles, energy spectra, velocity moments) of every species.
 Each prints one line with its own CUDA-event time.
 """
 from __future__ import annotations
@@ -89,6 +92,31 @@ def _unet(nodes, repeats=10):
     print(f"unet forward {n}x{n}: {e0.elapsed_time(e1) / int(repeats):.3f} ms")
 
 
+def _diag(deck_name, ppc, precision="mixed", repeats=5):
+    import time
+    from . import api, deck
+    from .simulation import Simulation
+    prec = api.PIC_PREC_MIXED if precision == "mixed" else api.PIC_PREC_FP64
+    sim = Simulation(deck.config(deck_name, ppc=int(ppc), precision=prec, diag_interval=1))
+    sim.initial_fields()
+    sim.set_solver("fcg")
+    sim.step()
+    ns = len(sim.species)
+    n = [sim.count(s) for s in range(ns)]
+    calls = {"average_x": lambda: sim.average_x(),
+             "energy_spectrum": lambda: [sim.energy_spectrum(s) for s in range(ns)],
+             "velocity_moments": lambda: [sim.velocity_moments(s) for s in range(ns)]}
+    res = {}
+    for name, fn in calls.items():
+        fn()
+        t0 = time.perf_counter()
+        for _ in range(int(repeats)):
+            fn()
+        res[name] = round((time.perf_counter() - t0) / int(repeats) * 1e3, 3)
+    print(f"diag {sim.cfg.name} {precision} particles {n}: host ms per call (all species) {res}")
+    sim.close()
+
+
 if __name__ == "__main__":
     case, rest = sys.argv[1], sys.argv[2:]
-    {"step": _step, "solve": _solve, "unet": _unet}[case](*rest)
+    {"step": _step, "solve": _solve, "unet": _unet, "diag": _diag}[case](*rest)

@@ -149,7 +149,8 @@ class Simulation:
 
     # ---- fields ---------------------------------------------------------
     FIELDS = {"rho": 0, "phi": 1, "efx": 2, "efy": 3, "rho_e": 4, "rho_i": 5, "ek_e": 8,
-              "ek_i": 9, "c2": 12, "c3": 13, "c4": 14, "c5": 15, "c6": 16, "b": 20}
+              "ek_i": 9, "c2": 12, "c3": 13, "c4": 14, "c5": 15, "c6": 16, "b": 20,
+              "ektot_e": 24, "ektot_i": 25}
 
     def field(self, name: str) -> np.ndarray:
         out = np.empty(self.mesh.nn)
@@ -159,6 +160,48 @@ class Simulation:
     def set_field(self, name: str, values: np.ndarray):
         v = np.ascontiguousarray(values, dtype=np.float64)
         api.check(self.lib.pic_set_field(self.FIELDS[name], api.dptr(v)), "pic_set_field")
+
+    # ---- diagnostics, computed on the device ------------------------------
+    SPECIES_TAGS = ("ele", "ion", "s2", "s3")
+
+    def average_x(self) -> dict:
+        """Average_x column profiles (Output_To_Tecplot_IJK_2D.f90:166-226) in
+        the file's units: x [m], Phi [V], Rho, Rho_<sp> [m^-3], Ek_<sp> [eV],
+        Ek_tot_<sp>."""
+        ns, nnx = len(self.species), self.mesh.nnx
+        out = np.empty((3 + 3 * ns) * nnx)
+        api.check(self.lib.pic_average_x(api.dptr(out)), "pic_average_x")
+        out = out.reshape(3 + 3 * ns, nnx)
+        tags = self.SPECIES_TAGS[:ns]
+        names = (["x", "Phi", "Rho"] + ["Rho_" + t for t in tags] + ["Ek_" + t for t in tags]
+                 + ["Ek_tot_" + t for t in tags])
+        return dict(zip(names, out))
+
+    def energy_spectrum(self, s: int, nbins: int = 100, e_max: float = 5.0,
+                        v_max: float | None = None):
+        """Output_Energy.f90:41-71 counts of species s: (energy counts, vx
+        counts), defaults N = 100, Ek_max = 5 eV, Vk_max = 10, 0.1, 0.01."""
+        if v_max is None:
+            v_max = (10.0, 0.1, 0.01, 0.01)[s]
+        ce, cv = np.zeros(nbins, np.int64), np.zeros(nbins, np.int64)
+        api.check(self.lib.pic_energy_spectrum(s, nbins, e_max, v_max, api.lptr(ce), api.lptr(cv)),
+                  "pic_energy_spectrum")
+        return ce, cv
+
+    def velocity_moments(self, s: int, nbins: int = 1024):
+        """OUTPUT_velocity.f90:48-103 of species s: per x column the count,
+        drift velocity [3, nbins] and thermal velocity [3, nbins]."""
+        cnt = np.zeros(nbins, np.int64)
+        drift, thermal = np.zeros((3, nbins)), np.zeros((3, nbins))
+        api.check(self.lib.pic_velocity_moments(s, nbins, api.lptr(cnt), api.dptr(drift),
+                                                api.dptr(thermal)), "pic_velocity_moments")
+        return cnt, drift, thermal
+
+    def particle_totals(self):
+        """Main_IFE_Test_2.f90:473-497 (equal weights): real particles per
+        species, Npar * Weight, and their sum."""
+        ns = [self.count(s) * self.species[s][2] for s in range(len(self.species))]
+        return sum(ns), ns
 
     def close(self):
         self.lib.pic_finalize()

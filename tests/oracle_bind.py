@@ -54,6 +54,11 @@ def load():
     lib.or_mcc.restype = C.c_int64
     lib.or_ife_closed_form.argtypes = [C.c_int, C.c_int, C.c_int, C.c_double, C.c_double,
                                        C.c_double, _d]
+    lib.or_ek_tot.argtypes = [M, _l, C.c_double, C.c_double, C.c_double, _d]
+    lib.or_average_x.argtypes = [C.c_int, C.c_int, _d, C.c_double, _d]
+    lib.or_energy_spectrum.argtypes = [C.c_int64, _d, _d, _d, _i, C.c_double, C.c_double, C.c_int,
+                                       C.c_double, C.c_double, _l, _l]
+    lib.or_velocity_moments.argtypes = [C.c_int64, _d, _d, _d, _d, _i, C.c_int, _l, _d, _d]
     _lib = lib
     return lib
 
@@ -169,3 +174,33 @@ def closed_form(typ, bi, pf, a, b, R):
     C4 = np.zeros(4)
     ok = load().or_ife_closed_form(typ, bi, pf, a, b, R, d(C4))
     return C4 if ok else None
+
+
+def ek_tot(mesh_ptr, e_acc, weight, L_ref, n_ref, nn):
+    out = np.zeros(nn)
+    load().or_ek_tot(mesh_ptr, i64(e_acc), weight, L_ref, n_ref, d(out))
+    return out
+
+
+def average_x(f, nnx, nny, scale):
+    f = np.ascontiguousarray(f, dtype=np.float64)
+    out = np.zeros(nnx)
+    load().or_average_x(nnx, nny, d(f), scale, d(out))
+    return out
+
+
+def energy_spectrum(parts, mass, vref, nbins, e_max, v_max):
+    ce, cv = np.zeros(nbins, np.int64), np.zeros(nbins, np.int64)
+    n = parts["vx"].size
+    load().or_energy_spectrum(n, d(parts["vx"]), d(parts["vy"]), d(parts["vz"]), i32(parts["loc"]),
+                              mass, vref, nbins, e_max, v_max, i64(ce), i64(cv))
+    return ce, cv
+
+
+def velocity_moments(parts, nbins):
+    cnt = np.zeros(nbins, np.int64)
+    drift, thermal = np.zeros((3, nbins)), np.zeros((3, nbins))
+    n = parts["vx"].size
+    load().or_velocity_moments(n, d(parts["x"]), d(parts["vx"]), d(parts["vy"]), d(parts["vz"]),
+                               i32(parts["loc"]), nbins, i64(cnt), d(drift), d(thermal))
+    return cnt, drift, thermal

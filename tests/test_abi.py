@@ -30,6 +30,13 @@ def test_calls_before_init_fail_cleanly():
     rc = lib.pic_step(1, None)
     assert rc == -6
     assert b"pic_init" in lib.pic_last_error()
+    import numpy as np
+    out = np.zeros(64)
+    cnt = np.zeros(8, np.int64)
+    assert lib.pic_average_x(api.dptr(out)) == -6
+    assert lib.pic_energy_spectrum(0, 8, 5.0, 1.0, api.lptr(cnt), api.lptr(cnt)) == -6
+    assert b"pic_init" in lib.pic_last_error()
+    assert lib.pic_velocity_moments(0, 8, api.lptr(cnt), api.dptr(out), api.dptr(out)) == -6
 
 
 def test_mesh_builder_rejects_bad_decks():
