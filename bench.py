@@ -7,10 +7,11 @@ deposit of all particles, RHS + Poisson solve to the deck's tolerance, PPR
 field recovery, MCC null collisions, counting sort every sort_interval
 steps), data resident in HBM.  The metric is particle pushes/s with the
 Poisson ms/step of the solvers side by side: the reference's Jacobi-PCG,
-flexible CG with smoothing + coarse space, and the same with the learned
-U-Net stage, all at the deck's tolerance on the same systems.
+flexible CG with smoothing + a two-level coarse space or a multigrid V-cycle,
+and the two-level one with the learned U-Net stage, all at the deck's
+tolerance on the same systems.
 
-The default workload is the 1024x1024-cell, 8-ellipse deck (about 134M
+The default workload is the 1024x1024-cell, 8-ellipse deck (about 101M
 particles, Poisson tolerance 1e-8).  The run (1) trains the learned stage
 online on --train-steps Jacobi-PCG steps, (2) solves the same systems with
 every solver, (3) times --plain-steps steps of the plain FP64 Jacobi-PCG path,
@@ -331,9 +332,16 @@ def run_ours(args, dist, rank, ws):
     def sel_fcg32():
         sim.set_solver("fcg", coarse_cells=64, window=1, inner_fp32=True)
 
-    variants = {"jacobi_pcg": sel_jpcg, "fcg_smooth_coarse": sel_fcg}
+    def sel_mg():
+        sim.set_solver("fcg", window=1, multigrid=True)
+
+    def sel_mg32():
+        sim.set_solver("fcg", window=1, multigrid=True, inner_fp32=True)
+
+    variants = {"jacobi_pcg": sel_jpcg, "fcg_smooth_coarse": sel_fcg, "fcg_smooth_multigrid": sel_mg}
     if args.precision == "mixed":
         variants["fcg_smooth_coarse_fp32_iterations_in_fp64_refinement"] = sel_fcg32
+        variants["fcg_smooth_multigrid_fp32_iterations_in_fp64_refinement"] = sel_mg32
     if lp is not None:
         variants["fcg_smooth_coarse_learned"] = sel_learned
     poisson = _poisson_compare(sim, lib, api, variants)

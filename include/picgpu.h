@@ -326,11 +326,22 @@ int pic_set_fcg_inner(int32_t fp32);
  * Defaults: smoothing off, learned on, no coarse space, so registering fn
  * alone gives M = fn. */
 int pic_set_precond_stages(int32_t smoothing, double omega, int32_t learned);
-/* Builds the coarse space of stage 2: bilinear prolongation P from a uniform
- * coarse grid whose spacing is about min(cells)/coarse_cells nodes (a divisor
- * of both cell counts), Ac = P^T A P from mesh's stiffness matrix, inverted
- * on the host (at most 4500 coarse nodes).  coarse_cells = 0 removes it. */
+/* Builds the coarse space of stage 2 as a two-level method: bilinear
+ * prolongation P from a uniform coarse grid whose spacing is about
+ * min(cells)/coarse_cells nodes (a divisor of both cell counts), Ac = P^T A P
+ * from mesh's stiffness matrix, inverted on the device and applied from a
+ * scaled FP16 copy (at most 9000 coarse nodes).  coarse_cells = 0 removes it.
+ * Replaces a multigrid hierarchy. */
 int pic_coarse_setup(const pic_mesh_desc *mesh, int32_t coarse_cells);
+/* Builds the coarse space of stage 2 as a geometric multigrid V-cycle: the
+ * grid halved (every second node) until at most max_coarse_nodes remain
+ * (nnx-1 and nny-1 need enough factors of 2; at most 9000 nodes), Galerkin
+ * operators A_{l+1} = P^T A_l P of bilinear P from mesh's stiffness matrix,
+ * one damped-Jacobi sweep (stage 1's omega) down and up at each level, the
+ * coarsest level solved with its dense inverse (FP16 copy, FP64
+ * accumulation).  max_coarse_nodes <= 0 removes it.  Replaces a two-level
+ * coarse space.  No reference counterpart (MY_PCG is Jacobi-PCG). */
+int pic_multigrid_setup(const pic_mesh_desc *mesh, int32_t max_coarse_nodes);
 /* z = M(r) (full != 0), or stages 1-2 only (full == 0): the classical part
  * whose residual r - A z is the learned correction's input.  Device vectors,
  * enqueued on the library stream. */

@@ -40,7 +40,7 @@ EXPORTS = [
     "pic_deposit_noalloc", "pic_set_preconditioner", "pic_set_solver", "pic_set_fcg_window",
     "pic_cuda_stream", "pic_apply_operator", "pic_solver_vectors", "pic_set_precond_stages",
     "pic_coarse_setup", "pic_precond_apply", "pic_set_fcg_inner", "pic_average_x",
-    "pic_energy_spectrum", "pic_velocity_moments",
+    "pic_energy_spectrum", "pic_velocity_moments", "pic_multigrid_setup",
 ]
 
 # z = M(r) callback of flexible CG: (r_dev, z_dev, user) -> 0 or failure
@@ -185,6 +185,7 @@ def load() -> C.CDLL:
     lib.pic_solver_vectors.argtypes = [_P(C.c_void_p), _P(C.c_void_p)]
     lib.pic_set_precond_stages.argtypes = [C.c_int32, C.c_double, C.c_int32]
     lib.pic_coarse_setup.argtypes = [_P(MeshDesc), C.c_int32]
+    lib.pic_multigrid_setup.argtypes = [_P(MeshDesc), C.c_int32]
     lib.pic_precond_apply.argtypes = [C.c_int32, C.c_void_p, C.c_void_p]
     lib.pic_deposit_noalloc.argtypes = [C.c_int32, C.c_int32, C.c_double, C.c_double, C.c_double,
                                         C.c_double, C.c_int64, C.c_void_p, C.c_void_p, C.c_void_p,

@@ -83,19 +83,15 @@ __device__ __forceinline__ double v_edge(double v_max, int i, int n) {
   return (v_max * (double)((float)i - 0.5f * (float)n)) / (double)n;
 }
 
-// the bin b (0-based) of (edge(b), edge(b+1)] that holds v, or -1; the
-// candidate from the arithmetic is checked against the exact edges with its
-// two neighbours
-template <bool kVel>
-__device__ __forceinline__ int find_bin(double v, double vmax, int n) {
-  double t = kVel ? (v / vmax) * n + 0.5 * n : (v / vmax) * n;
+// the bin b (0-based) of (edge[b], edge[b+1]] that holds v, or -1.  t is
+// v's position in bin widths from edge[0] (a product with a reciprocal, good
+// to a few ulps); the candidate and its two neighbours are checked against
+// the exact edges.
+__device__ __forceinline__ int find_bin(double v, double t, const double *edge, int n) {
   if (!(t > -2.0) || !(t < n + 2.0)) return -1;
   const int b0 = (int)floor(t);
-  for (int b = max(b0 - 1, 0); b <= min(b0 + 1, n - 1); ++b) {
-    const double lo = kVel ? v_edge(vmax, b, n) : e_edge(vmax, b, n);
-    const double hi = kVel ? v_edge(vmax, b + 1, n) : e_edge(vmax, b + 1, n);
-    if (v <= hi && v > lo) return b;
-  }
+  for (int b = max(b0 - 1, 0); b <= min(b0 + 1, n - 1); ++b)
+    if (v <= edge[b + 1] && v > edge[b]) return b;
   return -1;
 }
 
@@ -111,6 +107,7 @@ struct SpecK {
   PartK s;
   int nbins;
   double mass, vref, e_max, v_max;
+  double e_inv, v_inv;  // nbins / e_max, nbins / v_max
   unsigned long long *ce, *cv;
 };
 
@@ -118,7 +115,13 @@ struct SpecK {
 // same number of iterations on every lane of a warp (the base index is
 // uniform), so the whole-warp match is legal.
 __global__ void __launch_bounds__(256) k_spectrum(SpecK k) {
-  extern __shared__ unsigned int sh[];  // [2][nbins]
+  extern __shared__ double edges[];  // [nbins+1] energy, [nbins+1] vx edges, then [2][nbins] counts
+  double *ee = edges, *ve = edges + k.nbins + 1;
+  unsigned int *sh = reinterpret_cast<unsigned int *>(edges + 2 * (k.nbins + 1));
+  for (int b = threadIdx.x; b <= k.nbins; b += blockDim.x) {
+    ee[b] = e_edge(k.e_max, b, k.nbins);
+    ve[b] = v_edge(k.v_max, b, k.nbins);
+  }
   for (int b = threadIdx.x; b < 2 * k.nbins; b += blockDim.x) sh[b] = 0u;
   __syncthreads();
   const int64_t stride = (int64_t)gridDim.x * blockDim.x;
@@ -129,8 +132,8 @@ __global__ void __launch_bounds__(256) k_spectrum(SpecK k) {
       const double vx = vget(k.s.vx, k.s.f32, p), vy = vget(k.s.vy, k.s.f32, p), vz = vget(k.s.vz, k.s.f32, p);
       // ParticleOne.f90:235-244 EnergyParticleOne with VFactor, then / JtoeV
       const double e = ((((0.5 * k.mass) * ((vx * vx + vy * vy) + vz * vz)) * k.vref) * k.vref) / PIC_JTOEV;
-      be = find_bin<false>(e, k.e_max, k.nbins);
-      bv = find_bin<true>(vx, k.v_max, k.nbins);
+      be = find_bin(e, e * k.e_inv, ee, k.nbins);
+      bv = find_bin(vx, vx * k.v_inv + 0.5 * k.nbins, ve, k.nbins);
     }
     warp_count(sh, be);
     warp_count(sh + k.nbins, bv);
@@ -188,15 +191,26 @@ __global__ void __launch_bounds__(256) k_vmoments(MomK k) {
       }
     }
     if (!kSecond) warp_count(cnt, b);
-    if (b >= 0) {
-      for (int c = 0; c < 3; ++c) {
-        double t = v[c];
-        if (kSecond) {
-          const double d = t - dr[c * k.nbins + b];
-          t = d * d;
-        }
-        atomicAdd(&acc[c * k.nbins + b], t);
+    double t[3];
+    for (int c = 0; c < 3; ++c) {
+      t[c] = v[c];
+      if (kSecond && b >= 0) {
+        const double d = v[c] - dr[c * k.nbins + b];
+        t[c] = d * d;
       }
+    }
+    // particles sorted by cell: the 32 lanes usually share a column, and then
+    // the warp sums first and adds once per component (every lane takes part
+    // in the shuffles; none is skipped by short-circuiting)
+    const int b_first = __shfl_sync(0xffffffffu, b, 0);
+    const bool same = __all_sync(0xffffffffu, b == b_first);
+    if (same) {
+      for (int c = 0; c < 3; ++c)
+        for (int o = 16; o > 0; o >>= 1) t[c] += __shfl_xor_sync(0xffffffffu, t[c], o);
+      if (b_first >= 0 && (threadIdx.x & 31) == 0)
+        for (int c = 0; c < 3; ++c) atomicAdd(&acc[c * k.nbins + b_first], t[c]);
+    } else if (b >= 0) {
+      for (int c = 0; c < 3; ++c) atomicAdd(&acc[c * k.nbins + b], t[c]);
     }
   }
   __syncthreads();
@@ -330,8 +344,10 @@ int pic_energy_spectrum(int32_t species, int32_t nbins, double e_max_ev, double 
   unsigned long long *cnt = static_cast<unsigned long long *>(d);
   PIC_CUDA(cudaMemsetAsync(cnt, 0, bytes, g.st));
   if (s.n_slots > 0) {
-    SpecK k{part_k(s), nbins, s.mass, g.v_ref, e_max_ev, v_max, cnt, cnt + nbins};
-    k_spectrum<<<grid_for(s.n_slots), 256, 2 * nbins * sizeof(unsigned int), g.st>>>(k);
+    SpecK k{part_k(s), nbins, s.mass, g.v_ref, e_max_ev, v_max, nbins / e_max_ev, nbins / v_max, cnt, cnt + nbins};
+    const size_t shb = 2 * (nbins + 1) * sizeof(double) + 2 * nbins * sizeof(unsigned int);
+    PIC_CUDA(cudaFuncSetAttribute(k_spectrum, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)shb));
+    k_spectrum<<<grid_for(s.n_slots), 256, shb, g.st>>>(k);
     PIC_LAUNCHED();
   }
   std::vector<unsigned long long> h(2 * (size_t)nbins);

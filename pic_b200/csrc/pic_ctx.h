@@ -10,6 +10,7 @@
 #include <vector>
 
 #include "../../include/picgpu.h"
+#include "mg_dev.h"
 #include "pic_common.h"
 
 namespace pic {
@@ -163,6 +164,7 @@ struct Ctx {
   __half *d_pc_ainv = nullptr;             // coarse inverse / pc_ainv_scale, FP16, row-major
   double pc_ainv_scale = 1.0;
   double *d_pc_rc = nullptr, *d_pc_ec = nullptr;
+  MgK mg{};                                 // multigrid hierarchy (mg.L = 0: none)
   // CUDA graphs of one FCG iteration: [0] stage A, [1 + slot] stage B + FCG
   // kernels of ring slot `slot`; rebuilt when the configuration key changes
   cudaGraphExec_t fcg_graph[2 + PIC_FCG_MAX_WINDOW] = {};
@@ -208,6 +210,9 @@ int launch_spmv(const double *v, double *out);  // out = A v (solver operator)
 int coarse_setup(const pic_mesh_desc *mesh, int coarse_cells);
 int precond_apply(int full, const double *r, double *z);
 int coarse_correct(const double *t, double *z, int assign);
+int mg_setup(const pic_mesh_desc *mesh, int max_coarse_nodes);
+int mg_correct(const double *t, double *z, int assign);
+inline bool coarse_on() { return g.pc_cs > 0 || g.mg.L > 1; }
 int precond_learned_on();
 int precond_prepare();
 int precond_callback();

@@ -1540,6 +1540,7 @@ struct FcgP {
   double ainv_scale;
   double *rc, *ec;
   int nnx, cs, ncx, ncy, coarse;
+  MgK mg;                        // multigrid V-cycle (mg.L > 1) in place of the two-level space
   double omega;
   FcgState *s;
   unsigned int *bar;
@@ -1661,7 +1662,42 @@ __global__ void __launch_bounds__(kWide, 1) k_fcg_persist(FcgP<V> F) {
       }
     }
     const V *r = rc_;
-    if (F.coarse) {
+    const MgK &M = F.mg;
+    if (M.L > 1) {
+      // (B') multigrid V-cycle of t: restriction and down-sweeps, the dense
+      // coarsest solve, up-sweeps; a grid barrier between dependent steps
+      const int64_t gtid = (int64_t)blockIdx.x * kWide + threadIdx.x, gth = (int64_t)gridDim.x * kWide;
+      for (int l = 1; l < M.L && ok; ++l) {
+        const MgLevel &L = M.lv[l];
+        const int64_t nl = (int64_t)L.nx * L.ny;
+        for (int64_t n = gtid; n < nl; n += gth) {
+          const int I = (int)(n / L.ny), J = (int)(n - (int64_t)I * L.ny);
+          L.r[n] = l == 1 ? mg_restrict(F.t, F.nnx, k.nny, I, J)
+                          : mg_restrict(M.lv[l - 1].t, M.lv[l - 1].nx, M.lv[l - 1].ny, I, J);
+        }
+        if (!(ok = barrier())) break;
+        if (l < M.L - 1) {
+          for (int64_t n = gtid; n < nl; n += gth) mg_smooth_node(L, omega, n);
+          if (!(ok = barrier())) break;
+        }
+      }
+      if (!ok) break;
+      for (int row = gwarp; row < nc; row += nwarps) {
+        const __half *arow = F.ainv + (size_t)row * nc;
+        double acc = 0.0;
+        for (int q = lane; q < nc; q += 32) acc = fma((double)__half2float(arow[q]), __ldcg(F.rc + q), acc);
+        for (int off = 16; off > 0; off >>= 1) acc += __shfl_xor_sync(0xffffffffu, acc, off);
+        if (lane == 0) F.ec[row] = acc * F.ainv_scale;
+      }
+      for (int l = M.L - 2; l >= 1; --l) {
+        if (!(ok = barrier())) break;
+        const MgLevel &L = M.lv[l];
+        const double *ec = mg_e(M, l + 1);
+        const int nyc = M.lv[l + 1].ny;
+        for (int64_t n = gtid; n < (int64_t)L.nx * L.ny; n += gth) mg_post_node(L, ec, nyc, omega, n);
+      }
+      if (!ok) break;
+    } else if (F.coarse) {
       // (B) restriction
       for (int C = gwarp; C < nc; C += nwarps) {
         const int I = C / F.ncy, J = C % F.ncy;
@@ -1713,8 +1749,20 @@ __global__ void __launch_bounds__(kWide, 1) k_fcg_persist(FcgP<V> F) {
         if (n < nn) {
           V zf = (V)0;
           if (k.row_kind[n] >= 0) {
-            auto za = [&](int64_t m) { return F.zA[m]; };
-            zf = vfma(om * F.dinv[n], r[n] - row_apply_v<V>(k, n, za), za(n));
+            if (M.L > 1) {
+              // zA + P e_1 formed at each neighbour (0 on Dirichlet nodes)
+              const double *e1 = mg_e(M, 1);
+              const int ny1 = M.lv[1].ny;
+              auto za = [&](int64_t m) {
+                if (k.row_kind[m] < 0) return (V)0;
+                const int i = (int)(m / k.nny), j = (int)(m - (int64_t)i * k.nny);
+                return (V)((double)F.zA[m] + mg_prolong(e1, ny1, i, j));
+              };
+              zf = vfma(om * F.dinv[n], r[n] - row_apply_v<V>(k, n, za), za(n));
+            } else {
+              auto za = [&](int64_t m) { return F.zA[m]; };
+              zf = vfma(om * F.dinv[n], r[n] - row_apply_v<V>(k, n, za), za(n));
+            }
           }
           F.zF[n] = zf;
           if (have_old) acc_zq = fma((double)zf, (double)Ql[n], acc_zq);
@@ -2257,7 +2305,10 @@ static int precond_stage_a(const double *r, double *zA, int learned) {
   if (g.pc_sweeps > 0) {
     k_pc_pre<<<nb, 256, 0, g.st>>>(k0, r, g.d_pc_dinv, g.pc_omega, zA, g.d_pc_t);
     PIC_LAUNCHED();
+    if (g.mg.L > 1 && (rc = mg_correct(g.d_pc_t, zA, 0))) return rc;
     if (g.pc_cs > 0 && (rc = coarse_correct(g.d_pc_t, zA, 0))) return rc;
+  } else if (g.mg.L > 1) {
+    if ((rc = mg_correct(r, zA, 1))) return rc;
   } else if (g.pc_cs > 0) {
     if ((rc = coarse_correct(r, zA, 1))) return rc;
   } else {
@@ -2282,7 +2333,7 @@ static int precond_stage_b(const double *r, const double *zA, double *zF, int le
     k.ring = 1;
     k.window = 1;
   }
-  const int smooth = (g.pc_sweeps > 0 && (g.pc_cs > 0 || learned)) ? 1 : 0;
+  const int smooth = (g.pc_sweeps > 0 && (coarse_on() || learned)) ? 1 : 0;
   k_fcg_post<<<g.red_blocks, PIC_RED_THREADS, 0, g.st>>>(k, r, zA, learned ? g.d_pc_y : nullptr, g.d_pc_dinv,
                                                          g.pc_omega, smooth, zF);
   PIC_LAUNCHED();
@@ -2412,6 +2463,7 @@ static int run_fcg(pic_solve_stats *stats, int *fcg_iters, int *rc_out) {
     key = key * 1000003ull + (unsigned long long)g.fcg_window;
     key = key * 1000003ull + (unsigned long long)(g.pc_sweeps * 2 + learned);
     key = key * 1000003ull + (unsigned long long)g.pc_cs;
+    key = key * 1000003ull + (unsigned long long)g.mg.L;
     key = key * 1000003ull + (unsigned long long)std::llround(g.pc_omega * 1e9);
     if (key != g.fcg_graph_key) {
       fcg_graphs_free();
@@ -2432,6 +2484,14 @@ static int run_fcg(pic_solve_stats *stats, int *fcg_iters, int *rc_out) {
       F.ncx = g.pc_ncx;
       F.ncy = g.pc_ncy;
       F.coarse = g.pc_cs > 0 ? 1 : 0;
+      F.mg = g.mg;
+      if (g.mg.L > 1) {  // the coarsest level's r and z feed the dense solve
+        const MgLevel &C = g.mg.lv[g.mg.L - 1];
+        F.rc = C.r;
+        F.ec = C.z;
+        F.ncx = C.nx;
+        F.ncy = C.ny;
+      }
       F.omega = g.pc_omega;
       F.s = g.d_fcg;
       F.bar = g.d_bar;
@@ -2621,7 +2681,7 @@ static int run_fcg(pic_solve_stats *stats, int *fcg_iters, int *rc_out) {
 // Solver dispatch: flexible CG with the registered preconditioner, else (or
 // after an FCG hand-over) Jacobi-PCG warm-started from the FCG iterate.
 static int run_solve(pic_solve_stats *stats) {
-  if (g.solver == PIC_SOLVER_FCG_UNET && ((g.pc_learned && g.precond) || g.pc_cs > 0 || g.pc_sweeps > 0)) {
+  if (g.solver == PIC_SOLVER_FCG_UNET && ((g.pc_learned && g.precond) || coarse_on() || g.pc_sweeps > 0)) {
     int fcg_iters = 0, rc = PIC_OK;
     if (stats) stats->outer = 0;
     int fallback = run_fcg(stats, &fcg_iters, &rc);
@@ -2731,6 +2791,22 @@ int pic_coarse_setup(const pic_mesh_desc *mesh, int32_t coarse_cells) {
     return PIC_ERR_ARG;
   }
   return coarse_setup(mesh, coarse_cells);
+}
+
+int pic_multigrid_setup(const pic_mesh_desc *mesh, int32_t max_coarse_nodes) {
+  if (!g.inited) {
+    set_error("pic_multigrid_setup: library not initialised (pic_init)");
+    return PIC_ERR_STATE;
+  }
+  if (!mesh || mesh->nnx != g.m.nnx || mesh->nny != g.m.nny) {
+    set_error("pic_multigrid_setup: mesh does not match the initialised one");
+    return PIC_ERR_ARG;
+  }
+  if (max_coarse_nodes > 9000) {
+    set_error("pic_multigrid_setup: max_coarse_nodes above 9000");
+    return PIC_ERR_ARG;
+  }
+  return mg_setup(mesh, max_coarse_nodes);
 }
 
 int pic_precond_apply(int32_t full, const double *r_dev, double *z_dev) {

@@ -13,6 +13,7 @@
 // none of this has a counterpart there.
 #include <cuda_fp16.h>
 
+#include <algorithm>
 #include <cmath>
 #include <cstring>
 #include <vector>
@@ -95,6 +96,41 @@ __global__ void k_pc_prolong(CoarseK c, const double *__restrict__ ec, const int
   z[n] = assign ? v : z[n] + v;
 }
 
+// ---- multigrid V-cycle, one launch per operation (the persistent solver
+// runs the same per-node functions between grid barriers)
+
+__global__ void k_mg_restrict(MgLevel L, const double *__restrict__ tf, int nxf, int nyf) {
+  const int64_t n = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (n >= (int64_t)L.nx * L.ny) return;
+  const int I = (int)(n / L.ny), J = (int)(n - (int64_t)I * L.ny);
+  L.r[n] = mg_restrict(tf, nxf, nyf, I, J);
+}
+
+__global__ void k_mg_smooth(MgLevel L, double w) {
+  const int64_t n = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (n < (int64_t)L.nx * L.ny) mg_smooth_node(L, w, n);
+}
+
+__global__ void k_mg_post(MgLevel L, const double *__restrict__ ec, int nyc, double w) {
+  const int64_t n = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (n < (int64_t)L.nx * L.ny) mg_post_node(L, ec, nyc, w, n);
+}
+
+// z (+)= P e_1 on unknown nodes of the solver's grid (z = P e_1 and 0 on
+// Dirichlet nodes with assign)
+__global__ void k_mg_prolong0(const double *__restrict__ e1, int ny1, const int32_t *__restrict__ row_kind, int nny,
+                              int assign, double *__restrict__ z, int64_t nn) {
+  const int64_t n = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (n >= nn) return;
+  if (row_kind[n] < 0) {
+    if (assign) z[n] = 0.0;
+    return;
+  }
+  const int i = (int)(n / nny), j = (int)(n - (int64_t)i * nny);
+  const double pe = mg_prolong(e1, ny1, i, j);
+  z[n] = assign ? pe : z[n] + pe;
+}
+
 __global__ void k_pc_dinv(const double *__restrict__ diag, double *__restrict__ dinv, int64_t nn) {
   int64_t n = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
   if (n < nn) dinv[n] = 1.0 / diag[n];
@@ -133,6 +169,39 @@ int coarse_correct(const double *t, double *z, int assign) {
   PIC_LAUNCHED();
   k_pc_prolong<<<blocks_for(g.nn, PC_THREADS), PC_THREADS, 0, g.st>>>(c, g.d_pc_ec, g.d_row_kind, assign, z,
                                                                         g.nn);
+  PIC_LAUNCHED();
+  return PIC_OK;
+}
+
+// z += P V(t) (z = P V(t) with assign): the multigrid V-cycle of t, the
+// solver-grid residual after pre-smoothing (0 on Dirichlet nodes)
+int mg_correct(const double *t, double *z, int assign) {
+  const MgK &M = g.mg;
+  const double w = g.pc_omega;
+  for (int l = 1; l < M.L; ++l) {
+    const MgLevel &L = M.lv[l];
+    const int64_t nl = (int64_t)L.nx * L.ny;
+    const double *tf = l == 1 ? t : M.lv[l - 1].t;
+    const int nxf = l == 1 ? g.m.nnx : M.lv[l - 1].nx, nyf = l == 1 ? g.m.nny : M.lv[l - 1].ny;
+    k_mg_restrict<<<blocks_for(nl, PC_THREADS), PC_THREADS, 0, g.st>>>(L, tf, nxf, nyf);
+    PIC_LAUNCHED();
+    if (l < M.L - 1) {
+      k_mg_smooth<<<blocks_for(nl, PC_THREADS), PC_THREADS, 0, g.st>>>(L, w);
+      PIC_LAUNCHED();
+    }
+  }
+  const MgLevel &C = M.lv[M.L - 1];
+  const int nc = C.nx * C.ny;
+  k_pc_gemv<<<(nc + 7) / 8, 256, 0, g.st>>>(g.d_pc_ainv, g.pc_ainv_scale, C.r, C.z, nc);
+  PIC_LAUNCHED();
+  for (int l = M.L - 2; l >= 1; --l) {
+    const MgLevel &L = M.lv[l];
+    k_mg_post<<<blocks_for((int64_t)L.nx * L.ny, PC_THREADS), PC_THREADS, 0, g.st>>>(L, mg_e(M, l + 1),
+                                                                                     M.lv[l + 1].ny, w);
+    PIC_LAUNCHED();
+  }
+  k_mg_prolong0<<<blocks_for(g.nn, PC_THREADS), PC_THREADS, 0, g.st>>>(mg_e(M, 1), M.lv[1].ny, g.d_row_kind,
+                                                                        g.m.nny, assign, z, g.nn);
   PIC_LAUNCHED();
   return PIC_OK;
 }
@@ -178,19 +247,97 @@ __global__ void k_diag_of(const double *__restrict__ a, double *__restrict__ d, 
   if (i < n) d[i] = a[(size_t)i * n + i];
 }
 
+// Inverts the dense SPD nc x nc matrix Ac on the device (Gauss-Jordan, FP64)
+// and keeps the scaled FP16 copy the solver reads in g.d_pc_ainv.
+int dense_inverse_f16(const std::vector<double> &Ac, int nc, const char *who) {
+  int rc;
+  double *d_a = nullptr, *d_row = nullptr, *d_col = nullptr;
+  int *d_bad = nullptr;
+  const size_t nc2 = (size_t)nc * nc;
+  if ((rc = pc_alloc(&d_a, nc2))) return rc;
+  if ((rc = pc_alloc(&d_row, nc)) || (rc = pc_alloc(&d_col, nc)) || (rc = pc_alloc(&d_bad, 1))) {
+    cudaFree(d_a);
+    return rc;
+  }
+  auto release = [&]() {
+    cudaFree(d_a);
+    cudaFree(d_row);
+    cudaFree(d_col);
+    cudaFree(d_bad);
+  };
+  int bad = 0;
+  cudaError_t e = cudaMemcpyAsync(d_a, Ac.data(), nc2 * sizeof(double), cudaMemcpyHostToDevice, g.st);
+  if (e == cudaSuccess) e = cudaMemsetAsync(d_bad, 0, sizeof(int), g.st);
+  for (int k = 0; e == cudaSuccess && k < nc; ++k) {
+    k_gj_pivot<<<(nc + 255) / 256, 256, 0, g.st>>>(d_a, nc, k, d_row, d_col, d_bad);
+    k_gj_update<<<(unsigned)((nc2 + 255) / 256), 256, 0, g.st>>>(d_a, nc, k, d_row, d_col);
+    e = cudaPeekAtLastError();
+  }
+  if (e == cudaSuccess) e = cudaMemcpyAsync(&bad, d_bad, sizeof(int), cudaMemcpyDeviceToHost, g.st);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(g.st);
+  if (e != cudaSuccess) {
+    release();
+    return cuda_fail(e, "coarse operator inversion");
+  }
+  if (bad) {
+    release();
+    set_error(std::string(who) + ": coarse operator is not positive definite");
+    return PIC_ERR_SETUP;
+  }
+  // The per-iteration GEMV reads a scaled FP16 copy (a quarter of the FP64
+  // bytes: 36 MB at 65x65 coarse nodes, so it and the solver's vectors fit in
+  // L2 together) and accumulates in FP64.  A preconditioner tolerates the
+  // 2^-11 relative rounding of the coarse correction; convergence is always
+  // judged on the FP64 residual.
+  std::vector<double> dg(nc);
+  k_diag_of<<<(nc + 255) / 256, 256, 0, g.st>>>(d_a, d_row, nc);
+  e = cudaMemcpyAsync(dg.data(), d_row, nc * sizeof(double), cudaMemcpyDeviceToHost, g.st);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(g.st);
+  double dmax = 0.0;
+  for (double v : dg) dmax = std::max(dmax, std::fabs(v));
+  g.pc_ainv_scale = (dmax > 0.0) ? dmax / 16384.0 : 1.0;
+  rc = (e == cudaSuccess) ? pc_alloc(&g.d_pc_ainv, nc2) : cuda_fail(e, "coarse inverse diagonal");
+  if (!rc) {
+    k_to_f16<<<(unsigned)((nc2 + 255) / 256), 256, 0, g.st>>>(d_a, g.d_pc_ainv, 1.0 / g.pc_ainv_scale,
+                                                               (int64_t)nc2);
+    e = cudaStreamSynchronize(g.st);
+    if (e != cudaSuccess) rc = cuda_fail(e, "coarse inverse copy");
+  }
+  release();
+  if (rc) return rc;
+  return PIC_OK;
+}
+
+void coarse_free() {
+  if (g.d_pc_ainv) cudaFree(g.d_pc_ainv);
+  if (g.d_pc_rc) cudaFree(g.d_pc_rc);
+  if (g.d_pc_ec) cudaFree(g.d_pc_ec);
+  g.d_pc_ainv = nullptr;
+  g.d_pc_rc = g.d_pc_ec = nullptr;
+  g.pc_cs = 0;
+}
+
+void mg_free() {
+  for (int l = 1; l < PIC_MG_MAX_LEVELS; ++l) {
+    MgLevel &L = g.mg.lv[l];
+    for (void *p : {(void *)L.st, (void *)L.dinv, (void *)L.r, (void *)L.z, (void *)L.t})
+      if (p) cudaFree(p);
+    L = MgLevel{};
+  }
+  if (g.mg.L > 1 && g.d_pc_ainv) {
+    cudaFree(g.d_pc_ainv);
+    g.d_pc_ainv = nullptr;
+  }
+  g.mg.L = 0;
+}
+
 }  // namespace
 
 // Builds Ac = P^T A P from the mesh's CSR stiffness matrix (unknowns,
 // 1-based) and uploads its inverse.
 int coarse_setup(const pic_mesh_desc *mesh, int coarse_cells) {
-  if (g.d_pc_ainv) {
-    cudaFree(g.d_pc_ainv);
-    cudaFree(g.d_pc_rc);
-    cudaFree(g.d_pc_ec);
-    g.d_pc_ainv = nullptr;
-    g.d_pc_rc = g.d_pc_ec = nullptr;
-  }
-  g.pc_cs = 0;
+  coarse_free();
+  mg_free();
   ++g.fcg_graph_gen;  // captured iterations hold the old buffers
   if (coarse_cells <= 0) return PIC_OK;
   const int ex = g.m.nnx - 1, ey = g.m.nny - 1;
@@ -240,65 +387,166 @@ int coarse_setup(const pic_mesh_desc *mesh, int coarse_cells) {
   for (int C = 0; C < nc; ++C)  // coarse nodes without unknowns in their support
     if (Ac[(size_t)C * nc + C] == 0.0) Ac[(size_t)C * nc + C] = 1.0;
   int rc;
-  double *d_a = nullptr, *d_row = nullptr, *d_col = nullptr;
-  int *d_bad = nullptr;
-  const size_t nc2 = (size_t)nc * nc;
-  if ((rc = pc_alloc(&d_a, nc2))) return rc;
-  if ((rc = pc_alloc(&d_row, nc)) || (rc = pc_alloc(&d_col, nc)) || (rc = pc_alloc(&d_bad, 1))) {
-    cudaFree(d_a);
-    return rc;
-  }
-  auto release = [&]() {
-    cudaFree(d_a);
-    cudaFree(d_row);
-    cudaFree(d_col);
-    cudaFree(d_bad);
-  };
-  int bad = 0;
-  cudaError_t e = cudaMemcpyAsync(d_a, Ac.data(), nc2 * sizeof(double), cudaMemcpyHostToDevice, g.st);
-  if (e == cudaSuccess) e = cudaMemsetAsync(d_bad, 0, sizeof(int), g.st);
-  for (int k = 0; e == cudaSuccess && k < nc; ++k) {
-    k_gj_pivot<<<(nc + 255) / 256, 256, 0, g.st>>>(d_a, nc, k, d_row, d_col, d_bad);
-    k_gj_update<<<(unsigned)((nc2 + 255) / 256), 256, 0, g.st>>>(d_a, nc, k, d_row, d_col);
-    e = cudaPeekAtLastError();
-  }
-  if (e == cudaSuccess) e = cudaMemcpyAsync(&bad, d_bad, sizeof(int), cudaMemcpyDeviceToHost, g.st);
-  if (e == cudaSuccess) e = cudaStreamSynchronize(g.st);
-  if (e != cudaSuccess) {
-    release();
-    return cuda_fail(e, "coarse operator inversion");
-  }
-  if (bad) {
-    release();
-    set_error("pic_coarse_setup: coarse operator is not positive definite");
-    return PIC_ERR_SETUP;
-  }
-  // The per-iteration GEMV reads a scaled FP16 copy (a quarter of the FP64
-  // bytes: 36 MB at 65x65 coarse nodes, so it and the solver's vectors fit in
-  // L2 together) and accumulates in FP64.  A preconditioner tolerates the
-  // 2^-11 relative rounding of the coarse correction; convergence is always
-  // judged on the FP64 residual.
-  std::vector<double> dg(nc);
-  k_diag_of<<<(nc + 255) / 256, 256, 0, g.st>>>(d_a, d_row, nc);
-  e = cudaMemcpyAsync(dg.data(), d_row, nc * sizeof(double), cudaMemcpyDeviceToHost, g.st);
-  if (e == cudaSuccess) e = cudaStreamSynchronize(g.st);
-  double dmax = 0.0;
-  for (double v : dg) dmax = std::max(dmax, std::fabs(v));
-  g.pc_ainv_scale = (dmax > 0.0) ? dmax / 16384.0 : 1.0;
-  rc = (e == cudaSuccess) ? pc_alloc(&g.d_pc_ainv, nc2) : cuda_fail(e, "coarse inverse diagonal");
-  if (!rc) {
-    k_to_f16<<<(unsigned)((nc2 + 255) / 256), 256, 0, g.st>>>(d_a, g.d_pc_ainv, 1.0 / g.pc_ainv_scale,
-                                                               (int64_t)nc2);
-    e = cudaStreamSynchronize(g.st);
-    if (e != cudaSuccess) rc = cuda_fail(e, "coarse inverse copy");
-  }
-  release();
-  if (rc) return rc;
+  if ((rc = dense_inverse_f16(Ac, nc, "pic_coarse_setup"))) return rc;
   if ((rc = pc_alloc(&g.d_pc_rc, nc))) return rc;
   if ((rc = pc_alloc(&g.d_pc_ec, nc))) return rc;
   g.pc_cs = cs;
   g.pc_ncx = ncx;
   g.pc_ncy = ncy;
+  return PIC_OK;
+}
+
+namespace {
+
+// Row of bilinear interpolation P for the node (i, j) of a grid whose
+// coarser grid has nyc columns: up to 4 (coarse node, weight) pairs.
+int p_row(int i, int j, int nyc, int *cc, double *ww) {
+  const int I = i >> 1, J = j >> 1;
+  const int nxp = (i & 1) ? 2 : 1, nyp = (j & 1) ? 2 : 1;
+  const double wx = (i & 1) ? 0.5 : 1.0, wy = (j & 1) ? 0.5 : 1.0;
+  int k = 0;
+  for (int a = 0; a < nxp; ++a)
+    for (int b = 0; b < nyp; ++b) {
+      cc[k] = (I + a) * nyc + (J + b);
+      ww[k] = wx * wy;
+      ++k;
+    }
+  return k;
+}
+
+// st[k*nc + C] += wu * a * wv for the coarse pair (C, C2); false when C2 is
+// not among C's 9 neighbours (the finer operator is not a 9-point stencil)
+inline bool rap_add(std::vector<double> &st, int64_t nc, int nyc, int C, int C2, double v) {
+  const int dI = C2 / nyc - C / nyc, dJ = C2 % nyc - C % nyc;
+  if (dI < -1 || dI > 1 || dJ < -1 || dJ > 1) return false;
+  st[(size_t)((dI + 1) * 3 + (dJ + 1)) * nc + C] += v;
+  return true;
+}
+
+}  // namespace
+
+// Galerkin hierarchy A_{l+1} = P^T A_l P on grids halved until at most
+// max_coarse_nodes remain (each halving needs nnx-1 and nny-1 even), level 1
+// from the mesh's CSR stiffness matrix over the unknowns, the coarsest level
+// inverted densely.  Replaces the two-level coarse space.
+int mg_setup(const pic_mesh_desc *mesh, int max_coarse) {
+  coarse_free();
+  mg_free();
+  ++g.fcg_graph_gen;  // captured iterations hold the old buffers
+  if (max_coarse <= 0) return PIC_OK;
+  int nx[PIC_MG_MAX_LEVELS], ny[PIC_MG_MAX_LEVELS];
+  nx[0] = g.m.nnx;
+  ny[0] = g.m.nny;
+  int L = 1;
+  while (L < PIC_MG_MAX_LEVELS && (int64_t)nx[L - 1] * ny[L - 1] > max_coarse && (nx[L - 1] - 1) % 2 == 0 &&
+         (ny[L - 1] - 1) % 2 == 0 && nx[L - 1] >= 5 && ny[L - 1] >= 5) {
+    nx[L] = (nx[L - 1] - 1) / 2 + 1;
+    ny[L] = (ny[L - 1] - 1) / 2 + 1;
+    ++L;
+  }
+  if (L < 2 || (int64_t)nx[L - 1] * ny[L - 1] > 9000) {
+    set_error("pic_multigrid_setup: the grid does not halve down to 9000 nodes or fewer "
+              "(nnx-1 and nny-1 need enough factors of 2)");
+    return PIC_ERR_ARG;
+  }
+  std::vector<std::vector<double>> st(L);
+  std::vector<std::vector<char>> act(L);
+  int cu[4], cv[4];
+  double wu[4], wv[4];
+  bool ok = true;
+  {  // level 1 from the CSR rows of the unknowns (1-based)
+    const int64_t nn = (int64_t)g.m.nnx * g.m.nny, n1 = (int64_t)nx[1] * ny[1];
+    const int nu = mesh->n_unknowns, nny = g.m.nny;
+    std::vector<int64_t> node_of(nu);
+    for (int64_t n = 0; n < nn; ++n)
+      if (mesh->node_type[n] > 0) node_of[mesh->node_type[n] - 1] = n;
+    st[1].assign((size_t)9 * n1, 0.0);
+    for (int u = 0; u < nu && ok; ++u) {
+      const int64_t n = node_of[u];
+      const int ku = p_row((int)(n / nny), (int)(n % nny), ny[1], cu, wu);
+      for (int64_t e = mesh->a_srow[u] - 1; e < mesh->a_srow[u + 1] - 1 && ok; ++e) {
+        const int64_t m = node_of[mesh->a_jcol[e] - 1];
+        const double a = mesh->a_k[e];
+        const int kv = p_row((int)(m / nny), (int)(m % nny), ny[1], cv, wv);
+        for (int p = 0; p < ku; ++p)
+          for (int q = 0; q < kv; ++q) ok = ok && rap_add(st[1], n1, ny[1], cu[p], cv[q], (wu[p] * a) * wv[q]);
+      }
+    }
+  }
+  for (int l = 1; l < L && ok; ++l) {
+    const int64_t nl = (int64_t)nx[l] * ny[l];
+    act[l].resize(nl);
+    for (int64_t n = 0; n < nl; ++n) act[l][n] = st[l][4 * (size_t)nl + n] != 0.0;
+    if (l + 1 == L) break;
+    const int64_t nc = (int64_t)nx[l + 1] * ny[l + 1];
+    st[l + 1].assign((size_t)9 * nc, 0.0);
+    for (int64_t f = 0; f < nl && ok; ++f) {
+      if (!act[l][f]) continue;
+      const int i = (int)(f / ny[l]), j = (int)(f % ny[l]);
+      const int ku = p_row(i, j, ny[l + 1], cu, wu);
+      for (int k = 0; k < 9 && ok; ++k) {
+        const int i2 = i + k / 3 - 1, j2 = j + k % 3 - 1;
+        if (i2 < 0 || i2 >= nx[l] || j2 < 0 || j2 >= ny[l]) continue;
+        const int64_t f2 = (int64_t)i2 * ny[l] + j2;
+        const double a = st[l][(size_t)k * nl + f];
+        if (a == 0.0 || !act[l][f2]) continue;
+        const int kv = p_row(i2, j2, ny[l + 1], cv, wv);
+        for (int p = 0; p < ku; ++p)
+          for (int q = 0; q < kv; ++q) ok = ok && rap_add(st[l + 1], nc, ny[l + 1], cu[p], cv[q], (wu[p] * a) * wv[q]);
+      }
+    }
+  }
+  if (!ok) {
+    set_error("pic_multigrid_setup: the stiffness matrix couples nodes more than one cell apart");
+    return PIC_ERR_SETUP;
+  }
+  int rc = PIC_OK;
+  for (int l = 1; l < L && !rc; ++l) {  // FP32 stencils and 1/diag, FP64 vectors
+    const int64_t nl = (int64_t)nx[l] * ny[l];
+    std::vector<float> s32((size_t)9 * nl), d32(nl);
+    for (size_t q = 0; q < s32.size(); ++q) s32[q] = (float)st[l][q];
+    for (int64_t n = 0; n < nl; ++n) d32[n] = act[l][n] ? (float)(1.0 / st[l][4 * (size_t)nl + n]) : 0.0f;
+    MgLevel &V = g.mg.lv[l];
+    V.nx = nx[l];
+    V.ny = ny[l];
+    float *dst = nullptr, *ddi = nullptr;
+    if ((rc = pc_alloc(&dst, s32.size())) || (rc = pc_alloc(&ddi, (size_t)nl))) break;
+    V.st = dst;
+    V.dinv = ddi;
+    if ((rc = pc_alloc(&V.r, (size_t)nl)) || (rc = pc_alloc(&V.z, (size_t)nl)) || (rc = pc_alloc(&V.t, (size_t)nl)))
+      break;
+    cudaError_t e = cudaMemcpy(dst, s32.data(), s32.size() * sizeof(float), cudaMemcpyHostToDevice);
+    if (e == cudaSuccess) e = cudaMemcpy(ddi, d32.data(), d32.size() * sizeof(float), cudaMemcpyHostToDevice);
+    if (e == cudaSuccess) e = cudaMemset(V.r, 0, nl * sizeof(double));
+    if (e == cudaSuccess) e = cudaMemset(V.z, 0, nl * sizeof(double));
+    if (e == cudaSuccess) e = cudaMemset(V.t, 0, nl * sizeof(double));
+    if (e != cudaSuccess) rc = cuda_fail(e, "pic_multigrid_setup upload");
+  }
+  if (!rc) {  // the coarsest operator, dense (identity rows on inactive nodes)
+    const int nc = nx[L - 1] * ny[L - 1];
+    std::vector<double> Ac((size_t)nc * nc, 0.0);
+    const std::vector<double> &sc = st[L - 1];
+    for (int C = 0; C < nc; ++C) {
+      if (!act[L - 1][C]) {
+        Ac[(size_t)C * nc + C] = 1.0;
+        continue;
+      }
+      const int I = C / ny[L - 1], J = C % ny[L - 1];
+      for (int k = 0; k < 9; ++k) {
+        const int i2 = I + k / 3 - 1, j2 = J + k % 3 - 1;
+        if (i2 < 0 || i2 >= nx[L - 1] || j2 < 0 || j2 >= ny[L - 1]) continue;
+        Ac[(size_t)C * nc + (size_t)i2 * ny[L - 1] + j2] += sc[(size_t)k * nc + C];
+      }
+    }
+    rc = dense_inverse_f16(Ac, nc, "pic_multigrid_setup");
+  }
+  if (rc) {
+    mg_free();
+    return rc;
+  }
+  g.mg.lv[0].nx = g.m.nnx;
+  g.mg.lv[0].ny = g.m.nny;
+  g.mg.L = L;
   return PIC_OK;
 }
 
@@ -311,6 +559,7 @@ int precond_learned_on() { return (g.pc_learned && g.precond) ? 1 : 0; }
 int precond_callback() { return g.precond(g.d_pc_t, g.d_pc_y, g.precond_user) != 0 ? 1 : 0; }
 
 void precond_free() {
+  mg_free();
   auto F = [](void *p) {
     if (p) cudaFree(p);
   };

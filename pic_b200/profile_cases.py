@@ -2,13 +2,14 @@
 ncu (each runs a few launches of its kernels and exits):
 
     python -m pic_b200.profile_cases step  <deck> <ppc> <steps> [jpcg|fcg] [fp64|mixed]
-    python -m pic_b200.profile_cases solve <cells> [jpcg|fcg] [repeats] [coarse_cells] [fp64|mixed]
+    python -m pic_b200.profile_cases solve <cells> [jpcg|fcg|mg] [repeats] [coarse_cells] [fp64|mixed] [omega]
     python -m pic_b200.profile_cases unet  <nodes> [repeats]
     python -m pic_b200.profile_cases diag  <deck> <ppc> [fp64|mixed] [repeats]
 
 step:  the deck at <ppc> particles per cell and species, <steps> steps.
 solve: the 8-ellipse deck at <cells>^2 without particles, a seeded random
-       charge density, Poisson solves from phi = 0.
+       charge density, Poisson solves from phi = 0 (mg: the multigrid
+       V-cycle in place of the two-level coarse space).
 unet:  forward passes of the learned stage's network on a <nodes>^2 grid.
 diag:  the deck after one step, then the device diagnostics (Average_x
        profiles, energy spectra, velocity moments) of every species.
@@ -44,7 +45,7 @@ def _step(deck_name, ppc, steps, solver="fcg", precision="fp64"):
     sim.close()
 
 
-def _solve(cells, solver="fcg", repeats=3, coarse_cells=64, precision="fp64"):
+def _solve(cells, solver="fcg", repeats=3, coarse_cells=64, precision="fp64", omega=2.0 / 3.0):
     import torch
     from . import api, deck
     from .simulation import Simulation
@@ -55,7 +56,10 @@ def _solve(cells, solver="fcg", repeats=3, coarse_cells=64, precision="fp64"):
     sim.set_field("rho", np.random.default_rng(0).standard_normal(sim.mesh.nn))
     import time
     t0 = time.perf_counter()
-    sim.set_solver(solver, coarse_cells=int(coarse_cells))
+    if solver == "mg":
+        sim.set_solver("fcg", multigrid=True, omega=float(omega))
+    else:
+        sim.set_solver(solver, coarse_cells=int(coarse_cells), omega=float(omega))
     setup = time.perf_counter() - t0
     out = []
     for _ in range(int(repeats)):

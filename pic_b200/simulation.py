@@ -130,11 +130,14 @@ class Simulation:
 
     # ---- Poisson solver ---------------------------------------------------
     def set_solver(self, kind: str = "jpcg", coarse_cells: int = 64, window: int = 1,
-                   omega: float = 2.0 / 3.0, inner_fp32: bool = False):
+                   omega: float = 2.0 / 3.0, inner_fp32: bool = False,
+                   multigrid: bool = False, max_coarse_nodes: int = 4500):
         """'jpcg': the reference's Jacobi-PCG.  'fcg': flexible CG with damped
-        Jacobi smoothing and a Galerkin coarse space (no learned stage);
-        inner_fp32 (mixed precision only): FP32 iterations in FP64 refinement.
-        'fcg-learned' is set up by unet.LearnedPreconditioner on top of 'fcg'."""
+        Jacobi smoothing and a Galerkin coarse space (no learned stage): the
+        two-level space of about coarse_cells^2 cells, or with multigrid the
+        V-cycle down to max_coarse_nodes; inner_fp32 (mixed precision only):
+        FP32 iterations in FP64 refinement.  'fcg-learned' is set up by
+        unet.LearnedPreconditioner on top of 'fcg'."""
         lib = self.lib
         if kind == "jpcg":
             api.check(lib.pic_set_solver(api.PIC_SOLVER_JPCG), "pic_set_solver")
@@ -142,7 +145,10 @@ class Simulation:
         if kind != "fcg":
             raise ValueError(kind)
         api.check(lib.pic_set_precond_stages(1, omega, 0), "pic_set_precond_stages")
-        api.check(lib.pic_coarse_setup(self.mesh.ptr, coarse_cells), "pic_coarse_setup")
+        if multigrid:
+            api.check(lib.pic_multigrid_setup(self.mesh.ptr, max_coarse_nodes), "pic_multigrid_setup")
+        else:
+            api.check(lib.pic_coarse_setup(self.mesh.ptr, coarse_cells), "pic_coarse_setup")
         api.check(lib.pic_set_fcg_window(window), "pic_set_fcg_window")
         api.check(lib.pic_set_fcg_inner(int(inner_fp32)), "pic_set_fcg_inner")
         api.check(lib.pic_set_solver(api.PIC_SOLVER_FCG_UNET), "pic_set_solver")
