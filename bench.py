@@ -332,11 +332,13 @@ def run_ours(args, dist, rank, ws):
     def sel_fcg32():
         sim.set_solver("fcg", coarse_cells=64, window=1, inner_fp32=True)
 
+    # damped-Jacobi weight 0.8 with the V-cycle: 11 iterations at 1024^2
+    # against 12 with 2/3
     def sel_mg():
-        sim.set_solver("fcg", window=1, multigrid=True)
+        sim.set_solver("fcg", window=1, multigrid=True, omega=0.8)
 
     def sel_mg32():
-        sim.set_solver("fcg", window=1, multigrid=True, inner_fp32=True)
+        sim.set_solver("fcg", window=1, multigrid=True, omega=0.8, inner_fp32=True)
 
     variants = {"jacobi_pcg": sel_jpcg, "fcg_smooth_coarse": sel_fcg, "fcg_smooth_multigrid": sel_mg}
     if args.precision == "mixed":

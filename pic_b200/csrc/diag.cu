@@ -199,16 +199,30 @@ __global__ void __launch_bounds__(256) k_vmoments(MomK k) {
         t[c] = d * d;
       }
     }
-    // particles sorted by cell: the 32 lanes usually share a column, and then
-    // the warp sums first and adds once per component (every lane takes part
-    // in the shuffles; none is skipped by short-circuiting)
-    const int b_first = __shfl_sync(0xffffffffu, b, 0);
-    const bool same = __all_sync(0xffffffffu, b == b_first);
-    if (same) {
-      for (int c = 0; c < 3; ++c)
-        for (int o = 16; o > 0; o >>= 1) t[c] += __shfl_xor_sync(0xffffffffu, t[c], o);
-      if (b_first >= 0 && (threadIdx.x & 31) == 0)
-        for (int c = 0; c < 3; ++c) atomicAdd(&acc[c * k.nbins + b_first], t[c]);
+    // particles sorted by cell: a warp's particles fall in one x column, or
+    // in two when a column edge (one Debye length, about one cell) crosses
+    // their cells.  Then the warp sums per column first and adds once per
+    // column and component; otherwise every lane adds its own.  Every lane
+    // takes part in each ballot and shuffle (none is skipped by
+    // short-circuiting).
+    const unsigned full = 0xffffffffu;
+    const int b0 = __shfl_sync(full, b, 0);
+    const unsigned m0 = __ballot_sync(full, b == b0);
+    const int src1 = (m0 == full) ? 0 : __ffs(~m0) - 1;
+    const int b1 = __shfl_sync(full, b, src1);
+    const unsigned m1 = __ballot_sync(full, b == b1);
+    if ((m0 | m1) == full) {
+      for (int c = 0; c < 3; ++c) {
+        double s0 = (b == b0) ? t[c] : 0.0, s1 = (b == b1 && b1 != b0) ? t[c] : 0.0;
+        for (int o = 16; o > 0; o >>= 1) {
+          s0 += __shfl_xor_sync(full, s0, o);
+          s1 += __shfl_xor_sync(full, s1, o);
+        }
+        if ((threadIdx.x & 31) == 0) {
+          if (b0 >= 0) atomicAdd(&acc[c * k.nbins + b0], s0);
+          if (b1 != b0 && b1 >= 0) atomicAdd(&acc[c * k.nbins + b1], s1);
+        }
+      }
     } else if (b >= 0) {
       for (int c = 0; c < 3; ++c) atomicAdd(&acc[c * k.nbins + b], t[c]);
     }
