@@ -1,7 +1,7 @@
 """Small, self-contained workloads for profiling one part of the step under
 ncu (each runs a few launches of its kernels and exits):
 
-    python -m pic_b200.profile_cases step  <deck> <ppc> <steps> [jpcg|fcg] [fp64|mixed]
+    python -m pic_b200.profile_cases step  <deck> <ppc> <steps> [jpcg|fcg|mg] [fp64|mixed]
     python -m pic_b200.profile_cases solve <cells> [jpcg|fcg|mg] [repeats] [coarse_cells] [fp64|mixed] [omega]
     python -m pic_b200.profile_cases unet  <nodes> [repeats]
     python -m pic_b200.profile_cases diag  <deck> <ppc> [fp64|mixed] [repeats]
@@ -31,7 +31,9 @@ def _step(deck_name, ppc, steps, solver="fcg", precision="fp64"):
     cfg = deck.config(deck_name, ppc=int(ppc), precision=prec)
     sim = Simulation(cfg)
     sim.initial_fields()
-    if solver != "jpcg":
+    if solver == "mg":
+        sim.set_solver("fcg", multigrid=True, omega=0.8)
+    elif solver != "jpcg":
         sim.set_solver("fcg")
     sim.step()
     torch.cuda.synchronize()
