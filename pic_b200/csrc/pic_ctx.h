@@ -193,6 +193,11 @@ struct Ctx {
   int32_t *d_cand_slot = nullptr;
   int64_t mcc_cap = 0;
   int64_t *d_mcc_misc = nullptr;       // [16] counters
+  uint64_t *d_mlist_key = nullptr;     // bounded selection: (key << 32 | id) below the bound
+  int32_t *d_mlist_slot = nullptr;     //   and their slots
+  int64_t mlist_cap = 0;
+  int mcc_full = 0;                    // 1: always the full-histogram selection
+  int64_t *d_msel = nullptr;           // [8]: list count, keys below the bound, b*, count below b*
   int64_t *d_ion_parent = nullptr;     // ionising parents: (id<<32 | slot)
   double *d_ion_data = nullptr;        // per ionisation: new e- v(3), ion v(3)
   int32_t *d_mcc_pslot = nullptr;      // created particles: parent slots, velocities

@@ -2114,7 +2114,7 @@ static void free_all() {
   fcg_graphs_free();
   F(g.d_cell_count); F(g.d_cell_start); F(g.d_cell_fill); F(g.d_perm); F(g.d_perm2); F(g.d_sort_id);
   F(g.d_scan_blk); F(g.d_counters); F(g.d_hist); F(g.d_sel); F(g.d_cand); F(g.d_cand_slot);
-  F(g.d_mcc_misc); F(g.d_ion_parent); F(g.d_ion_data); F(g.d_mcc_pslot); F(g.d_mcc_vel);
+  F(g.d_mcc_misc); F(g.d_mlist_key); F(g.d_mlist_slot); F(g.d_msel); F(g.d_ion_parent); F(g.d_ion_data); F(g.d_mcc_pslot); F(g.d_mcc_vel);
   for (int s = 0; s < PIC_MAX_SPECIES; ++s) {
     Species &p = g.sp[s];
     F(p.x); F(p.y); F(p.vx); F(p.vy); F(p.vz); F(p.loc); F(p.id);
@@ -3409,6 +3409,8 @@ int pic_init(const pic_mesh_desc *mesh, const pic_params *params) {
     // with S-stage cp.async (2..4; 4 by default: 2.56 ms against 2.81 ms per
     // step at 101M particles), or 0 for one particle per thread loaded
     // directly
+    const char *mf = getenv("PIC_MCC_FULL");  // 1: MCC selection by the full key histogram
+    g.mcc_full = (mf && atoi(mf) == 1) ? 1 : 0;
     const char *ps = getenv("PIC_PUSH_STAGES");
     g.push_stages = ps ? atoi(ps) : g.push_stages;
     if (g.push_stages != 0 && (g.push_stages < 2 || g.push_stages > 4)) g.push_stages = 0;

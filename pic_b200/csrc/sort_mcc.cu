@@ -264,6 +264,118 @@ __global__ void k_mcc_pick(MccK k, const uint32_t *__restrict__ keys, uint32_t b
   }
 }
 
+// ---- selection under a key bound: only the live particles whose key lies
+// below `bound` (chosen so that about 2 ncoll + 64 of them are expected
+// there) enter a 65536-bin histogram of [0, bound) and a compact list of
+// (key << 32 | id, slot); the threshold bin, the particles below it and the
+// order of the ties are then found on the device.  The selected set is the
+// one the full histogram gives: the ncoll smallest (key, id).  When fewer
+// than ncoll keys lie below the bound, or the list overflows, the host
+// reruns the selection with the full histogram.
+__device__ __forceinline__ uint32_t mcc_bin(uint32_t key, uint64_t bound) {
+  return (uint32_t)(((uint64_t)key << 16) / bound);
+}
+
+__global__ void k_mcc_scan(MccK k, uint64_t bound, uint32_t *__restrict__ hist, uint64_t *__restrict__ lkey,
+                           int32_t *__restrict__ lslot, int64_t cap, unsigned long long *__restrict__ cnt) {
+  const int64_t p = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  const int lane = threadIdx.x & 31;
+  bool want = false;
+  uint32_t key = 0;
+  if (p < k.n && k.loc[p] >= 0) {
+    key = mcc_select_key(k.id[p], k.step_lo, k.step_hi, k.species, k.seed0, k.seed1);
+    want = (uint64_t)key < bound;
+  }
+  // one list slot reservation per warp; every lane takes part in the ballot
+  const unsigned m = __ballot_sync(0xffffffffu, want);
+  if (!m) return;  // the same for every lane of the warp
+  const int leader = __ffs(m) - 1;
+  unsigned long long base = 0;
+  if (lane == leader) base = atomicAdd(cnt, (unsigned long long)__popc(m));
+  base = __shfl_sync(0xffffffffu, base, leader);
+  if (want) {
+    atomicAdd(hist + mcc_bin(key, bound), 1u);
+    const int64_t i = (int64_t)base + __popc(m & ((1u << lane) - 1u));
+    if (i < cap) {
+      lkey[i] = ((uint64_t)key << 32) | (uint64_t)k.id[p];
+      lslot[i] = (int32_t)p;
+    }
+  }
+}
+
+// one block of 1024 threads: the bin b* where the running count of the
+// histogram reaches ncoll, and the count below it.  ms[1] = keys below the
+// bound, ms[2] = b* (-1 when fewer than ncoll keys lie below the bound),
+// ms[3] = particles in bins below b*.
+__global__ void __launch_bounds__(1024) k_mcc_bstar(const uint32_t *__restrict__ hist, int64_t ncoll,
+                                                    int64_t *__restrict__ ms) {
+  __shared__ unsigned long long part[1024];
+  const int t = threadIdx.x;
+  if (t == 0) ms[2] = -1;
+  unsigned long long s = 0;
+  for (int b = 0; b < 64; ++b) s += hist[t * 64 + b];
+  part[t] = s;
+  __syncthreads();
+  for (int off = 1; off < 1024; off <<= 1) {  // inclusive scan
+    const unsigned long long v = t >= off ? part[t - off] : 0ull;
+    __syncthreads();
+    part[t] += v;
+    __syncthreads();
+  }
+  const unsigned long long incl = part[t], excl = t ? part[t - 1] : 0ull, nc = (unsigned long long)ncoll;
+  if (t == 1023) ms[1] = (int64_t)incl;
+  if (excl < nc && incl >= nc) {  // exactly one thread
+    unsigned long long below = excl;
+    int b = t * 64;
+    while (below + hist[b] < nc) below += hist[b++];  // ends inside this thread's 64 bins
+    ms[2] = b;
+    ms[3] = (int64_t)below;
+  }
+}
+
+// list entries below b* are selected; those in b* are the ties
+__global__ void k_mcc_pick_list(const uint64_t *__restrict__ lkey, const int32_t *__restrict__ lslot,
+                                const unsigned long long *__restrict__ cnt, int64_t cap, uint64_t bound,
+                                const int64_t *__restrict__ ms, int32_t *__restrict__ sel,
+                                uint64_t *__restrict__ tkey, int32_t *__restrict__ tslot, int64_t tcap,
+                                int64_t *__restrict__ misc) {
+  const int64_t m = min((int64_t)*cnt, cap), bstar = ms[2];
+  if (bstar < 0) return;
+  for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < m; i += (int64_t)gridDim.x * blockDim.x) {
+    const uint64_t kv = lkey[i];
+    const int64_t bin = mcc_bin((uint32_t)(kv >> 32), bound);
+    if (bin < bstar) {
+      const long long j = atomicAdd((unsigned long long *)&misc[0], 1ull);
+      sel[j] = lslot[i];
+    } else if (bin == bstar) {
+      const long long j = atomicAdd((unsigned long long *)&misc[1], 1ull);
+      if (j < tcap) {
+        tkey[j] = kv;
+        tslot[j] = lslot[i];
+      }
+    }
+  }
+}
+
+// one block: each tie's rank among the ties by (key, id); the first
+// ncoll - below of them complete the selection.  Quadratic in the tie count,
+// so it leaves more than kMaxTies ties to the full selection (a bin holds
+// about 2 ncoll / 65536 keys: a few hundred at most in practice).
+constexpr int64_t kMaxTies = 8192;
+__global__ void __launch_bounds__(1024) k_mcc_ties(const uint64_t *__restrict__ tkey,
+                                                   const int32_t *__restrict__ tslot, int64_t tcap,
+                                                   const int64_t *__restrict__ ms, const int64_t *__restrict__ misc,
+                                                   int64_t ncoll, int32_t *__restrict__ sel) {
+  if (ms[2] < 0 || misc[1] > kMaxTies) return;
+  const int64_t c = min(misc[1], tcap), below = ms[3], need = ncoll - below;
+  for (int64_t i = threadIdx.x; i < c; i += blockDim.x) {
+    const uint64_t ki = tkey[i];
+    int64_t rank = 0;
+    for (int64_t j = 0; j < c; ++j) rank += tkey[j] < ki ? 1 : 0;
+    if (rank < need) sel[below + rank] = tslot[i];
+  }
+}
+
 struct CollK {
   MccK k;
   const int32_t *sel;
@@ -359,6 +471,22 @@ static int mcc_alloc(int64_t need) {
   return PIC_OK;
 }
 
+// compact list of the bounded selection and its counters (kept across steps)
+static int mcc_list_alloc(int64_t need) {
+  if (!g.d_msel) PIC_CUDA(cudaMalloc(&g.d_msel, 8 * sizeof(int64_t)));
+  if (need <= g.mlist_cap) return PIC_OK;
+  const int64_t cap = std::max<int64_t>(need + need / 2, 1 << 16);
+  cudaFree(g.d_mlist_key);
+  cudaFree(g.d_mlist_slot);
+  g.d_mlist_key = nullptr;
+  g.d_mlist_slot = nullptr;
+  g.mlist_cap = 0;
+  PIC_CUDA(cudaMalloc(&g.d_mlist_key, cap * sizeof(uint64_t)));
+  PIC_CUDA(cudaMalloc(&g.d_mlist_slot, cap * sizeof(int32_t)));
+  g.mlist_cap = cap;
+  return PIC_OK;
+}
+
 struct Pending {
   int32_t from_species;
   std::vector<int64_t> parent;  // sorted (id<<32 | slot)
@@ -383,49 +511,87 @@ int mcc_run(uint64_t step, pic_mcc_stats *stats) {
            sp.f32 ? 1 : 0};
     PIC_CUDA(cudaMemsetAsync(g.d_hist, 0, 65536 * sizeof(uint32_t), g.st));
     PIC_CUDA(cudaMemsetAsync(g.d_mcc_misc, 0, 16 * sizeof(int64_t), g.st));
-    uint32_t *keys = g.d_sort_id;  // sort scratch, free while MCC runs
-    k_mcc_hist<<<blocks_for(sp.n_slots, 256), 256, 0, g.st>>>(k, g.d_hist, keys);
-    PIC_LAUNCHED();
-    std::vector<uint32_t> hist(65536);
-    PIC_CUDA(cudaMemcpyAsync(hist.data(), g.d_hist, 65536 * 4, cudaMemcpyDeviceToHost, g.st));
-    PIC_CUDA(cudaStreamSynchronize(g.st));
-    int64_t below = 0;
-    uint32_t bstar = 0;
-    for (; bstar < 65536; ++bstar) {
-      if (below + hist[bstar] >= ncoll) break;
-      below += hist[bstar];
+    bool selected = false;
+    // bounded selection: the bound holds about 2 ncoll + 64 live keys (plus 8
+    // standard deviations); used while that is a small part of the species
+    const double target = 2.0 * (double)ncoll + 64.0 + 8.0 * std::sqrt(2.0 * (double)ncoll + 64.0);
+    if (!g.mcc_full && target < 0.25 * (double)npar) {
+      const uint64_t bound =
+          std::max<uint64_t>(1, (uint64_t)std::ceil(target / (double)npar * 4294967296.0));
+      const int64_t lcap = (int64_t)(1.5 * target) + 4096;
+      if ((rc = mcc_list_alloc(lcap))) return rc;
+      if ((rc = mcc_alloc(std::max<int64_t>(ncoll, 1 << 16) + 4096))) return rc;
+      PIC_CUDA(cudaMemsetAsync(g.d_msel, 0, 8 * sizeof(int64_t), g.st));
+      unsigned long long *cnt = reinterpret_cast<unsigned long long *>(g.d_msel);
+      k_mcc_scan<<<blocks_for(sp.n_slots, 256), 256, 0, g.st>>>(k, bound, g.d_hist, g.d_mlist_key, g.d_mlist_slot,
+                                                                 lcap, cnt);
+      PIC_LAUNCHED();
+      k_mcc_bstar<<<1, 1024, 0, g.st>>>(g.d_hist, ncoll, g.d_msel);
+      PIC_LAUNCHED();
+      k_mcc_pick_list<<<(unsigned)std::min<int64_t>(blocks_for(lcap, 256), 1184), 256, 0, g.st>>>(
+          g.d_mlist_key, g.d_mlist_slot, cnt, lcap, bound, g.d_msel, g.d_sel, g.d_cand, g.d_cand_slot, g.mcc_cap,
+          g.d_mcc_misc);
+      PIC_LAUNCHED();
+      k_mcc_ties<<<1, 1024, 0, g.st>>>(g.d_cand, g.d_cand_slot, g.mcc_cap, g.d_msel, g.d_mcc_misc, ncoll, g.d_sel);
+      PIC_LAUNCHED();
+      int64_t ms[4], mc[2];
+      PIC_CUDA(cudaMemcpyAsync(ms, g.d_msel, sizeof ms, cudaMemcpyDeviceToHost, g.st));
+      PIC_CUDA(cudaMemcpyAsync(mc, g.d_mcc_misc, sizeof mc, cudaMemcpyDeviceToHost, g.st));
+      PIC_CUDA(cudaStreamSynchronize(g.st));
+      // ms[0] list entries, ms[2] b*, ms[3] below b*; mc[0] selected below
+      // b*, mc[1] ties
+      selected = ms[0] <= lcap && ms[2] >= 0 && mc[0] == ms[3] && mc[1] >= ncoll - ms[3] && mc[1] <= g.mcc_cap &&
+                 mc[1] <= kMaxTies;
+      if (!selected) {  // start the full selection from clean counters
+        PIC_CUDA(cudaMemsetAsync(g.d_hist, 0, 65536 * sizeof(uint32_t), g.st));
+        PIC_CUDA(cudaMemsetAsync(g.d_mcc_misc, 0, 16 * sizeof(int64_t), g.st));
+      }
     }
-    if (bstar >= 65536) {
-      set_error("mcc: fewer live particles than collisions requested");
-      return PIC_ERR_STATE;
-    }
-    int64_t need = ncoll - below;
-    int64_t ncand_expect = hist[bstar];
-    rc = mcc_alloc(std::max<int64_t>(ncoll, ncand_expect) + 4096);
-    if (rc) return rc;
-    k_mcc_pick<<<blocks_for(sp.n_slots, 256), 256, 0, g.st>>>(k, keys, bstar, g.d_sel, g.d_mcc_misc, g.d_cand,
-                                                              g.d_cand_slot, g.mcc_cap);
-    PIC_LAUNCHED();
-    int64_t misc[2];
-    PIC_CUDA(cudaMemcpyAsync(misc, g.d_mcc_misc, 2 * sizeof(int64_t), cudaMemcpyDeviceToHost, g.st));
-    PIC_CUDA(cudaStreamSynchronize(g.st));
-    int64_t nsel = misc[0], ncand = misc[1];
-    if (ncand != ncand_expect || nsel != below) {
-      set_error("mcc: selection histogram mismatch");
-      return PIC_ERR_CUDA;
-    }
-    {
-      std::vector<uint64_t> cand(ncand);
-      std::vector<int32_t> cslot(ncand);
-      PIC_CUDA(cudaMemcpy(cand.data(), g.d_cand, ncand * 8, cudaMemcpyDeviceToHost));
-      PIC_CUDA(cudaMemcpy(cslot.data(), g.d_cand_slot, ncand * 4, cudaMemcpyDeviceToHost));
-      std::vector<int64_t> order(ncand);
-      for (int64_t i = 0; i < ncand; ++i) order[i] = i;
-      std::sort(order.begin(), order.end(), [&](int64_t a, int64_t b) { return cand[a] < cand[b]; });
-      std::vector<int32_t> add(need);
-      for (int64_t i = 0; i < need; ++i) add[i] = cslot[order[i]];
-      if (need > 0)
-        PIC_CUDA(cudaMemcpy(g.d_sel + nsel, add.data(), need * 4, cudaMemcpyHostToDevice));
+    if (!selected) {
+      uint32_t *keys = g.d_sort_id;  // sort scratch, free while MCC runs
+      k_mcc_hist<<<blocks_for(sp.n_slots, 256), 256, 0, g.st>>>(k, g.d_hist, keys);
+      PIC_LAUNCHED();
+      std::vector<uint32_t> hist(65536);
+      PIC_CUDA(cudaMemcpyAsync(hist.data(), g.d_hist, 65536 * 4, cudaMemcpyDeviceToHost, g.st));
+      PIC_CUDA(cudaStreamSynchronize(g.st));
+      int64_t below = 0;
+      uint32_t bstar = 0;
+      for (; bstar < 65536; ++bstar) {
+        if (below + hist[bstar] >= ncoll) break;
+        below += hist[bstar];
+      }
+      if (bstar >= 65536) {
+        set_error("mcc: fewer live particles than collisions requested");
+        return PIC_ERR_STATE;
+      }
+      int64_t need = ncoll - below;
+      int64_t ncand_expect = hist[bstar];
+      rc = mcc_alloc(std::max<int64_t>(ncoll, ncand_expect) + 4096);
+      if (rc) return rc;
+      k_mcc_pick<<<blocks_for(sp.n_slots, 256), 256, 0, g.st>>>(k, keys, bstar, g.d_sel, g.d_mcc_misc, g.d_cand,
+                                                                g.d_cand_slot, g.mcc_cap);
+      PIC_LAUNCHED();
+      int64_t misc[2];
+      PIC_CUDA(cudaMemcpyAsync(misc, g.d_mcc_misc, 2 * sizeof(int64_t), cudaMemcpyDeviceToHost, g.st));
+      PIC_CUDA(cudaStreamSynchronize(g.st));
+      int64_t nsel = misc[0], ncand = misc[1];
+      if (ncand != ncand_expect || nsel != below) {
+        set_error("mcc: selection histogram mismatch");
+        return PIC_ERR_CUDA;
+      }
+      {
+        std::vector<uint64_t> cand(ncand);
+        std::vector<int32_t> cslot(ncand);
+        PIC_CUDA(cudaMemcpy(cand.data(), g.d_cand, ncand * 8, cudaMemcpyDeviceToHost));
+        PIC_CUDA(cudaMemcpy(cslot.data(), g.d_cand_slot, ncand * 4, cudaMemcpyDeviceToHost));
+        std::vector<int64_t> order(ncand);
+        for (int64_t i = 0; i < ncand; ++i) order[i] = i;
+        std::sort(order.begin(), order.end(), [&](int64_t a, int64_t b) { return cand[a] < cand[b]; });
+        std::vector<int32_t> add(need);
+        for (int64_t i = 0; i < need; ++i) add[i] = cslot[order[i]];
+        if (need > 0)
+          PIC_CUDA(cudaMemcpy(g.d_sel + nsel, add.data(), need * 4, cudaMemcpyHostToDevice));
+      }
     }
     CollK c;
     c.k = k;

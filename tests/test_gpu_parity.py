@@ -405,3 +405,34 @@ def test_edge_cases():
         assert sim.count(0) == 0 or sim.count(0) < n
     finally:
         sim.close()
+
+
+@pytest.mark.parametrize("precision", [api.PIC_PREC_FP64, api.PIC_PREC_MIXED])
+def test_mcc_bounded_selection_matches_full(precision, monkeypatch):
+    """The selection under a key bound (histogram and compact list of the
+    keys below it, threshold and ties found on the device) picks the same
+    ncoll smallest (key, id) as the full key histogram (PIC_MCC_FULL=1):
+    after 6 steps with MCC the particles, fields and reaction counts are
+    bit-identical."""
+    out = []
+    for full in ("1", "0"):
+        monkeypatch.setenv("PIC_MCC_FULL", full)
+        sim = Simulation(deck.config("cfg1", precision=precision))
+        try:
+            sim.initial_fields()
+            counts = []
+            for _ in range(6):
+                st = sim.step()
+                counts.append([list(st.mcc.n_by_reaction[s]) for s in range(2)] +
+                              [list(st.mcc.n_selected)[:2], list(st.mcc.n_created)[:2]])
+            parts = [_by_id(sim.download(s)) for s in range(2)]
+            out.append((counts, parts, sim.field("rho"), sim.field("phi")))
+        finally:
+            sim.close()
+    (ca, pa, ra, fa), (cb, pb, rb, fb) = out
+    assert ca == cb
+    assert sum(ca[-1][2]) > 0  # collisions were selected
+    for a, b in zip(pa, pb):
+        for k in ("id", "loc", "x", "y", "vx", "vy", "vz"):
+            assert np.array_equal(a[k], b[k]), k
+    assert np.array_equal(ra, rb) and np.array_equal(fa, fb)
