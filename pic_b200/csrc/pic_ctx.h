@@ -166,6 +166,7 @@ struct Ctx {
   double *d_pc_rc = nullptr, *d_pc_ec = nullptr;
   MgK mg{};                                 // multigrid hierarchy (mg.L = 0: none)
   int push_stages = 4, push_grid = 0;       // tiled mixed push stages (0: one particle per thread)
+  int push_minb = 5;                        // resident CTAs per SM the 4-stage push is built for
   // CUDA graphs of one FCG iteration: [0] stage A, [1 + slot] stage B + FCG
   // kernels of ring slot `slot`; rebuilt when the configuration key changes
   cudaGraphExec_t fcg_graph[2 + PIC_FCG_MAX_WINDOW] = {};

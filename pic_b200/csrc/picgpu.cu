@@ -546,8 +546,8 @@ __device__ __forceinline__ void push_tile_load(PushTile *T, const SpK &s, int64_
   }
 }
 
-template <int S>
-__global__ void __launch_bounds__(256, 4) k_push_mixed_tiled(MeshK m, const float *__restrict__ c32, PushM prm,
+template <int S, int MINB = 4>
+__global__ void __launch_bounds__(256, MINB) k_push_mixed_tiled(MeshK m, const float *__restrict__ c32, PushM prm,
                                                               SpK s, int64_t ntiles) {
   extern __shared__ __align__(16) unsigned char push_smem[];
   PushTile *T = reinterpret_cast<PushTile *>(push_smem);
@@ -2185,6 +2185,10 @@ static int run_push(int sidx, bool do_push, bool do_deposit, bool do_energy) {
         k_push_mixed_tiled<2><<<grid, kPushTile, smem, g.st>>>(m, g.d_coef32, pm, k, ntiles);
       else if (g.push_stages == 3)
         k_push_mixed_tiled<3><<<grid, kPushTile, smem, g.st>>>(m, g.d_coef32, pm, k, ntiles);
+      else if (g.push_minb == 5)
+        k_push_mixed_tiled<4, 5><<<grid, kPushTile, smem, g.st>>>(m, g.d_coef32, pm, k, ntiles);
+      else if (g.push_minb == 6)
+        k_push_mixed_tiled<4, 6><<<grid, kPushTile, smem, g.st>>>(m, g.d_coef32, pm, k, ntiles);
       else
         k_push_mixed_tiled<4><<<grid, kPushTile, smem, g.st>>>(m, g.d_coef32, pm, k, ntiles);
     } else {
@@ -3419,8 +3423,15 @@ int pic_init(const pic_mesh_desc *mesh, const pic_params *params) {
     PIC_CUDA(cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev));
     g.push_grid = 0;
     if (g.push_stages) {
-      const void *fn = g.push_stages == 2 ? (const void *)k_push_mixed_tiled<2>
+      // resident CTAs per SM the 4-stage kernel is compiled for: 5 (48
+      // registers) measured 2.42 ms/step against 2.56 with 4 (56 registers)
+      // and 2.43 with 6 (40 registers, small spills)
+      const char *mb = getenv("PIC_PUSH_MINB");
+      g.push_minb = mb ? atoi(mb) : g.push_minb;
+      const void *fn = g.push_stages == 2   ? (const void *)k_push_mixed_tiled<2>
                        : g.push_stages == 3 ? (const void *)k_push_mixed_tiled<3>
+                       : g.push_minb == 5   ? (const void *)k_push_mixed_tiled<4, 5>
+                       : g.push_minb == 6   ? (const void *)k_push_mixed_tiled<4, 6>
                                             : (const void *)k_push_mixed_tiled<4>;
       int per_sm = 0;
       PIC_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, fn, kPushTile,

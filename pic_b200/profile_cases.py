@@ -2,7 +2,7 @@
 ncu (each runs a few launches of its kernels and exits):
 
     python -m pic_b200.profile_cases step  <deck> <ppc> <steps> [jpcg|fcg|mg] [fp64|mixed]
-    python -m pic_b200.profile_cases solve <cells> [jpcg|fcg|mg] [repeats] [coarse_cells] [fp64|mixed] [omega]
+    python -m pic_b200.profile_cases solve <cells> [jpcg|fcg|mg] [repeats] [coarse_cells] [fp64|mixed] [omega] [max_coarse_nodes]
     python -m pic_b200.profile_cases unet  <nodes> [repeats]
     python -m pic_b200.profile_cases diag  <deck> <ppc> [fp64|mixed] [repeats]
 
@@ -47,7 +47,8 @@ def _step(deck_name, ppc, steps, solver="fcg", precision="fp64"):
     sim.close()
 
 
-def _solve(cells, solver="fcg", repeats=3, coarse_cells=64, precision="fp64", omega=2.0 / 3.0):
+def _solve(cells, solver="fcg", repeats=3, coarse_cells=64, precision="fp64", omega=2.0 / 3.0,
+           max_coarse_nodes=4500):
     import torch
     from . import api, deck
     from .simulation import Simulation
@@ -59,7 +60,7 @@ def _solve(cells, solver="fcg", repeats=3, coarse_cells=64, precision="fp64", om
     import time
     t0 = time.perf_counter()
     if solver == "mg":
-        sim.set_solver("fcg", multigrid=True, omega=float(omega))
+        sim.set_solver("fcg", multigrid=True, omega=float(omega), max_coarse_nodes=int(max_coarse_nodes))
     else:
         sim.set_solver(solver, coarse_cells=int(coarse_cells), omega=float(omega))
     setup = time.perf_counter() - t0
@@ -74,7 +75,8 @@ def _solve(cells, solver="fcg", repeats=3, coarse_cells=64, precision="fp64", om
         e1.record()
         torch.cuda.synchronize()
         out.append((st.iterations, st.outer, round(e0.elapsed_time(e1), 3)))
-    print(f"solve {n}^2 {solver} {precision} coarse_cells={coarse_cells} (setup {setup:.2f} s): "
+    print(f"solve {n}^2 {solver} {precision} coarse_cells={coarse_cells} max_coarse_nodes={max_coarse_nodes} "
+          f"omega={float(omega):.3f} (setup {setup:.2f} s): "
           f"(iterations, outer, ms) {out}")
     sim.close()
 
