@@ -29,12 +29,28 @@ namespace pic {
 // counting sort
 // ---------------------------------------------------------------------------
 
+// Runs of equal keys in a warp (particles are nearly cell-sorted): the head
+// lane of each run, the run's length and each lane's rank in its run.  Equal
+// keys that are not adjacent form separate runs.  Every lane takes part.
+__device__ __forceinline__ void warp_runs(int key, int lane, int *head, int *len, int *rank) {
+  const int prev = __shfl_up_sync(0xffffffffu, key, 1);
+  const bool is_head = lane == 0 || key != prev;
+  const unsigned heads = __ballot_sync(0xffffffffu, is_head);
+  const unsigned upto = heads & (0xffffffffu >> (31 - lane));  // heads at lanes <= lane
+  *head = 31 - __clz(upto);
+  const unsigned above = lane == 31 ? 0u : heads & (0xfffffffeu << lane);  // heads after lane
+  const int end = above ? __ffs(above) - 1 : 32;
+  *len = end - *head;
+  *rank = lane - *head;
+}
+
 __global__ void k_sort_count(const int32_t *__restrict__ loc, int64_t n, int32_t *__restrict__ count) {
   int64_t p = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
   int key = (p < n) ? loc[p] : -1;
-  unsigned int peers = __match_any_sync(0xffffffffu, key);
-  int lane = threadIdx.x & 31;
-  if (key >= 0 && (__ffs(peers) - 1) == lane) atomicAdd(count + key, __popc(peers));
+  const int lane = threadIdx.x & 31;
+  int head, len, rank;
+  warp_runs(key, lane, &head, &len, &rank);
+  if (key >= 0 && rank == 0) atomicAdd(count + key, len);
 }
 
 // exclusive scan, 3 passes of 4096 items per block
@@ -95,25 +111,26 @@ __global__ void k_sort_scatter(const int32_t *__restrict__ loc, const uint32_t *
                                uint32_t *__restrict__ sid) {
   int64_t p = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
   int key = (p < n) ? loc[p] : -1;
-  unsigned int peers = __match_any_sync(0xffffffffu, key);
-  int lane = threadIdx.x & 31;
-  int leader = __ffs(peers) - 1;
+  const int lane = threadIdx.x & 31;
+  int head, len, rank;
+  warp_runs(key, lane, &head, &len, &rank);
   int base = 0;
-  if (key >= 0 && lane == leader) base = atomicAdd(cursor + key, __popc(peers));
-  base = __shfl_sync(peers, base, leader);
+  if (key >= 0 && rank == 0) base = atomicAdd(cursor + key, len);
+  base = __shfl_sync(0xffffffffu, base, head);
   if (key >= 0) {
-    int rank = __popc(peers & ((1u << lane) - 1u));
-    int dst = base + rank;
+    const int dst = base + rank;
     perm[dst] = (int32_t)p;
     sid[dst] = id[p];
   }
 }
 
 // One warp per element: order its segment by id (ids are unique), writing the
-// source slots to perm2.
+// source slots to perm2.  Segments of up to 128 are ranked from shared
+// memory, four ids per read (padded with the largest id, which ranks after
+// every real one).
 __global__ void k_sort_cells(const int32_t *__restrict__ start, int64_t ne, const int32_t *__restrict__ perm,
                              const uint32_t *__restrict__ sid, int32_t *__restrict__ perm2) {
-  __shared__ uint32_t sh[8][128];
+  __shared__ __align__(16) uint32_t sh[8][128];
   int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   int64_t c = (int64_t)blockIdx.x * 8 + warp;
   if (c >= ne) return;
@@ -123,14 +140,26 @@ __global__ void k_sort_cells(const int32_t *__restrict__ start, int64_t ne, cons
     if (lane == 0) perm2[s0] = perm[s0];
     return;
   }
-  const bool in_smem = m <= 128;
-  if (in_smem)
-    for (int k = lane; k < m; k += 32) sh[warp][k] = sid[s0 + k];
-  __syncwarp();
+  if (m <= 128) {
+    const int m4 = (m + 3) & ~3;
+    for (int k = lane; k < m4; k += 32) sh[warp][k] = k < m ? sid[s0 + k] : 0xffffffffu;
+    __syncwarp();
+    const uint4 *v = reinterpret_cast<const uint4 *>(sh[warp]);
+    for (int k = lane; k < m; k += 32) {
+      const uint32_t me = sh[warp][k];
+      int rank = 0;
+      for (int q = 0; q < m4 / 4; ++q) {
+        const uint4 w = v[q];
+        rank += (w.x < me) + (w.y < me) + (w.z < me) + (w.w < me);
+      }
+      perm2[s0 + rank] = perm[s0 + k];
+    }
+    return;
+  }
   for (int k = lane; k < m; k += 32) {
-    uint32_t me = in_smem ? sh[warp][k] : sid[s0 + k];
+    const uint32_t me = sid[s0 + k];
     int rank = 0;
-    for (int q = 0; q < m; ++q) rank += ((in_smem ? sh[warp][q] : sid[s0 + q]) < me);
+    for (int q = 0; q < m; ++q) rank += (sid[s0 + q] < me);
     perm2[s0 + rank] = perm[s0 + k];
   }
 }
@@ -154,18 +183,44 @@ struct Gather7 {
   uint32_t *oid;
 };
 
+// four particles per thread, their slot indices then all their loads issued
+// together (memory-level parallelism for the scattered reads)
+constexpr int kGatherItems = 4;
 template <class T>
 __global__ void k_gather_all(Gather7<T> g7, const int32_t *__restrict__ perm, int64_t n) {
-  int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
-  if (i >= n) return;
-  int32_t p = perm[i];
-  g7.ox[i] = g7.x[p];
-  g7.oy[i] = g7.y[p];
-  g7.ovx[i] = g7.vx[p];
-  g7.ovy[i] = g7.vy[p];
-  g7.ovz[i] = g7.vz[p];
-  g7.oloc[i] = g7.loc[p];
-  g7.oid[i] = g7.id[p];
+  const int64_t i0 = (int64_t)blockIdx.x * blockDim.x * kGatherItems + threadIdx.x;
+  int32_t p[kGatherItems];
+#pragma unroll
+  for (int u = 0; u < kGatherItems; ++u) {
+    const int64_t i = i0 + (int64_t)u * blockDim.x;
+    p[u] = i < n ? perm[i] : -1;
+  }
+  T x[kGatherItems], y[kGatherItems], vx[kGatherItems], vy[kGatherItems], vz[kGatherItems];
+  int32_t lc[kGatherItems];
+  uint32_t id[kGatherItems];
+#pragma unroll
+  for (int u = 0; u < kGatherItems; ++u) {
+    if (p[u] < 0) continue;
+    x[u] = g7.x[p[u]];
+    y[u] = g7.y[p[u]];
+    vx[u] = g7.vx[p[u]];
+    vy[u] = g7.vy[p[u]];
+    vz[u] = g7.vz[p[u]];
+    lc[u] = g7.loc[p[u]];
+    id[u] = g7.id[p[u]];
+  }
+#pragma unroll
+  for (int u = 0; u < kGatherItems; ++u) {
+    if (p[u] < 0) continue;
+    const int64_t i = i0 + (int64_t)u * blockDim.x;
+    g7.ox[i] = x[u];
+    g7.oy[i] = y[u];
+    g7.ovx[i] = vx[u];
+    g7.ovy[i] = vy[u];
+    g7.ovz[i] = vz[u];
+    g7.oloc[i] = lc[u];
+    g7.oid[i] = id[u];
+  }
 }
 
 int sort_species(int sidx) {
@@ -192,10 +247,10 @@ int sort_species(int sidx) {
       auto F = [](double *v) { return reinterpret_cast<float *>(v); };
       Gather7<float> g7{F(s.x), F(s.y), F(s.vx), F(s.vy), F(s.vz), s.loc, s.id,
                         F(s.x2), F(s.y2), F(s.vx2), F(s.vy2), F(s.vz2), s.loc2, s.id2};
-      k_gather_all<float><<<blocks_for(total, 256), 256, 0, g.st>>>(g7, g.d_perm2, total);
+      k_gather_all<float><<<blocks_for(total, 256 * kGatherItems), 256, 0, g.st>>>(g7, g.d_perm2, total);
     } else {
       Gather7<double> g7{s.x, s.y, s.vx, s.vy, s.vz, s.loc, s.id, s.x2, s.y2, s.vx2, s.vy2, s.vz2, s.loc2, s.id2};
-      k_gather_all<double><<<blocks_for(total, 256), 256, 0, g.st>>>(g7, g.d_perm2, total);
+      k_gather_all<double><<<blocks_for(total, 256 * kGatherItems), 256, 0, g.st>>>(g7, g.d_perm2, total);
     }
     PIC_LAUNCHED();
   }

@@ -137,7 +137,10 @@ def config(name: str, **over) -> Config:
                 objs.append(ObjectSpec(api.PIC_SHAPE_ELLIPSE, cx, cy, a, b, ang, eps=eps))
         c = Config("cfg4-1024x1024-8ellipses", 0.16, 0.16, 1024, 1024, objects=objs,
                    wall_V=(0.0, 0.0, 0.0, 0.0), n0=5e15, ppc=64, Te_eV=3.0, nt=5000,
-                   pcg_tol=1e-8, seed=4)
+                   pcg_tol=1e-8, seed=4, sort_interval=20)
+        # counting sort every 20 steps: 6.10 ms/step against 6.23 with 10 and
+        # 6.55 with 5 (B200; the push slows only slightly as particles leave
+        # their sorted cells)
     elif name == "tiny":
         c = Config("tiny-16x16-disk", 0.01, 0.01, 16, 16,
                    objects=[ObjectSpec(api.PIC_SHAPE_CIRCLE, 0.005, 0.0051, 0.0023, eps=4.0)],
