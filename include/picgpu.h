@@ -234,6 +234,15 @@ int pic_download_particles(int32_t species, int64_t capacity, double *x, double 
                            double *vx, double *vy, double *vz, int32_t *loc,
                            uint32_t *id, int64_t *n_out);
 int pic_particle_count(int32_t species, int64_t *n);
+/* The id the next particle created in `species` (MCC ionisation) receives.
+ * pic_upload_particles sets it to the largest uploaded id + 1; a restart
+ * restores the saved value with pic_set_next_id, which refuses values below
+ * the current one (ids would repeat).  Created particles draw their random
+ * numbers by id, so a restart that kept a smaller next id would diverge.
+ * The reference keeps no particle ids (ParticleBundle.f90:286-375 dumps the
+ * particles without them). */
+int pic_get_next_id(int32_t species, uint32_t *next_id);
+int pic_set_next_id(int32_t species, uint32_t next_id);
 
 /* ParticlePositioning / InjectPositioning (ParticlePositioning.f90,
  * InjectPositioning.f90:1-24, call site GetParChg_2D.f90:137-163):

@@ -3553,6 +3553,28 @@ int pic_particle_count(int32_t species, int64_t *n) {
   return PIC_OK;
 }
 
+int pic_get_next_id(int32_t species, uint32_t *next_id) {
+  int rc;
+  if ((rc = check_init()) || (rc = check_species(species))) return rc;
+  if (!next_id) {
+    set_error("pic_get_next_id: null output");
+    return PIC_ERR_ARG;
+  }
+  *next_id = g.sp[species].next_id;
+  return PIC_OK;
+}
+
+int pic_set_next_id(int32_t species, uint32_t next_id) {
+  int rc;
+  if ((rc = check_init()) || (rc = check_species(species))) return rc;
+  if (next_id < g.sp[species].next_id) {
+    set_error("pic_set_next_id: below the largest id in use + 1 (ids would repeat)");
+    return PIC_ERR_ARG;
+  }
+  g.sp[species].next_id = next_id;
+  return PIC_OK;
+}
+
 int pic_download_particles(int32_t species, int64_t capacity, double *x, double *y, double *vx,
                            double *vy, double *vz, int32_t *loc, uint32_t *id, int64_t *n_out) {
   int rc;

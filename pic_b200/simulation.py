@@ -20,7 +20,9 @@ from .mcc_tables import ar_tables
 
 class Simulation:
     def __init__(self, cfg: Config, capacity_factor: float = 1.5, load: bool = True,
-                 mcc: bool | None = None):
+                 mcc: bool | None = None, capacity: list | None = None):
+        """load: generate and upload the deck's initial particles.  capacity:
+        particle slots per species (default: 1.5 x the initial count)."""
         self.lib = api.load()
         self.cfg = cfg
         self.mesh = Mesh(cfg)
@@ -38,6 +40,8 @@ class Simulation:
             p.species[s].mass = m
             p.species[s].weight = w
             p.species[s].capacity = max(int(n0 * capacity_factor) + 1024, 1024)
+            if capacity is not None:
+                p.species[s].capacity = int(capacity[s])
         p.dt = cfg.dt
         p.n_ref = cfg.n0
         p.T_ref_eV = cfg.Te_eV
