@@ -48,7 +48,7 @@ MIXED_PUSH_BYTES = 40  # read elem + 4 FP32 (20 B), write the same (20 B)
 # DRAM bytes per particle of one push launch measured by ncu (dram__bytes_read
 # + dram__bytes_write on the 1024^2 deck at 8 particles per cell; the traffic
 # grows in proportion to the particle count)
-NCU_PUSH_TRAFFIC = {"fp64": 68.0, "mixed": 37.9}
+NCU_PUSH_TRAFFIC = {"fp64": 68.0, "mixed": 38.3}
 
 
 def _dist():
@@ -441,7 +441,8 @@ def run_ours(args, dist, rank, ws):
         "learned_training": None if lp is None else {
             "warmup_steps": args.train_steps, "adam_steps": len(lp.losses), "seconds": train_s,
             "loss_first": lp.losses[0], "loss_last": lp.losses[-1]},
-        "roofline": {"kernel": "k_push (fused push+locate+deposit)", "bound": "hbm",
+        "roofline": {"kernel": ("k_push_mixed_tiled" if args.precision == "mixed" else "k_push")
+                     + " (fused push+locate+deposit)", "bound": "hbm",
                      "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
                      "peak_source": peak_src, "bytes_per_particle": push_bytes,
                      "traffic": NCU_PUSH_TRAFFIC[args.precision] * push_n,
