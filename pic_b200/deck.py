@@ -238,6 +238,43 @@ def species_params(cfg: Config):
     return out, L
 
 
+def _inside(o, x, y):
+    """Particles strictly inside object o (the test k_push and the oracle
+    apply), elementwise on arrays."""
+    if o.shape == api.PIC_SHAPE_CIRCLE:
+        return (x - o.cx) ** 2 + (y - o.cy) ** 2 < o.a * o.a
+    if o.shape == api.PIC_SHAPE_BOX:
+        return (x > o.cx) & (x < o.a) & (y > o.cy) & (y < o.b)
+    if o.shape == api.PIC_SHAPE_ELLIPSE:
+        c, s = math.cos(o.angle), math.sin(o.angle)
+        u = (x - o.cx) * c + (y - o.cy) * s
+        v = -(x - o.cx) * s + (y - o.cy) * c
+        return u * u / (o.a * o.a) + v * v / (o.b * o.b) < 1.0
+    return np.zeros(x.shape, dtype=bool)
+
+
+def _cells_box(o, mesh, ncell, ncy, ppc):
+    """Indices of the loaded particles whose cell meets object o's bounding
+    box (particles are generated cell by cell, ppc per cell, cell = i*ncy + j,
+    so a box is one index range per cell column); only they can be inside."""
+    if o.shape == api.PIC_SHAPE_BOX:
+        x0, x1, y0, y1 = o.cx, o.a, o.cy, o.b
+    else:
+        r = o.a if o.shape == api.PIC_SHAPE_CIRCLE else max(o.a, o.b)
+        x0, x1, y0, y1 = o.cx - r, o.cx + r, o.cy - r, o.cy + r
+    i0 = max(int(math.floor(x0 / mesh.hx)) - 1, 0)
+    i1 = int(math.floor(x1 / mesh.hx)) + 1
+    j0 = max(int(math.floor(y0 / mesh.hy)) - 1, 0)
+    j1 = min(int(math.floor(y1 / mesh.hy)) + 1, ncy - 1)
+    parts = []
+    for i in range(i0, i1 + 1):
+        c0, c1 = i * ncy + j0, min(i * ncy + j1, ncell - 1)
+        if c0 >= ncell or c1 < c0:
+            continue
+        parts.append(np.arange(c0 * ppc, (c1 + 1) * ppc, dtype=np.int64))
+    return np.concatenate(parts) if parts else np.zeros(0, dtype=np.int64)
+
+
 def load_particles(cfg: Config, mesh: Mesh, species: int, n_cells_limit: int | None = None):
     """Seeded uniform loading, ppc per cell, outside the objects; Maxwellian velocities."""
     sp, _ = species_params(cfg)
@@ -254,15 +291,9 @@ def load_particles(cfg: Config, mesh: Mesh, species: int, n_cells_limit: int | N
     dk = mesh.deck
     for k in range(dk.n_objects):
         o = dk.objects[k]
-        if o.shape == api.PIC_SHAPE_CIRCLE:
-            keep &= ~((x - o.cx) ** 2 + (y - o.cy) ** 2 < o.a * o.a)
-        elif o.shape == api.PIC_SHAPE_BOX:
-            keep &= ~((x > o.cx) & (x < o.a) & (y > o.cy) & (y < o.b))
-        elif o.shape == api.PIC_SHAPE_ELLIPSE:
-            c, s = math.cos(o.angle), math.sin(o.angle)
-            u = (x - o.cx) * c + (y - o.cy) * s
-            v = -(x - o.cx) * s + (y - o.cy) * c
-            keep &= ~(u * u / (o.a * o.a) + v * v / (o.b * o.b) < 1.0)
+        idx = _cells_box(o, mesh, ncell, ncy, cfg.ppc)
+        xs, ys = x[idx], y[idx]
+        keep[idx] &= ~_inside(o, xs, ys)
     x, y = x[keep], y[keep]
     m = x.size
     v = rng.standard_normal((3, m)) * sigma
