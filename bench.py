@@ -93,12 +93,16 @@ def _sum_over_ranks(dist, v: float) -> float:
 
 
 class ClockSampler:
-    """nvidia-smi clocks and throttle reasons during the timed region."""
+    """nvidia-smi clocks and throttle reasons, every 50 ms, each sample
+    stamped with the host time it arrived; summary() keeps the samples inside
+    a marked window (the timed region).  Started before the warm-up so that
+    nvidia-smi's own start-up does not eat the short timed region."""
 
     def __init__(self, index: int):
         self.index = index
         self.rows = []
         self.proc = None
+        self.window = None
 
     def __enter__(self):
         q = ("clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.hw_slowdown,"
@@ -107,7 +111,7 @@ class ClockSampler:
         try:
             self.proc = subprocess.Popen(
                 ["nvidia-smi", "-i", str(self.index), "--query-gpu=" + q,
-                 "--format=csv,noheader,nounits", "-lms", "200"],
+                 "--format=csv,noheader,nounits", "-lms", "50"],
                 stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
             self.thread = threading.Thread(target=self._read, daemon=True)
             self.thread.start()
@@ -119,7 +123,11 @@ class ClockSampler:
         for line in self.proc.stdout:
             parts = [p.strip() for p in line.split(",")]
             if len(parts) == 7:
-                self.rows.append(parts)
+                self.rows.append((time.perf_counter(), parts))
+
+    def mark(self, t0: float, t1: float):
+        """The host-time window [t0, t1] of the timed region."""
+        self.window = (t0, t1)
 
     def __exit__(self, *a):
         if self.proc is not None:
@@ -130,14 +138,24 @@ class ClockSampler:
                 self.proc.kill()
 
     def summary(self):
-        if not self.rows:
+        rows, where = [r for _, r in self.rows], "all"
+        if self.window and self.rows:
+            t0, t1 = self.window
+            inside = [r for t, r in self.rows if t0 <= t <= t1]
+            if inside:
+                rows, where = inside, "timed region"
+            else:  # the timed region fell between two samples: the nearest one
+                tm = 0.5 * (t0 + t1)
+                rows, where = [min(self.rows, key=lambda tr: abs(tr[0] - tm))[1]], "nearest to the timed region"
+        if not rows:
             return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"]}
-        sm = [float(r[0]) for r in self.rows if r[0].replace(".", "").isdigit()]
-        mx = [float(r[1]) for r in self.rows if r[1].replace(".", "").isdigit()]
+        sm = [float(r[0]) for r in rows if r[0].replace(".", "").isdigit()]
+        mx = [float(r[1]) for r in rows if r[1].replace(".", "").isdigit()]
         names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
-        reasons = sorted({names[k] for r in self.rows for k in range(4) if r[3 + k] == "Active"})
+        reasons = sorted({names[k] for r in rows for k in range(4) if r[3 + k] == "Active"})
         return {"sm_mhz": statistics.median(sm) if sm else None,
-                "sm_max_mhz": max(mx) if mx else None, "reasons": reasons, "samples": len(self.rows)}
+                "sm_max_mhz": max(mx) if mx else None, "reasons": reasons, "samples": len(rows),
+                "samples_from": where, "interval_ms": 50}
 
 
 def _peaks():
@@ -362,14 +380,17 @@ def run_ours(args, dist, rank, ws):
     variants[best]()
     if lp is not None and best != "fcg_smooth_coarse_learned":
         lp.set_learned(False)
-    for _ in range(args.warmup):
-        sim.step()
-    _barrier(dist)
-    if torch.cuda.is_available():
-        torch.cuda.synchronize()
-    launches0 = lib.pic_kernel_launches()
     with ClockSampler(dev) as clk:
+        for _ in range(args.warmup):
+            sim.step()
+        _barrier(dist)
+        if torch.cuda.is_available():
+            torch.cuda.synchronize()
+        launches0 = lib.pic_kernel_launches()
+        t_clk0 = time.perf_counter()
         ms_total, stats = _timed_steps(sim, lib, api, args.steps)
+        clk.mark(t_clk0, time.perf_counter())
+        time.sleep(0.06)  # let the sample that covers the end arrive
     launches = lib.pic_kernel_launches() - launches0
     if torch.cuda.is_available():
         torch.cuda.synchronize()
