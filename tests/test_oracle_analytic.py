@@ -1,8 +1,9 @@
 """Analytic known answers for the parts of the oracle that the reference
-holds no outputs for (push, stiffness, Jacobi-PCG): free streaming, a
+holds no outputs for (push, stiffness, Jacobi-PCG, MCC): free streaming, a
 uniform field through both gathers (bilinear nodal E and the interface
-elements' PPR gradients), the Q1 stiffness stencil, and the PCG solution
-against a direct sparse solve.  CPU only."""
+elements' PPR gradients), the Q1 stiffness stencil, the PCG solution
+against a direct sparse solve, and the energy bookkeeping of elastic,
+excitation and ionisation collisions.  CPU only."""
 import numpy as np
 import scipy.sparse as sp
 import scipy.sparse.linalg as spl
@@ -109,3 +110,92 @@ def test_pcg_matches_direct_solve():
         assert np.array_equal(phi[nt <= 0], phi0[nt <= 0])
     finally:
         mesh.close()
+
+
+# ---- MCC collision laws in the limit of an infinitely heavy, cold gas: the
+# target is at rest and the mass ratio M/(m+M) rounds to 1, so an elastic
+# scattering keeps the speed, an excitation leaves E - E_thr, and an
+# ionisation splits E - E_thr between the scattered and the created electron
+# (the ion is created at rest).
+
+import ctypes as C  # noqa: E402
+
+from pic_b200 import api  # noqa: E402
+
+_JTOEV = 1.6022e-19
+
+
+def _table(rtype, thr):
+    """Every particle collides (ratio 1) and takes reaction `rtype`
+    (cumulative probability 1 from its column on, at every energy)."""
+    t = api.MccTable()
+    t.species, t.n_reaction, t.n_sigma = 0, 3, 12
+    t.energy_min, t.energy_interval, t.energy_max = -3.0, 0.5, 1e6
+    t.collision_ratio = 1.0
+    types = (11, 12, 13)
+    col = types.index(rtype)
+    for j in range(3):
+        t.reaction_type[j] = types[j]
+        t.threshold[j] = 0.0 if types[j] == 11 else thr
+        t.resultant[j] = 1 if types[j] == 13 else -1
+    prob = np.zeros((12, 3))
+    prob[:, col:] = 1.0
+    keep = np.ascontiguousarray(prob.ravel())
+    t.probability = keep.ctypes.data_as(C.POINTER(C.c_double))
+    return t, keep
+
+
+def _electrons(n, vref, seed=3):
+    rng = np.random.default_rng(seed)
+    # speeds for 5..60 eV electrons, random directions (normalised by vref)
+    e = rng.uniform(5.0, 60.0, n)
+    v = np.sqrt(2.0 * e * _JTOEV / deck.ME) / vref
+    d = rng.standard_normal((3, n))
+    d /= np.linalg.norm(d, axis=0)
+    return {"x": np.zeros(n), "loc": np.zeros(n, np.int32), "id": np.arange(n, dtype=np.uint32),
+            "vx": v * d[0], "vy": v * d[1], "vz": v * d[2]}
+
+
+def _energy(p, vref):
+    v2 = p["vx"] ** 2 + p["vy"] ** 2 + p["vz"] ** 2
+    return 0.5 * deck.ME * v2 * vref * vref / _JTOEV
+
+
+def _run(rtype, thr=11.5):
+    vref = 5.93e5
+    gas = api.Gas()
+    gas.mass, gas.temperature, gas.density = 1e30, 0.0, 1e21
+    t, keep = _table(rtype, thr)
+    p = _electrons(3000, vref)
+    e0 = _energy(p, vref)
+    ncoll, counts, par, ne, ni = ob.mcc(t, gas, deck.ME, vref, 17, 5, 0, p)
+    return p, e0, ncoll, counts, par, ne, ni, vref, keep
+
+
+def test_mcc_elastic_keeps_the_speed():
+    p, e0, ncoll, counts, _, _, _, vref, _ = _run(11)
+    assert ncoll == p["vx"].size and counts[0] == ncoll
+    assert np.allclose(_energy(p, vref), e0, rtol=1e-12, atol=0)
+
+
+def test_mcc_excitation_loses_the_threshold():
+    thr = 11.5
+    p, e0, ncoll, counts, _, _, _, vref, _ = _run(12, thr)
+    hit = e0 > thr
+    assert counts[1] == hit.sum() and counts[0] == 0
+    e1 = _energy(p, vref)
+    assert np.allclose(e1[hit], e0[hit] - thr, rtol=1e-12, atol=1e-12 * e0.max())
+    # below threshold no reaction: the speed only passes through SI units and back
+    assert np.allclose(e1[~hit], e0[~hit], rtol=1e-14, atol=0)
+
+
+def test_mcc_ionisation_balances_energy():
+    thr = 11.5
+    p, e0, ncoll, counts, par, ne, ni, vref, _ = _run(13, thr)
+    hit = e0 > thr
+    assert counts[2] == hit.sum() == par.size
+    assert np.all(np.diff(p["id"][par].astype(np.int64)) > 0)  # created in parent-id order
+    e1 = _energy(p, vref)
+    e_new = 0.5 * deck.ME * (ne ** 2).sum(axis=1) * vref * vref / _JTOEV
+    assert np.allclose(e1[par] + e_new, e0[par] - thr, rtol=1e-12, atol=1e-12 * e0.max())
+    assert np.all(ni == 0.0)  # the ion takes the (resting) target's velocity
