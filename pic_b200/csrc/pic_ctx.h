@@ -198,6 +198,7 @@ struct Ctx {
   int32_t *d_mlist_slot = nullptr;     //   and their slots
   int64_t mlist_cap = 0;
   int mcc_full = 0;                    // 1: always the full-histogram selection
+  double mcc_bound_scale = 1.0;        // test hook: < 1 forces the bounded selection's fallback
   int64_t *d_msel = nullptr;           // [8]: list count, keys below the bound, b*, count below b*
   int64_t *d_ion_parent = nullptr;     // ionising parents: (id<<32 | slot)
   double *d_ion_data = nullptr;        // per ionisation: new e- v(3), ion v(3)

@@ -3415,6 +3415,8 @@ int pic_init(const pic_mesh_desc *mesh, const pic_params *params) {
     // directly
     const char *mf = getenv("PIC_MCC_FULL");  // 1: MCC selection by the full key histogram
     g.mcc_full = (mf && atoi(mf) == 1) ? 1 : 0;
+    const char *mb2 = getenv("PIC_MCC_BOUND_SCALE");  // test hook (see mcc_bound_scale)
+    g.mcc_bound_scale = mb2 ? std::max(1e-6, atof(mb2)) : 1.0;
     const char *ps = getenv("PIC_PUSH_STAGES");
     g.push_stages = ps ? atoi(ps) : g.push_stages;
     if (g.push_stages != 0 && (g.push_stages < 2 || g.push_stages > 4)) g.push_stages = 0;

@@ -571,8 +571,10 @@ int mcc_run(uint64_t step, pic_mcc_stats *stats) {
     // standard deviations); used while that is a small part of the species
     const double target = 2.0 * (double)ncoll + 64.0 + 8.0 * std::sqrt(2.0 * (double)ncoll + 64.0);
     if (!g.mcc_full && target < 0.25 * (double)npar) {
-      const uint64_t bound =
-          std::max<uint64_t>(1, (uint64_t)std::ceil(target / (double)npar * 4294967296.0));
+      // g.mcc_bound_scale < 1 (a test hook) makes the bound too small, so the
+      // selection takes its fallback
+      const uint64_t bound = std::max<uint64_t>(
+          1, (uint64_t)std::ceil(g.mcc_bound_scale * target / (double)npar * 4294967296.0));
       const int64_t lcap = (int64_t)(1.5 * target) + 4096;
       if ((rc = mcc_list_alloc(lcap))) return rc;
       if ((rc = mcc_alloc(std::max<int64_t>(ncoll, 1 << 16) + 4096))) return rc;

@@ -407,16 +407,21 @@ def test_edge_cases():
         sim.close()
 
 
-@pytest.mark.parametrize("precision", [api.PIC_PREC_FP64, api.PIC_PREC_MIXED])
-def test_mcc_bounded_selection_matches_full(precision, monkeypatch):
+@pytest.mark.parametrize("precision,mode", [(api.PIC_PREC_FP64, "bounded"), (api.PIC_PREC_MIXED, "bounded"),
+                                            (api.PIC_PREC_MIXED, "fallback")])
+def test_mcc_bounded_selection_matches_full(precision, mode, monkeypatch):
     """The selection under a key bound (histogram and compact list of the
     keys below it, threshold and ties found on the device) picks the same
     ncoll smallest (key, id) as the full key histogram (PIC_MCC_FULL=1):
     after 6 steps with MCC the particles, fields and reaction counts are
-    bit-identical."""
+    bit-identical.  "fallback": the bound made too small (a test hook), so
+    every bounded selection finds too few keys and redoes the selection with
+    the full histogram."""
     out = []
     for full in ("1", "0"):
         monkeypatch.setenv("PIC_MCC_FULL", full)
+        if mode == "fallback":
+            monkeypatch.setenv("PIC_MCC_BOUND_SCALE", "0.01")
         sim = Simulation(deck.config("cfg1", precision=precision))
         try:
             sim.initial_fields()
