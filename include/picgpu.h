@@ -77,7 +77,9 @@ typedef struct pic_object {
 typedef struct pic_deck {
   int32_t nnx, nny;            /* nodes per direction                        */
   double xmin, xmax, ymin, ymax;
-  int32_t delta;               /* 0 Cartesian (1 axisymmetric: not built)    */
+  int32_t delta;               /* 0 Cartesian; 1 axisymmetric r-z (r = y, the
+                                  axis at y = ymin = 0): pic_mesh_build only,
+                                  pic_init refuses it                         */
   int32_t wall_dirichlet[4];   /* left, right, bottom, top: 1 Dirichlet       */
   double wall_phi[4];          /* Dirichlet values                            */
   int32_t n_objects;
@@ -112,6 +114,8 @@ typedef struct pic_mesh_desc {
   const int32_t *patch_nodes; /* 1-based node ids (point_patch(i,2:))             */
   int32_t n_objects;
   const pic_object *objects;
+  const double *mass_rows; /* delta 1: [ (nny-1) * 16 ] r-weighted Q1 load matrix
+                              of each element row, row-major; NULL for delta 0 */
 } pic_mesh_desc;
 
 typedef struct pic_species_desc {

@@ -272,7 +272,9 @@ void or_rhs(const pic_mesh_desc *d, const double *rho, double *b) {
     for (int ej = 0; ej < m.ney; ++ej) {
       int64_t e = (int64_t)ei * m.ney + ej;
       int id = d->element_index[e];
-      const double *M = id > 0 ? d->ife_mass + 16 * (size_t)(id - 1) : d->mass_q1;
+      /* axisymmetric (Global_RHS_PDE_2D.f90:98): the element row's r-weighted matrix */
+      const double *Mreg = (d->delta == 1 && d->mass_rows) ? d->mass_rows + 16 * (size_t)ej : d->mass_q1;
+      const double *M = id > 0 ? d->ife_mass + 16 * (size_t)(id - 1) : Mreg;
       int64_t n1 = (int64_t)ei * m.nny + ej;
       int64_t nd[4] = {n1, n1 + m.nny, n1 + m.nny + 1, n1 + 1};
       double R[4] = {rho[nd[0]], rho[nd[1]], rho[nd[2]], rho[nd[3]]};

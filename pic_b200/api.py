@@ -85,7 +85,7 @@ class MeshDesc(C.Structure):
                 ("mass_q1", _P(C.c_double)), ("n_interface", C.c_int32),
                 ("ife_mass", _P(C.c_double)), ("patch_ptr", _P(C.c_int32)),
                 ("patch_nodes", _P(C.c_int32)), ("n_objects", C.c_int32),
-                ("objects", _P(Object))]
+                ("objects", _P(Object)), ("mass_rows", _P(C.c_double))]
 
 
 class SpeciesDesc(C.Structure):

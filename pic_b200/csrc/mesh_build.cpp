@@ -57,7 +57,7 @@ struct MeshStore {
   std::vector<int32_t> node_type, node_index, element_index;
   std::vector<double> phi_dirichlet, cell_volume;
   std::vector<int32_t> a_srow, a_jcol, xt_srow, xt_jcol;
-  std::vector<double> a_k, xt_k, a_diag, rhs_fix, mass_q1, ife_mass;
+  std::vector<double> a_k, xt_k, a_diag, rhs_fix, mass_q1, ife_mass, mass_rows;
   std::vector<int32_t> patch_ptr, patch_nodes;
   std::vector<pic_object> objects;
   std::vector<IfeElem> ife;
@@ -290,11 +290,45 @@ void ife_stiffness(const IfeElem &f, double K[4][4]) {
   }
 }
 
+// Axisymmetric (r = y) element stiffness of an interface element: the
+// integrand is now cubic, so each sub-triangle takes a collapsed 3x3
+// Gauss-Legendre rule (exact to degree 4 on the triangle), in place of the
+// reference's nine-point triangle rule (Gauss_integration_local_stiffness_IFE.f90,
+// delta == 1 branch): both are exact here, so they agree to rounding.
+void ife_stiffness_axi(const IfeElem &f, double K[4][4]) {
+  for (int j = 0; j < 4; ++j)
+    for (int k = 0; k < 4; ++k) K[j][k] = 0;
+  double T[4][3][2];
+  int piece[4];
+  int nt = ife_triangles(f, T, piece);
+  const double g = std::sqrt(0.6);
+  const double u[3] = {0.5 * (1.0 - g), 0.5, 0.5 * (1.0 + g)};
+  const double w[3] = {5.0 / 18.0, 8.0 / 18.0, 5.0 / 18.0};
+  for (int t = 0; t < nt; ++t) {
+    const double A = tri_area(T[t]);
+    const double beta = f.beta[piece[t]];
+    const double *P0 = T[t][0], *P1 = T[t][1], *P2 = T[t][2];
+    for (int a = 0; a < 3; ++a)
+      for (int b = 0; b < 3; ++b) {
+        // (s, q) in the unit square -> P0 + s (P1 - P0) + s q (P2 - P1), Jacobian 2 A s
+        const double sa = u[a], qb = u[b];
+        const double x = P0[0] + sa * (P1[0] - P0[0]) + sa * qb * (P2[0] - P1[0]);
+        const double y = P0[1] + sa * (P1[1] - P0[1]) + sa * qb * (P2[1] - P1[1]);
+        const double wt = w[a] * w[b] * 2.0 * A * sa * y;
+        double gx[4], gy[4];
+        for (int rb = 0; rb < 4; ++rb) ife_eval(f, rb, piece[t], x, y, nullptr, &gx[rb], &gy[rb]);
+        for (int rj = 0; rj < 4; ++rj)
+          for (int rk = 0; rk < 4; ++rk)
+            K[f.ref2loc[rj]][f.ref2loc[rk]] += wt * beta * (gx[rj] * gx[rk] + gy[rj] * gy[rk]);
+      }
+  }
+}
+
 // Load matrix of an interface element (IFE_RHS_2D.f90) with the reference's
 // piecewise-bilinear "linear IFE" interpolation (Linear_IFE_Basis_Coeff_2D.f90),
 // its sub-triangles (Inter_Tetra_Partition_2D.f90) and edge-midpoint rule
 // (Gauss_Nodes_Elem_2D).  Coordinates are taken relative to reference vertex 1.
-bool ife_load_matrix(const IfeElem &f, double Mout[16]) {
+bool ife_load_matrix(const IfeElem &f, double Mout[16], int axi) {
   double ox = f.X[0][0], oy = f.X[0][1];
   double v[4][2];
   for (int r = 0; r < 4; ++r) { v[r][0] = f.X[r][0] - ox; v[r][1] = f.X[r][1] - oy; }
@@ -350,9 +384,11 @@ bool ife_load_matrix(const IfeElem &f, double Mout[16]) {
         const double *c = coef[b] + 4 * reg;
         ps[b] = c[0] + c[1] * x + c[2] * y + c[3] * x * y;
       }
+      // axisymmetric (IFE_RHS_2D.f90:95): the same points, weighted by r = y
+      const double rw = axi ? (y + oy) : 1.0;
       for (int rj = 0; rj < 4; ++rj)
         for (int rk = 0; rk < 4; ++rk)
-          Mout[f.ref2loc[rj] * 4 + f.ref2loc[rk]] += V * (1.0 / 3.0) * ps[rj] * ps[rk];
+          Mout[f.ref2loc[rj] * 4 + f.ref2loc[rk]] += V * (1.0 / 3.0) * ps[rj] * ps[rk] * rw;
     }
   }
   return true;
@@ -371,10 +407,11 @@ int pic_mesh_build(const pic_deck *deck, pic_mesh_desc **out) {
     pic::set_error("pic_mesh_build: bad mesh extent or object count");
     return PIC_ERR_ARG;
   }
-  if (deck->delta != 0) {
-    pic::set_error("pic_mesh_build: axisymmetric (delta=1) meshes are not built");
-    return PIC_ERR_SETUP;
+  if (deck->delta != 0 && deck->delta != 1) {
+    pic::set_error("pic_mesh_build: delta must be 0 (Cartesian) or 1 (axisymmetric)");
+    return PIC_ERR_ARG;
   }
+  const bool axi = deck->delta == 1;
   MeshStore *S = new (std::nothrow) MeshStore();
   if (!S) return PIC_ERR_ARG;
   const int64_t nn = (int64_t)nnx * nny;
@@ -593,6 +630,30 @@ int pic_mesh_build(const pic_deck *deck, pic_mesh_desc **out) {
     for (int a = 0; a < 4; ++a)
       for (int b = 0; b < 4; ++b) Kq1[a][b] = (hy / hx * Kx[a][b] + hx / hy * Ky[a][b]) / 6.0;
   }
+  // Axisymmetric (r = y): the Q1 stiffness and load matrices of element row j
+  // weighted by r (Gauss_integration_local_stiffness.f90:88,
+  // Global_RHS_PDE_2D.f90:98), by 2x2 Gauss-Legendre, exact for these
+  // degrees (quadratic x linear).  HT order: (0,0), (1,0), (1,1), (0,1).
+  std::vector<double> Kaxi, Maxi;
+  if (axi) {
+    Kaxi.assign((size_t)16 * ney, 0.0);
+    Maxi.assign((size_t)16 * ney, 0.0);
+    const double gq = 0.5 / std::sqrt(3.0), t[2] = {0.5 - gq, 0.5 + gq};
+    for (int j = 0; j < ney; ++j) {
+      const double r0 = Y(j), hr = Y(j + 1) - Y(j);
+      for (int a = 0; a < 2; ++a)
+        for (int b = 0; b < 2; ++b) {
+          const double xi = t[a], et = t[b], r = r0 + hr * et, w = 0.25 * hx * hr * r;
+          const double X1[4] = {1 - xi, xi, xi, 1 - xi}, R1[4] = {1 - et, 1 - et, et, et};
+          const double dX[4] = {-1 / hx, 1 / hx, 1 / hx, -1 / hx}, dR[4] = {-1 / hr, -1 / hr, 1 / hr, 1 / hr};
+          for (int p = 0; p < 4; ++p)
+            for (int q = 0; q < 4; ++q) {
+              Kaxi[16 * j + 4 * p + q] += w * (dX[p] * R1[p] * dX[q] * R1[q] + X1[p] * dR[p] * X1[q] * dR[q]);
+              Maxi[16 * j + 4 * p + q] += w * (X1[p] * R1[p]) * (X1[q] * R1[q]);
+            }
+        }
+    }
+  }
   auto find_col = [&](const std::vector<int32_t> &srow, const std::vector<int32_t> &jcol,
                       int64_t r, int32_t col) -> int64_t {
     for (int64_t m = srow[r] - 1; m < srow[r + 1] - 1; ++m)
@@ -604,10 +665,14 @@ int pic_mesh_build(const pic_deck *deck, pic_mesh_desc **out) {
       int64_t e = elem(i, j);
       double K[4][4];
       int32_t eid = S->element_index[e];
-      if (eid > 0) ife_stiffness(S->ife[eid - 1], K);
-      else
+      if (eid > 0) {
+        if (axi) ife_stiffness_axi(S->ife[eid - 1], K);
+        else ife_stiffness(S->ife[eid - 1], K);
+      } else {
         for (int a = 0; a < 4; ++a)
-          for (int b = 0; b < 4; ++b) K[a][b] = elem_beta[e] * Kq1[a][b];
+          for (int b = 0; b < 4; ++b)
+            K[a][b] = elem_beta[e] * (axi ? Kaxi[16 * j + 4 * a + b] : Kq1[a][b]);
+      }
       int64_t nodes[4];
       for (int c = 0; c < 4; ++c) nodes[c] = node(i + loc_di[c], j + loc_dj[c]);
       for (int k = 0; k < 4; ++k) {
@@ -639,11 +704,13 @@ int pic_mesh_build(const pic_deck *deck, pic_mesh_desc **out) {
   }
   S->ife_mass.resize(16 * S->ife.size());
   for (size_t k = 0; k < S->ife.size(); ++k)
-    if (!ife_load_matrix(S->ife[k], &S->ife_mass[16 * k])) {
+    if (!ife_load_matrix(S->ife[k], &S->ife_mass[16 * k], axi ? 1 : 0)) {
       pic::set_error("pic_mesh_build: singular interface load-matrix system");
       delete S;
       return PIC_ERR_SETUP;
     }
+
+  if (axi) S->mass_rows = Maxi;
 
   // ---- dual-cell volume (Cartesian): corners hx*hy/4, edges hx*hy/2, interior hx*hy
   S->cell_volume.assign(nn, 0.0);
@@ -652,8 +719,20 @@ int pic_mesh_build(const pic_deck *deck, pic_mesh_desc **out) {
       int ie = std::min(i, nnx - 2), je = std::min(j, nny - 2);
       double hxp = X(ie + 1) - X(ie), hyp = Y(je + 1) - Y(je);
       bool bx = (i == 0 || i == nnx - 1), by = (j == 0 || j == nny - 1);
-      double div = (bx && by) ? 4.0 : ((bx || by) ? 2.0 : 1.0);
-      S->cell_volume[node(i, j)] = hxp * hyp / div;
+      if (!axi) {
+        double div = (bx && by) ? 4.0 : ((bx || by) ? 2.0 : 1.0);
+        S->cell_volume[node(i, j)] = hxp * hyp / div;
+        continue;
+      }
+      // axisymmetric (SetupGrids_2D_QLL.f90:233-289): rings of the dual cell,
+      // r = y; on r = ymin / ymax the half cell's mean radius R +- hy/4
+      const double pi = 3.14159265358979, y = Y(j);
+      double v;
+      if (j == 0) v = 2.0 * pi * (deck->ymin + hyp / 4.0) * (hyp / 2.0) * hxp;
+      else if (j == nny - 1) v = 2.0 * pi * (deck->ymax - hyp / 4.0) * (hyp / 2.0) * hxp;
+      else v = 2.0 * pi * y * hyp * hxp;
+      if (bx) v = v / 2.0;  // on the z walls (and at the corners) half the cell
+      S->cell_volume[node(i, j)] = v;
     }
 
   // ---- PPR patches (Get_PointPatch.f90)
@@ -764,6 +843,7 @@ int pic_mesh_build(const pic_deck *deck, pic_mesh_desc **out) {
   d.a_diag = S->a_diag.data();
   d.rhs_fix = S->rhs_fix.data();
   d.mass_q1 = S->mass_q1.data();
+  d.mass_rows = axi ? S->mass_rows.data() : nullptr;
   d.n_interface = (int32_t)S->ife.size();
   d.ife_mass = S->ife_mass.data();
   d.patch_ptr = S->patch_ptr.data();

@@ -204,7 +204,8 @@ class Mesh:
                  "a_srow": d.n_unknowns + 1, "a_jcol": d.nnz, "a_k": d.nnz,
                  "xt_srow": d.n_unknowns + 1, "xt_jcol": d.nnz_xt, "xt_k": d.nnz_xt,
                  "a_diag": d.n_unknowns, "rhs_fix": d.n_unknowns, "mass_q1": 16,
-                 "ife_mass": 16 * d.n_interface, "patch_ptr": self.nn + 1}
+                 "ife_mass": 16 * d.n_interface, "patch_ptr": self.nn + 1,
+                 "mass_rows": 16 * (self.nny - 1)}
         if name == "patch_nodes":
             n = int(self.array("patch_ptr")[-1])
         else:

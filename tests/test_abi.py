@@ -46,8 +46,8 @@ def test_mesh_builder_rejects_bad_decks():
     ptr = C.POINTER(api.MeshDesc)()
     assert lib.pic_mesh_build(C.byref(d), C.byref(ptr)) == -1
     d = deck.make_deck(deck.config("tiny"))
-    d.delta = 1
-    assert lib.pic_mesh_build(C.byref(d), C.byref(ptr)) == -8
+    d.delta = 2  # neither Cartesian (0) nor axisymmetric (1)
+    assert lib.pic_mesh_build(C.byref(d), C.byref(ptr)) == -1
     # two overlapping objects
     d = deck.make_deck(deck.config("tiny"))
     d.n_objects = 2

@@ -1,0 +1,159 @@
+"""Axisymmetric (r-z, delta = 1) assembly of the mesh builder, checked on
+the CPU with a direct sparse solve: the dual volumes of the reference
+(SetupGrids_2D_QLL.f90:233-289) sum to the cylinder's volume, a
+manufactured solution of -(1/r) d/dr(r dphi/dr) - d2phi/dz2 = f converges
+at second order through the r-weighted stiffness and load matrices, and a
+dielectric slab across the whole radius gives the exact piecewise-linear
+potential through the r-weighted interface-element matrices."""
+import ctypes as C
+import math
+
+import numpy as np
+import scipy.sparse as sp
+import scipy.sparse.linalg as spl
+
+import oracle_bind as ob
+from pic_b200 import api
+
+
+class _AxiMesh:
+    """pic_mesh_build of an r-z box: z = x in [0, lz], r = y in [0, rr]."""
+
+    def __init__(self, nz, nr, lz, rr, walls, wall_phi=(0.0, 0.0, 0.0, 0.0), objects=()):
+        d = api.Deck()
+        d.nnx, d.nny = nz + 1, nr + 1
+        d.xmin, d.xmax, d.ymin, d.ymax = 0.0, lz, 0.0, rr
+        d.delta = 1
+        for k in range(4):
+            d.wall_dirichlet[k] = walls[k]
+            d.wall_phi[k] = wall_phi[k]
+        d.n_objects = len(objects)
+        for k, o in enumerate(objects):
+            d.objects[k] = o
+        self.lib = api.load()
+        self.ptr = C.POINTER(api.MeshDesc)()
+        api.check(self.lib.pic_mesh_build(C.byref(d), C.byref(self.ptr)), "pic_mesh_build")
+        self.d = self.ptr.contents
+        self.nnx, self.nny = d.nnx, d.nny
+        self.nn = d.nnx * d.nny
+        self.x = np.repeat(np.linspace(0.0, lz, d.nnx), d.nny)
+        self.y = np.tile(np.linspace(0.0, rr, d.nny), d.nnx)
+
+    def arr(self, name, n, dtype):
+        return api.as_np(getattr(self.d, name), n, dtype)
+
+    def solve(self, rho):
+        """phi on every node: A phi_u = b_u (b from the oracle's RHS), Dirichlet values kept."""
+        nu = self.d.n_unknowns
+        nt = self.arr("node_type", self.nn, np.int32)
+        srow = self.arr("a_srow", nu + 1, np.int32)
+        nnz = int(srow[-1] - 1)
+        A = sp.csr_matrix((self.arr("a_k", nnz, np.float64), self.arr("a_jcol", nnz, np.int32) - 1, srow - 1),
+                          shape=(nu, nu))
+        b = ob.rhs(self.ptr, np.ascontiguousarray(rho, dtype=np.float64), self.nn)
+        node_of = np.zeros(nu, np.int64)
+        node_of[nt[nt > 0] - 1] = np.nonzero(nt > 0)[0]
+        phi = self.arr("phi_dirichlet", self.nn, np.float64).copy()
+        phi[node_of] = spl.spsolve(A.tocsc(), b[node_of])
+        return phi
+
+    def close(self):
+        self.lib.pic_mesh_free(self.ptr)
+
+
+def test_dual_volumes_sum_to_the_cylinder():
+    lz, rr = 1.7, 0.9
+    m = _AxiMesh(24, 18, lz, rr, (1, 1, 0, 1))
+    try:
+        vol = m.arr("cell_volume", m.nn, np.float64)
+        assert abs(vol.sum() - math.pi * rr * rr * lz) <= 1e-12 * math.pi * rr * rr * lz
+        assert np.all(vol > 0)
+        assert m.d.mass_rows  # the per-row load matrices exist for delta = 1
+    finally:
+        m.close()
+
+
+def test_manufactured_solution_converges_at_second_order():
+    """Second order in the r-weighted L2 norm and in the maximum away from
+    the axis (the largest error sits on the axis, where the weight r
+    vanishes; it converges there too, at about 1.7)."""
+    lz, rr = 2.0, 1.0
+    a, b = math.pi / lz, math.pi / (2.0 * rr)
+    l2, far, axis = [], [], []
+    for n in (8, 16, 32):
+        m = _AxiMesh(2 * n, n, lz, rr, (1, 1, 0, 1))  # the axis r = 0 is a symmetry line
+        try:
+            z, r = m.x, m.y
+            exact = np.sin(a * z) * np.cos(b * r)
+            with np.errstate(invalid="ignore", divide="ignore"):
+                radial = np.where(r > 0, b * b * np.cos(b * r) + (b / r) * np.sin(b * r), 2.0 * b * b)
+            f = a * a * exact + np.sin(a * z) * radial
+            e = m.solve(f) - exact
+            vol = m.arr("cell_volume", m.nn, np.float64)
+            l2.append(math.sqrt((vol * e * e).sum() / vol.sum()))
+            far.append(np.abs(e[r > 0.25 * rr]).max())
+            axis.append(np.abs(e).max())
+        finally:
+            m.close()
+    rate = lambda v: [math.log2(v[k] / v[k + 1]) for k in range(len(v) - 1)]  # noqa: E731
+    print(f"\naxisymmetric manufactured solution: L2_r {l2} rates {rate(l2)}; max r>R/4 rates {rate(far)}; "
+          f"max rates {rate(axis)}")
+    assert min(rate(l2)) > 1.9 and min(rate(far)) > 1.9 and min(rate(axis)) > 1.5
+    assert l2[-1] < 1e-4
+
+
+def test_dielectric_slab_is_exact():
+    """A slab of eps = 3.9 across the whole radius between z0 and z1 (not on
+    grid lines), 0 V at z = 0 and 1 V at z = lz, natural conditions on the
+    axis and at r = rr: phi depends on z only and is piecewise linear with
+    eps * dphi/dz continuous, which the IFE space contains."""
+    lz, rr, eps, v = 1.0, 0.5, 3.9, 1.0
+    z0, z1 = 0.3137, 0.5071
+    slab = api.Object()
+    slab.shape, slab.conductor = api.PIC_SHAPE_BOX, 0
+    slab.cx, slab.cy, slab.a, slab.b = z0, -1.0, z1, rr + 1.0
+    slab.eps, slab.phi, slab.angle = eps, 0.0, 0.0
+    m = _AxiMesh(40, 16, lz, rr, (1, 1, 0, 0), (0.0, v, 0.0, 0.0), [slab])
+    try:
+        assert m.d.n_interface > 0
+        phi = m.solve(np.zeros(m.nn))
+        w = z1 - z0
+        e1 = v / (lz - w + w / eps)  # field outside the slab; inside e1 / eps
+        z = m.x
+        exact = np.where(z <= z0, e1 * z, np.where(z <= z1, e1 * z0 + e1 / eps * (z - z0),
+                                                    e1 * z0 + e1 / eps * w + e1 * (z - z1)))
+        err = np.abs(phi - exact).max()
+        print(f"\naxisymmetric dielectric slab: max |phi - exact| = {err:.2e}")
+        assert err <= 1e-10
+    finally:
+        m.close()
+
+
+def test_dielectric_rod_converges_to_the_cylindrical_solution():
+    """A rod of eps = 3.9 along the axis (r < r0, every z) in uniform charge
+    rho = 1, phi = 0 at r = rr, natural conditions elsewhere: phi depends on
+    r only, -(1/r)(r eps phi')' = 1, so phi = (rr^2 - r^2)/4 outside and
+    (rr^2 - r0^2)/4 + (r0^2 - r^2)/(4 eps) inside.  A Cartesian weighting
+    would converge to twice that; the r-weighted interface-element matrices
+    converge to it at second order."""
+    lz, rr, eps, r0 = 0.6, 1.0, 3.9, 0.4137
+    rod = api.Object()
+    rod.shape, rod.conductor = api.PIC_SHAPE_BOX, 0
+    rod.cx, rod.cy, rod.a, rod.b = -1.0, -1.0, lz + 1.0, r0
+    rod.eps, rod.phi, rod.angle = eps, 0.0, 0.0
+    l2 = []
+    for n in (8, 16, 32):
+        m = _AxiMesh(n, 2 * n, lz, rr, (0, 0, 0, 1), objects=[rod])
+        try:
+            assert m.d.n_interface > 0
+            phi = m.solve(np.ones(m.nn))
+            r = m.y
+            exact = np.where(r >= r0, (rr * rr - r * r) / 4.0, (rr * rr - r0 * r0) / 4.0 + (r0 * r0 - r * r) / (4.0 * eps))
+            vol = m.arr("cell_volume", m.nn, np.float64)
+            e = phi - exact
+            l2.append(math.sqrt((vol * e * e).sum() / vol.sum()))
+        finally:
+            m.close()
+    rates = [math.log2(l2[k] / l2[k + 1]) for k in range(2)]
+    print(f"\naxisymmetric dielectric rod: L2_r errors {l2}, rates {rates}")
+    assert min(rates) > 1.8 and l2[-1] < 1e-4
