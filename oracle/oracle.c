@@ -124,6 +124,24 @@ static void weights(const Mesh *m, int e, double x, double y, double W[4], int64
   nodes[0] = n1; nodes[1] = n1 + m->nny; nodes[2] = n1 + m->nny + 1; nodes[3] = n1 + 1;
 }
 
+/* axisymmetric (r = y) deposit weights, GetParChg_2D.f90:803-821: linear in
+ * r^2 across the element, the two lower nodes scaled by beta = 0.75 in the
+ * element row on the axis (R1 = dymin + y1 with dymin = ymin, as there). */
+static void weights_axi(const Mesh *m, int e, double x, double y, double W[4], int64_t nodes[4]) {
+  int i = e / m->ney, j = e % m->ney;
+  double x1 = m->xs[i], x2 = m->xs[i + 1], y1 = m->ys[j], y4 = m->ys[j + 1];
+  double dx = (x - x1) / (x2 - x1), xc = 1.0 - dx;
+  double beta = (fabs(y1 - m->d->ymin) < 1e-5) ? 0.75 : 1.0;
+  double R1 = m->d->ymin + y1, R2 = m->d->ymin + y4, R = y;
+  double den = R2 * R2 - R1 * R1;
+  W[0] = ((xc * (R2 * R2 - R * R)) / den) * beta;
+  W[1] = ((dx * (R2 * R2 - R * R)) / den) * beta;
+  W[2] = (dx * (R * R - R1 * R1)) / den;
+  W[3] = (xc * (R * R - R1 * R1)) / den;
+  int64_t n1 = (int64_t)i * m->nny + j;
+  nodes[0] = n1; nodes[1] = n1 + m->nny; nodes[2] = n1 + m->nny + 1; nodes[3] = n1 + 1;
+}
+
 static int in_object(const pic_object *o, double x, double y) {
   if (o->shape == PIC_SHAPE_CIRCLE) { /* MCCInterface.f90:493-497 */
     double dx = x - o->cx, dy = y - o->cy;
@@ -205,6 +223,76 @@ int64_t or_move_all(const pic_mesh_desc *d, int64_t n, double *x, double *y, dou
 }
 
 /* ------------------------------------------------------------------ */
+/* Axisymmetric MoveOne (IMPIC/MoveOne.f90:213-263, delta == 1, no B).   */
+/* x = z (axial), y = r; the velocity is held in the particle's own      */
+/* frame: vx = v_z, vy = v_r, vz = v_theta (the reference keeps the      */
+/* angle PO%Z and Cartesian transverse components instead; the two agree */
+/* in exact arithmetic, and this form needs no angle and no cos/sin).    */
+/* E_theta = 0: v_z += qm E_z dt, v_r += qm E_r dt; the transverse move  */
+/* X = r + dt v_r, Y = dt v_theta (X = 0 -> hy * 1e-5 as there), r' =    */
+/* |(X, Y)|, then (v_r, v_theta) rotated into the new frame by           */
+/* (X, Y)/r'.  Walls and objects as or_move_all.                          */
+/* ------------------------------------------------------------------ */
+int64_t or_move_all_axi(const pic_mesh_desc *d, int64_t n, double *x, double *y, double *vx, double *vy,
+                        double *vz, int32_t *loc, const double *efx, const double *efy, const double *coef,
+                        double qm, double dt, const int32_t wall[4]) {
+  Mesh m;
+  mesh_open(&m, d);
+  const int64_t nn = m.nn;
+  int64_t lost = 0;
+#pragma omp parallel for schedule(static) reduction(+ : lost)
+  for (int64_t p = 0; p < n; ++p) {
+    int e = loc[p];
+    if (e < 0) continue;
+    double W[4];
+    int64_t nd[4];
+    weights(&m, e, x[p], y[p], W, nd); /* the field gather is bilinear, as in Cartesian */
+    double Ez, Er;
+    if (d->element_index[e] > 0) {
+      double ex = 0.0, ey = 0.0;
+      int cnt = 0;
+      for (int c = 0; c < 4; ++c) {
+        int64_t q = nd[c];
+        if (d->node_index[q] == -1) {
+          ++cnt;
+          double xr = x[p] - m.xs[q / m.nny], yr = y[p] - m.ys[q % m.nny];
+          ex = ((ex + coef[0 * nn + q]) + (2.0 * coef[2 * nn + q]) * xr) + coef[3 * nn + q] * yr;
+          ey = ((ey + coef[1 * nn + q]) + (2.0 * coef[4 * nn + q]) * yr) + coef[3 * nn + q] * xr;
+        }
+      }
+      Ez = -(ex / (double)cnt);
+      Er = -(ey / (double)cnt);
+    } else {
+      Ez = ((W[0] * efx[nd[0]] + W[1] * efx[nd[1]]) + W[2] * efx[nd[2]]) + W[3] * efx[nd[3]];
+      Er = ((W[0] * efy[nd[0]] + W[1] * efy[nd[1]]) + W[2] * efy[nd[2]]) + W[3] * efy[nd[3]];
+    }
+    vx[p] = vx[p] + (qm * Ez) * dt;
+    vy[p] = vy[p] + (qm * Er) * dt;
+    double X = y[p] + dt * vy[p], Y = dt * vz[p];
+    if (X == 0.0) X = m.hy * (double)1.0e-5f;
+    double rn = sqrt(X * X + Y * Y), c = X / rn, s = Y / rn;
+    double vr = c * vy[p] + s * vz[p], vt = c * vz[p] - s * vy[p];
+    vy[p] = vr;
+    vz[p] = vt;
+    x[p] = x[p] + dt * vx[p];
+    y[p] = rn;
+    int dead = 0;
+    if (x[p] <= d->xmin) {
+      if (wall[0] == PIC_WALL_REFLECT) { x[p] = d->xmin + (d->xmin - x[p]); vx[p] = -vx[p]; } else dead = 1;
+    } else if (x[p] > d->xmax) {
+      if (wall[1] == PIC_WALL_REFLECT) { x[p] = d->xmax - (x[p] - d->xmax); vx[p] = -vx[p]; } else dead = 1;
+    } else if (y[p] > d->ymax) {
+      if (wall[3] == PIC_WALL_REFLECT) { y[p] = d->ymax - (y[p] - d->ymax); vy[p] = -vy[p]; } else dead = 1;
+    }
+    for (int k = 0; k < d->n_objects && !dead; ++k)
+      if (in_object(&d->objects[k], x[p], y[p])) dead = 1;
+    if (dead) { loc[p] = -1; ++lost; }
+  }
+  mesh_close(&m);
+  return lost;
+}
+
+/* ------------------------------------------------------------------ */
 /* GetParChg_2D.f90:122-911 for one species: locate (137-163), bilinear  */
 /* weights accumulated per node (788-866) as int64 fixed point with      */
 /* 2^-40 per unit weight and 2^-32 per unit weight*eV.                    */
@@ -224,7 +312,8 @@ int64_t or_deposit(const pic_mesh_desc *d, int64_t n, const double *x, const dou
     loc[p] = e;
     double W[4];
     int64_t nd[4];
-    weights(&m, e, x[p], y[p], W, nd);
+    if (d->delta == 1) weights_axi(&m, e, x[p], y[p], W, nd);
+    else weights(&m, e, x[p], y[p], W, nd);
     double energy = ((((0.5 * mass) * ((vx[p] * vx[p] + vy[p] * vy[p]) + vz[p] * vz[p])) * vref) * vref) / OR_JTOEV;
     for (int c = 0; c < 4; ++c) {
       const int64_t dq = llrint(W[c] * OR_QSCALE), de = llrint((W[c] * energy) * OR_ESCALE);

@@ -55,6 +55,9 @@ def load():
     lib.or_ife_closed_form.argtypes = [C.c_int, C.c_int, C.c_int, C.c_double, C.c_double,
                                        C.c_double, _d]
     lib.or_ek_tot.argtypes = [M, _l, C.c_double, C.c_double, C.c_double, _d]
+    lib.or_move_all_axi.argtypes = [M, C.c_int64, _d, _d, _d, _d, _d, _i, _d, _d, _d, C.c_double,
+                                    C.c_double, _i]
+    lib.or_move_all_axi.restype = C.c_int64
     lib.or_average_x.argtypes = [C.c_int, C.c_int, _d, C.c_double, _d]
     lib.or_energy_spectrum.argtypes = [C.c_int64, _d, _d, _d, _i, C.c_double, C.c_double, C.c_int,
                                        C.c_double, C.c_double, _l, _l]
@@ -99,6 +102,15 @@ def move_all(mesh_ptr, parts, efx, efy, coef, qm, dt, wall=(0, 0, 0, 0)):
     return load().or_move_all(mesh_ptr, parts["x"].size, d(parts["x"]), d(parts["y"]),
                               d(parts["vx"]), d(parts["vy"]), d(parts["vz"]), i32(parts["loc"]),
                               d(efx), d(efy), d(coef), qm, dt, w)
+
+
+def move_all_axi(mesh_ptr, parts, efx, efy, coef, qm, dt, wall=(0, 0, 0, 0)):
+    """Axisymmetric push: x = z, y = r, (vx, vy, vz) = (v_z, v_r, v_theta)
+    in the particle's frame (modified in place).  Returns the lost count."""
+    w = (C.c_int32 * 4)(*wall)
+    return load().or_move_all_axi(mesh_ptr, parts["x"].size, d(parts["x"]), d(parts["y"]),
+                                  d(parts["vx"]), d(parts["vy"]), d(parts["vz"]), i32(parts["loc"]),
+                                  d(efx), d(efy), d(coef), qm, dt, w)
 
 
 def deposit(mesh_ptr, parts, mass, vref, nn):

@@ -157,3 +157,90 @@ def test_dielectric_rod_converges_to_the_cylindrical_solution():
     rates = [math.log2(l2[k] / l2[k + 1]) for k in range(2)]
     print(f"\naxisymmetric dielectric rod: L2_r errors {l2}, rates {rates}")
     assert min(rates) > 1.8 and l2[-1] < 1e-4
+
+
+# ---- the oracle's axisymmetric push and deposit (MoveOne.f90:213-263,
+# GetParChg_2D.f90:803-821)
+
+def _axi_parts(m, n, seed=4, lz=2.0, rr=1.0, vscale=0.02):
+    """Particles well inside the domain (they stay inside over the tests' moves)."""
+    rng = np.random.default_rng(seed)
+    z = rng.uniform(0.3 * lz, 0.7 * lz, n)
+    r = rng.uniform(0.0, 0.6 * rr, n)
+    loc = np.array([ob.load().or_locate(m.ptr, a, b) for a, b in zip(z, r)], np.int32)
+    v = rng.standard_normal((3, n)) * vscale
+    return {"x": z, "y": r, "vx": v[0].copy(), "vy": v[1].copy(), "vz": v[2].copy(), "loc": loc}
+
+
+def test_axi_push_free_streaming_is_the_straight_line():
+    """No field: every step moves the particle on its 3D straight line; the
+    radius after k steps is |(r0 + t v_r0, t v_theta0)|, the speed and the
+    angular momentum r v_theta are conserved."""
+    lz, rr = 2.0, 1.0
+    m = _AxiMesh(32, 16, lz, rr, (1, 1, 0, 1))
+    try:
+        p = _axi_parts(m, 400)
+        p0 = {k: v.copy() for k, v in p.items()}
+        zeros = np.zeros(m.nn)
+        coef = np.zeros(5 * m.nn)
+        dt, steps = 0.37, 12
+        for _ in range(steps):
+            for k in range(len(p["loc"])):  # re-locate as the step does after the push
+                if p["loc"][k] >= 0:
+                    p["loc"][k] = ob.load().or_locate(m.ptr, p["x"][k], p["y"][k])
+            ob.move_all_axi(m.ptr, p, zeros, zeros, coef, -1.0, dt)
+        live = p["loc"] >= 0
+        assert live.all()
+        t = dt * steps
+        r_line = np.hypot(p0["y"] + t * p0["vy"], t * p0["vz"])
+        assert np.allclose(p["y"], r_line, rtol=1e-12, atol=1e-14)
+        assert np.allclose(p["x"], p0["x"] + t * p0["vx"], rtol=1e-13, atol=0)
+        speed0 = np.sqrt(p0["vx"] ** 2 + p0["vy"] ** 2 + p0["vz"] ** 2)
+        assert np.allclose(np.sqrt(p["vx"] ** 2 + p["vy"] ** 2 + p["vz"] ** 2), speed0, rtol=1e-13, atol=0)
+        assert np.allclose(p["y"] * p["vz"], p0["y"] * p0["vz"], rtol=1e-11, atol=1e-15)
+    finally:
+        m.close()
+
+
+def test_axi_push_axial_field():
+    lz, rr = 2.0, 1.0
+    m = _AxiMesh(32, 16, lz, rr, (1, 1, 0, 1))
+    try:
+        p = _axi_parts(m, 300)
+        p0 = {k: v.copy() for k, v in p.items()}
+        e0, qm, dt = 0.21, -1.0, 0.1
+        efx, efy = np.full(m.nn, e0), np.zeros(m.nn)
+        coef = np.zeros((5, m.nn))
+        coef[0] = -e0
+        ob.move_all_axi(m.ptr, p, efx, efy, np.ascontiguousarray(coef.ravel()), qm, dt)
+        want = p0["vx"] + qm * e0 * dt
+        assert np.allclose(p["vx"], want, rtol=0, atol=1e-15)
+        assert np.allclose(p["x"], p0["x"] + dt * p["vx"], rtol=0, atol=1e-15)
+    finally:
+        m.close()
+
+
+def test_axi_deposit_splits_a_uniform_ring_evenly():
+    """Particles on a node line in z and uniform in r^2 across one element
+    row (equal volume each) give its lower and upper nodes half the charge
+    each: the weights are linear in r^2 (the midpoint rule in r^2 is exact).
+    On the axis row the lower node keeps the reference's 0.75 of its half."""
+    lz, rr = 2.0, 1.0
+    m = _AxiMesh(8, 8, lz, rr, (1, 1, 0, 1))
+    try:
+        hy = rr / 8
+        npart = 1000
+        for j in (0, 3):
+            r1, r2 = j * hy, (j + 1) * hy
+            r = np.sqrt(r1 * r1 + (np.arange(npart) + 0.5) / npart * (r2 * r2 - r1 * r1))
+            z = np.full(npart, 4 * (lz / 8))  # node column i = 4
+            parts = {"x": z, "y": r, "vx": np.zeros(npart), "vy": np.zeros(npart), "vz": np.zeros(npart),
+                     "loc": np.zeros(npart, np.int32)}
+            q, _, bad = ob.deposit(m.ptr, parts, 9.1e-31, 1.0, m.nn)
+            assert bad == 0
+            lower, upper = q[4 * m.nny + j] / 2.0 ** 40, q[4 * m.nny + j + 1] / 2.0 ** 40
+            beta = 0.75 if j == 0 else 1.0
+            assert abs(lower - beta * npart / 2) <= 1e-9 * npart
+            assert abs(upper - npart / 2) <= 1e-9 * npart
+    finally:
+        m.close()
