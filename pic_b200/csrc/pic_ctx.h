@@ -109,6 +109,8 @@ struct Ctx {
   uint8_t *d_elem_near = nullptr;
   double *d_phi_dir = nullptr, *d_cell_volume = nullptr, *d_rhs_fix = nullptr;
   double *d_mass_q1 = nullptr, *d_ife_mass = nullptr;
+  double *d_mass_rows = nullptr;  // delta = 1 only
+  bool axi = false;               // delta = 1: r-z push and deposit
   int32_t *d_xt_ptr = nullptr, *d_xt_col = nullptr;  // per unknown row, 0-based node columns
   double *d_xt_val = nullptr;
   // PCG operator: row kind per node (-1 Dirichlet, 0..n_mat-1 stencil, >= n_mat explicit row)

@@ -250,8 +250,36 @@ __device__ __forceinline__ void warp_deposit(const SpK &s, int lane, int key, co
     for (int c = 0; c < 4; ++c) atomicAdd(s.e_acc + nodes[c], (unsigned long long)ev[c]);
 }
 
+// Axisymmetric deposit weights (delta = 1, r = y), GetParChg_2D.f90:803-821:
+// linear in r^2 across the element, the two lower nodes scaled by 0.75 in
+// the element row on the axis; R1 = ymin + y1 and R2 = ymin + y2 as there.
+__device__ __forceinline__ void weights_axi(const MeshK &m, int e, double x, double y, double W[4],
+                                            int nodes[4]) {
+  int i = elem_column(m, e), j = e - i * m.ney;
+  double x1 = m.xs[i], x2 = m.xs[i + 1], y1 = m.ys[j], y2 = m.ys[j + 1];
+  double dx = (x - x1) / (x2 - x1), xc = 1.0 - dx;
+  double beta = (fabs(y1 - m.ymin) < 1e-5) ? 0.75 : 1.0;
+  double R1 = m.ymin + y1, R2 = m.ymin + y2;
+  double den = R2 * R2 - R1 * R1;
+  W[0] = ((xc * (R2 * R2 - y * y)) / den) * beta;
+  W[1] = ((dx * (R2 * R2 - y * y)) / den) * beta;
+  W[2] = (dx * (y * y - R1 * R1)) / den;
+  W[3] = (xc * (y * y - R1 * R1)) / den;
+  int n1 = i * m.nny + j;
+  nodes[0] = n1;
+  nodes[1] = n1 + m.nny;
+  nodes[2] = n1 + m.nny + 1;
+  nodes[3] = n1 + 1;
+}
+
 // One particle per thread: gather E (old element), leapfrog push, wall/object
 // absorption, locate, fixed-point deposit of weight and weight*energy.
+// AXI (delta = 1, MoveOne.f90:213-263): x = z, y = r and the velocity held in
+// the particle's own frame (vx = v_z, vy = v_r, vz = v_theta); after the kick
+// the transverse move X = r + dt v_r, Y = dt v_theta gives r' = |(X, Y)| and
+// (v_r, v_theta) is rotated into the new frame by (X, Y)/r'; the deposit
+// weights are weights_axi.
+template <bool AXI>
 __global__ void __launch_bounds__(256, 4) k_push(MeshK m, FieldK f, PushK prm, SpK s) {
   int64_t p = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
   int lane = threadIdx.x & 31;
@@ -296,16 +324,29 @@ __global__ void __launch_bounds__(256, 4) k_push(MeshK m, FieldK f, PushK prm, S
         }
         vx = vx + (prm.qm * Ex) * prm.dt;
         vy = vy + (prm.qm * Ey) * prm.dt;
-        x = x + prm.dt * vx;
-        y = y + prm.dt * vy;
-        // walls: left, right, bottom, top
+        if (AXI) {
+          double vt = s.vz[p];
+          double X = y + prm.dt * vy, Y = prm.dt * vt;
+          if (X == 0.0) X = m.hy * (double)1.0e-5f;
+          const double rn = sqrt(X * X + Y * Y), c = X / rn, sn = Y / rn;
+          const double vr = c * vy + sn * vt;
+          vt = c * vt - sn * vy;
+          vy = vr;
+          s.vz[p] = vt;
+          x = x + prm.dt * vx;
+          y = rn;
+        } else {
+          x = x + prm.dt * vx;
+          y = y + prm.dt * vy;
+        }
+        // walls: left, right, bottom (not the axis), top
         if (x <= m.xmin) {
           if (prm.wall[0] == PIC_WALL_REFLECT) { x = m.xmin + (m.xmin - x); vx = -vx; }
           else lost = true;
         } else if (x > m.xmax) {
           if (prm.wall[1] == PIC_WALL_REFLECT) { x = m.xmax - (x - m.xmax); vx = -vx; }
           else lost = true;
-        } else if (y < m.ymin) {
+        } else if (!AXI && y < m.ymin) {
           if (prm.wall[2] == PIC_WALL_REFLECT) { y = m.ymin + (m.ymin - y); vy = -vy; }
           else lost = true;
         } else if (y > m.ymax) {
@@ -329,8 +370,12 @@ __global__ void __launch_bounds__(256, 4) k_push(MeshK m, FieldK f, PushK prm, S
         } else {
           s.loc[p] = en;
           key = en;
-          int ie, je;
-          bilinear(m, en, x, y, W, nodes, &ie, &je);
+          if (AXI) {
+            weights_axi(m, en, x, y, W, nodes);
+          } else {
+            int ie, je;
+            bilinear(m, en, x, y, W, nodes, &ie, &je);
+          }
           double vz = prm.do_energy ? s.vz[p] : 0.0;
           energy = ((((0.5 * prm.mass) * ((vx * vx + vy * vy) + vz * vz)) * prm.vref) * prm.vref) /
                    PIC_JTOEV;
@@ -669,6 +714,7 @@ __global__ void k_rho(RhoK r, const double *__restrict__ vol, double *__restrict
 
 struct RhsK {
   const double *rho, *mass_q1, *ife_mass, *rhs_fix, *phi_dir, *xt_val;
+  const double *mass_rows;  // delta = 1: [ney][16] r-weighted Q1 load matrix per element row, else null
   const int32_t *node_type, *element_index, *xt_ptr, *xt_col;
   double *b;
   int nnx, nny, ney;
@@ -693,7 +739,9 @@ __global__ void k_rhs(RhsK k) {
     if (ei < 0 || ej < 0 || ei >= k.nnx - 1 || ej >= k.nny - 1) continue;
     int e = ei * k.ney + ej;
     int id = k.element_index[e];
-    const double *M = (id > 0) ? (k.ife_mass + 16 * (size_t)(id - 1)) : k.mass_q1;
+    const double *M = (id > 0)       ? (k.ife_mass + 16 * (size_t)(id - 1))
+                      : k.mass_rows ? (k.mass_rows + 16 * (size_t)ej)
+                                    : k.mass_q1;
     int n1 = ei * k.nny + ej;
     double R0 = k.rho[n1], R1 = k.rho[n1 + k.nny], R2 = k.rho[n1 + k.nny + 1], R3 = k.rho[n1 + 1];
     const double *Mr = M + 4 * corner[t];
@@ -2103,7 +2151,7 @@ static void free_all() {
     if (p) cudaFree(p);
   };
   F(g.d_xs); F(g.d_ys); F(g.d_element_index); F(g.d_node_index); F(g.d_node_type); F(g.d_elem_near);
-  F(g.d_phi_dir); F(g.d_cell_volume); F(g.d_rhs_fix); F(g.d_mass_q1); F(g.d_ife_mass);
+  F(g.d_phi_dir); F(g.d_cell_volume); F(g.d_rhs_fix); F(g.d_mass_q1); F(g.d_ife_mass); F(g.d_mass_rows);
   F(g.d_xt_ptr); F(g.d_xt_col); F(g.d_xt_val); F(g.d_row_kind); F(g.d_ex_cnt); F(g.d_ex_col);
   F(g.d_ex_val); F(g.d_ex_val32); F(g.d_fcg32); F(g.d_diag); F(g.d_ppr_kind); F(g.d_ppr_ptr); F(g.d_ppr_nodes); F(g.d_ppr_rows);
   F(g.d_ppr_h); F(g.d_phi); F(g.d_rho); F(g.d_efx); F(g.d_efy); F(g.d_coef); F(g.d_coef32); F(g.d_b); F(g.d_x);
@@ -2195,7 +2243,10 @@ static int run_push(int sidx, bool do_push, bool do_deposit, bool do_energy) {
       k_push_mixed<<<blocks_for(s.n_slots, 256), 256, 0, g.st>>>(m, g.d_coef32, pm, k);
     }
   } else {
-    k_push<<<blocks_for(s.n_slots, 256), 256, 0, g.st>>>(mesh_k(), f, prm, k);
+    if (g.axi)
+      k_push<true><<<blocks_for(s.n_slots, 256), 256, 0, g.st>>>(mesh_k(), f, prm, k);
+    else
+      k_push<false><<<blocks_for(s.n_slots, 256), 256, 0, g.st>>>(mesh_k(), f, prm, k);
   }
   PIC_LAUNCHED();
   return PIC_OK;
@@ -2286,6 +2337,7 @@ static int run_rhs() {
   k.rho = g.d_rho;
   k.mass_q1 = g.d_mass_q1;
   k.ife_mass = g.d_ife_mass;
+  k.mass_rows = g.d_mass_rows;
   k.rhs_fix = g.d_rhs_fix;
   k.phi_dir = g.d_phi_dir;
   k.xt_val = g.d_xt_val;
@@ -3017,8 +3069,12 @@ int pic_init(const pic_mesh_desc *mesh, const pic_params *params) {
     set_error("pic_init: unknown precision");
     return PIC_ERR_ARG;
   }
-  if (mesh->delta != 0) {
-    set_error("pic_init: axisymmetric meshes (delta=1) are not supported by this build");
+  if (mesh->delta != 0 && mesh->delta != 1) {
+    set_error("pic_init: delta must be 0 (Cartesian) or 1 (axisymmetric)");
+    return PIC_ERR_ARG;
+  }
+  if (mesh->delta == 1 && (P.precision != PIC_PREC_FP64 || !mesh->mass_rows || mesh->ymin != 0.0)) {
+    set_error("pic_init: axisymmetric meshes need FP64 precision, the per-row load matrices and the axis at ymin = 0");
     return PIC_ERR_ARG;
   }
   if ((int64_t)mesh->nnx * mesh->nny > (int64_t)1 << 30) {
@@ -3027,6 +3083,7 @@ int pic_init(const pic_mesh_desc *mesh, const pic_params *params) {
   }
   g = Ctx();
   g.P = P;
+  g.axi = (mesh->delta == 1);
   g.solver = (P.solver == PIC_SOLVER_FCG_UNET) ? PIC_SOLVER_FCG_UNET : PIC_SOLVER_JPCG;
   if (g.P.sort_interval < 1) g.P.sort_interval = 1;
   MeshK &m = g.m;
@@ -3094,6 +3151,7 @@ int pic_init(const pic_mesh_desc *mesh, const pic_params *params) {
   if ((rc = upload(&g.d_rhs_fix, rhs_fix.data(), rhs_fix.size()))) return rc;
   if ((rc = upload(&g.d_mass_q1, mesh->mass_q1, 16))) return rc;
   if ((rc = upload(&g.d_ife_mass, mesh->ife_mass, 16 * (size_t)mesh->n_interface))) return rc;
+  if (g.axi && (rc = upload(&g.d_mass_rows, mesh->mass_rows, 16 * (size_t)m.ney))) return rc;
   ObjK ob;
   std::memset(&ob, 0, sizeof ob);
   ob.n = mesh->n_objects;
@@ -3670,8 +3728,8 @@ int pic_move_all(int32_t species, int32_t push_flag) {
 int pic_get_par_chg(int32_t delta, double *rho_out) {
   int rc;
   if ((rc = check_init())) return rc;
-  if (delta != 0) {
-    set_error("pic_get_par_chg: only delta = 0 is supported");
+  if (delta != (g.axi ? 1 : 0)) {
+    set_error("pic_get_par_chg: delta differs from the mesh's");
     return PIC_ERR_ARG;
   }
   if ((rc = zero_deposit(true))) return rc;

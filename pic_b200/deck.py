@@ -74,6 +74,8 @@ class Config:
     mcc: bool = True
     precision: int = api.PIC_PREC_FP64
     sort_interval: int = 10
+    # 0: Cartesian x-y; 1: axisymmetric, x = z and y = r with the axis at y = 0
+    delta: int = 0
     # per-node energy deposit (a diagnostic) only on output steps; the
     # reference writes its profiles every 1000 steps (Main_IFE_Test_2.f90:466-470)
     diag_interval: int = 1000
@@ -146,6 +148,14 @@ def config(name: str, **over) -> Config:
                    objects=[ObjectSpec(api.PIC_SHAPE_CIRCLE, 0.005, 0.0051, 0.0023, eps=4.0)],
                    wall_V=(5.0, 0.0, 0.0, 0.0), n0=1e15, ppc=8, Te_eV=2.0, nt=10,
                    pcg_tol=1e-10, seed=3)
+    elif name == "tiny_axi":
+        # r-z cylinder (z = x, r = y, axis at the bottom: a symmetry line, not
+        # a wall) holding a dielectric torus; Dirichlet on the ends and the
+        # outer radius
+        c = Config("tiny-axi-16x16-torus", 0.01, 0.01, 16, 16,
+                   objects=[ObjectSpec(api.PIC_SHAPE_CIRCLE, 0.005, 0.0055, 0.0023, eps=4.0)],
+                   wall_dirichlet=(1, 1, 0, 1), wall_V=(5.0, 0.0, 0.0, 0.0), n0=1e15, ppc=8,
+                   Te_eV=2.0, nt=10, pcg_tol=1e-10, seed=5, delta=1)
     else:
         raise KeyError(name)
     for k, v in over.items():
@@ -159,7 +169,7 @@ def make_deck(cfg: Config) -> api.Deck:
     d = api.Deck()
     d.nnx, d.nny = cfg.ncx + 1, cfg.ncy + 1
     d.xmin, d.xmax, d.ymin, d.ymax = 0.0, cfg.Lx / L, 0.0, cfg.Ly / L
-    d.delta = 0
+    d.delta = cfg.delta
     for k in range(4):
         d.wall_dirichlet[k] = int(cfg.wall_dirichlet[k])
         d.wall_phi[k] = cfg.wall_V[k] / P

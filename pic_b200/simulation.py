@@ -101,7 +101,7 @@ class Simulation:
         api.check(self.lib.pic_move_all(s, 0), "pic_move_all")
 
     def get_par_chg(self, rho_out: np.ndarray | None = None):
-        api.check(self.lib.pic_get_par_chg(0, api.dptr(rho_out)), "pic_get_par_chg")
+        api.check(self.lib.pic_get_par_chg(self.cfg.delta, api.dptr(rho_out)), "pic_get_par_chg")
 
     def ife_solve(self, phi: np.ndarray | None = None) -> api.SolveStats:
         st = api.SolveStats()

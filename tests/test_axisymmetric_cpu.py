@@ -244,3 +244,24 @@ def test_axi_deposit_splits_a_uniform_ring_evenly():
             assert abs(upper - npart / 2) <= 1e-9 * npart
     finally:
         m.close()
+
+
+def test_pic_init_refuses_axisymmetric_mixed_precision():
+    """The axisymmetric push and deposit exist in FP64 only: pic_init turns
+    down delta = 1 with PIC_PREC_MIXED before it touches the device."""
+    from pic_b200 import deck
+    cfg = deck.config("tiny_axi", precision=api.PIC_PREC_MIXED)
+    mesh = deck.Mesh(cfg)
+    try:
+        p = api.Params()
+        p.n_species = 1
+        p.species[0].charge, p.species[0].mass, p.species[0].weight = -1.0, deck.ME, 1.0
+        p.species[0].capacity = 1024
+        p.dt, p.n_ref, p.T_ref_eV = cfg.dt, cfg.n0, cfg.Te_eV
+        p.pcg_tol, p.pcg_maxit = cfg.pcg_tol, cfg.pcg_maxit
+        p.precision = api.PIC_PREC_MIXED
+        lib = api.load()
+        assert lib.pic_init(mesh.ptr, C.byref(p)) == api.PIC_ERR_ARG
+        assert b"axisymmetric" in lib.pic_last_error()
+    finally:
+        mesh.close()

@@ -281,7 +281,8 @@ def _oracle_step(sim, parts, phi, step):
     for s in range(2):
         p = parts[s]
         qm = sim.species[s][0] / (sim.species[s][1] / deck.ME)
-        ob.move_all(m.ptr, p, efx, efy, coef, qm, sim.cfg.dt)
+        mover = ob.move_all_axi if sim.cfg.delta == 1 else ob.move_all
+        mover(m.ptr, p, efx, efy, coef, qm, sim.cfg.dt)
         q, e, bad = ob.deposit(m.ptr, p, sim.species[s][1], sim.scales["v_ref"], nn)
         qs.append(q)
         es.append(e)
@@ -318,8 +319,9 @@ def _oracle_step(sim, parts, phi, step):
     return phi, st, rho
 
 
-def test_full_steps_match_oracle():
-    sim = _sim("tiny", gas_p_Pa=300.0, Te_eV=20.0, sort_interval=3, diag_interval=4)
+@pytest.mark.parametrize("name", ["tiny", "tiny_axi"])
+def test_full_steps_match_oracle(name):
+    sim = _sim(name, gas_p_Pa=300.0, Te_eV=20.0, sort_interval=3, diag_interval=4)
     try:
         st0 = sim.initial_fields()
         parts = {}
