@@ -77,9 +77,9 @@ typedef struct pic_object {
 typedef struct pic_deck {
   int32_t nnx, nny;            /* nodes per direction                        */
   double xmin, xmax, ymin, ymax;
-  int32_t delta;               /* 0 Cartesian; 1 axisymmetric r-z (r = y, the
-                                  axis at y = ymin = 0): pic_mesh_build only,
-                                  pic_init refuses it                         */
+  int32_t delta;               /* 0 Cartesian; 1 axisymmetric r-z (x = z,
+                                  y = r, the axis at y = ymin = 0); pic_init
+                                  takes delta 1 with PIC_PREC_FP64 only       */
   int32_t wall_dirichlet[4];   /* left, right, bottom, top: 1 Dirichlet       */
   double wall_phi[4];          /* Dirichlet values                            */
   int32_t n_objects;
@@ -259,12 +259,15 @@ int pic_sort_particles(int32_t species);
 
 /* MoveAll (MCCInterface.f90:574-640) -> MoveOne (IMPIC/MoveOne.f90) with
  * Get_ParticleEField_PPR (PPR/Get_ParticleEField_PPR.f90) and
- * AdjustParticleBoundary (MCCInterface.f90:217-534).  push_flag as MoveAll. */
+ * AdjustParticleBoundary (MCCInterface.f90:217-534).  push_flag as MoveAll.
+ * On an axisymmetric mesh (vx, vy, vz) = (v_z, v_r, v_theta) in the
+ * particle's own frame (MoveOne.f90:213-263 without the stored angle). */
 int pic_move_all(int32_t species, int32_t push_flag);
 
 /* GetParChg_2D (PIC/GetParChg_2D.f90:1-911): locate, int64 fixed-point
- * bilinear deposit, normalisation by the dual volume.  rho_out (host,
- * [nodes]) may be NULL. */
+ * bilinear deposit (r-weighted for delta 1, GetParChg_2D.f90:803-821),
+ * normalisation by the dual volume.  delta must be the mesh's.  rho_out
+ * (host, [nodes]) may be NULL. */
 int pic_get_par_chg(int32_t delta, double *rho_out);
 
 /* IFE_Solve_2D (IFE-Rectangular/IFE_Solve_2D.f90:1-260) -> MY_JPCG_Solver ->
