@@ -36,7 +36,7 @@ extern long long g_launches;
 struct MeshK {
   int nnx, nny, nex, ney;
   double xmin, xmax, ymin, ymax, hx, hy;
-  double inv_ney;                 // 1/ney for the element -> column split
+  uint32_t ney_magic;             // floor(2^32 / ney) + 1, for the element -> column split
   const double *xs, *ys;          // node coordinates (x_s + h_x*(i))
   const int32_t *element_index;   // [ne]
   const int32_t *node_index;      // [nn]

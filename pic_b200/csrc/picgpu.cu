@@ -61,12 +61,12 @@ __device__ __forceinline__ int locate_elem(const MeshK &m, double x, double y) {
   return (i - 1) * m.ney + (j - 1);
 }
 
-// e / ney without an integer division: a double-reciprocal estimate and an
-// exact integer correction.
+// e / ney without a division: with M = floor(2^32 / ney) + 1, umulhi(e, M)
+// exceeds e / ney by less than e / 2^32 < 1, so it is the quotient or one
+// more, and one correction makes it exact for every element id (ney >= 2).
 __device__ __forceinline__ int elem_column(const MeshK &m, int e) {
-  int i = (int)((double)e * m.inv_ney);
+  int i = (int)__umulhi((unsigned)e, m.ney_magic);
   if (i * m.ney > e) --i;
-  if ((i + 1) * m.ney <= e) ++i;
   return i;
 }
 
@@ -573,22 +573,37 @@ __device__ __forceinline__ void cp_async_wait() {
   asm volatile("cp.async.wait_group %0;\n" ::"n"(N) : "memory");
 }
 
-// the tile starting at particle `base`: 5 arrays x 64 chunks of 16 B; chunks
-// past the end read only their valid bytes (zero fill), none when empty
-__device__ __forceinline__ void push_tile_load(PushTile *T, const SpK &s, int64_t base) {
-  for (int c = threadIdx.x; c < 5 * (kPushTile / 4); c += blockDim.x) {
-    const int a = c / (kPushTile / 4), q = c % (kPushTile / 4);
-    const int64_t first = base + 4 * q;
-    const int valid = (int)max((int64_t)0, min((int64_t)4, s.n - first));
-    const void *arr = a == 0 ? (const void *)s.loc
-                      : a == 1 ? (const void *)s.x
-                      : a == 2 ? (const void *)s.y
-                      : a == 3 ? (const void *)s.vx
-                               : (const void *)s.vy;
-    const char *src = reinterpret_cast<const char *>(arr) + (valid > 0 ? 4 * first : 0);
-    char *dst = reinterpret_cast<char *>(T) + (size_t)a * 4 * kPushTile + 16 * q;
-    cp_async16(dst, src, 4 * valid);
-  }
+// One thread's share of a tile's copy (blockDim.x == kPushTile): the tile
+// is 5 arrays x 64 chunks of 16 B; thread t copies chunk t & 63 of array
+// t >> 6, and threads below 64 also that chunk of the fifth array (vy).
+struct TileCopy {
+  const char *src0, *src1;
+  int dst0, dst1, q;
+};
+
+__device__ __forceinline__ TileCopy tile_copy_of(const SpK &s) {
+  TileCopy c;
+  const int a = threadIdx.x >> 6;
+  c.q = threadIdx.x & 63;
+  c.src0 = reinterpret_cast<const char *>(a == 0 ? (const void *)s.loc
+                                          : a == 1 ? (const void *)s.x
+                                          : a == 2 ? (const void *)s.y
+                                                   : (const void *)s.vx);
+  c.src1 = reinterpret_cast<const char *>(s.vy);
+  c.dst0 = a * 4 * kPushTile + 16 * c.q;
+  c.dst1 = 4 * 4 * kPushTile + 16 * c.q;
+  return c;
+}
+
+// the tile starting at particle `base`; chunks past the end read only their
+// valid bytes (zero fill), none when empty
+__device__ __forceinline__ void push_tile_load(PushTile *T, const TileCopy &c, int64_t n, int64_t base) {
+  const int64_t first = base + 4 * c.q;
+  const int valid = (int)max((int64_t)0, min((int64_t)4, n - first));
+  const int64_t off = valid > 0 ? 4 * first : 0;
+  char *t = reinterpret_cast<char *>(T);
+  cp_async16(t + c.dst0, c.src0 + off, 4 * valid);
+  if (threadIdx.x < 64) cp_async16(t + c.dst1, c.src1 + off, 4 * valid);
 }
 
 template <int S, int MINB = 4>
@@ -598,16 +613,17 @@ __global__ void __launch_bounds__(256, MINB) k_push_mixed_tiled(MeshK m, const f
   PushTile *T = reinterpret_cast<PushTile *>(push_smem);
   const int lane = threadIdx.x & 31;
   const int64_t G = gridDim.x;
+  const TileCopy cp = tile_copy_of(s);
 #pragma unroll
   for (int k = 0; k < S - 1; ++k) {
     const int64_t t = blockIdx.x + k * G;
-    if (t < ntiles) push_tile_load(&T[k], s, t * kPushTile);
+    if (t < ntiles) push_tile_load(&T[k], cp, s.n, t * kPushTile);
     cp_async_commit();
   }
   int it = 0;
   for (int64_t t = blockIdx.x; t < ntiles; t += G, ++it) {
     const int64_t tn = t + (S - 1) * G;
-    if (tn < ntiles) push_tile_load(&T[(it + S - 1) % S], s, tn * kPushTile);
+    if (tn < ntiles) push_tile_load(&T[(it + S - 1) % S], cp, s.n, tn * kPushTile);
     cp_async_commit();
     cp_async_wait<S - 1>();  // this thread's copies of tile t are complete
     __syncthreads();         // and every thread's
@@ -3097,7 +3113,7 @@ int pic_init(const pic_mesh_desc *mesh, const pic_params *params) {
   m.ymax = mesh->ymax;
   m.hx = (m.xmax - m.xmin) / (m.nnx - 1);
   m.hy = (m.ymax - m.ymin) / (m.nny - 1);
-  m.inv_ney = 1.0 / m.ney;
+  m.ney_magic = (uint32_t)((1ull << 32) / (unsigned)m.ney + 1ull);
   g.nn = (int64_t)m.nnx * m.nny;
   g.ne = (int64_t)m.nex * m.ney;
   const int64_t nn = g.nn, ne = g.ne;
