@@ -338,7 +338,10 @@ void or_normalize(const pic_mesh_desc *d, int ns, const int64_t *const *q_acc, c
     for (int s = 0; s < ns; ++s) {
       double cnt = (double)q_acc[s][i] * (1.0 / OR_QSCALE);
       double es = (double)e_acc[s][i] * (1.0 / OR_ESCALE);
-      double r = ((((wq[s] * cnt) / L_ref) / L_ref) / n_ref) / V;
+      /* one more 1/L_ref for delta 1 (:900-904): the dual volume is a volume */
+      double t = ((wq[s] * cnt) / L_ref) / L_ref;
+      if (d->delta == 1) t = t / L_ref;
+      double r = (t / n_ref) / V;
       rho_s[s][i] = r;
       ek_s[s][i] = (cnt != 0.0) ? es / cnt : 0.0;
       acc = acc + r;
@@ -870,7 +873,9 @@ void or_ek_tot(const pic_mesh_desc *d, const int64_t *e_acc, double weight, doub
   int64_t nn = (int64_t)d->nnx * d->nny;
   for (int64_t i = 0; i < nn; ++i) {
     double es = (double)e_acc[i] * (1.0 / OR_ESCALE);
-    ek_tot[i] = ((((weight * es) / L_ref) / L_ref) / n_ref) / d->cell_volume[i];
+    double t = ((weight * es) / L_ref) / L_ref;
+    if (d->delta == 1) t = t / L_ref;
+    ek_tot[i] = (t / n_ref) / d->cell_volume[i];
   }
 }
 

@@ -704,6 +704,7 @@ struct RhoK {
   int ns;
   double L_ref, n_ref;
   int energy;  // update the per-node mean energy (diagnostic steps)
+  int axi;     // delta = 1
 };
 
 // GetParChg_2D.f90:869-911: rho_s = Weight*qs*sum/L_ref/L_ref/n_ref/V; on
@@ -717,11 +718,17 @@ __global__ void k_rho(RhoK r, const double *__restrict__ vol, double *__restrict
   for (int s = 0; s < r.ns; ++s) {
     double cnt = (double)(long long)r.q[s][n] * (1.0 / PIC_Q_SCALE);
     double esum = (double)(long long)r.e[s][n] * (1.0 / PIC_E_SCALE);
-    double rs = ((((r.wq[s] * cnt) / r.L_ref) / r.L_ref) / r.n_ref) / V;
+    // one more 1/L_ref for delta = 1 (GetParChg_2D.f90:900-904): the dual
+    // volume is then a volume, not an area
+    double t = ((r.wq[s] * cnt) / r.L_ref) / r.L_ref;
+    if (r.axi) t = t / r.L_ref;
+    double rs = (t / r.n_ref) / V;
     r.rho_s[s][n] = rs;
     if (r.energy) {
       r.ek_s[s][n] = (cnt != 0.0) ? esum / cnt : 0.0;
-      r.ek_tot[s][n] = ((((r.w[s] * esum) / r.L_ref) / r.L_ref) / r.n_ref) / V;
+      double te = ((r.w[s] * esum) / r.L_ref) / r.L_ref;
+      if (r.axi) te = te / r.L_ref;
+      r.ek_tot[s][n] = (te / r.n_ref) / V;
     }
     acc = acc + rs;
   }
@@ -2308,6 +2315,7 @@ static int run_rho(bool energy) {
   r.energy = energy;
   r.L_ref = g.L_ref;
   r.n_ref = g.P.n_ref;
+  r.axi = g.axi;
   for (int s = 0; s < g.ns; ++s) {
     r.q[s] = g.sp[s].q_acc;
     r.e[s] = g.sp[s].e_acc;

@@ -265,3 +265,32 @@ def test_pic_init_refuses_axisymmetric_mixed_precision():
         assert b"axisymmetric" in lib.pic_last_error()
     finally:
         mesh.close()
+
+
+def test_uniform_plasma_deposits_the_density():
+    """Particles uniform in volume with weight n0 V / N deposit rho = n0
+    (normalised: 1) at every node off the axis, through the r^2-linear
+    weights, the L_ref^3 normalisation (GetParChg_2D.f90:900-904) and the
+    axisymmetric dual volumes; the axis row reads 1.5 n0, the reference's
+    axis factor beta = 0.75 applied to weights whose integral over the first
+    ring is twice the axis node's dual volume."""
+    lz, rr, L_ref, n0 = 2.0, 1.5, 1e-3, 1e15
+    m = _AxiMesh(16, 12, lz, rr, (1, 1, 0, 1))
+    try:
+        rng = np.random.default_rng(17)
+        N = 4_000_000
+        z = rng.random(N) * lz
+        r = rr * np.sqrt(rng.random(N))
+        zero = np.zeros(N)
+        parts = {"x": z, "y": r, "vx": zero, "vy": zero, "vz": zero, "loc": np.zeros(N, np.int32)}
+        q, e, bad = ob.deposit(m.ptr, parts, 1.0, 1.0, m.nn)
+        assert bad == 0
+        weight = n0 * math.pi * (rr * L_ref) ** 2 * (lz * L_ref) / N
+        _, rs, _ = ob.normalize(m.ptr, [q], [e], [weight], L_ref, n0, m.nn)
+        rho = rs[0].reshape(m.nnx, m.nny)
+        inner = rho[1:-1, 1:-1]
+        assert abs(inner.mean() - 1.0) < 5e-3
+        assert np.abs(inner - 1.0).max() < 0.1
+        assert abs(rho[1:-1, 0].mean() - 1.5) < 0.06
+    finally:
+        m.close()
