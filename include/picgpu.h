@@ -270,6 +270,17 @@ int pic_move_all(int32_t species, int32_t push_flag);
  * (host, [nodes]) may be NULL. */
 int pic_get_par_chg(int32_t delta, double *rho_out);
 
+/* Time-dependent potential on the Dirichlet wall x = xmin (wall 0) or
+ * x = xmax (wall 1): at every solve its nodes (corners included, as the mesh
+ * builder assigns them; conductor-object nodes excluded) take their static
+ * value + amplitude * sin(2 pi frequency_hz * time * t_ref + phase), time
+ * being pic_ife_solve's argument or step * dt in pic_step.  amplitude in
+ * Phi_ref units; 0 switches it off and restores the static values.  The
+ * reference's bc_value(1) = V/Phi_ref*SIN(2*Pi*Frequency*time*time_ref) on
+ * the left boundary (IFE_Solve_2D.f90:104-121, commented out there).
+ * PIC_ERR_ARG for another wall or one that is not Dirichlet. */
+int pic_set_wall_rf(int32_t wall, double amplitude, double frequency_hz, double phase);
+
 /* IFE_Solve_2D (IFE-Rectangular/IFE_Solve_2D.f90:1-260) -> MY_JPCG_Solver ->
  * MY_PCG (IFE-Solver/MY_PCG.f90).  phi_inout (host, [nodes]) may be NULL:
  * then the device phi is the warm start and stays on the device. */

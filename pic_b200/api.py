@@ -41,7 +41,7 @@ EXPORTS = [
     "pic_cuda_stream", "pic_apply_operator", "pic_solver_vectors", "pic_set_precond_stages",
     "pic_coarse_setup", "pic_precond_apply", "pic_set_fcg_inner", "pic_average_x",
     "pic_energy_spectrum", "pic_velocity_moments", "pic_multigrid_setup", "pic_get_next_id",
-    "pic_set_next_id",
+    "pic_set_next_id", "pic_set_wall_rf",
 ]
 
 # z = M(r) callback of flexible CG: (r_dev, z_dev, user) -> 0 or failure
@@ -189,6 +189,7 @@ def load() -> C.CDLL:
     lib.pic_multigrid_setup.argtypes = [_P(MeshDesc), C.c_int32]
     lib.pic_get_next_id.argtypes = [C.c_int32, _P(C.c_uint32)]
     lib.pic_set_next_id.argtypes = [C.c_int32, C.c_uint32]
+    lib.pic_set_wall_rf.argtypes = [C.c_int32, C.c_double, C.c_double, C.c_double]
     lib.pic_precond_apply.argtypes = [C.c_int32, C.c_void_p, C.c_void_p]
     lib.pic_deposit_noalloc.argtypes = [C.c_int32, C.c_int32, C.c_double, C.c_double, C.c_double,
                                         C.c_double, C.c_int64, C.c_void_p, C.c_void_p, C.c_void_p,

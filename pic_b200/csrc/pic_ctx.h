@@ -208,6 +208,17 @@ struct Ctx {
   double *d_mcc_vel = nullptr;
   int64_t mcc_new_cap = 0;
   int64_t step_count = 0;
+  // time-dependent wall potential (pic_set_wall_rf): the Dirichlet nodes of
+  // the lines x = xmin (0) and x = xmax (1) other than conductor nodes, their
+  // static values, and whether every node of the line is Dirichlet
+  std::vector<int32_t> rf_line[2];
+  std::vector<double> rf_base[2];
+  bool rf_ok[2] = {false, false};
+  int rf_wall = -1;  // -1: off
+  int rf_count = 0;
+  double rf_amp = 0.0, rf_omega = 0.0, rf_phase = 0.0;  // omega: radians per normalised time
+  int32_t *d_rf_nodes = nullptr;
+  double *d_rf_base = nullptr;
 };
 
 extern Ctx g;

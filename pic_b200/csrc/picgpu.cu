@@ -2175,6 +2175,7 @@ static void free_all() {
   };
   F(g.d_xs); F(g.d_ys); F(g.d_element_index); F(g.d_node_index); F(g.d_node_type); F(g.d_elem_near);
   F(g.d_phi_dir); F(g.d_cell_volume); F(g.d_rhs_fix); F(g.d_mass_q1); F(g.d_ife_mass); F(g.d_mass_rows);
+  F(g.d_rf_nodes); F(g.d_rf_base);
   F(g.d_xt_ptr); F(g.d_xt_col); F(g.d_xt_val); F(g.d_row_kind); F(g.d_ex_cnt); F(g.d_ex_col);
   F(g.d_ex_val); F(g.d_ex_val32); F(g.d_fcg32); F(g.d_diag); F(g.d_ppr_kind); F(g.d_ppr_ptr); F(g.d_ppr_nodes); F(g.d_ppr_rows);
   F(g.d_ppr_h); F(g.d_phi); F(g.d_rho); F(g.d_efx); F(g.d_efy); F(g.d_coef); F(g.d_coef32); F(g.d_b); F(g.d_x);
@@ -2354,6 +2355,30 @@ static PcgK pcg_k(int parity) {
   k.nn = g.nn;
   k.nb = g.red_blocks;
   return k;
+}
+
+// Time-dependent wall potential: phi_D = base + value on the wall's nodes,
+// written into the Dirichlet table the RHS reads and into phi.
+__global__ void k_rf_set(const int32_t *__restrict__ nodes, const double *__restrict__ base, int count,
+                         double value, double *__restrict__ phi_dir, double *__restrict__ phi) {
+  const int k = blockIdx.x * blockDim.x + threadIdx.x;
+  if (k >= count) return;
+  const int32_t n = nodes[k];
+  const double v = base[k] + value;
+  phi_dir[n] = v;
+  phi[n] = v;
+}
+
+// IFE_Solve_2D.f90:104-121: bc_value(1) = V/Phi_ref*SIN(2*Pi*Frequency*time*time_ref)
+// on the left Dirichlet boundary (there a commented-out line; here a switch,
+// for either x wall): amplitude * sin(omega * time + phase).
+static int rf_apply(double time) {
+  if (g.rf_wall < 0 || g.rf_count == 0) return PIC_OK;
+  const double value = g.rf_amp * std::sin(g.rf_omega * time + g.rf_phase);
+  k_rf_set<<<(g.rf_count + 127) / 128, 128, 0, g.st>>>(g.d_rf_nodes, g.d_rf_base, g.rf_count, value, g.d_phi_dir,
+                                                      g.d_phi);
+  PIC_LAUNCHED();
+  return PIC_OK;
 }
 
 static int run_rhs() {
@@ -3168,6 +3193,21 @@ int pic_init(const pic_mesh_desc *mesh, const pic_params *params) {
   if ((rc = upload(&g.d_node_index, mesh->node_index, nn))) return rc;
   if ((rc = upload(&g.d_node_type, mesh->node_type, nn))) return rc;
   if ((rc = upload(&g.d_phi_dir, mesh->phi_dirichlet, nn))) return rc;
+  for (int w = 0; w < 2; ++w) {
+    const int64_t i = (w == 0) ? 0 : m.nnx - 1;
+    g.rf_ok[w] = true;
+    for (int j = 0; j < m.nny; ++j) {
+      const int64_t n = i * m.nny + j;
+      if (mesh->node_type[n] > 0) {
+        g.rf_ok[w] = false;
+        continue;
+      }
+      const int reg = mesh->node_index[n];
+      if (reg <= -2 && reg >= -(mesh->n_objects + 1) && mesh->objects[-reg - 2].conductor) continue;
+      g.rf_line[w].push_back((int32_t)n);
+      g.rf_base[w].push_back(mesh->phi_dirichlet[n]);
+    }
+  }
   if ((rc = upload(&g.d_cell_volume, mesh->cell_volume, nn))) return rc;
   const int nu = mesh->n_unknowns;
   std::vector<double> rhs_fix(nu, 0.0);
@@ -3780,10 +3820,10 @@ int pic_get_par_chg(int32_t delta, double *rho_out) {
 int pic_ife_solve(double *phi_inout, double time, pic_solve_stats *stats) {
   int rc;
   if ((rc = check_init())) return rc;
-  (void)time;
   if (phi_inout)
     PIC_CUDA(cudaMemcpyAsync(g.d_phi, phi_inout, g.nn * sizeof(double), cudaMemcpyHostToDevice, g.st));
   PIC_CUDA(cudaEventRecord(g.ev0, g.st));
+  if ((rc = rf_apply(time))) return rc;
   if ((rc = run_rhs())) return rc;
   int src = run_solve(stats);
   PIC_CUDA(cudaEventRecord(g.ev1, g.st));
@@ -3796,6 +3836,42 @@ int pic_ife_solve(double *phi_inout, double time, pic_solve_stats *stats) {
     stats->ms = ms;
   }
   return src;
+}
+
+int pic_set_wall_rf(int32_t wall, double amplitude, double frequency_hz, double phase) {
+  int rc;
+  if ((rc = check_init())) return rc;
+  if (wall < 0 || wall > 1 || !std::isfinite(amplitude) || !std::isfinite(frequency_hz) || !std::isfinite(phase)) {
+    set_error("pic_set_wall_rf: wall must be 0 (x = xmin) or 1 (x = xmax), values finite");
+    return PIC_ERR_ARG;
+  }
+  if (amplitude != 0.0 && !g.rf_ok[wall]) {
+    set_error("pic_set_wall_rf: the wall is not a Dirichlet wall");
+    return PIC_ERR_ARG;
+  }
+  // the previous wall back to its static values
+  if (g.rf_wall >= 0 && g.rf_count > 0) {
+    k_rf_set<<<(g.rf_count + 127) / 128, 128, 0, g.st>>>(g.d_rf_nodes, g.d_rf_base, g.rf_count, 0.0, g.d_phi_dir,
+                                                        g.d_phi);
+    PIC_LAUNCHED();
+  }
+  PIC_CUDA(cudaStreamSynchronize(g.st));
+  if (g.d_rf_nodes) cudaFree(g.d_rf_nodes);
+  if (g.d_rf_base) cudaFree(g.d_rf_base);
+  g.d_rf_nodes = nullptr;
+  g.d_rf_base = nullptr;
+  g.rf_wall = -1;
+  g.rf_count = 0;
+  if (amplitude == 0.0) return PIC_OK;
+  const size_t cnt = g.rf_line[wall].size();
+  if ((rc = upload(&g.d_rf_nodes, g.rf_line[wall].data(), cnt))) return rc;
+  if ((rc = upload(&g.d_rf_base, g.rf_base[wall].data(), cnt))) return rc;
+  g.rf_wall = wall;
+  g.rf_count = (int)cnt;
+  g.rf_amp = amplitude;
+  g.rf_omega = (2.0 * M_PI * frequency_hz) * g.t_ref;
+  g.rf_phase = phase;
+  return PIC_OK;
 }
 
 int pic_get_efield_ppr(double *efx_out, double *efy_out) {
@@ -3845,6 +3921,7 @@ int pic_step(uint64_t step, pic_step_stats *stats) {
   // 2. Poisson (IFE_Solve_2D)
   pic_solve_stats ss;
   std::memset(&ss, 0, sizeof ss);
+  if ((rc = rf_apply((double)step * g.P.dt))) return rc;  // xt = it*dt (Main_IFE_Test_2.f90:279)
   if ((rc = run_rhs())) return rc;
   int solve_rc = run_solve(&ss);
   PIC_CUDA(cudaEventRecord(e[2], g.st));

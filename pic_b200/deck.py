@@ -76,6 +76,9 @@ class Config:
     sort_interval: int = 10
     # 0: Cartesian x-y; 1: axisymmetric, x = z and y = r with the axis at y = 0
     delta: int = 0
+    # (wall, volts, frequency_hz[, phase]): RF potential added to the Dirichlet
+    # wall x = xmin (0) or x = xmax (1); None: static walls
+    rf: tuple | None = None
     # per-node energy deposit (a diagnostic) only on output steps; the
     # reference writes its profiles every 1000 steps (Main_IFE_Test_2.f90:466-470)
     diag_interval: int = 1000
@@ -148,6 +151,20 @@ def config(name: str, **over) -> Config:
                    objects=[ObjectSpec(api.PIC_SHAPE_CIRCLE, 0.005, 0.0051, 0.0023, eps=4.0)],
                    wall_V=(5.0, 0.0, 0.0, 0.0), n0=1e15, ppc=8, Te_eV=2.0, nt=10,
                    pcg_tol=1e-10, seed=3)
+    elif name == "cfg5":
+        # r-z capacitively coupled cell: z = x in [0, 0.2] m (2048 cells), r =
+        # y in [0, 0.1] m (1024 cells), the axis at r = 0; 200 V at 13.56 MHz
+        # on the electrode z = 0, grounded z = 0.2 m and r = 0.1 m; a
+        # dielectric wafer (eps 3.9, 1 mm thick, r < 0.075 m) 10 mm above the
+        # electrode.  r = 0.075 m is the node line j = 768, where the interface
+        # would pass through vertices: the wafer's edge sits a quarter cell
+        # further out.  FP64: the r-z push has no mixed-precision form yet.
+        r_wafer = 0.075 + 0.25 * 0.1 / 1024
+        c = Config("cfg5-axi-2048x1024-rf-wafer", 0.2, 0.1, 2048, 1024,
+                   objects=[ObjectSpec(api.PIC_SHAPE_BOX, 0.010, -0.001, 0.011, r_wafer, eps=3.9)],
+                   wall_dirichlet=(1, 1, 0, 1), wall_V=(0.0, 0.0, 0.0, 0.0), n0=1e16, ppc=32,
+                   Te_eV=3.0, gas_p_Pa=2.66, nt=20000, pcg_tol=1e-8, seed=5, delta=1,
+                   rf=(0, 200.0, 13.56e6))
     elif name == "tiny_axi":
         # r-z cylinder (z = x, r = y, axis at the bottom: a symmetry line, not
         # a wall) holding a dielectric torus; Dirichlet on the ends and the
@@ -241,7 +258,12 @@ def species_params(cfg: Config):
     sc = cfg.scales
     L = sc["L_ref"]
     hx_m, hy_m = cfg.Lx / cfg.ncx, cfg.Ly / cfg.ncy
-    weight = cfg.n0 * hx_m * hy_m / cfg.ppc
+    if cfg.delta == 1:
+        # real particles per macro-particle: n0 times the cylinder's volume over
+        # the particle count (ppc per cell on average)
+        weight = cfg.n0 * math.pi * cfg.Ly * cfg.Ly * cfg.Lx / (cfg.ncx * cfg.ncy * cfg.ppc)
+    else:
+        weight = cfg.n0 * hx_m * hy_m / cfg.ppc  # per unit depth
     out = []
     for q, m, T in ((-1.0, ME, cfg.Te_eV), (1.0, AR_MASS, cfg.Ti_eV)):
         sigma = math.sqrt(KB * T * EVTOK / m) / sc["v_ref"]
@@ -286,13 +308,41 @@ def _cells_box(o, mesh, ncell, ncy, ppc):
     return np.concatenate(parts) if parts else np.zeros(0, dtype=np.int64)
 
 
+def _load_axi(cfg: Config, mesh: Mesh, rng, sigma, ncell):
+    """Uniform in volume on an r-z mesh: cell (i, j) holds ppc (2j + 1)/ncy
+    particles on average (its ring's share of the cylinder; stochastic
+    rounding), r drawn with density proportional to r inside the cell."""
+    ncy = cfg.ncy
+    cell = np.arange(ncell, dtype=np.int64)
+    cj = cell % ncy
+    mean = cfg.ppc * (2.0 * cj + 1.0) / ncy
+    counts = np.floor(mean + rng.random(ncell)).astype(np.int64)
+    cells = np.repeat(cell, counts)
+    n = cells.size
+    ci, cj = cells // ncy, cells % ncy
+    x = (ci + rng.random(n)) * mesh.hx
+    r0, r1 = cj * mesh.hy, (cj + 1) * mesh.hy
+    y = np.sqrt(r0 * r0 + rng.random(n) * (r1 * r1 - r0 * r0))
+    keep = np.ones(n, dtype=bool)
+    dk = mesh.deck
+    for k in range(dk.n_objects):
+        keep &= ~_inside(dk.objects[k], x, y)
+    x, y = x[keep], y[keep]
+    v = rng.standard_normal((3, x.size)) * sigma
+    return (np.ascontiguousarray(x), np.ascontiguousarray(y), np.ascontiguousarray(v[0]),
+            np.ascontiguousarray(v[1]), np.ascontiguousarray(v[2]))
+
+
 def load_particles(cfg: Config, mesh: Mesh, species: int, n_cells_limit: int | None = None):
-    """Seeded uniform loading, ppc per cell, outside the objects; Maxwellian velocities."""
+    """Seeded uniform loading, ppc per cell, outside the objects; Maxwellian
+    velocities (on an r-z mesh: uniform in volume, vz = v_theta)."""
     sp, _ = species_params(cfg)
     sigma = sp[species][3]
     rng = np.random.default_rng([cfg.seed, species, 7919])
     ncx, ncy = cfg.ncx, cfg.ncy
     ncell = ncx * ncy if n_cells_limit is None else min(n_cells_limit, ncx * ncy)
+    if cfg.delta == 1:
+        return _load_axi(cfg, mesh, rng, sigma, ncell)
     cell = np.arange(ncell, dtype=np.int64)
     ci, cj = cell // ncy, cell % ncy
     n = ncell * cfg.ppc

@@ -57,6 +57,8 @@ class Simulation:
         self.params = p
         api.check(self.lib.pic_init(self.mesh.ptr, C.byref(p)), "pic_init")
         self.scales = cfg.scales
+        if cfg.rf is not None:
+            self.set_wall_rf(*cfg.rf)
         use_mcc = cfg.mcc if mcc is None else mcc
         if use_mcc:
             dt_s = cfg.dt * self.scales["time_ref"]
@@ -103,10 +105,17 @@ class Simulation:
     def get_par_chg(self, rho_out: np.ndarray | None = None):
         api.check(self.lib.pic_get_par_chg(self.cfg.delta, api.dptr(rho_out)), "pic_get_par_chg")
 
-    def ife_solve(self, phi: np.ndarray | None = None) -> api.SolveStats:
+    def ife_solve(self, phi: np.ndarray | None = None, time: float = 0.0) -> api.SolveStats:
+        """IFE_Solve_2D at normalised time `time` (it drives a wall RF potential)."""
         st = api.SolveStats()
-        api.check(self.lib.pic_ife_solve(api.dptr(phi), 0.0, C.byref(st)), "pic_ife_solve")
+        api.check(self.lib.pic_ife_solve(api.dptr(phi), float(time), C.byref(st)), "pic_ife_solve")
         return st
+
+    def set_wall_rf(self, wall: int, volts: float, frequency_hz: float, phase: float = 0.0):
+        """Potential volts * sin(2 pi f t + phase) added to the Dirichlet wall
+        x = xmin (0) or x = xmax (1); volts = 0 switches it off."""
+        api.check(self.lib.pic_set_wall_rf(int(wall), volts / self.scales["Phi_ref"], float(frequency_hz),
+                                           float(phase)), "pic_set_wall_rf")
 
     def get_efield_ppr(self, efx=None, efy=None):
         api.check(self.lib.pic_get_efield_ppr(api.dptr(efx), api.dptr(efy)), "pic_get_efield_ppr")

@@ -37,6 +37,7 @@ def test_calls_before_init_fail_cleanly():
     assert lib.pic_energy_spectrum(0, 8, 5.0, 1.0, api.lptr(cnt), api.lptr(cnt)) == -6
     assert b"pic_init" in lib.pic_last_error()
     assert lib.pic_velocity_moments(0, 8, api.lptr(cnt), api.dptr(out), api.dptr(out)) == -6
+    assert lib.pic_set_wall_rf(0, 1.0, 13.56e6, 0.0) == -6
 
 
 def test_mesh_builder_rejects_bad_decks():

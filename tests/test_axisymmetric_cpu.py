@@ -294,3 +294,46 @@ def test_uniform_plasma_deposits_the_density():
         assert abs(rho[1:-1, 0].mean() - 1.5) < 0.06
     finally:
         m.close()
+
+
+def test_deck_loading_is_uniform_in_volume():
+    """The r-z deck loader (counts per cell by ring volume, r drawn with
+    density r) with its macro-weight n0 V / N deposits rho_s = n0 off the axis
+    through the oracle's deposit and normalisation."""
+    from pic_b200 import deck
+    cfg = deck.config("tiny_axi", objects=[], ppc=2000)
+    mesh = deck.Mesh(cfg)
+    try:
+        x, y, vx, vy, vz = deck.load_particles(cfg, mesh, 1)
+        n_mean = cfg.ncx * cfg.ncy * cfg.ppc
+        assert abs(x.size - n_mean) < 5 * math.sqrt(n_mean)
+        sp, L = deck.species_params(cfg)
+        parts = {"x": x, "y": y, "vx": vx, "vy": vy, "vz": vz, "loc": np.zeros(x.size, np.int32)}
+        q, e, bad = ob.deposit(mesh.ptr, parts, 1.0, 1.0, mesh.nn)
+        assert bad == 0
+        _, rs, _ = ob.normalize(mesh.ptr, [q], [e], [sp[1][2] * sp[1][0]], L, cfg.n0, mesh.nn)
+        rho = rs[0].reshape(mesh.nnx, mesh.nny)
+        inner = rho[1:-1, 1:-1]
+        assert abs(inner.mean() - 1.0) < 5e-3
+        assert np.abs(inner - 1.0).max() < 0.08
+    finally:
+        mesh.close()
+
+
+def test_cfg5_mesh_builds():
+    """The config-5 geometry (r-z, a wafer box crossing the axis) assembles;
+    the wafer's elements are interface elements along its top, bottom and
+    outer faces."""
+    from pic_b200 import deck
+    cfg = deck.config("cfg5")
+    mesh = deck.Mesh(cfg)
+    try:
+        d = mesh.desc
+        assert d.delta == 1 and d.n_interface > 0 and d.mass_rows
+        nt = mesh.array("node_type").reshape(mesh.nnx, mesh.nny)
+        assert np.all(nt[0] <= 0) and np.all(nt[-1] <= 0) and np.all(nt[:, -1] <= 0)
+        assert np.all(nt[1:-1, 0] > 0)  # the axis is not a wall
+        sp, _ = deck.species_params(cfg)
+        assert abs(sp[0][2] * cfg.ncx * cfg.ncy * cfg.ppc - cfg.n0 * math.pi * 0.1 ** 2 * 0.2) < 1e-6 * cfg.n0
+    finally:
+        mesh.close()

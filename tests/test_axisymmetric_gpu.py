@@ -95,3 +95,29 @@ def test_axi_ife_solve_bit_exact():
         assert np.array_equal(phi, po)
     finally:
         sim.close()
+
+
+def test_cfg5_geometry_steps_with_the_rf_electrode():
+    """The config-5 cell (r-z, RF electrode at z = 0, dielectric wafer) at a
+    reduced mesh and particle count: steps solve, keep every particle off
+    the axis' far side (r >= 0) and drive the electrode at 200 V sin(2 pi f t)."""
+    import math
+    cfg = deck.config("cfg5", ncx=512, ncy=100, ppc=4, nt=5)
+    cfg.objects = [deck.ObjectSpec(deck.api.PIC_SHAPE_BOX, 0.010, -0.001, 0.011, 0.0755, eps=3.9)]
+    sim = Simulation(cfg)
+    try:
+        assert sim.initial_fields().ierr == 0
+        static = sim.mesh.array("phi_dirichlet").copy()
+        amp = 200.0 / sim.scales["Phi_ref"]
+        w = 2.0 * math.pi * 13.56e6 * sim.scales["time_ref"]
+        for k in range(1, 6):
+            st = sim.step()
+            assert st.solve.ierr == 0, k
+            phi = sim.field("phi")
+            left = np.arange(sim.mesh.nny)
+            assert np.allclose(phi[left] - static[left], amp * math.sin(w * k * cfg.dt), rtol=0, atol=1e-9)
+        for s in range(2):
+            p = sim.download(s)
+            assert p["y"].size > 0 and np.all(p["y"] >= 0.0) and np.all(np.isfinite(p["vz"]))
+    finally:
+        sim.close()
