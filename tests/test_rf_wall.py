@@ -35,7 +35,8 @@ def test_rf_wall_solve_matches_oracle():
         nn = sim.mesh.nn
         rho = np.random.default_rng(8).standard_normal(nn) * 0.05
         sim.set_field("rho", rho)
-        pd = sim.mesh.array("phi_dirichlet")
+        # a view onto the descriptor's own table, which the oracle reads
+        pd = np.ctypeslib.as_array(sim.mesh.desc.phi_dirichlet, shape=(nn,))
         static = pd.copy()
         phi = static.copy()
         t = 2000.0
