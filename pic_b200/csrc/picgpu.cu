@@ -390,6 +390,7 @@ struct PushM {
   float qmdt;      // q/m * dt
   float dtx, dty;  // dt/hx, dt/hy: cells moved per unit velocity per step
   float hx, hy;
+  double dt, hyd, inv_hy;  // the r-z move (FP64): dt, hy and 1/hy
   double mass, vref;
   int do_push, do_deposit, do_energy;
   int wall[4];
@@ -405,14 +406,24 @@ struct PushM {
 // push_mixed_one: one live particle p (element e, offsets ax, ay,
 // velocities vx, vy as loaded): gather, push, walls, objects, locate; writes
 // the particle back and returns what the warp deposit needs.
+// AXI (r-z, y = r with the axis at ymin = 0; vx, vy, vz = v_z, v_r, v_theta
+// in the particle's frame): the axial move as above; the transverse move, as
+// k_push<true> does it, in FP64 from the absolute radius r = (j + ay) hy --
+// X = r + dt v_r, Y = dt v_theta, r' = |(X, Y)|, (v_r, v_theta) rotated by
+// (X, Y)/r' -- and r' split back into (j, ay); the deposit weights are
+// k_push<true>'s r^2-linear ones written in the offsets:
+// (1 - a)(2j + 1 + a)/(2j + 1) below, a(2j + a)/(2j + 1) above, x 0.75 below
+// in the axis row.
+template <bool AXI>
 __device__ __forceinline__ void push_mixed_one(const MeshK &m, const float *__restrict__ c32, const PushM &prm,
                                                const SpK &s, int64_t p, int e, float ax, float ay, float vx,
                                                float vy, int &key, double W[4], int nodes[4], double &energy,
                                                bool &lost) {
   float *fx = reinterpret_cast<float *>(s.x), *fy = reinterpret_cast<float *>(s.y);
   float *fvx = reinterpret_cast<float *>(s.vx), *fvy = reinterpret_cast<float *>(s.vy);
-  const float *fvz = reinterpret_cast<const float *>(s.vz);
+  float *fvz = reinterpret_cast<float *>(s.vz);
   int i = elem_column(m, e), j = e - i * m.ney;
+  float vt = 0.f;  // AXI: v_theta after the push
   if (prm.do_push) {
     const int n1 = i * m.nny + j;
     const int cn[4] = {n1, n1 + m.nny, n1 + m.nny + 1, n1 + 1};
@@ -449,7 +460,22 @@ __device__ __forceinline__ void push_mixed_one(const MeshK &m, const float *__re
     vx = fmaf(prm.qmdt, Ex, vx);
     vy = fmaf(prm.qmdt, Ey, vy);
     ax = fmaf(prm.dtx, vx, ax);
-    ay = fmaf(prm.dty, vy, ay);
+    if (AXI) {
+      vt = fvz[p];
+      double X = ((double)j + (double)ay) * prm.hyd + prm.dt * (double)vy, Y = prm.dt * (double)vt;
+      if (X == 0.0) X = prm.hyd * (double)1.0e-5f;
+      const double rn = sqrt(X * X + Y * Y), c = X / rn, sn = Y / rn;
+      const double vr = c * (double)vy + sn * (double)vt, vtn = c * (double)vt - sn * (double)vy;
+      vy = (float)vr;
+      vt = (float)vtn;
+      fvz[p] = vt;
+      const double u = rn * prm.inv_hy, fu = floor(u);
+      j = (int)fu;
+      ay = (float)(u - fu);
+      if (ay >= 1.f) { ay -= 1.f; ++j; }
+    } else {
+      ay = fmaf(prm.dty, vy, ay);
+    }
     // re-home the offsets into [0, 1)
     const float dfx = floorf(ax), dfy = floorf(ay);
     ax -= dfx;
@@ -516,23 +542,33 @@ __device__ __forceinline__ void push_mixed_one(const MeshK &m, const float *__re
     if (prm.do_deposit) {
       key = en;
       const double dx = ax, dy = ay, xc = 1.0 - dx, yc = 1.0 - dy;
-      W[0] = xc * yc;
-      W[1] = dx * yc;
-      W[2] = dx * dy;
-      W[3] = xc * dy;
+      if (AXI) {
+        const double jj = (double)j, den = 2.0 * jj + 1.0, beta = (j == 0) ? 0.75 : 1.0;
+        const double lo = (yc * (den + dy)) / den, hi = (dy * (2.0 * jj + dy)) / den;
+        W[0] = (xc * lo) * beta;
+        W[1] = (dx * lo) * beta;
+        W[2] = dx * hi;
+        W[3] = xc * hi;
+      } else {
+        W[0] = xc * yc;
+        W[1] = dx * yc;
+        W[2] = dx * dy;
+        W[3] = xc * dy;
+      }
       const int n1 = i * m.nny + j;
       nodes[0] = n1;
       nodes[1] = n1 + m.nny;
       nodes[2] = n1 + m.nny + 1;
       nodes[3] = n1 + 1;
       if (prm.do_energy) {
-        const double vz = fvz[p], wx = vx, wy = vy;
+        const double vz = (AXI && prm.do_push) ? (double)vt : (double)fvz[p], wx = vx, wy = vy;
         energy = ((((0.5 * prm.mass) * ((wx * wx + wy * wy) + vz * vz)) * prm.vref) * prm.vref) / PIC_JTOEV;
       }
     }
   }
 }
 
+template <bool AXI>
 __global__ void __launch_bounds__(256, 4) k_push_mixed(MeshK m, const float *__restrict__ c32, PushM prm, SpK s) {
   const int64_t p = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
   const int lane = threadIdx.x & 31;
@@ -546,7 +582,7 @@ __global__ void __launch_bounds__(256, 4) k_push_mixed(MeshK m, const float *__r
     if (e >= 0) {
       const float *fx = reinterpret_cast<const float *>(s.x), *fy = reinterpret_cast<const float *>(s.y);
       const float *fvx = reinterpret_cast<const float *>(s.vx), *fvy = reinterpret_cast<const float *>(s.vy);
-      push_mixed_one(m, c32, prm, s, p, e, fx[p], fy[p], fvx[p], fvy[p], key, W, nodes, energy, lost);
+      push_mixed_one<AXI>(m, c32, prm, s, p, e, fx[p], fy[p], fvx[p], fvy[p], key, W, nodes, energy, lost);
     }
   }
   warp_deposit(s, lane, key, W, nodes, energy, lost, prm.do_deposit, prm.do_energy);
@@ -606,7 +642,7 @@ __device__ __forceinline__ void push_tile_load(PushTile *T, const TileCopy &c, i
   if (threadIdx.x < 64) cp_async16(t + c.dst1, c.src1 + off, 4 * valid);
 }
 
-template <int S, int MINB = 4>
+template <int S, int MINB = 4, bool AXI = false>
 __global__ void __launch_bounds__(256, MINB) k_push_mixed_tiled(MeshK m, const float *__restrict__ c32, PushM prm,
                                                               SpK s, int64_t ntiles) {
   extern __shared__ __align__(16) unsigned char push_smem[];
@@ -637,8 +673,8 @@ __global__ void __launch_bounds__(256, MINB) k_push_mixed_tiled(MeshK m, const f
     if (p < s.n) {
       const int e = C.loc[threadIdx.x];
       if (e >= 0)
-        push_mixed_one(m, c32, prm, s, p, e, C.ax[threadIdx.x], C.ay[threadIdx.x], C.vx[threadIdx.x],
-                       C.vy[threadIdx.x], key, W, nodes, energy, lost);
+        push_mixed_one<AXI>(m, c32, prm, s, p, e, C.ax[threadIdx.x], C.ay[threadIdx.x], C.vx[threadIdx.x],
+                            C.vy[threadIdx.x], key, W, nodes, energy, lost);
     }
     warp_deposit(s, lane, key, W, nodes, energy, lost, prm.do_deposit, prm.do_energy);
     __syncthreads();  // tile t is read before its stage is refilled
@@ -2243,13 +2279,25 @@ static int run_push(int sidx, bool do_push, bool do_deposit, bool do_energy) {
     pm.dty = (float)(g.P.dt / m.hy);
     pm.hx = (float)m.hx;
     pm.hy = (float)m.hy;
+    pm.dt = g.P.dt;
+    pm.hyd = m.hy;
+    pm.inv_hy = 1.0 / m.hy;
     pm.mass = s.mass;
     pm.vref = g.v_ref;
     pm.do_push = do_push;
     pm.do_deposit = do_deposit;
     pm.do_energy = do_deposit && do_energy;
     for (int w = 0; w < 4; ++w) pm.wall[w] = g.P.wall_bc[w];
-    if (g.push_stages) {
+    if (g.axi) {
+      // r-z: the default tiled form (4 stages, 5 CTAs per SM) or the direct one
+      if (g.push_stages) {
+        const int64_t ntiles = (s.n_slots + kPushTile - 1) / kPushTile;
+        const unsigned grid = (unsigned)std::min<int64_t>(ntiles, g.push_grid);
+        k_push_mixed_tiled<4, 5, true><<<grid, kPushTile, 4 * sizeof(PushTile), g.st>>>(m, g.d_coef32, pm, k, ntiles);
+      } else {
+        k_push_mixed<true><<<blocks_for(s.n_slots, 256), 256, 0, g.st>>>(m, g.d_coef32, pm, k);
+      }
+    } else if (g.push_stages) {
       const int64_t ntiles = (s.n_slots + kPushTile - 1) / kPushTile;
       const unsigned grid = (unsigned)std::min<int64_t>(ntiles, g.push_grid);
       const size_t smem = (size_t)g.push_stages * sizeof(PushTile);
@@ -2264,7 +2312,7 @@ static int run_push(int sidx, bool do_push, bool do_deposit, bool do_energy) {
       else
         k_push_mixed_tiled<4><<<grid, kPushTile, smem, g.st>>>(m, g.d_coef32, pm, k, ntiles);
     } else {
-      k_push_mixed<<<blocks_for(s.n_slots, 256), 256, 0, g.st>>>(m, g.d_coef32, pm, k);
+      k_push_mixed<false><<<blocks_for(s.n_slots, 256), 256, 0, g.st>>>(m, g.d_coef32, pm, k);
     }
   } else {
     if (g.axi)
@@ -3122,8 +3170,8 @@ int pic_init(const pic_mesh_desc *mesh, const pic_params *params) {
     set_error("pic_init: delta must be 0 (Cartesian) or 1 (axisymmetric)");
     return PIC_ERR_ARG;
   }
-  if (mesh->delta == 1 && (P.precision != PIC_PREC_FP64 || !mesh->mass_rows || mesh->ymin != 0.0)) {
-    set_error("pic_init: axisymmetric meshes need FP64 precision, the per-row load matrices and the axis at ymin = 0");
+  if (mesh->delta == 1 && (!mesh->mass_rows || mesh->ymin != 0.0)) {
+    set_error("pic_init: axisymmetric meshes need the per-row load matrices and the axis at ymin = 0");
     return PIC_ERR_ARG;
   }
   if ((int64_t)mesh->nnx * mesh->nny > (int64_t)1 << 30) {
@@ -3552,7 +3600,9 @@ int pic_init(const pic_mesh_desc *mesh, const pic_params *params) {
       // and 2.43 with 6 (40 registers, small spills)
       const char *mb = getenv("PIC_PUSH_MINB");
       g.push_minb = mb ? atoi(mb) : g.push_minb;
-      const void *fn = g.push_stages == 2   ? (const void *)k_push_mixed_tiled<2>
+      if (g.axi) g.push_stages = 4;  // the r-z push has the 4-stage, 5-CTA form only
+      const void *fn = g.axi                ? (const void *)k_push_mixed_tiled<4, 5, true>
+                       : g.push_stages == 2 ? (const void *)k_push_mixed_tiled<2>
                        : g.push_stages == 3 ? (const void *)k_push_mixed_tiled<3>
                        : g.push_minb == 5   ? (const void *)k_push_mixed_tiled<4, 5>
                        : g.push_minb == 6   ? (const void *)k_push_mixed_tiled<4, 6>

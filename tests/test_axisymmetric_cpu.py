@@ -246,12 +246,16 @@ def test_axi_deposit_splits_a_uniform_ring_evenly():
         m.close()
 
 
-def test_pic_init_refuses_axisymmetric_mixed_precision():
-    """The axisymmetric push and deposit exist in FP64 only: pic_init turns
-    down delta = 1 with PIC_PREC_MIXED before it touches the device."""
+def test_pic_init_refuses_an_axisymmetric_mesh_off_the_axis():
+    """The r-z push and deposit take the axis at y = ymin = 0: pic_init turns
+    down delta = 1 with ymin != 0 before it touches the device."""
     from pic_b200 import deck
-    cfg = deck.config("tiny_axi", precision=api.PIC_PREC_MIXED)
-    mesh = deck.Mesh(cfg)
+    cfg = deck.config("tiny_axi", objects=[])
+    d = deck.make_deck(cfg)
+    d.ymin, d.ymax = 0.5, 0.5 + d.ymax
+    lib = api.load()
+    ptr = C.POINTER(api.MeshDesc)()
+    api.check(lib.pic_mesh_build(C.byref(d), C.byref(ptr)), "pic_mesh_build")
     try:
         p = api.Params()
         p.n_species = 1
@@ -259,12 +263,10 @@ def test_pic_init_refuses_axisymmetric_mixed_precision():
         p.species[0].capacity = 1024
         p.dt, p.n_ref, p.T_ref_eV = cfg.dt, cfg.n0, cfg.Te_eV
         p.pcg_tol, p.pcg_maxit = cfg.pcg_tol, cfg.pcg_maxit
-        p.precision = api.PIC_PREC_MIXED
-        lib = api.load()
-        assert lib.pic_init(mesh.ptr, C.byref(p)) == api.PIC_ERR_ARG
-        assert b"axisymmetric" in lib.pic_last_error()
+        assert lib.pic_init(ptr, C.byref(p)) == api.PIC_ERR_ARG
+        assert b"ymin = 0" in lib.pic_last_error()
     finally:
-        mesh.close()
+        lib.pic_mesh_free(ptr)
 
 
 def test_uniform_plasma_deposits_the_density():

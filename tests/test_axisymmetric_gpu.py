@@ -121,3 +121,76 @@ def test_cfg5_geometry_steps_with_the_rf_electrode():
             assert p["y"].size > 0 and np.all(p["y"] >= 0.0) and np.all(np.isfinite(p["vz"]))
     finally:
         sim.close()
+
+
+def _both_prec(fn, **over):
+    out = []
+    for prec in (deck.api.PIC_PREC_FP64, deck.api.PIC_PREC_MIXED):
+        sim = Simulation(deck.config("tiny_axi", precision=prec, **over))
+        try:
+            out.append(fn(sim))
+        finally:
+            sim.close()
+    return out
+
+
+def test_axi_mixed_push_and_deposit_match_fp64():
+    """The mixed-precision r-z push (element + FP32 offsets, FP64 radial
+    move) against the FP64 one after one push: positions within 1e-5 of a
+    cell, velocities (v_theta included) within 1e-5 relative; node charge
+    within 1e-4 of the largest, before and after."""
+    def fn(sim):
+        sim.initial_fields()
+        rho0 = sim.field("rho")
+        for s in range(2):
+            sim.move_all(s)
+        sim.get_par_chg()
+        return rho0, sim.field("rho"), [_by_id(sim.download(s)) for s in range(2)], sim.mesh.hy
+
+    (r0d, r1d, pd, hy), (r0m, r1m, pm, _) = _both_prec(fn)
+    assert np.abs(r0d - r0m).max() <= 1e-6 * np.abs(r0d).max()
+    assert np.abs(r1d - r1m).max() <= 1e-4 * np.abs(r1d).max()
+    for a, b in zip(pd, pm):
+        common, ia, ib = np.intersect1d(a["id"], b["id"], return_indices=True)
+        assert common.size >= 0.999 * max(a["id"].size, b["id"].size)
+        assert np.abs(a["x"][ia] - b["x"][ib]).max() <= 1e-5 * hy
+        assert np.abs(a["y"][ia] - b["y"][ib]).max() <= 1e-5 * hy
+        for v in ("vx", "vy", "vz"):
+            assert np.allclose(a[v][ia], b[v][ib], rtol=1e-5, atol=1e-5 * np.abs(a[v]).max()), v
+
+
+def test_axi_mixed_steps_track_fp64():
+    def fn(sim):
+        sim.initial_fields()
+        for _ in range(10):
+            sim.step()
+        return {f: sim.field(f) for f in ("phi", "efx", "efy")}, [sim.count(s) for s in range(2)]
+
+    (fd, nd), (fm, nm) = _both_prec(fn, ppc=40)
+    for f in ("phi", "efx", "efy"):
+        err = np.abs(fd[f] - fm[f]).max() / np.abs(fd[f]).max()
+        assert err <= 1e-2, f
+    for a, b in zip(nd, nm):
+        assert abs(a - b) <= 0.01 * a
+
+
+def test_axi_tiled_push_matches_direct(monkeypatch):
+    def fn(sim):
+        sim.initial_fields()
+        for _ in range(5):
+            sim.step()
+        return [_by_id(sim.download(s)) for s in range(2)], sim.field("rho"), sim.field("phi")
+
+    out = []
+    for st in ("0", "4"):
+        monkeypatch.setenv("PIC_PUSH_STAGES", st)
+        sim = Simulation(deck.config("tiny_axi", precision=deck.api.PIC_PREC_MIXED))
+        try:
+            out.append(fn(sim))
+        finally:
+            sim.close()
+    (pa, ra, fa), (pb, rb, fb) = out
+    for a, b in zip(pa, pb):
+        for k in ("id", "loc", "x", "y", "vx", "vy", "vz"):
+            assert np.array_equal(a[k], b[k]), k
+    assert np.array_equal(ra, rb) and np.array_equal(fa, fb)
