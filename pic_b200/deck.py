@@ -158,13 +158,13 @@ def config(name: str, **over) -> Config:
         # dielectric wafer (eps 3.9, 1 mm thick, r < 0.075 m) 10 mm above the
         # electrode.  r = 0.075 m is the node line j = 768, where the interface
         # would pass through vertices: the wafer's edge sits a quarter cell
-        # further out.  FP64: the r-z push has no mixed-precision form yet.
+        # further out.  Mixed precision, as the benchmark decks 3 and 4.
         r_wafer = 0.075 + 0.25 * 0.1 / 1024
         c = Config("cfg5-axi-2048x1024-rf-wafer", 0.2, 0.1, 2048, 1024,
                    objects=[ObjectSpec(api.PIC_SHAPE_BOX, 0.010, -0.001, 0.011, r_wafer, eps=3.9)],
                    wall_dirichlet=(1, 1, 0, 1), wall_V=(0.0, 0.0, 0.0, 0.0), n0=1e16, ppc=32,
                    Te_eV=3.0, gas_p_Pa=2.66, nt=20000, pcg_tol=1e-8, seed=5, delta=1,
-                   rf=(0, 200.0, 13.56e6))
+                   rf=(0, 200.0, 13.56e6), precision=api.PIC_PREC_MIXED)
     elif name == "tiny_axi":
         # r-z cylinder (z = x, r = y, axis at the bottom: a symmetry line, not
         # a wall) holding a dielectric torus; Dirichlet on the ends and the

@@ -97,12 +97,14 @@ def test_axi_ife_solve_bit_exact():
         sim.close()
 
 
-def test_cfg5_geometry_steps_with_the_rf_electrode():
+@pytest.mark.parametrize("precision", ["fp64", "mixed"])
+def test_cfg5_geometry_steps_with_the_rf_electrode(precision):
     """The config-5 cell (r-z, RF electrode at z = 0, dielectric wafer) at a
     reduced mesh and particle count: steps solve, keep every particle off
     the axis' far side (r >= 0) and drive the electrode at 200 V sin(2 pi f t)."""
     import math
-    cfg = deck.config("cfg5", ncx=512, ncy=100, ppc=4, nt=5)
+    prec = deck.api.PIC_PREC_MIXED if precision == "mixed" else deck.api.PIC_PREC_FP64
+    cfg = deck.config("cfg5", ncx=512, ncy=100, ppc=4, nt=5, precision=prec)
     cfg.objects = [deck.ObjectSpec(deck.api.PIC_SHAPE_BOX, 0.010, -0.001, 0.011, 0.0755, eps=3.9)]
     sim = Simulation(cfg)
     try:
