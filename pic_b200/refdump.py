@@ -15,11 +15,14 @@ read back as Restart_2D (code/PIC/Restart_2D.f90:37-79) and LoadParticleBundle
                        [NPar, NParNormal] int32; [Charge, Mass, Weight]
                        float64; then one record a particle: X, Y, Z, Vx, Vy,
                        Vz, Ax, Ay, Az, Wq float64 and Location int32 (84
-                       bytes), positions in metres and velocities in m/s (the
-                       bundle is rescaled by PosRes/VelRes before the write)
+                       bytes); the bundle is rescaled before the write by
+                       PosRes, which scales X alone (ParticleOne.f90,
+                       PositionRescaleParticleOne), and VelRes: X in metres,
+                       Y in L_ref units, velocities in m/s
 
 A Fortran unformatted sequential record is its payload between two int32
-byte counts (little-endian, as gfortran and ifort write records below 2 GiB).
+byte counts (little-endian, as gfortran and ifort write records below 2 GiB),
+a derived type's components one after another without padding.
 The name 10000<Name>.dat is DefaultNameIndex (MCC_jw/code/base/ControlFlow.f90:12)
 and the species' name; the reference builds it with a list-directed internal
 write, whose blanks depend on the compiler, so the reader also accepts a
@@ -178,7 +181,7 @@ def dump(sim, directory: str, lap: int, period_res: float = 0.0, istep_previous:
         counts.append(n)
         zero = np.zeros(n)
         # an r-z particle's own frame is the Cartesian one at angle 0: Z = 0
-        cols = {"X": p["x"] * L, "Y": p["y"] * L, "Z": zero, "Vx": p["vx"] * V, "Vy": p["vy"] * V,
+        cols = {"X": p["x"] * L, "Y": p["y"], "Z": zero, "Vx": p["vx"] * V, "Vy": p["vy"] * V,
                 "Vz": p["vz"] * V, "Ax": zero, "Ay": zero, "Az": zero, "Wq": np.full(n, weight),
                 "Location": p["loc"].astype(np.int64) + 1}
         # SpecyOne.f90:159-160: charge in coulomb, mass in kg
@@ -209,7 +212,7 @@ def restore(sim, directory: str, lap: int) -> dict:
             raise ValueError("species %d: %d particles in its file, %d in the var file" % (s, r["npar"], var["ns"][s]))
         vy, vz = transverse_to_frame(r["Z"], r["Vy"], r["Vz"]) if axi else (r["Vy"], r["Vz"])
         x = np.ascontiguousarray(r["X"] / L)
-        y = np.ascontiguousarray(r["Y"] / L)
+        y = np.ascontiguousarray(r["Y"])  # PosRes leaves Y in L_ref units
         vx = np.ascontiguousarray(r["Vx"] / V)
         vy = np.ascontiguousarray(vy / V)
         vz = np.ascontiguousarray(vz / V)

@@ -1,8 +1,9 @@
 """A simulation written as the reference's restart files (Dump_2D +
 ParticleBundle%Dump) and read back into a fresh one (Restart_2D +
-LoadParticleBundle): phi and E bit for bit, particles to the rounding of
-the SI round trip (x * L_ref / L_ref), and the next steps agree (MCC off:
-restored particles get new ids, which key the collision draws)."""
+LoadParticleBundle): phi and E bit for bit, y (kept in L_ref units as the
+reference's PosRes keeps it) bit for bit, x and the velocities to the
+rounding of the SI round trip (x * L_ref / L_ref), and the next steps agree
+(MCC off: restored particles get new ids, which key the collision draws)."""
 import numpy as np
 import pytest
 
@@ -41,7 +42,8 @@ def test_dump_restore_round_trip(tmp_path, name):
         for s in range(2):
             assert b.count(s) == counts[s]
             pb = _by_pos(b.download(s))
-            for k in ("x", "y", "vx", "vy", "vz"):
+            assert np.array_equal(pb["y"], parts_a[s]["y"])
+            for k in ("x", "vx", "vy", "vz"):
                 assert np.allclose(pb[k], parts_a[s][k], rtol=4e-16, atol=0), (s, k)
             assert np.array_equal(pb["loc"], parts_a[s]["loc"])
         b.step()
