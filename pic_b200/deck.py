@@ -309,7 +309,10 @@ def _cells_box(o, mesh, ncell, ncy, ppc):
 
 
 def _load_axi(cfg: Config, mesh: Mesh, rng, sigma, ncell):
-    """Uniform in volume on an r-z mesh: cell (i, j) holds ppc (2j + 1)/ncy
+    """Uniform in volume on an r-z mesh, the distribution of the reference's
+    equal-weight loading (MCC_jw/code/base/ParticleOne.f90,
+    PositionRandomInitializationParticleOne for delta 1: r = sqrt(r0^2 +
+    u (r1^2 - r0^2))), drawn cell by cell: cell (i, j) holds ppc (2j + 1)/ncy
     particles on average (its ring's share of the cylinder; stochastic
     rounding), r drawn with density proportional to r inside the cell."""
     ncy = cfg.ncy
