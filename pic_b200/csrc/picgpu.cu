@@ -201,6 +201,13 @@ __device__ __forceinline__ long long seg_sum(long long v, int lane, int seg_end)
 // element (particles are cell-sorted, so neighbouring lanes usually share an
 // element), then one atomic per node and value from the segment head.
 // Integer sums are exact: node totals do not depend on the segmentation.
+// CONSERVE (the Cartesian mixed-precision push): corner 2's charge is 2^40
+// minus the other three rounded corners, so every particle deposits exactly
+// 2^40 and a run of L particles 2^40 L minus three sums -- one 64-bit warp
+// sum fewer.  Without it (the FP64 path, bit-exact with the oracle, and the
+// r-z weights, which do not sum to 1 on the axis row) each corner is rounded
+// on its own.
+template <bool CONSERVE = false>
 __device__ __forceinline__ void warp_deposit(const SpK &s, int lane, int key, const double W[4], const int nodes[4],
                                              double energy, bool lost, int do_deposit, int do_energy) {
   unsigned int lm = __ballot_sync(0xffffffffu, lost);
@@ -217,7 +224,9 @@ __device__ __forceinline__ void warp_deposit(const SpK &s, int lane, int key, co
     };
     long long qv[4];
 #pragma unroll
-    for (int c = 0; c < 4; ++c) qv[c] = wsum(__double2ll_rn(W[c] * PIC_Q_SCALE));
+    for (int c = 0; c < 4; ++c)
+      if (!CONSERVE || c != 2) qv[c] = wsum(__double2ll_rn(W[c] * PIC_Q_SCALE));
+    if (CONSERVE) qv[2] = 32ll * (1ll << 40) - ((qv[0] + qv[1]) + qv[3]);
     if (lane == 0)
 #pragma unroll
       for (int c = 0; c < 4; ++c) atomicAdd(s.q_acc + nodes[c], (unsigned long long)qv[c]);
@@ -236,7 +245,10 @@ __device__ __forceinline__ void warp_deposit(const SpK &s, int lane, int key, co
   int seg_end = above ? (__ffs(above) - 2) : 31;
   long long qv[4];
 #pragma unroll
-  for (int c = 0; c < 4; ++c) qv[c] = seg_sum((key >= 0) ? __double2ll_rn(W[c] * PIC_Q_SCALE) : 0ll, lane, seg_end);
+  for (int c = 0; c < 4; ++c)
+    if (!CONSERVE || c != 2) qv[c] = seg_sum((key >= 0) ? __double2ll_rn(W[c] * PIC_Q_SCALE) : 0ll, lane, seg_end);
+  // the head's sums cover its run, lanes [lane, seg_end]
+  if (CONSERVE) qv[2] = (long long)(seg_end - lane + 1) * (1ll << 40) - ((qv[0] + qv[1]) + qv[3]);
   if (head && key >= 0)
 #pragma unroll
     for (int c = 0; c < 4; ++c) atomicAdd(s.q_acc + nodes[c], (unsigned long long)qv[c]);
@@ -585,7 +597,7 @@ __global__ void __launch_bounds__(256, 4) k_push_mixed(MeshK m, const float *__r
       push_mixed_one<AXI>(m, c32, prm, s, p, e, fx[p], fy[p], fvx[p], fvy[p], key, W, nodes, energy, lost);
     }
   }
-  warp_deposit(s, lane, key, W, nodes, energy, lost, prm.do_deposit, prm.do_energy);
+  warp_deposit<!AXI>(s, lane, key, W, nodes, energy, lost, prm.do_deposit, prm.do_energy);
 }
 
 // ---- the same push with the particle data staged through shared memory:
@@ -676,7 +688,7 @@ __global__ void __launch_bounds__(256, MINB) k_push_mixed_tiled(MeshK m, const f
         push_mixed_one<AXI>(m, c32, prm, s, p, e, C.ax[threadIdx.x], C.ay[threadIdx.x], C.vx[threadIdx.x],
                             C.vy[threadIdx.x], key, W, nodes, energy, lost);
     }
-    warp_deposit(s, lane, key, W, nodes, energy, lost, prm.do_deposit, prm.do_energy);
+    warp_deposit<!AXI>(s, lane, key, W, nodes, energy, lost, prm.do_deposit, prm.do_energy);
     __syncthreads();  // tile t is read before its stage is refilled
   }
   cp_async_wait<0>();
