@@ -15,7 +15,12 @@
  * Pinned against the reference's own known answers: normalisation constants
  * (OUTPUT/physics_parameter.inp:42-47), the closed-form Q1 IFE basis
  * (IFE-Rectangular/Retangular_reference_basis_IFE.f90) and the IFE
- * convergence rates of Norm_Error_{0064,0128,0256}.txt; see tests/.
+ * convergence rates of Norm_Error_{0064,0128,0256}.txt; see tests/.  The
+ * axisymmetric (delta 1) branches have no reference outputs; they are
+ * pinned by analytic answers in tests/: dual volumes that sum to the
+ * cylinder, a manufactured solution at second order, an exact dielectric
+ * slab, free streaming along the 3D straight line, and a plasma uniform in
+ * volume that deposits its density.
  */
 #include <math.h>
 #ifdef _OPENMP
