@@ -100,3 +100,89 @@ def test_rz_frame_of_reference_velocities():
     # at angle 0 the frames coincide: what dump writes reads back unchanged
     a, b = rd.transverse_to_frame(np.zeros(3), np.array([1.0, 2.0, 3.0]), np.array([4.0, 5.0, 6.0]))
     assert np.array_equal(a, [1.0, 2.0, 3.0]) and np.array_equal(b, [4.0, 5.0, 6.0])
+
+
+class _FakeSim:
+    """The parts of Simulation that dump/restore use, on host arrays."""
+
+    def __init__(self, nnx=5, nny=4, delta=0, n=(6, 3), seed=1):
+        from types import SimpleNamespace
+        rng = np.random.default_rng(seed)
+        self.cfg = SimpleNamespace(delta=delta)
+        self.mesh = SimpleNamespace(nnx=nnx, nny=nny, nn=nnx * nny)
+        self.scales = {"L_ref": 2.5e-4, "v_ref": 5.9e5}
+        self.species = [(-1.0, 9.1095e-31, 3.0e3, 0.0), (1.0, 6.63e-26, 3.0e3, 0.0)]
+        self.parts = [{"x": rng.random(k), "y": rng.random(k), "vx": rng.standard_normal(k),
+                       "vy": rng.standard_normal(k), "vz": rng.standard_normal(k),
+                       "loc": rng.integers(0, (nnx - 1) * (nny - 1), k).astype(np.int32)} for k in n]
+        self.phi = rng.standard_normal(nnx * nny)
+        self.uploaded, self.step_index, self.ppr_calls = {}, 0, 0
+
+    def download(self, s):
+        return {k: v.copy() for k, v in self.parts[s].items()}
+
+    def field(self, name):
+        assert name == "phi"
+        return self.phi.copy()
+
+    def upload(self, s, x, y, vx, vy, vz):
+        self.uploaded[s] = (x, y, vx, vy, vz)
+
+    def set_field(self, name, v):
+        assert name == "phi"
+        self.phi = np.asarray(v).copy()
+
+    def get_efield_ppr(self):
+        self.ppr_calls += 1
+
+
+def test_dump_writes_reference_units_and_restore_inverts_them(tmp_path):
+    a = _FakeSim()
+    rd.dump(a, str(tmp_path), 40, period_res=12.5, istep_previous=3, nperiod=1)
+    var = rd.read_var(rd.var_path(str(tmp_path), 40), 2)
+    assert var == {"lap": 40, "ntot": 9, "ns": [6, 3], "nx": 5, "ny": 4, "period_res": 12.5,
+                   "istep_previous": 3, "nperiod": 1}
+    r = rd.read_particles(str(tmp_path / "10000Electron.dat"))
+    p = a.parts[0]
+    L, V = a.scales["L_ref"], a.scales["v_ref"]
+    assert np.array_equal(r["X"], p["x"] * L) and np.array_equal(r["Y"], p["y"])  # PosRes scales X alone
+    assert np.array_equal(r["Vz"], p["vz"] * V) and np.all(r["Z"] == 0.0)
+    assert np.array_equal(r["Location"], p["loc"] + 1)
+    assert r["charge"] == -1.6022e-19 and r["weight"] == 3.0e3
+    b = _FakeSim(seed=2)
+    got = rd.restore(b, str(tmp_path), 40)
+    assert got["lap"] == 40 and b.step_index == 40 and b.ppr_calls == 1
+    assert np.array_equal(b.phi, a.phi)
+    x, y, vx, vy, vz = b.uploaded[1]
+    q = a.parts[1]
+    assert np.array_equal(y, q["y"])
+    assert np.allclose(x, q["x"], rtol=4e-16, atol=0) and np.allclose(vz, q["vz"], rtol=4e-16, atol=0)
+
+
+def test_restore_refuses_another_mesh_or_inconsistent_counts(tmp_path):
+    rd.dump(_FakeSim(), str(tmp_path), 7)
+    with pytest.raises(ValueError, match="node mesh"):
+        rd.restore(_FakeSim(nnx=6), str(tmp_path), 7)
+    # the var file says 6 electrons; a particle file holding 5 is refused
+    rd.write_particles(str(tmp_path / "10000Electron.dat"), -1.6022e-19, 9.1095e-31, 1.0, _cols(5), 5)
+    with pytest.raises(ValueError, match="particles in its file"):
+        rd.restore(_FakeSim(), str(tmp_path), 7)
+
+
+def test_restore_rotates_rz_velocities_into_the_particle_frame(tmp_path):
+    a = _FakeSim(delta=1)
+    rd.dump(a, str(tmp_path), 1)
+    # a reference-written file: the same particles at angle pi/2, velocities Cartesian
+    f = str(tmp_path / "10000Ar(+).dat")
+    r = rd.read_particles(f)
+    ang = np.full(r["npar"], math.pi / 2)
+    cols = {k: r[k] for k in ("X", "Y", "Vx", "Ax", "Ay", "Az", "Wq", "Location")}
+    cols["Z"] = ang
+    cols["Vy"] = -r["Vz"]  # (v_r, v_theta) at angle pi/2 in Cartesian components
+    cols["Vz"] = r["Vy"]
+    rd.write_particles(f, r["charge"], r["mass"], r["weight"], cols, r["npar_normal"])
+    b = _FakeSim(delta=1)
+    rd.restore(b, str(tmp_path), 1)
+    x, y, vx, vy, vz = b.uploaded[1]
+    q = a.parts[1]
+    assert np.allclose(vy, q["vy"], rtol=1e-14, atol=1e-14) and np.allclose(vz, q["vz"], rtol=1e-14, atol=1e-14)
