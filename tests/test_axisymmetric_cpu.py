@@ -220,6 +220,32 @@ def test_axi_push_axial_field():
         m.close()
 
 
+def test_axi_push_radial_field_without_swirl():
+    """A uniform radial field and no azimuthal velocity: the move stays in
+    the r-z plane, so it is the 1-D leapfrog v_r += qm E_r dt, r += dt v_r
+    (the interface elements' PPR gradient carries the same field)."""
+    lz, rr = 2.0, 1.0
+    m = _AxiMesh(32, 16, lz, rr, (1, 1, 0, 1))
+    try:
+        p = _axi_parts(m, 300)
+        p["vz"][:] = 0.0
+        p["y"] = 0.2 + 0.3 * p["y"]  # off the axis: r stays positive over the step
+        p["loc"] = np.array([ob.load().or_locate(m.ptr, a, b) for a, b in zip(p["x"], p["y"])], np.int32)
+        p0 = {k: v.copy() for k, v in p.items()}
+        e1, qm, dt = 0.17, -1.0, 0.1
+        efx, efy = np.zeros(m.nn), np.full(m.nn, e1)
+        coef = np.zeros((5, m.nn))
+        coef[1] = -e1
+        ob.move_all_axi(m.ptr, p, efx, efy, np.ascontiguousarray(coef.ravel()), qm, dt)
+        assert np.all(p["loc"] >= 0)
+        vr = p0["vy"] + qm * e1 * dt
+        assert np.allclose(p["vy"], vr, rtol=0, atol=1e-15)
+        assert np.allclose(p["y"], p0["y"] + dt * vr, rtol=0, atol=1e-15)
+        assert np.all(p["vz"] == 0.0)
+    finally:
+        m.close()
+
+
 def test_axi_deposit_splits_a_uniform_ring_evenly():
     """Particles on a node line in z and uniform in r^2 across one element
     row (equal volume each) give its lower and upper nodes half the charge
