@@ -199,12 +199,13 @@ def cpu_baseline(cfg_name: str, sample_particles: int, steps: int, pcg_iters: in
     coef = np.zeros(5 * nn)
     t_part = t_field = 0.0
     note = ""
+    mover = ob.move_all_axi if cfg.delta == 1 else ob.move_all  # MoveOne's r-z or Cartesian branch
     for step in range(steps):
         t0 = time.perf_counter()
         qs, es, wq = [], [], []
         for s in range(2):
             qm = sp[s][0] / (sp[s][1] / deck.ME)
-            ob.move_all(mesh.ptr, parts[s], efx, efy, coef, qm, cfg.dt)
+            mover(mesh.ptr, parts[s], efx, efy, coef, qm, cfg.dt)
             q, e, _ = ob.deposit(mesh.ptr, parts[s], sp[s][1], sc["v_ref"], nn)
             qs.append(q)
             es.append(e)
