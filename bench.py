@@ -45,6 +45,9 @@ sys.path.insert(0, ROOT)
 METRIC = "particle pushes/s + Poisson ms/step: learned-precond FCG vs plain PCG at 1e-8"
 FP64_PUSH_BYTES = 80   # read x,y,vx,vy,elem (36 B) + vz on diagnostic steps, write x,y,vx,vy,elem (36 B)
 MIXED_PUSH_BYTES = 40  # read elem + 4 FP32 (20 B), write the same (20 B)
+# r-z decks (delta 1): v_theta is read and written on every step
+FP64_PUSH_BYTES_RZ = 88
+MIXED_PUSH_BYTES_RZ = 48
 # DRAM bytes per particle of one push launch measured by ncu (dram__bytes_read
 # + dram__bytes_write on the 1024^2 deck at 8 particles per cell; the traffic
 # grows in proportion to the particle count)
@@ -423,7 +426,11 @@ def run_ours(args, dist, rank, ws):
     # ---- roofline of the fused push kernel
     push_ms = sum(s.ms_push_kernel for s in stats) / len(stats)
     push_n = sum(s.pushed for s in stats) / len(stats)
-    push_bytes = MIXED_PUSH_BYTES if args.precision == "mixed" else FP64_PUSH_BYTES
+    rz = cfg.delta == 1
+    if args.precision == "mixed":
+        push_bytes = MIXED_PUSH_BYTES_RZ if rz else MIXED_PUSH_BYTES
+    else:
+        push_bytes = FP64_PUSH_BYTES_RZ if rz else FP64_PUSH_BYTES
     achieved = push_bytes * push_n / (push_ms / 1e3) / 1e9
     peaks = _peaks()
     if peaks and peaks.get("hbm_gbs"):
@@ -467,8 +474,10 @@ def run_ours(args, dist, rank, ws):
                      + " (fused push+locate+deposit)", "bound": "hbm",
                      "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
                      "peak_source": peak_src, "bytes_per_particle": push_bytes,
-                     "traffic": NCU_PUSH_TRAFFIC[args.precision] * push_n,
-                     "traffic_note": "ncu DRAM bytes/particle of a 6.4M-particle launch x particles per step"},
+                     # the ncu capture is of the Cartesian push; an r-z deck has none yet
+                     "traffic": None if rz else NCU_PUSH_TRAFFIC[args.precision] * push_n,
+                     "traffic_note": ("no ncu capture of the r-z push" if rz else
+                                      "ncu DRAM bytes/particle of a 6.4M-particle launch x particles per step")},
         "e2e": {"value": e2e_value, "unit": "particle pushes/s", "steps": e2e_steps,
                 "h2d_bytes_per_step": 8 * nn, "d2h_bytes_per_step": 4 * 8 * nn},
         "gpu_launches": int(launches),
