@@ -3,7 +3,7 @@
  *
  * Every entry point is plain C: pointers, sizes, return codes.  No torch or
  * CUDA types cross this boundary, so a Fortran main program binds it with
- * ISO_C_BINDING and Python binds it with ctypes.
+ * ISO_C_BINDING interface blocks and Python binds it with ctypes.
  *
  * Each entry point names the reference subroutine it replaces.  Paths are
  * relative to the PIC-IFE_GEC project of weqwoueu/pic-.
@@ -278,6 +278,11 @@ int pic_get_par_chg(int32_t delta, double *rho_out);
  * Phi_ref units; 0 switches it off and restores the static values.  The
  * reference's bc_value(1) = V/Phi_ref*SIN(2*Pi*Frequency*time*time_ref) on
  * the left boundary (IFE_Solve_2D.f90:104-121, commented out there).
+ * Deviation: the reference REPLACES the left wall's value by the sine (no
+ * static offset) and drives only the left wall; here the sine is ADDED to the
+ * wall's static value and either x wall may be driven.  The two agree when
+ * the driven wall's static value is 0, as on the r-z electrode deck; give the
+ * wall a static value of 0 in the deck to get the reference's form.
  * PIC_ERR_ARG for another wall or one that is not Dirichlet. */
 int pic_set_wall_rf(int32_t wall, double amplitude, double frequency_hz, double phase);
 
@@ -309,7 +314,13 @@ int pic_get_field(int32_t which, double *host_out);
 int pic_set_field(int32_t which, const double *host_in);
 
 /* Device pointers of the particle SoA, for zero-copy callers on the same
- * device.  Order: x, y, vx, vy, vz (double*), loc (int32*), id (uint32*). */
+ * device.  Order: x, y, vx, vy, vz (double*: absolute normalised position and
+ * velocity), loc (int32*), id (uint32*).  Only the PIC_PREC_FP64 layout is
+ * handed out.  With PIC_PREC_MIXED the same storage holds FP32 data (x, y the
+ * offsets inside element loc in element widths, [0, 1]; vx, vy, vz FP32
+ * velocities), which a caller expecting doubles would misread, so the call
+ * returns PIC_ERR_STATE there; pic_download_particles converts that layout
+ * back to FP64 positions. */
 int pic_particle_device_ptrs(int32_t species, void **ptrs7, int64_t *n_slots);
 
 /* Number of library kernels launched since init (for launch accounting). */
@@ -434,8 +445,16 @@ int pic_velocity_moments(int32_t species, int32_t nbins, int64_t *count, double 
  * array shared by every call on a device: calls that overlap on the GPU
  * (different streams, or several host threads) race on it.  The first call
  * on a device looks up the array's device address (cudaGetSymbolAddress); make
- * that first call before any stream capture.  Meshes above
- * PIC_NOALLOC_MAX_NODES nodes are rejected with PIC_ERR_ARG. */
+ * that first call before any stream capture.  The address is kept for the
+ * life of the process: after a cudaDeviceReset of that device, unload and
+ * reload the library before calling again.  Meshes above
+ * PIC_NOALLOC_MAX_NODES nodes are rejected with PIC_ERR_ARG.
+ *
+ * Scope: Cartesian meshes (delta 0) and FP64 absolute positions.  It matches
+ * pic_get_par_chg's rho_s bit for bit only on that path: it has no r-weighted
+ * (delta 1) weights, axis-row factor or L_ref^3 normalisation, and it reads
+ * x, y as doubles, so the FP32 offsets of a PIC_PREC_MIXED context are not
+ * valid input (pic_particle_device_ptrs refuses them). */
 int pic_deposit_noalloc(int32_t nnx, int32_t nny, double xmin, double xmax, double ymin,
                         double ymax, int64_t n, const double *x, const double *y,
                         const int32_t *loc, const double *cell_volume, double weight_charge,

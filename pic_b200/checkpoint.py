@@ -10,8 +10,11 @@ live particles (absolute FP64 position, velocity, element, id) and the id
 the next created particle receives.  Random numbers are counter-based
 (Philox keyed by seed, step and particle id), so nothing else carries state:
 a restored run continues bit for bit like the uninterrupted one.
-The deck is not stored; restore() checks that the mesh size, seed and
-precision of the deck it is given match the checkpoint's.
+The deck itself is not stored.  restore() checks that the deck it is given
+matches the checkpoint's: mesh size, seed, precision, and the physics the
+state depends on (Cartesian or r-z, extent, dt, n0, Te, gas, per-species
+charge, mass and macro-weight, the RF wall drive).  A mismatch raises
+ValueError before anything touches the device.
 """
 from __future__ import annotations
 
@@ -20,17 +23,35 @@ import ctypes as C
 import numpy as np
 
 from . import api
-from .deck import Config
+from .deck import Config, species_params
 from .simulation import Simulation
 
-_VERSION = 1
+_VERSION = 2
+
+
+def _physics(cfg: Config) -> np.ndarray:
+    """The deck's physics parameters the saved state depends on, as one
+    FP64 vector: geometry kind and extent, time step, reference density and
+    temperature, gas, per-species (charge, mass, weight), RF drive (wall,
+    volts, frequency, phase; NaN when static)."""
+    rf = list(cfg.rf) if cfg.rf is not None else [np.nan] * 4
+    rf = (rf + [0.0])[:4] if cfg.rf is not None and len(rf) == 3 else rf
+    sp, _ = species_params(cfg)
+    v = [cfg.delta, cfg.Lx, cfg.Ly, cfg.dt, cfg.n0, cfg.Te_eV, cfg.gas_p_Pa, cfg.gas_T_K]
+    for q, m, w, _ in sp:
+        v += [q, m, w]
+    return np.array(v + [float(x) for x in rf], dtype=np.float64)
+
+
+_PHYSICS_NAMES = ["delta", "Lx", "Ly", "dt", "n0", "Te_eV", "gas_p_Pa", "gas_T_K"]
 
 
 def save(sim: Simulation, path: str) -> None:
     out = {"version": np.int64(_VERSION), "step": np.int64(sim.step_index),
            "nnx": np.int64(sim.mesh.nnx), "nny": np.int64(sim.mesh.nny),
            "seed": np.uint64(sim.cfg.seed), "precision": np.int64(sim.cfg.precision),
-           "n_species": np.int64(len(sim.species)), "phi": sim.field("phi")}
+           "n_species": np.int64(len(sim.species)), "phi": sim.field("phi"),
+           "physics": _physics(sim.cfg)}
     for s in range(len(sim.species)):
         p = sim.download(s)
         for k, v in p.items():
@@ -51,6 +72,16 @@ def restore(cfg: Config, path: str, capacity_factor: float = 1.5, **sim_kw) -> S
     for k, v in want.items():
         if int(z[k]) != int(v):
             raise ValueError(f"checkpoint {k} = {int(z[k])} does not match the deck's {v}")
+    got, want_p = np.asarray(z["physics"]), _physics(cfg)
+    if got.shape != want_p.shape:
+        raise ValueError("checkpoint physics: another number of species or parameters than the deck's")
+    same = (got == want_p) | (np.isnan(got) & np.isnan(want_p))
+    if not same.all():
+        k = int(np.flatnonzero(~same)[0])
+        nsp = (got.size - len(_PHYSICS_NAMES) - 4) // 3
+        names = _PHYSICS_NAMES + [f"species{s}_{f}" for s in range(nsp) for f in ("charge", "mass", "weight")]
+        names += ["rf_wall", "rf_volts", "rf_frequency", "rf_phase"]
+        raise ValueError(f"checkpoint {names[k]} = {got[k]!r} does not match the deck's {want_p[k]!r}")
     ns = int(z["n_species"])
     counts = [z[f"s{s}_x"].size for s in range(ns)]
     sim = Simulation(cfg, load=False, capacity=[max(int(n * capacity_factor) + 1024, 1024) for n in counts],

@@ -11,9 +11,12 @@
 //
 // The arithmetic is the one of the GetParChg_2D path of libpicgpu (locate,
 // bilinear weights, 2^-40 fixed point, normalisation by the dual volume), so
-// the result equals pic_get_par_chg's per-species density bit for bit.
+// on a Cartesian mesh with FP64 positions the result equals pic_get_par_chg's
+// per-species density bit for bit.  It has no r-z (delta 1) weighting and
+// takes no FP32 element offsets (the mixed-precision particle layout).
 #include <cuda_runtime.h>
 
+#include <atomic>
 #include <cstdio>
 #include <string>
 
@@ -31,7 +34,10 @@ static __device__ __align__(256) unsigned long long g_noalloc_acc[PIC_NOALLOC_MA
 namespace {
 
 constexpr int kMaxDevices = 64;
-unsigned long long *g_acc_ptr[kMaxDevices] = {nullptr};
+// Device address of g_noalloc_acc per device ordinal, looked up on the first
+// call with that device current.  Atomic: host threads driving different
+// devices may make their first calls at the same time.
+std::atomic<unsigned long long *> g_acc_ptr[kMaxDevices];
 
 __global__ void k_na_clear(unsigned long long *acc, int64_t nn) {
   int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
@@ -106,13 +112,14 @@ extern "C" int pic_deposit_noalloc(int32_t nnx, int32_t nny, double xmin, double
   }
   // Set-up, once per device with that device current: the device address of
   // the scratch array (its host-side name is only a stand-in).
-  if (!g_acc_ptr[dev]) {
+  unsigned long long *acc = g_acc_ptr[dev].load(std::memory_order_acquire);
+  if (!acc) {
     void *ptr = nullptr;
     e = cudaGetSymbolAddress(&ptr, g_noalloc_acc);
     if (e != cudaSuccess) return na_fail(e, "cudaGetSymbolAddress");
-    g_acc_ptr[dev] = (unsigned long long *)ptr;
+    acc = (unsigned long long *)ptr;
+    g_acc_ptr[dev].store(acc, std::memory_order_release);
   }
-  unsigned long long *acc = g_acc_ptr[dev];
   cudaStream_t st = (cudaStream_t)stream;
   const double hx = (xmax - xmin) / (nnx - 1), hy = (ymax - ymin) / (nny - 1);
   k_na_clear<<<(unsigned)((nn + 255) / 256), 256, 0, st>>>(acc, nn);

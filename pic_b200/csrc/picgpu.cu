@@ -3808,6 +3808,15 @@ int pic_particle_device_ptrs(int32_t species, void **ptrs7, int64_t *n_slots) {
   int rc;
   if ((rc = check_init()) || (rc = check_species(species))) return rc;
   Species &s = g.sp[species];
+  if (s.f32) {
+    // The FP32 element-offset layout is not the documented double* one: hand
+    // it to no zero-copy caller (a deposit or diagnostic fed from it would
+    // read FP32 offsets as FP64 positions without any error).
+    set_error("pic_particle_device_ptrs: the particles are stored in the mixed-precision layout "
+              "(FP32 element offsets and velocities), not as FP64 positions; use "
+              "pic_download_particles");
+    return PIC_ERR_STATE;
+  }
   if (ptrs7) {
     ptrs7[0] = s.x; ptrs7[1] = s.y; ptrs7[2] = s.vx; ptrs7[3] = s.vy; ptrs7[4] = s.vz;
     ptrs7[5] = s.loc; ptrs7[6] = s.id;

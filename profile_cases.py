@@ -1,10 +1,10 @@
 """Small, self-contained workloads for profiling one part of the step under
 ncu (each runs a few launches of its kernels and exits):
 
-    python -m pic_b200.profile_cases step  <deck> <ppc> <steps> [jpcg|fcg|mg] [fp64|mixed]
-    python -m pic_b200.profile_cases solve <cells> [jpcg|fcg|mg] [repeats] [coarse_cells] [fp64|mixed] [omega] [max_coarse_nodes]
-    python -m pic_b200.profile_cases unet  <nodes> [repeats]
-    python -m pic_b200.profile_cases diag  <deck> <ppc> [fp64|mixed] [repeats]
+    python profile_cases.py step  <deck> <ppc> <steps> [jpcg|fcg|mg] [fp64|mixed]
+    python profile_cases.py solve <cells> [jpcg|fcg|mg] [repeats] [coarse_cells] [fp64|mixed] [omega] [max_coarse_nodes]
+    python profile_cases.py unet  <nodes> [repeats]
+    python profile_cases.py diag  <deck> <ppc> [fp64|mixed] [repeats]
 
 step:  the deck at <ppc> particles per cell and species, <steps> steps.
 solve: the 8-ellipse deck at <cells>^2 without particles, a seeded random
@@ -18,15 +18,18 @@ Each prints one line with its own CUDA-event time.
 from __future__ import annotations
 
 import ctypes as C
+import os
 import sys
+
+sys.path.insert(0, os.path.dirname(os.path.abspath(__file__)))
 
 import numpy as np
 
 
 def _step(deck_name, ppc, steps, solver="fcg", precision="fp64"):
     import torch
-    from . import api, deck
-    from .simulation import Simulation
+    from pic_b200 import api, deck
+    from pic_b200.simulation import Simulation
     prec = api.PIC_PREC_MIXED if precision == "mixed" else api.PIC_PREC_FP64
     cfg = deck.config(deck_name, ppc=int(ppc), precision=prec)
     sim = Simulation(cfg)
@@ -50,8 +53,8 @@ def _step(deck_name, ppc, steps, solver="fcg", precision="fp64"):
 def _solve(cells, solver="fcg", repeats=3, coarse_cells=64, precision="fp64", omega=2.0 / 3.0,
            max_coarse_nodes=4500):
     import torch
-    from . import api, deck
-    from .simulation import Simulation
+    from pic_b200 import api, deck
+    from pic_b200.simulation import Simulation
     n = int(cells)
     prec = api.PIC_PREC_MIXED if precision == "mixed" else api.PIC_PREC_FP64
     cfg = deck.config("cfg4", ncx=n, ncy=n, ppc=1, precision=prec)
@@ -83,7 +86,7 @@ def _solve(cells, solver="fcg", repeats=3, coarse_cells=64, precision="fp64", om
 
 def _unet(nodes, repeats=10):
     import torch
-    from . import unet
+    from pic_b200 import unet
     n = int(nodes)
     net = unet.UNet(seed=0)
     net._ensure(1, n, n)
@@ -102,8 +105,8 @@ def _unet(nodes, repeats=10):
 
 def _diag(deck_name, ppc, precision="mixed", repeats=5):
     import time
-    from . import api, deck
-    from .simulation import Simulation
+    from pic_b200 import api, deck
+    from pic_b200.simulation import Simulation
     prec = api.PIC_PREC_MIXED if precision == "mixed" else api.PIC_PREC_FP64
     sim = Simulation(deck.config(deck_name, ppc=int(ppc), precision=prec, diag_interval=1))
     sim.initial_fields()
@@ -126,5 +129,7 @@ def _diag(deck_name, ppc, precision="mixed", repeats=5):
 
 
 if __name__ == "__main__":
+    if len(sys.argv) < 2:
+        sys.exit(__doc__)
     case, rest = sys.argv[1], sys.argv[2:]
     {"step": _step, "solve": _solve, "unet": _unet, "diag": _diag}[case](*rest)

@@ -59,4 +59,9 @@ def main(root):
 
 
 if __name__ == "__main__":
-    main(sys.argv[1] if len(sys.argv) > 1 else "/root/reference/PIC-IFE_GEC")
+    # the PIC-IFE_GEC project directory of a checkout of weqwoueu/pic-
+    _root = sys.argv[1] if len(sys.argv) > 1 else os.environ.get("PIC_REFERENCE_ROOT")
+    if not _root:
+        sys.exit(f"usage: python {os.path.basename(__file__)} <path to PIC-IFE_GEC> "
+                 "(or set PIC_REFERENCE_ROOT)")
+    main(_root)

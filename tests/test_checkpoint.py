@@ -57,11 +57,32 @@ def test_restore_rejects_another_deck(tmp_path):
     """Checked before anything touches the device."""
     cfg = deck.config("cfg1")
     path = str(tmp_path / "other.npz")
-    np.savez(path, version=np.int64(1), step=np.int64(3), nnx=np.int64(cfg.ncx + 2),
+    np.savez(path, version=np.int64(checkpoint._VERSION), step=np.int64(3), nnx=np.int64(cfg.ncx + 2),
              nny=np.int64(cfg.ncy + 1), seed=np.uint64(cfg.seed), precision=np.int64(cfg.precision),
-             n_species=np.int64(2), phi=np.zeros(4))
+             n_species=np.int64(2), phi=np.zeros(4), physics=checkpoint._physics(cfg))
     with pytest.raises(ValueError, match="nnx"):
         checkpoint.restore(cfg, path)
-    np.savez(path, version=np.int64(2))
+    np.savez(path, version=np.int64(1))
     with pytest.raises(ValueError, match="version"):
+        checkpoint.restore(cfg, path)
+
+
+def _fake(path, cfg, physics):
+    np.savez(path, version=np.int64(checkpoint._VERSION), step=np.int64(3), nnx=np.int64(cfg.ncx + 1),
+             nny=np.int64(cfg.ncy + 1), seed=np.uint64(cfg.seed), precision=np.int64(cfg.precision),
+             n_species=np.int64(2), phi=np.zeros(4), physics=physics)
+
+
+@pytest.mark.parametrize("change,field", [
+    ({"delta": 1}, "delta"), ({"dt": 0.04}, "dt"), ({"n0": 2e15}, "n0"),
+    ({"ppc": 40}, "species0_weight"), ({"gas_p_Pa": 2.0}, "gas_p_Pa"),
+    ({"rf": (0, 100.0, 13.56e6)}, "rf_wall"),
+])
+def test_restore_rejects_other_physics_on_the_same_mesh(tmp_path, change, field):
+    """A checkpoint of a deck with the same mesh size and seed but other
+    physics is refused, naming the first parameter that differs."""
+    cfg = deck.config("cfg1")
+    path = str(tmp_path / "phys.npz")
+    _fake(path, deck.config("cfg1", **change), checkpoint._physics(deck.config("cfg1", **change)))
+    with pytest.raises(ValueError, match=field):
         checkpoint.restore(cfg, path)

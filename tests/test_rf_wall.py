@@ -3,7 +3,11 @@ bc_value(1) = V/Phi_ref*SIN(2*Pi*Frequency*time*time_ref) on the left
 Dirichlet boundary (IFE_Solve_2D.f90:104-121).  The wall's nodes carry
 static value + A sin(omega t + phase) into the RHS and into phi; the solve
 is bit-exact against the oracle given the same Dirichlet values, and the
-step drives it with t = step * dt."""
+step drives it with t = step * dt.
+
+The tiny deck's left wall has a static value of 5 V, so these tests pin the
+additive form (static + sine).  The reference's commented-out line replaces
+the wall value by the sine; the two coincide when the static value is 0."""
 import ctypes as C
 import math
 

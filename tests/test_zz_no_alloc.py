@@ -54,6 +54,24 @@ def test_noalloc_deposit_matches_get_par_chg():
         sim.close()
 
 
+def test_noalloc_inputs_refused_in_mixed_precision():
+    """A mixed-precision context stores FP32 element offsets where the FP64
+    layout keeps positions: its particle buffers are not valid input for the
+    allocation-free deposit, and the zero-copy pointer query refuses them
+    rather than hand out buffers that would be misread as doubles."""
+    lib = api.load()
+    sim = Simulation(deck.config("tiny", precision=api.PIC_PREC_MIXED))
+    try:
+        ptrs = (C.c_void_p * 7)()
+        nslots = C.c_int64()
+        rc = lib.pic_particle_device_ptrs(0, ptrs, C.byref(nslots))
+        assert rc == api.PIC_ERR_STATE, rc
+        assert b"mixed-precision layout" in lib.pic_last_error()
+        assert ptrs[0] is None  # nothing handed out
+    finally:
+        sim.close()
+
+
 def api_max_nodes():
     import os
     import re
