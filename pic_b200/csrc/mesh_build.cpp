@@ -550,9 +550,14 @@ int pic_mesh_build(const pic_deck *deck, pic_mesh_desc **out) {
         }
       } else {
         f.type = 2;
-        // cut edges opposite: choose r1 so that reference edges 1-2 and 4-3 are cut
+        // cut edges opposite; reference edges 1-2 and 4-3 are the cut ones.
+        // The reference's case table (El_Object_Intersection_info_2D_BL.f90)
+        // takes local corner 1 as reference vertex 1 when edges 1-2 and 3-4
+        // are cut, local corner 4 when edges 2-3 and 4-1 are.  The choice
+        // fixes the sub-triangles of the load-matrix quadrature, which is not
+        // exact for r-weighted integrands, so it is the reference's here.
         if (has_cut[0] && has_cut[2]) r1 = 0;
-        else if (has_cut[1] && has_cut[3]) r1 = 1;
+        else if (has_cut[1] && has_cut[3]) r1 = 3;
         else {
           pic::set_error("pic_mesh_build: saddle-type interface element is not supported");
           delete S;

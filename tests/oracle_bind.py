@@ -26,8 +26,8 @@ def load():
     global _lib
     if _lib is not None:
         return _lib
-    src = os.path.join(ORACLE_DIR, "oracle.c")
-    if not os.path.exists(ORACLE_LIB) or os.path.getmtime(ORACLE_LIB) < os.path.getmtime(src):
+    srcs = [os.path.join(ORACLE_DIR, f) for f in ("oracle.c", "oracle_mesh.c")]
+    if not os.path.exists(ORACLE_LIB) or os.path.getmtime(ORACLE_LIB) < max(map(os.path.getmtime, srcs)):
         subprocess.run(["make", "-s", "-C", ORACLE_DIR], check=True)
     lib = C.CDLL(ORACLE_LIB)
     M = _P(api.MeshDesc)
@@ -62,6 +62,11 @@ def load():
     lib.or_energy_spectrum.argtypes = [C.c_int64, _d, _d, _d, _i, C.c_double, C.c_double, C.c_int,
                                        C.c_double, C.c_double, _l, _l]
     lib.or_velocity_moments.argtypes = [C.c_int64, _d, _d, _d, _d, _i, C.c_int, _l, _d, _d]
+    lib.or_mesh_build.argtypes = [_P(api.Deck), C.c_int, _P(M)]
+    lib.or_mesh_build.restype = C.c_int
+    lib.or_mesh_free.argtypes = [M]
+    lib.or_mesh_interface.argtypes = [M, C.c_int32, _i, _i, _i, _d, _d, _d]
+    lib.or_quad_constants.argtypes = [C.c_int, _d]
     _lib = lib
     return lib
 
@@ -216,3 +221,63 @@ def velocity_moments(parts, nbins):
     load().or_velocity_moments(n, d(parts["x"]), d(parts["vx"]), d(parts["vy"]), d(parts["vz"]),
                                i32(parts["loc"]), nbins, i64(cnt), d(drift), d(thermal))
     return cnt, drift, thermal
+
+
+OR_QUAD_AS_COMPILED, OR_QUAD_EXACT = 0, 1
+
+
+class OracleMesh:
+    """The oracle's own mesh descriptor (or_mesh_build), built from the same
+    deck as the product's pic_mesh_build; same array() accessors as
+    pic_b200.deck.Mesh."""
+
+    def __init__(self, deck, quad=OR_QUAD_AS_COMPILED):
+        lib = load()
+        self.deck = deck
+        self.ptr = C.POINTER(api.MeshDesc)()
+        rc = lib.or_mesh_build(C.byref(deck), int(quad), C.byref(self.ptr))
+        if rc != 0:
+            raise RuntimeError(f"or_mesh_build failed ({rc})")
+        self.desc = self.ptr.contents
+        d = self.desc
+        self.nnx, self.nny = d.nnx, d.nny
+        self.nn = d.nnx * d.nny
+        self.ne = (d.nnx - 1) * (d.nny - 1)
+
+    def array(self, name):
+        d = self.desc
+        sizes = {"node_type": self.nn, "node_index": self.nn, "element_index": self.ne,
+                 "phi_dirichlet": self.nn, "cell_volume": self.nn,
+                 "a_srow": d.n_unknowns + 1, "a_jcol": d.nnz, "a_k": d.nnz,
+                 "xt_srow": d.n_unknowns + 1, "xt_jcol": d.nnz_xt, "xt_k": d.nnz_xt,
+                 "a_diag": d.n_unknowns, "rhs_fix": d.n_unknowns, "mass_q1": 16,
+                 "ife_mass": 16 * d.n_interface, "patch_ptr": self.nn + 1,
+                 "mass_rows": 16 * (self.nny - 1)}
+        n = int(self.array("patch_ptr")[-1]) if name == "patch_nodes" else sizes[name]
+        ptr = getattr(d, name)
+        dt = np.float64 if ptr._type_ is C.c_double else np.int32
+        return api.as_np(ptr, int(n), dt).copy()
+
+    def interface(self, k):
+        el, ty = C.c_int32(), C.c_int32()
+        r2l = np.zeros(4, np.int32)
+        beta, D, E = np.zeros(2), np.zeros(2), np.zeros(2)
+        load().or_mesh_interface(self.ptr, int(k), C.byref(el), C.byref(ty), i32(r2l), d(beta), d(D), d(E))
+        return {"element": el.value, "type": ty.value, "r2l": r2l, "beta": beta, "D": D, "E": E}
+
+    def close(self):
+        if self.ptr:
+            load().or_mesh_free(self.ptr)
+            self.ptr = C.POINTER(api.MeshDesc)()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+def quad_constants(quad):
+    out = np.zeros(9 + 18 + 9 + 18 + 4 + 8 + 1)
+    load().or_quad_constants(int(quad), d(out))
+    return out
