@@ -100,7 +100,9 @@ def build_table(bundle: dict, species: int, mass: float, gas_mass: float, n_gas:
     nr = len(reactions)
     sig = np.stack([sigma_table(r, emin, eint, nsigma) for r in reactions])  # [nr, ns]
     miu = mass * gas_mass / (mass + gas_mass)
-    energy = 10.0 ** (emin + np.arange(nsigma) * eint)
+    # 10^x per point through libm's pow, as the reference's 10.d0**x: numpy's
+    # vectorised power differs from it by an ulp at some grid energies
+    energy = np.array([math.pow(10.0, emin + i * eint) for i in range(nsigma)])
     v = np.sqrt(2.0 * energy * JTOEV / miu)
     prob = sig * v[None, :] * n_gas
     prob = np.cumsum(prob, axis=0)

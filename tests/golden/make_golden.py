@@ -7,6 +7,11 @@ committed outputs (weqwoueu/pic-, PIC-IFE_GEC):
   norm_error.json         <- Norm_Error_{0064,0128,0256}.txt (IFE L2/H1 errors)
   philox4x32_10_kat.json  <- known-answer vectors of Philox4x32-10 published
                              with the Random123 library (Salmon et al., SC'11)
+  pegasus_ar_digest.json  <- MCC_jw/gas/pegasus/Ar: per reaction of the e-Ar and
+                             Ar+-Ar bundles, the header fields and the raw
+                             (E, sigma) points summarised (count, sums, first and
+                             last rows) and the SHA-256 of the file, read with a
+                             token stream of its own (not the extractor's parser)
 
 Usage: python tests/golden/make_golden.py [/path/to/PIC-IFE_GEC]
 """
@@ -20,6 +25,43 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 
 def numbers(line):
     return [float(v.replace("D", "E")) for v in re.findall(r"[-+]?\d+\.\d*(?:[EeDd][-+]?\d+)?", line)]
+
+
+def _tokens(path):
+    """Whitespace tokens of a Pegasus file after its '#' comment lines, the
+    order LoadReactionOnePegasus (mc/ReactionOnePegasus.f90:92-110) reads."""
+    out = []
+    for line in open(path):
+        if line.lstrip().startswith("#"):
+            continue
+        out.extend(line.split())
+    return out
+
+
+def pegasus_digest(root):
+    import hashlib
+    gas = os.path.join(root, "MCC_jw", "gas", "pegasus", "Ar")
+    out = {}
+    for bundle in ("ElectronAr.txt", "Ar(+)Ar.txt"):
+        tok = open(os.path.join(gas, bundle)).read().split()
+        model, nr = int(tok[0]), int(tok[1])
+        files = [tok[2 + 3 * k] for k in range(nr)]
+        reactions = []
+        for f in files:
+            path = os.path.join(gas, f)
+            t = _tokens(path)
+            # Index, Name, Threshold, NSpecy, species(NSpecy), changes(NSpecy), type, n, pairs
+            ns = int(t[3])
+            rtype = int(t[4 + 2 * ns])
+            n = int(t[5 + 2 * ns])
+            vals = [float(v) for v in t[6 + 2 * ns:6 + 2 * ns + 2 * n]]
+            e, sg = vals[0::2], vals[1::2]
+            reactions.append({"file": f, "index": int(t[0]), "threshold": float(t[2]), "type": rtype,
+                              "n": n, "sum_e": sum(e), "sum_sigma_cm2": sum(sg), "first": [e[0], sg[0]],
+                              "last": [e[-1], sg[-1]],
+                              "sha256": hashlib.sha256(open(path, "rb").read()).hexdigest()})
+        out[bundle] = {"model": model, "reactions": reactions}
+    json.dump(out, open(os.path.join(HERE, "pegasus_ar_digest.json"), "w"), indent=1)
 
 
 def main(root):
@@ -56,6 +98,7 @@ def main(root):
          "out": [0xd16cfe09, 0x94fdcceb, 0x5001e420, 0x24126ea1]},
     ]
     json.dump(kat, open(os.path.join(HERE, "philox4x32_10_kat.json"), "w"), indent=1)
+    pegasus_digest(root)
 
 
 if __name__ == "__main__":

@@ -26,7 +26,7 @@ def load():
     global _lib
     if _lib is not None:
         return _lib
-    srcs = [os.path.join(ORACLE_DIR, f) for f in ("oracle.c", "oracle_mesh.c")]
+    srcs = [os.path.join(ORACLE_DIR, f) for f in ("oracle.c", "oracle_mesh.c", "oracle_tables.c")]
     if not os.path.exists(ORACLE_LIB) or os.path.getmtime(ORACLE_LIB) < max(map(os.path.getmtime, srcs)):
         subprocess.run(["make", "-s", "-C", ORACLE_DIR], check=True)
     lib = C.CDLL(ORACLE_LIB)
@@ -67,6 +67,10 @@ def load():
     lib.or_mesh_free.argtypes = [M]
     lib.or_mesh_interface.argtypes = [M, C.c_int32, _i, _i, _i, _d, _d, _d]
     lib.or_quad_constants.argtypes = [C.c_int, _d]
+    lib.or_mcc_sigma.argtypes = [C.c_int, _d, _d, C.c_double, C.c_double, C.c_double, C.c_int, _d]
+    lib.or_mcc_sigma.restype = C.c_int
+    lib.or_mcc_probability.argtypes = [C.c_int, C.c_int, _d, C.c_double, C.c_double, C.c_double, C.c_double,
+                                       C.c_double, C.c_double, C.c_double, C.c_double, _d, _d]
     _lib = lib
     return lib
 
@@ -281,3 +285,29 @@ def quad_constants(quad):
     out = np.zeros(9 + 18 + 9 + 18 + 4 + 8 + 1)
     load().or_quad_constants(int(quad), d(out))
     return out
+
+
+def mcc_table(bundle, mass, gas_mass, n_gas, dt_s, jtoev=1.6022e-19):
+    """The oracle's collision table for one raw bundle ({"model", "reactions":
+    [{"threshold", "table": [[E eV, sigma cm^2], ...]}]}): (sigma [nr][ns] in
+    m^2, prob [ns][nr], SigmaMax, CollisionRatio, EnergyMax).  The grid is
+    MCCSigma.f90:9-11's: 10001 points, log10 E over [-3, 3] (model 1) or
+    [-1, 3] (model 2)."""
+    lib = load()
+    emin, emax = (-3.0, 3.0) if bundle["model"] == 1 else (-1.0, 3.0)
+    ns = 10001
+    eint = (emax - emin) / (ns - 1)
+    nr = len(bundle["reactions"])
+    sig = np.zeros((nr, ns))
+    for j, r in enumerate(bundle["reactions"]):
+        raw = np.ascontiguousarray(np.array(r["table"], dtype=np.float64))
+        e, s = np.ascontiguousarray(raw[:, 0]), np.ascontiguousarray(raw[:, 1])
+        row = np.zeros(ns)
+        if lib.or_mcc_sigma(len(e), d(e), d(s), float(r["threshold"]), emin, eint, ns, d(row)) != 0:
+            raise RuntimeError("or_mcc_sigma")
+        sig[j] = row
+    prob = np.zeros((ns, nr))
+    o3 = np.zeros(3)
+    lib.or_mcc_probability(nr, ns, d(np.ascontiguousarray(sig)), mass, gas_mass, n_gas, emin, eint, emax,
+                           dt_s, jtoev, d(prob), d(o3))
+    return sig, prob, o3[0], o3[1], o3[2]
