@@ -177,12 +177,16 @@ def cpu_baseline(cfg_name: str, sample_particles: int, steps: int, pcg_iters: in
     iterations per step and its time is scaled to `pcg_iters` iterations (the
     count the reference's PCG needs for the step: the GPU Jacobi-PCG's, which
     runs the same algorithm, or one full oracle solve when None).  Returns
-    (pushes/s, description, seconds per step)."""
+    (pushes/s, description, seconds per step, threads, particles loaded).
+    Everything it runs is the oracle's: the mesh, interface geometry,
+    operator, load matrices, volumes and patches come from or_mesh_build
+    (with the quadrature constants as the reference compiles them), so this
+    leg loads no library of the product."""
     sys.path.insert(0, os.path.join(ROOT, "tests"))
     import oracle_bind as ob
     from pic_b200 import deck
     cfg = deck.config(cfg_name)
-    mesh = deck.Mesh(cfg)
+    mesh = ob.OracleMesh(deck.make_deck(cfg), ob.OR_QUAD_AS_COMPILED)
     sp, _ = deck.species_params(cfg)
     sc = cfg.scales
     nn = mesh.nn
@@ -238,8 +242,9 @@ def cpu_baseline(cfg_name: str, sample_particles: int, steps: int, pcg_iters: in
     desc = (f"{cfg.name}: {threads} host threads; push+deposit of {sample_n} of {full_n} particles for {steps} "
             f"step(s), extrapolated "
             f"by particle count; RHS+Jacobi-PCG+PPR on the full {cfg.ncx}x{cfg.ncy} mesh, the PCG timed over "
-            f"<= {pcg_cap} iterations and scaled to the step's {pcg_iters} iterations{note}")
-    return full_n / per_step, desc, per_step, threads
+            f"<= {pcg_cap} iterations and scaled to the step's {pcg_iters} iterations{note}; mesh and "
+            f"operator built by the oracle")
+    return full_n / per_step, desc, per_step, threads, full_n
 
 
 def run_reference(args, dist, rank, ws):
@@ -247,13 +252,16 @@ def run_reference(args, dist, rank, ws):
         return 0
     cpu_baseline(args.config, min(args.cpu_sample, 20000), 1, pcg_iters=1, pcg_cap=1)  # warm-up (caches)
     steps = max(1, args.steps)
-    v, desc, per_step, threads = cpu_baseline(args.config, args.cpu_sample, min(steps, 2))
+    v, desc, per_step, threads, n_loaded = cpu_baseline(args.config, args.cpu_sample, min(steps, 2))
+    from pic_b200 import deck
     line = {
         "impl": "reference", "metric": METRIC, "value": v, "unit": "particle pushes/s",
         "n_gpus": args.gpus, "steps": steps, "warmup": args.warmup,
         "ms_per_step": per_step * 1e3, "higher_is_better": True, "scaling": "weak",
-        "vs_baseline": None, "dtype": "f64", "data": "synthetic",
-        "config": {"workload": args.config},
+        "vs_baseline": None, "dtype": "f64",
+        "data": "synthetic (seeded uniform Maxwellian plasma, seeded objects)",
+        "config": _config(deck.config(args.config), "fp64", n_loaded, ws),
+        "solver": "jacobi_pcg",
         "cpu_baseline": {"value": v, "unit": "particle pushes/s", "cores": threads, "kind": "port",
                          "sample": desc},
         "e2e": {"value": v, "unit": "particle pushes/s", "h2d_bytes_per_step": 0,
@@ -301,6 +309,86 @@ def _poisson_compare(sim, lib, api, variants, repeats=3):
     return out
 
 
+def _config(cfg, precision: str, particles: int, ws: int) -> dict:
+    """The workload as both arms print it (same keys, same values)."""
+    soa = 48 if precision == "fp64" else 28  # bytes a particle holds in HBM (x, y, v, elem, id)
+    return {"workload": cfg.name, "cells": [cfg.ncx, cfg.ncy], "particles": int(particles),
+            "objects": len(cfg.objects), "geometry": "r-z" if cfg.delta == 1 else "x-y",
+            "precision": precision, "pcg_tol": cfg.pcg_tol, "sort_interval": cfg.sort_interval,
+            "mcc": bool(cfg.mcc), "parallelism": f"replicas x{ws}",
+            "l2": ("inputs larger than L2" if particles * soa > 126e6 else "inputs fit in L2, not flushed")
+                  + " (particle SoA %.2f GB)" % (particles * soa / 1e9)}
+
+
+def _push_roofline(precision: str, rz: bool, stats, peak, peak_src):
+    """Algorithmic bytes of the fused push per launch / its CUDA-event time."""
+    push_ms = sum(s.ms_push_kernel for s in stats) / len(stats)
+    push_n = sum(s.pushed for s in stats) / len(stats)
+    if precision == "mixed":
+        nbytes = MIXED_PUSH_BYTES_RZ if rz else MIXED_PUSH_BYTES
+        kernel = "k_push_mixed_tiled"
+    else:
+        nbytes = FP64_PUSH_BYTES_RZ if rz else FP64_PUSH_BYTES
+        kernel = "k_push"
+    achieved = nbytes * push_n / (push_ms / 1e3) / 1e9
+    tr = None if rz else NCU_PUSH_TRAFFIC[precision] * push_n
+    return {"kernel": kernel + (" r-z" if rz else "") + " (fused push+locate+deposit)", "bound": "hbm",
+            "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
+            "peak_source": peak_src, "bytes_per_particle": nbytes, "traffic": tr,
+            "traffic_note": ("no ncu capture of the r-z push" if rz else
+                             "ncu DRAM bytes/particle of a 6.4M-particle launch x particles per step")}, push_ms
+
+
+def _sel(sim, name, lp=None):
+    """Select a Poisson solver variant by its bench name (set_solver switches
+    the learned stage off; it is switched on after, for the learned variant)."""
+    if name == "jacobi_pcg":
+        sim.set_solver("jpcg")
+    elif name == "fcg_smooth_coarse":
+        sim.set_solver("fcg", coarse_cells=64, window=1)
+    elif name == "fcg_smooth_coarse_learned":
+        sim.set_solver("fcg", coarse_cells=64, window=4)
+    elif name == "fcg_smooth_coarse_fp32_iterations_in_fp64_refinement":
+        sim.set_solver("fcg", coarse_cells=64, window=1, inner_fp32=True)
+    elif name == "fcg_smooth_multigrid":
+        # damped-Jacobi weight 0.8 with the V-cycle: 11 iterations at 1024^2 against 12 with 2/3
+        sim.set_solver("fcg", window=1, multigrid=True, omega=0.8)
+    elif name == "fcg_smooth_multigrid_fp32_iterations_in_fp64_refinement":
+        sim.set_solver("fcg", window=1, multigrid=True, omega=0.8, inner_fp32=True)
+    else:
+        raise KeyError(name)
+    if lp is not None and name.endswith("_learned"):
+        lp.set_learned(True)
+
+
+def _side_run(name, precision, solver, steps, warmup, peak, peak_src, dist):
+    """A deck measured on its own simulation: setup, warm-up, timed steps."""
+    from pic_b200 import api, deck
+    from pic_b200.simulation import Simulation
+    cfg = deck.config(name, precision=api.PIC_PREC_MIXED if precision == "mixed" else api.PIC_PREC_FP64)
+    t0 = time.perf_counter()
+    sim = Simulation(cfg)
+    try:
+        sim.initial_fields()
+        n0 = sim.count(0) + sim.count(1)
+        setup_s = time.perf_counter() - t0
+        _sel(sim, solver)
+        for _ in range(warmup):
+            sim.step()
+        _barrier(dist)
+        ms, st = _timed_steps(sim, sim.lib, api, steps)
+        roof, push_ms = _push_roofline(precision, cfg.delta == 1, st, peak, peak_src)
+        pushed = sum(s.pushed for s in st)
+        return {"config": _config(cfg, precision, n0, 1), "solver": solver, "steps": steps,
+                "ms_per_step": ms / steps, "value": pushed / (ms / 1e3), "unit": "particle pushes/s",
+                "poisson_ms_per_step": sum(s.ms_solve for s in st) / steps,
+                "poisson_iterations_per_step": sum(s.solve.iterations for s in st) / steps,
+                "push_ms_per_step": push_ms, "mcc_ms_per_step": sum(s.ms_mcc for s in st) / steps,
+                "setup_s": setup_s, "roofline": roof}
+    finally:
+        sim.close()
+
+
 def run_ours(args, dist, rank, ws):
     import torch
     from pic_b200 import api, build, deck, unet
@@ -310,24 +398,20 @@ def run_ours(args, dist, rank, ws):
     dev = int(os.environ.get("LOCAL_RANK", "0"))
     if torch.cuda.is_available():
         torch.cuda.set_device(dev)
+    peaks = _peaks()
+    if peaks and peaks.get("hbm_gbs"):
+        peak, peak_src = peaks["hbm_gbs"], "measured"
+    else:
+        peak, peak_src = 6650.0, "fallback"
     cfg = deck.config(args.config)
     cfg.seed = cfg.seed + 1000 * rank
-    plain = None
-    if args.precision == "mixed":
-        # the plain FP64 Jacobi-PCG path runs on its own simulation first (the
-        # library holds one simulation at a time)
-        sim = Simulation(cfg)
-        sim.initial_fields()
-        sim.set_solver("jpcg")
-        sim.step()
-        _barrier(dist)
-        plain = _timed_steps(sim, sim.lib, api, max(1, args.plain_steps))
-        sim.close()
-    cfg.precision = api.PIC_PREC_MIXED if args.precision == "mixed" else api.PIC_PREC_FP64
+    prec = args.precision
+    cfg.precision = api.PIC_PREC_MIXED if prec == "mixed" else api.PIC_PREC_FP64
     t_setup = time.perf_counter()
     sim = Simulation(cfg)
     lib = sim.lib
     st0 = sim.initial_fields()
+    n_initial = sim.count(0) + sim.count(1)
     setup_s = time.perf_counter() - t_setup
     # ---- online training of the learned stage on Jacobi-PCG warm-up steps
     lp = None
@@ -340,50 +424,25 @@ def run_ours(args, dist, rank, ws):
             sim.step()
             lp.after_step(train_iters=8)
     train_s = time.perf_counter() - t_train
-
-    def sel_jpcg():
-        sim.set_solver("jpcg")
-
-    def sel_fcg():
-        sim.set_solver("fcg", coarse_cells=64, window=1)
-
-    def sel_learned():
-        sim.set_solver("fcg", coarse_cells=64, window=4)
-        lp.set_learned(True)
-
-    def sel_fcg32():
-        sim.set_solver("fcg", coarse_cells=64, window=1, inner_fp32=True)
-
-    # damped-Jacobi weight 0.8 with the V-cycle: 11 iterations at 1024^2
-    # against 12 with 2/3
-    def sel_mg():
-        sim.set_solver("fcg", window=1, multigrid=True, omega=0.8)
-
-    def sel_mg32():
-        sim.set_solver("fcg", window=1, multigrid=True, omega=0.8, inner_fp32=True)
-
-    variants = {"jacobi_pcg": sel_jpcg, "fcg_smooth_coarse": sel_fcg, "fcg_smooth_multigrid": sel_mg}
-    if args.precision == "mixed":
-        variants["fcg_smooth_coarse_fp32_iterations_in_fp64_refinement"] = sel_fcg32
-        variants["fcg_smooth_multigrid_fp32_iterations_in_fp64_refinement"] = sel_mg32
+    names = ["jacobi_pcg", "fcg_smooth_coarse", "fcg_smooth_multigrid"]
+    if prec == "mixed":
+        names += ["fcg_smooth_coarse_fp32_iterations_in_fp64_refinement",
+                  "fcg_smooth_multigrid_fp32_iterations_in_fp64_refinement"]
     if lp is not None:
-        variants["fcg_smooth_coarse_learned"] = sel_learned
+        names.append("fcg_smooth_coarse_learned")
+    variants = {k: (lambda k=k: _sel(sim, k, lp)) for k in names}
     poisson = _poisson_compare(sim, lib, api, variants)
     # product path: the fastest FCG variant that converged without falling back
     fcg_names = [k for k in variants if k != "jacobi_pcg" and poisson[k]["fallback"] == 0]
     best = min(fcg_names, key=lambda k: poisson[k]["ms"]) if fcg_names else "jacobi_pcg"
-    # ---- the plain FP64 GPU path (the reference's algorithms, Jacobi-PCG)
-    if plain is None:
-        sel_jpcg()
-        sim.step()
-        _barrier(dist)
-        plain = _timed_steps(sim, lib, api, max(1, args.plain_steps))
-    ms_plain, st_plain = plain
+    # ---- the plain path: the same particles with the reference's Jacobi-PCG
+    _sel(sim, "jacobi_pcg", lp)
+    sim.step()
+    _barrier(dist)
+    ms_plain, st_plain = _timed_steps(sim, lib, api, max(1, args.plain_steps))
     ms_plain_max = _max_over_ranks(dist, ms_plain)
     # ---- product path, device-resident timed region
-    variants[best]()
-    if lp is not None and best != "fcg_smooth_coarse_learned":
-        lp.set_learned(False)
+    _sel(sim, best, lp)
     with ClockSampler(dev) as clk:
         for _ in range(args.warmup):
             sim.step()
@@ -423,41 +482,25 @@ def run_ours(args, dist, rank, ws):
     _barrier(dist)
     ms_e2e_max = _max_over_ranks(dist, ms_e2e.value)
     e2e_value = _sum_over_ranks(dist, float(e2e_pushed)) / (ms_e2e_max / 1e3)
-    # ---- roofline of the fused push kernel
-    push_ms = sum(s.ms_push_kernel for s in stats) / len(stats)
-    push_n = sum(s.pushed for s in stats) / len(stats)
-    rz = cfg.delta == 1
-    if args.precision == "mixed":
-        push_bytes = MIXED_PUSH_BYTES_RZ if rz else MIXED_PUSH_BYTES
-    else:
-        push_bytes = FP64_PUSH_BYTES_RZ if rz else FP64_PUSH_BYTES
-    achieved = push_bytes * push_n / (push_ms / 1e3) / 1e9
-    peaks = _peaks()
-    if peaks and peaks.get("hbm_gbs"):
-        peak, peak_src = peaks["hbm_gbs"], "measured"
-    else:
-        peak, peak_src = 6650.0, "fallback"
+    roof, push_ms = _push_roofline(prec, cfg.delta == 1, stats, peak, peak_src)
     solve_ms = [s.ms_solve for s in stats]
     its = [s.solve.iterations for s in stats]
     ms_step = ms_total / args.steps
     plain_step = ms_plain_max / len(st_plain)
+    sim.close()
     line = {
         "metric": METRIC, "value": value, "unit": "particle pushes/s", "n_gpus": ws,
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms_step,
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
-        "dtype": "f32 particles/f64 fields" if args.precision == "mixed" else "f64",
+        "dtype": "f32 particles/f64 fields" if prec == "mixed" else "f64",
         "data": "synthetic (seeded uniform Maxwellian plasma, seeded objects)",
-        "config": {"workload": cfg.name, "cells": [cfg.ncx, cfg.ncy],
-                   "particles": int(stats[0].pushed), "objects": len(cfg.objects),
-                   "precision": args.precision, "solver": best, "pcg_tol": cfg.pcg_tol,
-                   "sort_interval": cfg.sort_interval, "mcc": bool(cfg.mcc),
-                   "parallelism": f"replicas x{ws}",
-                   "l2": "inputs larger than L2 (particle SoA %.1f GB)" % (push_n * 48 / 1e9)},
+        "config": _config(cfg, prec, n_initial, ws),
+        "solver": best,
         "poisson_ms_per_step": sum(solve_ms) / len(solve_ms),
         "poisson_iterations_per_step": sum(its) / len(its),
         "poisson_solvers_same_systems": poisson,
-        "plain_fp64_jacobi_pcg_path": {
-            "ms_per_step": plain_step, "steps": len(st_plain),
+        "plain_jacobi_pcg_path": {
+            "precision": prec, "ms_per_step": plain_step, "steps": len(st_plain),
             "poisson_ms_per_step": sum(s.ms_solve for s in st_plain) / len(st_plain),
             "pcg_iterations_per_step": sum(s.solve.iterations for s in st_plain) / len(st_plain),
             "speedup_of_product_path": plain_step / ms_step},
@@ -470,27 +513,103 @@ def run_ours(args, dist, rank, ws):
         "learned_training": None if lp is None else {
             "warmup_steps": args.train_steps, "adam_steps": len(lp.losses), "seconds": train_s,
             "loss_first": lp.losses[0], "loss_last": lp.losses[-1]},
-        "roofline": {"kernel": ("k_push_mixed_tiled" if args.precision == "mixed" else "k_push")
-                     + " (fused push+locate+deposit)", "bound": "hbm",
-                     "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
-                     "peak_source": peak_src, "bytes_per_particle": push_bytes,
-                     # the ncu capture is of the Cartesian push; an r-z deck has none yet
-                     "traffic": None if rz else NCU_PUSH_TRAFFIC[args.precision] * push_n,
-                     "traffic_note": ("no ncu capture of the r-z push" if rz else
-                                      "ncu DRAM bytes/particle of a 6.4M-particle launch x particles per step")},
+        "roofline": roof,
         "e2e": {"value": e2e_value, "unit": "particle pushes/s", "steps": e2e_steps,
                 "h2d_bytes_per_step": 8 * nn, "d2h_bytes_per_step": 4 * 8 * nn},
         "gpu_launches": int(launches),
         "clocks": clk.summary(),
     }
+    # ---- the north star's chosen form (mixed precision) and the other decks,
+    # each on its own simulation (one rank; untimed by the driver's ratio)
+    if rank == 0 and ws == 1 and not args.no_side_runs:
+        if prec == "fp64":
+            mixed = _side_run(args.config, "mixed", best, args.steps, args.warmup, peak, peak_src, None)
+            mixed["speedup_vs_plain_fp64_jacobi_pcg"] = plain_step / mixed["ms_per_step"]
+            line["mixed_precision_path"] = mixed
+        line["other_configs"] = {
+            "cfg2": _side_run("cfg2", "fp64", "jacobi_pcg", 5, 2, peak, peak_src, None),
+            "cfg5": _side_run("cfg5", "mixed", "fcg_smooth_multigrid", 5, 2, peak, peak_src, None)}
     if rank == 0 and ws == 1 and not args.no_cpu_baseline:
         jp = poisson["jacobi_pcg"]["iterations"]
-        v, desc, _, threads = cpu_baseline(args.config, args.cpu_sample, 1, pcg_iters=int(jp))
+        v, desc, _, threads, _ = cpu_baseline(args.config, args.cpu_sample, 1, pcg_iters=int(jp))
         line["cpu_baseline"] = {"value": v, "unit": "particle pushes/s", "cores": threads, "kind": "port",
                                 "sample": desc}
-    sim.close()
     if rank == 0:
         print(json.dumps(line), flush=True)
+    return 0
+
+
+def run_accuracy(args):
+    """The mixed-precision error table on one deck: the plain FP64 path
+    (FP64 particles, the reference's Jacobi-PCG; bit-exact with the oracle on
+    the small decks), FP64 particles with the product's multigrid FCG, and
+    the mixed-precision product path (element + FP32 offsets, multigrid FCG),
+    all from the same seed for the same steps.  At each checkpoint step: the
+    relative error (max |x - x_fp64| / max |x_fp64|) of phi, E and the
+    Average_x profiles (Output_To_Tecplot_IJK_2D.f90:166-226) of the ion
+    density and the electron mean energy (2/3 of it is the temperature).
+    Prints one JSON line."""
+    import torch
+    from pic_b200 import api, build, deck
+    from pic_b200.simulation import Simulation
+
+    build.build()
+    steps = args.acc_steps
+    checks = sorted({c for c in (20, 100, 500, steps) if c <= steps})
+
+    def run(precision, solver):
+        cfg = deck.config(args.accuracy, precision=precision, diag_interval=1)
+        sim = Simulation(cfg)
+        try:
+            sim.initial_fields()
+            if solver == "mg":
+                sim.set_solver("fcg", window=1, multigrid=True, omega=0.8)
+            else:
+                sim.set_solver("jpcg")
+            out, ms, its, done = {}, 0.0, 0, 0
+            for c in checks:
+                m, st = _timed_steps(sim, sim.lib, api, c - done)
+                ms += m
+                its += sum(s.solve.iterations for s in st)
+                done = c
+                avg = sim.average_x()
+                out[c] = {"phi": sim.field("phi"), "efx": sim.field("efx"), "efy": sim.field("efy"),
+                          "ion_density_profile": avg["Rho_" + sim.SPECIES_TAGS[1]].copy(),
+                          "electron_energy_profile": avg["Ek_" + sim.SPECIES_TAGS[0]].copy(),
+                          "counts": [sim.count(q) for q in range(2)]}
+            particles = sum(out[checks[0]]["counts"])
+            return out, {"ms_per_step": ms / steps, "poisson_iterations_per_step": its / steps,
+                         "particles_at_start": particles}
+        finally:
+            sim.close()
+
+    ref, t_ref = run(api.PIC_PREC_FP64, "jpcg")
+    f64mg, t_f64mg = run(api.PIC_PREC_FP64, "mg")
+    mix, t_mix = run(api.PIC_PREC_MIXED, "mg")
+    fields = ("phi", "efx", "efy", "ion_density_profile", "electron_energy_profile")
+
+    def table(other):
+        t = {}
+        for c in checks:
+            a, b = ref[c], other[c]
+            row = {f: float(np.abs(b[f] - a[f]).max() / np.abs(a[f]).max()) for f in fields}
+            row["counts_fp64"], row["counts"] = a["counts"], b["counts"]
+            t[str(c)] = row
+        return t
+
+    bars = {"phi": 1e-5, "ion_density_profile": 1e-2}
+    mixed = table(mix)
+    last = mixed[str(steps)]
+    line = {"accuracy": deck.config(args.accuracy).name, "steps": steps, "seed": deck.config(args.accuracy).seed,
+            "reference_path": "fp64 particles, Jacobi-PCG (MY_PCG), pcg_tol of the deck",
+            "errors_mixed_multigrid_vs_fp64_jpcg": mixed,
+            "errors_fp64_multigrid_vs_fp64_jpcg": table(f64mg),
+            "bars_at_last_step": bars,
+            "pass": {f: last[f] <= b for f, b in bars.items()},
+            "timing": {"fp64_jacobi_pcg": t_ref, "fp64_multigrid_fcg": t_f64mg, "mixed_multigrid_fcg": t_mix,
+                       "speedup_mixed_vs_plain_fp64": t_ref["ms_per_step"] / t_mix["ms_per_step"]},
+            "device": torch.cuda.get_device_name(0) if torch.cuda.is_available() else None}
+    print(json.dumps(line), flush=True)
     return 0
 
 
@@ -505,11 +624,19 @@ def main():
     ap.add_argument("--plain-steps", type=int, default=5,
                     help="steps of the plain FP64 Jacobi-PCG path timed for comparison")
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--precision", default="mixed", choices=["fp64", "mixed"],
-                    help="particles in FP64, or element + FP32 offsets and velocities")
+    ap.add_argument("--precision", default="fp64", choices=["fp64", "mixed"],
+                    help="particles in FP64 (the headline, like the reference), or element + FP32 "
+                         "offsets and velocities (then measured beside it)")
+    ap.add_argument("--no-side-runs", action="store_true",
+                    help="skip the mixed-precision path and the other decks")
     ap.add_argument("--cpu-sample", type=int, default=400000)
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--accuracy", default=None,
+                    help="print the mixed-precision error table of this deck (e.g. cfg3) instead of a bench line")
+    ap.add_argument("--acc-steps", type=int, default=1000)
     args = ap.parse_args()
+    if args.accuracy:
+        return run_accuracy(args)
     dist, rank, ws = _dist()
     try:
         if args.impl == "reference":

@@ -247,6 +247,8 @@ class OracleMesh:
         self.nnx, self.nny = d.nnx, d.nny
         self.nn = d.nnx * d.nny
         self.ne = (d.nnx - 1) * (d.nny - 1)
+        self.hx = (d.xmax - d.xmin) / (d.nnx - 1)
+        self.hy = (d.ymax - d.ymin) / (d.nny - 1)
 
     def array(self, name):
         d = self.desc

@@ -34,3 +34,25 @@ def test_clock_summary_nearest_sample_when_none_inside():
 
 def test_clock_summary_unsampled():
     assert bench.ClockSampler(0).summary()["reasons"] == ["unsampled"]
+
+
+def test_reference_arm_loads_only_the_oracle():
+    """bench.py --impl reference builds its mesh, operator and particles with
+    the oracle alone: the process maps no library of the product, and its
+    JSON line carries the same config keys as the product arm."""
+    import json
+    import subprocess
+    root = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+    code = ("import sys, os; sys.argv = ['bench.py', '--impl', 'reference', '--config', 'cfg1', "
+            "'--cpu-sample', '2000', '--steps', '1']; sys.path.insert(0, %r); import bench; bench.main(); "
+            "print('SO', sorted({l.split()[-1] for l in open('/proc/self/maps') "
+            "if l.rstrip().endswith('.so') and %r in l}))" % (root, root))
+    out = subprocess.run([sys.executable, "-c", code], capture_output=True, text=True, timeout=300, cwd=root)
+    assert out.returncode == 0, out.stderr[-2000:]
+    lines = out.stdout.strip().splitlines()
+    line = json.loads([l for l in lines if l.startswith("{")][0])
+    so = __import__("ast").literal_eval(lines[-1][3:])
+    assert so == [os.path.join(root, "oracle", "liboracle.so")], so
+    assert line["impl"] == "reference" and line["dtype"] == "f64"
+    assert set(line["config"]) >= {"workload", "cells", "particles", "precision", "pcg_tol", "mcc"}
+    assert line["config"]["particles"] > 300000 and line["value"] > 0
