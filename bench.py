@@ -348,6 +348,8 @@ def _sel(sim, name, lp=None):
         sim.set_solver("fcg", coarse_cells=64, window=1)
     elif name == "fcg_smooth_coarse_learned":
         sim.set_solver("fcg", coarse_cells=64, window=4)
+    elif name == "fcg_smooth_multigrid_learned":
+        sim.set_solver("fcg", window=4, multigrid=True, omega=0.8)
     elif name == "fcg_smooth_coarse_fp32_iterations_in_fp64_refinement":
         sim.set_solver("fcg", coarse_cells=64, window=1, inner_fp32=True)
     elif name == "fcg_smooth_multigrid":
@@ -417,7 +419,10 @@ def run_ours(args, dist, rank, ws):
     lp = None
     t_train = time.perf_counter()
     if args.train_steps > 0:
-        lp = unet.LearnedPreconditioner(sim, seed=rank, crop=128, batch=4, lr=2e-3, window=4)
+        # the network learns the error the multigrid V-cycle leaves (its
+        # training pairs pass through the same classical stages)
+        lp = unet.LearnedPreconditioner(sim, seed=rank, crop=128, batch=4, lr=2e-3, window=4,
+                                        multigrid=True, omega=0.8)
         sim.set_solver("jpcg")
         for _ in range(args.train_steps):
             lp.before_step()
@@ -429,7 +434,7 @@ def run_ours(args, dist, rank, ws):
         names += ["fcg_smooth_coarse_fp32_iterations_in_fp64_refinement",
                   "fcg_smooth_multigrid_fp32_iterations_in_fp64_refinement"]
     if lp is not None:
-        names.append("fcg_smooth_coarse_learned")
+        names.append("fcg_smooth_multigrid_learned")
     variants = {k: (lambda k=k: _sel(sim, k, lp)) for k in names}
     poisson = _poisson_compare(sim, lib, api, variants)
     # product path: the fastest FCG variant that converged without falling back

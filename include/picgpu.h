@@ -203,6 +203,14 @@ typedef struct pic_step_stats {
  * On success *out points at storage owned by the library until
  * pic_mesh_free(*out). */
 int pic_mesh_build(const pic_deck *deck, pic_mesh_desc **out);
+/* The same descriptor, with the interface elements' Q1 IFE basis, element
+ * stiffness and load matrices (Retangular_reference_basis_IFE.f90,
+ * Gauss_integration_local_stiffness_IFE.f90, IFE_RHS_2D.f90) computed in
+ * FP64 on the current CUDA device, one thread per interface element, by the
+ * same code the host builder runs: the result equals pic_mesh_build's bit
+ * for bit.  Allocates and frees its own device scratch; PIC_ERR_CUDA if no
+ * device is usable. */
+int pic_mesh_build_device(const pic_deck *deck, pic_mesh_desc **out);
 void pic_mesh_free(pic_mesh_desc *mesh);
 /* Interface-element geometry for diagnostics/tests: per interface element
  * (1-based id k) the element number, type (1 corner cut, 2 opposite edges),

@@ -31,7 +31,7 @@ ERRORS = {
 
 # every entry point declared in include/picgpu.h
 EXPORTS = [
-    "pic_mesh_build", "pic_mesh_free", "pic_mesh_interface_info", "pic_mesh_ife_basis",
+    "pic_mesh_build", "pic_mesh_build_device", "pic_mesh_free", "pic_mesh_interface_info", "pic_mesh_ife_basis",
     "pic_init", "pic_finalize", "pic_last_error", "pic_mcc_init", "pic_upload_particles",
     "pic_download_particles", "pic_particle_count", "pic_particle_positioning",
     "pic_sort_particles", "pic_move_all", "pic_get_par_chg", "pic_ife_solve",
@@ -149,6 +149,7 @@ def load() -> C.CDLL:
     lib.pic_last_error.restype = C.c_char_p
     lib.pic_kernel_launches.restype = C.c_int64
     lib.pic_mesh_build.argtypes = [_P(Deck), _P(_P(MeshDesc))]
+    lib.pic_mesh_build_device.argtypes = [_P(Deck), _P(_P(MeshDesc))]
     lib.pic_mesh_free.argtypes = [_P(MeshDesc)]
     lib.pic_mesh_free.restype = None
     lib.pic_mesh_interface_info.argtypes = [_P(MeshDesc), C.c_int32, _P(C.c_int32),

@@ -26,8 +26,9 @@ OBJ = os.path.join(HERE, "_obj")
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 
 LIBS = {
-    "libpicgpu.so": {"sources": ["picgpu.cu", "sort_mcc.cu", "precond.cu", "mesh_build.cpp", "noalloc.cu", "diag.cu"],
-                     "headers": ["csrc/pic_ctx.h", "csrc/pic_common.h", "csrc/pic_mcc_kin.h",
+    "libpicgpu.so": {"sources": ["picgpu.cu", "sort_mcc.cu", "precond.cu", "mesh_build.cpp", "ife_dev.cu", "noalloc.cu",
+                                 "diag.cu"],
+                     "headers": ["csrc/pic_ctx.h", "csrc/pic_common.h", "csrc/pic_mcc_kin.h", "csrc/ife_elem.h",
                                  "../include/picgpu.h"],
                      "flags": ["--fmad=false"], "cutlass": False},
     "libpicunet.so": {"sources": ["unet_conv.cu", "unet_ops.cu"], "headers": ["../include/picunet.h"],

@@ -214,28 +214,55 @@ __device__ __forceinline__ void warp_deposit(const SpK &s, int lane, int key, co
   if (lane == 0 && lm) atomicAdd(s.lost, (unsigned long long)__popc(lm));
   if (!do_deposit) return;
   const int key0 = __shfl_sync(0xffffffffu, key, 0);  // every lane, before any test
-  if (__all_sync(0xffffffffu, key >= 0 && key == key0)) {
-    // one element for the whole warp: exact integer warp sums with redux on
-    // the low 24 bits and the rest (values are non-negative; the sums fit in
-    // 32 bits for values below 2^51, i.e. particle energies below ~5e5 eV)
+  const int key31 = __shfl_sync(0xffffffffu, key, 31);
+  if (__all_sync(0xffffffffu, key < 0 || key == key0 || key == key31)) {
+    // at most two elements in the warp (a cell-sorted species' warp mostly
+    // holds one run, or the end of one and the start of the next; absorbed
+    // lanes carry nothing): exact integer sums over the full warp of the
+    // values masked to each element, by redux on the low 24 bits and the
+    // rest (values are non-negative; the sums fit in 32 bits for values below
+    // 2^51, i.e. particle energies below ~5e5 eV)
+    const int ka = key0 >= 0 ? key0 : key31, kb = key31;
+    if (ka < 0) return;  // every lane absorbed
+    const bool two = kb >= 0 && kb != ka;
+    const bool in_a = key == ka, in_b = two && key == kb;
+    const unsigned ma = __ballot_sync(0xffffffffu, in_a), mb = __ballot_sync(0xffffffffu, in_b);
+    const int lead_a = __ffs(ma) - 1, lead_b = two ? __ffs(mb) - 1 : -1;
     auto wsum = [&](long long v) {
       const unsigned lo = (unsigned)(v & 0xffffff), hi = (unsigned)(v >> 24);
       return ((long long)__reduce_add_sync(0xffffffffu, hi) << 24) + (long long)__reduce_add_sync(0xffffffffu, lo);
     };
-    long long qv[4];
+    long long va[4], vb[4];
 #pragma unroll
     for (int c = 0; c < 4; ++c)
-      if (!CONSERVE || c != 2) qv[c] = wsum(__double2ll_rn(W[c] * PIC_Q_SCALE));
-    if (CONSERVE) qv[2] = 32ll * (1ll << 40) - ((qv[0] + qv[1]) + qv[3]);
-    if (lane == 0)
+      if (!CONSERVE || c != 2) {
+        const long long v = (key >= 0) ? __double2ll_rn(W[c] * PIC_Q_SCALE) : 0ll;
+        va[c] = wsum(in_a ? v : 0ll);
+        vb[c] = two ? wsum(in_b ? v : 0ll) : 0ll;
+      }
+    if (CONSERVE) {
+      va[2] = (long long)__popc(ma) * (1ll << 40) - ((va[0] + va[1]) + va[3]);
+      vb[2] = (long long)__popc(mb) * (1ll << 40) - ((vb[0] + vb[1]) + vb[3]);
+    }
+    if (lane == lead_a)
 #pragma unroll
-      for (int c = 0; c < 4; ++c) atomicAdd(s.q_acc + nodes[c], (unsigned long long)qv[c]);
+      for (int c = 0; c < 4; ++c) atomicAdd(s.q_acc + nodes[c], (unsigned long long)va[c]);
+    if (lane == lead_b)
+#pragma unroll
+      for (int c = 0; c < 4; ++c) atomicAdd(s.q_acc + nodes[c], (unsigned long long)vb[c]);
     if (!do_energy) return;
 #pragma unroll
-    for (int c = 0; c < 4; ++c) qv[c] = wsum(__double2ll_rn((W[c] * energy) * PIC_E_SCALE));
-    if (lane == 0)
+    for (int c = 0; c < 4; ++c) {
+      const long long v = (key >= 0) ? __double2ll_rn((W[c] * energy) * PIC_E_SCALE) : 0ll;
+      va[c] = wsum(in_a ? v : 0ll);
+      vb[c] = two ? wsum(in_b ? v : 0ll) : 0ll;
+    }
+    if (lane == lead_a)
 #pragma unroll
-      for (int c = 0; c < 4; ++c) atomicAdd(s.e_acc + nodes[c], (unsigned long long)qv[c]);
+      for (int c = 0; c < 4; ++c) atomicAdd(s.e_acc + nodes[c], (unsigned long long)va[c]);
+    if (lane == lead_b)
+#pragma unroll
+      for (int c = 0; c < 4; ++c) atomicAdd(s.e_acc + nodes[c], (unsigned long long)vb[c]);
     return;
   }
   int prev = __shfl_up_sync(0xffffffffu, key, 1);
@@ -284,13 +311,110 @@ __device__ __forceinline__ void weights_axi(const MeshK &m, int e, double x, dou
   nodes[3] = n1 + 1;
 }
 
-// One particle per thread: gather E (old element), leapfrog push, wall/object
-// absorption, locate, fixed-point deposit of weight and weight*energy.
+// One live FP64 particle p (element e, position and velocity as loaded):
+// gather E (old element), leapfrog push, wall/object absorption, locate;
+// writes the particle back and returns what the warp deposit needs.
 // AXI (delta = 1, MoveOne.f90:213-263): x = z, y = r and the velocity held in
 // the particle's own frame (vx = v_z, vy = v_r, vz = v_theta); after the kick
 // the transverse move X = r + dt v_r, Y = dt v_theta gives r' = |(X, Y)| and
 // (v_r, v_theta) is rotated into the new frame by (X, Y)/r'; the deposit
 // weights are weights_axi.
+template <bool AXI>
+__device__ __forceinline__ void push_fp64_one(const MeshK &m, const FieldK &f, const PushK &prm, const SpK &s,
+                                              int64_t p, int e, double x, double y, double vx, double vy,
+                                              int &key, double W[4], int nodes[4], double &energy, bool &lost) {
+  if (prm.do_push) {
+    int ie, je;
+    bilinear(m, e, x, y, W, nodes, &ie, &je);
+    double Ex, Ey;
+    if (m.element_index[e] > 0) {
+      // Get_ParticleEField_PPR.f90:19-33: average of the PPR gradients of the
+      // element's outside nodes
+      double ex = 0.0, ey = 0.0;
+      int cnt = 0;
+      for (int c = 0; c < 4; ++c) {
+        int n = nodes[c];
+        if (m.node_index[n] == -1) {
+          ++cnt;
+          int ni = n / m.nny, nj = n - ni * m.nny;
+          double xr = x - m.xs[ni], yr = y - m.ys[nj];
+          ex = ((ex + f.c2[n]) + (2.0 * f.c4[n]) * xr) + f.c5[n] * yr;
+          ey = ((ey + f.c3[n]) + (2.0 * f.c6[n]) * yr) + f.c5[n] * xr;
+        }
+      }
+      ex = ex / (double)cnt;
+      ey = ey / (double)cnt;
+      Ex = -ex;
+      Ey = -ey;
+    } else {
+      Ex = ((W[0] * f.efx[nodes[0]] + W[1] * f.efx[nodes[1]]) + W[2] * f.efx[nodes[2]]) +
+           W[3] * f.efx[nodes[3]];
+      Ey = ((W[0] * f.efy[nodes[0]] + W[1] * f.efy[nodes[1]]) + W[2] * f.efy[nodes[2]]) +
+           W[3] * f.efy[nodes[3]];
+    }
+    vx = vx + (prm.qm * Ex) * prm.dt;
+    vy = vy + (prm.qm * Ey) * prm.dt;
+    if (AXI) {
+      double vt = s.vz[p];
+      double X = y + prm.dt * vy, Y = prm.dt * vt;
+      if (X == 0.0) X = m.hy * (double)1.0e-5f;
+      const double rn = sqrt(X * X + Y * Y), c = X / rn, sn = Y / rn;
+      const double vr = c * vy + sn * vt;
+      vt = c * vt - sn * vy;
+      vy = vr;
+      s.vz[p] = vt;
+      x = x + prm.dt * vx;
+      y = rn;
+    } else {
+      x = x + prm.dt * vx;
+      y = y + prm.dt * vy;
+    }
+    // walls: left, right, bottom (not the axis), top
+    if (x <= m.xmin) {
+      if (prm.wall[0] == PIC_WALL_REFLECT) { x = m.xmin + (m.xmin - x); vx = -vx; }
+      else lost = true;
+    } else if (x > m.xmax) {
+      if (prm.wall[1] == PIC_WALL_REFLECT) { x = m.xmax - (x - m.xmax); vx = -vx; }
+      else lost = true;
+    } else if (!AXI && y < m.ymin) {
+      if (prm.wall[2] == PIC_WALL_REFLECT) { y = m.ymin + (m.ymin - y); vy = -vy; }
+      else lost = true;
+    } else if (y > m.ymax) {
+      if (prm.wall[3] == PIC_WALL_REFLECT) { y = m.ymax - (y - m.ymax); vy = -vy; }
+      else lost = true;
+    }
+    if (!lost && absorbed_by_object(x, y)) lost = true;
+    s.x[p] = x;
+    s.y[p] = y;
+    s.vx[p] = vx;
+    s.vy[p] = vy;
+  }
+  if (lost) {
+    s.loc[p] = -1;
+  } else if (prm.do_deposit) {
+    int en = locate_elem(m, x, y);
+    if (en < 0) {
+      atomicAdd(s.bad, 1ull);
+      s.loc[p] = -1;
+      lost = true;
+    } else {
+      s.loc[p] = en;
+      key = en;
+      if (AXI) {
+        weights_axi(m, en, x, y, W, nodes);
+      } else {
+        int ie, je;
+        bilinear(m, en, x, y, W, nodes, &ie, &je);
+      }
+      double vz = prm.do_energy ? s.vz[p] : 0.0;
+      energy = ((((0.5 * prm.mass) * ((vx * vx + vy * vy) + vz * vz)) * prm.vref) * prm.vref) /
+               PIC_JTOEV;
+    }
+  }
+}
+
+// One particle per thread, loaded directly: push_fp64_one, then the warp's
+// fixed-point deposit of weight and weight*energy.
 template <bool AXI>
 __global__ void __launch_bounds__(256, 4) k_push(MeshK m, FieldK f, PushK prm, SpK s) {
   int64_t p = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
@@ -302,98 +426,7 @@ __global__ void __launch_bounds__(256, 4) k_push(MeshK m, FieldK f, PushK prm, S
   bool lost = false;
   if (p < s.n) {
     int e = s.loc[p];
-    if (e >= 0) {
-      double x = s.x[p], y = s.y[p];
-      double vx = s.vx[p], vy = s.vy[p];
-      if (prm.do_push) {
-        int ie, je;
-        bilinear(m, e, x, y, W, nodes, &ie, &je);
-        double Ex, Ey;
-        if (m.element_index[e] > 0) {
-          // Get_ParticleEField_PPR.f90:19-33: average of the PPR gradients of the
-          // element's outside nodes
-          double ex = 0.0, ey = 0.0;
-          int cnt = 0;
-          for (int c = 0; c < 4; ++c) {
-            int n = nodes[c];
-            if (m.node_index[n] == -1) {
-              ++cnt;
-              int ni = n / m.nny, nj = n - ni * m.nny;
-              double xr = x - m.xs[ni], yr = y - m.ys[nj];
-              ex = ((ex + f.c2[n]) + (2.0 * f.c4[n]) * xr) + f.c5[n] * yr;
-              ey = ((ey + f.c3[n]) + (2.0 * f.c6[n]) * yr) + f.c5[n] * xr;
-            }
-          }
-          ex = ex / (double)cnt;
-          ey = ey / (double)cnt;
-          Ex = -ex;
-          Ey = -ey;
-        } else {
-          Ex = ((W[0] * f.efx[nodes[0]] + W[1] * f.efx[nodes[1]]) + W[2] * f.efx[nodes[2]]) +
-               W[3] * f.efx[nodes[3]];
-          Ey = ((W[0] * f.efy[nodes[0]] + W[1] * f.efy[nodes[1]]) + W[2] * f.efy[nodes[2]]) +
-               W[3] * f.efy[nodes[3]];
-        }
-        vx = vx + (prm.qm * Ex) * prm.dt;
-        vy = vy + (prm.qm * Ey) * prm.dt;
-        if (AXI) {
-          double vt = s.vz[p];
-          double X = y + prm.dt * vy, Y = prm.dt * vt;
-          if (X == 0.0) X = m.hy * (double)1.0e-5f;
-          const double rn = sqrt(X * X + Y * Y), c = X / rn, sn = Y / rn;
-          const double vr = c * vy + sn * vt;
-          vt = c * vt - sn * vy;
-          vy = vr;
-          s.vz[p] = vt;
-          x = x + prm.dt * vx;
-          y = rn;
-        } else {
-          x = x + prm.dt * vx;
-          y = y + prm.dt * vy;
-        }
-        // walls: left, right, bottom (not the axis), top
-        if (x <= m.xmin) {
-          if (prm.wall[0] == PIC_WALL_REFLECT) { x = m.xmin + (m.xmin - x); vx = -vx; }
-          else lost = true;
-        } else if (x > m.xmax) {
-          if (prm.wall[1] == PIC_WALL_REFLECT) { x = m.xmax - (x - m.xmax); vx = -vx; }
-          else lost = true;
-        } else if (!AXI && y < m.ymin) {
-          if (prm.wall[2] == PIC_WALL_REFLECT) { y = m.ymin + (m.ymin - y); vy = -vy; }
-          else lost = true;
-        } else if (y > m.ymax) {
-          if (prm.wall[3] == PIC_WALL_REFLECT) { y = m.ymax - (y - m.ymax); vy = -vy; }
-          else lost = true;
-        }
-        if (!lost && absorbed_by_object(x, y)) lost = true;
-        s.x[p] = x;
-        s.y[p] = y;
-        s.vx[p] = vx;
-        s.vy[p] = vy;
-      }
-      if (lost) {
-        s.loc[p] = -1;
-      } else if (prm.do_deposit) {
-        int en = locate_elem(m, x, y);
-        if (en < 0) {
-          atomicAdd(s.bad, 1ull);
-          s.loc[p] = -1;
-          lost = true;
-        } else {
-          s.loc[p] = en;
-          key = en;
-          if (AXI) {
-            weights_axi(m, en, x, y, W, nodes);
-          } else {
-            int ie, je;
-            bilinear(m, en, x, y, W, nodes, &ie, &je);
-          }
-          double vz = prm.do_energy ? s.vz[p] : 0.0;
-          energy = ((((0.5 * prm.mass) * ((vx * vx + vy * vy) + vz * vz)) * prm.vref) * prm.vref) /
-                   PIC_JTOEV;
-        }
-      }
-    }
+    if (e >= 0) push_fp64_one<AXI>(m, f, prm, s, p, e, s.x[p], s.y[p], s.vx[p], s.vy[p], key, W, nodes, energy, lost);
   }
   warp_deposit(s, lane, key, W, nodes, energy, lost, prm.do_deposit, prm.do_energy);
 }
@@ -689,6 +722,77 @@ __global__ void __launch_bounds__(256, MINB) k_push_mixed_tiled(MeshK m, const f
                             C.vy[threadIdx.x], key, W, nodes, energy, lost);
     }
     warp_deposit<!AXI>(s, lane, key, W, nodes, energy, lost, prm.do_deposit, prm.do_energy);
+    __syncthreads();  // tile t is read before its stage is refilled
+  }
+  cp_async_wait<0>();
+}
+
+// ---- the FP64 push with the particle data staged through shared memory,
+// as k_push_mixed_tiled: persistent CTAs walk 256-particle tiles and copy the
+// next S-1 tiles' element and FP64 position and velocity (9 KB a tile) with
+// cp.async while they push the current one.  The per-particle code is
+// k_push's (push_fp64_one), so the results are the same bits.
+struct __align__(16) PushTile64 {
+  double x[kPushTile], y[kPushTile], vx[kPushTile], vy[kPushTile];
+  int32_t loc[kPushTile];
+};
+// 16-byte chunks of a tile: 4 x 128 for the doubles, 64 for the elements
+constexpr int kTile64Chunks = 4 * 128 + 64;
+
+__device__ __forceinline__ void push_tile64_chunk(PushTile64 *T, const SpK &s, int64_t base, int c) {
+  char *t = reinterpret_cast<char *>(T);
+  if (c < 512) {  // array c >> 7, chunk c & 127 (two doubles)
+    const int a = c >> 7, q = c & 127;
+    const double *arr = a == 0 ? s.x : a == 1 ? s.y : a == 2 ? s.vx : s.vy;
+    const int64_t first = base + 2 * q;
+    const int valid = (int)max((int64_t)0, min((int64_t)2, s.n - first));
+    cp_async16(t + 16 * c, reinterpret_cast<const char *>(arr) + (valid > 0 ? 8 * first : 0), 8 * valid);
+  } else {  // element ids, chunk c - 512 (four int32)
+    const int q = c - 512;
+    const int64_t first = base + 4 * q;
+    const int valid = (int)max((int64_t)0, min((int64_t)4, s.n - first));
+    cp_async16(t + 4 * 8 * kPushTile + 16 * q, reinterpret_cast<const char *>(s.loc) + (valid > 0 ? 4 * first : 0),
+               4 * valid);
+  }
+}
+
+__device__ __forceinline__ void push_tile64_load(PushTile64 *T, const SpK &s, int64_t base) {
+  for (int c = threadIdx.x; c < kTile64Chunks; c += kPushTile) push_tile64_chunk(T, s, base, c);
+}
+
+template <int S, bool AXI>
+__global__ void __launch_bounds__(256, 4) k_push_tiled(MeshK m, FieldK f, PushK prm, SpK s, int64_t ntiles) {
+  extern __shared__ __align__(16) unsigned char push_smem[];
+  PushTile64 *T = reinterpret_cast<PushTile64 *>(push_smem);
+  const int lane = threadIdx.x & 31;
+  const int64_t G = gridDim.x;
+#pragma unroll
+  for (int k = 0; k < S - 1; ++k) {
+    const int64_t t = blockIdx.x + k * G;
+    if (t < ntiles) push_tile64_load(&T[k], s, t * kPushTile);
+    cp_async_commit();
+  }
+  int it = 0;
+  for (int64_t t = blockIdx.x; t < ntiles; t += G, ++it) {
+    const int64_t tn = t + (S - 1) * G;
+    if (tn < ntiles) push_tile64_load(&T[(it + S - 1) % S], s, tn * kPushTile);
+    cp_async_commit();
+    cp_async_wait<S - 1>();  // this thread's copies of tile t are complete
+    __syncthreads();         // and every thread's
+    const PushTile64 &C = T[it % S];
+    const int64_t p = t * kPushTile + threadIdx.x;
+    int key = -1;
+    double W[4] = {0, 0, 0, 0};
+    int nodes[4] = {0, 0, 0, 0};
+    double energy = 0.0;
+    bool lost = false;
+    if (p < s.n) {
+      const int e = C.loc[threadIdx.x];
+      if (e >= 0)
+        push_fp64_one<AXI>(m, f, prm, s, p, e, C.x[threadIdx.x], C.y[threadIdx.x], C.vx[threadIdx.x],
+                           C.vy[threadIdx.x], key, W, nodes, energy, lost);
+    }
+    warp_deposit(s, lane, key, W, nodes, energy, lost, prm.do_deposit, prm.do_energy);
     __syncthreads();  // tile t is read before its stage is refilled
   }
   cp_async_wait<0>();
@@ -2326,6 +2430,14 @@ static int run_push(int sidx, bool do_push, bool do_deposit, bool do_energy) {
     } else {
       k_push_mixed<false><<<blocks_for(s.n_slots, 256), 256, 0, g.st>>>(m, g.d_coef32, pm, k);
     }
+  } else if (g.push64_grid > 0) {
+    const int64_t ntiles = (s.n_slots + kPushTile - 1) / kPushTile;
+    const unsigned grid = (unsigned)std::min<int64_t>(ntiles, g.push64_grid);
+    const size_t smem = 3 * sizeof(PushTile64);
+    if (g.axi)
+      k_push_tiled<3, true><<<grid, kPushTile, smem, g.st>>>(mesh_k(), f, prm, k, ntiles);
+    else
+      k_push_tiled<3, false><<<grid, kPushTile, smem, g.st>>>(mesh_k(), f, prm, k, ntiles);
   } else {
     if (g.axi)
       k_push<true><<<blocks_for(s.n_slots, 256), 256, 0, g.st>>>(mesh_k(), f, prm, k);
@@ -3624,6 +3736,17 @@ int pic_init(const pic_mesh_desc *mesh, const pic_params *params) {
                                                              (size_t)g.push_stages * sizeof(PushTile)));
       g.push_grid = per_sm * nsm;
       if (g.push_grid <= 0) g.push_stages = 0;
+    }
+    // FP64 push: particle tiles (9 KB each, 3 stages = 27 KB per CTA) staged
+    // through shared memory when PIC_PUSH64_TILED is 1; otherwise one
+    // particle per thread loaded directly (same bits either way)
+    const char *p64 = getenv("PIC_PUSH64_TILED");
+    g.push64_grid = 0;
+    if (p64 ? atoi(p64) == 1 : g.push64_default) {
+      const void *fn = g.axi ? (const void *)k_push_tiled<3, true> : (const void *)k_push_tiled<3, false>;
+      int per_sm = 0;
+      PIC_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, fn, kPushTile, 3 * sizeof(PushTile64)));
+      g.push64_grid = per_sm * nsm;
     }
   }
   if ((rc = dalloc(&g.d_counters, 32))) return rc;

@@ -207,15 +207,30 @@ def make_deck(cfg: Config) -> api.Deck:
     return d
 
 
-class Mesh:
-    """Mesh built by pic_mesh_build; owns the library storage."""
+def _cuda_visible() -> bool:
+    try:
+        import torch
+        return torch.cuda.is_available()
+    except ImportError:
+        return False
 
-    def __init__(self, cfg: Config):
+
+class Mesh:
+    """Mesh built by the library; owns the library storage.  device: the
+    interface elements' basis and element matrices computed on the CUDA device
+    (pic_mesh_build_device; the same bits as the host builder); None picks
+    the device when one is visible."""
+
+    def __init__(self, cfg: Config, device: bool | None = None):
         lib = api.load()
         self.cfg = cfg
         self.deck = make_deck(cfg)
         self.ptr = C.POINTER(api.MeshDesc)()
-        api.check(lib.pic_mesh_build(C.byref(self.deck), C.byref(self.ptr)), "pic_mesh_build")
+        if device is None:
+            device = _cuda_visible()
+        build = lib.pic_mesh_build_device if device else lib.pic_mesh_build
+        api.check(build(C.byref(self.deck), C.byref(self.ptr)),
+                  "pic_mesh_build_device" if device else "pic_mesh_build")
         self.desc = self.ptr.contents
         d = self.desc
         self.nnx, self.nny = d.nnx, d.nny

@@ -298,7 +298,8 @@ class LearnedPreconditioner:
 
     def __init__(self, sim, seed: int = 0, crop: int = 128, batch: int = 4, buffer: int = 32,
                  lr: float = 1e-3, synthetic: float = 0.5, smoothing: bool = True, omega: float = 2.0 / 3.0,
-                 coarse_cells: int = 64, window: int = 4, use_graph: bool = True):
+                 coarse_cells: int = 64, window: int = 4, use_graph: bool = True, multigrid: bool = False,
+                 max_coarse_nodes: int = 4500):
         import torch
         self.torch = torch
         self.sim = sim
@@ -344,7 +345,13 @@ class LearnedPreconditioner:
         self.phi_dev = torch.as_tensor(DeviceArray(phi.value, self.npix), device="cuda")
         self.smoothing, self.omega = int(smoothing), omega
         api.check(self.plib.pic_set_precond_stages(self.smoothing, omega, 1), "pic_set_precond_stages")
-        api.check(self.plib.pic_coarse_setup(sim.mesh.ptr, coarse_cells), "pic_coarse_setup")
+        # the classical coarse stage the network learns to complement: the
+        # two-level space, or the multigrid V-cycle
+        if multigrid:
+            api.check(self.plib.pic_multigrid_setup(sim.mesh.ptr, max_coarse_nodes), "pic_multigrid_setup")
+        else:
+            api.check(self.plib.pic_coarse_setup(sim.mesh.ptr, coarse_cells), "pic_coarse_setup")
+        self.multigrid = multigrid
         api.check(self.plib.pic_set_fcg_window(window), "pic_set_fcg_window")
         self._cb = api.PRECOND_FN(self._apply)
         api.check(self.plib.pic_set_preconditioner(self._cb, None), "pic_set_preconditioner")
