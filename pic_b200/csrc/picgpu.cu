@@ -161,6 +161,7 @@ struct SpK {
   unsigned long long *q_acc, *e_acc;
   unsigned long long *lost, *bad;
   int64_t n;
+  int pairs;  // warp deposit: 1 takes the full-warp path for up to two elements, 0 for one
 };
 
 __constant__ ObjK c_obj;
@@ -214,8 +215,8 @@ __device__ __forceinline__ void warp_deposit(const SpK &s, int lane, int key, co
   if (lane == 0 && lm) atomicAdd(s.lost, (unsigned long long)__popc(lm));
   if (!do_deposit) return;
   const int key0 = __shfl_sync(0xffffffffu, key, 0);  // every lane, before any test
-  const int key31 = __shfl_sync(0xffffffffu, key, 31);
-  if (__all_sync(0xffffffffu, key < 0 || key == key0 || key == key31)) {
+  const int key31 = s.pairs ? __shfl_sync(0xffffffffu, key, 31) : key0;
+  if (__all_sync(0xffffffffu, s.pairs ? (key < 0 || key == key0 || key == key31) : (key >= 0 && key == key0))) {
     // at most two elements in the warp (a cell-sorted species' warp mostly
     // holds one run, or the end of one and the start of the next; absorbed
     // lanes carry nothing): exact integer sums over the full warp of the
@@ -323,6 +324,7 @@ template <bool AXI>
 __device__ __forceinline__ void push_fp64_one(const MeshK &m, const FieldK &f, const PushK &prm, const SpK &s,
                                               int64_t p, int e, double x, double y, double vx, double vy,
                                               int &key, double W[4], int nodes[4], double &energy, bool &lost) {
+  int en = -2;  // the new element, once located
   if (prm.do_push) {
     int ie, je;
     bilinear(m, e, x, y, W, nodes, &ie, &je);
@@ -383,7 +385,13 @@ __device__ __forceinline__ void push_fp64_one(const MeshK &m, const FieldK &f, c
       if (prm.wall[3] == PIC_WALL_REFLECT) { y = m.ymax - (y - m.ymax); vy = -vy; }
       else lost = true;
     }
-    if (!lost && absorbed_by_object(x, y)) lost = true;
+    // objects: only a particle in an element whose box meets an object's
+    // bounding box (a flag built at init, with a cell of margin) can be
+    // inside one, so the exact test runs there only
+    if (!lost) {
+      en = locate_elem(m, x, y);
+      if ((en < 0 || m.elem_near[en]) && absorbed_by_object(x, y)) lost = true;
+    }
     s.x[p] = x;
     s.y[p] = y;
     s.vx[p] = vx;
@@ -392,7 +400,7 @@ __device__ __forceinline__ void push_fp64_one(const MeshK &m, const FieldK &f, c
   if (lost) {
     s.loc[p] = -1;
   } else if (prm.do_deposit) {
-    int en = locate_elem(m, x, y);
+    if (en == -2) en = locate_elem(m, x, y);
     if (en < 0) {
       atomicAdd(s.bad, 1ull);
       s.loc[p] = -1;
@@ -2387,6 +2395,7 @@ static int run_push(int sidx, bool do_push, bool do_deposit, bool do_energy) {
   for (int w = 0; w < 4; ++w) prm.wall[w] = g.P.wall_bc[w];
   SpK k{s.x, s.y, s.vx, s.vy, s.vz, s.loc, s.q_acc, s.e_acc, g.d_counters + 8 + sidx, g.d_counters + 1,
         s.n_slots};
+  k.pairs = g.dep_pairs;
   if (s.f32) {
     const MeshK m = mesh_k();
     PushM pm;
@@ -3740,6 +3749,8 @@ int pic_init(const pic_mesh_desc *mesh, const pic_params *params) {
     // FP64 push: particle tiles (9 KB each, 3 stages = 27 KB per CTA) staged
     // through shared memory when PIC_PUSH64_TILED is 1; otherwise one
     // particle per thread loaded directly (same bits either way)
+    const char *dp = getenv("PIC_DEPOSIT_PAIRS");  // 0: the full-warp deposit path for one element only
+    g.dep_pairs = (dp && atoi(dp) == 0) ? 0 : 1;
     const char *p64 = getenv("PIC_PUSH64_TILED");
     g.push64_grid = 0;
     if (p64 ? atoi(p64) == 1 : g.push64_default) {
