@@ -42,6 +42,16 @@ struct MgK {
   MgLevel lv[PIC_MG_MAX_LEVELS];
 };
 
+// (i, j) of node m, a node of the 3x3 neighbourhood of node n = (I, J) on a
+// grid of ny nodes per column, without an integer division: m - n = a ny + c
+// with a, c in {-1, 0, 1} (ny >= 3).
+__device__ __forceinline__ void mg_nb_ij(int64_t n, int I, int J, int64_t m, int ny, int &i, int &j) {
+  const int64_t d = m - n;
+  const int a = d >= ny - 1 ? 1 : (d <= 1 - ny ? -1 : 0);
+  i = I + a;
+  j = J + (int)(d - (int64_t)a * ny);
+}
+
 // r_l[I,J] = sum over the 3x3 finer nodes around (2I, 2J) of w_x w_y t[f],
 // w = 1 at the centre and 1/2 beside it (P^T of bilinear interpolation);
 // fixed order, rows then columns.
@@ -106,7 +116,7 @@ __device__ __forceinline__ void mg_smooth_node(const MgLevel &L, double w, int64
     L.t[n] = 0.0;
     return;
   }
-  const int I = (int)(n / L.ny), J = (int)(n - (int64_t)I * L.ny);
+  const int I = (int)n / L.ny, J = (int)n - I * L.ny;  // level grids hold < 2^31 nodes
   auto z = [&](int64_t m) { return (w * L.r[m]) * (double)L.dinv[m]; };
   L.z[n] = z(n);
   L.t[n] = L.r[n] - mg_apply(L, I, J, z);
@@ -120,9 +130,10 @@ __device__ __forceinline__ void mg_post_node(const MgLevel &L, const double *__r
     L.t[n] = 0.0;
     return;
   }
-  const int I = (int)(n / L.ny), J = (int)(n - (int64_t)I * L.ny);
+  const int I = (int)n / L.ny, J = (int)n - I * L.ny;
   auto y = [&](int64_t m) {
-    const int i = (int)(m / L.ny), j = (int)(m - (int64_t)i * L.ny);
+    int i, j;
+    mg_nb_ij(n, I, J, m, L.ny, i, j);
     return L.dinv[m] != 0.0f ? L.z[m] + mg_prolong(ec, nyc, i, j) : 0.0;
   };
   const double yn = y(n);

@@ -170,8 +170,7 @@ struct Ctx {
   int push_stages = 4, push_grid = 0;       // tiled mixed push stages (0: one particle per thread)
   int push_minb = 5;                        // resident CTAs per SM the 4-stage push is built for
   int push64_grid = 0;                      // tiled FP64 push: persistent CTAs (0: direct kernel)
-  int push64_default = 0;                   // tiled FP64 push unless PIC_PUSH64_TILED says otherwise
-  int dep_pairs = 1;                        // warp deposit's full-warp path for two elements (PIC_DEPOSIT_PAIRS)
+  int push64_default = 1;                   // tiled FP64 push unless PIC_PUSH64_TILED=0
   // CUDA graphs of one FCG iteration: [0] stage A, [1 + slot] stage B + FCG
   // kernels of ring slot `slot`; rebuilt when the configuration key changes
   cudaGraphExec_t fcg_graph[2 + PIC_FCG_MAX_WINDOW] = {};

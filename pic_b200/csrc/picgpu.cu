@@ -161,7 +161,6 @@ struct SpK {
   unsigned long long *q_acc, *e_acc;
   unsigned long long *lost, *bad;
   int64_t n;
-  int pairs;  // warp deposit: 1 takes the full-warp path for up to two elements, 0 for one
 };
 
 __constant__ ObjK c_obj;
@@ -215,55 +214,28 @@ __device__ __forceinline__ void warp_deposit(const SpK &s, int lane, int key, co
   if (lane == 0 && lm) atomicAdd(s.lost, (unsigned long long)__popc(lm));
   if (!do_deposit) return;
   const int key0 = __shfl_sync(0xffffffffu, key, 0);  // every lane, before any test
-  const int key31 = s.pairs ? __shfl_sync(0xffffffffu, key, 31) : key0;
-  if (__all_sync(0xffffffffu, s.pairs ? (key < 0 || key == key0 || key == key31) : (key >= 0 && key == key0))) {
-    // at most two elements in the warp (a cell-sorted species' warp mostly
-    // holds one run, or the end of one and the start of the next; absorbed
-    // lanes carry nothing): exact integer sums over the full warp of the
-    // values masked to each element, by redux on the low 24 bits and the
-    // rest (values are non-negative; the sums fit in 32 bits for values below
-    // 2^51, i.e. particle energies below ~5e5 eV)
-    const int ka = key0 >= 0 ? key0 : key31, kb = key31;
-    if (ka < 0) return;  // every lane absorbed
-    const bool two = kb >= 0 && kb != ka;
-    const bool in_a = key == ka, in_b = two && key == kb;
-    const unsigned ma = __ballot_sync(0xffffffffu, in_a), mb = __ballot_sync(0xffffffffu, in_b);
-    const int lead_a = __ffs(ma) - 1, lead_b = two ? __ffs(mb) - 1 : -1;
+  if (__all_sync(0xffffffffu, key >= 0 && key == key0)) {
+    // one element for the whole warp: exact integer warp sums with redux on
+    // the low 24 bits and the rest (values are non-negative; the sums fit in
+    // 32 bits for values below 2^51, i.e. particle energies below ~5e5 eV)
     auto wsum = [&](long long v) {
       const unsigned lo = (unsigned)(v & 0xffffff), hi = (unsigned)(v >> 24);
       return ((long long)__reduce_add_sync(0xffffffffu, hi) << 24) + (long long)__reduce_add_sync(0xffffffffu, lo);
     };
-    long long va[4], vb[4];
+    long long qv[4];
 #pragma unroll
     for (int c = 0; c < 4; ++c)
-      if (!CONSERVE || c != 2) {
-        const long long v = (key >= 0) ? __double2ll_rn(W[c] * PIC_Q_SCALE) : 0ll;
-        va[c] = wsum(in_a ? v : 0ll);
-        vb[c] = two ? wsum(in_b ? v : 0ll) : 0ll;
-      }
-    if (CONSERVE) {
-      va[2] = (long long)__popc(ma) * (1ll << 40) - ((va[0] + va[1]) + va[3]);
-      vb[2] = (long long)__popc(mb) * (1ll << 40) - ((vb[0] + vb[1]) + vb[3]);
-    }
-    if (lane == lead_a)
+      if (!CONSERVE || c != 2) qv[c] = wsum(__double2ll_rn(W[c] * PIC_Q_SCALE));
+    if (CONSERVE) qv[2] = 32ll * (1ll << 40) - ((qv[0] + qv[1]) + qv[3]);
+    if (lane == 0)
 #pragma unroll
-      for (int c = 0; c < 4; ++c) atomicAdd(s.q_acc + nodes[c], (unsigned long long)va[c]);
-    if (lane == lead_b)
-#pragma unroll
-      for (int c = 0; c < 4; ++c) atomicAdd(s.q_acc + nodes[c], (unsigned long long)vb[c]);
+      for (int c = 0; c < 4; ++c) atomicAdd(s.q_acc + nodes[c], (unsigned long long)qv[c]);
     if (!do_energy) return;
 #pragma unroll
-    for (int c = 0; c < 4; ++c) {
-      const long long v = (key >= 0) ? __double2ll_rn((W[c] * energy) * PIC_E_SCALE) : 0ll;
-      va[c] = wsum(in_a ? v : 0ll);
-      vb[c] = two ? wsum(in_b ? v : 0ll) : 0ll;
-    }
-    if (lane == lead_a)
+    for (int c = 0; c < 4; ++c) qv[c] = wsum(__double2ll_rn((W[c] * energy) * PIC_E_SCALE));
+    if (lane == 0)
 #pragma unroll
-      for (int c = 0; c < 4; ++c) atomicAdd(s.e_acc + nodes[c], (unsigned long long)va[c]);
-    if (lane == lead_b)
-#pragma unroll
-      for (int c = 0; c < 4; ++c) atomicAdd(s.e_acc + nodes[c], (unsigned long long)vb[c]);
+      for (int c = 0; c < 4; ++c) atomicAdd(s.e_acc + nodes[c], (unsigned long long)qv[c]);
     return;
   }
   int prev = __shfl_up_sync(0xffffffffu, key, 1);
@@ -1990,7 +1962,7 @@ __global__ void __launch_bounds__(kWide, 1) k_fcg_persist(FcgP<V> F) {
         const MgLevel &L = M.lv[l];
         const int64_t nl = (int64_t)L.nx * L.ny;
         for (int64_t n = gtid; n < nl; n += gth) {
-          const int I = (int)(n / L.ny), J = (int)(n - (int64_t)I * L.ny);
+          const int I = (int)n / L.ny, J = (int)n - I * L.ny;
           L.r[n] = l == 1 ? mg_restrict(F.t, F.nnx, k.nny, I, J)
                           : mg_restrict(M.lv[l - 1].t, M.lv[l - 1].nx, M.lv[l - 1].ny, I, J);
         }
@@ -2072,9 +2044,11 @@ __global__ void __launch_bounds__(kWide, 1) k_fcg_persist(FcgP<V> F) {
               // zA + P e_1 formed at each neighbour (0 on Dirichlet nodes)
               const double *e1 = mg_e(M, 1);
               const int ny1 = M.lv[1].ny;
+              const int I0 = (int)n / k.nny, J0 = (int)n - I0 * k.nny;  // the grid holds < 2^31 nodes
               auto za = [&](int64_t m) {
                 if (k.row_kind[m] < 0) return (V)0;
-                const int i = (int)(m / k.nny), j = (int)(m - (int64_t)i * k.nny);
+                int i, j;  // m is a stencil neighbour of n (multigrid set-up checks it)
+                mg_nb_ij(n, I0, J0, m, k.nny, i, j);
                 return (V)((double)F.zA[m] + mg_prolong(e1, ny1, i, j));
               };
               zf = vfma(om * F.dinv[n], r[n] - row_apply_v<V>(k, n, za), za(n));
@@ -2395,7 +2369,6 @@ static int run_push(int sidx, bool do_push, bool do_deposit, bool do_energy) {
   for (int w = 0; w < 4; ++w) prm.wall[w] = g.P.wall_bc[w];
   SpK k{s.x, s.y, s.vx, s.vy, s.vz, s.loc, s.q_acc, s.e_acc, g.d_counters + 8 + sidx, g.d_counters + 1,
         s.n_slots};
-  k.pairs = g.dep_pairs;
   if (s.f32) {
     const MeshK m = mesh_k();
     PushM pm;
@@ -3749,8 +3722,6 @@ int pic_init(const pic_mesh_desc *mesh, const pic_params *params) {
     // FP64 push: particle tiles (9 KB each, 3 stages = 27 KB per CTA) staged
     // through shared memory when PIC_PUSH64_TILED is 1; otherwise one
     // particle per thread loaded directly (same bits either way)
-    const char *dp = getenv("PIC_DEPOSIT_PAIRS");  // 0: the full-warp deposit path for one element only
-    g.dep_pairs = (dp && atoi(dp) == 0) ? 0 : 1;
     const char *p64 = getenv("PIC_PUSH64_TILED");
     g.push64_grid = 0;
     if (p64 ? atoi(p64) == 1 : g.push64_default) {
