@@ -49,9 +49,10 @@ MIXED_PUSH_BYTES = 40  # read elem + 4 FP32 (20 B), write the same (20 B)
 FP64_PUSH_BYTES_RZ = 88
 MIXED_PUSH_BYTES_RZ = 48
 # DRAM bytes per particle of one push launch measured by ncu (dram__bytes_read
-# + dram__bytes_write on the 1024^2 deck at 8 particles per cell; the traffic
-# grows in proportion to the particle count)
-NCU_PUSH_TRAFFIC = {"fp64": 68.0, "mixed": 38.3}
+# + dram__bytes_write; the traffic grows in proportion to the particle count):
+# the 1024^2 eight-ellipse deck at 8 particles per cell (FP64 k_push_tiled,
+# mixed k_push_mixed_tiled) and the 2048x1024 r-z deck at 8 (mixed r-z)
+NCU_PUSH_TRAFFIC = {"fp64": 68.1, "mixed": 38.3, "mixed_rz": 51.8}
 
 
 def _dist():
@@ -331,12 +332,14 @@ def _push_roofline(precision: str, rz: bool, stats, peak, peak_src):
         nbytes = FP64_PUSH_BYTES_RZ if rz else FP64_PUSH_BYTES
         kernel = "k_push"
     achieved = nbytes * push_n / (push_ms / 1e3) / 1e9
-    tr = None if rz else NCU_PUSH_TRAFFIC[precision] * push_n
+    key = precision + ("_rz" if rz else "")
+    tr = NCU_PUSH_TRAFFIC[key] * push_n if key in NCU_PUSH_TRAFFIC else None
     return {"kernel": kernel + (" r-z" if rz else "") + " (fused push+locate+deposit)", "bound": "hbm",
             "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
             "peak_source": peak_src, "bytes_per_particle": nbytes, "traffic": tr,
-            "traffic_note": ("no ncu capture of the r-z push" if rz else
-                             "ncu DRAM bytes/particle of a 6.4M-particle launch x particles per step")}, push_ms
+            "traffic_note": ("no ncu capture of this push" if tr is None else
+                             "ncu DRAM bytes/particle of one launch at 8 particles per cell (6.4M particles; "
+                             "r-z 16.7M) x particles per step")}, push_ms
 
 
 def _sel(sim, name, lp=None):
