@@ -163,8 +163,9 @@ struct Ctx {
   int pc_learned = 1;                       // apply the registered callback as stage 3
   int pc_cs = 0, pc_ncx = 0, pc_ncy = 0;    // coarse spacing in nodes (0: no coarse space)
   double *d_pc_t = nullptr, *d_pc_y = nullptr, *d_pc_za = nullptr, *d_pc_dinv = nullptr;
-  __half *d_pc_ainv = nullptr;             // coarse inverse / pc_ainv_scale, FP16, row-major
+  __half *d_pc_ainv = nullptr;             // coarse inverse / pc_ainv_scale, FP16, row-major, rows of pc_ainv_ld
   double pc_ainv_scale = 1.0;
+  int pc_ainv_ld = 0;                       // coarse inverse row length: coarse nodes rounded up to 8
   double *d_pc_rc = nullptr, *d_pc_ec = nullptr;
   MgK mg{};                                 // multigrid hierarchy (mg.L = 0: none)
   int push_stages = 4, push_grid = 0;       // tiled mixed push stages (0: one particle per thread)

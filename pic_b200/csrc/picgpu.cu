@@ -1827,8 +1827,9 @@ struct FcgP {
   const V *dinv;
   V *zA, *t, *zF, *P0, *P1, *Q0, *Q1;
   double *part;                  // [4][grid] partials: F p.q, F p.r, A r.r, E zF.Q
-  const __half *ainv;            // coarse inverse / ainv_scale
+  const __half *ainv;            // coarse inverse / ainv_scale, rows padded to ainv_ld (a multiple of 8)
   double ainv_scale;
+  int ainv_ld;
   double *rc, *ec;
   int nnx, cs, ncx, ncy, coarse;
   MgK mg;                        // multigrid V-cycle (mg.L > 1) in place of the two-level space
@@ -1882,8 +1883,51 @@ __device__ __forceinline__ V row_apply_v(const PcgK &k, int64_t n, F v) {
 // V = double: the FP64 solve.  V = float: the inner solve A e = r of the FP64
 // iterative refinement (vectors and coefficients FP32, dot products and the
 // coarse solve accumulated in FP64), started from e = 0.
+// ec = Ainv rc with the scaled FP16 inverse: the CTA stages rc in shared
+// memory (s_rc, ainv_ld doubles, zero past nc), each warp takes rows and each
+// lane reads eight coefficients (16 bytes) at a time, accumulating in FP64.
+// The caller separates it from the writes of rc by a grid barrier.
+template <class V>
+__device__ __forceinline__ void coarse_gemv(const FcgP<V> &F, int nc, double *s_rc, int gwarp, int nwarps,
+                                            int lane) {
+  const int ld = F.ainv_ld;
+  for (int q = threadIdx.x; q < ld; q += blockDim.x) s_rc[q] = q < nc ? __ldcg(F.rc + q) : 0.0;
+  __syncthreads();
+  const int nq = ld / 8;  // 16-byte groups of a row
+  for (int row = gwarp; row < nc; row += nwarps) {
+    const uint4 *arow = reinterpret_cast<const uint4 *>(F.ainv + (size_t)row * ld);
+    double acc = 0.0;
+    // four loads in flight per lane before their FMAs (the row comes from
+    // DRAM: one load at a time would make the row a chain of latencies)
+    for (int q0 = lane; q0 < nq; q0 += 4 * 32) {
+      uint4 v[4];
+#pragma unroll
+      for (int u = 0; u < 4; ++u) {
+        const int q = q0 + 32 * u;
+        v[u] = q < nq ? __ldg(arow + q) : make_uint4(0u, 0u, 0u, 0u);
+      }
+#pragma unroll
+      for (int u = 0; u < 4; ++u) {
+        const int q = q0 + 32 * u;
+        if (q >= nq) break;
+        const __half2 *h = reinterpret_cast<const __half2 *>(&v[u]);
+        const double *xr = s_rc + 8 * q;
+#pragma unroll
+        for (int c = 0; c < 4; ++c) {
+          const float2 f = __half22float2(h[c]);
+          acc = fma((double)f.x, xr[2 * c], acc);
+          acc = fma((double)f.y, xr[2 * c + 1], acc);
+        }
+      }
+    }
+    for (int off = 16; off > 0; off >>= 1) acc += __shfl_xor_sync(0xffffffffu, acc, off);
+    if (lane == 0) F.ec[row] = acc * F.ainv_scale;
+  }
+}
+
 template <class V>
 __global__ void __launch_bounds__(kWide, 1) k_fcg_persist(FcgP<V> F) {
+  extern __shared__ double fcg_smem[];  // the coarse right-hand side (coarse_gemv)
   const PcgK &k = F.k;
   FcgState *S = F.s;
   const int64_t nn = k.nn;
@@ -1973,13 +2017,7 @@ __global__ void __launch_bounds__(kWide, 1) k_fcg_persist(FcgP<V> F) {
         }
       }
       if (!ok) break;
-      for (int row = gwarp; row < nc; row += nwarps) {
-        const __half *arow = F.ainv + (size_t)row * nc;
-        double acc = 0.0;
-        for (int q = lane; q < nc; q += 32) acc = fma((double)__half2float(arow[q]), __ldcg(F.rc + q), acc);
-        for (int off = 16; off > 0; off >>= 1) acc += __shfl_xor_sync(0xffffffffu, acc, off);
-        if (lane == 0) F.ec[row] = acc * F.ainv_scale;
-      }
+      coarse_gemv(F, nc, fcg_smem, gwarp, nwarps, lane);
       for (int l = M.L - 2; l >= 1; --l) {
         if (!(ok = barrier())) break;
         const MgLevel &L = M.lv[l];
@@ -2007,13 +2045,7 @@ __global__ void __launch_bounds__(kWide, 1) k_fcg_persist(FcgP<V> F) {
       }
       if (!(ok = barrier())) break;
       // (C) coarse solve
-      for (int row = gwarp; row < nc; row += nwarps) {
-        const __half *arow = F.ainv + (size_t)row * nc;
-        double acc = 0.0;
-        for (int q = lane; q < nc; q += 32) acc = fma((double)__half2float(arow[q]), __ldcg(F.rc + q), acc);
-        for (int off = 16; off > 0; off >>= 1) acc += __shfl_xor_sync(0xffffffffu, acc, off);
-        if (lane == 0) F.ec[row] = acc * F.ainv_scale;
-      }
+      coarse_gemv(F, nc, fcg_smem, gwarp, nwarps, lane);
       if (!(ok = barrier())) break;
       // (D) prolongation
       for (int c = blockIdx.x; c < nb; c += gridDim.x) {
@@ -2032,6 +2064,20 @@ __global__ void __launch_bounds__(kWide, 1) k_fcg_persist(FcgP<V> F) {
       }
     }
     if (!(ok = barrier())) break;
+    if (M.L > 1) {
+      // (E1) zA += P e_1 once per unknown node (Dirichlet nodes keep 0), so
+      // that the post-smoothing reads it at its neighbours
+      const double *e1 = mg_e(M, 1);
+      const int ny1 = M.lv[1].ny;
+      for (int c = blockIdx.x; c < nb; c += gridDim.x) {
+        const int64_t n = (int64_t)c * kWide + threadIdx.x;
+        if (n < nn && k.row_kind[n] >= 0) {
+          const int i = (int)n / k.nny, j = (int)n - i * k.nny;  // the grid holds < 2^31 nodes
+          F.zA[n] = (V)((double)F.zA[n] + mg_prolong(e1, ny1, i, j));
+        }
+      }
+      if (!(ok = barrier())) break;
+    }
     // (E) post-smoothing and zF.Q_old (Q_old is this iteration's Ql)
     {
       double acc_zq = 0.0;
@@ -2040,22 +2086,8 @@ __global__ void __launch_bounds__(kWide, 1) k_fcg_persist(FcgP<V> F) {
         if (n < nn) {
           V zf = (V)0;
           if (k.row_kind[n] >= 0) {
-            if (M.L > 1) {
-              // zA + P e_1 formed at each neighbour (0 on Dirichlet nodes)
-              const double *e1 = mg_e(M, 1);
-              const int ny1 = M.lv[1].ny;
-              const int I0 = (int)n / k.nny, J0 = (int)n - I0 * k.nny;  // the grid holds < 2^31 nodes
-              auto za = [&](int64_t m) {
-                if (k.row_kind[m] < 0) return (V)0;
-                int i, j;  // m is a stencil neighbour of n (multigrid set-up checks it)
-                mg_nb_ij(n, I0, J0, m, k.nny, i, j);
-                return (V)((double)F.zA[m] + mg_prolong(e1, ny1, i, j));
-              };
-              zf = vfma(om * F.dinv[n], r[n] - row_apply_v<V>(k, n, za), za(n));
-            } else {
-              auto za = [&](int64_t m) { return F.zA[m]; };
-              zf = vfma(om * F.dinv[n], r[n] - row_apply_v<V>(k, n, za), za(n));
-            }
+            auto za = [&](int64_t m) { return F.zA[m]; };
+            zf = vfma(om * F.dinv[n], r[n] - row_apply_v<V>(k, n, za), za(n));
           }
           F.zF[n] = zf;
           if (have_old) acc_zq = fma((double)zf, (double)Ql[n], acc_zq);
@@ -2836,6 +2868,7 @@ static int run_fcg(pic_solve_stats *stats, int *fcg_iters, int *rc_out) {
       F.part = g.d_fcg_part;
       F.ainv = g.d_pc_ainv;
       F.ainv_scale = g.pc_ainv_scale;
+      F.ainv_ld = g.pc_ainv_ld;
       F.rc = g.d_pc_rc;
       F.ec = g.d_pc_ec;
       F.nnx = g.m.nnx;
@@ -2861,7 +2894,9 @@ static int run_fcg(pic_solve_stats *stats, int *fcg_iters, int *rc_out) {
     auto launch = [&](auto &F, const void *fn) -> int {
       PIC_CUDA(cudaMemsetAsync(g.d_bar, 0, 4 * sizeof(unsigned int), g.st));
       void *args[] = {&F};
-      PIC_CUDA(cudaLaunchCooperativeKernel(fn, dim3(g.fcg_coop_grid), dim3(kWide), args, 0, g.st));
+      const size_t smem = (size_t)g.pc_ainv_ld * sizeof(double);  // coarse_gemv's staging
+      PIC_CUDA(cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+      PIC_CUDA(cudaLaunchCooperativeKernel(fn, dim3(g.fcg_coop_grid), dim3(kWide), args, smem, g.st));
       PIC_LAUNCHED();
       return PIC_OK;
     };

@@ -62,13 +62,13 @@ __global__ void __launch_bounds__(PC_THREADS) k_pc_restrict(CoarseK c, const dou
   }
 }
 
-// ec = Ainv rc, one warp per row (row-major FP64 inverse)
-__global__ void k_pc_gemv(const __half *__restrict__ ainv, double scale, const double *__restrict__ rc,
+// ec = Ainv rc, one warp per row (row-major scaled FP16 inverse, rows of ld)
+__global__ void k_pc_gemv(const __half *__restrict__ ainv, int ld, double scale, const double *__restrict__ rc,
                           double *__restrict__ ec, int nc) {
   const int row = blockIdx.x * (blockDim.x / 32) + (threadIdx.x >> 5);
   const int lane = threadIdx.x & 31;
   if (row >= nc) return;
-  const __half *a = ainv + (size_t)row * nc;
+  const __half *a = ainv + (size_t)row * ld;
   double s = 0.0;
   for (int k = lane; k < nc; k += 32) s = fma((double)__half2float(a[k]), rc[k], s);
   for (int off = 16; off > 0; off >>= 1) s += __shfl_xor_sync(0xffffffffu, s, off);
@@ -165,7 +165,7 @@ int coarse_correct(const double *t, double *z, int assign) {
   const int nc = c.ncx * c.ncy;
   k_pc_restrict<<<nc, PC_THREADS, 0, g.st>>>(c, t, g.d_pc_rc);
   PIC_LAUNCHED();
-  k_pc_gemv<<<(nc + 7) / 8, 256, 0, g.st>>>(g.d_pc_ainv, g.pc_ainv_scale, g.d_pc_rc, g.d_pc_ec, nc);
+  k_pc_gemv<<<(nc + 7) / 8, 256, 0, g.st>>>(g.d_pc_ainv, g.pc_ainv_ld, g.pc_ainv_scale, g.d_pc_rc, g.d_pc_ec, nc);
   PIC_LAUNCHED();
   k_pc_prolong<<<blocks_for(g.nn, PC_THREADS), PC_THREADS, 0, g.st>>>(c, g.d_pc_ec, g.d_row_kind, assign, z,
                                                                         g.nn);
@@ -192,7 +192,7 @@ int mg_correct(const double *t, double *z, int assign) {
   }
   const MgLevel &C = M.lv[M.L - 1];
   const int nc = C.nx * C.ny;
-  k_pc_gemv<<<(nc + 7) / 8, 256, 0, g.st>>>(g.d_pc_ainv, g.pc_ainv_scale, C.r, C.z, nc);
+  k_pc_gemv<<<(nc + 7) / 8, 256, 0, g.st>>>(g.d_pc_ainv, g.pc_ainv_ld, g.pc_ainv_scale, C.r, C.z, nc);
   PIC_LAUNCHED();
   for (int l = M.L - 2; l >= 1; --l) {
     const MgLevel &L = M.lv[l];
@@ -237,9 +237,13 @@ __global__ void k_gj_update(double *__restrict__ A, int n, int k, const double *
 
 // FP16 copy of the inverse, divided by `scale` so the largest entry (on the
 // diagonal, as for any SPD matrix) sits near 2^14
-__global__ void k_to_f16(const double *__restrict__ a, __half *__restrict__ b, double inv_scale, int64_t n) {
+// b (rows of ld, zero past column n) = a (n x n) / scale, in FP16
+__global__ void k_to_f16(const double *__restrict__ a, __half *__restrict__ b, double inv_scale, int n, int ld) {
   const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
-  if (i < n) b[i] = __float2half_rn((float)(a[i] * inv_scale));
+  if (i >= (int64_t)n * ld) return;
+  const int64_t row = i / ld;
+  const int col = (int)(i - row * ld);
+  b[i] = col < n ? __float2half_rn((float)(a[row * n + col] * inv_scale)) : __float2half_rn(0.0f);
 }
 
 __global__ void k_diag_of(const double *__restrict__ a, double *__restrict__ d, int n) {
@@ -296,10 +300,13 @@ int dense_inverse_f16(const std::vector<double> &Ac, int nc, const char *who) {
   double dmax = 0.0;
   for (double v : dg) dmax = std::max(dmax, std::fabs(v));
   g.pc_ainv_scale = (dmax > 0.0) ? dmax / 16384.0 : 1.0;
-  rc = (e == cudaSuccess) ? pc_alloc(&g.d_pc_ainv, nc2) : cuda_fail(e, "coarse inverse diagonal");
+  // rows padded to a multiple of 8 coefficients (16 bytes) for vector loads
+  g.pc_ainv_ld = (nc + 7) & ~7;
+  const size_t nld = (size_t)nc * g.pc_ainv_ld;
+  rc = (e == cudaSuccess) ? pc_alloc(&g.d_pc_ainv, nld) : cuda_fail(e, "coarse inverse diagonal");
   if (!rc) {
-    k_to_f16<<<(unsigned)((nc2 + 255) / 256), 256, 0, g.st>>>(d_a, g.d_pc_ainv, 1.0 / g.pc_ainv_scale,
-                                                               (int64_t)nc2);
+    k_to_f16<<<(unsigned)((nld + 255) / 256), 256, 0, g.st>>>(d_a, g.d_pc_ainv, 1.0 / g.pc_ainv_scale, nc,
+                                                               g.pc_ainv_ld);
     e = cudaStreamSynchronize(g.st);
     if (e != cudaSuccess) rc = cuda_fail(e, "coarse inverse copy");
   }
