@@ -330,7 +330,7 @@ def _push_roofline(precision: str, rz: bool, stats, peak, peak_src):
         kernel = "k_push_mixed_tiled"
     else:
         nbytes = FP64_PUSH_BYTES_RZ if rz else FP64_PUSH_BYTES
-        kernel = "k_push"
+        kernel = "k_push_tiled"
     achieved = nbytes * push_n / (push_ms / 1e3) / 1e9
     key = precision + ("_rz" if rz else "")
     tr = NCU_PUSH_TRAFFIC[key] * push_n if key in NCU_PUSH_TRAFFIC else None

@@ -14,8 +14,8 @@
 //
 // One V-cycle, with damped Jacobi (weight w) as smoother, one sweep down and
 // one up at every level:
-//   down, l = 1..L-1:  r_l = P^T t_{l-1}
-//                      z_l = w D_l^-1 r_l,  t_l = r_l - A_l z_l      (l < L-1)
+//   down, l = 1..L-1:  r_l = P^T t_{l-1}, z_l = w D_l^-1 r_l (one pass)
+//                      t_l = r_l - A_l z_l                          (l < L-1)
 //                      z_{L-1} = A_{L-1}^-1 r_{L-1}                 (coarsest)
 //   up,   l = L-2..1:  y = z_l + P e_{l+1},  e_l = y + w D_l^-1 (r_l - A_l y)
 //   level 0:           zA += P e_1, then the solver's own post-smoothing.
@@ -107,18 +107,28 @@ __device__ __forceinline__ double mg_apply(const MgLevel &L, int I, int J, Fv v)
   return acc;
 }
 
-// down-sweep at node n: z = w D^-1 r, t = r - A z (z at the neighbours
-// formed from their r)
-__device__ __forceinline__ void mg_smooth_node(const MgLevel &L, double w, int64_t n) {
+// restriction at node n of a level that is smoothed next: r = P^T t_f and
+// z = w D^-1 r (0 on inactive nodes), so the down-sweep reads z at the
+// neighbours instead of forming it from their r and D^-1
+template <class T>
+__device__ __forceinline__ void mg_restrict_node(const MgLevel &L, const T *__restrict__ tf, int nxf, int nyf,
+                                                 double w, bool smoothed, int64_t n) {
+  const int I = (int)n / L.ny, J = (int)n - I * L.ny;  // level grids hold < 2^31 nodes
+  const double r = mg_restrict(tf, nxf, nyf, I, J);
+  L.r[n] = r;
+  if (smoothed) L.z[n] = (w * r) * (double)L.dinv[n];
+}
+
+// down-sweep at node n: t = r - A z with z = w D^-1 r stored by the
+// restriction (mg_restrict_node)
+__device__ __forceinline__ void mg_smooth_node(const MgLevel &L, int64_t n) {
   const double dn = (double)L.dinv[n];
   if (dn == 0.0) {
-    L.z[n] = 0.0;
     L.t[n] = 0.0;
     return;
   }
-  const int I = (int)n / L.ny, J = (int)n - I * L.ny;  // level grids hold < 2^31 nodes
-  auto z = [&](int64_t m) { return (w * L.r[m]) * (double)L.dinv[m]; };
-  L.z[n] = z(n);
+  const int I = (int)n / L.ny, J = (int)n - I * L.ny;
+  auto z = [&](int64_t m) { return L.z[m]; };
   L.t[n] = L.r[n] - mg_apply(L, I, J, z);
 }
 

@@ -1884,16 +1884,18 @@ __device__ __forceinline__ V row_apply_v(const PcgK &k, int64_t n, F v) {
 // iterative refinement (vectors and coefficients FP32, dot products and the
 // coarse solve accumulated in FP64), started from e = 0.
 // ec = Ainv rc with the scaled FP16 inverse: the CTA stages rc in shared
-// memory (s_rc, ainv_ld doubles, zero past nc), each warp takes rows and each
-// lane reads eight coefficients (16 bytes) at a time, accumulating in FP64.
-// The caller separates it from the writes of rc by a grid barrier.
+// memory (ainv_ld doubles, zero past nc) as eight planes, element 8q + k at
+// k*nq + q, so that the lanes of a warp, each reading the eight coefficients
+// of its 16-byte group q, read consecutive doubles of a plane (no bank
+// conflicts); each warp takes rows, accumulating in FP64.  The caller
+// separates it from the writes of rc by a grid barrier.
 template <class V>
 __device__ __forceinline__ void coarse_gemv(const FcgP<V> &F, int nc, double *s_rc, int gwarp, int nwarps,
                                             int lane) {
   const int ld = F.ainv_ld;
-  for (int q = threadIdx.x; q < ld; q += blockDim.x) s_rc[q] = q < nc ? __ldcg(F.rc + q) : 0.0;
-  __syncthreads();
   const int nq = ld / 8;  // 16-byte groups of a row
+  for (int i = threadIdx.x; i < ld; i += blockDim.x) s_rc[(i & 7) * nq + (i >> 3)] = i < nc ? __ldcg(F.rc + i) : 0.0;
+  __syncthreads();
   for (int row = gwarp; row < nc; row += nwarps) {
     const uint4 *arow = reinterpret_cast<const uint4 *>(F.ainv + (size_t)row * ld);
     double acc = 0.0;
@@ -1911,12 +1913,11 @@ __device__ __forceinline__ void coarse_gemv(const FcgP<V> &F, int nc, double *s_
         const int q = q0 + 32 * u;
         if (q >= nq) break;
         const __half2 *h = reinterpret_cast<const __half2 *>(&v[u]);
-        const double *xr = s_rc + 8 * q;
 #pragma unroll
         for (int c = 0; c < 4; ++c) {
           const float2 f = __half22float2(h[c]);
-          acc = fma((double)f.x, xr[2 * c], acc);
-          acc = fma((double)f.y, xr[2 * c + 1], acc);
+          acc = fma((double)f.x, s_rc[(2 * c) * nq + q], acc);
+          acc = fma((double)f.y, s_rc[(2 * c + 1) * nq + q], acc);
         }
       }
     }
@@ -2005,14 +2006,14 @@ __global__ void __launch_bounds__(kWide, 1) k_fcg_persist(FcgP<V> F) {
       for (int l = 1; l < M.L && ok; ++l) {
         const MgLevel &L = M.lv[l];
         const int64_t nl = (int64_t)L.nx * L.ny;
+        const bool smoothed = l < M.L - 1;
         for (int64_t n = gtid; n < nl; n += gth) {
-          const int I = (int)n / L.ny, J = (int)n - I * L.ny;
-          L.r[n] = l == 1 ? mg_restrict(F.t, F.nnx, k.nny, I, J)
-                          : mg_restrict(M.lv[l - 1].t, M.lv[l - 1].nx, M.lv[l - 1].ny, I, J);
+          if (l == 1) mg_restrict_node(L, F.t, F.nnx, k.nny, omega, smoothed, n);
+          else mg_restrict_node(L, M.lv[l - 1].t, M.lv[l - 1].nx, M.lv[l - 1].ny, omega, smoothed, n);
         }
         if (!(ok = barrier())) break;
-        if (l < M.L - 1) {
-          for (int64_t n = gtid; n < nl; n += gth) mg_smooth_node(L, omega, n);
+        if (smoothed) {
+          for (int64_t n = gtid; n < nl; n += gth) mg_smooth_node(L, n);
           if (!(ok = barrier())) break;
         }
       }

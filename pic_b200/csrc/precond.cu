@@ -99,16 +99,14 @@ __global__ void k_pc_prolong(CoarseK c, const double *__restrict__ ec, const int
 // ---- multigrid V-cycle, one launch per operation (the persistent solver
 // runs the same per-node functions between grid barriers)
 
-__global__ void k_mg_restrict(MgLevel L, const double *__restrict__ tf, int nxf, int nyf) {
+__global__ void k_mg_restrict(MgLevel L, const double *__restrict__ tf, int nxf, int nyf, double w, int smoothed) {
   const int64_t n = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
-  if (n >= (int64_t)L.nx * L.ny) return;
-  const int I = (int)(n / L.ny), J = (int)(n - (int64_t)I * L.ny);
-  L.r[n] = mg_restrict(tf, nxf, nyf, I, J);
+  if (n < (int64_t)L.nx * L.ny) mg_restrict_node(L, tf, nxf, nyf, w, smoothed != 0, n);
 }
 
-__global__ void k_mg_smooth(MgLevel L, double w) {
+__global__ void k_mg_smooth(MgLevel L) {
   const int64_t n = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
-  if (n < (int64_t)L.nx * L.ny) mg_smooth_node(L, w, n);
+  if (n < (int64_t)L.nx * L.ny) mg_smooth_node(L, n);
 }
 
 __global__ void k_mg_post(MgLevel L, const double *__restrict__ ec, int nyc, double w) {
@@ -183,10 +181,10 @@ int mg_correct(const double *t, double *z, int assign) {
     const int64_t nl = (int64_t)L.nx * L.ny;
     const double *tf = l == 1 ? t : M.lv[l - 1].t;
     const int nxf = l == 1 ? g.m.nnx : M.lv[l - 1].nx, nyf = l == 1 ? g.m.nny : M.lv[l - 1].ny;
-    k_mg_restrict<<<blocks_for(nl, PC_THREADS), PC_THREADS, 0, g.st>>>(L, tf, nxf, nyf);
+    k_mg_restrict<<<blocks_for(nl, PC_THREADS), PC_THREADS, 0, g.st>>>(L, tf, nxf, nyf, w, l < M.L - 1 ? 1 : 0);
     PIC_LAUNCHED();
     if (l < M.L - 1) {
-      k_mg_smooth<<<blocks_for(nl, PC_THREADS), PC_THREADS, 0, g.st>>>(L, w);
+      k_mg_smooth<<<blocks_for(nl, PC_THREADS), PC_THREADS, 0, g.st>>>(L);
       PIC_LAUNCHED();
     }
   }
