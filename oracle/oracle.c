@@ -320,8 +320,14 @@ int64_t or_deposit(const pic_mesh_desc *d, int64_t n, const double *x, const dou
     if (d->delta == 1) weights_axi(&m, e, x[p], y[p], W, nd);
     else weights(&m, e, x[p], y[p], W, nd);
     double energy = ((((0.5 * mass) * ((vx[p] * vx[p] + vy[p] * vy[p]) + vz[p] * vz[p])) * vref) * vref) / OR_JTOEV;
+    /* Cartesian weights sum to 1: corner 2 takes the rest of the particle's
+     * 2^40, so every particle deposits its charge exactly; the r-z weights
+     * (0.75 below on the axis row) round each corner on its own */
+    int64_t q[4];
+    for (int c = 0; c < 4; ++c) q[c] = llrint(W[c] * OR_QSCALE);
+    if (d->delta != 1) q[2] = ((int64_t)1 << 40) - ((q[0] + q[1]) + q[3]);
     for (int c = 0; c < 4; ++c) {
-      const int64_t dq = llrint(W[c] * OR_QSCALE), de = llrint((W[c] * energy) * OR_ESCALE);
+      const int64_t dq = q[c], de = llrint((W[c] * energy) * OR_ESCALE);
 #pragma omp atomic
       q_acc[nd[c]] += dq;
 #pragma omp atomic

@@ -10,7 +10,8 @@
 // of fixed size, so no call allocates or frees anything.
 //
 // The arithmetic is the one of the GetParChg_2D path of libpicgpu (locate,
-// bilinear weights, 2^-40 fixed point, normalisation by the dual volume), so
+// bilinear weights, 2^-40 fixed point with each particle depositing exactly
+// 2^40, normalisation by the dual volume), so
 // on a Cartesian mesh with FP64 positions the result equals pic_get_par_chg's
 // per-species density bit for bit.  It has no r-z (delta 1) weighting and
 // takes no FP32 element offsets (the mixed-precision particle layout).
@@ -66,8 +67,13 @@ __global__ void k_na_deposit(int nnx, int nny, double xmin, double ymin, double 
   double W[4] = {xc * yc, dx * yc, dx * dy, xc * dy};
   int64_t n1 = (int64_t)ie * nny + je;
   int64_t nodes[4] = {n1, n1 + nny, n1 + nny + 1, n1 + 1};
-  for (int c = 0; c < 4; ++c)
-    atomicAdd(acc + nodes[c], (unsigned long long)__double2ll_rn(W[c] * PIC_Q_SCALE));
+  // corner 2 takes the rest of the particle's 2^40, as pic_get_par_chg does
+  long long q[4];
+  q[0] = __double2ll_rn(W[0] * PIC_Q_SCALE);
+  q[1] = __double2ll_rn(W[1] * PIC_Q_SCALE);
+  q[3] = __double2ll_rn(W[3] * PIC_Q_SCALE);
+  q[2] = (1ll << 40) - ((q[0] + q[1]) + q[3]);
+  for (int c = 0; c < 4; ++c) atomicAdd(acc + nodes[c], (unsigned long long)q[c]);
 }
 
 __global__ void k_na_normalize(const unsigned long long *acc, const double *__restrict__ vol, double wq,

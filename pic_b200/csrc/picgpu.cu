@@ -201,12 +201,12 @@ __device__ __forceinline__ long long seg_sum(long long v, int lane, int seg_end)
 // element (particles are cell-sorted, so neighbouring lanes usually share an
 // element), then one atomic per node and value from the segment head.
 // Integer sums are exact: node totals do not depend on the segmentation.
-// CONSERVE (the Cartesian mixed-precision push): corner 2's charge is 2^40
-// minus the other three rounded corners, so every particle deposits exactly
-// 2^40 and a run of L particles 2^40 L minus three sums -- one 64-bit warp
-// sum fewer.  Without it (the FP64 path, bit-exact with the oracle, and the
-// r-z weights, which do not sum to 1 on the axis row) each corner is rounded
-// on its own.
+// CONSERVE (Cartesian meshes, FP64 and mixed precision): corner 2's charge
+// is 2^40 minus the other three rounded corners, so every particle deposits
+// exactly 2^40 and a run of L particles 2^40 L minus three sums -- one 64-bit
+// warp sum fewer (the oracle rounds the same way).  Without it (the r-z
+// weights, which do not sum to 1 on the axis row) each corner is rounded on
+// its own.
 template <bool CONSERVE = false>
 __device__ __forceinline__ void warp_deposit(const SpK &s, int lane, int key, const double W[4], const int nodes[4],
                                              double energy, bool lost, int do_deposit, int do_energy) {
@@ -408,7 +408,7 @@ __global__ void __launch_bounds__(256, 4) k_push(MeshK m, FieldK f, PushK prm, S
     int e = s.loc[p];
     if (e >= 0) push_fp64_one<AXI>(m, f, prm, s, p, e, s.x[p], s.y[p], s.vx[p], s.vy[p], key, W, nodes, energy, lost);
   }
-  warp_deposit(s, lane, key, W, nodes, energy, lost, prm.do_deposit, prm.do_energy);
+  warp_deposit<!AXI>(s, lane, key, W, nodes, energy, lost, prm.do_deposit, prm.do_energy);
 }
 
 struct PushM {
@@ -772,7 +772,7 @@ __global__ void __launch_bounds__(256, 4) k_push_tiled(MeshK m, FieldK f, PushK 
         push_fp64_one<AXI>(m, f, prm, s, p, e, C.x[threadIdx.x], C.y[threadIdx.x], C.vx[threadIdx.x],
                            C.vy[threadIdx.x], key, W, nodes, energy, lost);
     }
-    warp_deposit(s, lane, key, W, nodes, energy, lost, prm.do_deposit, prm.do_energy);
+    warp_deposit<!AXI>(s, lane, key, W, nodes, energy, lost, prm.do_deposit, prm.do_energy);
     __syncthreads();  // tile t is read before its stage is refilled
   }
   cp_async_wait<0>();

@@ -75,9 +75,10 @@ def test_mixed_push_and_deposit_match_fp64():
 
 
 def test_mixed_charge_is_conserved():
-    """Each particle deposits four fixed-point weights that sum to 2^40 within
-    2 units in either precision, so the total charge of the mixed path equals
-    the FP64 path's to that rounding (relative 1e-10)."""
+    """On a Cartesian mesh each particle deposits exactly 2^40 in either
+    precision (corner 2 takes the rest), so the total charge of the mixed
+    path equals the FP64 path's to the rounding of rho's normalisation
+    (relative 1e-10)."""
     def fn(sim):
         vol = sim.mesh.array("cell_volume")
         sim.get_par_chg()
