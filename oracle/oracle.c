@@ -694,6 +694,36 @@ static void scale(Rel *s, double v[3], double f) {
   v[0] *= f; v[1] *= f; v[2] *= f;
 }
 
+/* Selection keys of the null-collision candidates: two 32-bit round keys
+ * per (seed, step, species) from one Philox block (purpose byte 1, counter
+ * word 0 = 0), and per particle two rounds of C. Wellons' lowbias32 integer
+ * hash ("Prospecting for hash functions", 2018), each after an xor of a
+ * round key into the id.  A bijection of the id for a fixed step. */
+static uint32_t lowbias32(uint32_t x) {
+  x ^= x >> 16;
+  x *= 0x7feb352du;
+  x ^= x >> 15;
+  x *= 0x846ca68bu;
+  x ^= x >> 16;
+  return x;
+}
+static void select_round_keys(uint64_t seed, uint64_t step, int32_t species, uint32_t rk[2]) {
+  uint32_t key[2] = {(uint32_t)seed, (uint32_t)(seed >> 32)};
+  uint32_t c[4] = {0u, (uint32_t)step, (1u << 24) | ((uint32_t)species << 16), (uint32_t)(step >> 32)}, o[4];
+  or_philox(c, key, o);
+  rk[0] = o[0];
+  rk[1] = o[1];
+}
+static uint32_t select_key(uint32_t id, const uint32_t rk[2]) { return lowbias32(lowbias32(id ^ rk[0]) ^ rk[1]); }
+
+/* the selection keys of n ids at one step (for the statistical tests) */
+void or_mcc_select_keys(uint64_t seed, uint64_t step, int32_t species, int64_t n, const uint32_t *id,
+                        uint32_t *out) {
+  uint32_t rk[2];
+  select_round_keys(seed, step, species, rk);
+  for (int64_t i = 0; i < n; ++i) out[i] = select_key(id[i], rk);
+}
+
 static const uint64_t *g_key_arr;
 static int cmp_key(const void *a, const void *b) {
   uint64_t x = g_key_arr[*(const int64_t *)a], y = g_key_arr[*(const int64_t *)b];
@@ -727,15 +757,16 @@ int64_t or_mcc(const pic_mcc_table *t, const pic_gas *gas, double mass, double v
   for (int r = 0; r < t->n_reaction; ++r) out_counts[r] = 0;
   *n_new = 0;
   if (ncoll <= 0) return 0;
-  /* uniform random N-subset: smallest (Philox key, id) */
+  /* uniform random N-subset: smallest (key, id), the key a keyed hash of
+   * the id (or_mcc_select_keys) */
   uint64_t *k64 = malloc(8 * (size_t)n);
   int64_t *idx = malloc(8 * (size_t)npar);
   int64_t m = 0;
+  uint32_t rk[2];
+  select_round_keys(seed, step, species, rk);
   for (int64_t p = 0; p < n; ++p) {
     if (loc[p] < 0) continue;
-    uint32_t c[4] = {id[p], slo, (1u << 24) | ((uint32_t)species << 16), shi}, o[4];
-    or_philox(c, key, o);
-    k64[p] = ((uint64_t)o[0] << 32) | id[p];
+    k64[p] = ((uint64_t)select_key(id[p], rk) << 32) | id[p];
     idx[m++] = p;
   }
   g_key_arr = k64;

@@ -8,8 +8,9 @@ step index, phi (the solver's warm start; E and the PPR coefficients are
 recomputed from it, as the step itself computes them), and per species the
 live particles (absolute FP64 position, velocity, element, id) and the id
 the next created particle receives.  Random numbers are counter-based
-(Philox keyed by seed, step and particle id), so nothing else carries state:
-a restored run continues bit for bit like the uninterrupted one.
+(Philox, and the selection hash, keyed by seed, step and particle id), so
+nothing else carries state: a restored run continues bit for bit like the
+uninterrupted one.
 The deck itself is not stored.  restore() checks that the deck it is given
 matches the checkpoint's: mesh size, seed, precision, and the physics the
 state depends on (Cartesian or r-z, extent, dt, n0, Te, gas, per-species

@@ -78,7 +78,7 @@ PIC_HD double pic_u01(uint32_t a, uint32_t b) {
 }
 
 /* Purposes (third counter word, high byte) of the MCC draws. */
-#define PIC_RNG_SELECT 1u   /* selection key of null-collision candidates */
+#define PIC_RNG_SELECT 1u   /* round keys of the null-collision selection */
 #define PIC_RNG_RESIDUE 2u  /* Bernoulli residue of N_coll                 */
 #define PIC_RNG_COLLIDE 3u  /* draws of one collision (blocks of 4)        */
 #define PIC_RNG_LOAD 4u     /* particle loader                             */

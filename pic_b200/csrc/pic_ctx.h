@@ -197,16 +197,22 @@ struct Ctx {
   int32_t *d_sel = nullptr;            // selected slots
   uint64_t *d_cand = nullptr;          // candidates (key<<32 | id), slot in d_cand_slot
   int32_t *d_cand_slot = nullptr;
-  int64_t mcc_cap = 0;
-  int64_t *d_mcc_misc = nullptr;       // [16] counters
+  int64_t mcc_cap = 0;                 // d_sel entries; ionisation entries per species
+  int64_t cand_cap = 0;                // d_cand, d_cand_slot entries
+  int64_t *d_mcc_misc = nullptr;       // [16] counters per species
   uint64_t *d_mlist_key = nullptr;     // bounded selection: (key << 32 | id) below the bound
   int32_t *d_mlist_slot = nullptr;     //   and their slots
   int64_t mlist_cap = 0;
   int mcc_full = 0;                    // 1: always the full-histogram selection
   double mcc_bound_scale = 1.0;        // test hook: < 1 forces the bounded selection's fallback
-  int64_t *d_msel = nullptr;           // [8]: list count, keys below the bound, b*, count below b*
-  int64_t *d_ion_parent = nullptr;     // ionising parents: (id<<32 | slot)
+  int64_t *d_msel = nullptr;           // [8] per species: list count, keys below the bound, b*,
+                                       //   count below b*, selection held
+  int64_t *d_ion_parent = nullptr;     // ionising parents: (id<<32 | slot), mcc_cap per species
   double *d_ion_data = nullptr;        // per ionisation: new e- v(3), ion v(3)
+  void *h_ion = nullptr;               // pinned staging: ionisations read back
+  int64_t h_ion_cap = 0;
+  void *h_new = nullptr;               // pinned staging: created particles' slots and velocities
+  int64_t h_new_cap = 0;
   int32_t *d_mcc_pslot = nullptr;      // created particles: parent slots, velocities
   double *d_mcc_vel = nullptr;
   int64_t mcc_new_cap = 0;

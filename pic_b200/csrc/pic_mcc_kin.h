@@ -66,10 +66,35 @@ static inline McTable mc_table_from(const pic_mcc_table &t) {
   return m;
 }
 
-PIC_HD uint32_t mcc_select_key(uint32_t id, uint32_t slo, uint32_t shi, uint32_t sp, uint32_t k0,
-                               uint32_t k1) {
-  return pic_philox(id, slo, (PIC_RNG_SELECT << 24) | (sp << 16), shi, k0, k1).v[0];
+// Selection keys.  One Philox block per species and step draws two 32-bit
+// round keys; a particle's key is two rounds of the lowbias32 integer hash
+// (C. Wellons, "Prospecting for hash functions", 2018), each after an xor of
+// a round key into the id.  For a given step the key is a bijection of the
+// 32-bit id, so no two particles share a key, and it costs a dozen integer
+// instructions where a Philox block per particle costs about eighty: the
+// selection pass reads 8 bytes a particle and stays memory-bound.
+PIC_HD uint32_t mcc_hash32(uint32_t x) {
+  x ^= x >> 16;
+  x *= 0x7feb352du;
+  x ^= x >> 15;
+  x *= 0x846ca68bu;
+  x ^= x >> 16;
+  return x;
 }
+
+typedef struct McSelect {
+  uint32_t r0, r1;
+} McSelect;
+
+PIC_HD McSelect mcc_select_round_keys(uint32_t slo, uint32_t shi, uint32_t sp, uint32_t k0, uint32_t k1) {
+  const pic_u32x4 o = pic_philox(0u, slo, (PIC_RNG_SELECT << 24) | (sp << 16), shi, k0, k1);
+  McSelect r;
+  r.r0 = o.v[0];
+  r.r1 = o.v[1];
+  return r;
+}
+
+PIC_HD uint32_t mcc_select_key(uint32_t id, McSelect k) { return mcc_hash32(mcc_hash32(id ^ k.r0) ^ k.r1); }
 
 static inline int64_t mcc_n_collisions(int64_t npar, double ratio, uint32_t slo, uint32_t shi,
                                        uint32_t sp, uint32_t k0, uint32_t k1) {

@@ -185,15 +185,23 @@ __device__ __forceinline__ bool absorbed_by_object(double x, double y) {
   return false;
 }
 
-// Segmented warp sum of an int64 value over lanes [lane, seg_end] of one
-// segment (reduction toward the segment head).
-__device__ __forceinline__ long long seg_sum(long long v, int lane, int seg_end) {
+// Segmented warp sums of N int64 values over lanes [lane, seg_end] of one
+// segment (reduction toward the segment head).  After the steps off = 1, 2,
+// .., 2^(k-1) lane i holds the sum over [i, min(i + 2^k - 1, seg_end)], so
+// the steps stop once off reaches the warp's longest run `maxlen` (the same
+// for every lane): a warp of runs of at most 8 takes 3 steps instead of 5.
+template <int N>
+__device__ __forceinline__ void seg_sums(long long (&v)[N], int lane, int seg_end, int maxlen) {
 #pragma unroll
   for (int off = 1; off < 32; off <<= 1) {
-    long long o = __shfl_down_sync(0xffffffffu, v, off);
-    if (lane + off <= seg_end) v += o;
+    if (off >= maxlen) break;
+    const bool take = lane + off <= seg_end;
+#pragma unroll
+    for (int c = 0; c < N; ++c) {
+      const long long o = __shfl_down_sync(0xffffffffu, v[c], off);
+      if (take) v[c] += o;
+    }
   }
-  return v;
 }
 
 // Lost-particle count and fixed-point deposit of one warp's particles (key =
@@ -243,20 +251,31 @@ __device__ __forceinline__ void warp_deposit(const SpK &s, int lane, int key, co
   unsigned int heads = __ballot_sync(0xffffffffu, head);
   unsigned int above = (lane == 31) ? 0u : (heads & ~((2u << lane) - 1u));
   int seg_end = above ? (__ffs(above) - 2) : 31;
+  const int maxlen = (int)__reduce_max_sync(0xffffffffu, head ? (unsigned)(seg_end - lane + 1) : 0u);
   long long qv[4];
+  if (CONSERVE) {
+    long long q3[3];
 #pragma unroll
-  for (int c = 0; c < 4; ++c)
-    if (!CONSERVE || c != 2) qv[c] = seg_sum((key >= 0) ? __double2ll_rn(W[c] * PIC_Q_SCALE) : 0ll, lane, seg_end);
-  // the head's sums cover its run, lanes [lane, seg_end]
-  if (CONSERVE) qv[2] = (long long)(seg_end - lane + 1) * (1ll << 40) - ((qv[0] + qv[1]) + qv[3]);
+    for (int c = 0; c < 3; ++c) q3[c] = (key >= 0) ? __double2ll_rn(W[c == 2 ? 3 : c] * PIC_Q_SCALE) : 0ll;
+    seg_sums(q3, lane, seg_end, maxlen);
+    // the head's sums cover its run, lanes [lane, seg_end]
+    qv[0] = q3[0];
+    qv[1] = q3[1];
+    qv[3] = q3[2];
+    qv[2] = (long long)(seg_end - lane + 1) * (1ll << 40) - ((qv[0] + qv[1]) + qv[3]);
+  } else {
+#pragma unroll
+    for (int c = 0; c < 4; ++c) qv[c] = (key >= 0) ? __double2ll_rn(W[c] * PIC_Q_SCALE) : 0ll;
+    seg_sums(qv, lane, seg_end, maxlen);
+  }
   if (head && key >= 0)
 #pragma unroll
     for (int c = 0; c < 4; ++c) atomicAdd(s.q_acc + nodes[c], (unsigned long long)qv[c]);
   if (!do_energy) return;
   long long ev[4];
 #pragma unroll
-  for (int c = 0; c < 4; ++c)
-    ev[c] = seg_sum((key >= 0) ? __double2ll_rn((W[c] * energy) * PIC_E_SCALE) : 0ll, lane, seg_end);
+  for (int c = 0; c < 4; ++c) ev[c] = (key >= 0) ? __double2ll_rn((W[c] * energy) * PIC_E_SCALE) : 0ll;
+  seg_sums(ev, lane, seg_end, maxlen);
   if (head && key >= 0)
 #pragma unroll
     for (int c = 0; c < 4; ++c) atomicAdd(s.e_acc + nodes[c], (unsigned long long)ev[c]);
@@ -2354,6 +2373,8 @@ static void free_all() {
   F(g.d_cell_count); F(g.d_cell_start); F(g.d_cell_fill); F(g.d_perm); F(g.d_perm2); F(g.d_sort_id);
   F(g.d_scan_blk); F(g.d_counters); F(g.d_hist); F(g.d_sel); F(g.d_cand); F(g.d_cand_slot);
   F(g.d_mcc_misc); F(g.d_mlist_key); F(g.d_mlist_slot); F(g.d_msel); F(g.d_ion_parent); F(g.d_ion_data); F(g.d_mcc_pslot); F(g.d_mcc_vel);
+  if (g.h_ion) cudaFreeHost(g.h_ion);
+  if (g.h_new) cudaFreeHost(g.h_new);
   for (int s = 0; s < PIC_MAX_SPECIES; ++s) {
     Species &p = g.sp[s];
     F(p.x); F(p.y); F(p.vx); F(p.vy); F(p.vz); F(p.loc); F(p.id);

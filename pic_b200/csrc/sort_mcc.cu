@@ -7,10 +7,11 @@
 //
 // MCC: the reference picks N = INT(NPar*P_null) (+1 with probability equal to
 // the residue) distinct particles by a partial Fisher-Yates shuffle
-// (mc/MCCPublic.F90:113-171).  Here every live particle gets a Philox key
-// keyed by (seed, id, step, species); the N particles with the smallest
-// (key, id) are selected.  That is the same law -- a uniform random N-subset --
-// computed with a histogram instead of a serial shuffle.  The collision itself
+// (mc/MCCPublic.F90:113-171).  Here every live particle gets a 32-bit key,
+// a keyed hash of its id with round keys drawn from Philox per (seed, step,
+// species); the N particles with the smallest (key, id) are selected.  That
+// is the same law -- a uniform random N-subset -- computed with a histogram
+// instead of a serial shuffle.  The collision itself
 // restates mc/TypeMCC.f90:58-198, mc/MCCChi.f90, mc/MCCElectron.F90:13-148 and
 // mc/MCCIon.F90:6-75 with Philox draws instead of RANDOM_NUMBER.
 #include <cuda_runtime.h>
@@ -270,6 +271,13 @@ int sort_species(int sidx) {
 // MCC
 // ---------------------------------------------------------------------------
 
+// per-species device blocks: kMccSel status words of the bounded selection
+// ([0] list entries, [1] keys below the bound, [2] b*, [3] count below b*,
+// [4] 1 when the selection holds) and kMccMisc counters ([0] selected below
+// b*, [1] ties, [2..2+NR) reaction counts, [12] ionisations)
+constexpr int kMccSel = 8;
+constexpr int kMccMisc = 16;
+
 struct MccK {
   double *x, *y, *vx, *vy, *vz;  // FP32 data in the same storage when f32
   const int32_t *loc;
@@ -277,6 +285,7 @@ struct MccK {
   int64_t n;
   uint32_t seed0, seed1, step_lo, step_hi, species;
   int f32;
+  McSelect sel;  // round keys of the selection keys of this species and step
 };
 
 __device__ __forceinline__ double mcc_get(const double *a, int f32, int64_t p) {
@@ -289,11 +298,11 @@ __device__ __forceinline__ void mcc_put(double *a, int f32, int64_t p, double v)
 }
 
 // Selection keys of the live particles: histogram of their top 16 bits, and
-// the key itself for k_mcc_pick (one Philox evaluation per particle and step).
+// the key itself for k_mcc_pick.
 __global__ void k_mcc_hist(MccK k, uint32_t *__restrict__ hist, uint32_t *__restrict__ keys) {
   int64_t p = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
   if (p >= k.n || k.loc[p] < 0) return;
-  uint32_t key = mcc_select_key(k.id[p], k.step_lo, k.step_hi, k.species, k.seed0, k.seed1);
+  uint32_t key = mcc_select_key(k.id[p], k.sel);
   keys[p] = key;
   atomicAdd(hist + (key >> 16), 1u);
 }
@@ -338,7 +347,7 @@ __global__ void k_mcc_scan(MccK k, uint64_t bound, uint32_t *__restrict__ hist, 
   bool want = false;
   uint32_t key = 0;
   if (p < k.n && k.loc[p] >= 0) {
-    key = mcc_select_key(k.id[p], k.step_lo, k.step_hi, k.species, k.seed0, k.seed1);
+    key = mcc_select_key(k.id[p], k.sel);
     want = (uint64_t)key < bound;
   }
   // one list slot reservation per warp; every lane takes part in the ballot
@@ -416,11 +425,19 @@ __global__ void k_mcc_pick_list(const uint64_t *__restrict__ lkey, const int32_t
 // ncoll - below of them complete the selection.  Quadratic in the tie count,
 // so it leaves more than kMaxTies ties to the full selection (a bin holds
 // about 2 ncoll / 65536 keys: a few hundred at most in practice).
+// Thread 0 also records in ms[4] whether the selection holds: the list did
+// not overflow, b* exists, every entry below b* was picked, the ties fill
+// the selection and fit their buffer and this kernel's quadratic rank.
 constexpr int64_t kMaxTies = 8192;
 __global__ void __launch_bounds__(1024) k_mcc_ties(const uint64_t *__restrict__ tkey,
-                                                   const int32_t *__restrict__ tslot, int64_t tcap,
-                                                   const int64_t *__restrict__ ms, const int64_t *__restrict__ misc,
+                                                   const int32_t *__restrict__ tslot, int64_t tcap, int64_t lcap,
+                                                   int64_t *__restrict__ ms, const int64_t *__restrict__ misc,
                                                    int64_t ncoll, int32_t *__restrict__ sel) {
+  if (threadIdx.x == 0)
+    ms[4] = (ms[0] <= lcap && ms[2] >= 0 && misc[0] == ms[3] && misc[1] >= ncoll - ms[3] && misc[1] <= tcap &&
+             misc[1] <= kMaxTies)
+                ? 1
+                : 0;
   if (ms[2] < 0 || misc[1] > kMaxTies) return;
   const int64_t c = min(misc[1], tcap), below = ms[3], need = ncoll - below;
   for (int64_t i = threadIdx.x; i < c; i += blockDim.x) {
@@ -435,6 +452,7 @@ struct CollK {
   MccK k;
   const int32_t *sel;
   int64_t n_sel;
+  const int64_t *ok;  // nullptr, or a flag that must be 1 (the bounded selection held)
   const double *prob;
   McTable tab;
   McGas gas;
@@ -447,7 +465,7 @@ struct CollK {
 
 __global__ void k_mcc_collide(CollK c) {
   int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
-  if (t >= c.n_sel) return;
+  if (t >= c.n_sel || (c.ok && *c.ok != 1)) return;
   int32_t p = c.sel[t];
   McParticle P;
   P.vx = mcc_get(c.k.vx, c.k.f32, p) * c.vref;
@@ -509,26 +527,44 @@ __global__ void k_mcc_append(AppendK a) {
   a.id[d] = a.id_base + (uint32_t)r;
 }
 
+// selected slots and the ionisation outputs (one region of mcc_cap entries
+// per species); grown only before anything of the step is queued
 static int mcc_alloc(int64_t need) {
   if (need <= g.mcc_cap) return PIC_OK;
   int64_t cap = std::max<int64_t>(need, 1 << 16);
   cudaFree(g.d_sel);
-  cudaFree(g.d_cand);
-  cudaFree(g.d_cand_slot);
   cudaFree(g.d_ion_parent);
   cudaFree(g.d_ion_data);
+  g.d_sel = nullptr;
+  g.d_ion_parent = nullptr;
+  g.d_ion_data = nullptr;
+  g.mcc_cap = 0;
   PIC_CUDA(cudaMalloc(&g.d_sel, cap * sizeof(int32_t)));
+  PIC_CUDA(cudaMalloc(&g.d_ion_parent, PIC_MAX_SPECIES * cap * sizeof(int64_t)));
+  PIC_CUDA(cudaMalloc(&g.d_ion_data, PIC_MAX_SPECIES * 6 * cap * sizeof(double)));
+  g.mcc_cap = cap;
+  return PIC_OK;
+}
+
+// candidates of the threshold bin (key << 32 | id) and their slots; the
+// caller has no queued kernel using them when they grow
+static int mcc_cand_alloc(int64_t need) {
+  if (need <= g.cand_cap) return PIC_OK;
+  const int64_t cap = std::max<int64_t>(need, 1 << 16);
+  cudaFree(g.d_cand);
+  cudaFree(g.d_cand_slot);
+  g.d_cand = nullptr;
+  g.d_cand_slot = nullptr;
+  g.cand_cap = 0;
   PIC_CUDA(cudaMalloc(&g.d_cand, cap * sizeof(uint64_t)));
   PIC_CUDA(cudaMalloc(&g.d_cand_slot, cap * sizeof(int32_t)));
-  PIC_CUDA(cudaMalloc(&g.d_ion_parent, cap * sizeof(int64_t)));
-  PIC_CUDA(cudaMalloc(&g.d_ion_data, 6 * cap * sizeof(double)));
-  g.mcc_cap = cap;
+  g.cand_cap = cap;
   return PIC_OK;
 }
 
 // compact list of the bounded selection and its counters (kept across steps)
 static int mcc_list_alloc(int64_t need) {
-  if (!g.d_msel) PIC_CUDA(cudaMalloc(&g.d_msel, 8 * sizeof(int64_t)));
+  if (!g.d_msel) PIC_CUDA(cudaMalloc(&g.d_msel, PIC_MAX_SPECIES * kMccSel * sizeof(int64_t)));
   if (need <= g.mlist_cap) return PIC_OK;
   const int64_t cap = std::max<int64_t>(need + need / 2, 1 << 16);
   cudaFree(g.d_mlist_key);
@@ -549,200 +585,279 @@ struct Pending {
   int32_t e_species, ion_species;
 };
 
+// Full-histogram selection of species s (used when the bounded selection
+// does not apply or did not hold the ncoll smallest keys): histogram of all
+// keys, the threshold bin found on the host, its candidates ordered on the
+// host.  Leaves the ncoll selected slots in g.d_sel.
+static int mcc_select_full(const MccK &k, int64_t ncoll, int64_t *misc_d) {
+  PIC_CUDA(cudaMemsetAsync(g.d_hist, 0, 65536 * sizeof(uint32_t), g.st));
+  PIC_CUDA(cudaMemsetAsync(misc_d, 0, kMccMisc * sizeof(int64_t), g.st));
+  uint32_t *keys = g.d_sort_id;  // sort scratch, free while MCC runs
+  k_mcc_hist<<<blocks_for(k.n, 256), 256, 0, g.st>>>(k, g.d_hist, keys);
+  PIC_LAUNCHED();
+  std::vector<uint32_t> hist(65536);
+  PIC_CUDA(cudaMemcpyAsync(hist.data(), g.d_hist, 65536 * 4, cudaMemcpyDeviceToHost, g.st));
+  PIC_CUDA(cudaStreamSynchronize(g.st));
+  int64_t below = 0;
+  uint32_t bstar = 0;
+  for (; bstar < 65536; ++bstar) {
+    if (below + hist[bstar] >= ncoll) break;
+    below += hist[bstar];
+  }
+  if (bstar >= 65536) {
+    set_error("mcc: fewer live particles than collisions requested");
+    return PIC_ERR_STATE;
+  }
+  const int64_t need = ncoll - below;
+  const int64_t ncand_expect = hist[bstar];
+  int rc = mcc_cand_alloc(ncand_expect + 4096);
+  if (rc) return rc;
+  k_mcc_pick<<<blocks_for(k.n, 256), 256, 0, g.st>>>(k, keys, bstar, g.d_sel, misc_d, g.d_cand, g.d_cand_slot,
+                                                     g.cand_cap);
+  PIC_LAUNCHED();
+  int64_t misc[2];
+  PIC_CUDA(cudaMemcpyAsync(misc, misc_d, 2 * sizeof(int64_t), cudaMemcpyDeviceToHost, g.st));
+  PIC_CUDA(cudaStreamSynchronize(g.st));
+  const int64_t nsel = misc[0], ncand = misc[1];
+  if (ncand != ncand_expect || nsel != below) {
+    set_error("mcc: selection histogram mismatch");
+    return PIC_ERR_CUDA;
+  }
+  std::vector<uint64_t> cand(ncand);
+  std::vector<int32_t> cslot(ncand);
+  PIC_CUDA(cudaMemcpy(cand.data(), g.d_cand, ncand * 8, cudaMemcpyDeviceToHost));
+  PIC_CUDA(cudaMemcpy(cslot.data(), g.d_cand_slot, ncand * 4, cudaMemcpyDeviceToHost));
+  std::vector<int64_t> order(ncand);
+  for (int64_t i = 0; i < ncand; ++i) order[i] = i;
+  std::sort(order.begin(), order.end(), [&](int64_t a, int64_t b) { return cand[a] < cand[b]; });
+  std::vector<int32_t> add(need);
+  for (int64_t i = 0; i < need; ++i) add[i] = cslot[order[i]];
+  if (need > 0) PIC_CUDA(cudaMemcpy(g.d_sel + nsel, add.data(), need * 4, cudaMemcpyHostToDevice));
+  return PIC_OK;
+}
+
+// pinned host staging, grown on demand (kept across steps)
+static int mcc_host_alloc(void **buf, int64_t *cap, int64_t bytes) {
+  if (bytes <= *cap) return PIC_OK;
+  if (*buf) PIC_CUDA(cudaFreeHost(*buf));
+  *buf = nullptr;
+  *cap = 0;
+  const int64_t c = std::max<int64_t>(bytes + bytes / 2, 1 << 16);
+  PIC_CUDA(cudaMallocHost(buf, c));
+  *cap = c;
+  return PIC_OK;
+}
+
+// MCC of every species with tables, one step.  Each species' selection and
+// collisions are queued without waiting for the host: k_mcc_ties records
+// whether the bounded selection holds the ncoll smallest keys and
+// k_mcc_collide does nothing when it does not.  One read of the status
+// blocks then finds the species (rarely any) that need the full selection,
+// and one more brings back the ionisations; the created particles are
+// appended from pinned staging without a further wait.
 int mcc_run(uint64_t step, pic_mcc_stats *stats) {
-  std::vector<Pending> pend;
   const uint32_t seed0 = (uint32_t)g.P.seed, seed1 = (uint32_t)(g.P.seed >> 32);
   const uint32_t slo = (uint32_t)step, shi = (uint32_t)(step >> 32);
+  int64_t ncoll[PIC_MAX_SPECIES] = {0};
+  bool bounded[PIC_MAX_SPECIES] = {false};
+  int64_t most = 0;
   for (int s = 0; s < g.ns; ++s) {
     Species &sp = g.sp[s];
     if (!sp.has_mcc || sp.n_live == 0) continue;
-    int64_t npar = sp.n_live;
-    int64_t ncoll = mcc_n_collisions(npar, sp.tab.collision_ratio, slo, shi, (uint32_t)s, seed0, seed1);
-    if (stats) stats->n_selected[s] = ncoll;
-    if (ncoll <= 0) continue;
-    int rc = mcc_alloc(ncoll + 4096);
-    if (rc) return rc;
-    MccK k{sp.x, sp.y, sp.vx, sp.vy, sp.vz, sp.loc, sp.id, sp.n_slots, seed0, seed1, slo, shi, (uint32_t)s,
-           sp.f32 ? 1 : 0};
-    PIC_CUDA(cudaMemsetAsync(g.d_hist, 0, 65536 * sizeof(uint32_t), g.st));
-    PIC_CUDA(cudaMemsetAsync(g.d_mcc_misc, 0, 16 * sizeof(int64_t), g.st));
-    bool selected = false;
-    // bounded selection: the bound holds about 2 ncoll + 64 live keys (plus 8
-    // standard deviations); used while that is a small part of the species
-    const double target = 2.0 * (double)ncoll + 64.0 + 8.0 * std::sqrt(2.0 * (double)ncoll + 64.0);
-    if (!g.mcc_full && target < 0.25 * (double)npar) {
-      // g.mcc_bound_scale < 1 (a test hook) makes the bound too small, so the
-      // selection takes its fallback
-      const uint64_t bound = std::max<uint64_t>(
-          1, (uint64_t)std::ceil(g.mcc_bound_scale * target / (double)npar * 4294967296.0));
-      const int64_t lcap = (int64_t)(1.5 * target) + 4096;
-      if ((rc = mcc_list_alloc(lcap))) return rc;
-      if ((rc = mcc_alloc(std::max<int64_t>(ncoll, 1 << 16) + 4096))) return rc;
-      PIC_CUDA(cudaMemsetAsync(g.d_msel, 0, 8 * sizeof(int64_t), g.st));
-      unsigned long long *cnt = reinterpret_cast<unsigned long long *>(g.d_msel);
-      k_mcc_scan<<<blocks_for(sp.n_slots, 256), 256, 0, g.st>>>(k, bound, g.d_hist, g.d_mlist_key, g.d_mlist_slot,
-                                                                 lcap, cnt);
-      PIC_LAUNCHED();
-      k_mcc_bstar<<<1, 1024, 0, g.st>>>(g.d_hist, ncoll, g.d_msel);
-      PIC_LAUNCHED();
-      k_mcc_pick_list<<<(unsigned)std::min<int64_t>(blocks_for(lcap, 256), 1184), 256, 0, g.st>>>(
-          g.d_mlist_key, g.d_mlist_slot, cnt, lcap, bound, g.d_msel, g.d_sel, g.d_cand, g.d_cand_slot, g.mcc_cap,
-          g.d_mcc_misc);
-      PIC_LAUNCHED();
-      k_mcc_ties<<<1, 1024, 0, g.st>>>(g.d_cand, g.d_cand_slot, g.mcc_cap, g.d_msel, g.d_mcc_misc, ncoll, g.d_sel);
-      PIC_LAUNCHED();
-      int64_t ms[4], mc[2];
-      PIC_CUDA(cudaMemcpyAsync(ms, g.d_msel, sizeof ms, cudaMemcpyDeviceToHost, g.st));
-      PIC_CUDA(cudaMemcpyAsync(mc, g.d_mcc_misc, sizeof mc, cudaMemcpyDeviceToHost, g.st));
-      PIC_CUDA(cudaStreamSynchronize(g.st));
-      // ms[0] list entries, ms[2] b*, ms[3] below b*; mc[0] selected below
-      // b*, mc[1] ties
-      selected = ms[0] <= lcap && ms[2] >= 0 && mc[0] == ms[3] && mc[1] >= ncoll - ms[3] && mc[1] <= g.mcc_cap &&
-                 mc[1] <= kMaxTies;
-      if (!selected) {  // start the full selection from clean counters
-        PIC_CUDA(cudaMemsetAsync(g.d_hist, 0, 65536 * sizeof(uint32_t), g.st));
-        PIC_CUDA(cudaMemsetAsync(g.d_mcc_misc, 0, 16 * sizeof(int64_t), g.st));
-      }
-    }
-    if (!selected) {
-      uint32_t *keys = g.d_sort_id;  // sort scratch, free while MCC runs
-      k_mcc_hist<<<blocks_for(sp.n_slots, 256), 256, 0, g.st>>>(k, g.d_hist, keys);
-      PIC_LAUNCHED();
-      std::vector<uint32_t> hist(65536);
-      PIC_CUDA(cudaMemcpyAsync(hist.data(), g.d_hist, 65536 * 4, cudaMemcpyDeviceToHost, g.st));
-      PIC_CUDA(cudaStreamSynchronize(g.st));
-      int64_t below = 0;
-      uint32_t bstar = 0;
-      for (; bstar < 65536; ++bstar) {
-        if (below + hist[bstar] >= ncoll) break;
-        below += hist[bstar];
-      }
-      if (bstar >= 65536) {
-        set_error("mcc: fewer live particles than collisions requested");
-        return PIC_ERR_STATE;
-      }
-      int64_t need = ncoll - below;
-      int64_t ncand_expect = hist[bstar];
-      rc = mcc_alloc(std::max<int64_t>(ncoll, ncand_expect) + 4096);
-      if (rc) return rc;
-      k_mcc_pick<<<blocks_for(sp.n_slots, 256), 256, 0, g.st>>>(k, keys, bstar, g.d_sel, g.d_mcc_misc, g.d_cand,
-                                                                g.d_cand_slot, g.mcc_cap);
-      PIC_LAUNCHED();
-      int64_t misc[2];
-      PIC_CUDA(cudaMemcpyAsync(misc, g.d_mcc_misc, 2 * sizeof(int64_t), cudaMemcpyDeviceToHost, g.st));
-      PIC_CUDA(cudaStreamSynchronize(g.st));
-      int64_t nsel = misc[0], ncand = misc[1];
-      if (ncand != ncand_expect || nsel != below) {
-        set_error("mcc: selection histogram mismatch");
-        return PIC_ERR_CUDA;
-      }
-      {
-        std::vector<uint64_t> cand(ncand);
-        std::vector<int32_t> cslot(ncand);
-        PIC_CUDA(cudaMemcpy(cand.data(), g.d_cand, ncand * 8, cudaMemcpyDeviceToHost));
-        PIC_CUDA(cudaMemcpy(cslot.data(), g.d_cand_slot, ncand * 4, cudaMemcpyDeviceToHost));
-        std::vector<int64_t> order(ncand);
-        for (int64_t i = 0; i < ncand; ++i) order[i] = i;
-        std::sort(order.begin(), order.end(), [&](int64_t a, int64_t b) { return cand[a] < cand[b]; });
-        std::vector<int32_t> add(need);
-        for (int64_t i = 0; i < need; ++i) add[i] = cslot[order[i]];
-        if (need > 0)
-          PIC_CUDA(cudaMemcpy(g.d_sel + nsel, add.data(), need * 4, cudaMemcpyHostToDevice));
-      }
-    }
+    ncoll[s] = mcc_n_collisions(sp.n_live, sp.tab.collision_ratio, slo, shi, (uint32_t)s, seed0, seed1);
+    if (stats) stats->n_selected[s] = ncoll[s];
+    most = std::max(most, ncoll[s]);
+  }
+  if (most <= 0) return PIC_OK;
+  // every buffer the queued kernels use is sized first: the bounded
+  // selection's list for its largest species, the selection for the
+  // largest ncoll
+  int64_t lcap[PIC_MAX_SPECIES] = {0}, lmax = 0;
+  for (int s = 0; s < g.ns; ++s) {
+    if (ncoll[s] <= 0) continue;
+    const double npar = (double)g.sp[s].n_live, nc = (double)ncoll[s];
+    // the bound holds about 2 ncoll + 64 live keys (plus 8 standard
+    // deviations); used while that is a small part of the species
+    const double target = 2.0 * nc + 64.0 + 8.0 * std::sqrt(2.0 * nc + 64.0);
+    if (g.mcc_full || target >= 0.25 * npar) continue;
+    bounded[s] = true;
+    lcap[s] = (int64_t)(1.5 * target) + 4096;
+    lmax = std::max(lmax, lcap[s]);
+  }
+  int rc;
+  if ((rc = mcc_alloc(std::max<int64_t>(most, 1 << 16) + 4096))) return rc;
+  if ((rc = mcc_cand_alloc(g.mcc_cap))) return rc;
+  if ((rc = mcc_list_alloc(lmax))) return rc;
+  PIC_CUDA(cudaMemsetAsync(g.d_mcc_misc, 0, PIC_MAX_SPECIES * kMccMisc * sizeof(int64_t), g.st));
+  PIC_CUDA(cudaMemsetAsync(g.d_msel, 0, PIC_MAX_SPECIES * kMccSel * sizeof(int64_t), g.st));
+  auto mk = [&](int s) {
+    Species &sp = g.sp[s];
+    return MccK{sp.x, sp.y, sp.vx, sp.vy, sp.vz, sp.loc, sp.id, sp.n_slots, seed0, seed1, slo, shi, (uint32_t)s,
+                sp.f32 ? 1 : 0, mcc_select_round_keys(slo, shi, (uint32_t)s, seed0, seed1)};
+  };
+  auto collide = [&](int s, const int64_t *ok) -> int {
+    Species &sp = g.sp[s];
     CollK c;
-    c.k = k;
+    c.k = mk(s);
     c.sel = g.d_sel;
-    c.n_sel = ncoll;
+    c.n_sel = ncoll[s];
+    c.ok = ok;
     c.prob = sp.prob;
     c.tab = mc_table_from(sp.tab);
     c.gas.mass = g.gas.mass;
     c.gas.temperature = g.gas.temperature;
     c.mass = sp.mass;
     c.vref = g.v_ref;
-    c.misc = g.d_mcc_misc;
-    c.ion_parent = g.d_ion_parent;
-    c.ion_data = g.d_ion_data;
+    c.misc = g.d_mcc_misc + s * kMccMisc;
+    c.ion_parent = g.d_ion_parent + s * g.mcc_cap;
+    c.ion_data = g.d_ion_data + 6 * s * g.mcc_cap;
     c.ion_cap = g.mcc_cap;
-    k_mcc_collide<<<blocks_for(ncoll, 128), 128, 0, g.st>>>(c);
+    k_mcc_collide<<<blocks_for(ncoll[s], 128), 128, 0, g.st>>>(c);
     PIC_LAUNCHED();
-    int64_t m2[16];
-    PIC_CUDA(cudaMemcpyAsync(m2, g.d_mcc_misc, sizeof m2, cudaMemcpyDeviceToHost, g.st));
+    return PIC_OK;
+  };
+  // 1. bounded selections and their collisions, queued
+  for (int s = 0; s < g.ns; ++s) {
+    if (!bounded[s]) continue;
+    const double npar = (double)g.sp[s].n_live, nc = (double)ncoll[s];
+    const double target = 2.0 * nc + 64.0 + 8.0 * std::sqrt(2.0 * nc + 64.0);
+    // g.mcc_bound_scale < 1 (a test hook) makes the bound too small, so the
+    // selection takes its fallback
+    const uint64_t bound =
+        std::max<uint64_t>(1, (uint64_t)std::ceil(g.mcc_bound_scale * target / npar * 4294967296.0));
+    const MccK k = mk(s);
+    int64_t *ms = g.d_msel + s * kMccSel, *misc = g.d_mcc_misc + s * kMccMisc;
+    unsigned long long *cnt = reinterpret_cast<unsigned long long *>(ms);
+    PIC_CUDA(cudaMemsetAsync(g.d_hist, 0, 65536 * sizeof(uint32_t), g.st));
+    k_mcc_scan<<<blocks_for(k.n, 256), 256, 0, g.st>>>(k, bound, g.d_hist, g.d_mlist_key, g.d_mlist_slot,
+                                                       lcap[s], cnt);
+    PIC_LAUNCHED();
+    k_mcc_bstar<<<1, 1024, 0, g.st>>>(g.d_hist, ncoll[s], ms);
+    PIC_LAUNCHED();
+    k_mcc_pick_list<<<(unsigned)std::min<int64_t>(blocks_for(lcap[s], 256), 1184), 256, 0, g.st>>>(
+        g.d_mlist_key, g.d_mlist_slot, cnt, lcap[s], bound, ms, g.d_sel, g.d_cand, g.d_cand_slot, g.cand_cap, misc);
+    PIC_LAUNCHED();
+    k_mcc_ties<<<1, 1024, 0, g.st>>>(g.d_cand, g.d_cand_slot, g.cand_cap, lcap[s], ms, misc, ncoll[s], g.d_sel);
+    PIC_LAUNCHED();
+    if ((rc = collide(s, ms + 4))) return rc;
+  }
+  // 2. one read of every status block; full selections where needed
+  int64_t ms_h[PIC_MAX_SPECIES * kMccSel], misc_h[PIC_MAX_SPECIES * kMccMisc];
+  PIC_CUDA(cudaMemcpyAsync(ms_h, g.d_msel, sizeof ms_h, cudaMemcpyDeviceToHost, g.st));
+  PIC_CUDA(cudaMemcpyAsync(misc_h, g.d_mcc_misc, sizeof misc_h, cudaMemcpyDeviceToHost, g.st));
+  PIC_CUDA(cudaStreamSynchronize(g.st));
+  for (int s = 0; s < g.ns; ++s) {
+    if (ncoll[s] <= 0 || (bounded[s] && ms_h[s * kMccSel + 4] == 1)) continue;
+    int64_t *misc = g.d_mcc_misc + s * kMccMisc;
+    if ((rc = mcc_select_full(mk(s), ncoll[s], misc))) return rc;
+    if ((rc = collide(s, nullptr))) return rc;
+    PIC_CUDA(cudaMemcpyAsync(misc_h + s * kMccMisc, misc, kMccMisc * sizeof(int64_t), cudaMemcpyDeviceToHost,
+                             g.st));
     PIC_CUDA(cudaStreamSynchronize(g.st));
+  }
+  // 3. ionisations: parents and velocities of every species in one read
+  int64_t nion[PIC_MAX_SPECIES] = {0}, nion_all = 0;
+  for (int s = 0; s < g.ns; ++s) {
+    if (ncoll[s] <= 0) continue;
+    const int64_t *m2 = misc_h + s * kMccMisc;
     if (stats)
-      for (int r = 0; r < sp.tab.n_reaction && r < 8; ++r) stats->n_by_reaction[s][r] = m2[2 + r];
-    int64_t nion = m2[12];
-    if (nion > g.mcc_cap) {
+      for (int r = 0; r < g.sp[s].tab.n_reaction && r < 8; ++r) stats->n_by_reaction[s][r] = m2[2 + r];
+    nion[s] = m2[12];
+    if (nion[s] > g.mcc_cap) {
       set_error("mcc: ionisation buffer overflow");
       return PIC_ERR_CAPACITY;
     }
-    if (nion > 0) {
+    nion_all += nion[s];
+  }
+  if (nion_all == 0) return PIC_OK;
+  if ((rc = mcc_host_alloc(&g.h_ion, &g.h_ion_cap, nion_all * 56))) return rc;
+  {
+    char *h = static_cast<char *>(g.h_ion);
+    for (int s = 0; s < g.ns; ++s) {
+      if (nion[s] == 0) continue;
+      PIC_CUDA(cudaMemcpyAsync(h, g.d_ion_parent + s * g.mcc_cap, nion[s] * 8, cudaMemcpyDeviceToHost, g.st));
+      PIC_CUDA(cudaMemcpyAsync(h + nion[s] * 8, g.d_ion_data + 6 * s * g.mcc_cap, nion[s] * 48,
+                               cudaMemcpyDeviceToHost, g.st));
+      h += nion[s] * 56;
+    }
+    PIC_CUDA(cudaStreamSynchronize(g.st));
+  }
+  std::vector<Pending> pend;
+  {
+    const char *h = static_cast<const char *>(g.h_ion);
+    for (int s = 0; s < g.ns; ++s) {
+      const int64_t n = nion[s];
+      if (n == 0) continue;
+      const int64_t *par = reinterpret_cast<const int64_t *>(h);
+      const double *data = reinterpret_cast<const double *>(h + n * 8);
+      h += n * 56;
+      std::vector<int64_t> order(n);
+      for (int64_t i = 0; i < n; ++i) order[i] = i;
+      std::sort(order.begin(), order.end(), [&](int64_t a, int64_t b) { return par[a] < par[b]; });
       Pending pd;
       pd.from_species = s;
-      pd.parent.resize(nion);
-      std::vector<double> data(6 * nion);
-      PIC_CUDA(cudaMemcpy(pd.parent.data(), g.d_ion_parent, nion * 8, cudaMemcpyDeviceToHost));
-      PIC_CUDA(cudaMemcpy(data.data(), g.d_ion_data, nion * 48, cudaMemcpyDeviceToHost));
-      std::vector<int64_t> order(nion);
-      for (int64_t i = 0; i < nion; ++i) order[i] = i;
-      std::sort(order.begin(), order.end(), [&](int64_t a, int64_t b) { return pd.parent[a] < pd.parent[b]; });
-      std::vector<int64_t> par2(nion);
-      pd.data.resize(6 * nion);
-      for (int64_t i = 0; i < nion; ++i) {
-        par2[i] = pd.parent[order[i]];
+      pd.parent.resize(n);
+      pd.data.resize(6 * n);
+      for (int64_t i = 0; i < n; ++i) {
+        pd.parent[i] = par[order[i]];
         for (int q = 0; q < 6; ++q) pd.data[6 * i + q] = data[6 * order[i] + q];
       }
-      pd.parent.swap(par2);
       pd.e_species = s;
       // resultant of the ionisation reaction
       pd.ion_species = -1;
-      for (int r = 0; r < sp.tab.n_reaction; ++r)
-        if (sp.tab.reaction_type[r] == 13) pd.ion_species = sp.tab.resultant[r];
+      for (int r = 0; r < g.sp[s].tab.n_reaction; ++r)
+        if (g.sp[s].tab.reaction_type[r] == 13) pd.ion_species = g.sp[s].tab.resultant[r];
       pend.push_back(std::move(pd));
     }
   }
-  // MCCAddNewParticle: append the created particles after all species collided
+  // 4. MCCAddNewParticle: append the created particles after all species
+  // collided, from pinned staging (one region per copy, so that no copy
+  // still queued reads a region the host is filling)
+  int64_t stage = 0;
+  for (auto &pd : pend) stage += (int64_t)pd.parent.size() * (4 + 2 * 24);
+  if ((rc = mcc_host_alloc(&g.h_new, &g.h_new_cap, stage))) return rc;
+  char *h = static_cast<char *>(g.h_new);
   for (auto &pd : pend) {
-    int64_t nion = (int64_t)pd.parent.size();
-    std::vector<int32_t> pslot(nion);
-    for (int64_t i = 0; i < nion; ++i) pslot[i] = (int32_t)(pd.parent[i] & 0xffffffff);
-    if (nion > g.mcc_new_cap) {  // grow the created-particle staging (kept across steps)
+    const int64_t n = (int64_t)pd.parent.size();
+    if (n > g.mcc_new_cap) {  // grow the created-particle staging (kept across steps)
+      PIC_CUDA(cudaStreamSynchronize(g.st));
       cudaFree(g.d_mcc_pslot);
       cudaFree(g.d_mcc_vel);
       g.d_mcc_pslot = nullptr;
       g.d_mcc_vel = nullptr;
       g.mcc_new_cap = 0;
-      const int64_t cap = std::max<int64_t>(2 * nion, 1 << 16);
+      const int64_t cap = std::max<int64_t>(2 * n, 1 << 16);
       PIC_CUDA(cudaMalloc(&g.d_mcc_pslot, cap * 4));
       PIC_CUDA(cudaMalloc(&g.d_mcc_vel, 3 * cap * 8));
       g.mcc_new_cap = cap;
     }
-    int32_t *d_pslot = g.d_mcc_pslot;
-    double *d_vel = g.d_mcc_vel;
-    PIC_CUDA(cudaMemcpyAsync(d_pslot, pslot.data(), nion * 4, cudaMemcpyHostToDevice, g.st));
+    int32_t *pslot = reinterpret_cast<int32_t *>(h);
+    h += n * 4;
+    for (int64_t i = 0; i < n; ++i) pslot[i] = (int32_t)(pd.parent[i] & 0xffffffff);
+    PIC_CUDA(cudaMemcpyAsync(g.d_mcc_pslot, pslot, n * 4, cudaMemcpyHostToDevice, g.st));
     Species &from = g.sp[pd.from_species];
     for (int which = 0; which < 2; ++which) {
-      int ts = which == 0 ? pd.e_species : pd.ion_species;
+      const int ts = which == 0 ? pd.e_species : pd.ion_species;
+      double *vel = reinterpret_cast<double *>(h);
+      h += n * 24;
       if (ts < 0 || ts >= g.ns) continue;
       Species &to = g.sp[ts];
-      if (to.n_slots + nion > to.capacity) {
+      if (to.n_slots + n > to.capacity) {
         set_error("mcc: particle capacity exceeded by ionisation");
         return PIC_ERR_CAPACITY;
       }
-      std::vector<double> vel(3 * nion);
-      for (int64_t i = 0; i < nion; ++i)
+      for (int64_t i = 0; i < n; ++i)
         for (int q = 0; q < 3; ++q)
           vel[3 * i + q] = which == 0 ? pd.data[6 * i + q] : pd.data[6 * i + 3 + q] / g.v_ref;
-      PIC_CUDA(cudaMemcpyAsync(d_vel, vel.data(), 3 * nion * 8, cudaMemcpyHostToDevice, g.st));
+      PIC_CUDA(cudaMemcpyAsync(g.d_mcc_vel, vel, 3 * n * 8, cudaMemcpyHostToDevice, g.st));
       AppendK a{from.x, from.y, from.loc, to.x, to.y, to.vx, to.vy, to.vz, to.loc, to.id,
-                to.n_slots, to.next_id, d_pslot, d_vel, nion, to.f32 ? 1 : 0};
-      k_mcc_append<<<blocks_for(nion, 256), 256, 0, g.st>>>(a);
+                to.n_slots, to.next_id, g.d_mcc_pslot, g.d_mcc_vel, n, to.f32 ? 1 : 0};
+      k_mcc_append<<<blocks_for(n, 256), 256, 0, g.st>>>(a);
       PIC_LAUNCHED();
-      PIC_CUDA(cudaStreamSynchronize(g.st));
-      to.n_slots += nion;
-      to.n_live += nion;
-      to.next_id += (uint32_t)nion;
-      if (stats) stats->n_created[ts] += nion;
+      to.n_slots += n;
+      to.n_live += n;
+      to.next_id += (uint32_t)n;
+      if (stats) stats->n_created[ts] += n;
     }
   }
   return PIC_OK;
@@ -779,7 +894,7 @@ extern "C" int pic_mcc_init(const pic_gas *gas, int32_t n_tables, const pic_mcc_
     sp.tab.probability = nullptr;
   }
   if (!g.d_hist) PIC_CUDA(cudaMalloc(&g.d_hist, 65536 * sizeof(uint32_t)));
-  if (!g.d_mcc_misc) PIC_CUDA(cudaMalloc(&g.d_mcc_misc, 16 * sizeof(int64_t)));
+  if (!g.d_mcc_misc) PIC_CUDA(cudaMalloc(&g.d_mcc_misc, PIC_MAX_SPECIES * kMccMisc * sizeof(int64_t)));
   g.mcc_ready = n_tables > 0;
   return PIC_OK;
 }

@@ -52,6 +52,7 @@ def load():
     lib.or_mcc.argtypes = [_P(api.MccTable), _P(api.Gas), C.c_double, C.c_double, C.c_uint64,
                            C.c_uint64, C.c_int32, C.c_int64, _i, _u, _d, _d, _d, _l, _l, _l, _d, _d]
     lib.or_mcc.restype = C.c_int64
+    lib.or_mcc_select_keys.argtypes = [C.c_uint64, C.c_uint64, C.c_int32, C.c_int64, _u, _u]
     lib.or_ife_closed_form.argtypes = [C.c_int, C.c_int, C.c_int, C.c_double, C.c_double,
                                        C.c_double, _d]
     lib.or_ek_tot.argtypes = [M, _l, C.c_double, C.c_double, C.c_double, _d]
@@ -313,3 +314,11 @@ def mcc_table(bundle, mass, gas_mass, n_gas, dt_s, jtoev=1.6022e-19):
     lib.or_mcc_probability(nr, ns, d(np.ascontiguousarray(sig)), mass, gas_mass, n_gas, emin, eint, emax,
                            dt_s, jtoev, d(prob), d(o3))
     return sig, prob, o3[0], o3[1], o3[2]
+
+
+def mcc_select_keys(seed, step, species, ids):
+    """The oracle's null-collision selection keys of `ids` at one step."""
+    ids = np.ascontiguousarray(ids, dtype=np.uint32)
+    out = np.empty_like(ids)
+    load().or_mcc_select_keys(seed, step, species, ids.size, u32(ids), u32(out))
+    return out

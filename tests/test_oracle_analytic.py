@@ -199,3 +199,32 @@ def test_mcc_ionisation_balances_energy():
     e_new = 0.5 * deck.ME * (ne ** 2).sum(axis=1) * vref * vref / _JTOEV
     assert np.allclose(e1[par] + e_new, e0[par] - thr, rtol=1e-12, atol=1e-12 * e0.max())
     assert np.all(ni == 0.0)  # the ion takes the (resting) target's velocity
+
+
+def test_mcc_selection_keys_pick_uniform_subsets():
+    """The null-collision selection (the ncoll smallest keys of the live
+    ids) behaves as the reference's uniform random N-subset
+    (MCCPublic.F90:148-171): every id is picked at the rate ncoll/n, ids next
+    to each other and the same id on consecutive steps are picked together
+    at the product rate, keys of one step are distinct, and species and
+    seeds draw different keys.  Bounds are 5 standard deviations."""
+    n, ncoll, steps, seed = 4096, 64, 2000, 12345
+    ids = np.arange(n, dtype=np.uint32) * np.uint32(7) + np.uint32(1000)  # ids need not be contiguous
+    picked = np.zeros((steps, n), bool)
+    for t in range(steps):
+        k = ob.mcc_select_keys(seed, t, 0, ids)
+        if t == 0:
+            assert np.unique(k).size == n
+        picked[t, np.argpartition(k, ncoll)[:ncoll]] = True
+    p = ncoll / n
+    counts = picked.sum(0)
+    chi2 = ((counts - steps * p) ** 2 / (steps * p * (1 - p))).sum()
+    assert abs(chi2 - n) < 5 * np.sqrt(2 * n)
+    for a, b in ((picked[:, :-1], picked[:, 1:]), (picked[:-1], picked[1:])):
+        both = int((a & b).sum())
+        q = p * (ncoll - 1) / (n - 1) if a.shape[1] == n - 1 else p * p
+        mean = a.size * q
+        assert abs(both - mean) < 5 * np.sqrt(mean), (both, mean)
+    k0 = ob.mcc_select_keys(seed, 5, 0, ids)
+    assert (k0 != ob.mcc_select_keys(seed, 5, 1, ids)).mean() > 0.99
+    assert (k0 != ob.mcc_select_keys(seed + 1, 5, 0, ids)).mean() > 0.99
