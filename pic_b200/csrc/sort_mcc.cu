@@ -340,29 +340,46 @@ __device__ __forceinline__ uint32_t mcc_bin(uint32_t key, uint64_t bound) {
   return (uint32_t)(((uint64_t)key << 16) / bound);
 }
 
+// Four consecutive slots per thread: their elements and ids come in one
+// 16-byte load each, issued together and unconditionally, so every thread
+// keeps 32 bytes in flight (one 4-byte load that a second one waits on left
+// the pass latency-bound at a quarter of the memory bandwidth).
 __global__ void k_mcc_scan(MccK k, uint64_t bound, uint32_t *__restrict__ hist, uint64_t *__restrict__ lkey,
                            int32_t *__restrict__ lslot, int64_t cap, unsigned long long *__restrict__ cnt) {
-  const int64_t p = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  const int64_t p0 = 4 * ((int64_t)blockIdx.x * blockDim.x + threadIdx.x);
   const int lane = threadIdx.x & 31;
-  bool want = false;
-  uint32_t key = 0;
-  if (p < k.n && k.loc[p] >= 0) {
-    key = mcc_select_key(k.id[p], k.sel);
-    want = (uint64_t)key < bound;
+  int loc[4];
+  uint32_t id[4];
+  if (p0 + 3 < k.n) {
+    const int4 l = __ldcs(reinterpret_cast<const int4 *>(k.loc + p0));
+    const uint4 d = __ldcs(reinterpret_cast<const uint4 *>(k.id + p0));
+    loc[0] = l.x; loc[1] = l.y; loc[2] = l.z; loc[3] = l.w;
+    id[0] = d.x; id[1] = d.y; id[2] = d.z; id[3] = d.w;
+  } else {
+#pragma unroll
+    for (int u = 0; u < 4; ++u) {
+      loc[u] = p0 + u < k.n ? k.loc[p0 + u] : -1;
+      id[u] = p0 + u < k.n ? k.id[p0 + u] : 0u;
+    }
   }
-  // one list slot reservation per warp; every lane takes part in the ballot
-  const unsigned m = __ballot_sync(0xffffffffu, want);
-  if (!m) return;  // the same for every lane of the warp
-  const int leader = __ffs(m) - 1;
-  unsigned long long base = 0;
-  if (lane == leader) base = atomicAdd(cnt, (unsigned long long)__popc(m));
-  base = __shfl_sync(0xffffffffu, base, leader);
-  if (want) {
-    atomicAdd(hist + mcc_bin(key, bound), 1u);
-    const int64_t i = (int64_t)base + __popc(m & ((1u << lane) - 1u));
-    if (i < cap) {
-      lkey[i] = ((uint64_t)key << 32) | (uint64_t)k.id[p];
-      lslot[i] = (int32_t)p;
+#pragma unroll
+  for (int u = 0; u < 4; ++u) {
+    const uint32_t key = mcc_select_key(id[u], k.sel);
+    const bool want = loc[u] >= 0 && (uint64_t)key < bound;
+    // one list slot reservation per warp; every lane takes part in the ballot
+    const unsigned m = __ballot_sync(0xffffffffu, want);
+    if (!m) continue;  // the same for every lane of the warp
+    const int leader = __ffs(m) - 1;
+    unsigned long long base = 0;
+    if (lane == leader) base = atomicAdd(cnt, (unsigned long long)__popc(m));
+    base = __shfl_sync(0xffffffffu, base, leader);
+    if (want) {
+      atomicAdd(hist + mcc_bin(key, bound), 1u);
+      const int64_t i = (int64_t)base + __popc(m & ((1u << lane) - 1u));
+      if (i < cap) {
+        lkey[i] = ((uint64_t)key << 32) | (uint64_t)id[u];
+        lslot[i] = (int32_t)(p0 + u);
+      }
     }
   }
 }
@@ -370,14 +387,32 @@ __global__ void k_mcc_scan(MccK k, uint64_t bound, uint32_t *__restrict__ hist, 
 // one block of 1024 threads: the bin b* where the running count of the
 // histogram reaches ncoll, and the count below it.  ms[1] = keys below the
 // bound, ms[2] = b* (-1 when fewer than ncoll keys lie below the bound),
-// ms[3] = particles in bins below b*.
+// ms[3] = particles in bins below b*.  Each thread sums its 64 bins from
+// sixteen 16-byte loads (eight in flight at a time); after the block scan
+// warp 0 finds b* inside the one thread's 64 bins that reaches ncoll, two
+// bins a lane.
 __global__ void __launch_bounds__(1024) k_mcc_bstar(const uint32_t *__restrict__ hist, int64_t ncoll,
                                                     int64_t *__restrict__ ms) {
   __shared__ unsigned long long part[1024];
+  __shared__ int owner;
+  __shared__ unsigned long long owner_excl;
   const int t = threadIdx.x;
-  if (t == 0) ms[2] = -1;
+  if (t == 0) {
+    ms[2] = -1;
+    owner = -1;
+  }
+  const uint4 *h4 = reinterpret_cast<const uint4 *>(hist) + 16 * t;
   unsigned long long s = 0;
-  for (int b = 0; b < 64; ++b) s += hist[t * 64 + b];
+#pragma unroll
+  for (int half = 0; half < 2; ++half) {
+    uint4 v[8];
+#pragma unroll
+    for (int u = 0; u < 8; ++u) v[u] = h4[8 * half + u];
+#pragma unroll
+    for (int u = 0; u < 8; ++u)
+      s += (unsigned long long)v[u].x + (unsigned long long)v[u].y + (unsigned long long)v[u].z +
+           (unsigned long long)v[u].w;
+  }
   part[t] = s;
   __syncthreads();
   for (int off = 1; off < 1024; off <<= 1) {  // inclusive scan
@@ -389,11 +424,33 @@ __global__ void __launch_bounds__(1024) k_mcc_bstar(const uint32_t *__restrict__
   const unsigned long long incl = part[t], excl = t ? part[t - 1] : 0ull, nc = (unsigned long long)ncoll;
   if (t == 1023) ms[1] = (int64_t)incl;
   if (excl < nc && incl >= nc) {  // exactly one thread
-    unsigned long long below = excl;
-    int b = t * 64;
-    while (below + hist[b] < nc) below += hist[b++];  // ends inside this thread's 64 bins
-    ms[2] = b;
-    ms[3] = (int64_t)below;
+    owner = t;
+    owner_excl = excl;
+  }
+  __syncthreads();
+  const int o = owner;
+  if (o < 0 || t >= 32) return;
+  // lane t holds bins b0 and b0 + 1 of the owner's range
+  const int b0 = o * 64 + 2 * t;
+  const unsigned long long h0 = hist[b0], h1 = hist[b0 + 1];
+  unsigned long long x = h0 + h1;
+#pragma unroll
+  for (int off = 1; off < 32; off <<= 1) {  // inclusive warp scan of the pairs
+    const unsigned long long y = __shfl_up_sync(0xffffffffu, x, off);
+    if (t >= off) x += y;
+  }
+  const unsigned long long before = owner_excl + x - (h0 + h1);  // keys in bins below b0
+  // reached within this pair (true from the first such lane on: the last
+  // lane's pair ends at the owner's inclusive count, which reaches ncoll)
+  const unsigned hit = __ballot_sync(0xffffffffu, before + h0 + h1 >= nc);
+  if (t == __ffs(hit) - 1) {
+    if (before + h0 >= nc) {
+      ms[2] = b0;
+      ms[3] = (int64_t)before;
+    } else {
+      ms[2] = b0 + 1;
+      ms[3] = (int64_t)(before + h0);
+    }
   }
 }
 
@@ -729,8 +786,8 @@ int mcc_run(uint64_t step, pic_mcc_stats *stats) {
     int64_t *ms = g.d_msel + s * kMccSel, *misc = g.d_mcc_misc + s * kMccMisc;
     unsigned long long *cnt = reinterpret_cast<unsigned long long *>(ms);
     PIC_CUDA(cudaMemsetAsync(g.d_hist, 0, 65536 * sizeof(uint32_t), g.st));
-    k_mcc_scan<<<blocks_for(k.n, 256), 256, 0, g.st>>>(k, bound, g.d_hist, g.d_mlist_key, g.d_mlist_slot,
-                                                       lcap[s], cnt);
+    k_mcc_scan<<<blocks_for((k.n + 3) / 4, 256), 256, 0, g.st>>>(k, bound, g.d_hist, g.d_mlist_key,
+                                                                 g.d_mlist_slot, lcap[s], cnt);
     PIC_LAUNCHED();
     k_mcc_bstar<<<1, 1024, 0, g.st>>>(g.d_hist, ncoll[s], ms);
     PIC_LAUNCHED();
