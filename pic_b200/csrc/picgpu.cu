@@ -1154,8 +1154,11 @@ __device__ __forceinline__ unsigned int atom_add_release_gpu(unsigned int *p, un
 // reaches the end of its round.  The wait is bounded: after `limit` polls the
 // CTA records the timeout in *err and leaves; every CTA then exits the solve,
 // so a lost CTA ends the kernel with an error status instead of a hang.
+// Thread 0 reads the error word once and hands it to the CTA through shared
+// memory (one global round trip per barrier instead of one per warp).
 __device__ __forceinline__ bool grid_barrier(unsigned int *bar, int *err, long long limit,
                                              unsigned int extra) {
+  __shared__ int s_ok;
   __syncthreads();
   if (threadIdx.x == 0) {
     const unsigned int n = gridDim.x + extra;
@@ -1168,9 +1171,10 @@ __device__ __forceinline__ bool grid_barrier(unsigned int *bar, int *err, long l
         break;
       }
     }
+    s_ok = *(volatile int *)err == 0;
   }
   __syncthreads();
-  return *(volatile int *)err == 0;
+  return s_ok != 0;
 }
 
 // The persistent solver runs CTAs of PIC_RED_CHUNK (1024) threads, one chunk
@@ -2087,14 +2091,28 @@ __global__ void __launch_bounds__(kWide, 1) k_fcg_persist(FcgP<V> F) {
     if (M.L > 1) {
       // (E1) zA += P e_1 once per unknown node (Dirichlet nodes keep 0), so
       // that the post-smoothing reads it at its neighbours
+      // two chunks a thread at a time: both nodes' loads are issued before
+      // either store (the stores would otherwise hold back the next chunk's
+      // loads, which the compiler cannot prove independent of them)
       const double *e1 = mg_e(M, 1);
       const int ny1 = M.lv[1].ny;
-      for (int c = blockIdx.x; c < nb; c += gridDim.x) {
-        const int64_t n = (int64_t)c * kWide + threadIdx.x;
-        if (n < nn && k.row_kind[n] >= 0) {
-          const int i = (int)n / k.nny, j = (int)n - i * k.nny;  // the grid holds < 2^31 nodes
-          F.zA[n] = (V)((double)F.zA[n] + mg_prolong(e1, ny1, i, j));
+      for (int c = blockIdx.x; c < nb; c += 2 * gridDim.x) {
+        const int64_t na = (int64_t)c * kWide + threadIdx.x, nb2 = na + (int64_t)gridDim.x * kWide;
+        const bool ua = na < nn && k.row_kind[na] >= 0;
+        const bool ub = nb2 < nn && k.row_kind[nb2] >= 0;
+        double pa = 0.0, pb = 0.0, za = 0.0, zb = 0.0;
+        if (ua) {
+          const int i = (int)na / k.nny, j = (int)na - i * k.nny;  // the grid holds < 2^31 nodes
+          pa = mg_prolong(e1, ny1, i, j);
+          za = (double)F.zA[na];
         }
+        if (ub) {
+          const int i = (int)nb2 / k.nny, j = (int)nb2 - i * k.nny;
+          pb = mg_prolong(e1, ny1, i, j);
+          zb = (double)F.zA[nb2];
+        }
+        if (ua) F.zA[na] = (V)(za + pa);
+        if (ub) F.zA[nb2] = (V)(zb + pb);
       }
       if (!(ok = barrier())) break;
     }

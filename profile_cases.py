@@ -5,6 +5,7 @@ ncu (each runs a few launches of its kernels and exits):
     python profile_cases.py solve <cells> [jpcg|fcg|mg] [repeats] [coarse_cells] [fp64|mixed] [omega] [max_coarse_nodes]
     python profile_cases.py unet  <nodes> [repeats]
     python profile_cases.py diag  <deck> <ppc> [fp64|mixed] [repeats]
+    python profile_cases.py sort  <deck> <ppc> <drift_steps> [fp64|mixed] [repeats]
 
 step:  the deck at <ppc> particles per cell and species, <steps> steps.
 solve: the 8-ellipse deck at <cells>^2 without particles, a seeded random
@@ -13,6 +14,9 @@ solve: the 8-ellipse deck at <cells>^2 without particles, a seeded random
 unet:  forward passes of the learned stage's network on a <nodes>^2 grid.
 diag:  the deck after one step, then the device diagnostics (Average_x
        profiles, energy spectra, velocity moments) of every species.
+sort:  the deck after <drift_steps> steps from the initial sort, then the
+       counting sort of every species, <repeats> times with <drift_steps>
+       steps between (the sort alone is timed).
 Each prints one line with its own CUDA-event time.
 """
 from __future__ import annotations
@@ -128,8 +132,35 @@ def _diag(deck_name, ppc, precision="mixed", repeats=5):
     sim.close()
 
 
+def _sort(deck_name, ppc, drift_steps, precision="fp64", repeats=2):
+    import torch
+    from pic_b200 import api, deck
+    from pic_b200.simulation import Simulation
+    prec = api.PIC_PREC_MIXED if precision == "mixed" else api.PIC_PREC_FP64
+    # sort_interval beyond the run: only the sorts called here reorder
+    sim = Simulation(deck.config(deck_name, ppc=int(ppc), precision=prec, sort_interval=1 << 30))
+    sim.initial_fields()
+    sim.set_solver("fcg", multigrid=True, omega=0.8)
+    ms = 0.0
+    for _ in range(int(repeats)):
+        for _ in range(int(drift_steps)):
+            sim.step()
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        for s in range(len(sim.species)):
+            sim.sort(s)
+        e1.record()
+        torch.cuda.synchronize()
+        ms += e0.elapsed_time(e1)
+    n = [sim.count(s) for s in range(len(sim.species))]
+    print(f"sort {sim.cfg.name} {precision} particles {n} after {drift_steps} steps: "
+          f"{ms / int(repeats):.3f} ms (all species)")
+    sim.close()
+
+
 if __name__ == "__main__":
     if len(sys.argv) < 2:
         sys.exit(__doc__)
     case, rest = sys.argv[1], sys.argv[2:]
-    {"step": _step, "solve": _solve, "unet": _unet, "diag": _diag}[case](*rest)
+    {"step": _step, "solve": _solve, "unet": _unet, "diag": _diag, "sort": _sort}[case](*rest)
