@@ -171,7 +171,11 @@ struct Ctx {
   int push_stages = 4, push_grid = 0;       // tiled mixed push stages (0: one particle per thread)
   int push_minb = 5;                        // resident CTAs per SM the 4-stage push is built for
   int push64_grid = 0;                      // tiled FP64 push: persistent CTAs (0: direct kernel)
-  int push64_default = 1;                   // tiled FP64 push unless PIC_PUSH64_TILED=0
+  int push64_default = 2;                   // bulk-tiled FP64 push unless PIC_PUSH64_TILED=0 or 1
+  bool push64_bulk = false;                 // tiles bulk-copied (PIC_PUSH64_TILED=2)
+  bool push_bulk = false;                   // mixed-precision tiles bulk-copied (PIC_PUSH_BULK=1)
+  int push_bulk_default = 1;
+  long long push_wait_limit = 1ll << 22;    // polls of a tile's mbarrier before the push gives up
   // CUDA graphs of one FCG iteration: [0] stage A, [1 + slot] stage B + FCG
   // kernels of ring slot `slot`; rebuilt when the configuration key changes
   cudaGraphExec_t fcg_graph[2 + PIC_FCG_MAX_WINDOW] = {};

@@ -161,6 +161,7 @@ struct SpK {
   unsigned long long *q_acc, *e_acc;
   unsigned long long *lost, *bad;
   int64_t n;
+  unsigned long long *fail;  // a bounded wait of the bulk-staged push ran out
 };
 
 __constant__ ObjK c_obj;
@@ -799,6 +800,176 @@ __global__ void __launch_bounds__(256, 4) k_push_tiled(MeshK m, FieldK f, PushK 
 
 // FP64 absolute particles (staging set) -> FP32 offsets inside the located
 // element and FP32 velocities (live set).  Slots with loc < 0 are copied as 0.
+// FP64 push with bulk-copied tiles: one thread issues five 1-D
+// cp.async.bulk copies per 256-particle tile (x, y, vx, vy: 2 KB each; the
+// elements: 1 KB), which complete on the stage's mbarrier; the other threads
+// only wait on it, so no thread computes copy addresses.  Whole tiles are
+// copied, the last one too: the particle arrays are allocated in whole
+// tiles and slots at or beyond n are never used.  The wait is bounded: a
+// tile not complete after `limit` polls sets *s.fail, and the CTA leaves at
+// the next tile boundary.  The per-particle code is k_push's, bit for bit.
+__device__ __forceinline__ unsigned smem_u32(const void *p) { return (unsigned)__cvta_generic_to_shared(p); }
+
+__device__ __forceinline__ void mbar_init(uint64_t *b, unsigned count) {
+  asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;\n" ::"r"(smem_u32(b)), "r"(count) : "memory");
+}
+
+__device__ __forceinline__ void mbar_expect_tx(uint64_t *b, unsigned bytes) {
+  asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;\n" ::"r"(smem_u32(b)), "r"(bytes)
+               : "memory");
+}
+
+__device__ __forceinline__ bool mbar_try_wait(uint64_t *b, unsigned parity) {
+  unsigned ok;
+  asm volatile(
+      "{\n"
+      " .reg .pred p;\n"
+      " mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n"
+      " selp.u32 %0, 1, 0, p;\n"
+      "}\n"
+      : "=r"(ok)
+      : "r"(smem_u32(b)), "r"(parity)
+      : "memory");
+  return ok != 0;
+}
+
+__device__ __forceinline__ void bulk_g2s(void *dst, const void *src, unsigned bytes, uint64_t *b) {
+  asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];\n" ::"r"(
+                   smem_u32(dst)),
+               "l"(src), "r"(bytes), "r"(smem_u32(b))
+               : "memory");
+}
+
+__device__ __forceinline__ void push_tile64_bulk(PushTile64 *T, uint64_t *b, const SpK &s, int64_t base) {
+  mbar_expect_tx(b, (unsigned)sizeof(PushTile64));
+  bulk_g2s(T->x, s.x + base, 8 * kPushTile, b);
+  bulk_g2s(T->y, s.y + base, 8 * kPushTile, b);
+  bulk_g2s(T->vx, s.vx + base, 8 * kPushTile, b);
+  bulk_g2s(T->vy, s.vy + base, 8 * kPushTile, b);
+  bulk_g2s(T->loc, s.loc + base, 4 * kPushTile, b);
+}
+
+template <int S, bool AXI>
+__global__ void __launch_bounds__(256, 4) k_push_bulk(MeshK m, FieldK f, PushK prm, SpK s, int64_t ntiles,
+                                                      long long limit) {
+  extern __shared__ __align__(16) unsigned char push_smem[];
+  PushTile64 *T = reinterpret_cast<PushTile64 *>(push_smem);
+  uint64_t *bar = reinterpret_cast<uint64_t *>(push_smem + S * sizeof(PushTile64));
+  __shared__ int s_fail;
+  const int lane = threadIdx.x & 31;
+  const int64_t G = gridDim.x;
+  if (threadIdx.x == 0) {
+#pragma unroll
+    for (int k = 0; k < S; ++k) mbar_init(&bar[k], 1);
+    asm volatile("fence.mbarrier_init.release.cluster;\n" ::: "memory");
+    s_fail = 0;
+#pragma unroll
+    for (int k = 0; k < S - 1; ++k) {
+      const int64_t t = blockIdx.x + k * G;
+      if (t < ntiles) push_tile64_bulk(&T[k], &bar[k], s, t * kPushTile);
+    }
+  }
+  __syncthreads();
+  int it = 0;
+  for (int64_t t = blockIdx.x; t < ntiles; t += G, ++it) {
+    if (s_fail) break;  // read after the CTA barrier that ends each tile: the same for every thread
+    if (threadIdx.x == 0) {
+      const int64_t tn = t + (S - 1) * G;
+      // the stage refilled here was read in the previous tile, before its
+      // closing barrier; order those reads before the copy's writes
+      asm volatile("fence.proxy.async.shared::cta;\n" ::: "memory");
+      if (tn < ntiles) push_tile64_bulk(&T[(it + S - 1) % S], &bar[(it + S - 1) % S], s, tn * kPushTile);
+    }
+    const int st = it % S;
+    bool ready = false;
+    for (long long k = 0; k < limit && !ready; ++k) ready = mbar_try_wait(&bar[st], (unsigned)((it / S) & 1));
+    if (!ready) {
+      s_fail = 1;
+      atomicAdd(s.fail, 1ull);
+    }
+    const PushTile64 &C = T[st];
+    const int64_t p = t * kPushTile + threadIdx.x;
+    int key = -1;
+    double W[4] = {0, 0, 0, 0};
+    int nodes[4] = {0, 0, 0, 0};
+    double energy = 0.0;
+    bool lost = false;
+    if (ready && p < s.n) {
+      const int e = C.loc[threadIdx.x];
+      if (e >= 0)
+        push_fp64_one<AXI>(m, f, prm, s, p, e, C.x[threadIdx.x], C.y[threadIdx.x], C.vx[threadIdx.x],
+                           C.vy[threadIdx.x], key, W, nodes, energy, lost);
+    }
+    warp_deposit<!AXI>(s, lane, key, W, nodes, energy, lost, prm.do_deposit, prm.do_energy);
+    __syncthreads();  // tile t is read before its stage is refilled
+  }
+}
+
+// The mixed-precision push with bulk-copied tiles (elements and FP32
+// offsets and velocities: five 1 KB copies a tile), as k_push_bulk.
+__device__ __forceinline__ void push_tile_bulk(PushTile *T, uint64_t *b, const SpK &s, int64_t base) {
+  mbar_expect_tx(b, (unsigned)sizeof(PushTile));
+  bulk_g2s(T->loc, s.loc + base, 4 * kPushTile, b);
+  bulk_g2s(T->ax, reinterpret_cast<const float *>(s.x) + base, 4 * kPushTile, b);
+  bulk_g2s(T->ay, reinterpret_cast<const float *>(s.y) + base, 4 * kPushTile, b);
+  bulk_g2s(T->vx, reinterpret_cast<const float *>(s.vx) + base, 4 * kPushTile, b);
+  bulk_g2s(T->vy, reinterpret_cast<const float *>(s.vy) + base, 4 * kPushTile, b);
+}
+
+template <int S, int MINB, bool AXI>
+__global__ void __launch_bounds__(256, MINB) k_push_mixed_bulk(MeshK m, const float *__restrict__ c32, PushM prm,
+                                                             SpK s, int64_t ntiles, long long limit) {
+  extern __shared__ __align__(16) unsigned char push_smem[];
+  PushTile *T = reinterpret_cast<PushTile *>(push_smem);
+  uint64_t *bar = reinterpret_cast<uint64_t *>(push_smem + S * sizeof(PushTile));
+  __shared__ int s_fail;
+  const int lane = threadIdx.x & 31;
+  const int64_t G = gridDim.x;
+  if (threadIdx.x == 0) {
+#pragma unroll
+    for (int k = 0; k < S; ++k) mbar_init(&bar[k], 1);
+    asm volatile("fence.mbarrier_init.release.cluster;\n" ::: "memory");
+    s_fail = 0;
+#pragma unroll
+    for (int k = 0; k < S - 1; ++k) {
+      const int64_t t = blockIdx.x + k * G;
+      if (t < ntiles) push_tile_bulk(&T[k], &bar[k], s, t * kPushTile);
+    }
+  }
+  __syncthreads();
+  int it = 0;
+  for (int64_t t = blockIdx.x; t < ntiles; t += G, ++it) {
+    if (s_fail) break;  // read after the CTA barrier that ends each tile: the same for every thread
+    if (threadIdx.x == 0) {
+      const int64_t tn = t + (S - 1) * G;
+      asm volatile("fence.proxy.async.shared::cta;\n" ::: "memory");
+      if (tn < ntiles) push_tile_bulk(&T[(it + S - 1) % S], &bar[(it + S - 1) % S], s, tn * kPushTile);
+    }
+    const int st = it % S;
+    bool ready = false;
+    for (long long k = 0; k < limit && !ready; ++k) ready = mbar_try_wait(&bar[st], (unsigned)((it / S) & 1));
+    if (!ready) {
+      s_fail = 1;
+      atomicAdd(s.fail, 1ull);
+    }
+    const PushTile &C = T[st];
+    const int64_t p = t * kPushTile + threadIdx.x;
+    int key = -1;
+    double W[4] = {0, 0, 0, 0};
+    int nodes[4] = {0, 0, 0, 0};
+    double energy = 0.0;
+    bool lost = false;
+    if (ready && p < s.n) {
+      const int e = C.loc[threadIdx.x];
+      if (e >= 0)
+        push_mixed_one<AXI>(m, c32, prm, s, p, e, C.ax[threadIdx.x], C.ay[threadIdx.x], C.vx[threadIdx.x],
+                            C.vy[threadIdx.x], key, W, nodes, energy, lost);
+    }
+    warp_deposit<!AXI>(s, lane, key, W, nodes, energy, lost, prm.do_deposit, prm.do_energy);
+    __syncthreads();  // tile t is read before its stage is refilled
+  }
+}
+
 __global__ void k_to_mixed(MeshK m, const double *__restrict__ x, const double *__restrict__ y,
                            const double *__restrict__ vx, const double *__restrict__ vy,
                            const double *__restrict__ vz, const int32_t *__restrict__ loc, float *__restrict__ ox,
@@ -2440,7 +2611,7 @@ static int run_push(int sidx, bool do_push, bool do_deposit, bool do_energy) {
   prm.do_energy = do_deposit && do_energy;
   for (int w = 0; w < 4; ++w) prm.wall[w] = g.P.wall_bc[w];
   SpK k{s.x, s.y, s.vx, s.vy, s.vz, s.loc, s.q_acc, s.e_acc, g.d_counters + 8 + sidx, g.d_counters + 1,
-        s.n_slots};
+        s.n_slots, g.d_counters + 2};
   if (s.f32) {
     const MeshK m = mesh_k();
     PushM pm;
@@ -2458,7 +2629,18 @@ static int run_push(int sidx, bool do_push, bool do_deposit, bool do_energy) {
     pm.do_deposit = do_deposit;
     pm.do_energy = do_deposit && do_energy;
     for (int w = 0; w < 4; ++w) pm.wall[w] = g.P.wall_bc[w];
-    if (g.axi) {
+    if (g.push_bulk && g.push_stages) {
+      // tiles bulk-copied by one thread (4 stages, 5 CTAs per SM)
+      const int64_t ntiles = (s.n_slots + kPushTile - 1) / kPushTile;
+      const unsigned grid = (unsigned)std::min<int64_t>(ntiles, g.push_grid);
+      const size_t smem = 4 * sizeof(PushTile) + 4 * sizeof(uint64_t);
+      if (g.axi)
+        k_push_mixed_bulk<4, 5, true><<<grid, kPushTile, smem, g.st>>>(m, g.d_coef32, pm, k, ntiles,
+                                                                       g.push_wait_limit);
+      else
+        k_push_mixed_bulk<4, 5, false><<<grid, kPushTile, smem, g.st>>>(m, g.d_coef32, pm, k, ntiles,
+                                                                        g.push_wait_limit);
+    } else if (g.axi) {
       // r-z: the default tiled form (4 stages, 5 CTAs per SM) or the direct one
       if (g.push_stages) {
         const int64_t ntiles = (s.n_slots + kPushTile - 1) / kPushTile;
@@ -2484,6 +2666,14 @@ static int run_push(int sidx, bool do_push, bool do_deposit, bool do_energy) {
     } else {
       k_push_mixed<false><<<blocks_for(s.n_slots, 256), 256, 0, g.st>>>(m, g.d_coef32, pm, k);
     }
+  } else if (g.push64_grid > 0 && g.push64_bulk) {
+    const int64_t ntiles = (s.n_slots + kPushTile - 1) / kPushTile;
+    const unsigned grid = (unsigned)std::min<int64_t>(ntiles, g.push64_grid);
+    const size_t smem = 3 * sizeof(PushTile64) + 3 * sizeof(uint64_t);
+    if (g.axi)
+      k_push_bulk<3, true><<<grid, kPushTile, smem, g.st>>>(mesh_k(), f, prm, k, ntiles, g.push_wait_limit);
+    else
+      k_push_bulk<3, false><<<grid, kPushTile, smem, g.st>>>(mesh_k(), f, prm, k, ntiles, g.push_wait_limit);
   } else if (g.push64_grid > 0) {
     const int64_t ntiles = (s.n_slots + kPushTile - 1) / kPushTile;
     const unsigned grid = (unsigned)std::min<int64_t>(ntiles, g.push64_grid);
@@ -3788,21 +3978,32 @@ int pic_init(const pic_mesh_desc *mesh, const pic_params *params) {
                        : g.push_minb == 5   ? (const void *)k_push_mixed_tiled<4, 5>
                        : g.push_minb == 6   ? (const void *)k_push_mixed_tiled<4, 6>
                                             : (const void *)k_push_mixed_tiled<4>;
+      // PIC_PUSH_BULK=1 (default): the 4-stage, 5-CTA form with tiles
+      // bulk-copied by one thread and completing on mbarriers
+      const char *pb = getenv("PIC_PUSH_BULK");
+      g.push_bulk = (pb ? atoi(pb) == 1 : g.push_bulk_default) && g.push_stages == 4 && (g.axi || g.push_minb == 5);
+      if (g.push_bulk)
+        fn = g.axi ? (const void *)k_push_mixed_bulk<4, 5, true> : (const void *)k_push_mixed_bulk<4, 5, false>;
       int per_sm = 0;
-      PIC_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, fn, kPushTile,
-                                                             (size_t)g.push_stages * sizeof(PushTile)));
+      PIC_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(
+          &per_sm, fn, kPushTile, (size_t)g.push_stages * sizeof(PushTile) + (g.push_bulk ? 4 * sizeof(uint64_t) : 0)));
       g.push_grid = per_sm * nsm;
       if (g.push_grid <= 0) g.push_stages = 0;
     }
     // FP64 push: particle tiles (9 KB each, 3 stages = 27 KB per CTA) staged
     // through shared memory when PIC_PUSH64_TILED is 1; otherwise one
     // particle per thread loaded directly (same bits either way)
+    // (2: the tiles are bulk-copied by one thread and complete on mbarriers)
     const char *p64 = getenv("PIC_PUSH64_TILED");
+    const int mode64 = p64 ? atoi(p64) : g.push64_default;
     g.push64_grid = 0;
-    if (p64 ? atoi(p64) == 1 : g.push64_default) {
-      const void *fn = g.axi ? (const void *)k_push_tiled<3, true> : (const void *)k_push_tiled<3, false>;
+    g.push64_bulk = mode64 == 2;
+    if (mode64 == 1 || mode64 == 2) {
+      const void *fn = g.push64_bulk ? (g.axi ? (const void *)k_push_bulk<3, true> : (const void *)k_push_bulk<3, false>)
+                                     : (g.axi ? (const void *)k_push_tiled<3, true> : (const void *)k_push_tiled<3, false>);
+      const size_t smem = 3 * sizeof(PushTile64) + (g.push64_bulk ? 3 * sizeof(uint64_t) : 0);
       int per_sm = 0;
-      PIC_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, fn, kPushTile, 3 * sizeof(PushTile64)));
+      PIC_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, fn, kPushTile, smem));
       g.push64_grid = per_sm * nsm;
     }
   }
@@ -3830,7 +4031,9 @@ int pic_init(const pic_mesh_desc *mesh, const pic_params *params) {
     sp.capacity = d.capacity;
     sp.f32 = (P.precision == PIC_PREC_MIXED);
     maxcap = std::max(maxcap, d.capacity);
-    size_t c = (size_t)std::max<int64_t>(d.capacity, 1);
+    // whole 256-particle tiles, so that a push tile copy never reads past
+    // the allocation
+    size_t c = (size_t)(std::max<int64_t>(d.capacity, 1) + kPushTile - 1) / kPushTile * kPushTile;
     for (double **v : {&sp.x, &sp.y, &sp.vx, &sp.vy, &sp.vz, &sp.x2, &sp.y2, &sp.vx2, &sp.vy2, &sp.vz2})
       if ((rc = dalloc(v, c))) return rc;
     if ((rc = dalloc(&sp.loc, c))) return rc;
@@ -4022,6 +4225,19 @@ int pic_particle_positioning(int32_t species) {
   return PIC_OK;
 }
 
+// the bulk-staged FP64 push counts the tiles whose bounded wait ran out
+static int check_push_fail(const char *who) {
+  unsigned long long fail = 0;
+  int rc = read_counter(2, &fail);
+  if (rc) return rc;
+  if (fail) {
+    zero_counter(2);
+    set_error(std::string(who) + ": a push tile copy did not complete within its bounded wait");
+    return PIC_ERR_CUDA;
+  }
+  return PIC_OK;
+}
+
 static int count_live(int sidx) {
   Species &s = g.sp[sidx];
   unsigned long long lost = 0;
@@ -4037,6 +4253,7 @@ int pic_move_all(int32_t species, int32_t push_flag) {
   (void)push_flag;
   if ((rc = zero_counter(8 + species))) return rc;
   if ((rc = run_push(species, true, false, false))) return rc;
+  if ((rc = check_push_fail("pic_move_all"))) return rc;
   return count_live(species);
 }
 
@@ -4195,6 +4412,7 @@ int pic_step(uint64_t step, pic_step_stats *stats) {
   PIC_CUDA(cudaStreamSynchronize(g.st));
   unsigned long long bad = 0;
   if ((rc = read_counter(1, &bad))) return rc;
+  if ((rc = check_push_fail("pic_step"))) return rc;
   ++g.step_count;
   if (stats) {
     std::memset(stats, 0, sizeof *stats);

@@ -176,7 +176,12 @@ def test_axi_mixed_steps_track_fp64():
         assert abs(a - b) <= 0.01 * a
 
 
-def test_axi_tiled_push_matches_direct(monkeypatch):
+@pytest.mark.parametrize("bulk", ["0", "1"])
+def test_axi_tiled_push_matches_direct(bulk, monkeypatch):
+    """The r-z push with tiles (cp.async, or bulk copies on mbarriers) is
+    bit-identical to the one-particle-per-thread kernel over 5 steps."""
+    monkeypatch.setenv("PIC_PUSH_BULK", bulk)
+
     def fn(sim):
         sim.initial_fields()
         for _ in range(5):

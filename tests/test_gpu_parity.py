@@ -64,14 +64,15 @@ def _random_fields(sim, seed=1, scale=0.2):
 
 @pytest.fixture
 def push64(request, monkeypatch):
-    """FP64 push form: one particle per thread loaded directly, or particle
-    tiles staged through shared memory (PIC_PUSH64_TILED); both run the same
-    per-particle code."""
-    monkeypatch.setenv("PIC_PUSH64_TILED", "1" if request.param == "tiled" else "0")
+    """FP64 push form: one particle per thread loaded directly, particle
+    tiles staged through shared memory by per-thread cp.async copies, or by
+    one thread's bulk copies completing on mbarriers (PIC_PUSH64_TILED
+    0 / 1 / 2); all run the same per-particle code."""
+    monkeypatch.setenv("PIC_PUSH64_TILED", {"direct": "0", "tiled": "1", "bulk": "2"}[request.param])
     return request.param
 
 
-@pytest.mark.parametrize("push64", ["direct", "tiled"], indirect=True)
+@pytest.mark.parametrize("push64", ["direct", "tiled", "bulk"], indirect=True)
 @pytest.mark.parametrize("species", [0, 1])
 def test_move_all_bit_exact(species, push64):
     sim = _sim()
@@ -329,7 +330,7 @@ def _oracle_step(sim, parts, phi, step):
     return phi, st, rho
 
 
-@pytest.mark.parametrize("push64", ["direct", "tiled"], indirect=True)
+@pytest.mark.parametrize("push64", ["direct", "tiled", "bulk"], indirect=True)
 @pytest.mark.parametrize("name", ["tiny", "tiny_axi"])
 def test_full_steps_match_oracle(name, push64):
     sim = _sim(name, gas_p_Pa=300.0, Te_eV=20.0, sort_interval=3, diag_interval=4)

@@ -174,13 +174,17 @@ def test_fp32_inner_fcg_in_fp64_refinement():
     assert np.abs(pd - pm).max() <= 1e-5 * np.abs(pd).max()
 
 
-@pytest.mark.parametrize("stages", ["2", "3", "4"])
+@pytest.mark.parametrize("stages", ["2", "3", "4", "4-bulk"])
 def test_tiled_push_matches_direct(stages, monkeypatch):
-    """The push with particle tiles staged through shared memory (cp.async,
-    PIC_PUSH_STAGES = 2..4) runs the same per-particle code as the
-    one-particle-per-thread kernel: after 5 steps with MCC the particles,
-    counts and fields are bit-identical (the deposit sums are integers, so
-    their order does not matter)."""
+    """The push with particle tiles staged through shared memory (per-thread
+    cp.async copies, PIC_PUSH_STAGES = 2..4, or one thread's bulk copies
+    completing on mbarriers, PIC_PUSH_BULK=1) runs the same per-particle code
+    as the one-particle-per-thread kernel: after 5 steps with MCC the
+    particles, counts and fields are bit-identical (the deposit sums are
+    integers, so their order does not matter)."""
+    bulk = stages.endswith("-bulk")
+    monkeypatch.setenv("PIC_PUSH_BULK", "1" if bulk else "0")
+    stages = stages.split("-")[0]
     def fn(sim):
         sim.initial_fields()
         for _ in range(5):
