@@ -50,9 +50,9 @@ FP64_PUSH_BYTES_RZ = 88
 MIXED_PUSH_BYTES_RZ = 48
 # DRAM bytes per particle of one push launch measured by ncu (dram__bytes_read
 # + dram__bytes_write; the traffic grows in proportion to the particle count):
-# the 1024^2 eight-ellipse deck at 8 particles per cell (FP64 k_push_tiled,
-# mixed k_push_mixed_tiled) and the 2048x1024 r-z deck at 8 (mixed r-z)
-NCU_PUSH_TRAFFIC = {"fp64": 68.1, "mixed": 38.3, "mixed_rz": 51.8}
+# the 1024^2 eight-ellipse deck at 8 particles per cell (FP64 k_push_bulk,
+# mixed k_push_mixed_bulk) and the 2048x1024 r-z deck at 8 (mixed r-z)
+NCU_PUSH_TRAFFIC = {"fp64": 68.0, "mixed": 38.0, "mixed_rz": 51.4}
 
 
 def _dist():
@@ -327,10 +327,10 @@ def _push_roofline(precision: str, rz: bool, stats, peak, peak_src):
     push_n = sum(s.pushed for s in stats) / len(stats)
     if precision == "mixed":
         nbytes = MIXED_PUSH_BYTES_RZ if rz else MIXED_PUSH_BYTES
-        kernel = "k_push_mixed_tiled"
+        kernel = "k_push_mixed_bulk"
     else:
         nbytes = FP64_PUSH_BYTES_RZ if rz else FP64_PUSH_BYTES
-        kernel = "k_push_tiled"
+        kernel = "k_push_bulk"
     achieved = nbytes * push_n / (push_ms / 1e3) / 1e9
     key = precision + ("_rz" if rz else "")
     tr = NCU_PUSH_TRAFFIC[key] * push_n if key in NCU_PUSH_TRAFFIC else None
