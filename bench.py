@@ -43,8 +43,10 @@ ROOT = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, ROOT)
 
 METRIC = "particle pushes/s + Poisson ms/step: learned-precond FCG vs plain PCG at 1e-8"
-FP64_PUSH_BYTES = 80   # read x,y,vx,vy,elem (36 B) + vz on diagnostic steps, write x,y,vx,vy,elem (36 B)
+FP64_PUSH_BYTES = 72   # read x,y,vx,vy,elem (36 B; vz only on diagnostic steps), write the same (36 B)
 MIXED_PUSH_BYTES = 40  # read elem + 4 FP32 (20 B), write the same (20 B)
+# + the particle id (4 B) when the push builds the step's MCC selection
+SELECT_BYTES = 4
 # r-z decks (delta 1): v_theta is read and written on every step
 FP64_PUSH_BYTES_RZ = 88
 MIXED_PUSH_BYTES_RZ = 48
@@ -321,8 +323,9 @@ def _config(cfg, precision: str, particles: int, ws: int) -> dict:
                   + " (particle SoA %.2f GB)" % (particles * soa / 1e9)}
 
 
-def _push_roofline(precision: str, rz: bool, stats, peak, peak_src):
-    """Algorithmic bytes of the fused push per launch / its CUDA-event time."""
+def _push_roofline(precision: str, rz: bool, stats, peak, peak_src, select: bool = False):
+    """Algorithmic bytes of the fused push per launch / its CUDA-event time
+    (select: the push also reads each particle's id for the MCC selection)."""
     push_ms = sum(s.ms_push_kernel for s in stats) / len(stats)
     push_n = sum(s.pushed for s in stats) / len(stats)
     if precision == "mixed":
@@ -331,6 +334,7 @@ def _push_roofline(precision: str, rz: bool, stats, peak, peak_src):
     else:
         nbytes = FP64_PUSH_BYTES_RZ if rz else FP64_PUSH_BYTES
         kernel = "k_push_bulk"
+    nbytes += SELECT_BYTES if select else 0
     achieved = nbytes * push_n / (push_ms / 1e3) / 1e9
     key = precision + ("_rz" if rz else "")
     tr = NCU_PUSH_TRAFFIC[key] * push_n if key in NCU_PUSH_TRAFFIC else None
@@ -340,6 +344,12 @@ def _push_roofline(precision: str, rz: bool, stats, peak, peak_src):
             "traffic_note": ("no ncu capture of this push" if tr is None else
                              "ncu DRAM bytes/particle of one launch at 8 particles per cell (6.4M particles; "
                              "r-z 16.7M) x particles per step")}, push_ms
+
+
+def _push_select(cfg) -> bool:
+    """Whether the push builds the step's MCC selection (decks with MCC,
+    unless PIC_MCC_PUSH_SELECT=0)."""
+    return bool(cfg.mcc) and os.environ.get("PIC_MCC_PUSH_SELECT", "1") != "0"
 
 
 def _sel(sim, name, lp=None):
@@ -382,7 +392,7 @@ def _side_run(name, precision, solver, steps, warmup, peak, peak_src, dist):
             sim.step()
         _barrier(dist)
         ms, st = _timed_steps(sim, sim.lib, api, steps)
-        roof, push_ms = _push_roofline(precision, cfg.delta == 1, st, peak, peak_src)
+        roof, push_ms = _push_roofline(precision, cfg.delta == 1, st, peak, peak_src, _push_select(cfg))
         pushed = sum(s.pushed for s in st)
         return {"config": _config(cfg, precision, n0, 1), "solver": solver, "steps": steps,
                 "ms_per_step": ms / steps, "value": pushed / (ms / 1e3), "unit": "particle pushes/s",
@@ -490,7 +500,7 @@ def run_ours(args, dist, rank, ws):
     _barrier(dist)
     ms_e2e_max = _max_over_ranks(dist, ms_e2e.value)
     e2e_value = _sum_over_ranks(dist, float(e2e_pushed)) / (ms_e2e_max / 1e3)
-    roof, push_ms = _push_roofline(prec, cfg.delta == 1, stats, peak, peak_src)
+    roof, push_ms = _push_roofline(prec, cfg.delta == 1, stats, peak, peak_src, _push_select(cfg))
     solve_ms = [s.ms_solve for s in stats]
     its = [s.solve.iterations for s in stats]
     ms_step = ms_total / args.steps
@@ -521,6 +531,22 @@ def run_ours(args, dist, rank, ws):
         "learned_training": None if lp is None else {
             "warmup_steps": args.train_steps, "adam_steps": len(lp.losses), "seconds": train_s,
             "loss_first": lp.losses[0], "loss_last": lp.losses[-1]},
+        # the metric names the learned-preconditioner FCG; the product path is
+        # the fastest FCG variant on the same systems, and this says whether
+        # the learned stage is it
+        "learned_stage": None if "fcg_smooth_multigrid_learned" not in poisson else {
+            "on_product_path": best.endswith("_learned"),
+            "learned_ms": poisson["fcg_smooth_multigrid_learned"]["ms"],
+            "learned_iterations": poisson["fcg_smooth_multigrid_learned"]["iterations"],
+            "without_ms": poisson["fcg_smooth_multigrid"]["ms"],
+            "without_iterations": poisson["fcg_smooth_multigrid"]["iterations"],
+            "note": "the learned stage is on the product path" if best.endswith("_learned") else
+                    ("the learned stage on top of the multigrid V-cycle needs more FCG iterations than the "
+                     "V-cycle alone, so the product path runs without it")
+                    if poisson["fcg_smooth_multigrid_learned"]["iterations"]
+                    > poisson["fcg_smooth_multigrid"]["iterations"] else
+                    ("the network's forward pass costs more than the iterations it saves, so the product "
+                     "path runs without it")},
         "roofline": roof,
         "e2e": {"value": e2e_value, "unit": "particle pushes/s", "steps": e2e_steps,
                 "h2d_bytes_per_step": 8 * nn, "d2h_bytes_per_step": 4 * 8 * nn},

@@ -12,6 +12,7 @@
 #include "../../include/picgpu.h"
 #include "mg_dev.h"
 #include "pic_common.h"
+#include "pic_mcc_kin.h"
 
 namespace pic {
 
@@ -197,7 +198,7 @@ struct Ctx {
   // MCC
   pic_gas gas;
   bool mcc_ready = false;
-  uint32_t *d_hist = nullptr;          // [65536]
+  uint32_t *d_hist = nullptr;          // [65536] per species (the full selection uses species 0's)
   int32_t *d_sel = nullptr;            // selected slots
   uint64_t *d_cand = nullptr;          // candidates (key<<32 | id), slot in d_cand_slot
   int32_t *d_cand_slot = nullptr;
@@ -205,8 +206,14 @@ struct Ctx {
   int64_t cand_cap = 0;                // d_cand, d_cand_slot entries
   int64_t *d_mcc_misc = nullptr;       // [16] counters per species
   uint64_t *d_mlist_key = nullptr;     // bounded selection: (key << 32 | id) below the bound
-  int32_t *d_mlist_slot = nullptr;     //   and their slots
+  int32_t *d_mlist_slot = nullptr;     //   and their slots; mlist_cap entries per species
   int64_t mlist_cap = 0;
+  // the bounded selection of this step's MCC, built by the push
+  // (sel_step = the step it is for; sel_push: run_push passes the sinks)
+  bool mcc_push_select = true;  // PIC_MCC_PUSH_SELECT=0: off
+  MccSink sel_sink[PIC_MAX_SPECIES];
+  uint64_t sel_step = ~0ull;
+  bool sel_push = false;
   int mcc_full = 0;                    // 1: always the full-histogram selection
   double mcc_bound_scale = 1.0;        // test hook: < 1 forces the bounded selection's fallback
   int64_t *d_msel = nullptr;           // [8] per species: list count, keys below the bound, b*,
@@ -239,7 +246,8 @@ extern Ctx g;
 // kernels launched from other translation units
 int launch_locate(Species &s, int64_t begin, int64_t end);
 int sort_species(int sidx);
-int mcc_run(uint64_t step, pic_mcc_stats *stats);
+int mcc_run(uint64_t step, pic_mcc_stats *stats, bool prepared = false);
+int mcc_prepare(uint64_t step);
 int launch_spmv(const double *v, double *out);  // out = A v (solver operator)
 int coarse_setup(const pic_mesh_desc *mesh, int coarse_cells);
 int precond_apply(int full, const double *r, double *z);

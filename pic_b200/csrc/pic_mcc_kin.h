@@ -96,6 +96,46 @@ PIC_HD McSelect mcc_select_round_keys(uint32_t slo, uint32_t shi, uint32_t sp, u
 
 PIC_HD uint32_t mcc_select_key(uint32_t id, McSelect k) { return mcc_hash32(mcc_hash32(id ^ k.r0) ^ k.r1); }
 
+// Bounded selection: a key below `bound` enters bin floor(key 2^16 / bound)
+// of a 65536-bin histogram and a compact list of (key << 32 | id, slot).
+PIC_HD uint32_t mcc_bin(uint32_t key, uint64_t bound) { return (uint32_t)(((uint64_t)key << 16) / bound); }
+
+// Where one species' bounded selection is built, by the key pass
+// (k_mcc_scan) or by the push of the step (the particles it leaves live).
+struct MccSink {
+  int on;                   // 0: the push builds nothing
+  McSelect rk;              // round keys of this step and species
+  uint64_t bound;
+  const uint32_t *id;       // particle ids (read by the push)
+  uint32_t *hist;           // [65536]
+  uint64_t *lkey;           // [cap]
+  int32_t *lslot;           // [cap]
+  int64_t cap;
+  unsigned long long *cnt;  // list entries (may exceed cap: the selection then falls back)
+};
+
+#ifdef __CUDACC__
+// One warp's particles (want: live and below the bound): one list
+// reservation per warp; every lane takes part in the ballot.
+__device__ __forceinline__ void mcc_sink_put(const MccSink &k, int lane, bool want, uint32_t key, uint32_t id,
+                                             int64_t slot) {
+  const unsigned m = __ballot_sync(0xffffffffu, want);
+  if (!m) return;  // the same for every lane of the warp
+  const int leader = __ffs(m) - 1;
+  unsigned long long base = 0;
+  if (lane == leader) base = atomicAdd(k.cnt, (unsigned long long)__popc(m));
+  base = __shfl_sync(0xffffffffu, base, leader);
+  if (want) {
+    atomicAdd(k.hist + mcc_bin(key, k.bound), 1u);
+    const int64_t i = (int64_t)base + __popc(m & ((1u << lane) - 1u));
+    if (i < k.cap) {
+      k.lkey[i] = ((uint64_t)key << 32) | (uint64_t)id;
+      k.lslot[i] = (int32_t)slot;
+    }
+  }
+}
+#endif
+
 static inline int64_t mcc_n_collisions(int64_t npar, double ratio, uint32_t slo, uint32_t shi,
                                        uint32_t sp, uint32_t k0, uint32_t k1) {
   double x = (double)npar * ratio;

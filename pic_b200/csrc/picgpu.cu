@@ -162,6 +162,7 @@ struct SpK {
   unsigned long long *lost, *bad;
   int64_t n;
   unsigned long long *fail;  // a bounded wait of the bulk-staged push ran out
+  MccSink sel;               // the step's MCC selection, built from the particles left live
 };
 
 __constant__ ObjK c_obj;
@@ -280,6 +281,74 @@ __device__ __forceinline__ void warp_deposit(const SpK &s, int lane, int key, co
   if (head && key >= 0)
 #pragma unroll
     for (int c = 0; c < 4; ++c) atomicAdd(s.e_acc + nodes[c], (unsigned long long)ev[c]);
+}
+
+// The MCC selection of the step (the bounded one of the MCC pass, same
+// keys, same histogram and list) from the particles this push leaves live
+// (key >= 0: deposited), so the MCC pass does not read the particles again.
+// Every lane takes part.  The id is loaded at the start of the particle's
+// work (push_select_id), so its latency hides behind the push.
+__device__ __forceinline__ uint32_t push_select_id(const SpK &s, int64_t p) {
+  return s.sel.on && p < s.n ? __ldcs(s.sel.id + p) : 0u;
+}
+
+__device__ __forceinline__ void push_select(const SpK &s, int lane, int key, int64_t p, uint32_t id) {
+  if (!s.sel.on) return;  // the same for every lane
+  uint32_t k = 0;
+  bool want = false;
+  if (key >= 0) {
+    k = mcc_select_key(id, s.sel.rk);
+    want = (uint64_t)k < s.sel.bound;
+  }
+  mcc_sink_put(s.sel, lane, want, k, id, p);
+}
+
+// The same for the persistent bulk-staged pushes, without a global atomic
+// that a warp waits on inside the tile loop: entries go to a per-CTA
+// shared-memory buffer (a shared atomic each) and reach the global list in
+// one reservation when the CTA ends; past kSelBuf entries they go straight
+// to the global list.  Only lanes with a selected particle do anything.
+constexpr int kSelBuf = 256;
+struct SelBuf {
+  uint64_t key[kSelBuf];
+  int32_t slot[kSelBuf];
+  int n;
+  unsigned long long base;
+};
+
+__device__ __forceinline__ void push_select_cta(const SpK &s, int key, int64_t p, uint32_t id, SelBuf &b) {
+  if (!s.sel.on || key < 0) return;
+  const uint32_t k = mcc_select_key(id, s.sel.rk);
+  if ((uint64_t)k >= s.sel.bound) return;
+  atomicAdd(s.sel.hist + mcc_bin(k, s.sel.bound), 1u);
+  const uint64_t kv = ((uint64_t)k << 32) | (uint64_t)id;
+  const int i = atomicAdd(&b.n, 1);
+  if (i < kSelBuf) {
+    b.key[i] = kv;
+    b.slot[i] = (int32_t)p;
+  } else {
+    const unsigned long long j = atomicAdd(s.sel.cnt, 1ull);
+    if (j < (unsigned long long)s.sel.cap) {
+      s.sel.lkey[j] = kv;
+      s.sel.lslot[j] = (int32_t)p;
+    }
+  }
+}
+
+// every thread of the CTA, after its last tile
+__device__ __forceinline__ void push_select_flush(const SpK &s, SelBuf &b) {
+  if (!s.sel.on) return;  // the same for every thread
+  __syncthreads();
+  const int n = min(b.n, kSelBuf);
+  if (threadIdx.x == 0) b.base = n > 0 ? atomicAdd(s.sel.cnt, (unsigned long long)n) : 0ull;
+  __syncthreads();
+  for (int i = threadIdx.x; i < n; i += blockDim.x) {
+    const unsigned long long j = b.base + (unsigned long long)i;
+    if (j < (unsigned long long)s.sel.cap) {
+      s.sel.lkey[j] = b.key[i];
+      s.sel.lslot[j] = b.slot[i];
+    }
+  }
 }
 
 // Axisymmetric deposit weights (delta = 1, r = y), GetParChg_2D.f90:803-821:
@@ -418,6 +487,7 @@ __device__ __forceinline__ void push_fp64_one(const MeshK &m, const FieldK &f, c
 template <bool AXI>
 __global__ void __launch_bounds__(256, 4) k_push(MeshK m, FieldK f, PushK prm, SpK s) {
   int64_t p = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  const uint32_t pid = push_select_id(s, p);  // issued early: used after the push
   int lane = threadIdx.x & 31;
   int key = -1;
   double W[4] = {0, 0, 0, 0};
@@ -429,6 +499,7 @@ __global__ void __launch_bounds__(256, 4) k_push(MeshK m, FieldK f, PushK prm, S
     if (e >= 0) push_fp64_one<AXI>(m, f, prm, s, p, e, s.x[p], s.y[p], s.vx[p], s.vy[p], key, W, nodes, energy, lost);
   }
   warp_deposit<!AXI>(s, lane, key, W, nodes, energy, lost, prm.do_deposit, prm.do_energy);
+  push_select(s, lane, key, p, pid);
 }
 
 struct PushM {
@@ -616,6 +687,7 @@ __device__ __forceinline__ void push_mixed_one(const MeshK &m, const float *__re
 template <bool AXI>
 __global__ void __launch_bounds__(256, 4) k_push_mixed(MeshK m, const float *__restrict__ c32, PushM prm, SpK s) {
   const int64_t p = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  const uint32_t pid = push_select_id(s, p);  // issued early: used after the push
   const int lane = threadIdx.x & 31;
   int key = -1;
   double W[4] = {0, 0, 0, 0};
@@ -631,6 +703,7 @@ __global__ void __launch_bounds__(256, 4) k_push_mixed(MeshK m, const float *__r
     }
   }
   warp_deposit<!AXI>(s, lane, key, W, nodes, energy, lost, prm.do_deposit, prm.do_energy);
+  push_select(s, lane, key, p, pid);
 }
 
 // ---- the same push with the particle data staged through shared memory:
@@ -710,6 +783,7 @@ __global__ void __launch_bounds__(256, MINB) k_push_mixed_tiled(MeshK m, const f
     __syncthreads();         // and every thread's
     const PushTile &C = T[it % S];
     const int64_t p = t * kPushTile + threadIdx.x;
+    const uint32_t pid = push_select_id(s, p);  // issued early: used after the push
     int key = -1;
     double W[4] = {0, 0, 0, 0};
     int nodes[4] = {0, 0, 0, 0};
@@ -722,6 +796,7 @@ __global__ void __launch_bounds__(256, MINB) k_push_mixed_tiled(MeshK m, const f
                             C.vy[threadIdx.x], key, W, nodes, energy, lost);
     }
     warp_deposit<!AXI>(s, lane, key, W, nodes, energy, lost, prm.do_deposit, prm.do_energy);
+    push_select(s, lane, key, p, pid);
     __syncthreads();  // tile t is read before its stage is refilled
   }
   cp_async_wait<0>();
@@ -781,6 +856,7 @@ __global__ void __launch_bounds__(256, 4) k_push_tiled(MeshK m, FieldK f, PushK 
     __syncthreads();         // and every thread's
     const PushTile64 &C = T[it % S];
     const int64_t p = t * kPushTile + threadIdx.x;
+    const uint32_t pid = push_select_id(s, p);  // issued early: used after the push
     int key = -1;
     double W[4] = {0, 0, 0, 0};
     int nodes[4] = {0, 0, 0, 0};
@@ -793,6 +869,7 @@ __global__ void __launch_bounds__(256, 4) k_push_tiled(MeshK m, FieldK f, PushK 
                            C.vy[threadIdx.x], key, W, nodes, energy, lost);
     }
     warp_deposit<!AXI>(s, lane, key, W, nodes, energy, lost, prm.do_deposit, prm.do_energy);
+    push_select(s, lane, key, p, pid);
     __syncthreads();  // tile t is read before its stage is refilled
   }
   cp_async_wait<0>();
@@ -856,6 +933,7 @@ __global__ void __launch_bounds__(256, 4) k_push_bulk(MeshK m, FieldK f, PushK p
   PushTile64 *T = reinterpret_cast<PushTile64 *>(push_smem);
   uint64_t *bar = reinterpret_cast<uint64_t *>(push_smem + S * sizeof(PushTile64));
   __shared__ int s_fail;
+  __shared__ SelBuf sel_buf;
   const int lane = threadIdx.x & 31;
   const int64_t G = gridDim.x;
   if (threadIdx.x == 0) {
@@ -863,6 +941,7 @@ __global__ void __launch_bounds__(256, 4) k_push_bulk(MeshK m, FieldK f, PushK p
     for (int k = 0; k < S; ++k) mbar_init(&bar[k], 1);
     asm volatile("fence.mbarrier_init.release.cluster;\n" ::: "memory");
     s_fail = 0;
+    sel_buf.n = 0;
 #pragma unroll
     for (int k = 0; k < S - 1; ++k) {
       const int64_t t = blockIdx.x + k * G;
@@ -889,6 +968,7 @@ __global__ void __launch_bounds__(256, 4) k_push_bulk(MeshK m, FieldK f, PushK p
     }
     const PushTile64 &C = T[st];
     const int64_t p = t * kPushTile + threadIdx.x;
+    const uint32_t pid = push_select_id(s, p);  // issued early: used after the push
     int key = -1;
     double W[4] = {0, 0, 0, 0};
     int nodes[4] = {0, 0, 0, 0};
@@ -901,8 +981,10 @@ __global__ void __launch_bounds__(256, 4) k_push_bulk(MeshK m, FieldK f, PushK p
                            C.vy[threadIdx.x], key, W, nodes, energy, lost);
     }
     warp_deposit<!AXI>(s, lane, key, W, nodes, energy, lost, prm.do_deposit, prm.do_energy);
+    push_select_cta(s, key, p, pid, sel_buf);
     __syncthreads();  // tile t is read before its stage is refilled
   }
+  push_select_flush(s, sel_buf);
 }
 
 // The mixed-precision push with bulk-copied tiles (elements and FP32
@@ -923,6 +1005,7 @@ __global__ void __launch_bounds__(256, MINB) k_push_mixed_bulk(MeshK m, const fl
   PushTile *T = reinterpret_cast<PushTile *>(push_smem);
   uint64_t *bar = reinterpret_cast<uint64_t *>(push_smem + S * sizeof(PushTile));
   __shared__ int s_fail;
+  __shared__ SelBuf sel_buf;
   const int lane = threadIdx.x & 31;
   const int64_t G = gridDim.x;
   if (threadIdx.x == 0) {
@@ -930,6 +1013,7 @@ __global__ void __launch_bounds__(256, MINB) k_push_mixed_bulk(MeshK m, const fl
     for (int k = 0; k < S; ++k) mbar_init(&bar[k], 1);
     asm volatile("fence.mbarrier_init.release.cluster;\n" ::: "memory");
     s_fail = 0;
+    sel_buf.n = 0;
 #pragma unroll
     for (int k = 0; k < S - 1; ++k) {
       const int64_t t = blockIdx.x + k * G;
@@ -954,6 +1038,7 @@ __global__ void __launch_bounds__(256, MINB) k_push_mixed_bulk(MeshK m, const fl
     }
     const PushTile &C = T[st];
     const int64_t p = t * kPushTile + threadIdx.x;
+    const uint32_t pid = push_select_id(s, p);  // issued early: used after the push
     int key = -1;
     double W[4] = {0, 0, 0, 0};
     int nodes[4] = {0, 0, 0, 0};
@@ -966,8 +1051,10 @@ __global__ void __launch_bounds__(256, MINB) k_push_mixed_bulk(MeshK m, const fl
                             C.vy[threadIdx.x], key, W, nodes, energy, lost);
     }
     warp_deposit<!AXI>(s, lane, key, W, nodes, energy, lost, prm.do_deposit, prm.do_energy);
+    push_select_cta(s, key, p, pid, sel_buf);
     __syncthreads();  // tile t is read before its stage is refilled
   }
+  push_select_flush(s, sel_buf);
 }
 
 __global__ void k_to_mixed(MeshK m, const double *__restrict__ x, const double *__restrict__ y,
@@ -2612,6 +2699,7 @@ static int run_push(int sidx, bool do_push, bool do_deposit, bool do_energy) {
   for (int w = 0; w < 4; ++w) prm.wall[w] = g.P.wall_bc[w];
   SpK k{s.x, s.y, s.vx, s.vy, s.vz, s.loc, s.q_acc, s.e_acc, g.d_counters + 8 + sidx, g.d_counters + 1,
         s.n_slots, g.d_counters + 2};
+  if (g.sel_push && do_deposit) k.sel = g.sel_sink[sidx];  // otherwise off (zero)
   if (s.f32) {
     const MeshK m = mesh_k();
     PushM pm;
@@ -3956,6 +4044,8 @@ int pic_init(const pic_mesh_desc *mesh, const pic_params *params) {
     // directly
     const char *mf = getenv("PIC_MCC_FULL");  // 1: MCC selection by the full key histogram
     g.mcc_full = (mf && atoi(mf) == 1) ? 1 : 0;
+    const char *mps = getenv("PIC_MCC_PUSH_SELECT");  // 0: the MCC pass reads the particles itself
+    g.mcc_push_select = mps ? atoi(mps) != 0 : true;
     const char *mb2 = getenv("PIC_MCC_BOUND_SCALE");  // test hook (see mcc_bound_scale)
     g.mcc_bound_scale = mb2 ? std::max(1e-6, atof(mb2)) : 1.0;
     const char *ps = getenv("PIC_PUSH_STAGES");
@@ -4380,9 +4470,16 @@ int pic_step(uint64_t step, pic_step_stats *stats) {
     pushed += before[s];
     if ((rc = zero_counter(8 + s))) return rc;
   }
+  // the MCC selection of this step is built by the push itself
+  if (g.mcc_ready && g.mcc_push_select && (rc = mcc_prepare(step))) return rc;
   PIC_CUDA(cudaEventRecord(e[6], g.st));
+  g.sel_push = g.sel_step == step;
   for (int s = 0; s < g.ns; ++s)
-    if ((rc = run_push(s, true, true, diag))) return rc;
+    if ((rc = run_push(s, true, true, diag))) {
+      g.sel_push = false;
+      return rc;
+    }
+  g.sel_push = false;
   PIC_CUDA(cudaEventRecord(e[7], g.st));
   if ((rc = run_rho(diag))) return rc;
   PIC_CUDA(cudaEventRecord(e[1], g.st));
@@ -4402,7 +4499,7 @@ int pic_step(uint64_t step, pic_step_stats *stats) {
   pic_mcc_stats ms;
   std::memset(&ms, 0, sizeof ms);
   if (g.mcc_ready)
-    if ((rc = mcc_run(step, &ms))) return rc;
+    if ((rc = mcc_run(step, &ms, true))) return rc;
   PIC_CUDA(cudaEventRecord(e[4], g.st));
   // 5. counting sort
   if ((int64_t)(step % (uint64_t)g.P.sort_interval) == 0)

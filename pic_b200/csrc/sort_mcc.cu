@@ -336,16 +336,12 @@ __global__ void k_mcc_pick(MccK k, const uint32_t *__restrict__ keys, uint32_t b
 // one the full histogram gives: the ncoll smallest (key, id).  When fewer
 // than ncoll keys lie below the bound, or the list overflows, the host
 // reruns the selection with the full histogram.
-__device__ __forceinline__ uint32_t mcc_bin(uint32_t key, uint64_t bound) {
-  return (uint32_t)(((uint64_t)key << 16) / bound);
-}
 
 // Four consecutive slots per thread: their elements and ids come in one
 // 16-byte load each, issued together and unconditionally, so every thread
 // keeps 32 bytes in flight (one 4-byte load that a second one waits on left
 // the pass latency-bound at a quarter of the memory bandwidth).
-__global__ void k_mcc_scan(MccK k, uint64_t bound, uint32_t *__restrict__ hist, uint64_t *__restrict__ lkey,
-                           int32_t *__restrict__ lslot, int64_t cap, unsigned long long *__restrict__ cnt) {
+__global__ void k_mcc_scan(MccK k, MccSink sink) {
   const int64_t p0 = 4 * ((int64_t)blockIdx.x * blockDim.x + threadIdx.x);
   const int lane = threadIdx.x & 31;
   int loc[4];
@@ -364,23 +360,8 @@ __global__ void k_mcc_scan(MccK k, uint64_t bound, uint32_t *__restrict__ hist, 
   }
 #pragma unroll
   for (int u = 0; u < 4; ++u) {
-    const uint32_t key = mcc_select_key(id[u], k.sel);
-    const bool want = loc[u] >= 0 && (uint64_t)key < bound;
-    // one list slot reservation per warp; every lane takes part in the ballot
-    const unsigned m = __ballot_sync(0xffffffffu, want);
-    if (!m) continue;  // the same for every lane of the warp
-    const int leader = __ffs(m) - 1;
-    unsigned long long base = 0;
-    if (lane == leader) base = atomicAdd(cnt, (unsigned long long)__popc(m));
-    base = __shfl_sync(0xffffffffu, base, leader);
-    if (want) {
-      atomicAdd(hist + mcc_bin(key, bound), 1u);
-      const int64_t i = (int64_t)base + __popc(m & ((1u << lane) - 1u));
-      if (i < cap) {
-        lkey[i] = ((uint64_t)key << 32) | (uint64_t)id[u];
-        lslot[i] = (int32_t)(p0 + u);
-      }
-    }
+    const uint32_t key = mcc_select_key(id[u], sink.rk);
+    mcc_sink_put(sink, lane, loc[u] >= 0 && (uint64_t)key < sink.bound, key, id[u], p0 + u);
   }
 }
 
@@ -629,8 +610,8 @@ static int mcc_list_alloc(int64_t need) {
   g.d_mlist_key = nullptr;
   g.d_mlist_slot = nullptr;
   g.mlist_cap = 0;
-  PIC_CUDA(cudaMalloc(&g.d_mlist_key, cap * sizeof(uint64_t)));
-  PIC_CUDA(cudaMalloc(&g.d_mlist_slot, cap * sizeof(int32_t)));
+  PIC_CUDA(cudaMalloc(&g.d_mlist_key, PIC_MAX_SPECIES * cap * sizeof(uint64_t)));
+  PIC_CUDA(cudaMalloc(&g.d_mlist_slot, PIC_MAX_SPECIES * cap * sizeof(int32_t)));
   g.mlist_cap = cap;
   return PIC_OK;
 }
@@ -712,7 +693,69 @@ static int mcc_host_alloc(void **buf, int64_t *cap, int64_t bytes) {
 // blocks then finds the species (rarely any) that need the full selection,
 // and one more brings back the ionisations; the created particles are
 // appended from pinned staging without a further wait.
-int mcc_run(uint64_t step, pic_mcc_stats *stats) {
+// the bounded selection's sink of species s: key bound, list capacity,
+// per-species histogram, list and counters
+static MccSink mcc_sink(int s, uint64_t bound, int64_t lcap, uint32_t slo, uint32_t shi) {
+  MccSink k;
+  k.on = 1;
+  k.rk = mcc_select_round_keys(slo, shi, (uint32_t)s, (uint32_t)g.P.seed, (uint32_t)(g.P.seed >> 32));
+  k.bound = bound;
+  k.id = g.sp[s].id;
+  k.hist = g.d_hist + (size_t)s * 65536;
+  k.lkey = g.d_mlist_key + (size_t)s * g.mlist_cap;
+  k.lslot = g.d_mlist_slot + (size_t)s * g.mlist_cap;
+  k.cap = lcap;
+  k.cnt = reinterpret_cast<unsigned long long *>(g.d_msel + s * kMccSel);
+  return k;
+}
+
+// the key bound that holds about `target` of n live keys (g.mcc_bound_scale
+// < 1, a test hook, makes it too small, so the selection takes its fallback)
+static uint64_t mcc_bound(double target, double n) {
+  return std::max<uint64_t>(1, (uint64_t)std::ceil(g.mcc_bound_scale * target / n * 4294967296.0));
+}
+
+// about 2 ncoll + 64 keys below the bound, plus 8 standard deviations
+static double mcc_target(double ncoll) { return 2.0 * ncoll + 64.0 + 8.0 * std::sqrt(2.0 * ncoll + 64.0); }
+
+// Before the push of a step: the bounded selection of every species with
+// MCC, sized for an upper bound of the step's ncoll (the push only removes
+// particles), histograms and counters zeroed; the push fills them from the
+// particles it leaves live (push_select) and mcc_run(prepared) goes on from
+// there without reading the particles again.
+int mcc_prepare(uint64_t step) {
+  g.sel_step = ~0ull;
+  const uint32_t slo = (uint32_t)step, shi = (uint32_t)(step >> 32);
+  int64_t lcap[PIC_MAX_SPECIES] = {0}, lmax = 0;
+  double target[PIC_MAX_SPECIES] = {0};
+  for (int s = 0; s < g.ns; ++s) {
+    g.sel_sink[s] = MccSink();
+    g.sel_sink[s].on = 0;
+    Species &sp = g.sp[s];
+    if (!sp.has_mcc || sp.n_live == 0) continue;
+    const int64_t nmax = (int64_t)((double)sp.n_live * sp.tab.collision_ratio) + 1;
+    target[s] = mcc_target((double)nmax);
+    if (g.mcc_full || target[s] >= 0.25 * (double)sp.n_live) continue;
+    lcap[s] = (int64_t)(1.5 * target[s]) + 4096;
+    lmax = std::max(lmax, lcap[s]);
+  }
+  if (lmax == 0) return PIC_OK;
+  int rc;
+  if ((rc = mcc_list_alloc(lmax))) return rc;
+  for (int s = 0; s < g.ns; ++s) {
+    if (lcap[s] == 0) continue;
+    g.sel_sink[s] = mcc_sink(s, mcc_bound(target[s], (double)g.sp[s].n_live), lcap[s], slo, shi);
+    PIC_CUDA(cudaMemsetAsync(g.sel_sink[s].hist, 0, 65536 * sizeof(uint32_t), g.st));
+    PIC_CUDA(cudaMemsetAsync(g.d_msel + s * kMccSel, 0, kMccSel * sizeof(int64_t), g.st));
+  }
+  g.sel_step = step;
+  return PIC_OK;
+}
+
+int mcc_run(uint64_t step, pic_mcc_stats *stats, bool prepared) {
+  // the push of this step built the bounded selections (mcc_prepare)
+  const bool prep = prepared && g.sel_step == step;
+  g.sel_step = ~0ull;
   const uint32_t seed0 = (uint32_t)g.P.seed, seed1 = (uint32_t)(g.P.seed >> 32);
   const uint32_t slo = (uint32_t)step, shi = (uint32_t)(step >> 32);
   int64_t ncoll[PIC_MAX_SPECIES] = {0};
@@ -732,10 +775,14 @@ int mcc_run(uint64_t step, pic_mcc_stats *stats) {
   int64_t lcap[PIC_MAX_SPECIES] = {0}, lmax = 0;
   for (int s = 0; s < g.ns; ++s) {
     if (ncoll[s] <= 0) continue;
-    const double npar = (double)g.sp[s].n_live, nc = (double)ncoll[s];
+    if (prep) {  // the prepared selections, whatever this step's ncoll
+      bounded[s] = g.sel_sink[s].on != 0;
+      continue;
+    }
+    const double npar = (double)g.sp[s].n_live;
     // the bound holds about 2 ncoll + 64 live keys (plus 8 standard
     // deviations); used while that is a small part of the species
-    const double target = 2.0 * nc + 64.0 + 8.0 * std::sqrt(2.0 * nc + 64.0);
+    const double target = mcc_target((double)ncoll[s]);
     if (g.mcc_full || target >= 0.25 * npar) continue;
     bounded[s] = true;
     lcap[s] = (int64_t)(1.5 * target) + 4096;
@@ -744,9 +791,8 @@ int mcc_run(uint64_t step, pic_mcc_stats *stats) {
   int rc;
   if ((rc = mcc_alloc(std::max<int64_t>(most, 1 << 16) + 4096))) return rc;
   if ((rc = mcc_cand_alloc(g.mcc_cap))) return rc;
-  if ((rc = mcc_list_alloc(lmax))) return rc;
+  if ((rc = mcc_list_alloc(lmax))) return rc;  // no growth when prepared (lmax 0)
   PIC_CUDA(cudaMemsetAsync(g.d_mcc_misc, 0, PIC_MAX_SPECIES * kMccMisc * sizeof(int64_t), g.st));
-  PIC_CUDA(cudaMemsetAsync(g.d_msel, 0, PIC_MAX_SPECIES * kMccSel * sizeof(int64_t), g.st));
   auto mk = [&](int s) {
     Species &sp = g.sp[s];
     return MccK{sp.x, sp.y, sp.vx, sp.vy, sp.vz, sp.loc, sp.id, sp.n_slots, seed0, seed1, slo, shi, (uint32_t)s,
@@ -776,25 +822,25 @@ int mcc_run(uint64_t step, pic_mcc_stats *stats) {
   // 1. bounded selections and their collisions, queued
   for (int s = 0; s < g.ns; ++s) {
     if (!bounded[s]) continue;
-    const double npar = (double)g.sp[s].n_live, nc = (double)ncoll[s];
-    const double target = 2.0 * nc + 64.0 + 8.0 * std::sqrt(2.0 * nc + 64.0);
-    // g.mcc_bound_scale < 1 (a test hook) makes the bound too small, so the
-    // selection takes its fallback
-    const uint64_t bound =
-        std::max<uint64_t>(1, (uint64_t)std::ceil(g.mcc_bound_scale * target / npar * 4294967296.0));
-    const MccK k = mk(s);
     int64_t *ms = g.d_msel + s * kMccSel, *misc = g.d_mcc_misc + s * kMccMisc;
-    unsigned long long *cnt = reinterpret_cast<unsigned long long *>(ms);
-    PIC_CUDA(cudaMemsetAsync(g.d_hist, 0, 65536 * sizeof(uint32_t), g.st));
-    k_mcc_scan<<<blocks_for((k.n + 3) / 4, 256), 256, 0, g.st>>>(k, bound, g.d_hist, g.d_mlist_key,
-                                                                 g.d_mlist_slot, lcap[s], cnt);
+    MccSink sink;
+    if (prep) {
+      sink = g.sel_sink[s];
+    } else {
+      sink = mcc_sink(s, mcc_bound(mcc_target((double)ncoll[s]), (double)g.sp[s].n_live), lcap[s], slo, shi);
+      PIC_CUDA(cudaMemsetAsync(sink.hist, 0, 65536 * sizeof(uint32_t), g.st));
+      PIC_CUDA(cudaMemsetAsync(ms, 0, kMccSel * sizeof(int64_t), g.st));
+      const MccK k = mk(s);
+      k_mcc_scan<<<blocks_for((k.n + 3) / 4, 256), 256, 0, g.st>>>(k, sink);
+      PIC_LAUNCHED();
+    }
+    k_mcc_bstar<<<1, 1024, 0, g.st>>>(sink.hist, ncoll[s], ms);
     PIC_LAUNCHED();
-    k_mcc_bstar<<<1, 1024, 0, g.st>>>(g.d_hist, ncoll[s], ms);
+    k_mcc_pick_list<<<(unsigned)std::min<int64_t>(blocks_for(sink.cap, 256), 1184), 256, 0, g.st>>>(
+        sink.lkey, sink.lslot, sink.cnt, sink.cap, sink.bound, ms, g.d_sel, g.d_cand, g.d_cand_slot, g.cand_cap,
+        misc);
     PIC_LAUNCHED();
-    k_mcc_pick_list<<<(unsigned)std::min<int64_t>(blocks_for(lcap[s], 256), 1184), 256, 0, g.st>>>(
-        g.d_mlist_key, g.d_mlist_slot, cnt, lcap[s], bound, ms, g.d_sel, g.d_cand, g.d_cand_slot, g.cand_cap, misc);
-    PIC_LAUNCHED();
-    k_mcc_ties<<<1, 1024, 0, g.st>>>(g.d_cand, g.d_cand_slot, g.cand_cap, lcap[s], ms, misc, ncoll[s], g.d_sel);
+    k_mcc_ties<<<1, 1024, 0, g.st>>>(g.d_cand, g.d_cand_slot, g.cand_cap, sink.cap, ms, misc, ncoll[s], g.d_sel);
     PIC_LAUNCHED();
     if ((rc = collide(s, ms + 4))) return rc;
   }
@@ -950,7 +996,7 @@ extern "C" int pic_mcc_init(const pic_gas *gas, int32_t n_tables, const pic_mcc_
     PIC_CUDA(cudaMemcpy(sp.prob, T.probability, n * sizeof(double), cudaMemcpyHostToDevice));
     sp.tab.probability = nullptr;
   }
-  if (!g.d_hist) PIC_CUDA(cudaMalloc(&g.d_hist, 65536 * sizeof(uint32_t)));
+  if (!g.d_hist) PIC_CUDA(cudaMalloc(&g.d_hist, PIC_MAX_SPECIES * 65536 * sizeof(uint32_t)));
   if (!g.d_mcc_misc) PIC_CUDA(cudaMalloc(&g.d_mcc_misc, PIC_MAX_SPECIES * kMccMisc * sizeof(int64_t)));
   g.mcc_ready = n_tables > 0;
   return PIC_OK;

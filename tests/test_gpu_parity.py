@@ -425,8 +425,9 @@ def test_edge_cases():
                                             (api.PIC_PREC_MIXED, "fallback")])
 def test_mcc_bounded_selection_matches_full(precision, mode, monkeypatch):
     """The selection under a key bound (histogram and compact list of the
-    keys below it, threshold and ties found on the device) picks the same
-    ncoll smallest (key, id) as the full key histogram (PIC_MCC_FULL=1):
+    keys below it, built by the step's push from the particles it leaves
+    live; threshold and ties found on the device) picks the same ncoll
+    smallest (key, id) as the full key histogram (PIC_MCC_FULL=1):
     after 6 steps with MCC the particles, fields and reaction counts are
     bit-identical.  "fallback": the bound made too small (a test hook), so
     every bounded selection finds too few keys and redoes the selection with
