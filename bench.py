@@ -53,8 +53,10 @@ MIXED_PUSH_BYTES_RZ = 48
 # DRAM bytes per particle of one push launch measured by ncu (dram__bytes_read
 # + dram__bytes_write; the traffic grows in proportion to the particle count):
 # the 1024^2 eight-ellipse deck at 8 particles per cell (FP64 k_push_bulk,
-# mixed k_push_mixed_bulk) and the 2048x1024 r-z deck at 8 (mixed r-z)
-NCU_PUSH_TRAFFIC = {"fp64": 68.0, "mixed": 38.0, "mixed_rz": 51.4}
+# mixed k_push_mixed_bulk) and the 2048x1024 r-z deck at 8 (mixed r-z);
+# "_sel": the push also builds the MCC selection (reads the ids)
+NCU_PUSH_TRAFFIC = {"fp64": 68.0, "mixed": 38.0, "mixed_rz": 51.4,
+                    "fp64_sel": 72.3, "mixed_sel": 42.3}
 
 
 def _dist():
@@ -336,7 +338,7 @@ def _push_roofline(precision: str, rz: bool, stats, peak, peak_src, select: bool
         kernel = "k_push_bulk"
     nbytes += SELECT_BYTES if select else 0
     achieved = nbytes * push_n / (push_ms / 1e3) / 1e9
-    key = precision + ("_rz" if rz else "")
+    key = precision + ("_rz" if rz else "") + ("_sel" if select else "")
     tr = NCU_PUSH_TRAFFIC[key] * push_n if key in NCU_PUSH_TRAFFIC else None
     return {"kernel": kernel + (" r-z" if rz else "") + " (fused push+locate+deposit)", "bound": "hbm",
             "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,

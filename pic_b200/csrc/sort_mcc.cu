@@ -45,13 +45,26 @@ __device__ __forceinline__ void warp_runs(int key, int lane, int *head, int *len
   *rank = lane - *head;
 }
 
+// Both passes give each warp 128 consecutive slots, 32 per round: the four
+// rounds' loads are issued together (a single 4-byte load per thread left
+// the passes waiting on memory latency), then each round aggregates its runs.
+constexpr int kSortRounds = 4;
+
 __global__ void k_sort_count(const int32_t *__restrict__ loc, int64_t n, int32_t *__restrict__ count) {
-  int64_t p = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
-  int key = (p < n) ? loc[p] : -1;
   const int lane = threadIdx.x & 31;
-  int head, len, rank;
-  warp_runs(key, lane, &head, &len, &rank);
-  if (key >= 0 && rank == 0) atomicAdd(count + key, len);
+  const int64_t wbase = ((int64_t)blockIdx.x * blockDim.x + (threadIdx.x & ~31)) * kSortRounds;
+  int key[kSortRounds];
+#pragma unroll
+  for (int u = 0; u < kSortRounds; ++u) {
+    const int64_t p = wbase + 32 * u + lane;
+    key[u] = p < n ? loc[p] : -1;
+  }
+#pragma unroll
+  for (int u = 0; u < kSortRounds; ++u) {
+    int head, len, rank;
+    warp_runs(key[u], lane, &head, &len, &rank);
+    if (key[u] >= 0 && rank == 0) atomicAdd(count + key[u], len);
+  }
 }
 
 // exclusive scan, 3 passes of 4096 items per block
@@ -107,21 +120,33 @@ static int scan_exclusive(int32_t *in, int32_t *out, int64_t n) {
   return PIC_OK;
 }
 
+// the four rounds' cursor reservations are also in flight together
 __global__ void k_sort_scatter(const int32_t *__restrict__ loc, const uint32_t *__restrict__ id, int64_t n,
                                int32_t *__restrict__ cursor, int32_t *__restrict__ perm,
                                uint32_t *__restrict__ sid) {
-  int64_t p = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
-  int key = (p < n) ? loc[p] : -1;
   const int lane = threadIdx.x & 31;
-  int head, len, rank;
-  warp_runs(key, lane, &head, &len, &rank);
-  int base = 0;
-  if (key >= 0 && rank == 0) base = atomicAdd(cursor + key, len);
-  base = __shfl_sync(0xffffffffu, base, head);
-  if (key >= 0) {
-    const int dst = base + rank;
-    perm[dst] = (int32_t)p;
-    sid[dst] = id[p];
+  const int64_t wbase = ((int64_t)blockIdx.x * blockDim.x + (threadIdx.x & ~31)) * kSortRounds;
+  int key[kSortRounds], head[kSortRounds], len[kSortRounds], rank[kSortRounds], base[kSortRounds];
+  uint32_t pid[kSortRounds];
+#pragma unroll
+  for (int u = 0; u < kSortRounds; ++u) {
+    const int64_t p = wbase + 32 * u + lane;
+    key[u] = p < n ? loc[p] : -1;
+    pid[u] = p < n ? id[p] : 0u;
+  }
+#pragma unroll
+  for (int u = 0; u < kSortRounds; ++u) warp_runs(key[u], lane, &head[u], &len[u], &rank[u]);
+#pragma unroll
+  for (int u = 0; u < kSortRounds; ++u)
+    base[u] = (key[u] >= 0 && rank[u] == 0) ? atomicAdd(cursor + key[u], len[u]) : 0;
+#pragma unroll
+  for (int u = 0; u < kSortRounds; ++u) {
+    const int b = __shfl_sync(0xffffffffu, base[u], head[u]);
+    if (key[u] >= 0) {
+      const int dst = b + rank[u];
+      perm[dst] = (int32_t)(wbase + 32 * u + lane);
+      sid[dst] = pid[u];
+    }
   }
 }
 
@@ -229,7 +254,7 @@ int sort_species(int sidx) {
   const int64_t ne = g.ne;
   if (s.n_slots == 0) return PIC_OK;
   PIC_CUDA(cudaMemsetAsync(g.d_cell_count, 0, (ne + 1) * sizeof(int32_t), g.st));
-  k_sort_count<<<blocks_for(s.n_slots, 256), 256, 0, g.st>>>(s.loc, s.n_slots, g.d_cell_count);
+  k_sort_count<<<blocks_for(s.n_slots, 256 * kSortRounds), 256, 0, g.st>>>(s.loc, s.n_slots, g.d_cell_count);
   PIC_LAUNCHED();
   int rc = scan_exclusive(g.d_cell_count, g.d_cell_start, ne + 1);
   if (rc) return rc;
@@ -237,8 +262,8 @@ int sort_species(int sidx) {
                            cudaMemcpyDeviceToDevice, g.st));
   int32_t total = 0;
   PIC_CUDA(cudaMemcpyAsync(&total, g.d_cell_start + ne, sizeof total, cudaMemcpyDeviceToHost, g.st));
-  k_sort_scatter<<<blocks_for(s.n_slots, 256), 256, 0, g.st>>>(s.loc, s.id, s.n_slots, g.d_cell_fill,
-                                                               g.d_perm, g.d_sort_id);
+  k_sort_scatter<<<blocks_for(s.n_slots, 256 * kSortRounds), 256, 0, g.st>>>(s.loc, s.id, s.n_slots,
+                                                                             g.d_cell_fill, g.d_perm, g.d_sort_id);
   PIC_LAUNCHED();
   k_sort_cells<<<blocks_for(ne, 8), 256, 0, g.st>>>(g.d_cell_start, ne, g.d_perm, g.d_sort_id, g.d_perm2);
   PIC_LAUNCHED();
