@@ -119,35 +119,39 @@ __device__ __forceinline__ void mg_restrict_node(const MgLevel &L, const T *__re
   if (smoothed) L.z[n] = (w * r) * (double)L.dinv[n];
 }
 
-// down-sweep at node n: t = r - A z with z = w D^-1 r stored by the
-// restriction (mg_restrict_node)
-__device__ __forceinline__ void mg_smooth_node(const MgLevel &L, int64_t n) {
+// The down- and up-sweep values at node n.  Every load is issued whatever
+// the node's kind and the result selected at the end (0 on inactive nodes),
+// so no load waits on D^-1: the same numbers as testing D^-1 first.
+// down-sweep: t = r - A z with z = w D^-1 r stored by the restriction
+__device__ __forceinline__ double mg_smooth_val(const MgLevel &L, int64_t n) {
   const double dn = (double)L.dinv[n];
-  if (dn == 0.0) {
-    L.t[n] = 0.0;
-    return;
-  }
   const int I = (int)n / L.ny, J = (int)n - I * L.ny;
   auto z = [&](int64_t m) { return L.z[m]; };
-  L.t[n] = L.r[n] - mg_apply(L, I, J, z);
+  const double t = L.r[n] - mg_apply(L, I, J, z);
+  return dn == 0.0 ? 0.0 : t;
 }
 
-// up-sweep at node n: y = z + P e_c, e = y + w D^-1 (r - A y), into t
-__device__ __forceinline__ void mg_post_node(const MgLevel &L, const double *__restrict__ ec, int nyc, double w,
-                                             int64_t n) {
+// up-sweep: y = z + P e_c (0 on inactive nodes), e = y + w D^-1 (r - A y)
+__device__ __forceinline__ double mg_post_val(const MgLevel &L, const double *__restrict__ ec, int nyc, double w,
+                                              int64_t n) {
   const double dn = (double)L.dinv[n];
-  if (dn == 0.0) {
-    L.t[n] = 0.0;
-    return;
-  }
   const int I = (int)n / L.ny, J = (int)n - I * L.ny;
   auto y = [&](int64_t m) {
     int i, j;
     mg_nb_ij(n, I, J, m, L.ny, i, j);
-    return L.dinv[m] != 0.0f ? L.z[m] + mg_prolong(ec, nyc, i, j) : 0.0;
+    const double v = L.z[m] + mg_prolong(ec, nyc, i, j);
+    return L.dinv[m] != 0.0f ? v : 0.0;
   };
   const double yn = y(n);
-  L.t[n] = fma(w * dn, L.r[n] - mg_apply(L, I, J, y), yn);
+  const double e = fma(w * dn, L.r[n] - mg_apply(L, I, J, y), yn);
+  return dn == 0.0 ? 0.0 : e;
+}
+
+__device__ __forceinline__ void mg_smooth_node(const MgLevel &L, int64_t n) { L.t[n] = mg_smooth_val(L, n); }
+
+__device__ __forceinline__ void mg_post_node(const MgLevel &L, const double *__restrict__ ec, int nyc, double w,
+                                             int64_t n) {
+  L.t[n] = mg_post_val(L, ec, nyc, w, n);
 }
 
 // e of level l (the coarsest level's z, else its t)

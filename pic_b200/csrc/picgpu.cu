@@ -2294,7 +2294,14 @@ __global__ void __launch_bounds__(kWide, 1) k_fcg_persist(FcgP<V> F) {
         }
         if (!(ok = barrier())) break;
         if (smoothed) {
-          for (int64_t n = gtid; n < nl; n += gth) mg_smooth_node(L, n);
+          // two nodes a thread at a time: both nodes' loads ahead of the stores
+          for (int64_t n = gtid; n < nl; n += 2 * gth) {
+            const int64_t n2 = n + gth;
+            const double a = mg_smooth_val(L, n);
+            const double b = n2 < nl ? mg_smooth_val(L, n2) : 0.0;
+            L.t[n] = a;
+            if (n2 < nl) L.t[n2] = b;
+          }
           if (!(ok = barrier())) break;
         }
       }
@@ -2305,7 +2312,14 @@ __global__ void __launch_bounds__(kWide, 1) k_fcg_persist(FcgP<V> F) {
         const MgLevel &L = M.lv[l];
         const double *ec = mg_e(M, l + 1);
         const int nyc = M.lv[l + 1].ny;
-        for (int64_t n = gtid; n < (int64_t)L.nx * L.ny; n += gth) mg_post_node(L, ec, nyc, omega, n);
+        const int64_t nl = (int64_t)L.nx * L.ny;
+        for (int64_t n = gtid; n < nl; n += 2 * gth) {
+          const int64_t n2 = n + gth;
+          const double a = mg_post_val(L, ec, nyc, omega, n);
+          const double b = n2 < nl ? mg_post_val(L, ec, nyc, omega, n2) : 0.0;
+          L.t[n] = a;
+          if (n2 < nl) L.t[n2] = b;
+        }
       }
       if (!ok) break;
     } else if (F.coarse) {
