@@ -20,6 +20,7 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <map>
 #include <cmath>
 #include <cstdio>
 #include <cstring>
@@ -2476,6 +2477,12 @@ __global__ void k_add_f32(const int32_t *__restrict__ row_kind, const float *__r
 }
 
 __constant__ double c_ppr_reg[5][9];
+// Patch layouts shared by many nodes (kind 3 + t): the relative offsets of
+// the patch nodes in patch order and one pseudo-inverse for all of them.
+constexpr int kPprTpl = 4, kPprTplMax = 25;
+__constant__ int c_ppr_tpl_cnt[kPprTpl];
+__constant__ int c_ppr_tpl_off[kPprTpl][kPprTplMax];
+__constant__ double c_ppr_tpl_R[kPprTpl][5][kPprTplMax];
 
 struct PprK {
   const double *phi, *h;
@@ -2514,6 +2521,21 @@ __global__ void k_ppr(PprK k) {
     for (int r = 0; r < 5; ++r) {
       double acc = 0.0;
       for (int q = 0; q < cnt; ++q) acc = fma(R[(size_t)r * cnt + q], k.phi[k.nodes[b0 + q]], acc);
+      c[r] = acc;
+    }
+  } else if (kind >= 3) {
+    // a shared layout: the patch's potentials first (all loads in flight),
+    // then the rows, in patch order as for kind 1
+    const int t = kind - 3, cnt = c_ppr_tpl_cnt[t];
+    double ph[kPprTplMax];
+#pragma unroll
+    for (int q = 0; q < kPprTplMax; ++q) ph[q] = q < cnt ? k.phi[n + c_ppr_tpl_off[t][q]] : 0.0;
+#pragma unroll
+    for (int r = 0; r < 5; ++r) {
+      double acc = 0.0;
+#pragma unroll
+      for (int q = 0; q < kPprTplMax; ++q)
+        if (q < cnt) acc = fma(c_ppr_tpl_R[t][r][q], ph[q], acc);
       c[r] = acc;
     }
   }
@@ -3915,6 +3937,54 @@ int pic_init(const pic_mesh_desc *mesh, const pic_params *params) {
       for (int r = 0; r < 5; ++r)
         for (int q = 0; q < 9; ++q) g.h_ppr_reg[r][q] = R[r * 9 + q];
     }
+    // patch layouts (relative node offsets in patch order) shared by at
+    // least 1024 irregular nodes: one pseudo-inverse each, from the uniform
+    // spacing, used where a node's own offsets match it to 1e-12
+    std::map<std::vector<int32_t>, int64_t> layout_count;
+    auto layout_of = [&](int64_t n, int b0, int cnt) {
+      std::vector<int32_t> key(2 * cnt);
+      const int i0 = (int)(n / nny), j0 = (int)(n % nny);
+      for (int q = 0; q < cnt; ++q) {
+        const int32_t mm = mesh->patch_nodes[b0 + q] - 1;
+        key[2 * q] = mm / nny - i0;
+        key[2 * q + 1] = mm % nny - j0;
+      }
+      return key;
+    };
+    for (int64_t n = 0; n < nn; ++n) {
+      const int b0 = mesh->patch_ptr[n], cnt = mesh->patch_ptr[n + 1] - b0;
+      if (cnt >= 6 && cnt != 9 && cnt <= kPprTplMax) ++layout_count[layout_of(n, b0, cnt)];
+    }
+    std::vector<std::pair<int64_t, std::vector<int32_t>>> common;
+    for (auto &kv : layout_count)
+      if (kv.second >= 1024) common.push_back({kv.second, kv.first});
+    std::sort(common.begin(), common.end(), [](const auto &a, const auto &b) { return a.first > b.first; });
+    if ((int)common.size() > kPprTpl) common.resize(kPprTpl);
+    int tpl_cnt[kPprTpl] = {0}, tpl_off[kPprTpl][kPprTplMax] = {{0}};
+    double tpl_R[kPprTpl][5][kPprTplMax] = {{{0}}};
+    std::vector<std::vector<double>> tpl_px(common.size()), tpl_py(common.size());
+    int ntpl = 0;
+    for (auto &cl : common) {
+      const std::vector<int32_t> &key = cl.second;
+      const int cnt = (int)key.size() / 2;
+      double h = 0.0;
+      for (int q = 0; q < cnt; ++q) h = std::max(h, std::max(std::fabs(key[2 * q] * m.hx), std::fabs(key[2 * q + 1] * m.hy)));
+      std::vector<double> px(cnt), py(cnt), R(5 * cnt);
+      for (int q = 0; q < cnt; ++q) {
+        px[q] = key[2 * q] * m.hx / h;
+        py[q] = key[2 * q + 1] * m.hy / h;
+      }
+      if (!ppr_rows(px, py, R.data())) continue;
+      tpl_cnt[ntpl] = cnt;
+      for (int q = 0; q < cnt; ++q) {
+        tpl_off[ntpl][q] = key[2 * q] * nny + key[2 * q + 1];
+        for (int r = 0; r < 5; ++r) tpl_R[ntpl][r][q] = R[(size_t)r * cnt + q];
+      }
+      tpl_px[ntpl] = px;
+      tpl_py[ntpl] = py;
+      layout_count[key] = -1 - ntpl;  // marks the layout as template ntpl
+      ++ntpl;
+    }
     for (int64_t n = 0; n < nn; ++n) {
       ptr[n] = (int32_t)nodes.size();
       int b0 = mesh->patch_ptr[n], cnt = mesh->patch_ptr[n + 1] - b0;
@@ -3941,6 +4011,19 @@ int pic_init(const pic_mesh_desc *mesh, const pic_params *params) {
         px[q] = (xs[mm / nny] - xi) / h;
         py[q] = (ys[mm % nny] - yi) / h;
       }
+      if (ntpl > 0 && cnt <= kPprTplMax && cnt != 9) {
+        auto it = layout_count.find(layout_of(n, b0, cnt));
+        if (it != layout_count.end() && it->second < 0) {
+          const int t = (int)(-1 - it->second);
+          bool same = true;
+          for (int q = 0; q < cnt && same; ++q)
+            same = std::fabs(px[q] - tpl_px[t][q]) <= 1e-12 && std::fabs(py[q] - tpl_py[t][q]) <= 1e-12;
+          if (same) {
+            kind[n] = 3 + t;
+            continue;
+          }
+        }
+      }
       std::vector<double> R(5 * cnt);
       if (!ppr_rows(px, py, R.data())) continue;  // singular patch: no recovery at this node
       kind[n] = 1;
@@ -3951,6 +4034,9 @@ int pic_init(const pic_mesh_desc *mesh, const pic_params *params) {
     ptr[nn] = (int32_t)nodes.size();
     // kind 1 rows are stored at 5*ptr[n]; ptr for kinds 0/2 is unused
     PIC_CUDA(cudaMemcpyToSymbol(c_ppr_reg, g.h_ppr_reg, sizeof g.h_ppr_reg));
+    PIC_CUDA(cudaMemcpyToSymbol(c_ppr_tpl_cnt, tpl_cnt, sizeof tpl_cnt));
+    PIC_CUDA(cudaMemcpyToSymbol(c_ppr_tpl_off, tpl_off, sizeof tpl_off));
+    PIC_CUDA(cudaMemcpyToSymbol(c_ppr_tpl_R, tpl_R, sizeof tpl_R));
     if ((rc = upload(&g.d_ppr_kind, kind.data(), kind.size()))) return rc;
     // make ptr monotone for kind-1 lookups: ptr[n+1] must be the end of node n's patch
     std::vector<int32_t> ptr2(nn + 1, 0);
