@@ -177,6 +177,7 @@ struct Ctx {
   bool push_bulk = false;                   // mixed-precision tiles bulk-copied (PIC_PUSH_BULK=1)
   int push_bulk_default = 1;
   long long push_wait_limit = 1ll << 22;    // polls of a tile's mbarrier before the push gives up
+  int push_skip_copies = 0;                 // test hook: the bulk pushes issue no tile copies
   // CUDA graphs of one FCG iteration: [0] stage A, [1 + slot] stage B + FCG
   // kernels of ring slot `slot`; rebuilt when the configuration key changes
   cudaGraphExec_t fcg_graph[2 + PIC_FCG_MAX_WINDOW] = {};

@@ -929,7 +929,7 @@ __device__ __forceinline__ void push_tile64_bulk(PushTile64 *T, uint64_t *b, con
 
 template <int S, bool AXI>
 __global__ void __launch_bounds__(256, 4) k_push_bulk(MeshK m, FieldK f, PushK prm, SpK s, int64_t ntiles,
-                                                      long long limit) {
+                                                      long long limit, int skip_copies) {
   extern __shared__ __align__(16) unsigned char push_smem[];
   PushTile64 *T = reinterpret_cast<PushTile64 *>(push_smem);
   uint64_t *bar = reinterpret_cast<uint64_t *>(push_smem + S * sizeof(PushTile64));
@@ -946,7 +946,7 @@ __global__ void __launch_bounds__(256, 4) k_push_bulk(MeshK m, FieldK f, PushK p
 #pragma unroll
     for (int k = 0; k < S - 1; ++k) {
       const int64_t t = blockIdx.x + k * G;
-      if (t < ntiles) push_tile64_bulk(&T[k], &bar[k], s, t * kPushTile);
+      if (t < ntiles && !skip_copies) push_tile64_bulk(&T[k], &bar[k], s, t * kPushTile);
     }
   }
   __syncthreads();
@@ -958,7 +958,8 @@ __global__ void __launch_bounds__(256, 4) k_push_bulk(MeshK m, FieldK f, PushK p
       // the stage refilled here was read in the previous tile, before its
       // closing barrier; order those reads before the copy's writes
       asm volatile("fence.proxy.async.shared::cta;\n" ::: "memory");
-      if (tn < ntiles) push_tile64_bulk(&T[(it + S - 1) % S], &bar[(it + S - 1) % S], s, tn * kPushTile);
+      if (tn < ntiles && !skip_copies)
+        push_tile64_bulk(&T[(it + S - 1) % S], &bar[(it + S - 1) % S], s, tn * kPushTile);
     }
     const int st = it % S;
     bool ready = false;
@@ -1001,7 +1002,8 @@ __device__ __forceinline__ void push_tile_bulk(PushTile *T, uint64_t *b, const S
 
 template <int S, int MINB, bool AXI>
 __global__ void __launch_bounds__(256, MINB) k_push_mixed_bulk(MeshK m, const float *__restrict__ c32, PushM prm,
-                                                             SpK s, int64_t ntiles, long long limit) {
+                                                             SpK s, int64_t ntiles, long long limit,
+                                                             int skip_copies) {
   extern __shared__ __align__(16) unsigned char push_smem[];
   PushTile *T = reinterpret_cast<PushTile *>(push_smem);
   uint64_t *bar = reinterpret_cast<uint64_t *>(push_smem + S * sizeof(PushTile));
@@ -1018,7 +1020,7 @@ __global__ void __launch_bounds__(256, MINB) k_push_mixed_bulk(MeshK m, const fl
 #pragma unroll
     for (int k = 0; k < S - 1; ++k) {
       const int64_t t = blockIdx.x + k * G;
-      if (t < ntiles) push_tile_bulk(&T[k], &bar[k], s, t * kPushTile);
+      if (t < ntiles && !skip_copies) push_tile_bulk(&T[k], &bar[k], s, t * kPushTile);
     }
   }
   __syncthreads();
@@ -1028,7 +1030,8 @@ __global__ void __launch_bounds__(256, MINB) k_push_mixed_bulk(MeshK m, const fl
     if (threadIdx.x == 0) {
       const int64_t tn = t + (S - 1) * G;
       asm volatile("fence.proxy.async.shared::cta;\n" ::: "memory");
-      if (tn < ntiles) push_tile_bulk(&T[(it + S - 1) % S], &bar[(it + S - 1) % S], s, tn * kPushTile);
+      if (tn < ntiles && !skip_copies)
+        push_tile_bulk(&T[(it + S - 1) % S], &bar[(it + S - 1) % S], s, tn * kPushTile);
     }
     const int st = it % S;
     bool ready = false;
@@ -2760,10 +2763,10 @@ static int run_push(int sidx, bool do_push, bool do_deposit, bool do_energy) {
       const size_t smem = 4 * sizeof(PushTile) + 4 * sizeof(uint64_t);
       if (g.axi)
         k_push_mixed_bulk<4, 5, true><<<grid, kPushTile, smem, g.st>>>(m, g.d_coef32, pm, k, ntiles,
-                                                                       g.push_wait_limit);
+                                                                       g.push_wait_limit, g.push_skip_copies);
       else
         k_push_mixed_bulk<4, 5, false><<<grid, kPushTile, smem, g.st>>>(m, g.d_coef32, pm, k, ntiles,
-                                                                        g.push_wait_limit);
+                                                                        g.push_wait_limit, g.push_skip_copies);
     } else if (g.axi) {
       // r-z: the default tiled form (4 stages, 5 CTAs per SM) or the direct one
       if (g.push_stages) {
@@ -2795,9 +2798,11 @@ static int run_push(int sidx, bool do_push, bool do_deposit, bool do_energy) {
     const unsigned grid = (unsigned)std::min<int64_t>(ntiles, g.push64_grid);
     const size_t smem = 3 * sizeof(PushTile64) + 3 * sizeof(uint64_t);
     if (g.axi)
-      k_push_bulk<3, true><<<grid, kPushTile, smem, g.st>>>(mesh_k(), f, prm, k, ntiles, g.push_wait_limit);
+      k_push_bulk<3, true><<<grid, kPushTile, smem, g.st>>>(mesh_k(), f, prm, k, ntiles, g.push_wait_limit,
+                                                             g.push_skip_copies);
     else
-      k_push_bulk<3, false><<<grid, kPushTile, smem, g.st>>>(mesh_k(), f, prm, k, ntiles, g.push_wait_limit);
+      k_push_bulk<3, false><<<grid, kPushTile, smem, g.st>>>(mesh_k(), f, prm, k, ntiles, g.push_wait_limit,
+                                                              g.push_skip_copies);
   } else if (g.push64_grid > 0) {
     const int64_t ntiles = (s.n_slots + kPushTile - 1) / kPushTile;
     const unsigned grid = (unsigned)std::min<int64_t>(ntiles, g.push64_grid);
@@ -4184,6 +4189,13 @@ int pic_init(const pic_mesh_desc *mesh, const pic_params *params) {
     // through shared memory when PIC_PUSH64_TILED is 1; otherwise one
     // particle per thread loaded directly (same bits either way)
     // (2: the tiles are bulk-copied by one thread and complete on mbarriers)
+    // test hooks of the bulk-staged pushes' bounded wait: polls of a tile's
+    // mbarrier before giving up, and no copies issued at all (every wait then
+    // runs out and the step reports the failure)
+    const char *wl = getenv("PIC_PUSH_WAIT_LIMIT");
+    if (wl && atoll(wl) > 0) g.push_wait_limit = atoll(wl);
+    const char *sc = getenv("PIC_PUSH_SKIP_COPIES");
+    g.push_skip_copies = sc && atoi(sc) == 1 ? 1 : 0;
     const char *p64 = getenv("PIC_PUSH64_TILED");
     const int mode64 = p64 ? atoi(p64) : g.push64_default;
     g.push64_grid = 0;
