@@ -221,6 +221,9 @@ struct Ctx {
                                        //   count below b*, selection held
   int64_t *d_ion_parent = nullptr;     // ionising parents: (id<<32 | slot), mcc_cap per species
   double *d_ion_data = nullptr;        // per ionisation: new e- v(3), ion v(3)
+  void *h_fcg = nullptr;               // pinned FcgState of the fused persistent FCG
+  size_t fcg_smem_set = 0;             // dynamic shared memory the FCG kernel was opened to
+  int fcg_fused = 1;                   // PIC_FCG_FUSED=0: set-up and judge by separate kernels
   void *h_ion = nullptr;               // pinned staging: ionisations read back
   int64_t h_ion_cap = 0;
   void *h_new = nullptr;               // pinned staging: created particles' slots and velocities

@@ -1831,6 +1831,51 @@ __global__ void __launch_bounds__(PIC_RED_THREADS) k_dot(DotK k) {
 }
 
 // r = b - q on unknown nodes, 0 on Dirichlet nodes
+// The persistent FCG's set-up and judge in one launch each: r = b - A x (0
+// on Dirichlet rows) over k_dot's item layout, with r.r (and b.b) summed in
+// k_dot's order, so the numbers are those of k_pcg_x0 + k_spmv + k_fcg_r0 +
+// k_dot.  init: x is the Dirichlet-filled phi, formed at every neighbour as
+// k_pcg_x0 writes it, and the last block stores rhs = b.b, rr = best = r.r
+// in the FCG state; otherwise x is read and rr = r.r is stored.
+__global__ void __launch_bounds__(PIC_RED_THREADS) k_fcg_resid(PcgK k, unsigned int *__restrict__ ticket,
+                                                               FcgState *__restrict__ S, int init) {
+  double v0 = 0.0, v1 = 0.0;
+  auto x0 = [&](int64_t m) { return k.node_type[m] > 0 ? k.phi[m] : 0.0; };
+  for (int it = 0; it < PIC_RED_ITEMS; ++it) {
+    const int64_t n = (int64_t)blockIdx.x * PIC_RED_CHUNK + it * PIC_RED_THREADS + threadIdx.x;
+    if (n >= k.nn) continue;
+    double q;
+    if (init) {
+      k.x[n] = x0(n);
+      q = row_apply(k, n, x0);
+    } else {
+      q = row_apply(k, n, [&](int64_t m) { return k.x[m]; });
+    }
+    const double r = k.row_kind[n] < 0 ? 0.0 : k.b[n] - q;
+    k.r[n] = r;
+    v0 = fma(k.b[n], k.b[n], v0);
+    v1 = fma(r, r, v1);
+  }
+  double v[2] = {v0, v1}, out[2];
+  block_sum_canon<2>(v, out);
+  if (threadIdx.x == 0) {
+    k.part[blockIdx.x] = out[0];
+    k.part[k.nb + blockIdx.x] = out[1];
+  }
+  if (arrive_last(ticket)) {
+    double tot[2];
+    final_sum_canon<2>(k.part, k.nb, tot);
+    if (threadIdx.x == 0) {
+      if (init) {
+        S->rhs = tot[0];
+        S->best = tot[1];
+      }
+      S->rr = tot[1];
+      *ticket = 0;
+    }
+  }
+}
+
 __global__ void k_fcg_r0(const int32_t *__restrict__ row_kind, const double *__restrict__ b,
                          const double *__restrict__ q, double *__restrict__ r, int64_t nn) {
   int64_t n = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
@@ -2231,6 +2276,15 @@ __global__ void __launch_bounds__(kWide, 1) k_fcg_persist(FcgP<V> F) {
   const int gwarp = blockIdx.x * (kWide / 32) + warp, nwarps = gridDim.x * (kWide / 32);
   const int nc = F.ncx * F.ncy;
   auto barrier = [&]() { return grid_barrier(F.bar, F.bar_err, F.spin_limit, F.bar_extra); };
+  // already converged (the state came from k_fcg_resid): nothing to do
+  // (every CTA reads the same state)
+  if (!(rhs > 0.0) || rr / rhs <= tol2) {
+    if (blockIdx.x == 0 && threadIdx.x == 0) {
+      S->ierr = 0;
+      S->done = 1;
+    }
+    return;
+  }
   for (;;) {
     // the previous direction (written last iteration), the new one
     const V *Pl = parity ? F.P0 : F.P1, *Ql = parity ? F.Q0 : F.Q1;
@@ -2689,6 +2743,7 @@ static void free_all() {
   F(g.d_scan_blk); F(g.d_counters); F(g.d_hist); F(g.d_sel); F(g.d_cand); F(g.d_cand_slot);
   F(g.d_mcc_misc); F(g.d_mlist_key); F(g.d_mlist_slot); F(g.d_msel); F(g.d_ion_parent); F(g.d_ion_data); F(g.d_mcc_pslot); F(g.d_mcc_vel);
   if (g.h_ion) cudaFreeHost(g.h_ion);
+  if (g.h_fcg) cudaFreeHost(g.h_fcg);
   if (g.h_new) cudaFreeHost(g.h_new);
   for (int s = 0; s < PIC_MAX_SPECIES; ++s) {
     Species &p = g.sp[s];
@@ -3166,12 +3221,114 @@ static int fcg_alloc() {
 // dots); if the recursive residual drifted, the iteration restarts from the
 // true one with no previous directions.  Returns 0 when converged, else the
 // reason it hands over to Jacobi-PCG (the fallback codes of pic_solve_stats).
+// The FP64 FCG as one cooperative kernel between two k_fcg_resid launches:
+// the initial residual and its norms, the iterations, the true residual of
+// the result.  The host writes the state's fixed fields from pinned memory
+// and reads the state back once, after the judge (one wait per solve,
+// three kernels).  Returns as run_fcg: 0 converged, else the fallback code.
+static int run_fcg_persist64(pic_solve_stats *stats, int *fcg_iters, int *rc_out) {
+  const int64_t nn = g.nn;
+  int rc;
+  if (!g.h_fcg) PIC_CUDA(cudaMallocHost(&g.h_fcg, sizeof(FcgState)));
+  FcgState &hs = *static_cast<FcgState *>(g.h_fcg);
+  std::memset(&hs, 0, sizeof hs);
+  hs.tol2 = g.P.pcg_tol * g.P.pcg_tol;
+  hs.maxit = std::min(g.P.pcg_maxit, 1000);
+  hs.stall_window = 50;
+  PcgK k0 = pcg_k(0);
+  PIC_CUDA(cudaMemcpyAsync(g.d_fcg, &hs, sizeof hs, cudaMemcpyHostToDevice, g.st));
+  k_fcg_resid<<<g.red_blocks, PIC_RED_THREADS, 0, g.st>>>(k0, g.d_dot_ticket, g.d_fcg, 1);
+  PIC_LAUNCHED();
+  FcgP<double> F;
+  F.k = k0;
+  F.part = g.d_fcg_part;
+  F.ainv = g.d_pc_ainv;
+  F.ainv_scale = g.pc_ainv_scale;
+  F.ainv_ld = g.pc_ainv_ld;
+  F.rc = g.d_pc_rc;
+  F.ec = g.d_pc_ec;
+  F.nnx = g.m.nnx;
+  F.cs = g.pc_cs;
+  F.ncx = g.pc_ncx;
+  F.ncy = g.pc_ncy;
+  F.coarse = g.pc_cs > 0 ? 1 : 0;
+  F.mg = g.mg;
+  if (g.mg.L > 1) {  // the coarsest level's r and z feed the dense solve
+    const MgLevel &C = g.mg.lv[g.mg.L - 1];
+    F.rc = C.r;
+    F.ec = C.z;
+    F.ncx = C.nx;
+    F.ncy = C.ny;
+  }
+  F.omega = g.pc_omega;
+  F.s = g.d_fcg;
+  F.bar = g.d_bar;
+  F.bar_err = (int *)(g.d_bar + 2);
+  F.spin_limit = g.pcg_spin_limit;
+  F.bar_extra = g.pcg_bar_extra;
+  F.x = g.d_x;
+  F.r = g.d_r;
+  F.r2 = g.d_w;  // free while FCG runs
+  F.dinv = g.d_pc_dinv;
+  F.zA = g.d_pc_za;
+  F.t = g.d_pc_t;
+  F.zF = g.d_z;
+  F.P0 = g.d_fcg_P;
+  F.P1 = g.d_fcg_P + nn;
+  F.Q0 = g.d_fcg_Q;
+  F.Q1 = g.d_fcg_Q + nn;
+  const void *fn = (const void *)k_fcg_persist<double>;
+  const size_t smem = (size_t)g.pc_ainv_ld * sizeof(double);  // coarse_gemv's staging
+  if (!g.fcg_smem_set || g.fcg_smem_set != smem) {
+    PIC_CUDA(cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    g.fcg_smem_set = smem;
+  }
+  auto finish = [&](int fallback) {
+    *fcg_iters = hs.iter;
+    if (stats) {
+      stats->iterations = hs.iter;
+      stats->rel_residual = hs.rhs > 0 ? std::sqrt(hs.rr / hs.rhs) : 0.0;
+      stats->ierr = 0;
+    }
+    if (!fallback) g.fcg_last_iters = std::max(hs.iter, 1);
+    return fallback;
+  };
+  for (int judged = 0;; ++judged) {
+    PIC_CUDA(cudaMemsetAsync(g.d_bar, 0, 4 * sizeof(unsigned int), g.st));
+    void *args[] = {&F};
+    PIC_CUDA(cudaLaunchCooperativeKernel(fn, dim3(g.fcg_coop_grid), dim3(kWide), args, smem, g.st));
+    PIC_LAUNCHED();
+    // the judge: the true residual of the result (r is the next start)
+    k_fcg_resid<<<g.red_blocks, PIC_RED_THREADS, 0, g.st>>>(k0, g.d_dot_ticket, g.d_fcg, 0);
+    PIC_LAUNCHED();
+    PIC_CUDA(cudaMemcpyAsync(&hs, g.d_fcg, sizeof hs, cudaMemcpyDeviceToHost, g.st));
+    PIC_CUDA(cudaStreamSynchronize(g.st));
+    if (hs.ierr == 7) {
+      set_error("pic_ife_solve: FCG grid barrier timed out");
+      *rc_out = PIC_ERR_CUDA;
+      return 1;
+    }
+    if (hs.ierr) return finish(hs.ierr);
+    if (!(hs.rhs > 0.0) || hs.rr / hs.rhs <= hs.tol2) return finish(0);
+    if (judged >= 3 || hs.iter >= hs.maxit) return finish(6);
+    hs.done = 0;
+    hs.count = 0;
+    PIC_CUDA(cudaMemcpyAsync(g.d_fcg, &hs, sizeof hs, cudaMemcpyHostToDevice, g.st));
+  }
+  (void)rc;
+}
+
 static int run_fcg(pic_solve_stats *stats, int *fcg_iters, int *rc_out) {
   *rc_out = PIC_OK;
   const int64_t nn = g.nn;
   const int nb = blocks_for(nn, 256);
   int rc;
   if ((rc = fcg_alloc())) { *rc_out = rc; return 1; }
+  if (g.fcg_coop_grid > 0 && g.fcg_window == 1 && g.pc_sweeps > 0 && !(g.mixed && g.fcg_inner32) &&
+      g.fcg_fused) {
+    if ((rc = precond_prepare())) { *rc_out = rc; return 1; }
+    if (!precond_learned_on()) return run_fcg_persist64(stats, fcg_iters, rc_out);
+  }
   PcgK k0 = pcg_k(0);
   k0.w = g.d_z;
   FcgK fk{k0, g.d_fcg_P, g.d_fcg_Q, g.d_fcg_part, g.d_fcg, 0, g.fcg_window + 1, g.fcg_window};
@@ -4139,6 +4296,8 @@ int pic_init(const pic_mesh_desc *mesh, const pic_params *params) {
     g.pcg_bar_extra = extra ? (unsigned int)std::max(0, atoi(extra)) : 0u;
   }
   {
+    const char *ff = getenv("PIC_FCG_FUSED");  // 0: the persistent FCG's set-up and judge by separate kernels
+    g.fcg_fused = (ff && atoi(ff) == 0) ? 0 : 1;
     const char *fg = getenv("PIC_FCG_GRAPHS");  // 0: enqueue FCG iterations kernel by kernel
     g.fcg_graphs = (fg && atoi(fg) == 0) ? 0 : 1;
     const char *fi = getenv("PIC_FCG_INNER");  // "fp32": FP32 inner iterations in mixed precision

@@ -114,9 +114,10 @@ def test_vcycle_matches_scipy():
         sim.close()
 
 
-def _solve(sim, multigrid, omega=2.0 / 3.0):
-    sim.set_field("phi", np.zeros(sim.mesh.nn))
-    sim.set_solver("fcg", multigrid=multigrid, omega=omega)
+def _solve(sim, multigrid, omega=2.0 / 3.0, keep_phi=False):
+    if not keep_phi:
+        sim.set_field("phi", np.zeros(sim.mesh.nn))
+        sim.set_solver("fcg", multigrid=multigrid, omega=omega)
     st = api.SolveStats()
     api.check(sim.lib.pic_ife_solve(None, 0.0, C.byref(st)), "pic_ife_solve")
     return st, sim.field("phi")
@@ -159,6 +160,34 @@ def test_multigrid_persistent_matches_launch_path():
     print(f"\nmultigrid FCG iterations: launch path {out[0][0]}, persistent {out[1][0]}")
     assert abs(out[0][0] - out[1][0]) <= 2
     assert np.abs(out[0][1] - out[1][1]).max() <= 1e-7 * np.abs(out[0][1]).max()
+
+
+@pytest.mark.parametrize("warm", [False, True])
+def test_fused_setup_and_judge_match_separate_kernels(warm):
+    """The persistent FCG's set-up and judge as one launch each (residual
+    and norms in k_dot's order) give the same iterations and the same bits
+    as the separate x0 / SpMV / residual / dot kernels (PIC_FCG_FUSED=0),
+    from phi = 0 and from a warm start."""
+    out = []
+    for flag in ("0", "1"):
+        os.environ["PIC_FCG_FUSED"] = flag
+        try:
+            sim = _sim(256)
+        finally:
+            del os.environ["PIC_FCG_FUSED"]
+        try:
+            sim.set_field("rho", np.random.default_rng(2).standard_normal(sim.mesh.nn))
+            st, phi = _solve(sim, True)
+            if warm:  # a second solve from the first one's potential, a slightly changed charge
+                sim.set_field("rho", np.random.default_rng(3).standard_normal(sim.mesh.nn) * 1e-3
+                              + np.random.default_rng(2).standard_normal(sim.mesh.nn))
+                st, phi = _solve(sim, True, keep_phi=True)
+            assert st.fallback == 0 and st.rel_residual <= 1e-8
+            out.append((st.iterations, st.rel_residual, phi))
+        finally:
+            sim.close()
+    assert out[0][0] == out[1][0] and out[0][1] == out[1][1]
+    assert np.array_equal(out[0][2], out[1][2])
 
 
 def test_multigrid_rejects_grids_that_do_not_halve():
