@@ -103,6 +103,7 @@ struct Ctx {
   pic_params P;
   double L_ref = 0, t_ref = 0, v_ref = 0, phi_ref = 0;
   cudaStream_t st = nullptr;
+  cudaStream_t st2 = nullptr;  // the step's field recovery, alongside its MCC
   cudaEvent_t ev0 = nullptr, ev1 = nullptr;
   // mesh
   double *d_xs = nullptr, *d_ys = nullptr;
@@ -174,6 +175,7 @@ struct Ctx {
   int push64_grid = 0;                      // tiled FP64 push: persistent CTAs (0: direct kernel)
   int push64_default = 2;                   // bulk-tiled FP64 push unless PIC_PUSH64_TILED=0 or 1
   bool push64_bulk = false;                 // tiles bulk-copied (PIC_PUSH64_TILED=2)
+  int push64_minb = 4;                      // resident CTAs per SM the Cartesian bulk push is built for
   bool push_bulk = false;                   // mixed-precision tiles bulk-copied (PIC_PUSH_BULK=1)
   int push_bulk_default = 1;
   long long push_wait_limit = 1ll << 22;    // polls of a tile's mbarrier before the push gives up

@@ -927,8 +927,8 @@ __device__ __forceinline__ void push_tile64_bulk(PushTile64 *T, uint64_t *b, con
   bulk_g2s(T->loc, s.loc + base, 4 * kPushTile, b);
 }
 
-template <int S, bool AXI>
-__global__ void __launch_bounds__(256, 4) k_push_bulk(MeshK m, FieldK f, PushK prm, SpK s, int64_t ntiles,
+template <int S, bool AXI, int MINB = 4>
+__global__ void __launch_bounds__(256, MINB) k_push_bulk(MeshK m, FieldK f, PushK prm, SpK s, int64_t ntiles,
                                                       long long limit, int skip_copies) {
   extern __shared__ __align__(16) unsigned char push_smem[];
   PushTile64 *T = reinterpret_cast<PushTile64 *>(push_smem);
@@ -2753,6 +2753,7 @@ static void free_all() {
   }
   if (g.ev0) cudaEventDestroy(g.ev0);
   if (g.ev1) cudaEventDestroy(g.ev1);
+  if (g.st2) cudaStreamDestroy(g.st2);
   if (g.st) cudaStreamDestroy(g.st);
   g = Ctx();
 }
@@ -2856,8 +2857,12 @@ static int run_push(int sidx, bool do_push, bool do_deposit, bool do_energy) {
       k_push_bulk<3, true><<<grid, kPushTile, smem, g.st>>>(mesh_k(), f, prm, k, ntiles, g.push_wait_limit,
                                                              g.push_skip_copies);
     else
-      k_push_bulk<3, false><<<grid, kPushTile, smem, g.st>>>(mesh_k(), f, prm, k, ntiles, g.push_wait_limit,
-                                                              g.push_skip_copies);
+      if (g.push64_minb == 5)
+        k_push_bulk<3, false, 5><<<grid, kPushTile, smem, g.st>>>(mesh_k(), f, prm, k, ntiles, g.push_wait_limit,
+                                                                   g.push_skip_copies);
+      else
+        k_push_bulk<3, false><<<grid, kPushTile, smem, g.st>>>(mesh_k(), f, prm, k, ntiles, g.push_wait_limit,
+                                                                g.push_skip_copies);
   } else if (g.push64_grid > 0) {
     const int64_t ntiles = (s.n_slots + kPushTile - 1) / kPushTile;
     const unsigned grid = (unsigned)std::min<int64_t>(ntiles, g.push64_grid);
@@ -3612,7 +3617,7 @@ static int run_solve(pic_solve_stats *stats) {
   return run_pcg(stats);
 }
 
-static int run_ppr() {
+static int run_ppr(cudaStream_t stream = nullptr) {
   PprK k;
   k.phi = g.d_phi;
   k.h = g.d_ppr_h;
@@ -3626,7 +3631,7 @@ static int run_ppr() {
   k.coef32 = g.d_coef32;
   k.nny = g.m.nny;
   k.nn = g.nn;
-  k_ppr<<<blocks_for(g.nn, 256), 256, 0, g.st>>>(k);
+  k_ppr<<<blocks_for(g.nn, 256), 256, 0, stream ? stream : g.st>>>(k);
   PIC_LAUNCHED();
   return PIC_OK;
 }
@@ -3864,6 +3869,7 @@ int pic_init(const pic_mesh_desc *mesh, const pic_params *params) {
 
   int rc;
   PIC_CUDA(cudaStreamCreateWithFlags(&g.st, cudaStreamNonBlocking));
+  PIC_CUDA(cudaStreamCreateWithFlags(&g.st2, cudaStreamNonBlocking));
   PIC_CUDA(cudaEventCreate(&g.ev0));
   PIC_CUDA(cudaEventCreate(&g.ev1));
   std::vector<double> xs(m.nnx), ys(m.nny);
@@ -4360,7 +4366,11 @@ int pic_init(const pic_mesh_desc *mesh, const pic_params *params) {
     g.push64_grid = 0;
     g.push64_bulk = mode64 == 2;
     if (mode64 == 1 || mode64 == 2) {
-      const void *fn = g.push64_bulk ? (g.axi ? (const void *)k_push_bulk<3, true> : (const void *)k_push_bulk<3, false>)
+      const char *m64 = getenv("PIC_PUSH64_MINB");  // 5: the Cartesian bulk push built for 5 CTAs per SM
+      g.push64_minb = (m64 && atoi(m64) == 5 && !g.axi) ? 5 : 4;
+      const void *fn = g.push64_bulk ? (g.axi ? (const void *)k_push_bulk<3, true>
+                                              : g.push64_minb == 5 ? (const void *)k_push_bulk<3, false, 5>
+                                                                   : (const void *)k_push_bulk<3, false>)
                                      : (g.axi ? (const void *)k_push_tiled<3, true> : (const void *)k_push_tiled<3, false>);
       const size_t smem = 3 * sizeof(PushTile64) + (g.push64_bulk ? 3 * sizeof(uint64_t) : 0);
       int per_sm = 0;
@@ -4724,7 +4734,7 @@ int pic_sort_particles(int32_t species) {
 int pic_step(uint64_t step, pic_step_stats *stats) {
   int rc;
   if ((rc = check_init())) return rc;
-  cudaEvent_t e[8];
+  cudaEvent_t e[10];
   for (auto &ev : e) PIC_CUDA(cudaEventCreate(&ev));
   PIC_CUDA(cudaEventRecord(e[0], g.st));
   // 1. fused push + locate + deposit (MoveAll, then GetParChg_2D).  The
@@ -4761,9 +4771,13 @@ int pic_step(uint64_t step, pic_step_stats *stats) {
   if ((rc = run_rhs())) return rc;
   int solve_rc = run_solve(&ss);
   PIC_CUDA(cudaEventRecord(e[2], g.st));
-  // 3. PPR field recovery
-  if ((rc = run_ppr())) return rc;
+  // 3. PPR field recovery, on the second stream alongside the MCC: the PPR
+  // reads phi and writes the fields, the MCC reads and writes particles only
   PIC_CUDA(cudaEventRecord(e[3], g.st));
+  PIC_CUDA(cudaStreamWaitEvent(g.st2, e[3], 0));
+  PIC_CUDA(cudaEventRecord(e[8], g.st2));
+  if ((rc = run_ppr(g.st2))) return rc;
+  PIC_CUDA(cudaEventRecord(e[9], g.st2));
   for (int s = 0; s < g.ns; ++s)
     if ((rc = count_live(s))) return rc;
   // 4. MCC
@@ -4771,6 +4785,7 @@ int pic_step(uint64_t step, pic_step_stats *stats) {
   std::memset(&ms, 0, sizeof ms);
   if (g.mcc_ready)
     if ((rc = mcc_run(step, &ms, true))) return rc;
+  PIC_CUDA(cudaStreamWaitEvent(g.st, e[9], 0));  // the fields are ready for the next push
   PIC_CUDA(cudaEventRecord(e[4], g.st));
   // 5. counting sort
   if ((int64_t)(step % (uint64_t)g.P.sort_interval) == 0)
@@ -4793,7 +4808,7 @@ int pic_step(uint64_t step, pic_step_stats *stats) {
     float t;
     cudaEventElapsedTime(&t, e[0], e[1]); stats->ms_push = t;
     cudaEventElapsedTime(&t, e[1], e[2]); stats->ms_solve = t; stats->solve.ms = t;
-    cudaEventElapsedTime(&t, e[2], e[3]); stats->ms_ppr = t;
+    cudaEventElapsedTime(&t, e[8], e[9]); stats->ms_ppr = t;  // overlaps the MCC phase
     cudaEventElapsedTime(&t, e[3], e[4]); stats->ms_mcc = t;
     cudaEventElapsedTime(&t, e[4], e[5]); stats->ms_sort = t;
     cudaEventElapsedTime(&t, e[0], e[5]); stats->ms_total = t;
