@@ -43,6 +43,12 @@ ROOT = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, ROOT)
 
 METRIC = "particle pushes/s + Poisson ms/step: learned-precond FCG vs plain PCG at 1e-8"
+# The roofline's per-particle unit is the scope table's algorithmic figure for
+# push + gather + deposit: FP64 88 B (x, y, vx, vy, vz and the cell, read and
+# written), mixed precision 48 B.  The kernels move less (vz stays untouched
+# on steps without the energy diagnostic); their own bytes are reported
+# beside it.
+UNIT_PUSH_BYTES = {"fp64": 88, "mixed": 48}
 FP64_PUSH_BYTES = 72   # read x,y,vx,vy,elem (36 B; vz only on diagnostic steps), write the same (36 B)
 MIXED_PUSH_BYTES = 40  # read elem + 4 FP32 (20 B), write the same (20 B)
 # + the particle id (4 B) when the push builds the step's MCC selection
@@ -337,12 +343,16 @@ def _push_roofline(precision: str, rz: bool, stats, peak, peak_src, select: bool
         nbytes = FP64_PUSH_BYTES_RZ if rz else FP64_PUSH_BYTES
         kernel = "k_push_bulk"
     nbytes += SELECT_BYTES if select else 0
-    achieved = nbytes * push_n / (push_ms / 1e3) / 1e9
+    unit = UNIT_PUSH_BYTES[precision]
+    achieved = unit * push_n / (push_ms / 1e3) / 1e9
+    own = nbytes * push_n / (push_ms / 1e3) / 1e9
     key = precision + ("_rz" if rz else "") + ("_sel" if select else "")
     tr = NCU_PUSH_TRAFFIC[key] * push_n if key in NCU_PUSH_TRAFFIC else None
     return {"kernel": kernel + (" r-z" if rz else "") + " (fused push+locate+deposit)", "bound": "hbm",
             "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
-            "peak_source": peak_src, "bytes_per_particle": nbytes, "traffic": tr,
+            "peak_source": peak_src, "bytes_per_particle": unit,
+            "kernel_bytes_per_particle": nbytes, "kernel_bytes_achieved": own, "kernel_bytes_frac": own / peak,
+            "traffic": tr,
             "traffic_note": ("no ncu capture of this push" if tr is None else
                              "ncu DRAM bytes/particle of one launch at 8 particles per cell (6.4M particles; "
                              "r-z 16.7M) x particles per step")}, push_ms
