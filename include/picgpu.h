@@ -321,6 +321,22 @@ int pic_get_field(int32_t which, double *host_out);
 /* Field upload (host, [nodes]): which 1 phi, 2 efx, 3 efy, 12..16 coef_ppr. */
 int pic_set_field(int32_t which, const double *host_in);
 
+/* Asynchronous readback of the fields a step leaves (host, [nodes] each;
+ * any pointer may be NULL): phi, rho, efx, efy are copied in that order on
+ * a copy stream of their own and the call returns at once, so the copies
+ * run while the caller's next pic_step pushes the particles.  Every later
+ * call that writes one of these fields on the device first waits for its
+ * copy (pic_set_field of phi for the phi copy only).  The host arrays must
+ * stay valid, and are complete only after pic_wait_fields; they should be
+ * page-locked (cudaHostAlloc), or the copies cannot overlap anything.
+ * Replaces the synchronous per-field reads the reference's caller does
+ * after `IFE_Solve_2D` / `GetEField_SIDG_PPR` (Main_IFE_Test_2.f90:329-341)
+ * when it does not need the values before its next step. */
+int pic_get_fields_async(double *rho_out, double *phi_out, double *efx_out, double *efy_out);
+/* Waits for the copies of pic_get_fields_async; the library's stream is
+ * ordered after them too (a pic_device_timer stop covers them). */
+int pic_wait_fields(void);
+
 /* Device pointers of the particle SoA, for zero-copy callers on the same
  * device.  Order: x, y, vx, vy, vz (double*: absolute normalised position and
  * velocity), loc (int32*), id (uint32*).  Only the PIC_PREC_FP64 layout is

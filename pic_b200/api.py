@@ -41,7 +41,7 @@ EXPORTS = [
     "pic_cuda_stream", "pic_apply_operator", "pic_solver_vectors", "pic_set_precond_stages",
     "pic_coarse_setup", "pic_precond_apply", "pic_set_fcg_inner", "pic_average_x",
     "pic_energy_spectrum", "pic_velocity_moments", "pic_multigrid_setup", "pic_get_next_id",
-    "pic_set_next_id", "pic_set_wall_rf",
+    "pic_set_next_id", "pic_set_wall_rf", "pic_get_fields_async", "pic_wait_fields",
 ]
 
 # z = M(r) callback of flexible CG: (r_dev, z_dev, user) -> 0 or failure
@@ -177,6 +177,8 @@ def load() -> C.CDLL:
     lib.pic_step.argtypes = [C.c_uint64, _P(StepStats)]
     lib.pic_get_field.argtypes = [C.c_int32, d]
     lib.pic_set_field.argtypes = [C.c_int32, d]
+    lib.pic_get_fields_async.argtypes = [d, d, d, d]
+    lib.pic_wait_fields.argtypes = []
     lib.pic_device_timer.argtypes = [C.c_int32, _P(C.c_double)]
     lib.pic_set_preconditioner.argtypes = [PRECOND_FN, C.c_void_p]
     lib.pic_set_solver.argtypes = [C.c_int32]

@@ -104,6 +104,12 @@ struct Ctx {
   double L_ref = 0, t_ref = 0, v_ref = 0, phi_ref = 0;
   cudaStream_t st = nullptr;
   cudaStream_t st2 = nullptr;  // the step's field recovery, alongside its MCC
+  // asynchronous field readback (pic_get_fields_async): the copy stream, the
+  // event it starts after, one event per field (0 rho, 1 phi, 2 efx, 3 efy)
+  // and the fields whose copies may still run
+  cudaStream_t st_copy = nullptr;
+  cudaEvent_t ev_copy_start = nullptr, ev_field[4] = {nullptr, nullptr, nullptr, nullptr};
+  unsigned copy_pending = 0;
   cudaEvent_t ev0 = nullptr, ev1 = nullptr;
   // mesh
   double *d_xs = nullptr, *d_ys = nullptr;

@@ -2753,6 +2753,11 @@ static void free_all() {
   }
   if (g.ev0) cudaEventDestroy(g.ev0);
   if (g.ev1) cudaEventDestroy(g.ev1);
+  if (g.st_copy) cudaStreamSynchronize(g.st_copy);
+  for (auto &ev : g.ev_field)
+    if (ev) cudaEventDestroy(ev);
+  if (g.ev_copy_start) cudaEventDestroy(g.ev_copy_start);
+  if (g.st_copy) cudaStreamDestroy(g.st_copy);
   if (g.st2) cudaStreamDestroy(g.st2);
   if (g.st) cudaStreamDestroy(g.st);
   g = Ctx();
@@ -3636,6 +3641,15 @@ static int run_ppr(cudaStream_t stream = nullptr) {
   return PIC_OK;
 }
 
+// The library's stream waits for the copies of pic_get_fields_async still
+// reading the fields in `mask` (bit f: 0 rho, 1 phi, 2 efx, 3 efy) before
+// anything that writes them.
+static int fields_fence(unsigned mask) {
+  for (int f = 0; f < 4; ++f)
+    if (g.copy_pending & mask & (1u << f)) PIC_CUDA(cudaStreamWaitEvent(g.st, g.ev_field[f], 0));
+  return PIC_OK;
+}
+
 static int check_init() {
   if (!g.inited) {
     set_error("library not initialised (pic_init)");
@@ -3870,6 +3884,9 @@ int pic_init(const pic_mesh_desc *mesh, const pic_params *params) {
   int rc;
   PIC_CUDA(cudaStreamCreateWithFlags(&g.st, cudaStreamNonBlocking));
   PIC_CUDA(cudaStreamCreateWithFlags(&g.st2, cudaStreamNonBlocking));
+  PIC_CUDA(cudaStreamCreateWithFlags(&g.st_copy, cudaStreamNonBlocking));
+  PIC_CUDA(cudaEventCreateWithFlags(&g.ev_copy_start, cudaEventDisableTiming));
+  for (auto &ev : g.ev_field) PIC_CUDA(cudaEventCreateWithFlags(&ev, cudaEventDisableTiming));
   PIC_CUDA(cudaEventCreate(&g.ev0));
   PIC_CUDA(cudaEventCreate(&g.ev1));
   std::vector<double> xs(m.nnx), ys(m.nny);
@@ -4631,6 +4648,7 @@ int pic_move_all(int32_t species, int32_t push_flag) {
 int pic_get_par_chg(int32_t delta, double *rho_out) {
   int rc;
   if ((rc = check_init())) return rc;
+  if ((rc = fields_fence(0xFu))) return rc;
   if (delta != (g.axi ? 1 : 0)) {
     set_error("pic_get_par_chg: delta differs from the mesh's");
     return PIC_ERR_ARG;
@@ -4659,6 +4677,7 @@ int pic_get_par_chg(int32_t delta, double *rho_out) {
 int pic_ife_solve(double *phi_inout, double time, pic_solve_stats *stats) {
   int rc;
   if ((rc = check_init())) return rc;
+  if ((rc = fields_fence(0xFu))) return rc;
   if (phi_inout)
     PIC_CUDA(cudaMemcpyAsync(g.d_phi, phi_inout, g.nn * sizeof(double), cudaMemcpyHostToDevice, g.st));
   PIC_CUDA(cudaEventRecord(g.ev0, g.st));
@@ -4688,6 +4707,7 @@ int pic_set_wall_rf(int32_t wall, double amplitude, double frequency_hz, double 
     set_error("pic_set_wall_rf: the wall is not a Dirichlet wall");
     return PIC_ERR_ARG;
   }
+  if ((rc = fields_fence(0x2u))) return rc;  // writes phi
   // the previous wall back to its static values
   if (g.rf_wall >= 0 && g.rf_count > 0) {
     k_rf_set<<<(g.rf_count + 127) / 128, 128, 0, g.st>>>(g.d_rf_nodes, g.d_rf_base, g.rf_count, 0.0, g.d_phi_dir,
@@ -4716,6 +4736,7 @@ int pic_set_wall_rf(int32_t wall, double amplitude, double frequency_hz, double 
 int pic_get_efield_ppr(double *efx_out, double *efy_out) {
   int rc;
   if ((rc = check_init())) return rc;
+  if ((rc = fields_fence(0xFu))) return rc;
   if ((rc = run_ppr())) return rc;
   if (efx_out)
     PIC_CUDA(cudaMemcpyAsync(efx_out, g.d_efx, g.nn * sizeof(double), cudaMemcpyDeviceToHost, g.st));
@@ -4762,6 +4783,9 @@ int pic_step(uint64_t step, pic_step_stats *stats) {
     }
   g.sel_push = false;
   PIC_CUDA(cudaEventRecord(e[7], g.st));
+  // the fields' writers (deposit, solve, field recovery) follow the copies
+  // of the previous step's fields, which ran alongside the push
+  if ((rc = fields_fence(0xFu))) return rc;
   if ((rc = run_rho(diag))) return rc;
   PIC_CUDA(cudaEventRecord(e[1], g.st));
   // 2. Poisson (IFE_Solve_2D)
@@ -4823,6 +4847,33 @@ int pic_step(uint64_t step, pic_step_stats *stats) {
   return solve_rc;
 }
 
+int pic_get_fields_async(double *rho_out, double *phi_out, double *efx_out, double *efy_out) {
+  int rc;
+  if ((rc = check_init())) return rc;
+  PIC_CUDA(cudaEventRecord(g.ev_copy_start, g.st));
+  PIC_CUDA(cudaStreamWaitEvent(g.st_copy, g.ev_copy_start, 0));
+  struct {
+    double *host;
+    const double *dev;
+    int f;
+  } c[4] = {{phi_out, g.d_phi, 1}, {rho_out, g.d_rho, 0}, {efx_out, g.d_efx, 2}, {efy_out, g.d_efy, 3}};
+  for (auto &q : c) {
+    if (!q.host) continue;
+    PIC_CUDA(cudaMemcpyAsync(q.host, q.dev, g.nn * sizeof(double), cudaMemcpyDeviceToHost, g.st_copy));
+    PIC_CUDA(cudaEventRecord(g.ev_field[q.f], g.st_copy));
+    g.copy_pending |= 1u << q.f;
+  }
+  return PIC_OK;
+}
+
+int pic_wait_fields(void) {
+  int rc;
+  if ((rc = check_init())) return rc;
+  PIC_CUDA(cudaStreamSynchronize(g.st_copy));
+  g.copy_pending = 0;
+  return PIC_OK;
+}
+
 int pic_get_field(int32_t which, double *host_out) {
   int rc;
   if ((rc = check_init())) return rc;
@@ -4860,6 +4911,7 @@ int pic_set_field(int32_t which, const double *host_in) {
     set_error("pic_set_field: unknown field");
     return PIC_ERR_ARG;
   }
+  if ((rc = fields_fence(which <= 3 ? 1u << which : 0u))) return rc;
   PIC_CUDA(cudaMemcpyAsync(dst, host_in, g.nn * sizeof(double), cudaMemcpyHostToDevice, g.st));
   if (g.mixed && (which == 2 || which == 3 || which >= 12)) {
     k_coef32<<<blocks_for(g.nn, 256), 256, 0, g.st>>>(g.d_efx, g.d_efy, g.d_coef, g.d_coef32, g.nn);
