@@ -333,9 +333,19 @@ int pic_set_field(int32_t which, const double *host_in);
  * after `IFE_Solve_2D` / `GetEField_SIDG_PPR` (Main_IFE_Test_2.f90:329-341)
  * when it does not need the values before its next step. */
 int pic_get_fields_async(double *rho_out, double *phi_out, double *efx_out, double *efy_out);
-/* Waits for the copies of pic_get_fields_async; the library's stream is
- * ordered after them too (a pic_device_timer stop covers them). */
+/* Waits for the copies of pic_get_fields_async and pic_set_field_async; the
+ * library's stream is ordered after them too (a pic_device_timer stop
+ * covers them). */
 int pic_wait_fields(void);
+/* Asynchronous upload of rho (which 0) or phi (which 1) from host [nodes],
+ * on the same copy stream, after the copies already queued there (so phi can
+ * go back in from the array pic_get_fields_async is filling): the caller's
+ * next pic_step pushes its particles meanwhile and its deposit, solve and
+ * field recovery wait for the upload; any call that reads or writes the
+ * field first waits for it.  The host array must stay unchanged until
+ * pic_wait_fields.  The role of the Rho / Phi arguments of `IFE_Solve_2D`
+ * (IFE_Solve_2D.f90:1) when the caller keeps the loop going. */
+int pic_set_field_async(int32_t which, const double *host_in);
 
 /* Device pointers of the particle SoA, for zero-copy callers on the same
  * device.  Order: x, y, vx, vy, vz (double*: absolute normalised position and

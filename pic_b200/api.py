@@ -42,6 +42,7 @@ EXPORTS = [
     "pic_coarse_setup", "pic_precond_apply", "pic_set_fcg_inner", "pic_average_x",
     "pic_energy_spectrum", "pic_velocity_moments", "pic_multigrid_setup", "pic_get_next_id",
     "pic_set_next_id", "pic_set_wall_rf", "pic_get_fields_async", "pic_wait_fields",
+    "pic_set_field_async",
 ]
 
 # z = M(r) callback of flexible CG: (r_dev, z_dev, user) -> 0 or failure
@@ -179,6 +180,7 @@ def load() -> C.CDLL:
     lib.pic_set_field.argtypes = [C.c_int32, d]
     lib.pic_get_fields_async.argtypes = [d, d, d, d]
     lib.pic_wait_fields.argtypes = []
+    lib.pic_set_field_async.argtypes = [C.c_int32, d]
     lib.pic_device_timer.argtypes = [C.c_int32, _P(C.c_double)]
     lib.pic_set_preconditioner.argtypes = [PRECOND_FN, C.c_void_p]
     lib.pic_set_solver.argtypes = [C.c_int32]

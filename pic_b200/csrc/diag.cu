@@ -303,6 +303,7 @@ int pic_average_x(double *out) {
     set_error("pic_average_x: library not initialised (pic_init)");
     return PIC_ERR_STATE;
   }
+  if (int rc = fields_fence(0x3u)) return rc;  // reads rho and phi: after a queued upload
   if (!out) {
     set_error("pic_average_x: null output");
     return PIC_ERR_ARG;

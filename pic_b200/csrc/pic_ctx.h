@@ -260,6 +260,7 @@ int launch_locate(Species &s, int64_t begin, int64_t end);
 int sort_species(int sidx);
 int mcc_run(uint64_t step, pic_mcc_stats *stats, bool prepared = false);
 int mcc_prepare(uint64_t step);
+int fields_fence(unsigned mask);  // the library stream waits for queued copies of fields in mask
 int launch_spmv(const double *v, double *out);  // out = A v (solver operator)
 int coarse_setup(const pic_mesh_desc *mesh, int coarse_cells);
 int precond_apply(int full, const double *r, double *z);

@@ -3641,10 +3641,11 @@ static int run_ppr(cudaStream_t stream = nullptr) {
   return PIC_OK;
 }
 
-// The library's stream waits for the copies of pic_get_fields_async still
-// reading the fields in `mask` (bit f: 0 rho, 1 phi, 2 efx, 3 efy) before
-// anything that writes them.
-static int fields_fence(unsigned mask) {
+// The library's stream waits for the copies of pic_get_fields_async (still
+// reading the fields) and pic_set_field_async (still writing them) queued
+// for the fields in `mask` (bit f: 0 rho, 1 phi, 2 efx, 3 efy), before
+// anything that writes, or after an upload reads, them.
+int fields_fence(unsigned mask) {
   for (int f = 0; f < 4; ++f)
     if (g.copy_pending & mask & (1u << f)) PIC_CUDA(cudaStreamWaitEvent(g.st, g.ev_field[f], 0));
   return PIC_OK;
@@ -4866,6 +4867,24 @@ int pic_get_fields_async(double *rho_out, double *phi_out, double *efx_out, doub
   return PIC_OK;
 }
 
+int pic_set_field_async(int32_t which, const double *host_in) {
+  int rc;
+  if ((rc = check_init())) return rc;
+  if (!host_in || (which != 0 && which != 1)) {
+    set_error("pic_set_field_async: which must be 0 (rho) or 1 (phi), host_in not NULL");
+    return PIC_ERR_ARG;
+  }
+  double *dst = which == 0 ? g.d_rho : g.d_phi;
+  // after what the library's stream has queued (the field may still be
+  // read or written there) and after the copies already on the copy stream
+  PIC_CUDA(cudaEventRecord(g.ev_copy_start, g.st));
+  PIC_CUDA(cudaStreamWaitEvent(g.st_copy, g.ev_copy_start, 0));
+  PIC_CUDA(cudaMemcpyAsync(dst, host_in, g.nn * sizeof(double), cudaMemcpyHostToDevice, g.st_copy));
+  PIC_CUDA(cudaEventRecord(g.ev_field[which], g.st_copy));
+  g.copy_pending |= 1u << which;
+  return PIC_OK;
+}
+
 int pic_wait_fields(void) {
   int rc;
   if ((rc = check_init())) return rc;
@@ -4892,6 +4911,7 @@ int pic_get_field(int32_t which, double *host_out) {
     set_error("pic_get_field: unknown field");
     return PIC_ERR_ARG;
   }
+  if ((rc = fields_fence(which <= 3 ? 1u << which : 0u))) return rc;  // an upload of it may be queued
   PIC_CUDA(cudaMemcpyAsync(host_out, src, g.nn * sizeof(double), cudaMemcpyDeviceToHost, g.st));
   PIC_CUDA(cudaStreamSynchronize(g.st));
   return PIC_OK;

@@ -1,9 +1,11 @@
-"""pic_get_fields_async: the fields a step leaves are copied to host on the
-library's copy stream while the caller's next step runs, and every writer
-of a field waits for its copy.  Two identical runs, one reading the fields
-synchronously after every step and one asynchronously (feeding each step's
-phi back through pic_set_field, as a Fortran caller passes Phi in), give
-identical fields and an identical final state."""
+"""pic_get_fields_async and pic_set_field_async: the fields a step leaves
+are copied to host, and the next phi copied in, on the library's copy stream
+while the caller's next step pushes its particles; every reader or writer of
+a field on the device waits for its copies.  Two identical runs, one with
+synchronous pic_set_field / pic_get_field calls and one with the
+asynchronous ones (each step's phi goes back in from the array the previous
+step's readback filled, as a Fortran caller passes Phi in), give identical
+fields and an identical final state."""
 import ctypes as C
 
 import numpy as np
@@ -38,7 +40,10 @@ def test_async_readback_matches_synchronous(precision):
             phi_in[:] = sim.field("phi")
             for t in range(steps):
                 src = phi_in if t == 0 else bufs[t - 1]["phi"]
-                api.check(lib.pic_set_field(1, api.dptr(src)), "set phi")
+                if overlap:
+                    api.check(lib.pic_set_field_async(1, api.dptr(src)), "async set phi")
+                else:
+                    api.check(lib.pic_set_field(1, api.dptr(src)), "set phi")
                 sim.step()
                 if overlap:
                     b = bufs[t]
