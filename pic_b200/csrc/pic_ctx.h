@@ -110,6 +110,8 @@ struct Ctx {
   cudaStream_t st_copy = nullptr;
   cudaEvent_t ev_copy_start = nullptr, ev_field[4] = {nullptr, nullptr, nullptr, nullptr};
   unsigned copy_pending = 0;
+  cudaEvent_t step_ev[10] = {};                 // pic_step's phase events, created once
+  unsigned long long *h_counters = nullptr;     // pinned mirror of d_counters
   cudaEvent_t ev0 = nullptr, ev1 = nullptr;
   // mesh
   double *d_xs = nullptr, *d_ys = nullptr;
@@ -232,11 +234,8 @@ struct Ctx {
   void *h_fcg = nullptr;               // pinned FcgState of the fused persistent FCG
   size_t fcg_smem_set = 0;             // dynamic shared memory the FCG kernel was opened to
   int fcg_fused = 1;                   // PIC_FCG_FUSED=0: set-up and judge by separate kernels
-  void *h_ion = nullptr;               // pinned staging: ionisations read back
-  int64_t h_ion_cap = 0;
-  void *h_new = nullptr;               // pinned staging: created particles' slots and velocities
-  int64_t h_new_cap = 0;
-  int32_t *d_mcc_pslot = nullptr;      // created particles: parent slots, velocities
+  int32_t *d_mcc_pslot = nullptr;      // created particles: parent slots, velocities (e, ion), rank order
+  int32_t *d_ion_order = nullptr;
   double *d_mcc_vel = nullptr;
   int64_t mcc_new_cap = 0;
   int64_t step_count = 0;

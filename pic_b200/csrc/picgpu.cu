@@ -2741,10 +2741,8 @@ static void free_all() {
   fcg_graphs_free();
   F(g.d_cell_count); F(g.d_cell_start); F(g.d_cell_fill); F(g.d_perm); F(g.d_perm2); F(g.d_sort_id);
   F(g.d_scan_blk); F(g.d_counters); F(g.d_hist); F(g.d_sel); F(g.d_cand); F(g.d_cand_slot);
-  F(g.d_mcc_misc); F(g.d_mlist_key); F(g.d_mlist_slot); F(g.d_msel); F(g.d_ion_parent); F(g.d_ion_data); F(g.d_mcc_pslot); F(g.d_mcc_vel);
-  if (g.h_ion) cudaFreeHost(g.h_ion);
+  F(g.d_mcc_misc); F(g.d_mlist_key); F(g.d_mlist_slot); F(g.d_msel); F(g.d_ion_parent); F(g.d_ion_data); F(g.d_mcc_pslot); F(g.d_mcc_vel); F(g.d_ion_order);
   if (g.h_fcg) cudaFreeHost(g.h_fcg);
-  if (g.h_new) cudaFreeHost(g.h_new);
   for (int s = 0; s < PIC_MAX_SPECIES; ++s) {
     Species &p = g.sp[s];
     F(p.x); F(p.y); F(p.vx); F(p.vy); F(p.vz); F(p.loc); F(p.id);
@@ -2754,6 +2752,9 @@ static void free_all() {
   if (g.ev0) cudaEventDestroy(g.ev0);
   if (g.ev1) cudaEventDestroy(g.ev1);
   if (g.st_copy) cudaStreamSynchronize(g.st_copy);
+  for (auto &ev : g.step_ev)
+    if (ev) cudaEventDestroy(ev);
+  if (g.h_counters) cudaFreeHost(g.h_counters);
   for (auto &ev : g.ev_field)
     if (ev) cudaEventDestroy(ev);
   if (g.ev_copy_start) cudaEventDestroy(g.ev_copy_start);
@@ -2771,11 +2772,15 @@ int launch_locate(Species &s, int64_t begin, int64_t end) {
   return PIC_OK;
 }
 
-static int read_counter(int idx, unsigned long long *v) {
-  PIC_CUDA(cudaMemcpyAsync(v, g.d_counters + idx, sizeof *v, cudaMemcpyDeviceToHost, g.st));
+// counters [first, first + n) through the pinned mirror, one wait
+static int read_counters(int first, int n, unsigned long long *v) {
+  PIC_CUDA(cudaMemcpyAsync(g.h_counters + first, g.d_counters + first, n * sizeof *v, cudaMemcpyDeviceToHost, g.st));
   PIC_CUDA(cudaStreamSynchronize(g.st));
+  for (int k = 0; k < n; ++k) v[k] = g.h_counters[first + k];
   return PIC_OK;
 }
+
+static int read_counter(int idx, unsigned long long *v) { return read_counters(idx, 1, v); }
 
 static int zero_counter(int idx) {
   PIC_CUDA(cudaMemsetAsync(g.d_counters + idx, 0, sizeof(unsigned long long), g.st));
@@ -3886,6 +3891,8 @@ int pic_init(const pic_mesh_desc *mesh, const pic_params *params) {
   PIC_CUDA(cudaStreamCreateWithFlags(&g.st, cudaStreamNonBlocking));
   PIC_CUDA(cudaStreamCreateWithFlags(&g.st2, cudaStreamNonBlocking));
   PIC_CUDA(cudaStreamCreateWithFlags(&g.st_copy, cudaStreamNonBlocking));
+  for (auto &ev : g.step_ev) PIC_CUDA(cudaEventCreate(&ev));
+  PIC_CUDA(cudaMallocHost(&g.h_counters, 32 * sizeof(unsigned long long)));
   PIC_CUDA(cudaEventCreateWithFlags(&g.ev_copy_start, cudaEventDisableTiming));
   for (auto &ev : g.ev_field) PIC_CUDA(cudaEventCreateWithFlags(&ev, cudaEventDisableTiming));
   PIC_CUDA(cudaEventCreate(&g.ev0));
@@ -4756,8 +4763,7 @@ int pic_sort_particles(int32_t species) {
 int pic_step(uint64_t step, pic_step_stats *stats) {
   int rc;
   if ((rc = check_init())) return rc;
-  cudaEvent_t e[10];
-  for (auto &ev : e) PIC_CUDA(cudaEventCreate(&ev));
+  cudaEvent_t *e = g.step_ev;  // created once, at pic_init
   PIC_CUDA(cudaEventRecord(e[0], g.st));
   // 1. fused push + locate + deposit (MoveAll, then GetParChg_2D).  The
   // per-node energy (Ek_tot) is a diagnostic the reference only writes at its
@@ -4803,8 +4809,14 @@ int pic_step(uint64_t step, pic_step_stats *stats) {
   PIC_CUDA(cudaEventRecord(e[8], g.st2));
   if ((rc = run_ppr(g.st2))) return rc;
   PIC_CUDA(cudaEventRecord(e[9], g.st2));
-  for (int s = 0; s < g.ns; ++s)
-    if ((rc = count_live(s))) return rc;
+  {  // the particles each species lost in the push, one read for all
+    unsigned long long lost[PIC_MAX_SPECIES];
+    if ((rc = read_counters(8, g.ns, lost))) return rc;
+    for (int s = 0; s < g.ns; ++s) {
+      g.sp[s].n_live -= (int64_t)lost[s];
+      if ((rc = zero_counter(8 + s))) return rc;
+    }
+  }
   // 4. MCC
   pic_mcc_stats ms;
   std::memset(&ms, 0, sizeof ms);
@@ -4817,10 +4829,16 @@ int pic_step(uint64_t step, pic_step_stats *stats) {
     for (int s = 0; s < g.ns; ++s)
       if ((rc = sort_species(s))) return rc;
   PIC_CUDA(cudaEventRecord(e[5], g.st));
-  PIC_CUDA(cudaStreamSynchronize(g.st));
-  unsigned long long bad = 0;
-  if ((rc = read_counter(1, &bad))) return rc;
-  if ((rc = check_push_fail("pic_step"))) return rc;
+  // particles outside the mesh (counter 1) and push tiles that never
+  // arrived (counter 2), one read (it also waits for the step)
+  unsigned long long c12[2] = {0, 0};
+  if ((rc = read_counters(1, 2, c12))) return rc;
+  const unsigned long long bad = c12[0];
+  if (c12[1]) {
+    zero_counter(2);
+    set_error("pic_step: a push tile copy did not complete within its bounded wait");
+    return PIC_ERR_CUDA;
+  }
   ++g.step_count;
   if (stats) {
     std::memset(stats, 0, sizeof *stats);
@@ -4840,7 +4858,6 @@ int pic_step(uint64_t step, pic_step_stats *stats) {
     cudaEventElapsedTime(&t, e[6], e[7]); stats->ms_push_kernel = t;
     stats->pushed = pushed;
   }
-  for (auto &ev : e) cudaEventDestroy(ev);
   if (bad) {
     set_error("pic_step: particle outside the mesh after the push");
     return PIC_ERR_DOMAIN;

@@ -590,6 +590,45 @@ __global__ void k_mcc_append(AppendK a) {
   a.id[d] = a.id_base + (uint32_t)r;
 }
 
+// Rank of each ionisation of a species among the others by its parent key
+// (id << 32 | slot: ids are unique, so keys are), from shared-memory tiles of
+// all the keys: the created particles are appended in parent-id order, the
+// order the oracle appends them in, whatever order the collisions recorded
+// them in.  n^2 compares: a few thousand to some ten thousand a step.
+__global__ void __launch_bounds__(128) k_ion_rank(const int64_t *__restrict__ parent, int64_t n,
+                                                 int32_t *__restrict__ order) {
+  __shared__ int64_t tile[2048];
+  const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  const int64_t me = i < n ? parent[i] : 0;
+  int64_t rank = 0;
+  for (int64_t t0 = 0; t0 < n; t0 += 2048) {
+    const int m = n - t0 < 2048 ? (int)(n - t0) : 2048;
+    __syncthreads();
+    for (int k = threadIdx.x; k < m; k += blockDim.x) tile[k] = parent[t0 + k];
+    __syncthreads();
+    if (i < n)
+      for (int k = 0; k < m; ++k) rank += tile[k] < me ? 1 : 0;
+  }
+  if (i < n) order[rank] = (int32_t)i;
+}
+
+// The appended particles' parent slots and velocities in rank order: the
+// created electron's (normalised in k_mcc_collide), the ion's (SI, divided
+// by v_ref here, as MCCAddNewParticle normalises it)
+__global__ void k_ion_build(const int64_t *__restrict__ parent, const double *__restrict__ data,
+                            const int32_t *__restrict__ order, int64_t n, double vref, int32_t *__restrict__ pslot,
+                            double *__restrict__ vel_e, double *__restrict__ vel_i) {
+  const int64_t r = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (r >= n) return;
+  const int64_t src = order[r];
+  pslot[r] = (int32_t)(parent[src] & 0xffffffff);
+#pragma unroll
+  for (int q = 0; q < 3; ++q) {
+    vel_e[3 * r + q] = data[6 * src + q];
+    vel_i[3 * r + q] = data[6 * src + 3 + q] / vref;
+  }
+}
+
 // selected slots and the ionisation outputs (one region of mcc_cap entries
 // per species); grown only before anything of the step is queued
 static int mcc_alloc(int64_t need) {
@@ -641,12 +680,6 @@ static int mcc_list_alloc(int64_t need) {
   return PIC_OK;
 }
 
-struct Pending {
-  int32_t from_species;
-  std::vector<int64_t> parent;  // sorted (id<<32 | slot)
-  std::vector<double> data;     // 6 per entry, parent order
-  int32_t e_species, ion_species;
-};
 
 // Full-histogram selection of species s (used when the bounded selection
 // does not apply or did not hold the ncoll smallest keys): histogram of all
@@ -699,25 +732,6 @@ static int mcc_select_full(const MccK &k, int64_t ncoll, int64_t *misc_d) {
   return PIC_OK;
 }
 
-// pinned host staging, grown on demand (kept across steps)
-static int mcc_host_alloc(void **buf, int64_t *cap, int64_t bytes) {
-  if (bytes <= *cap) return PIC_OK;
-  if (*buf) PIC_CUDA(cudaFreeHost(*buf));
-  *buf = nullptr;
-  *cap = 0;
-  const int64_t c = std::max<int64_t>(bytes + bytes / 2, 1 << 16);
-  PIC_CUDA(cudaMallocHost(buf, c));
-  *cap = c;
-  return PIC_OK;
-}
-
-// MCC of every species with tables, one step.  Each species' selection and
-// collisions are queued without waiting for the host: k_mcc_ties records
-// whether the bounded selection holds the ncoll smallest keys and
-// k_mcc_collide does nothing when it does not.  One read of the status
-// blocks then finds the species (rarely any) that need the full selection,
-// and one more brings back the ionisations; the created particles are
-// appended from pinned staging without a further wait.
 // the bounded selection's sink of species s: key bound, list capacity,
 // per-species histogram, list and counters
 static MccSink mcc_sink(int s, uint64_t bound, int64_t lcap, uint32_t slo, uint32_t shi) {
@@ -777,6 +791,12 @@ int mcc_prepare(uint64_t step) {
   return PIC_OK;
 }
 
+// MCC of every species with tables, one step.  Each species' selection and
+// collisions are queued without waiting for the host: k_mcc_ties records
+// whether the bounded selection holds the ncoll smallest keys and
+// k_mcc_collide does nothing when it does not.  One read of the status
+// blocks then finds the species (rarely any) that need the full selection;
+// the created particles are ordered and appended on the device.
 int mcc_run(uint64_t step, pic_mcc_stats *stats, bool prepared) {
   // the push of this step built the bounded selections (mcc_prepare)
   const bool prep = prepared && g.sel_step == step;
@@ -883,8 +903,10 @@ int mcc_run(uint64_t step, pic_mcc_stats *stats, bool prepared) {
                              g.st));
     PIC_CUDA(cudaStreamSynchronize(g.st));
   }
-  // 3. ionisations: parents and velocities of every species in one read
-  int64_t nion[PIC_MAX_SPECIES] = {0}, nion_all = 0;
+  // 3. ionisations: the host reads only the counts; each species' are put in
+  // parent-id order and appended on the device (MCCAddNewParticle, after
+  // every species collided)
+  int64_t nion[PIC_MAX_SPECIES] = {0};
   for (int s = 0; s < g.ns; ++s) {
     if (ncoll[s] <= 0) continue;
     const int64_t *m2 = misc_h + s * kMccMisc;
@@ -895,91 +917,48 @@ int mcc_run(uint64_t step, pic_mcc_stats *stats, bool prepared) {
       set_error("mcc: ionisation buffer overflow");
       return PIC_ERR_CAPACITY;
     }
-    nion_all += nion[s];
   }
-  if (nion_all == 0) return PIC_OK;
-  if ((rc = mcc_host_alloc(&g.h_ion, &g.h_ion_cap, nion_all * 56))) return rc;
-  {
-    char *h = static_cast<char *>(g.h_ion);
-    for (int s = 0; s < g.ns; ++s) {
-      if (nion[s] == 0) continue;
-      PIC_CUDA(cudaMemcpyAsync(h, g.d_ion_parent + s * g.mcc_cap, nion[s] * 8, cudaMemcpyDeviceToHost, g.st));
-      PIC_CUDA(cudaMemcpyAsync(h + nion[s] * 8, g.d_ion_data + 6 * s * g.mcc_cap, nion[s] * 48,
-                               cudaMemcpyDeviceToHost, g.st));
-      h += nion[s] * 56;
-    }
-    PIC_CUDA(cudaStreamSynchronize(g.st));
-  }
-  std::vector<Pending> pend;
-  {
-    const char *h = static_cast<const char *>(g.h_ion);
-    for (int s = 0; s < g.ns; ++s) {
-      const int64_t n = nion[s];
-      if (n == 0) continue;
-      const int64_t *par = reinterpret_cast<const int64_t *>(h);
-      const double *data = reinterpret_cast<const double *>(h + n * 8);
-      h += n * 56;
-      std::vector<int64_t> order(n);
-      for (int64_t i = 0; i < n; ++i) order[i] = i;
-      std::sort(order.begin(), order.end(), [&](int64_t a, int64_t b) { return par[a] < par[b]; });
-      Pending pd;
-      pd.from_species = s;
-      pd.parent.resize(n);
-      pd.data.resize(6 * n);
-      for (int64_t i = 0; i < n; ++i) {
-        pd.parent[i] = par[order[i]];
-        for (int q = 0; q < 6; ++q) pd.data[6 * i + q] = data[6 * order[i] + q];
-      }
-      pd.e_species = s;
-      // resultant of the ionisation reaction
-      pd.ion_species = -1;
-      for (int r = 0; r < g.sp[s].tab.n_reaction; ++r)
-        if (g.sp[s].tab.reaction_type[r] == 13) pd.ion_species = g.sp[s].tab.resultant[r];
-      pend.push_back(std::move(pd));
-    }
-  }
-  // 4. MCCAddNewParticle: append the created particles after all species
-  // collided, from pinned staging (one region per copy, so that no copy
-  // still queued reads a region the host is filling)
-  int64_t stage = 0;
-  for (auto &pd : pend) stage += (int64_t)pd.parent.size() * (4 + 2 * 24);
-  if ((rc = mcc_host_alloc(&g.h_new, &g.h_new_cap, stage))) return rc;
-  char *h = static_cast<char *>(g.h_new);
-  for (auto &pd : pend) {
-    const int64_t n = (int64_t)pd.parent.size();
-    if (n > g.mcc_new_cap) {  // grow the created-particle staging (kept across steps)
+  for (int s = 0; s < g.ns; ++s) {
+    const int64_t n = nion[s];
+    if (n == 0) continue;
+    if (n > g.mcc_new_cap) {  // grow the created-particle buffers (kept across steps)
       PIC_CUDA(cudaStreamSynchronize(g.st));
       cudaFree(g.d_mcc_pslot);
       cudaFree(g.d_mcc_vel);
+      cudaFree(g.d_ion_order);
       g.d_mcc_pslot = nullptr;
       g.d_mcc_vel = nullptr;
+      g.d_ion_order = nullptr;
       g.mcc_new_cap = 0;
       const int64_t cap = std::max<int64_t>(2 * n, 1 << 16);
       PIC_CUDA(cudaMalloc(&g.d_mcc_pslot, cap * 4));
-      PIC_CUDA(cudaMalloc(&g.d_mcc_vel, 3 * cap * 8));
+      PIC_CUDA(cudaMalloc(&g.d_mcc_vel, 6 * cap * 8));
+      PIC_CUDA(cudaMalloc(&g.d_ion_order, cap * 4));
       g.mcc_new_cap = cap;
     }
-    int32_t *pslot = reinterpret_cast<int32_t *>(h);
-    h += n * 4;
-    for (int64_t i = 0; i < n; ++i) pslot[i] = (int32_t)(pd.parent[i] & 0xffffffff);
-    PIC_CUDA(cudaMemcpyAsync(g.d_mcc_pslot, pslot, n * 4, cudaMemcpyHostToDevice, g.st));
-    Species &from = g.sp[pd.from_species];
+    const int64_t *parent = g.d_ion_parent + s * g.mcc_cap;
+    double *vel_e = g.d_mcc_vel, *vel_i = g.d_mcc_vel + 3 * g.mcc_new_cap;
+    k_ion_rank<<<blocks_for(n, 128), 128, 0, g.st>>>(parent, n, g.d_ion_order);
+    PIC_LAUNCHED();
+    k_ion_build<<<blocks_for(n, 256), 256, 0, g.st>>>(parent, g.d_ion_data + 6 * s * g.mcc_cap, g.d_ion_order, n,
+                                                      g.v_ref, g.d_mcc_pslot, vel_e, vel_i);
+    PIC_LAUNCHED();
+    // the created electron joins species s; the ion the ionisation
+    // reaction's resultant
+    int ion_species = -1;
+    for (int r = 0; r < g.sp[s].tab.n_reaction; ++r)
+      if (g.sp[s].tab.reaction_type[r] == 13) ion_species = g.sp[s].tab.resultant[r];
+    Species &from = g.sp[s];
     for (int which = 0; which < 2; ++which) {
-      const int ts = which == 0 ? pd.e_species : pd.ion_species;
-      double *vel = reinterpret_cast<double *>(h);
-      h += n * 24;
+      const int ts = which == 0 ? s : ion_species;
       if (ts < 0 || ts >= g.ns) continue;
       Species &to = g.sp[ts];
       if (to.n_slots + n > to.capacity) {
         set_error("mcc: particle capacity exceeded by ionisation");
         return PIC_ERR_CAPACITY;
       }
-      for (int64_t i = 0; i < n; ++i)
-        for (int q = 0; q < 3; ++q)
-          vel[3 * i + q] = which == 0 ? pd.data[6 * i + q] : pd.data[6 * i + 3 + q] / g.v_ref;
-      PIC_CUDA(cudaMemcpyAsync(g.d_mcc_vel, vel, 3 * n * 8, cudaMemcpyHostToDevice, g.st));
       AppendK a{from.x, from.y, from.loc, to.x, to.y, to.vx, to.vy, to.vz, to.loc, to.id,
-                to.n_slots, to.next_id, g.d_mcc_pslot, g.d_mcc_vel, n, to.f32 ? 1 : 0};
+                to.n_slots, to.next_id, g.d_mcc_pslot, which == 0 ? vel_e : vel_i, n, to.f32 ? 1 : 0};
       k_mcc_append<<<blocks_for(n, 256), 256, 0, g.st>>>(a);
       PIC_LAUNCHED();
       to.n_slots += n;
