@@ -111,7 +111,8 @@ struct Ctx {
   cudaEvent_t ev_copy_start = nullptr, ev_field[4] = {nullptr, nullptr, nullptr, nullptr};
   unsigned copy_pending = 0;
   cudaEvent_t step_ev[10] = {};                 // pic_step's phase events, created once
-  unsigned long long *h_counters = nullptr;     // pinned mirror of d_counters
+  unsigned long long *h_counters = nullptr;     // mapped pinned mirror of d_counters
+  unsigned long long *hd_counters = nullptr;    // its device address (a kernel writes it)
   cudaEvent_t ev0 = nullptr, ev1 = nullptr;
   // mesh
   double *d_xs = nullptr, *d_ys = nullptr;
@@ -260,6 +261,7 @@ int sort_species(int sidx);
 int mcc_run(uint64_t step, pic_mcc_stats *stats, bool prepared = false);
 int mcc_prepare(uint64_t step);
 int fields_fence(unsigned mask);  // the library stream waits for queued copies of fields in mask
+int zero_async(void *p, size_t bytes, cudaStream_t st);  // zero fill by a kernel (bytes, p: multiples of 4)
 int launch_spmv(const double *v, double *out);  // out = A v (solver operator)
 int coarse_setup(const pic_mesh_desc *mesh, int coarse_cells);
 int precond_apply(int full, const double *r, double *z);

@@ -2772,20 +2772,52 @@ int launch_locate(Species &s, int64_t begin, int64_t end) {
   return PIC_OK;
 }
 
-// counters [first, first + n) through the pinned mirror, one wait
+// Counters and zero fills on the library's stream go through kernels, not
+// cudaMemcpyAsync / cudaMemsetAsync: copy-engine work of the stream queues
+// behind a caller's field transfers in the same direction on the copy
+// stream (pic_get_fields_async, ~0.6 ms for four 8 MB fields), and the
+// stream's next step then starts only after them instead of alongside.
+__global__ void k_counters_out(unsigned long long *dst, const unsigned long long *src, int n) {
+  if ((int)threadIdx.x < n) dst[threadIdx.x] = src[threadIdx.x];
+}
+
+__global__ void k_zero(uint32_t *head, int nhead, uint4 *mid, int64_t nmid, uint32_t *tail, int ntail) {
+  const int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x, stride = (int64_t)gridDim.x * blockDim.x;
+  if (t < nhead) head[t] = 0u;
+  if (t < ntail) tail[t] = 0u;
+  for (int64_t i = t; i < nmid; i += stride) mid[i] = make_uint4(0u, 0u, 0u, 0u);
+}
+
+int zero_async(void *p, size_t bytes, cudaStream_t st) {
+  if (bytes == 0) return PIC_OK;
+  const uintptr_t a = (uintptr_t)p, e = a + bytes;
+  if ((a | bytes) & 3u) {
+    set_error("zero_async: pointer and size must be multiples of 4 bytes");
+    return PIC_ERR_ARG;
+  }
+  uintptr_t m0 = (a + 15u) & ~(uintptr_t)15u, m1 = e & ~(uintptr_t)15u;
+  if (m1 < m0) m0 = m1 = e;  // under 16 aligned bytes: all in the head
+  const int nhead = (int)((m0 - a) / 4), ntail = (int)((e - m1) / 4);
+  const int64_t nmid = (int64_t)((m1 - m0) / 16);
+  const int64_t blocks = std::max<int64_t>(1, std::min<int64_t>((nmid + 255) / 256, 148 * 8));
+  k_zero<<<(unsigned)blocks, 256, 0, st>>>((uint32_t *)a, nhead, (uint4 *)m0, nmid, (uint32_t *)m1, ntail);
+  PIC_LAUNCHED();
+  return PIC_OK;
+}
+
+// counters [first, first + n) (n <= 32) through the mapped mirror, one wait
 static int read_counters(int first, int n, unsigned long long *v) {
-  PIC_CUDA(cudaMemcpyAsync(g.h_counters + first, g.d_counters + first, n * sizeof *v, cudaMemcpyDeviceToHost, g.st));
+  k_counters_out<<<1, 32, 0, g.st>>>(g.hd_counters + first, g.d_counters + first, n);
+  PIC_LAUNCHED();
   PIC_CUDA(cudaStreamSynchronize(g.st));
-  for (int k = 0; k < n; ++k) v[k] = g.h_counters[first + k];
+  const volatile unsigned long long *h = g.h_counters;
+  for (int k = 0; k < n; ++k) v[k] = h[first + k];
   return PIC_OK;
 }
 
 static int read_counter(int idx, unsigned long long *v) { return read_counters(idx, 1, v); }
 
-static int zero_counter(int idx) {
-  PIC_CUDA(cudaMemsetAsync(g.d_counters + idx, 0, sizeof(unsigned long long), g.st));
-  return PIC_OK;
-}
+static int zero_counter(int idx) { return zero_async(g.d_counters + idx, sizeof(unsigned long long), g.st); }
 
 // push and/or locate+deposit for one species
 static int run_push(int sidx, bool do_push, bool do_deposit, bool do_energy) {
@@ -2918,8 +2950,9 @@ static int from_mixed(Species &s) {
 
 static int zero_deposit(bool energy) {
   for (int s = 0; s < g.ns; ++s) {
-    PIC_CUDA(cudaMemsetAsync(g.sp[s].q_acc, 0, g.nn * sizeof(unsigned long long), g.st));
-    if (energy) PIC_CUDA(cudaMemsetAsync(g.sp[s].e_acc, 0, g.nn * sizeof(unsigned long long), g.st));
+    if (int rc = zero_async(g.sp[s].q_acc, g.nn * sizeof(unsigned long long), g.st)) return rc;
+    if (energy)
+      if (int rc = zero_async(g.sp[s].e_acc, g.nn * sizeof(unsigned long long), g.st)) return rc;
   }
   return PIC_OK;
 }
@@ -3044,7 +3077,7 @@ static int run_pcg(pic_solve_stats *stats) {
     P.bar_err = (int *)(g.d_bar + 2);
     P.spin_limit = g.pcg_spin_limit;
     P.bar_extra = g.pcg_bar_extra;
-    PIC_CUDA(cudaMemsetAsync(g.d_bar, 0, 4 * sizeof(unsigned int), g.st));
+    if (int rc_ = zero_async(g.d_bar, 4 * sizeof(unsigned int), g.st)) return rc_;
     if (g.smem_grid > 0) {
       PcgS Q;
       Q.k = pcg_k(0);
@@ -3132,7 +3165,7 @@ static int precond_stage_a(const double *r, double *zA, int learned) {
   } else if (g.pc_cs > 0) {
     if ((rc = coarse_correct(r, zA, 1))) return rc;
   } else {
-    PIC_CUDA(cudaMemsetAsync(zA, 0, g.nn * sizeof(double), g.st));
+    if (int rc_ = zero_async(zA, g.nn * sizeof(double), g.st)) return rc_;
   }
   if (learned) {
     k_pc_mid<<<nb, 256, 0, g.st>>>(k0, r, zA, g.d_pc_t);
@@ -3309,7 +3342,7 @@ static int run_fcg_persist64(pic_solve_stats *stats, int *fcg_iters, int *rc_out
     return fallback;
   };
   for (int judged = 0;; ++judged) {
-    PIC_CUDA(cudaMemsetAsync(g.d_bar, 0, 4 * sizeof(unsigned int), g.st));
+    if (int rc_ = zero_async(g.d_bar, 4 * sizeof(unsigned int), g.st)) return rc_;
     void *args[] = {&F};
     PIC_CUDA(cudaLaunchCooperativeKernel(fn, dim3(g.fcg_coop_grid), dim3(kWide), args, smem, g.st));
     PIC_LAUNCHED();
@@ -3423,7 +3456,7 @@ static int run_fcg(pic_solve_stats *stats, int *fcg_iters, int *rc_out) {
       F.bar_extra = g.pcg_bar_extra;
     };
     auto launch = [&](auto &F, const void *fn) -> int {
-      PIC_CUDA(cudaMemsetAsync(g.d_bar, 0, 4 * sizeof(unsigned int), g.st));
+      if (int rc_ = zero_async(g.d_bar, 4 * sizeof(unsigned int), g.st)) return rc_;
       void *args[] = {&F};
       const size_t smem = (size_t)g.pc_ainv_ld * sizeof(double);  // coarse_gemv's staging
       PIC_CUDA(cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
@@ -3476,7 +3509,7 @@ static int run_fcg(pic_solve_stats *stats, int *fcg_iters, int *rc_out) {
         }
         k_f64_to_f32<<<nb, 256, 0, g.st>>>(g.d_r, F.r, nn);
         PIC_LAUNCHED();
-        PIC_CUDA(cudaMemsetAsync(F.x, 0, nn * sizeof(float), g.st));
+        if (int rc_ = zero_async(F.x, nn * sizeof(float), g.st)) return rc_;
         FcgState in{};
         in.rhs = hs.rr;
         in.rr = hs.rr;
@@ -3892,7 +3925,8 @@ int pic_init(const pic_mesh_desc *mesh, const pic_params *params) {
   PIC_CUDA(cudaStreamCreateWithFlags(&g.st2, cudaStreamNonBlocking));
   PIC_CUDA(cudaStreamCreateWithFlags(&g.st_copy, cudaStreamNonBlocking));
   for (auto &ev : g.step_ev) PIC_CUDA(cudaEventCreate(&ev));
-  PIC_CUDA(cudaMallocHost(&g.h_counters, 32 * sizeof(unsigned long long)));
+  PIC_CUDA(cudaHostAlloc(&g.h_counters, 32 * sizeof(unsigned long long), cudaHostAllocMapped));
+  PIC_CUDA(cudaHostGetDevicePointer((void **)&g.hd_counters, g.h_counters, 0));
   PIC_CUDA(cudaEventCreateWithFlags(&g.ev_copy_start, cudaEventDisableTiming));
   for (auto &ev : g.ev_field) PIC_CUDA(cudaEventCreateWithFlags(&ev, cudaEventDisableTiming));
   PIC_CUDA(cudaEventCreate(&g.ev0));
@@ -4497,7 +4531,7 @@ int pic_upload_particles(int32_t species, int64_t n, const double *x, const doub
     PIC_CUDA(cudaMemcpyAsync(s.loc, loc, (size_t)n * 4, cudaMemcpyHostToDevice, g.st));
     PIC_CUDA(cudaStreamSynchronize(g.st));
   } else {
-    PIC_CUDA(cudaMemsetAsync(s.loc, 0, (size_t)n * 4, g.st));
+    if (int rc_ = zero_async(s.loc, (size_t)n * 4, g.st)) return rc_;
     if ((rc = zero_counter(1))) return rc;
     if ((rc = launch_locate(s, 0, n))) return rc;
     unsigned long long bad = 0;

@@ -253,7 +253,7 @@ int sort_species(int sidx) {
   Species &s = g.sp[sidx];
   const int64_t ne = g.ne;
   if (s.n_slots == 0) return PIC_OK;
-  PIC_CUDA(cudaMemsetAsync(g.d_cell_count, 0, (ne + 1) * sizeof(int32_t), g.st));
+  if (int rc_ = zero_async(g.d_cell_count, (ne + 1) * sizeof(int32_t), g.st)) return rc_;
   k_sort_count<<<blocks_for(s.n_slots, 256 * kSortRounds), 256, 0, g.st>>>(s.loc, s.n_slots, g.d_cell_count);
   PIC_LAUNCHED();
   int rc = scan_exclusive(g.d_cell_count, g.d_cell_start, ne + 1);
@@ -686,8 +686,8 @@ static int mcc_list_alloc(int64_t need) {
 // keys, the threshold bin found on the host, its candidates ordered on the
 // host.  Leaves the ncoll selected slots in g.d_sel.
 static int mcc_select_full(const MccK &k, int64_t ncoll, int64_t *misc_d) {
-  PIC_CUDA(cudaMemsetAsync(g.d_hist, 0, 65536 * sizeof(uint32_t), g.st));
-  PIC_CUDA(cudaMemsetAsync(misc_d, 0, kMccMisc * sizeof(int64_t), g.st));
+  if (int rc_ = zero_async(g.d_hist, 65536 * sizeof(uint32_t), g.st)) return rc_;
+  if (int rc_ = zero_async(misc_d, kMccMisc * sizeof(int64_t), g.st)) return rc_;
   uint32_t *keys = g.d_sort_id;  // sort scratch, free while MCC runs
   k_mcc_hist<<<blocks_for(k.n, 256), 256, 0, g.st>>>(k, g.d_hist, keys);
   PIC_LAUNCHED();
@@ -784,8 +784,8 @@ int mcc_prepare(uint64_t step) {
   for (int s = 0; s < g.ns; ++s) {
     if (lcap[s] == 0) continue;
     g.sel_sink[s] = mcc_sink(s, mcc_bound(target[s], (double)g.sp[s].n_live), lcap[s], slo, shi);
-    PIC_CUDA(cudaMemsetAsync(g.sel_sink[s].hist, 0, 65536 * sizeof(uint32_t), g.st));
-    PIC_CUDA(cudaMemsetAsync(g.d_msel + s * kMccSel, 0, kMccSel * sizeof(int64_t), g.st));
+    if (int rc_ = zero_async(g.sel_sink[s].hist, 65536 * sizeof(uint32_t), g.st)) return rc_;
+    if (int rc_ = zero_async(g.d_msel + s * kMccSel, kMccSel * sizeof(int64_t), g.st)) return rc_;
   }
   g.sel_step = step;
   return PIC_OK;
@@ -837,7 +837,7 @@ int mcc_run(uint64_t step, pic_mcc_stats *stats, bool prepared) {
   if ((rc = mcc_alloc(std::max<int64_t>(most, 1 << 16) + 4096))) return rc;
   if ((rc = mcc_cand_alloc(g.mcc_cap))) return rc;
   if ((rc = mcc_list_alloc(lmax))) return rc;  // no growth when prepared (lmax 0)
-  PIC_CUDA(cudaMemsetAsync(g.d_mcc_misc, 0, PIC_MAX_SPECIES * kMccMisc * sizeof(int64_t), g.st));
+  if (int rc_ = zero_async(g.d_mcc_misc, PIC_MAX_SPECIES * kMccMisc * sizeof(int64_t), g.st)) return rc_;
   auto mk = [&](int s) {
     Species &sp = g.sp[s];
     return MccK{sp.x, sp.y, sp.vx, sp.vy, sp.vz, sp.loc, sp.id, sp.n_slots, seed0, seed1, slo, shi, (uint32_t)s,
@@ -873,8 +873,8 @@ int mcc_run(uint64_t step, pic_mcc_stats *stats, bool prepared) {
       sink = g.sel_sink[s];
     } else {
       sink = mcc_sink(s, mcc_bound(mcc_target((double)ncoll[s]), (double)g.sp[s].n_live), lcap[s], slo, shi);
-      PIC_CUDA(cudaMemsetAsync(sink.hist, 0, 65536 * sizeof(uint32_t), g.st));
-      PIC_CUDA(cudaMemsetAsync(ms, 0, kMccSel * sizeof(int64_t), g.st));
+      if (int rc_ = zero_async(sink.hist, 65536 * sizeof(uint32_t), g.st)) return rc_;
+      if (int rc_ = zero_async(ms, kMccSel * sizeof(int64_t), g.st)) return rc_;
       const MccK k = mk(s);
       k_mcc_scan<<<blocks_for((k.n + 3) / 4, 256), 256, 0, g.st>>>(k, sink);
       PIC_LAUNCHED();
