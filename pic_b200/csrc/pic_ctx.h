@@ -142,6 +142,7 @@ struct Ctx {
   double h_ppr_reg[5][9];
   // fields
   double *d_phi = nullptr, *d_rho = nullptr, *d_efx = nullptr, *d_efy = nullptr;
+  double2 *d_efxy = nullptr;  // {efx, efy} per node, written with them (the FP64 push's gather)
   double *d_coef = nullptr;  // [5][nn] coef_ppr(2..6,:)
   bool mixed = false;        // PIC_PREC_MIXED
   float *d_coef32 = nullptr; // mixed: per node {c2, c3, c4, c5, c6, 0, 0, 0} in FP32 (32 B records)

@@ -48,6 +48,7 @@ int cuda_fail(cudaError_t e, const char *where) {
 struct FieldK {
   const double *efx, *efy;
   const double *c2, *c3, *c4, *c5, *c6;
+  const double2 *efxy;  // {efx, efy} per node: the gather's four nodes in four 16-byte loads
 };
 
 __device__ __forceinline__ int locate_elem(const MeshK &m, double x, double y) {
@@ -411,10 +412,9 @@ __device__ __forceinline__ void push_fp64_one(const MeshK &m, const FieldK &f, c
       Ex = -ex;
       Ey = -ey;
     } else {
-      Ex = ((W[0] * f.efx[nodes[0]] + W[1] * f.efx[nodes[1]]) + W[2] * f.efx[nodes[2]]) +
-           W[3] * f.efx[nodes[3]];
-      Ey = ((W[0] * f.efy[nodes[0]] + W[1] * f.efy[nodes[1]]) + W[2] * f.efy[nodes[2]]) +
-           W[3] * f.efy[nodes[3]];
+      const double2 e0 = f.efxy[nodes[0]], e1 = f.efxy[nodes[1]], e2 = f.efxy[nodes[2]], e3 = f.efxy[nodes[3]];
+      Ex = ((W[0] * e0.x + W[1] * e1.x) + W[2] * e2.x) + W[3] * e3.x;
+      Ey = ((W[0] * e0.y + W[1] * e1.y) + W[2] * e2.y) + W[3] * e3.y;
     }
     vx = vx + (prm.qm * Ex) * prm.dt;
     vy = vy + (prm.qm * Ey) * prm.dt;
@@ -476,9 +476,11 @@ __device__ __forceinline__ void push_fp64_one(const MeshK &m, const FieldK &f, c
         int ie, je;
         bilinear(m, en, x, y, W, nodes, &ie, &je);
       }
-      double vz = prm.do_energy ? s.vz[p] : 0.0;
-      energy = ((((0.5 * prm.mass) * ((vx * vx + vy * vy) + vz * vz)) * prm.vref) * prm.vref) /
-               PIC_JTOEV;
+      if (prm.do_energy) {  // the per-node energy is deposited on diagnostic steps only
+        const double vz = s.vz[p];
+        energy = ((((0.5 * prm.mass) * ((vx * vx + vy * vy) + vz * vz)) * prm.vref) * prm.vref) /
+                 PIC_JTOEV;
+      }
     }
   }
 }
@@ -2547,6 +2549,7 @@ struct PprK {
   const double *rows;
   double *coef;  // [5][nn]
   double *efx, *efy;
+  double2 *efxy;  // [nn] {efx, efy} (the FP64 push's gather)
   float *coef32;  // NULL, or [nn][8] FP32 records (mixed precision)
   int nny;
   int64_t nn;
@@ -2607,6 +2610,7 @@ __global__ void k_ppr(PprK k) {
   for (int r = 0; r < 5; ++r) k.coef[(size_t)r * k.nn + n] = c[r];
   k.efx[n] = -c[0];
   k.efy[n] = -c[1];
+  k.efxy[n] = make_double2(-c[0], -c[1]);
   if (k.coef32) {  // mixed precision: one 32-byte FP32 record per node
     float4 *o = reinterpret_cast<float4 *>(k.coef32 + 8 * (size_t)n);
     o[0] = make_float4((float)-c[0], (float)-c[1], (float)c[0], (float)c[1]);
@@ -2623,6 +2627,12 @@ __global__ void k_coef32(const double *__restrict__ efx, const double *__restric
   float4 *o = reinterpret_cast<float4 *>(coef32 + 8 * (size_t)n);
   o[0] = make_float4((float)efx[n], (float)efy[n], (float)coef[n], (float)coef[nn + n]);
   o[1] = make_float4((float)coef[2 * nn + n], (float)coef[3 * nn + n], (float)coef[4 * nn + n], 0.0f);
+}
+
+__global__ void k_efxy(const double *__restrict__ efx, const double *__restrict__ efy, double2 *__restrict__ efxy,
+                       int64_t nn) {
+  int64_t n = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (n < nn) efxy[n] = make_double2(efx[n], efy[n]);
 }
 
 __global__ void k_fill_u64(unsigned long long *a, int64_t n) {
@@ -2733,7 +2743,7 @@ static void free_all() {
   F(g.d_rf_nodes); F(g.d_rf_base);
   F(g.d_xt_ptr); F(g.d_xt_col); F(g.d_xt_val); F(g.d_row_kind); F(g.d_ex_cnt); F(g.d_ex_col);
   F(g.d_ex_val); F(g.d_ex_val32); F(g.d_fcg32); F(g.d_diag); F(g.d_ppr_kind); F(g.d_ppr_ptr); F(g.d_ppr_nodes); F(g.d_ppr_rows);
-  F(g.d_ppr_h); F(g.d_phi); F(g.d_rho); F(g.d_efx); F(g.d_efy); F(g.d_coef); F(g.d_coef32); F(g.d_b); F(g.d_x);
+  F(g.d_ppr_h); F(g.d_phi); F(g.d_rho); F(g.d_efx); F(g.d_efy); F(g.d_efxy); F(g.d_coef); F(g.d_coef32); F(g.d_b); F(g.d_x);
   F(g.d_r); F(g.d_w); F(g.d_p[0]); F(g.d_p[1]); F(g.d_q); F(g.d_part); F(g.d_pcg); F(g.d_bar);
   F(g.d_z); F(g.d_dot); F(g.d_dot_ticket); F(g.d_fcg); F(g.d_fcg_P); F(g.d_fcg_Q); F(g.d_fcg_part);
   precond_free();
@@ -2824,7 +2834,7 @@ static int run_push(int sidx, bool do_push, bool do_deposit, bool do_energy) {
   Species &s = g.sp[sidx];
   if (s.n_slots == 0) return PIC_OK;
   FieldK f{g.d_efx, g.d_efy, g.d_coef, g.d_coef + g.nn, g.d_coef + 2 * g.nn, g.d_coef + 3 * g.nn,
-           g.d_coef + 4 * g.nn};
+           g.d_coef + 4 * g.nn, g.d_efxy};
   PushK prm;
   prm.qm = s.qm;
   prm.dt = g.P.dt;
@@ -3671,6 +3681,7 @@ static int run_ppr(cudaStream_t stream = nullptr) {
   k.coef = g.d_coef;
   k.efx = g.d_efx;
   k.efy = g.d_efy;
+  k.efxy = g.d_efxy;
   k.coef32 = g.d_coef32;
   k.nny = g.m.nny;
   k.nn = g.nn;
@@ -4297,6 +4308,9 @@ int pic_init(const pic_mesh_desc *mesh, const pic_params *params) {
     if ((rc = dalloc(&g.d_coef32, 8 * nn))) return rc;
     PIC_CUDA(cudaMemset(g.d_coef32, 0, 8 * nn * sizeof(float)));
   }
+  // every context (a species can hold FP64 particles in a mixed one)
+  if ((rc = dalloc(&g.d_efxy, nn))) return rc;
+  PIC_CUDA(cudaMemset(g.d_efxy, 0, nn * sizeof(double2)));
   PIC_CUDA(cudaMemset(g.d_rho, 0, nn * sizeof(double)));
   PIC_CUDA(cudaMemcpy(g.d_phi, mesh->phi_dirichlet, nn * sizeof(double), cudaMemcpyHostToDevice));
   for (double **v : {&g.d_b, &g.d_x, &g.d_r, &g.d_w, &g.d_p[0], &g.d_p[1], &g.d_q}) {
@@ -4986,6 +5000,10 @@ int pic_set_field(int32_t which, const double *host_in) {
   PIC_CUDA(cudaMemcpyAsync(dst, host_in, g.nn * sizeof(double), cudaMemcpyHostToDevice, g.st));
   if (g.mixed && (which == 2 || which == 3 || which >= 12)) {
     k_coef32<<<blocks_for(g.nn, 256), 256, 0, g.st>>>(g.d_efx, g.d_efy, g.d_coef, g.d_coef32, g.nn);
+    PIC_LAUNCHED();
+  }
+  if (which == 2 || which == 3) {
+    k_efxy<<<blocks_for(g.nn, 256), 256, 0, g.st>>>(g.d_efx, g.d_efy, g.d_efxy, g.nn);
     PIC_LAUNCHED();
   }
   PIC_CUDA(cudaStreamSynchronize(g.st));
