@@ -72,10 +72,16 @@ __device__ __forceinline__ int elem_column(const MeshK &m, int e) {
   return i;
 }
 
+// The element's node coordinates are computed, not loaded: xs[i] is
+// xmin + hx*i (one product and one sum, correctly rounded on the host and,
+// without contraction, here), so the values are the same bits.
+__device__ __forceinline__ double node_x(const MeshK &m, int i) { return m.xmin + m.hx * (double)i; }
+__device__ __forceinline__ double node_y(const MeshK &m, int j) { return m.ymin + m.hy * (double)j; }
+
 __device__ __forceinline__ void bilinear(const MeshK &m, int e, double x, double y, double W[4],
                                          int nodes[4], int *ie, int *je) {
   int i = elem_column(m, e), j = e - i * m.ney;
-  double x1 = m.xs[i], x2 = m.xs[i + 1], y1 = m.ys[j], y2 = m.ys[j + 1];
+  double x1 = node_x(m, i), x2 = node_x(m, i + 1), y1 = node_y(m, j), y2 = node_y(m, j + 1);
   double hxp = x2 - x1, hyp = y2 - y1;
   double dx = (x - x1) / hxp;
   double dy = (y - y1) / hyp;
@@ -359,7 +365,7 @@ __device__ __forceinline__ void push_select_flush(const SpK &s, SelBuf &b) {
 __device__ __forceinline__ void weights_axi(const MeshK &m, int e, double x, double y, double W[4],
                                             int nodes[4]) {
   int i = elem_column(m, e), j = e - i * m.ney;
-  double x1 = m.xs[i], x2 = m.xs[i + 1], y1 = m.ys[j], y2 = m.ys[j + 1];
+  double x1 = node_x(m, i), x2 = node_x(m, i + 1), y1 = node_y(m, j), y2 = node_y(m, j + 1);
   double dx = (x - x1) / (x2 - x1), xc = 1.0 - dx;
   double beta = (fabs(y1 - m.ymin) < 1e-5) ? 0.75 : 1.0;
   double R1 = m.ymin + y1, R2 = m.ymin + y2;
@@ -3943,6 +3949,7 @@ int pic_init(const pic_mesh_desc *mesh, const pic_params *params) {
   PIC_CUDA(cudaEventCreate(&g.ev0));
   PIC_CUDA(cudaEventCreate(&g.ev1));
   std::vector<double> xs(m.nnx), ys(m.nny);
+  // node_x / node_y (the push) recompute these with the same expression
   for (int i = 0; i < m.nnx; ++i) xs[i] = m.xmin + m.hx * i;
   for (int j = 0; j < m.nny; ++j) ys[j] = m.ymin + m.hy * j;
   if ((rc = upload(&g.d_xs, xs.data(), xs.size()))) return rc;
