@@ -200,6 +200,9 @@ __device__ __forceinline__ bool absorbed_by_object(double x, double y) {
 // .., 2^(k-1) lane i holds the sum over [i, min(i + 2^k - 1, seg_end)], so
 // the steps stop once off reaches the warp's longest run `maxlen` (the same
 // for every lane): a warp of runs of at most 8 takes 3 steps instead of 5.
+constexpr double kNarrowScale = 16777216.0;  // 2^24: the mixed-precision charge's unit
+constexpr int kNarrowShift = 16;             // 2^24 -> 2^40 (PIC_Q_SCALE)
+
 template <int N>
 __device__ __forceinline__ void seg_sums(long long (&v)[N], int lane, int seg_end, int maxlen) {
 #pragma unroll
@@ -209,6 +212,21 @@ __device__ __forceinline__ void seg_sums(long long (&v)[N], int lane, int seg_en
 #pragma unroll
     for (int c = 0; c < N; ++c) {
       const long long o = __shfl_down_sync(0xffffffffu, v[c], off);
+      if (take) v[c] += o;
+    }
+  }
+}
+
+// The same over 32-bit values (the mixed-precision charge, below).
+template <int N>
+__device__ __forceinline__ void seg_sums32(unsigned (&v)[N], int lane, int seg_end, int maxlen) {
+#pragma unroll
+  for (int off = 1; off < 32; off <<= 1) {
+    if (off >= maxlen) break;
+    const bool take = lane + off <= seg_end;
+#pragma unroll
+    for (int c = 0; c < N; ++c) {
+      const unsigned o = __shfl_down_sync(0xffffffffu, v[c], off);
       if (take) v[c] += o;
     }
   }
@@ -225,7 +243,13 @@ __device__ __forceinline__ void seg_sums(long long (&v)[N], int lane, int seg_en
 // warp sum fewer (the oracle rounds the same way).  Without it (the r-z
 // weights, which do not sum to 1 on the axis row) each corner is rounded on
 // its own.
-template <bool CONSERVE = false>
+// NARROW (mixed precision, Cartesian, with CONSERVE): the three corners are
+// rounded to 2^-24 of a particle -- the resolution of the FP32 offsets they
+// come from -- so a warp's sums fit in 32 bits (32 x 2^24 < 2^30): one
+// shuffle and one add a value and step instead of two each; the head scales
+// them to the accumulator's 2^-40 units, and corner 2 keeps every particle's
+// charge exactly 2^40.  The energy deposit stays 64-bit.
+template <bool CONSERVE = false, bool NARROW = false>
 __device__ __forceinline__ void warp_deposit(const SpK &s, int lane, int key, const double W[4], const int nodes[4],
                                              double energy, bool lost, int do_deposit, int do_energy) {
   unsigned int lm = __ballot_sync(0xffffffffu, lost);
@@ -241,9 +265,17 @@ __device__ __forceinline__ void warp_deposit(const SpK &s, int lane, int key, co
       return ((long long)__reduce_add_sync(0xffffffffu, hi) << 24) + (long long)__reduce_add_sync(0xffffffffu, lo);
     };
     long long qv[4];
+    if (NARROW) {
 #pragma unroll
-    for (int c = 0; c < 4; ++c)
-      if (!CONSERVE || c != 2) qv[c] = wsum(__double2ll_rn(W[c] * PIC_Q_SCALE));
+      for (int c = 0; c < 4; ++c)
+        if (c != 2)
+          qv[c] = (long long)__reduce_add_sync(0xffffffffu, (unsigned)__double2uint_rn(W[c] * kNarrowScale))
+                  << kNarrowShift;
+    } else {
+#pragma unroll
+      for (int c = 0; c < 4; ++c)
+        if (!CONSERVE || c != 2) qv[c] = wsum(__double2ll_rn(W[c] * PIC_Q_SCALE));
+    }
     if (CONSERVE) qv[2] = 32ll * (1ll << 40) - ((qv[0] + qv[1]) + qv[3]);
     if (lane == 0)
 #pragma unroll
@@ -263,7 +295,16 @@ __device__ __forceinline__ void warp_deposit(const SpK &s, int lane, int key, co
   int seg_end = above ? (__ffs(above) - 2) : 31;
   const int maxlen = (int)__reduce_max_sync(0xffffffffu, head ? (unsigned)(seg_end - lane + 1) : 0u);
   long long qv[4];
-  if (CONSERVE) {
+  if (NARROW) {
+    unsigned q3[3];
+#pragma unroll
+    for (int c = 0; c < 3; ++c) q3[c] = (key >= 0) ? __double2uint_rn(W[c == 2 ? 3 : c] * kNarrowScale) : 0u;
+    seg_sums32(q3, lane, seg_end, maxlen);
+    qv[0] = (long long)q3[0] << kNarrowShift;
+    qv[1] = (long long)q3[1] << kNarrowShift;
+    qv[3] = (long long)q3[2] << kNarrowShift;
+    qv[2] = (long long)(seg_end - lane + 1) * (1ll << 40) - ((qv[0] + qv[1]) + qv[3]);
+  } else if (CONSERVE) {
     long long q3[3];
 #pragma unroll
     for (int c = 0; c < 3; ++c) q3[c] = (key >= 0) ? __double2ll_rn(W[c == 2 ? 3 : c] * PIC_Q_SCALE) : 0ll;
@@ -711,7 +752,7 @@ __global__ void __launch_bounds__(256, 4) k_push_mixed(MeshK m, const float *__r
       push_mixed_one<AXI>(m, c32, prm, s, p, e, fx[p], fy[p], fvx[p], fvy[p], key, W, nodes, energy, lost);
     }
   }
-  warp_deposit<!AXI>(s, lane, key, W, nodes, energy, lost, prm.do_deposit, prm.do_energy);
+  warp_deposit<!AXI, !AXI>(s, lane, key, W, nodes, energy, lost, prm.do_deposit, prm.do_energy);
   push_select(s, lane, key, p, pid);
 }
 
@@ -804,7 +845,7 @@ __global__ void __launch_bounds__(256, MINB) k_push_mixed_tiled(MeshK m, const f
         push_mixed_one<AXI>(m, c32, prm, s, p, e, C.ax[threadIdx.x], C.ay[threadIdx.x], C.vx[threadIdx.x],
                             C.vy[threadIdx.x], key, W, nodes, energy, lost);
     }
-    warp_deposit<!AXI>(s, lane, key, W, nodes, energy, lost, prm.do_deposit, prm.do_energy);
+    warp_deposit<!AXI, !AXI>(s, lane, key, W, nodes, energy, lost, prm.do_deposit, prm.do_energy);
     push_select(s, lane, key, p, pid);
     __syncthreads();  // tile t is read before its stage is refilled
   }
@@ -1062,7 +1103,7 @@ __global__ void __launch_bounds__(256, MINB) k_push_mixed_bulk(MeshK m, const fl
         push_mixed_one<AXI>(m, c32, prm, s, p, e, C.ax[threadIdx.x], C.ay[threadIdx.x], C.vx[threadIdx.x],
                             C.vy[threadIdx.x], key, W, nodes, energy, lost);
     }
-    warp_deposit<!AXI>(s, lane, key, W, nodes, energy, lost, prm.do_deposit, prm.do_energy);
+    warp_deposit<!AXI, !AXI>(s, lane, key, W, nodes, energy, lost, prm.do_deposit, prm.do_energy);
     push_select_cta(s, key, p, pid, sel_buf);
     __syncthreads();  // tile t is read before its stage is refilled
   }
