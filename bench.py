@@ -62,7 +62,7 @@ MIXED_PUSH_BYTES_RZ = 48
 # mixed k_push_mixed_bulk) and the 2048x1024 r-z deck at 8 (mixed r-z);
 # "_sel": the push also builds the MCC selection (reads the ids)
 NCU_PUSH_TRAFFIC = {"fp64": 68.0, "mixed": 38.0, "mixed_rz": 51.4,
-                    "fp64_sel": 72.2, "mixed_sel": 42.3, "mixed_rz_sel": 55.5}
+                    "fp64_sel": 72.2, "mixed_sel": 42.4, "mixed_rz_sel": 55.5}
 
 
 def _dist():
