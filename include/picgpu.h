@@ -329,6 +329,10 @@ int pic_set_field(int32_t which, const double *host_in);
  * copy (pic_set_field of phi for the phi copy only).  The host arrays must
  * stay valid, and are complete only after pic_wait_fields; they should be
  * page-locked (cudaHostAlloc), or the copies cannot overlap anything.
+ * Copy engines serve one direction in order, whatever the stream, so the
+ * step reads its counters through a mapped page-locked mirror and clears
+ * its accumulators with kernels: these copies, or a caller's own on another
+ * stream, run alongside the step instead of holding its start back.
  * Replaces the synchronous per-field reads the reference's caller does
  * after `IFE_Solve_2D` / `GetEField_SIDG_PPR` (Main_IFE_Test_2.f90:329-341)
  * when it does not need the values before its next step. */

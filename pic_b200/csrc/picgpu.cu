@@ -2864,6 +2864,10 @@ int zero_async(void *p, size_t bytes, cudaStream_t st) {
 
 // counters [first, first + n) (n <= 32) through the mapped mirror, one wait
 static int read_counters(int first, int n, unsigned long long *v) {
+  if (first < 0 || n < 0 || first + n > 32) {
+    set_error("read_counters: counter range outside the 32 counters");
+    return PIC_ERR_ARG;
+  }
   k_counters_out<<<1, 32, 0, g.st>>>(g.hd_counters + first, g.d_counters + first, n);
   PIC_LAUNCHED();
   PIC_CUDA(cudaStreamSynchronize(g.st));
