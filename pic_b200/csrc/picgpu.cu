@@ -51,7 +51,8 @@ struct FieldK {
   const double2 *efxy;  // {efx, efy} per node: the gather's four nodes in four 16-byte loads
 };
 
-__device__ __forceinline__ int locate_elem(const MeshK &m, double x, double y) {
+// ci, cj: the element's column and row (0-based), set when it is found
+__device__ __forceinline__ int locate_elem(const MeshK &m, double x, double y, int &ci, int &cj) {
   // InjectPositioning.f90:13-22: i = INT((x - dxmin)/dx) + 1 (1-based)
   double rxp = (x - m.xmin) / m.hx;
   double ryp = (y - m.ymin) / m.hy;
@@ -60,7 +61,14 @@ __device__ __forceinline__ int locate_elem(const MeshK &m, double x, double y) {
   if (i == m.nnx) i = m.nnx - 1;  // GetParChg_2D.f90:143-149 clamp
   if (j == m.nny) j = m.nny - 1;
   if (!(rxp >= 0.0) || !(ryp >= 0.0) || i < 1 || j < 1 || i > m.nex || j > m.ney) return -1;
+  ci = i - 1;
+  cj = j - 1;
   return (i - 1) * m.ney + (j - 1);
+}
+
+__device__ __forceinline__ int locate_elem(const MeshK &m, double x, double y) {
+  int ci, cj;
+  return locate_elem(m, x, y, ci, cj);
 }
 
 // e / ney without a division: with M = floor(2^32 / ney) + 1, umulhi(e, M)
@@ -78,9 +86,9 @@ __device__ __forceinline__ int elem_column(const MeshK &m, int e) {
 __device__ __forceinline__ double node_x(const MeshK &m, int i) { return m.xmin + m.hx * (double)i; }
 __device__ __forceinline__ double node_y(const MeshK &m, int j) { return m.ymin + m.hy * (double)j; }
 
-__device__ __forceinline__ void bilinear(const MeshK &m, int e, double x, double y, double W[4],
-                                         int nodes[4], int *ie, int *je) {
-  int i = elem_column(m, e), j = e - i * m.ney;
+// bilinear weights and nodes of the element in column i, row j
+__device__ __forceinline__ void bilinear_ij(const MeshK &m, int i, int j, double x, double y, double W[4],
+                                            int nodes[4]) {
   double x1 = node_x(m, i), x2 = node_x(m, i + 1), y1 = node_y(m, j), y2 = node_y(m, j + 1);
   double hxp = x2 - x1, hyp = y2 - y1;
   double dx = (x - x1) / hxp;
@@ -95,6 +103,12 @@ __device__ __forceinline__ void bilinear(const MeshK &m, int e, double x, double
   nodes[1] = n1 + m.nny;
   nodes[2] = n1 + m.nny + 1;
   nodes[3] = n1 + 1;
+}
+
+__device__ __forceinline__ void bilinear(const MeshK &m, int e, double x, double y, double W[4],
+                                         int nodes[4], int *ie, int *je) {
+  int i = elem_column(m, e), j = e - i * m.ney;
+  bilinear_ij(m, i, j, x, y, W, nodes);
   *ie = i;
   *je = j;
 }
@@ -434,7 +448,8 @@ template <bool AXI>
 __device__ __forceinline__ void push_fp64_one(const MeshK &m, const FieldK &f, const PushK &prm, const SpK &s,
                                               int64_t p, int e, double x, double y, double vx, double vy,
                                               int &key, double W[4], int nodes[4], double &energy, bool &lost) {
-  int en = -2;  // the new element, once located
+  int en = -2;          // the new element, once located
+  int ci = 0, cj = 0;   // and its column and row
   if (prm.do_push) {
     int ie, je;
     bilinear(m, e, x, y, W, nodes, &ie, &je);
@@ -498,7 +513,7 @@ __device__ __forceinline__ void push_fp64_one(const MeshK &m, const FieldK &f, c
     // bounding box (a flag built at init, with a cell of margin) can be
     // inside one, so the exact test runs there only
     if (!lost) {
-      en = locate_elem(m, x, y);
+      en = locate_elem(m, x, y, ci, cj);
       if ((en < 0 || m.elem_near[en]) && absorbed_by_object(x, y)) lost = true;
     }
     s.x[p] = x;
@@ -509,7 +524,7 @@ __device__ __forceinline__ void push_fp64_one(const MeshK &m, const FieldK &f, c
   if (lost) {
     s.loc[p] = -1;
   } else if (prm.do_deposit) {
-    if (en == -2) en = locate_elem(m, x, y);
+    if (en == -2) en = locate_elem(m, x, y, ci, cj);
     if (en < 0) {
       atomicAdd(s.bad, 1ull);
       s.loc[p] = -1;
@@ -520,8 +535,7 @@ __device__ __forceinline__ void push_fp64_one(const MeshK &m, const FieldK &f, c
       if (AXI) {
         weights_axi(m, en, x, y, W, nodes);
       } else {
-        int ie, je;
-        bilinear(m, en, x, y, W, nodes, &ie, &je);
+        bilinear_ij(m, ci, cj, x, y, W, nodes);
       }
       if (prm.do_energy) {  // the per-node energy is deposited on diagnostic steps only
         const double vz = s.vz[p];
